@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Zone-updates/s of the per-stage hot path (reconstruction -> Riemann -> flux
+divergence -> SSP-RK stage update with the CFL max-reduction) on B200.
+
+Headline workload: 3D Euler spherical Sod blast, 256^3 cells on [0,1]^3, outflow,
+gamma=1.4, kernel-based WENO-AO radius 2 with the KXRCF selector, HLLC, SSP(4,3)
+with the adaptive FSAL controller, CFL 0.8, plain FP64.  One "step" is one accepted
+time step (4 RHS evaluations + stage updates + error estimate) of the whole grid;
+one zone-update is one cell advanced by one accepted step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank advances an independent replica of the grid
+(the path has no cross-GPU exchange in this scope); value is the total over ranks
+divided by the slowest rank's device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "kfvm-kokkos_b200"))
+
+import kfvm_abi as abi  # noqa: E402
+
+METRIC = "zone-updates/s on 1 B200 (3D Euler Sod blast 256^3, plain FP64)"
+UNIT = "zone-updates/s"
+WORKLOAD = "sod3d"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=int, default=256, help="grid cells per axis")
+    p.add_argument("--e2e-steps", type=int, default=4)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def config_block(scale, extra=None):
+    c = {"workload": f"3D Euler spherical Sod blast {scale}^3, outflow, GP-WENO-AO r=2 + KXRCF, "
+                     "HLLC, SSP(4,3) FSAL adaptive, CFL 0.8, FP64",
+         "grid": [scale, scale, scale], "cells": scale ** 3,
+         "l2": "inputs larger than L2 (state + face arrays ~GBs >> 126 MB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ roofline
+def algorithmic_bytes(cls, cfg):
+    """Algorithmic HBM bytes per launch of each kernel class (8-byte reals;
+    stencil and halo re-reads are not counted)."""
+    n = abi.ncells(cfg)
+    nv = abi.nvars(cfg)
+    d = cfg.dim
+    nqf = 2 if d == 2 else 4
+    nf = 2 * d
+    nfaces = sum((cfg.nx + (k == 0)) * (cfg.ny + (k == 1)) * ((cfg.nz if d == 3 else 1) + (k == 2))
+                 for k in range(d))
+    per_cell = {
+        "select": nv * 8 + nf * nqf * 8,                  # U in, indicator per own face point out
+        "flag": 2 * nf * nqf * 8 + nv * 8 + 8 + 1,        # indicators both sides, U, theta, flag
+        "recon": nv * 8 + nf * nqf * nv * 8 + 8 + 2,       # U in, own face states out, theta, flags
+        "stage": (d * nv + 4 * nv) * 8,                   # fluxes, U, Uprev, Uhat in; U', Uhat out
+        "bc_fill": 0,
+    }
+    if cls == "riemann":
+        return nfaces * (2 * nqf * nv * 8 + nv * 8) / d   # per launch (one direction)
+    return per_cell.get(cls, 0) * n
+
+
+def load_json(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+    import kfvm
+
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    kfvm.lib()  # raises if the CUDA library is missing: no CPU fallback
+
+    cfg, ic = abi.workload(WORKLOAD, scale=args.scale, steps=args.warmup + args.steps + 10)
+    solver = kfvm.Solver(cfg)
+    solver.init_ic(ic)
+    n = abi.ncells(cfg)
+    nv = abi.nvars(cfg)
+    for _ in range(args.warmup):
+        solver.take_step()
+
+    stream = torch.cuda.ExternalStream(solver.stream_handle())
+    solver.set_timing(True)
+    launches0 = solver.launch_count()
+    sampler = ClockSampler(local)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    accepted = 0
+    attempts = 0
+    nweno = []
+    for _ in range(args.steps):
+        info = solver.take_step()
+        accepted += info.accepted
+        attempts += info.attempts
+        nweno.append(info.n_weno)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    sampler.stop()
+    ms = e0.elapsed_time(e1)
+    launches = solver.launch_count() - launches0
+    per_class = solver.timing()
+    solver.set_timing(False)
+
+    # max over ranks of the device time, sum of the work
+    t_max, work = ms, accepted * n
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        w = torch.tensor([float(work)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(w, op=dist.ReduceOp.SUM)
+        t_max, work = t.item(), w.item()
+    value = work / (t_max / 1e3)
+
+    # end to end through the public API with host buffers: per step upload the
+    # state from pinned host memory (set_state primes the FSAL stage), one
+    # TakeStep, read the state back
+    host = torch.empty((nv, n), dtype=torch.float64, pin_memory=True).numpy()
+    solver.get_state(host)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    e2e_acc = 0
+    for _ in range(args.e2e_steps):
+        solver.set_state(host)
+        info = solver.take_step()
+        e2e_acc += info.accepted
+        solver.get_state(host)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_work = e2e_acc * n
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        w = torch.tensor([float(e2e_work)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(w, op=dist.ReduceOp.SUM)
+        e2e_s, e2e_work = t.item(), w.item()
+    e2e = {"value": e2e_work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(nv * n * 8),
+           "d2h_bytes_per_step": int(nv * n * 8),
+           "how": "per step: kfvm_set_state from pinned host (re-primes FSAL), kfvm_take_step, "
+                  "kfvm_get_state to pinned host; wall clock"}
+
+    # roofline of the dominant kernel class
+    peaks = load_json(os.path.join(ROOT, "MEASURED_PEAKS.json"))
+    hbm_peak = peaks.get("hbm_gbs") if peaks else 6650.0
+    peak_src = "measured" if peaks else "fallback"
+    dom = max((k for k in per_class if per_class[k][1] > 0), key=lambda k: per_class[k][0])
+    dom_ms, dom_n = per_class[dom]
+    avg_ms = dom_ms / max(dom_n, 1)
+    algo = algorithmic_bytes(dom, cfg)
+    achieved = algo / (avg_ms / 1e3) / 1e9
+    traffic_tbl = load_json(os.path.join(ROOT, "profiles", "dram_traffic.json")) or {}
+    traffic = traffic_tbl.get(dom, {}).get("bytes_per_launch_at_256") if args.scale == 256 else None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
+                "peak_source": peak_src,
+                "note": "FP64 plain form is FP64-pipe bound, not HBM bound; see fp64 below"}
+    share = {k: round(v[0] / max(sum(x[0] for x in per_class.values()), 1e-9), 4)
+             for k, v in per_class.items() if v[1] > 0}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (analytic initial condition)",
+           "config": config_block(args.scale, {"parallelism": f"replicas x{ws}",
+                                               "accepted_steps": accepted, "attempts": attempts,
+                                               "weno_cells_last": nweno[-1] if nweno else None}),
+           "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+           "kernel_share": share,
+           "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0}}
+    out["clocks"] = sampler.summary()
+
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(sample_scale=64, sample_steps=1)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    solver.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------ CPU arms
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.lib()
+    return oracle
+
+
+def cpu_baseline(sample_scale, sample_steps, warmup=0):
+    """The oracle (CPU restatement of the reference path, OpenMP over cells) timed
+    on the host cores on a bounded sample of the workload."""
+    oracle = _oracle()
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    cfg, ic = abi.workload(WORKLOAD, scale=sample_scale, steps=sample_steps + warmup + 2)
+    s = oracle.OracleSolver(cfg)
+    s.init_ic(ic)
+    for _ in range(warmup):
+        s.take_step()
+    t0 = time.perf_counter()
+    acc = 0
+    for _ in range(sample_steps):
+        acc += s.take_step().accepted
+    dt = time.perf_counter() - t0
+    n = abi.ncells(cfg)
+    return {"value": acc * n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{sample_steps} accepted step(s) of the same problem on a {sample_scale}^3 grid "
+                      f"({acc * n} zone-updates in {dt:.1f} s)"}
+
+
+def run_reference(args):
+    ws, rank, local = dist_init()
+    if rank != 0:
+        return
+    oracle = _oracle()
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    sample = 48
+    cfg, ic = abi.workload(WORKLOAD, scale=sample, steps=args.warmup + args.steps + 2)
+    s = oracle.OracleSolver(cfg)
+    s.init_ic(ic)
+    for _ in range(args.warmup):
+        s.take_step()
+    t0 = time.perf_counter()
+    acc = 0
+    for _ in range(args.steps):
+        acc += s.take_step().accepted
+    dt = time.perf_counter() - t0
+    n = abi.ncells(cfg)
+    value = acc * n / dt
+    desc = (f"each step: one accepted time step of the same problem on a {sample}^3 grid "
+            f"(the reference build is unavailable here; this is the CPU restatement of its path)")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (analytic initial condition)",
+           "config": config_block(args.scale, {"sample_grid": [sample] * 3}),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                            "sample": desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,225 @@
+/*
+ * kfvm_b200.h -- C ABI of the B200-native per-stage hot path of the KFVM
+ * finite-volume solver (kernel-based WENO-AO reconstruction, HLLC/HLL Riemann
+ * fluxes, flux divergence, low-storage SSP-RK stage update with the CFL
+ * max-reduction), for one rank on one GPU.
+ *
+ * The reference has no FFI: its operator boundary is the C++ Solver class and
+ * the Stencil weight object.  Each entry point below names the reference member
+ * function it replaces (path within the reference project, file:line).  All
+ * entry points take plain pointers and sizes, return 0 on success and a
+ * negative KFVM_ERR_* code on failure, never abort, and never throw.
+ *
+ * State exchange format ("SoA interior"): double[NV][nz][ny][nx], x fastest,
+ * interior cells only (no halo).  nz == 1 in 2D.  The conserved-variable order
+ * is the reference's (src/physics/SimVar.H:12-66):
+ *   Euler / Navier-Stokes: dens, momx, momy, momz, etot            (NV = 5)
+ *   GLM-MHD:               dens, momx, momy, momz, etot,
+ *                          magx, magy, magz, psi                    (NV = 9)
+ */
+#ifndef KFVM_B200_H_
+#define KFVM_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enumerations (values match the reference's enums) ------------------ */
+
+/* src/physics/EquationTypes.H:8-16 */
+enum kfvm_eq { KFVM_EQ_HYDRO = 0, KFVM_EQ_NAVIERSTOKES = 1, KFVM_EQ_MHD_GLM = 2 };
+/* src/physics/RSTypes.H:6 */
+enum kfvm_rs { KFVM_RS_LLF = 0, KFVM_RS_HLL = 1, KFVM_RS_HLLC = 2 };
+/* src/numeric/RKTypes.H:6 (SSP4_3_2 is the only third-order SSP method there) */
+enum kfvm_rk {
+  KFVM_RK_THREESTARP = 0,
+  KFVM_RK_FOURSTARP = 1,
+  KFVM_RK_SSP4_3_2 = 2,
+  KFVM_RK_SSP10_4_3 = 3
+};
+/* src/Types.H:37 */
+enum kfvm_bc { KFVM_BC_PERIODIC = 0, KFVM_BC_OUTFLOW = 1 };
+/* src/Types.H:40 */
+enum kfvm_ts_status { KFVM_TS_ACCEPTED = 0, KFVM_TS_TOLERANCE = 1, KFVM_TS_UNPHYSICAL = 2 };
+/* Troubled-cell indicator choice.  KXRCF is the reference's selector
+ * (src/numeric/Numeric_K.H:292-398); ALL forces full WENO on every cell
+ * (the reference's wenothresh < 0 path); NONE never flags (linear only). */
+enum kfvm_indicator { KFVM_IND_KXRCF = 0, KFVM_IND_ALL = 1, KFVM_IND_NONE = 2 };
+/* Initial conditions built into the library (cell averages by Q^d Gauss
+ * quadrature, src/numeric/Numeric_K.H:31-107). */
+enum kfvm_ic {
+  KFVM_IC_ISENTROPIC_VORTEX = 0, /* 2D Euler, rho=u=v=p=1 + Shu vortex beta=5   */
+  KFVM_IC_SPHERICAL_SOD = 1,     /* 3D Euler, rho,p = 1,1 in r<0.2 else .125,.1 */
+  KFVM_IC_KELVIN_HELMHOLTZ = 2,  /* 2D Euler shear layer + seeded noise         */
+  KFVM_IC_TAYLOR_GREEN = 3,      /* 3D Navier-Stokes Taylor-Green vortex        */
+  KFVM_IC_ORSZAG_TANG = 4,       /* 2D GLM-MHD Orszag-Tang vortex               */
+  KFVM_IC_SMOOTH_WAVE = 5        /* any dim/eq: smooth density/velocity wave     */
+};
+
+/* ---- error codes -------------------------------------------------------- */
+#define KFVM_OK 0
+#define KFVM_ERR_ARG (-1)      /* bad argument / unsupported configuration   */
+#define KFVM_ERR_CUDA (-2)     /* a CUDA runtime call failed                 */
+#define KFVM_ERR_LAPACK (-3)   /* dgetrf/dgetrs reported a singular system   */
+#define KFVM_ERR_NOMEM (-4)    /* device or host allocation failed           */
+#define KFVM_ERR_STATE (-5)    /* call out of order (e.g. step before IC)    */
+
+/* ---- sizes -------------------------------------------------------------- */
+#define KFVM_RAD 2          /* stencil radius (STENCIL_RADIUS)                 */
+#define KFVM_MAX_CELLS 33   /* nCellsFull for r=2 in 3D (StencilInfo.H:69-84)  */
+#define KFVM_MAX_SUB 8      /* nSub in 3D                                      */
+#define KFVM_MAX_BIAS 6     /* nBias in 3D                                     */
+#define KFVM_MAX_BCELLS 11  /* nCellsBias in 3D                                */
+#define KFVM_MAX_INDIC 19   /* nIndic in 3D                                    */
+#define KFVM_MAX_NQ 3       /* NUM_QUAD_PTS supported by the weight precompute */
+#define KFVM_MAX_FACEQ 9    /* NQ^(d-1)                                        */
+#define KFVM_MAX_CELLQ 27   /* NQ^d                                            */
+
+/* Run configuration: the union of the reference's compile-time Definitions.H
+ * choices and its run-time .init settings (src/ProblemSetup.H:26-82,
+ * src/ParameterStructs.H:21-40).  Reals read from an .init file must already be
+ * rounded through float, as std::stof does in the reference. */
+typedef struct kfvm_config {
+  int32_t dim;        /* SPACE_DIM: 2 or 3                                   */
+  int32_t eq;         /* enum kfvm_eq                                        */
+  int32_t rs;         /* enum kfvm_rs                                        */
+  int32_t rk;         /* enum kfvm_rk                                        */
+  int32_t nq;         /* NUM_QUAD_PTS (GPU path: 2)                          */
+  int32_t indicator;  /* enum kfvm_indicator                                 */
+  int64_t nx, ny, nz; /* interior cells (nz = 1 in 2D)                       */
+  double xlo, xup, ylo, yup, zlo, zup;
+  int32_t bc[6];      /* enum kfvm_bc for west,east,south,north,bottom,top   */
+  double gamma, reynolds, prandtl;
+  double weno_thresh; /* eos:wenothresh; < 0 forces full WENO everywhere     */
+  double lfac;        /* stencil:lfac (SE kernel length scale in cells)      */
+  double cfl, atol, rtol, rejection_thresh, min_dt, final_time;
+  int32_t rejection_limit;
+  int32_t max_steps;  /* time:maxsteps (the stepping loop starts at nTS=1)   */
+  int32_t have_sources; /* forced on for MHD_GLM (ProblemSetup.H:81)        */
+  int32_t pad_;
+} kfvm_config;
+
+/* Precomputed stencil (the reference's Stencil object, src/stencil/Stencil.H:54-146).
+ * Array shapes follow the reference's views with fixed maximum extents:
+ *   off[3][C]                      lOff, tOff, ttOff
+ *   sub_idx[nBias][nCellsBias]      subIdx
+ *   face_w[nSub][2d][NQF][C]        faceWeights (zero-padded past each substencil)
+ *   cell_w[nSub][NQ^d][C]           cellWeights, point index = ((qx*NQ)+qy)*NQz+qz
+ *   deriv_w[nSub][nIndic][C]        derivWeights (already scaled by dx^px dy^py dz^pz) */
+typedef struct kfvm_stencil {
+  int32_t dim, nq;
+  int32_t n_cells, n_cells_ctr, n_cells_bias, n_sub, n_bias, n_indic, nqf, nqc;
+  int64_t off[3][KFVM_MAX_CELLS];
+  int64_t sub_idx[KFVM_MAX_BIAS][KFVM_MAX_BCELLS];
+  double face_w[KFVM_MAX_SUB][6][KFVM_MAX_FACEQ][KFVM_MAX_CELLS];
+  double cell_w[KFVM_MAX_SUB][KFVM_MAX_CELLQ][KFVM_MAX_CELLS];
+  double deriv_w[KFVM_MAX_SUB][KFVM_MAX_INDIC][KFVM_MAX_CELLS];
+} kfvm_stencil;
+
+/* Outcome of one TakeStep (src/Solver.cpp:188-343). */
+typedef struct kfvm_step_info {
+  double time;       /* simulation time after the step                     */
+  double dt;         /* next time step size                                */
+  double dt_taken;   /* size of the accepted step (0 if none was accepted) */
+  double max_vel;    /* max wave speed seen in the accepted attempt        */
+  double err_est;    /* errNew of the accepted attempt                     */
+  int32_t status;    /* enum kfvm_ts_status of the last attempt            */
+  int32_t attempts;  /* attempts made (<= rejection_limit)                 */
+  int32_t accepted;  /* 1 if a step was accepted                           */
+  int32_t last_step; /* 1 if the solver decided to stop                    */
+  int64_t n_weno;    /* cells sent to WENO in the last RHS evaluation      */
+  int64_t n_rhs;     /* total RHS evaluations so far                       */
+} kfvm_step_info;
+
+typedef struct kfvm_solver kfvm_solver;
+
+/* Fills a config with the reference's defaults (ProblemSetup.H:72-82,
+ * ParameterStructs.H:37). */
+void kfvm_default_config(kfvm_config *cfg);
+
+/* Stencil geometry and reconstruction weights, host FP64, LU by LAPACK
+ * dgetrf/dgetrs.  Replaces Stencil::Stencil(lfac, geom)
+ * (src/stencil/Stencil.H:105-135) -> Core::findStencil (Stencil.cpp:47-156),
+ * findSubStencils (Stencil.cpp:158-229), findWeights (Stencil.cpp:281-846). */
+int kfvm_stencil_build(const kfvm_config *cfg, kfvm_stencil *out);
+
+/* Allocates all device state for one solver.  Replaces the allocation part of
+ * Solver::Solver (src/Solver.cpp:36-81).  Uses the current CUDA device. */
+int kfvm_create(const kfvm_config *cfg, kfvm_solver **out);
+void kfvm_destroy(kfvm_solver *s);
+
+/* Fills U (and Uprev) with a built-in initial condition, evaluates the first
+ * RHS to prime the FSAL stepper and picks dt = 0.01 cfl dmin / maxVel.
+ * Replaces Solver::setIC (src/Solver.cpp:1948-1963) and the tail of
+ * Solver::Solver (src/Solver.cpp:73-80).  seed feeds KFVM_IC_KELVIN_HELMHOLTZ. */
+int kfvm_init_ic(kfvm_solver *s, int32_t ic_kind, uint64_t seed);
+
+/* Sets U = Uprev = host state (SoA interior), then primes FSAL as above. */
+int kfvm_set_state(kfvm_solver *s, const double *u_host);
+/* Copies U (SoA interior) to the host. */
+int kfvm_get_state(kfvm_solver *s, double *u_host);
+
+/* One RHS evaluation on the current U at time t.  Replaces
+ * Solver::evalRHS(U_halo, t) (src/Solver.cpp:410-530): cell BCs, linear
+ * reconstruction, KXRCF selection, sparse/full WENO, positivity limiter, face
+ * BCs, GLM speed and sources, Riemann fluxes with the max-speed reduction,
+ * flux divergence and viscous terms.  rhs_host (nullable) receives the RHS in
+ * SoA interior layout; max_vel (nullable) the max wave speed. */
+int kfvm_eval_rhs(kfvm_solver *s, double t, double *rhs_host, double *max_vel);
+
+/* One adaptive FSAL time step.  Replaces Solver::TakeStep (src/Solver.cpp:188-343). */
+int kfvm_take_step(kfvm_solver *s, kfvm_step_info *info);
+
+/* Steps until max_steps / final_time / stagnation, like the loop of
+ * Solver::Solve (src/Solver.cpp:84-140) without I/O.  n_steps_out (nullable)
+ * receives the number of accepted steps. */
+int kfvm_solve(kfvm_solver *s, int32_t max_steps, int64_t *n_steps_out,
+               kfvm_step_info *last);
+
+/* Current simulation time and dt (Solver::time, Solver::dt). */
+int kfvm_get_time(kfvm_solver *s, double *time, double *dt);
+
+/* Selects the troubled-cell indicator (enum kfvm_indicator). */
+int kfvm_set_indicator(kfvm_solver *s, int32_t indicator);
+
+/* Inspection of the last RHS evaluation, for parity tests:
+ * face states after the positivity limiter and face BCs, before the Riemann
+ * solve, in layout double[2 slots][NQF][NV][nfz][nfy][nfx] where (nfx,nfy,nfz)
+ * is the face grid of direction dir (nx+1,ny,nz for x, ...).  Slot 0 is the
+ * minus (left) state, slot 1 the plus (right) state, as in FaceDataView
+ * (src/Types.H:73,87-88). */
+int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out_host);
+/* Per-cell WENO flags of the last RHS evaluation (1 = WENO reconstruction was
+ * applied to the cell) and positivity theta (wenoFlag(.,1)); either pointer may
+ * be null.  Layout [nz][ny][nx]. */
+int kfvm_get_flags(kfvm_solver *s, uint8_t *weno_applied, double *theta);
+
+/* Device time of the last kfvm_take_step call, for measurement (ms). */
+int kfvm_last_stage_ms(kfvm_solver *s, double *ms);
+
+/* Measurement support (no counterpart in the reference, which has no timers).
+ * kfvm_get_stream: the cudaStream_t (as void*) all work of this solver runs on.
+ * kfvm_set_timing: when on, CUDA events bracket every kernel class and the device
+ *   time of each class accumulates; kfvm_get_timing copies the per-class totals
+ *   (ms) and launch counts for the classes listed by KFVM_KCLASS_*.
+ * kfvm_get_launch_count: kernels launched by this solver since creation. */
+enum kfvm_kernel_class {
+  KFVM_KCLASS_BC = 0, KFVM_KCLASS_SELECT = 1, KFVM_KCLASS_FLAG = 2, KFVM_KCLASS_RECON = 3,
+  KFVM_KCLASS_HEAVY = 4, KFVM_KCLASS_RIEMANN = 5, KFVM_KCLASS_STAGE = 6, KFVM_KCLASS_OTHER = 7,
+  KFVM_NUM_KCLASS = 8
+};
+int kfvm_get_stream(kfvm_solver *s, void **stream);
+int kfvm_set_timing(kfvm_solver *s, int32_t on);
+int kfvm_get_timing(kfvm_solver *s, double *ms_per_class, int64_t *launches_per_class);
+int kfvm_get_launch_count(kfvm_solver *s, int64_t *launches);
+
+/* Human-readable text for the last error on this thread. */
+const char *kfvm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KFVM_B200_H_ */

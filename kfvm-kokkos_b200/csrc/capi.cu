@@ -1,0 +1,827 @@
+// capi.cu -- the C ABI (include/kfvm_b200.h): solver context, device memory,
+// the per-stage launch sequence (Solver::evalRHS) and the adaptive FSAL time
+// stepper (Solver::TakeStep) of slug-cfd/kfvm-kokkos, src/Solver.cpp:36-530.
+//
+// Host control flow stays on the host, as in the reference: one stream per
+// solver, one device->host read per step attempt (max speed, error sum,
+// positivity minimum) instead of the reference's per-stage reads.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/kfvm_b200.h"
+#include "kernels.cuh"
+#include "launch.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(KFVM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+// RK coefficient tables (src/numeric/Numeric.H:111-203)
+struct RKTable {
+  int nStages;
+  double gam1[10], gam2[10], gam3[10], delta[10], beta[10], bhat[10], c[10];
+  double bhatfsal, ep1, ep2;
+  bool use_tmp;
+};
+
+bool rk_table(int rk, RKTable &r) {
+  std::memset(&r, 0, sizeof(r));
+  if (rk == KFVM_RK_SSP4_3_2) {
+    // SSP(4,3) of Kraaijevanger with the embedded pair and PI values of Conde et al.
+    r.nStages = 4;
+    const double g1[] = {0.0, 1.0, 1.0 / 3.0, 1.0}, g3[] = {0.0, 0.0, 2.0 / 3.0, 0.0};
+    const double be[] = {1.0 / 2.0, 1.0 / 2.0, 1.0 / 6.0, 1.0 / 2.0};
+    const double cc[] = {0.0, 1.0 / 2.0, 1.0, 1.0 / 2.0};
+    for (int i = 0; i < 4; i++) {
+      r.gam1[i] = g1[i];
+      r.gam3[i] = g3[i];
+      r.beta[i] = be[i];
+      r.bhat[i] = 1.0 / 4.0;
+      r.c[i] = cc[i];
+    }
+    r.bhatfsal = 0.0;
+    r.ep1 = 0.8 / 3.0;
+    r.ep2 = -0.31 / 3.0;
+  } else if (rk == KFVM_RK_THREESTARP) {
+    // third-order adaptive method of Ranocha et al.
+    r.nStages = 5;
+    const double g1[] = {0.0, 2.587771979725733308135192812685323706e-01,
+                         -1.324380360140723382965420909764953437e-01,
+                         5.056033948190826045833606441415585735e-02,
+                         5.670532000739313812633197158607642990e-01};
+    const double g2[] = {0.0, 5.528354909301389892439698870483746541e-01,
+                         6.731871608203061824849561782794643600e-01,
+                         2.803103963297672407841316576323901761e-01,
+                         5.521525447020610386070346724931300367e-01};
+    const double g3[] = {0.0, 0.0, 0.0, 2.752563273304676380891217287572780582e-01,
+                         -8.950526174674033822276061734289327568e-01};
+    const double de[] = {1.0, 3.407655879334525365094815965895763636e-01,
+                         3.414382655003386206551709871126405331e-01,
+                         7.229275366787987419692007421895451953e-01, 0.0};
+    const double be[] = {2.300298624518076223899418286314123354e-01,
+                         3.021434166948288809034402119555380003e-01,
+                         8.025606185416310937583009085873554681e-01,
+                         4.362158943603440930655148245148766471e-01,
+                         1.129272530455059129782111662594436580e-01};
+    const double bh[] = {9.484166705035703392326247283838082847e-02,
+                         1.726371339430353766966762629176676070e-01,
+                         3.998243189084371024483169698618455770e-01,
+                         1.718016807580178450618829007973835152e-01,
+                         5.881914422155740300718268359027168467e-02};
+    const double cc[] = {0.0, 2.300298624518076223899418286314123354e-01,
+                         4.050046072094990912268498160116125481e-01,
+                         8.947822893693433545220710894560512805e-01,
+                         7.235136928826589010272834603680114769e-01};
+    for (int i = 0; i < 5; i++) {
+      r.gam1[i] = g1[i];
+      r.gam2[i] = g2[i];
+      r.gam3[i] = g3[i];
+      r.delta[i] = de[i];
+      r.beta[i] = be[i];
+      r.bhat[i] = bh[i];
+      r.c[i] = cc[i];
+    }
+    r.bhatfsal = 1.020760551185952388626787099944507877e-01;
+    r.ep1 = 0.7 / 3.0;
+    r.ep2 = -0.23 / 3.0;
+  } else {
+    return false;
+  }
+  for (int i = 0; i < r.nStages; i++) r.use_tmp = r.use_tmp || r.delta[i] != 0.0 || r.gam2[i] != 0.0;
+  return true;
+}
+
+// The linear weights live in the constant bank, one set per (device, dimension).
+// They depend only on lfac, so solvers that share a device and dimension must
+// share lfac; the registry counts the live solvers of each slot.
+struct WeightSlot {
+  double lfac = 0.0;
+  int users = 0;
+};
+std::mutex g_slot_mu;
+std::map<std::pair<int, int>, WeightSlot> g_slots;
+
+} // namespace
+
+struct kfvm_solver {
+  kfvm_config cfg;
+  kfvm::Grid g;
+  int dim, eq, nv;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  kfvm::DevStencil *dS = nullptr;
+  double *Ub[3] = {nullptr, nullptr, nullptr};
+  int iPrev = 0; // buffer holding Uprev; the other two alternate within a step
+  int iCur = 0;  // buffer holding the current state U
+  double *Uhat = nullptr, *Utmp = nullptr, *K = nullptr;
+  double *F[3] = {nullptr, nullptr, nullptr}, *G[3] = {nullptr, nullptr, nullptr};
+  double *src = nullptr, *theta = nullptr, *part = nullptr;
+  uint8_t *flag = nullptr, *wset = nullptr, *applied = nullptr;
+  uint32_t *heavy = nullptr; // compacted WENO / limiter cell list (one slot per cell)
+  int heavyBlocks = 0;
+  kfvm::DevScalars *sc = nullptr;
+  kfvm::DevScalars *hsc = nullptr; // pinned host copy
+  RKTable rk;
+  double time = 0.0, dt = 0.0, errEst = 1.0;
+  bool lastTimeStep = false, useSparseWeno = true, primed = false;
+  int indicator = KFVM_IND_KXRCF;
+  int64_t nRhs = 0, nWenoLast = 0;
+  int nTS = 1;
+  double dmin = 0.0;
+  float lastMs = 0.0f;
+  int device = -1; // device holding this solver's constant-bank weights slot
+  // measurement: kernel launches, optional per-class event timing
+  int64_t launches = 0;
+  bool timing = false;
+  struct Mark {
+    int cls;
+    cudaEvent_t a, b;
+  };
+  std::vector<Mark> marks;    // recorded since the last harvest
+  std::vector<cudaEvent_t> evPool;
+  double clsMs[KFVM_NUM_KCLASS] = {0};
+  int64_t clsLaunches[KFVM_NUM_KCLASS] = {0};
+};
+
+namespace {
+
+int set_err_cuda(cudaError_t e, const char *what) {
+  return fail(KFVM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+cudaEvent_t pool_event(kfvm_solver *s) {
+  if (!s->evPool.empty()) {
+    cudaEvent_t e = s->evPool.back();
+    s->evPool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// run one launcher; count its kernels and, when timing, bracket it with events
+template <class Fn>
+cudaError_t run(kfvm_solver *s, int cls, int nKernels, Fn &&fn) {
+  kfvm_solver::Mark m{cls, nullptr, nullptr};
+  if (s->timing) {
+    m.a = pool_event(s);
+    m.b = pool_event(s);
+    cudaEventRecord(m.a, s->stream);
+  }
+  cudaError_t e = fn();
+  s->launches += nKernels;
+  s->clsLaunches[cls] += nKernels;
+  if (s->timing) {
+    cudaEventRecord(m.b, s->stream);
+    s->marks.push_back(m);
+  }
+  return e;
+}
+
+// accumulate the recorded kernel-class times (after the stream was synchronised)
+void harvest(kfvm_solver *s) {
+  for (auto &m : s->marks) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, m.a, m.b) == cudaSuccess) s->clsMs[m.cls] += ms;
+    s->evPool.push_back(m.a);
+    s->evPool.push_back(m.b);
+  }
+  s->marks.clear();
+}
+
+// one RHS evaluation on buffer b: BCs, selection, reconstruction, Riemann fluxes.
+// The caller launches the stage kernel that consumes the fluxes.
+int eval_front(kfvm_solver *s, int b) {
+  using namespace kfvm;
+  s->nRhs++;
+  cudaStream_t st = s->stream;
+  const int dim = s->dim, eq = s->eq;
+  cudaError_t e;
+  if ((e = run(s, KFVM_KCLASS_BC, 1, [&] { return launch_bc(dim, eq, s->Ub[b], s->g, st); })) != cudaSuccess)
+    return set_err_cuda(e, "bc");
+  // reset the per-evaluation counters (nflag, napplied, nheavy) and the GLM maxima
+  CK(cudaMemsetAsync(&s->sc->glm_lam_bits, 0, 2 * sizeof(unsigned long long) + 4 * sizeof(unsigned), st));
+  int mode;
+  if (s->indicator == KFVM_IND_NONE) {
+    mode = RECON_LINEAR;
+  } else if (s->useSparseWeno) {
+    mode = RECON_SPARSE;
+    const double thr = s->cfg.weno_thresh * std::pow(s->dmin, 1.5);
+    if ((e = run(s, KFVM_KCLASS_SELECT, 1, [&] { return launch_select(dim, eq, s->Ub[b], s->g, s->F, st); })) !=
+        cudaSuccess)
+      return set_err_cuda(e, "select");
+    if ((e = run(s, KFVM_KCLASS_FLAG, 1, [&] {
+           return launch_flag(dim, eq, s->Ub[b], s->g, s->F, s->theta, s->flag, s->sc, thr, st);
+         })) != cudaSuccess)
+      return set_err_cuda(e, "flag");
+  } else {
+    mode = RECON_FULL;
+    // after a full-WENO evaluation the sparse mode is allowed again (Solver.cpp:439-443)
+    s->useSparseWeno = s->cfg.weno_thresh > 0.0 && s->indicator == KFVM_IND_KXRCF;
+  }
+  if ((e = run(s, KFVM_KCLASS_RECON, 1, [&] {
+         return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, mode, s->flag, s->wset, s->applied, s->theta,
+                             s->F, s->src, s->heavy, s->sc, s->heavyBlocks, st);
+       })) != cudaSuccess)
+    return set_err_cuda(e, "recon");
+  if ((e = run(s, KFVM_KCLASS_HEAVY, 1, [&] {
+         return launch_heavy(dim, eq, s->Ub[b], s->g, s->dS, s->theta, s->F, s->src, s->heavy, s->sc,
+                             s->heavyBlocks, st);
+       })) != cudaSuccess)
+    return set_err_cuda(e, "heavy");
+  if ((e = run(s, KFVM_KCLASS_RIEMANN, dim, [&] { return launch_riemann(dim, eq, s->F, s->G, s->g, s->sc, st); })) !=
+      cudaSuccess)
+    return set_err_cuda(e, "riemann");
+  return KFVM_OK;
+}
+
+kfvm::StageArgs stage_args(kfvm_solver *s, int bIn, int bOut, int mode) {
+  kfvm::StageArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.U = s->Ub[bIn];
+  a.Unext = bOut >= 0 ? s->Ub[bOut] : nullptr;
+  a.Uprev = s->Ub[s->iPrev];
+  a.Uhat = s->Uhat;
+  a.Utmp = s->Utmp;
+  a.K = s->K;
+  a.G = s->G;
+  a.F = s->F;
+  a.src = s->src;
+  a.theta = s->theta;
+  a.mode = mode;
+  a.Re = s->cfg.reynolds;
+  a.Pr = s->cfg.prandtl;
+  a.atol = s->cfg.atol;
+  a.rtol = s->cfg.rtol;
+  a.part = s->part;
+  a.sc = s->sc;
+  a.co.use_tmp = s->rk.use_tmp ? 1 : 0;
+  return a;
+}
+
+// evalRHS(U_b) followed by K = RHS
+int eval_into_K(kfvm_solver *s, int b) {
+  int rc = eval_front(s, b);
+  if (rc) return rc;
+  kfvm::StageArgs a = stage_args(s, b, -1, kfvm::STAGE_EVAL);
+  cudaError_t e = run(s, KFVM_KCLASS_STAGE, 1, [&] { return kfvm::launch_stage(s->dim, s->eq, a, s->g, s->stream); });
+  if (e != cudaSuccess) return set_err_cuda(e, "stage");
+  return KFVM_OK;
+}
+
+double bits_to_double(unsigned long long b) {
+  double d;
+  std::memcpy(&d, &b, sizeof(d));
+  return d;
+}
+
+// tail of Solver::Solver: Uprev = U, prime FSAL, dt = 0.01 cfl dmin / maxVel
+int prime(kfvm_solver *s) {
+  s->iCur = s->iPrev;
+  s->time = 0.0;
+  s->errEst = 1.0;
+  s->lastTimeStep = false;
+  s->nTS = 1;
+  s->useSparseWeno = s->cfg.weno_thresh > 0.0 && s->indicator == KFVM_IND_KXRCF;
+  const int64_t n = s->g.n;
+  CK(cudaMemsetAsync(s->wset, 0, n, s->stream));
+  CK(cudaMemsetAsync(s->sc, 0, sizeof(kfvm::DevScalars), s->stream));
+  std::vector<double> one(n, 1.0);
+  CK(cudaMemcpyAsync(s->theta, one.data(), n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  int rc = eval_into_K(s, s->iPrev);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(kfvm::DevScalars), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const double maxVel = bits_to_double(s->hsc->maxvel_bits);
+  s->nWenoLast = s->hsc->napplied;
+  s->dt = 0.01 * s->cfg.cfl * s->dmin / maxVel;
+  s->primed = true;
+  return KFVM_OK;
+}
+
+// Solver::TakeStep (Solver.cpp:188-343)
+int take_step(kfvm_solver *s, kfvm_step_info *info) {
+  using namespace kfvm;
+  if (!s->primed) return fail(KFVM_ERR_STATE, "take_step before an initial condition was set");
+  const RKTable &rk = s->rk;
+  cudaStream_t st = s->stream;
+  if (s->time + s->dt > s->cfg.final_time) {
+    s->dt = s->cfg.final_time - s->time;
+    s->lastTimeStep = true;
+  }
+  bool accepted = false, firstUnphys = true;
+  double maxVel = 0.0, errNew = 0.0, dtTaken = 0.0;
+  int lStat = KFVM_TS_ACCEPTED, nT;
+  const int bA = (s->iPrev + 1) % 3, bB = (s->iPrev + 2) % 3;
+  CK(cudaEventRecord(s->ev0, st));
+  for (nT = 0; nT < s->cfg.rejection_limit; nT++) {
+    CK(cudaMemsetAsync(&s->sc->maxvel_bits, 0, sizeof(unsigned long long), st));
+    if (nT > 0) {
+      int rc = eval_into_K(s, s->iPrev);
+      if (rc) return rc;
+    }
+    cudaError_t e = run(s, KFVM_KCLASS_OTHER, 1, [&] {
+      return launch_stage_pre(s->dim, s->eq, s->Ub[bA], s->Ub[s->iPrev], s->Uhat, s->Utmp, s->K, s->g,
+                              rk.beta[0] * s->dt, rk.bhat[0] * s->dt, rk.use_tmp ? 1 : 0, st);
+    });
+    if (e != cudaSuccess) return set_err_cuda(e, "stage_pre");
+    int cur = bA, nxt = bB;
+    for (int nS = 1; nS < rk.nStages; nS++) {
+      int rc = eval_front(s, cur);
+      if (rc) return rc;
+      StageArgs a = stage_args(s, cur, nxt, STAGE_UPDATE);
+      a.co.delta = rk.delta[nS];
+      a.co.g1 = rk.gam1[nS];
+      a.co.g2 = rk.gam2[nS];
+      a.co.g3 = rk.gam3[nS];
+      a.co.betaDt = rk.beta[nS] * s->dt;
+      a.co.bhatDt = rk.bhat[nS] * s->dt;
+      if ((e = run(s, KFVM_KCLASS_STAGE, 1, [&] { return launch_stage(s->dim, s->eq, a, s->g, st); })) !=
+          cudaSuccess)
+        return set_err_cuda(e, "stage");
+      std::swap(cur, nxt);
+    }
+    // FSAL stage: K = RHS(U), Uhat += bhatfsal dt K, error estimate
+    int rc = eval_front(s, cur);
+    if (rc) return rc;
+    StageArgs a = stage_args(s, cur, -1, STAGE_FSAL);
+    a.co.bhatDt = rk.bhatfsal * s->dt;
+    if ((e = run(s, KFVM_KCLASS_STAGE, 2, [&] { return launch_stage(s->dim, s->eq, a, s->g, st); })) !=
+        cudaSuccess)
+      return set_err_cuda(e, "fsal");
+    CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    maxVel = bits_to_double(s->hsc->maxvel_bits);
+    s->nWenoLast = s->hsc->napplied;
+    const double nDofs = (double)(s->g.n * s->nv);
+    const double posFlag = s->hsc->posmin;
+    errNew = 1.0 / std::sqrt(s->hsc->err / nDofs);
+    double dtfac = std::pow(errNew, rk.ep1) * std::pow(s->errEst, rk.ep2);
+    dtfac = std::isnan(dtfac) ? 1.2 : 1.0 + std::atan(dtfac - 1.0);
+    if (posFlag < 0.0) lStat = KFVM_TS_UNPHYSICAL;
+    else if (dtfac >= s->cfg.rejection_thresh) lStat = KFVM_TS_ACCEPTED;
+    else lStat = KFVM_TS_TOLERANCE;
+
+    if (lStat == KFVM_TS_UNPHYSICAL) {
+      s->dt = firstUnphys ? std::fmin(0.25 * s->cfg.cfl * s->dmin / maxVel, s->dt / 4.0) : s->dt / 2.0;
+      firstUnphys = false;
+      s->useSparseWeno = false; // force full WENO on the retry
+      if (s->lastTimeStep) s->lastTimeStep = false;
+    } else if (lStat == KFVM_TS_ACCEPTED) {
+      accepted = true;
+      dtTaken = s->dt;
+      s->time += s->dt;
+      const double dterr = s->dt * dtfac, dtcfl = s->cfg.cfl * s->dmin / maxVel;
+      s->dt = std::fmin(dterr, dtcfl);
+      s->errEst = errNew;
+      // Uprev <- U by buffer rotation instead of a copy
+      s->iPrev = cur;
+      s->iCur = cur;
+      nT++;
+      break;
+    } else {
+      s->dt = s->dt * dtfac;
+      if (s->lastTimeStep) s->lastTimeStep = false;
+    }
+  }
+  CK(cudaEventRecord(s->ev1, st));
+  CK(cudaEventSynchronize(s->ev1));
+  CK(cudaEventElapsedTime(&s->lastMs, s->ev0, s->ev1));
+  harvest(s);
+  if (!accepted) s->lastTimeStep = true;
+  if (s->dt < s->cfg.min_dt) s->lastTimeStep = true;
+  if (info) {
+    info->time = s->time;
+    info->dt = s->dt;
+    info->dt_taken = dtTaken;
+    info->max_vel = maxVel;
+    info->err_est = errNew;
+    info->status = lStat;
+    info->attempts = nT;
+    info->accepted = accepted ? 1 : 0;
+    info->last_step = s->lastTimeStep ? 1 : 0;
+    info->n_weno = s->nWenoLast;
+    info->n_rhs = s->nRhs;
+  }
+  return KFVM_OK;
+}
+
+// host SoA interior <-> padded device buffer, one strided 3D copy per variable
+cudaMemcpy3DParms interior_copy(kfvm_solver *s, int b, int v, double *host, bool toDevice) {
+  const kfvm::Grid &g = s->g;
+  cudaMemcpy3DParms p;
+  std::memset(&p, 0, sizeof(p));
+  cudaPitchedPtr hp = make_cudaPitchedPtr(host + (size_t)v * g.n, g.nx * sizeof(double), g.nx, g.ny);
+  cudaPitchedPtr dp = make_cudaPitchedPtr(s->Ub[b] + (size_t)v * g.pvol, g.px * sizeof(double), g.px, g.py);
+  const cudaPos dpos = make_cudaPos(kfvm::kRad * sizeof(double), kfvm::kRad, g.rz);
+  if (toDevice) {
+    p.srcPtr = hp;
+    p.dstPtr = dp;
+    p.dstPos = dpos;
+    p.kind = cudaMemcpyHostToDevice;
+  } else {
+    p.srcPtr = dp;
+    p.srcPos = dpos;
+    p.dstPtr = hp;
+    p.kind = cudaMemcpyDeviceToHost;
+  }
+  p.extent = make_cudaExtent(g.nx * sizeof(double), g.ny, g.nz);
+  return p;
+}
+
+int upload_state(kfvm_solver *s, int b, const double *u) {
+  for (int v = 0; v < s->nv; v++) {
+    cudaMemcpy3DParms p = interior_copy(s, b, v, const_cast<double *>(u), true);
+    CK(cudaMemcpy3DAsync(&p, s->stream));
+  }
+  return KFVM_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *kfvm_last_error(void) { return g_err.c_str(); }
+
+void kfvm_default_config(kfvm_config *c) {
+  std::memset(c, 0, sizeof(*c));
+  c->dim = 2;
+  c->eq = KFVM_EQ_HYDRO;
+  c->rs = KFVM_RS_HLLC;
+  c->rk = KFVM_RK_SSP4_3_2;
+  c->nq = 2;
+  c->indicator = KFVM_IND_KXRCF;
+  c->nx = c->ny = c->nz = 1;
+  c->xlo = c->ylo = c->zlo = 0.0;
+  c->xup = c->yup = c->zup = 1.0;
+  c->gamma = (double)1.4f;
+  c->reynolds = 1.0;
+  c->prandtl = (double)0.71f;
+  c->weno_thresh = 10.0;
+  c->lfac = 20.0;
+  c->cfl = c->dim == 3 ? 0.5 : 0.75;
+  c->atol = (double)1.e-4f;
+  c->rtol = (double)1.e-4f;
+  c->rejection_thresh = (double)0.8f;
+  c->min_dt = (double)1.e-10f;
+  c->final_time = 1.0;
+  c->rejection_limit = 4;
+  c->max_steps = 1000;
+}
+
+int kfvm_stencil_build(const kfvm_config *cfg, kfvm_stencil *out) {
+  if (!cfg || !out) return fail(KFVM_ERR_ARG, "null argument");
+  const int rc = kfvm::build_stencil(cfg, out);
+  if (rc) return fail(rc, "stencil weight precompute failed");
+  return KFVM_OK;
+}
+
+int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
+  using namespace kfvm;
+  if (!cfg || !out) return fail(KFVM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (cfg->dim != 2 && cfg->dim != 3) return fail(KFVM_ERR_ARG, "dim must be 2 or 3");
+  if (cfg->nq != 2) return fail(KFVM_ERR_ARG, "the GPU path supports NUM_QUAD_PTS = 2");
+  if (cfg->eq < 0 || cfg->eq > 2) return fail(KFVM_ERR_ARG, "unknown equation type");
+  if (cfg->rs < 0 || cfg->rs > 2) return fail(KFVM_ERR_ARG, "unknown Riemann solver");
+  if (cfg->eq == KFVM_EQ_MHD_GLM && cfg->rs == KFVM_RS_HLLC)
+    return fail(KFVM_ERR_ARG, "HLLC is not defined for MHD_GLM");
+  const int64_t nz = cfg->dim == 3 ? cfg->nz : 1;
+  if (cfg->nx * cfg->ny * nz >= (int64_t)0x80000000LL) return fail(KFVM_ERR_ARG, "more than 2^31 cells");
+  if (cfg->nx < 3 || cfg->ny < 3 || nz < (cfg->dim == 3 ? 3 : 1))
+    return fail(KFVM_ERR_ARG, "grid too small for a radius-2 stencil");
+  for (int d = 0; d < cfg->dim; d++)
+    if ((cfg->bc[2 * d] == KFVM_BC_PERIODIC) != (cfg->bc[2 * d + 1] == KFVM_BC_PERIODIC))
+      return fail(KFVM_ERR_ARG, "periodic boundaries must come in pairs");
+  kfvm_solver *s = new kfvm_solver();
+  s->cfg = *cfg;
+  s->cfg.nz = nz;
+  s->dim = cfg->dim;
+  s->eq = cfg->eq;
+  s->nv = cfg->eq == KFVM_EQ_MHD_GLM ? 9 : 5;
+  s->indicator = cfg->indicator;
+  if (!rk_table(cfg->rk, s->rk)) {
+    delete s;
+    return fail(KFVM_ERR_ARG, "unsupported RK scheme");
+  }
+  Grid &g = s->g;
+  std::memset(&g, 0, sizeof(g));
+  g.nx = cfg->nx;
+  g.ny = cfg->ny;
+  g.nz = nz;
+  g.n = g.nx * g.ny * g.nz;
+  g.px = g.nx + 2 * kRad;
+  g.py = g.ny + 2 * kRad;
+  g.rz = cfg->dim == 3 ? kRad : 0;
+  g.pvol = g.px * g.py * (cfg->dim == 3 ? nz + 2 * kRad : 1);
+  for (int d = 0; d < 3; d++) {
+    g.fdim[d][0] = g.nx + (d == 0);
+    g.fdim[d][1] = g.ny + (d == 1);
+    g.fdim[d][2] = g.nz + (d == 2);
+    g.nface[d] = g.fdim[d][0] * g.fdim[d][1] * g.fdim[d][2];
+  }
+  g.dx = (cfg->xup - cfg->xlo) / cfg->nx;
+  g.dy = (cfg->yup - cfg->ylo) / cfg->ny;
+  g.dz = (cfg->zup - cfg->zlo) / nz;
+  for (int f = 0; f < 6; f++) g.bc[f] = cfg->bc[f];
+  g.gamma = cfg->gamma;
+  g.rs = cfg->rs;
+  s->dmin = cfg->dim == 2 ? std::fmin(g.dx, g.dy) : std::fmin(g.dx, std::fmin(g.dy, g.dz));
+
+  DevStencil hS;
+  std::memset(&hS, 0, sizeof(hS));
+  int rc = build_stencil(&s->cfg, &hS.w);
+  if (rc) {
+    delete s;
+    return fail(rc, "stencil weight precompute failed");
+  }
+  for (int c = 0; c < hS.w.n_cells; c++)
+    hS.loff[c] = (hS.w.off[2][c] * g.py + hS.w.off[1][c]) * g.px + hS.w.off[0][c];
+  for (int c = 0; c < hS.w.n_cells; c++) g.loff[c] = hS.loff[c];
+
+  auto cleanup = [&](cudaError_t e, const char *what) {
+    kfvm_destroy(s);
+    return set_err_cuda(e, what);
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) return cleanup(e, "stream");
+  if ((e = cudaEventCreate(&s->ev0)) != cudaSuccess) return cleanup(e, "event");
+  if ((e = cudaEventCreate(&s->ev1)) != cudaSuccess) return cleanup(e, "event");
+  const size_t nv = s->nv, n = g.n;
+  const int nqf = cfg->dim == 2 ? 2 : 4, nqc = cfg->dim == 2 ? 4 : 8;
+  auto dalloc = [&](void **p, size_t bytes) { return cudaMalloc(p, bytes); };
+  if ((e = dalloc((void **)&s->dS, sizeof(DevStencil))) != cudaSuccess) return cleanup(e, "alloc");
+  for (int b = 0; b < 3; b++)
+    if ((e = dalloc((void **)&s->Ub[b], g.pvol * nv * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc U");
+  if ((e = dalloc((void **)&s->Uhat, n * nv * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->K, n * nv * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
+  if (s->rk.use_tmp && (e = dalloc((void **)&s->Utmp, n * nv * sizeof(double))) != cudaSuccess)
+    return cleanup(e, "alloc");
+  for (int d = 0; d < cfg->dim; d++) {
+    if ((e = dalloc((void **)&s->F[d], 2 * nqf * nv * g.nface[d] * sizeof(double))) != cudaSuccess)
+      return cleanup(e, "alloc faces");
+    if ((e = dalloc((void **)&s->G[d], nv * g.nface[d] * sizeof(double))) != cudaSuccess)
+      return cleanup(e, "alloc fluxes");
+  }
+  if (cfg->eq == KFVM_EQ_MHD_GLM &&
+      (e = dalloc((void **)&s->src, (size_t)nqc * nv * n * sizeof(double))) != cudaSuccess)
+    return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->theta, n * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->flag, n)) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->wset, n)) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->applied, n)) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->heavy, n * sizeof(uint32_t))) != cudaSuccess) return cleanup(e, "alloc");
+  {
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    s->heavyBlocks = (nsm > 0 ? nsm : 148) * 4; // grid-stride over the device-side count
+  }
+  if ((e = dalloc((void **)&s->part, 2 * stage_blocks(g) * sizeof(double))) != cudaSuccess)
+    return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->sc, sizeof(DevScalars))) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = cudaMallocHost((void **)&s->hsc, sizeof(DevScalars))) != cudaSuccess) return cleanup(e, "alloc host");
+  for (int b = 0; b < 3; b++)
+    if ((e = cudaMemsetAsync(s->Ub[b], 0, g.pvol * nv * sizeof(double), s->stream)) != cudaSuccess)
+      return cleanup(e, "memset");
+  if ((e = cudaMemcpyAsync(s->dS, &hS, sizeof(DevStencil), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess)
+    return cleanup(e, "upload stencil");
+  if ((e = cudaMemsetAsync(s->sc, 0, sizeof(DevScalars), s->stream)) != cudaSuccess) return cleanup(e, "memset");
+  {
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cleanup(e, "device");
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    WeightSlot &ws = g_slots[{dev, cfg->dim}];
+    if (ws.users > 0 && ws.lfac != cfg->lfac) {
+      kfvm_destroy(s);
+      return fail(KFVM_ERR_ARG, "a live solver of this dimension on this device uses another lfac");
+    }
+    if (ws.users == 0) {
+      if ((e = upload_linear_weights(cfg->dim, hS.w, s->stream)) != cudaSuccess) return cleanup(e, "weights");
+      ws.lfac = cfg->lfac;
+    }
+    ws.users++;
+    s->device = dev;
+  }
+  if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return cleanup(e, "sync");
+  *out = s;
+  return KFVM_OK;
+}
+
+void kfvm_destroy(kfvm_solver *s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->device >= 0) {
+    std::lock_guard<std::mutex> lk(g_slot_mu);
+    g_slots[{s->device, s->dim}].users--;
+  }
+  cudaFree(s->dS);
+  for (int b = 0; b < 3; b++) cudaFree(s->Ub[b]);
+  cudaFree(s->Uhat);
+  cudaFree(s->Utmp);
+  cudaFree(s->K);
+  for (int d = 0; d < 3; d++) {
+    cudaFree(s->F[d]);
+    cudaFree(s->G[d]);
+  }
+  cudaFree(s->src);
+  cudaFree(s->theta);
+  cudaFree(s->flag);
+  cudaFree(s->wset);
+  cudaFree(s->applied);
+  cudaFree(s->heavy);
+  cudaFree(s->part);
+  cudaFree(s->sc);
+  if (s->hsc) cudaFreeHost(s->hsc);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  for (auto &m : s->marks) {
+    cudaEventDestroy(m.a);
+    cudaEventDestroy(m.b);
+  }
+  for (auto e : s->evPool) cudaEventDestroy(e);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+int kfvm_init_ic(kfvm_solver *s, int32_t ic_kind, uint64_t seed) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (ic_kind < 0 || ic_kind > KFVM_IC_SMOOTH_WAVE) return fail(KFVM_ERR_ARG, "unknown initial condition");
+  cudaError_t e = run(s, KFVM_KCLASS_OTHER, 1, [&] {
+    return kfvm::launch_ic(s->dim, s->eq, ic_kind, seed, s->cfg, s->Ub[s->iPrev], s->g, s->stream);
+  });
+  if (e != cudaSuccess) return set_err_cuda(e, "ic");
+  return prime(s);
+}
+
+int kfvm_set_state(kfvm_solver *s, const double *u) {
+  if (!s || !u) return fail(KFVM_ERR_ARG, "null argument");
+  int rc = upload_state(s, s->iPrev, u);
+  if (rc) return rc;
+  return prime(s);
+}
+
+int kfvm_get_state(kfvm_solver *s, double *u) {
+  if (!s || !u) return fail(KFVM_ERR_ARG, "null argument");
+  for (int v = 0; v < s->nv; v++) {
+    cudaMemcpy3DParms p = interior_copy(s, s->iCur, v, u, false);
+    CK(cudaMemcpy3DAsync(&p, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return KFVM_OK;
+}
+
+int kfvm_eval_rhs(kfvm_solver *s, double t, double *rhs, double *max_vel) {
+  (void)t;
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  CK(cudaMemsetAsync(&s->sc->maxvel_bits, 0, sizeof(unsigned long long), s->stream));
+  int rc = eval_into_K(s, s->iCur);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(kfvm::DevScalars), cudaMemcpyDeviceToHost, s->stream));
+  if (rhs)
+    CK(cudaMemcpyAsync(rhs, s->K, (size_t)s->g.n * s->nv * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->nWenoLast = s->hsc->napplied;
+  if (max_vel) *max_vel = bits_to_double(s->hsc->maxvel_bits);
+  return KFVM_OK;
+}
+
+int kfvm_take_step(kfvm_solver *s, kfvm_step_info *info) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  return take_step(s, info);
+}
+
+int kfvm_solve(kfvm_solver *s, int32_t max_steps, int64_t *n_steps_out, kfvm_step_info *last) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  kfvm_step_info info;
+  std::memset(&info, 0, sizeof(info));
+  int64_t acc = 0;
+  for (; s->nTS < max_steps && !s->lastTimeStep; ++s->nTS) {
+    int rc = take_step(s, &info);
+    if (rc) return rc;
+    acc += info.accepted;
+  }
+  if (n_steps_out) *n_steps_out = acc;
+  if (last) *last = info;
+  return KFVM_OK;
+}
+
+int kfvm_get_time(kfvm_solver *s, double *time, double *dt) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (time) *time = s->time;
+  if (dt) *dt = s->dt;
+  return KFVM_OK;
+}
+
+int kfvm_set_indicator(kfvm_solver *s, int32_t ind) {
+  if (!s || ind < 0 || ind > KFVM_IND_NONE) return fail(KFVM_ERR_ARG, "bad indicator");
+  s->indicator = ind;
+  s->useSparseWeno = s->cfg.weno_thresh > 0.0 && ind == KFVM_IND_KXRCF;
+  return KFVM_OK;
+}
+
+int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
+  if (!s || !out || dir < 0 || dir >= s->dim) return fail(KFVM_ERR_ARG, "bad argument");
+  const kfvm::Grid &g = s->g;
+  const int nqf = s->dim == 2 ? 2 : 4, nv = s->nv;
+  const int64_t nf = g.nface[dir];
+  CK(cudaMemcpyAsync(out, s->F[dir], (size_t)2 * nqf * nv * nf * sizeof(double), cudaMemcpyDeviceToHost,
+                     s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  // apply the face BCs to the boundary slots (setFaceBCs), as the kernels do on read
+  const int64_t fx = g.fdim[dir][0], fy = g.fdim[dir][1], fz = g.fdim[dir][2];
+  const int64_t nd = dir == 0 ? g.nx : (dir == 1 ? g.ny : g.nz);
+  const int64_t stride = dir == 0 ? 1 : (dir == 1 ? fx : fx * fy);
+  const bool per = g.bc[2 * dir] == KFVM_BC_PERIODIC;
+  for (int64_t k = 0; k < fz; k++)
+    for (int64_t j = 0; j < fy; j++)
+      for (int64_t i = 0; i < fx; i++) {
+        const int64_t m = dir == 0 ? i : (dir == 1 ? j : k);
+        if (m != 0) continue;
+        const int64_t lo = (k * fy + j) * fx + i, hi = lo + nd * stride;
+        for (int q = 0; q < nqf; q++)
+          for (int v = 0; v < nv; v++) {
+            const int64_t s0 = ((int64_t)(0 * nqf + q) * nv + v) * nf, s1 = ((int64_t)(1 * nqf + q) * nv + v) * nf;
+            if (per) {
+              out[s0 + lo] = out[s0 + hi];
+              out[s1 + hi] = out[s1 + lo];
+            } else {
+              out[s0 + lo] = out[s1 + lo];
+              out[s1 + hi] = out[s0 + hi];
+            }
+          }
+      }
+  return KFVM_OK;
+}
+
+int kfvm_get_flags(kfvm_solver *s, uint8_t *weno_applied, double *theta) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (weno_applied) CK(cudaMemcpyAsync(weno_applied, s->applied, s->g.n, cudaMemcpyDeviceToHost, s->stream));
+  if (theta) CK(cudaMemcpyAsync(theta, s->theta, s->g.n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return KFVM_OK;
+}
+
+int kfvm_last_stage_ms(kfvm_solver *s, double *ms) {
+  if (!s || !ms) return fail(KFVM_ERR_ARG, "null argument");
+  *ms = s->lastMs;
+  return KFVM_OK;
+}
+
+int kfvm_get_stream(kfvm_solver *s, void **stream) {
+  if (!s || !stream) return fail(KFVM_ERR_ARG, "null argument");
+  *stream = (void *)s->stream;
+  return KFVM_OK;
+}
+
+int kfvm_set_timing(kfvm_solver *s, int32_t on) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  CK(cudaStreamSynchronize(s->stream));
+  harvest(s);
+  s->timing = on != 0;
+  for (int c = 0; c < KFVM_NUM_KCLASS; c++) {
+    s->clsMs[c] = 0.0;
+    s->clsLaunches[c] = 0;
+  }
+  return KFVM_OK;
+}
+
+int kfvm_get_timing(kfvm_solver *s, double *ms, int64_t *launches) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  CK(cudaStreamSynchronize(s->stream));
+  harvest(s);
+  for (int c = 0; c < KFVM_NUM_KCLASS; c++) {
+    if (ms) ms[c] = s->clsMs[c];
+    if (launches) launches[c] = s->clsLaunches[c];
+  }
+  return KFVM_OK;
+}
+
+int kfvm_get_launch_count(kfvm_solver *s, int64_t *launches) {
+  if (!s || !launches) return fail(KFVM_ERR_ARG, "null argument");
+  *launches = s->launches;
+  return KFVM_OK;
+}
+
+} // extern "C"

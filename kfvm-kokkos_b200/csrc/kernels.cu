@@ -1,0 +1,989 @@
+// kernels.cu -- kernel bodies and host launchers of the per-stage hot path.
+// See kernels.cuh for the stage structure and the HBM layouts.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "launch.h"
+
+namespace kfvm {
+
+// ---------------------------------------------------------------------------
+// halo fill: every halo cell copies the interior cell given by per-axis maps
+// (periodic wrap or outflow mirror).  Applying the axis maps independently is
+// the same as the reference's sequential x, y, z fills with their corner ranges
+// (Solver.cpp:744-783, 826-930; BoundaryConditions_K.H:53-72).
+__device__ __forceinline__ int64_t axis_map(int64_t i, int64_t n, int bcLo, int bcHi) {
+  if (i < 0) return bcLo == KFVM_BC_PERIODIC ? i + n : -i - 1;
+  if (i >= n) return bcHi == KFVM_BC_PERIODIC ? i - n : 2 * n - i - 1;
+  return i;
+}
+
+template <int DIM, int NV>
+__global__ void __launch_bounds__(256) bc_fill_kernel(double *__restrict__ U, Grid g) {
+  const int64_t r = kRad;
+  const int64_t hx = g.nx + 2 * r, hy = g.ny + 2 * r;
+  const int64_t nxs = 2 * r * g.ny * g.nz;                 // x slabs (interior y,z)
+  const int64_t nys = hx * 2 * r * g.nz;                   // y slabs (all x, interior z)
+  const int64_t nzs = DIM == 3 ? hx * hy * 2 * r : 0;      // z slabs (all x, y)
+  const int64_t total = nxs + nys + nzs;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j, k;
+    if (t < nxs) {
+      const int64_t a = t % (2 * r), b = t / (2 * r);
+      i = a < r ? a - r : g.nx + (a - r);
+      j = b % g.ny;
+      k = b / g.ny;
+    } else if (t < nxs + nys) {
+      const int64_t u = t - nxs, a = u % hx, b = u / hx;
+      i = a - r;
+      const int64_t jj = b % (2 * r);
+      j = jj < r ? jj - r : g.ny + (jj - r);
+      k = b / (2 * r);
+    } else {
+      const int64_t u = t - nxs - nys, a = u % hx, b = u / hx;
+      i = a - r;
+      j = b % hy - r;
+      const int64_t kk = b / hy;
+      k = kk < r ? kk - r : g.nz + (kk - r);
+    }
+    const int64_t si = axis_map(i, g.nx, g.bc[0], g.bc[1]);
+    const int64_t sj = axis_map(j, g.ny, g.bc[2], g.bc[3]);
+    const int64_t sk = DIM == 3 ? axis_map(k, g.nz, g.bc[4], g.bc[5]) : k;
+    const int64_t dst = pidx(g, i, j, k), src = pidx(g, si, sj, sk);
+#pragma unroll
+    for (int v = 0; v < NV; v++) U[v * g.pvol + dst] = U[v * g.pvol + src];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Linear-reconstruction weights of the full stencil in the constant bank: face
+// points [f][q][c] followed by interior points [q][c].  They depend only on the
+// dimension and lfac (not on the grid), so one set per (device, dimension) serves
+// every solver with that lfac.  Loop indices are compile-time, so every weight is
+// an immediate constant-bank operand of its FMA.
+constexpr int kW2Face = 4 * 2 * 13, kW2Cell = 4 * 13;
+constexpr int kW3Face = 6 * 4 * 33, kW3Cell = 8 * 33;
+__constant__ double c_w2[kW2Face + kW2Cell];
+__constant__ double c_w3[kW3Face + kW3Cell];
+
+template <int DIM>
+__device__ __forceinline__ double cw(int idx) {
+  if constexpr (DIM == 2) return c_w2[idx];
+  else return c_w3[idx];
+}
+
+cudaError_t upload_linear_weights(int dim, const kfvm_stencil &st, cudaStream_t s) {
+  const int C = st.n_cells, NQF = st.nqf, NQC = st.nqc, NF = 2 * dim;
+  double w[kW3Face + kW3Cell];
+  int n = 0;
+  for (int f = 0; f < NF; f++)
+    for (int q = 0; q < NQF; q++)
+      for (int c = 0; c < C; c++) w[n++] = st.face_w[0][f][q][c];
+  for (int q = 0; q < NQC; q++)
+    for (int c = 0; c < C; c++) w[n++] = st.cell_w[0][q][c];
+  if (dim == 2) return cudaMemcpyToSymbolAsync(c_w2, w, n * sizeof(double), 0, cudaMemcpyHostToDevice, s);
+  return cudaMemcpyToSymbolAsync(c_w3, w, n * sizeof(double), 0, cudaMemcpyHostToDevice, s);
+}
+
+// st[p][v] = sum_c W0[R0 + p][c] U[c][v] for NP consecutive weight rows starting at
+// R0 (face points are rows f*NQF + q, interior points rows NF*NQF + q)
+template <int DIM, int EQ, int R0, int NP>
+__device__ __forceinline__ void lin_rows(const double *__restrict__ Uc, const Grid &g,
+                                         double (&st)[NP][Cfg<DIM, EQ>::NV]) {
+  using T = Cfg<DIM, EQ>;
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+#pragma unroll
+    for (int v = 0; v < T::NV; v++) st[p][v] = 0.0;
+#pragma unroll
+  for (int v = 0; v < T::NV; v++) {
+    const double *Uv = Uc + v * g.pvol;
+#pragma unroll
+    for (int c = 0; c < T::C; c++) {
+      const double u = __ldg(Uv + g.loff[c]);
+#pragma unroll
+      for (int p = 0; p < NP; p++) st[p][v] += cw<DIM>((R0 + p) * T::C + c) * u;
+    }
+  }
+}
+
+// number of face points reconstructed per pass over the stencil (register budget:
+// NP x NV accumulators)
+template <int DIM, int EQ>
+struct Groups {
+  static constexpr int NPF = Eos<EQ>::NV > 5 ? 4 : 8;
+  static constexpr int NG = (2 * DIM * (DIM == 2 ? 2 : 4)) / NPF;
+};
+
+// face-slot address of point q, variable v of face f of cell (i,j,k) in a
+// [slot][q][v][face] array with nvv variables
+__device__ __forceinline__ int64_t face_slot_addr(const Grid &g, int f, int64_t i, int64_t j, int64_t k,
+                                                  int q, int v, int nqf, int nvv) {
+  const int d = f >> 1, hi = f & 1;
+  const int64_t fi = i + (d == 0 && hi), fj = j + (d == 1 && hi), fk = k + (d == 2 && hi);
+  const int64_t fidx = (fk * g.fdim[d][1] + fj) * g.fdim[d][0] + fi;
+  const int slot = hi ? 0 : 1;
+  return ((int64_t)(slot * nqf + q) * nvv + v) * g.nface[d] + fidx;
+}
+
+// ---------------------------------------------------------------------------
+// KXRCF, part 1: linear face states of each cell -> indicator p/rho^gamma at its
+// own face slots (KernelLinearRecon_K + EOS::weno).  W[d] is [slot][q][face].
+template <int DIM, int EQ, int G>
+__device__ __forceinline__ void select_group(const double *__restrict__ Uc, const Grid &g,
+                                             int64_t i, int64_t j, int64_t k, double *const *W) {
+  using T = Cfg<DIM, EQ>;
+  constexpr int NP = Groups<DIM, EQ>::NPF;
+  if constexpr (G + 1 < Groups<DIM, EQ>::NG) select_group<DIM, EQ, G + 1>(Uc, g, i, j, k, W);
+  double st[NP][T::NV];
+  lin_rows<DIM, EQ, G * NP, NP>(Uc, g, st);
+#pragma unroll
+  for (int p = 0; p < NP; p++) {
+    const int f = (G * NP + p) / T::NQF, q = (G * NP + p) % T::NQF;
+    W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno(g.gamma, st[p]);
+  }
+}
+
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(128)
+    select_kernel(const double *__restrict__ U, Grid g, double *W0, double *W1, double *W2) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const double *Uc = U + pidx(g, i, j, k);
+  double *W[3] = {W0, W1, W2};
+  select_group<DIM, EQ, 0>(Uc, g, i, j, k, W);
+}
+
+// KXRCF, part 2 (WenoSelect_K, Numeric_K.H:292-398): largest indicator jump across
+// the cell's faces over the cell value; the outer slot of a boundary face follows
+// setFaceBCs (periodic partner face, or the inner slot at an outflow boundary).
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(128)
+    flag_kernel(const double *__restrict__ U, Grid g, const double *__restrict__ W0,
+                const double *__restrict__ W1, const double *__restrict__ W2,
+                const double *__restrict__ theta, uint8_t *__restrict__ flag,
+                DevScalars *__restrict__ sc, double wThresh) {
+  using T = Cfg<DIM, EQ>;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  bool f = false;
+  if (i < g.nx && j < g.ny) {
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    f = theta[c] < 1.0;
+    if (!f) {
+      const double *W[3] = {W0, W1, W2};
+      double maxJump = 0.0;
+#pragma unroll
+      for (int fc = 0; fc < T::NF; fc++) {
+        const int d = fc >> 1, hi = fc & 1;
+        const int64_t fx = g.fdim[d][0], fy = g.fdim[d][1], nf = g.nface[d];
+        const int64_t fi = i + (d == 0 && hi), fj = j + (d == 1 && hi), fk = k + (d == 2 && hi);
+        int64_t fidx = (fk * fy + fj) * fx + fi, oidx = fidx;
+        const int own = hi ? 0 : 1;
+        int oth = 1 - own;
+        const int64_t m = d == 0 ? fi : (d == 1 ? fj : fk);
+        const int64_t nd = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+        const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
+        if (m == 0 || m == nd) {
+          if (g.bc[fc] == KFVM_BC_PERIODIC) oidx = m == 0 ? fidx + nd * stride : fidx - nd * stride;
+          else oth = own;
+        }
+#pragma unroll
+        for (int q = 0; q < T::NQF; q++) {
+          const double wIn = W[d][(int64_t)(own * T::NQF + q) * nf + fidx];
+          const double wOut = W[d][(int64_t)(oth * T::NQF + q) * nf + oidx];
+          maxJump = fmax(maxJump, fabs(wOut - wIn));
+        }
+      }
+      double uAv[T::NV];
+      const double *Uc = U + pidx(g, i, j, k);
+#pragma unroll
+      for (int v = 0; v < T::NV; v++) uAv[v] = Uc[v * g.pvol];
+      const double w = maxJump / Eos<EQ>::weno(g.gamma, uAv);
+      f = w >= wThresh;
+    }
+    flag[c] = f ? 1 : 0;
+  }
+  const unsigned ball = __ballot_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0 && ball) atomicAdd(&sc->nflag, (unsigned)__popc(ball));
+}
+
+// ---------------------------------------------------------------------------
+// final face states, light pass: linear reconstruction with constant-bank weights
+// for every cell that is not sent to WENO.  The positivity limiter's bounds are
+// computed first; a cell whose states all lie strictly inside them keeps theta = 1
+// exactly as in the reference.  WENO cells and cells that need the limiter are
+// appended to the heavy list (bit 31 marks WENO) for heavy_kernel.
+constexpr uint32_t kHeavyWeno = 0x80000000u;
+
+template <int DIM, int EQ, int G>
+__device__ __forceinline__ bool recon_group(const double *__restrict__ Uc, const Grid &g,
+                                            const PosBounds &bd, int64_t i, int64_t j, int64_t k,
+                                            double *const *F, double &lam, double &vel) {
+  using T = Cfg<DIM, EQ>;
+  constexpr int NP = Groups<DIM, EQ>::NPF;
+  bool ok = true;
+  if constexpr (G + 1 < Groups<DIM, EQ>::NG) ok = recon_group<DIM, EQ, G + 1>(Uc, g, bd, i, j, k, F, lam, vel);
+  double st[NP][T::NV];
+  lin_rows<DIM, EQ, G * NP, NP>(Uc, g, st);
+#pragma unroll
+  for (int p = 0; p < NP; p++) {
+    const int f = (G * NP + p) / T::NQF, q = (G * NP + p) % T::NQF;
+    ok = ok && pos_inside<EQ>(bd, st[p]);
+    const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, T::NV);
+    const int64_t nf = g.nface[f >> 1];
+#pragma unroll
+    for (int v = 0; v < T::NV; v++) F[f >> 1][a + v * nf] = st[p][v];
+    if constexpr (T::SRC) {
+      // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
+      const double vv = fabs(st[p][MOMX] / st[p][DENS]);
+      const double l = Eos<EQ>::fastMagSonic(g.gamma, st[p], st[p][MAGX]) + vv;
+      vel = vv > vel ? vv : vel;
+      lam = l > lam ? l : lam;
+    }
+  }
+  return ok;
+}
+
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(128)
+    recon_kernel(const double *__restrict__ U, Grid g, int mode, const uint8_t *__restrict__ flag,
+                 uint8_t *__restrict__ wset, uint8_t *__restrict__ applied,
+                 double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
+                 double *__restrict__ F2, double *__restrict__ src, uint32_t *__restrict__ heavy,
+                 DevScalars *__restrict__ sc) {
+  using T = Cfg<DIM, EQ>;
+  constexpr int NV = T::NV;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  bool useWeno = false, push = false;
+  double lam = 0.0, vel = 0.0;
+  int64_t c = 0;
+  if (i < g.nx && j < g.ny) {
+    c = (k * g.ny + j) * g.nx + i;
+    if (mode == RECON_FULL) {
+      useWeno = true;
+    } else if (mode == RECON_SPARSE) {
+      // the flag set is replaced only when this evaluation flagged some cell
+      // (WenoSelector::update, Solver.cpp:687-742); otherwise the last set stays
+      if (sc->nflag > 0) {
+        useWeno = flag[c] != 0;
+        wset[c] = useWeno ? 1 : 0;
+      } else {
+        useWeno = wset[c] != 0;
+      }
+    }
+    applied[c] = useWeno ? 1 : 0;
+    if (useWeno) {
+      push = true;
+    } else {
+      const double *Uc = U + pidx(g, i, j, k);
+      const PosBounds bd = pos_bounds<DIM, EQ>(Uc, g);
+      double *F[3] = {F0, F1, F2};
+      bool ok = recon_group<DIM, EQ, 0>(Uc, g, bd, i, j, k, F, lam, vel);
+      if constexpr (T::SRC) {
+        double cs[T::NQC][NV];
+        lin_rows<DIM, EQ, T::NF * T::NQF, T::NQC>(Uc, g, cs);
+#pragma unroll
+        for (int q = 0; q < T::NQC; q++) {
+          ok = ok && pos_inside<EQ>(bd, cs[q]);
+#pragma unroll
+          for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = cs[q][v];
+        }
+      }
+      if (ok) theta[c] = 1.0;
+      else push = true;
+    }
+  }
+  // warp-aggregated append to the heavy list
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned ball = __ballot_sync(0xffffffffu, push);
+  const unsigned wball = __ballot_sync(0xffffffffu, useWeno);
+  unsigned base = 0;
+  if (lane == 0 && ball) base = atomicAdd(&sc->nheavy, (unsigned)__popc(ball));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (push) heavy[base + __popc(ball & ((1u << lane) - 1u))] = (uint32_t)c | (useWeno ? kHeavyWeno : 0u);
+  if (lane == 0 && wball) atomicAdd(&sc->napplied, (unsigned)__popc(wball));
+  if constexpr (T::SRC) {
+    lam = warp_max(lam);
+    vel = warp_max(vel);
+    if (lane == 0) {
+      atomic_max_pos(&sc->glm_lam_bits, lam);
+      atomic_max_pos(&sc->glm_vel_bits, vel);
+    }
+  }
+}
+
+// heavy pass over the listed cells: WENO-AO reconstruction (KernelWenoRecon_K) or the
+// linear states already written, then the full positivity procedure
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(128)
+    heavy_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S,
+                 double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
+                 double *__restrict__ F2, double *__restrict__ src,
+                 const uint32_t *__restrict__ heavy, DevScalars *__restrict__ sc) {
+  using T = Cfg<DIM, EQ>;
+  using E = Eos<EQ>;
+  constexpr int NV = T::NV;
+  const unsigned count = sc->nheavy;
+  double *F[3] = {F0, F1, F2};
+  double lam = 0.0, vel = 0.0;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+    const uint32_t e = heavy[t];
+    const int64_t c = e & ~kHeavyWeno;
+    const int64_t i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+    const double *Uc = U + pidx(g, i, j, k);
+    double fs[T::NF][T::NQF][NV];
+    double cs[T::SRC ? T::NQC : 1][NV];
+    if (e & kHeavyWeno) {
+      weno_cell<DIM, EQ>(Uc, g, S, fs, cs);
+    } else {
+      for (int f = 0; f < T::NF; f++)
+        for (int q = 0; q < T::NQF; q++) {
+          const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
+#pragma unroll
+          for (int v = 0; v < NV; v++) fs[f][q][v] = F[f >> 1][a + v * g.nface[f >> 1]];
+        }
+      if constexpr (T::SRC) {
+        for (int q = 0; q < T::NQC; q++)
+#pragma unroll
+          for (int v = 0; v < NV; v++) cs[q][v] = src[(q * NV + v) * g.n + c];
+      }
+    }
+    const PosBounds bd = pos_bounds<DIM, EQ>(Uc, g);
+    theta[c] = pos_apply<DIM, EQ>(Uc, g, bd, fs, cs);
+    for (int f = 0; f < T::NF; f++)
+      for (int q = 0; q < T::NQF; q++) {
+        const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
+#pragma unroll
+        for (int v = 0; v < NV; v++) F[f >> 1][a + v * g.nface[f >> 1]] = fs[f][q][v];
+        if constexpr (T::SRC) {
+          const double *u = fs[f][q];
+          const double vv = fabs(u[MOMX] / u[DENS]);
+          const double l = E::fastMagSonic(g.gamma, u, u[MAGX]) + vv;
+          vel = vv > vel ? vv : vel;
+          lam = l > lam ? l : lam;
+        }
+      }
+    if constexpr (T::SRC) {
+      for (int q = 0; q < T::NQC; q++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = cs[q][v];
+    }
+  }
+  if constexpr (T::SRC) {
+    lam = warp_max(lam);
+    vel = warp_max(vel);
+    if ((threadIdx.x & 31) == 0) {
+      atomic_max_pos(&sc->glm_lam_bits, lam);
+      atomic_max_pos(&sc->glm_vel_bits, vel);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// one thread per face of direction D: Riemann solve at every face point, the
+// quadrature-weighted flux sum per variable, and the max wave speed.
+template <int DIM, int EQ, int D>
+__global__ void __launch_bounds__(128)
+    riemann_kernel(const double *__restrict__ F, double *__restrict__ G, Grid g,
+                   DevScalars *__restrict__ sc) {
+  using T = Cfg<DIM, EQ>;
+  using E = Eos<EQ>;
+  constexpr int NV = T::NV;
+  const int64_t fx = g.fdim[D][0], fy = g.fdim[D][1], nf = g.nface[D];
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  double vmax = 0.0;
+  if (i < fx && j < fy) {
+    const int64_t fidx = (k * fy + j) * fx + i;
+    const int64_t m = D == 0 ? i : (D == 1 ? j : k);
+    const int64_t nd = D == 0 ? g.nx : (D == 1 ? g.ny : g.nz);
+    // face BCs (setFaceBCs): boundary faces take the missing slot from the
+    // periodic partner face, or copy the interior slot at an outflow boundary
+    int64_t f0 = fidx, f1 = fidx;
+    int s0 = 0, s1 = 1;
+    const int64_t stride = D == 0 ? 1 : (D == 1 ? fx : fx * fy);
+    if (m == 0) {
+      if (g.bc[2 * D] == KFVM_BC_PERIODIC) f0 = fidx + nd * stride;
+      else s0 = 1;
+    } else if (m == nd) {
+      if (g.bc[2 * D + 1] == KFVM_BC_PERIODIC) f1 = fidx - nd * stride;
+      else s1 = 0;
+    }
+    const double ch = EQ == EQ_GLM ? __longlong_as_double((long long)sc->glm_lam_bits) -
+                                         __longlong_as_double((long long)sc->glm_vel_bits)
+                                   : 0.0;
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) acc[v] = 0.0;
+#pragma unroll
+    for (int q = 0; q < T::NQF; q++) {
+      double uL[NV], uR[NV], Fq[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        uL[v] = __ldg(F + ((int64_t)(s0 * T::NQF + q) * NV + v) * nf + f0);
+        uR[v] = __ldg(F + ((int64_t)(s1 * T::NQF + q) * NV + v) * nf + f1);
+      }
+      const double s = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
+      vmax = s > vmax ? s : vmax;
+      const double wq = DIM == 2 ? 0.5 : 0.25; // Gauss weights 1/2 (x 1/2 in 3D)
+#pragma unroll
+      for (int v = 0; v < NV; v++) acc[v] += wq * Fq[v];
+    }
+#pragma unroll
+    for (int v = 0; v < NV; v++) G[(int64_t)v * nf + fidx] = acc[v];
+  }
+  vmax = warp_max(vmax);
+  if ((threadIdx.x & 31) == 0) atomic_max_pos(&sc->maxvel_bits, vmax);
+}
+
+// ---------------------------------------------------------------------------
+// GLM source terms at the interior points of a cell (SourceTerms_K<MHD_GLM>,
+// MHD_GLM_K.H:316-547, zero user forcing), added to rhs with the cell quadrature
+template <int DIM>
+__device__ void glm_sources(const double *__restrict__ Uc, const Grid &g, int64_t i, int64_t j,
+                            int64_t k, int64_t c, const double *__restrict__ F0,
+                            const double *__restrict__ F1, const double *__restrict__ F2,
+                            const double *__restrict__ src, double th, double *rhs) {
+  using T = Cfg<DIM, EQ_GLM>;
+  constexpr int NV = 9, NQ = 2, NQF = T::NQF;
+  constexpr int nzq = DIM == 3 ? NQ : 1;
+  // LGL -> GL differentiation matrix, 2 points (Numeric.cpp:50-52)
+  const double Dm[2][4] = {
+      {-2.7320508075688767, 1.732050807568877, 1.7320508075688767, -0.7320508075688767},
+      {0.7320508075688767, -1.7320508075688767, -1.732050807568877, 2.7320508075688767}};
+  const double *Fd[3] = {F0, F1, F2};
+  // face value of variable v at point q of face (d, index fi,fj,fk), slot s with face BCs
+  auto fv = [&](int d, int64_t fi, int64_t fj, int64_t fk, int s, int q, int v) {
+    const int64_t fx = g.fdim[d][0], fy = g.fdim[d][1];
+    const int64_t m = d == 0 ? fi : (d == 1 ? fj : fk);
+    const int64_t nd = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+    const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
+    int64_t fidx = (fk * fy + fj) * fx + fi;
+    if (m == 0 && s == 0) {
+      if (g.bc[2 * d] == KFVM_BC_PERIODIC) fidx += nd * stride;
+      else s = 1;
+    } else if (m == nd && s == 1) {
+      if (g.bc[2 * d + 1] == KFVM_BC_PERIODIC) fidx -= nd * stride;
+      else s = 0;
+    }
+    return Fd[d][((int64_t)(s * NQF + q) * NV + v) * g.nface[d] + fidx];
+  };
+  const double wt[2] = {0.5, 0.5};
+  double divB = 0.0;
+  for (int nQ = 0; nQ < NQ; nQ++)
+    for (int nS = 0; nS < nzq; nS++) {
+      const int qIdx = nS * NQ + nQ;
+      const double twt = DIM == 2 ? wt[nQ] : wt[nQ] * wt[nS];
+      const double bAvW = 0.5 * (fv(0, i, j, k, 1, qIdx, MAGX) + fv(0, i, j, k, 0, qIdx, MAGX));
+      const double bAvE = 0.5 * (fv(0, i + 1, j, k, 0, qIdx, MAGX) + fv(0, i + 1, j, k, 1, qIdx, MAGX));
+      divB += twt * (bAvE - bAvW) / g.dx;
+      const double bAvS = 0.5 * (fv(1, i, j, k, 1, qIdx, MAGY) + fv(1, i, j, k, 0, qIdx, MAGY));
+      const double bAvN = 0.5 * (fv(1, i, j + 1, k, 0, qIdx, MAGY) + fv(1, i, j + 1, k, 1, qIdx, MAGY));
+      divB += twt * (bAvN - bAvS) / g.dy;
+      if (DIM == 3) {
+        const double bAvB = 0.5 * (fv(2, i, j, k, 1, qIdx, MAGZ) + fv(2, i, j, k, 0, qIdx, MAGZ));
+        const double bAvT = 0.5 * (fv(2, i, j, k + 1, 0, qIdx, MAGZ) + fv(2, i, j, k + 1, 1, qIdx, MAGZ));
+        divB += twt * (bAvT - bAvB) / g.dz;
+      }
+    }
+  auto cv = [&](int a, int b, int e, int v) {
+    return src[((int64_t)((a * NQ + b) * nzq + e) * NV + v) * g.n + c];
+  };
+  const int64_t sy = g.px, sz = g.px * g.py;
+  for (int nQ = 0; nQ < NQ; nQ++)
+    for (int nR = 0; nR < NQ; nR++)
+      for (int nS = 0; nS < nzq; nS++) {
+        double st[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) st[v] = cv(nQ, nR, nS, v);
+        const double rho = st[DENS];
+        const double vx = st[MOMX] / rho, vy = st[MOMY] / rho, vz = st[MOMZ] / rho;
+        double dpx, dpy, dpz = 0.0;
+        if (th < 0.75) {
+          const double tdx = 1.0 / (2.0 * g.dx), tdy = 1.0 / (2.0 * g.dy);
+          dpx = tdx * (Uc[PSI * g.pvol + 1] - Uc[PSI * g.pvol - 1]);
+          dpy = tdy * (Uc[PSI * g.pvol + sy] - Uc[PSI * g.pvol - sy]);
+          if (DIM == 3) {
+            const double tdz = 1.0 / (2.0 * g.dz);
+            dpz = tdz * (Uc[PSI * g.pvol + sz] - Uc[PSI * g.pvol - sz]);
+          }
+        } else {
+          {
+            const int fIdx = DIM == 2 ? nR : nR * NQ + nS;
+            double d = Dm[nQ][0] * fv(0, i, j, k, 1, fIdx, PSI) + Dm[nQ][NQ + 1] * fv(0, i + 1, j, k, 0, fIdx, PSI);
+            for (int m = 1; m <= NQ; m++) d += Dm[nQ][m] * cv(m - 1, nR, nS, PSI);
+            dpx = d / g.dx;
+          }
+          {
+            const int fIdx = DIM == 2 ? nQ : nQ * NQ + nS;
+            double d = Dm[nR][0] * fv(1, i, j, k, 1, fIdx, PSI) + Dm[nR][NQ + 1] * fv(1, i, j + 1, k, 0, fIdx, PSI);
+            for (int m = 1; m <= NQ; m++) d += Dm[nR][m] * cv(nQ, m - 1, nS, PSI);
+            dpy = d / g.dy;
+          }
+          if (DIM == 3) {
+            const int fIdx = nQ * NQ + nR;
+            double d = Dm[nS][0] * fv(2, i, j, k, 1, fIdx, PSI) + Dm[nS][NQ + 1] * fv(2, i, j, k + 1, 0, fIdx, PSI);
+            for (int m = 1; m <= NQ; m++) d += Dm[nS][m] * cv(nQ, nR, m - 1, PSI);
+            dpz = d / g.dz;
+          }
+        }
+        const double gpsiDu = vx * dpx + vy * dpy + vz * dpz;
+        const double uDb = vx * st[MAGX] + vy * st[MAGY] + vz * st[MAGZ];
+        double sv[NV];
+        sv[DENS] = 0.0;
+        sv[MOMX] = -divB * st[MAGX];
+        sv[MOMY] = -divB * st[MAGY];
+        sv[MOMZ] = -divB * st[MAGZ];
+        sv[ETOT] = -(divB * uDb + gpsiDu * st[PSI]);
+        sv[MAGX] = -divB * vx;
+        sv[MAGY] = -divB * vy;
+        sv[MAGZ] = -divB * vz;
+        sv[PSI] = -gpsiDu;
+        const double w = DIM == 2 ? wt[nQ] * wt[nR] : wt[nQ] * wt[nR] * wt[nS];
+#pragma unroll
+        for (int v = 0; v < NV; v++) rhs[v] += w * sv[v];
+      }
+}
+
+// compact viscous stress and heat flux (Viscosity_K<NavierStokes>, NavierStokes_K.H:190-407)
+template <int DIM>
+__device__ void viscous(const double *__restrict__ Uc, const Grid &g, double Re, double Pr,
+                        double *rhs) {
+  using E = Eos<EQ_NS>;
+  const int64_t sy = g.px, sz = g.px * g.py;
+  auto prim = [&](int64_t o, double &u, double &v, double &w, double &T) {
+    double Uo[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) Uo[q] = Uc[q * g.pvol + o];
+    u = Uo[MOMX] / Uo[DENS];
+    v = Uo[MOMY] / Uo[DENS];
+    w = Uo[MOMZ] / Uo[DENS];
+    T = E::pres(g.gamma, Uo) / Uo[DENS];
+  };
+  if constexpr (DIM == 2) {
+    const double rdx = 1.0 / g.dx, rdy = 1.0 / g.dy;
+    double u[3][3], v[3][3], w[3][3], T[3][3];
+#pragma unroll
+    for (int xo = -1; xo <= 1; xo++)
+#pragma unroll
+      for (int yo = -1; yo <= 1; yo++)
+        prim(xo + yo * sy, u[xo + 1][yo + 1], v[xo + 1][yo + 1], w[xo + 1][yo + 1], T[xo + 1][yo + 1]);
+    double px[4], mx[4], py[4], my[4];
+    px[0] = 4.0 * rdx * (u[2][1] - u[1][1]) / 3.0;
+    px[0] -= rdy * (v[1][2] + v[2][2] - v[1][0] - v[2][0]) / 6.0;
+    px[1] = rdy * (u[1][2] + u[2][2] - u[1][0] - u[2][0]) / 4.0;
+    px[1] += rdx * (v[2][1] - v[1][1]);
+    px[2] = rdx * (w[2][1] - w[1][1]);
+    mx[0] = 4.0 * rdx * (u[1][1] - u[0][1]) / 3.0;
+    mx[0] -= rdy * (v[0][2] + v[1][2] - v[0][0] - v[1][0]) / 6.0;
+    mx[1] = rdy * (u[0][2] + u[1][2] - u[0][0] - u[1][0]) / 4.0;
+    mx[1] += rdx * (v[1][1] - v[0][1]);
+    mx[2] = rdx * (w[1][1] - w[0][1]);
+    py[0] = rdx * (v[2][2] + v[2][1] - v[0][2] - v[0][1]) / 4.0;
+    py[0] += rdy * (u[1][2] - u[1][1]);
+    py[1] = 4.0 * rdy * (v[1][2] - v[1][1]) / 3.0;
+    py[1] -= rdx * (u[2][2] + u[2][1] - u[0][2] - u[0][1]) / 6.0;
+    py[2] = rdy * (w[1][2] - w[1][1]);
+    my[0] = rdx * (v[2][1] + v[2][0] - v[0][1] - v[0][0]) / 4.0;
+    my[0] += rdy * (u[1][1] - u[1][0]);
+    my[1] = 4.0 * rdy * (v[1][1] - v[1][0]) / 3.0;
+    my[1] -= rdx * (u[2][1] + u[2][0] - u[0][1] - u[0][0]) / 6.0;
+    my[2] = rdy * (w[1][1] - w[1][0]);
+    px[3] = rdx * (T[2][1] - T[1][1]);
+    mx[3] = rdx * (T[1][1] - T[0][1]);
+    py[3] = rdy * (T[1][2] - T[1][1]);
+    my[3] = rdy * (T[1][1] - T[1][0]);
+    const double rRe = 1.0 / Re;
+    const double sru = rRe * (rdx * (px[0] - mx[0]) + rdy * (py[0] - my[0]));
+    const double srv = rRe * (rdx * (px[1] - mx[1]) + rdy * (py[1] - my[1]));
+    const double srw = rRe * (rdx * (px[2] - mx[2]) + rdy * (py[2] - my[2]));
+    const double rAl = 1.0 / (Pr * Re);
+    const double ste = rAl * (rdx * (px[3] - mx[3]) + rdy * (py[3] - my[3]));
+    rhs[MOMX] += sru;
+    rhs[MOMY] += srv;
+    rhs[MOMZ] += srw;
+    rhs[ETOT] += ste + u[1][1] * sru + v[1][1] * srv + w[1][1] * srw;
+  } else {
+    const double rdx = 1.0 / g.dx, rdy = 1.0 / g.dy, rdz = 1.0 / g.dz;
+    double u[3][3][3], v[3][3][3], w[3][3][3], T[3][3][3];
+#pragma unroll
+    for (int xo = -1; xo <= 1; xo++)
+#pragma unroll
+      for (int yo = -1; yo <= 1; yo++)
+#pragma unroll
+        for (int zo = -1; zo <= 1; zo++)
+          prim(xo + yo * sy + zo * sz, u[xo + 1][yo + 1][zo + 1], v[xo + 1][yo + 1][zo + 1],
+               w[xo + 1][yo + 1][zo + 1], T[xo + 1][yo + 1][zo + 1]);
+    double px[4], mx[4], py[4], my[4], pz[4], mz[4];
+    px[0] = 4.0 * rdx * (u[2][1][1] - u[1][1][1]) / 3.0;
+    px[0] -= rdy * (v[1][2][1] + v[2][2][1] - v[1][0][1] - v[2][0][1]) / 6.0;
+    px[0] -= rdz * (w[1][1][2] + w[2][1][2] - w[1][1][0] - w[2][1][0]) / 6.0;
+    px[1] = rdy * (u[1][2][1] + u[2][2][1] - u[1][0][1] - u[2][0][1]) / 4.0;
+    px[1] += rdx * (v[2][1][1] - v[1][1][1]);
+    px[2] = rdz * (u[2][1][2] + u[1][1][2] - u[2][1][0] - u[1][1][0]) / 4.0;
+    px[2] += rdx * (w[2][1][1] - w[1][1][1]);
+    mx[0] = 4.0 * rdx * (u[1][1][1] - u[0][1][1]) / 3.0;
+    mx[0] -= rdy * (v[0][2][1] + v[1][2][1] - v[0][0][1] - v[1][0][1]) / 6.0;
+    mx[0] -= rdz * (w[0][1][2] + w[1][1][2] - w[0][1][0] - w[1][1][0]) / 6.0;
+    mx[1] = rdy * (u[0][2][1] + u[1][2][1] - u[0][0][1] - u[1][0][1]) / 4.0;
+    mx[1] += rdx * (v[1][1][1] - v[0][1][1]);
+    mx[2] = rdz * (u[1][1][2] + u[0][1][2] - u[1][1][0] - u[0][1][0]) / 4.0;
+    mx[2] += rdx * (w[1][1][1] - w[0][1][1]);
+    py[0] = rdx * (v[2][2][1] + v[2][1][1] - v[0][2][1] - v[0][1][1]) / 4.0;
+    py[0] += rdy * (u[1][2][1] - u[1][1][1]);
+    py[1] = 4.0 * rdy * (v[1][2][1] - v[1][1][1]) / 3.0;
+    py[1] -= rdx * (u[2][2][1] + u[2][1][1] - u[0][2][1] - u[0][1][1]) / 6.0;
+    py[1] -= rdz * (w[1][2][2] + w[1][1][2] - w[1][2][0] - w[1][1][0]) / 6.0;
+    py[2] = rdz * (v[1][2][2] + v[1][1][2] - v[1][2][0] - v[1][1][0]) / 4.0;
+    py[2] += rdy * (w[1][2][1] - w[1][1][1]);
+    my[0] = rdx * (v[2][1][1] + v[2][0][1] - v[0][1][1] - v[0][0][1]) / 4.0;
+    my[0] += rdy * (u[1][1][1] - u[1][0][1]);
+    my[1] = 4.0 * rdy * (v[1][1][1] - v[1][0][1]) / 3.0;
+    my[1] -= rdx * (u[2][1][1] + u[2][0][1] - u[0][1][1] - u[0][0][1]) / 6.0;
+    my[1] -= rdz * (w[1][1][2] + w[1][0][2] - w[1][1][0] - w[1][0][0]) / 6.0;
+    my[2] = rdz * (v[1][1][2] + v[1][0][2] - v[1][1][0] - v[1][0][0]) / 4.0;
+    my[2] += rdy * (w[1][1][1] - w[1][0][1]);
+    pz[0] = rdx * (w[2][2][1] + w[2][1][1] - w[0][2][1] - w[0][1][1]) / 4.0;
+    pz[0] += rdz * (u[1][1][2] - u[1][1][1]);
+    pz[1] = rdy * (w[1][2][2] + w[1][2][1] - w[1][0][2] - w[1][0][1]) / 4.0;
+    pz[1] += rdz * (v[1][1][2] - v[1][1][1]);
+    pz[2] = 4.0 * rdz * (w[1][1][2] - w[1][1][1]) / 3.0;
+    pz[2] -= rdx * (u[2][2][1] + u[2][1][1] - u[0][2][1] - u[0][1][1]) / 6.0;
+    pz[2] -= rdy * (v[1][2][2] + v[1][2][1] - v[1][0][2] - v[1][0][1]) / 6.0;
+    mz[0] = rdx * (w[2][2][0] + w[2][1][0] - w[0][2][0] - w[0][1][0]) / 4.0;
+    mz[0] += rdz * (u[1][1][1] - u[1][1][0]);
+    mz[1] = rdy * (w[1][2][1] + w[1][2][0] - w[1][0][1] - w[1][0][0]) / 4.0;
+    mz[1] += rdz * (v[1][1][1] - v[1][1][0]);
+    mz[2] = 4.0 * rdz * (w[1][1][1] - w[1][1][0]) / 3.0;
+    mz[2] -= rdx * (u[2][2][0] + u[2][1][0] - u[0][2][0] - u[0][1][0]) / 6.0;
+    mz[2] -= rdy * (v[1][2][1] + v[1][2][0] - v[1][0][1] - v[1][0][0]) / 6.0;
+    px[3] = rdx * (T[2][1][1] - T[1][1][1]);
+    mx[3] = rdx * (T[1][1][1] - T[0][1][1]);
+    py[3] = rdy * (T[1][2][1] - T[1][1][1]);
+    my[3] = rdy * (T[1][1][1] - T[1][0][1]);
+    pz[3] = rdz * (T[1][1][2] - T[1][1][1]);
+    mz[3] = rdz * (T[1][1][1] - T[1][1][0]);
+    const double rRe = 1.0 / Re;
+    const double sru = rRe * (rdx * (px[0] - mx[0]) + rdy * (py[0] - my[0]) + rdz * (pz[0] - mz[0]));
+    const double srv = rRe * (rdx * (px[1] - mx[1]) + rdy * (py[1] - my[1]) + rdz * (pz[1] - mz[1]));
+    const double srw = rRe * (rdx * (px[2] - mx[2]) + rdy * (py[2] - my[2]) + rdz * (pz[2] - mz[2]));
+    const double rAl = 1.0 / (Re * Pr);
+    const double ste = rAl * (rdx * (px[3] - mx[3]) + rdy * (py[3] - my[3]) + rdz * (pz[3] - mz[3]));
+    rhs[MOMX] += sru;
+    rhs[MOMY] += srv;
+    rhs[MOMZ] += srw;
+    rhs[ETOT] += ste + u[1][1][1] * sru + v[1][1][1] * srv + w[1][1][1] * srw;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// flux divergence (+ viscous, + GLM sources) fused with the RK register update
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(128)
+    stage_kernel(const double *__restrict__ U, double *__restrict__ Unext,
+                 const double *__restrict__ Uprev, double *__restrict__ Uhat,
+                 double *__restrict__ Utmp, double *__restrict__ K, Grid g,
+                 const double *__restrict__ G0, const double *__restrict__ G1,
+                 const double *__restrict__ G2, const double *__restrict__ F0,
+                 const double *__restrict__ F1, const double *__restrict__ F2,
+                 const double *__restrict__ src, const double *__restrict__ theta, int mode,
+                 StageCoef co, double Re, double Pr, double atol, double rtol,
+                 double *__restrict__ part) {
+  using T = Cfg<DIM, EQ>;
+  using E = Eos<EQ>;
+  constexpr int NV = T::NV;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  double err = 0.0, pos = 1.0;
+  if (i < g.nx && j < g.ny) {
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    const int64_t p = pidx(g, i, j, k);
+    const double *Uc = U + p;
+    double r[NV];
+    {
+      const int64_t f0 = (k * g.fdim[0][1] + j) * g.fdim[0][0] + i;
+      const int64_t f1 = (k * g.fdim[1][1] + j) * g.fdim[1][0] + i;
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        r[v] = (G0[v * g.nface[0] + f0] - G0[v * g.nface[0] + f0 + 1]) / g.dx;
+        r[v] += (G1[v * g.nface[1] + f1] - G1[v * g.nface[1] + f1 + g.fdim[1][0]]) / g.dy;
+      }
+      if constexpr (DIM == 3) {
+        const int64_t f2 = (k * g.fdim[2][1] + j) * g.fdim[2][0] + i;
+        const int64_t sz = g.fdim[2][0] * g.fdim[2][1];
+#pragma unroll
+        for (int v = 0; v < NV; v++) r[v] += (G2[v * g.nface[2] + f2] - G2[v * g.nface[2] + f2 + sz]) / g.dz;
+      }
+    }
+    if constexpr (EQ == EQ_GLM) glm_sources<DIM>(Uc, g, i, j, k, c, F0, F1, F2, src, theta[c], r);
+    if constexpr (EQ == EQ_NS) viscous<DIM>(Uc, g, Re, Pr, r);
+
+    if (mode == STAGE_EVAL) {
+#pragma unroll
+      for (int v = 0; v < NV; v++) K[v * g.n + c] = r[v];
+    } else if (mode == STAGE_UPDATE) {
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        const double u = Uc[v * g.pvol];
+        double un = co.g1 * u;
+        if (co.use_tmp) {
+          const double ut = Utmp[v * g.n + c] + co.delta * u;
+          Utmp[v * g.n + c] = ut;
+          un += co.g2 * ut;
+        }
+        if (co.g3 != 0.0) un += co.g3 * Uprev[v * g.pvol + p];
+        un += co.betaDt * r[v];
+        Unext[v * g.pvol + p] = un;
+        Uhat[v * g.n + c] += co.bhatDt * r[v];
+      }
+    } else { // STAGE_FSAL: K = rhs, Uhat += bhat_fsal dt K, error estimate
+      bool hasNan = false;
+      double st[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        K[v * g.n + c] = r[v];
+        const double uh = Uhat[v * g.n + c] + co.bhatDt * r[v];
+        Uhat[v * g.n + c] = uh;
+        const double u = Uc[v * g.pvol];
+        st[v] = u;
+        hasNan = hasNan || isnan(u);
+        const double e = (u - uh) / (atol + rtol * fmax(fabs(u), fabs(uh)));
+        err += e * e;
+      }
+      pos = hasNan ? -1.0 : E::positivity(st);
+    }
+  }
+  if (mode == STAGE_FSAL) {
+    // deterministic two-level reduction: block partials here, fixed-order sum later
+    __shared__ double se[kBlockX * kBlockY / 32], sp[kBlockX * kBlockY / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      err += __shfl_xor_sync(0xffffffffu, err, o);
+      pos = fmin(pos, __shfl_xor_sync(0xffffffffu, pos, o));
+    }
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if ((tid & 31) == 0) {
+      se[tid >> 5] = err;
+      sp[tid >> 5] = pos;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double a = 0.0, b = 1.0;
+      for (int w = 0; w < (int)(blockDim.x * blockDim.y / 32); w++) {
+        a += se[w];
+        b = b > sp[w] ? sp[w] : b;
+      }
+      const int64_t blk = ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+      part[2 * blk] = a;
+      part[2 * blk + 1] = b;
+    }
+  }
+}
+
+// fixed-order sum of the block partials (one block)
+__global__ void __launch_bounds__(1024) finalize_kernel(const double *__restrict__ part,
+                                                         int64_t nblk, DevScalars *sc) {
+  __shared__ double se[1024], sp[1024];
+  double a = 0.0, b = 1.0;
+  for (int64_t t = threadIdx.x; t < nblk; t += blockDim.x) {
+    a += part[2 * t];
+    b = b > part[2 * t + 1] ? part[2 * t + 1] : b;
+  }
+  se[threadIdx.x] = a;
+  sp[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      se[threadIdx.x] += se[threadIdx.x + s];
+      sp[threadIdx.x] = sp[threadIdx.x] > sp[threadIdx.x + s] ? sp[threadIdx.x + s] : sp[threadIdx.x];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sc->err = se[0];
+    sc->posmin = sp[0];
+  }
+}
+
+// first stage of a step (RKFSAL_StagePre_K, Numeric_K.H:198-220)
+template <int NV>
+__global__ void __launch_bounds__(128)
+    stage_pre_kernel(double *__restrict__ U1, const double *__restrict__ Uprev,
+                     double *__restrict__ Uhat, double *__restrict__ Utmp,
+                     const double *__restrict__ K, Grid g, double betaDt, double bhatDt,
+                     int use_tmp) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const int64_t c = (k * g.ny + j) * g.nx + i, p = pidx(g, i, j, k);
+#pragma unroll
+  for (int v = 0; v < NV; v++) {
+    const double up = Uprev[v * g.pvol + p], kk = K[v * g.n + c];
+    U1[v * g.pvol + p] = up + betaDt * kk;
+    Uhat[v * g.n + c] = up + bhatDt * kk;
+    if (use_tmp) Utmp[v * g.n + c] = up;
+  }
+}
+
+// copy of the interior of one padded buffer into another
+template <int NV>
+__global__ void __launch_bounds__(128) copy_interior_kernel(double *__restrict__ dst,
+                                                            const double *__restrict__ src, Grid g) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  if (i >= g.nx || j >= g.ny) return;
+  const int64_t p = pidx(g, i, j, k);
+#pragma unroll
+  for (int v = 0; v < NV; v++) dst[v * g.pvol + p] = src[v * g.pvol + p];
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+static dim3 cell_grid(const Grid &g) {
+  return dim3((unsigned)((g.nx + kBlockX - 1) / kBlockX), (unsigned)((g.ny + kBlockY - 1) / kBlockY),
+              (unsigned)g.nz);
+}
+
+template <int DIM, int EQ>
+struct Launch {
+  static constexpr int NV = Eos<EQ>::NV;
+  static cudaError_t bc(double *U, const Grid &g, cudaStream_t s) {
+    const int64_t r = kRad, hx = g.nx + 2 * r, hy = g.ny + 2 * r;
+    const int64_t total = 2 * r * g.ny * g.nz + hx * 2 * r * g.nz + (DIM == 3 ? hx * hy * 2 * r : 0);
+    const int64_t blocks = (total + 255) / 256;
+    bc_fill_kernel<DIM, NV><<<(unsigned)(blocks < 65535 * 16 ? blocks : 65535 * 16), 256, 0, s>>>(U, g);
+    return cudaGetLastError();
+  }
+  static cudaError_t select(const double *U, const Grid &g, double *const *W, cudaStream_t s) {
+    select_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, W[0], W[1], W[2]);
+    return cudaGetLastError();
+  }
+  static cudaError_t flag(const double *U, const Grid &g, double *const *W, const double *theta,
+                          uint8_t *flag, DevScalars *sc, double thr, cudaStream_t s) {
+    flag_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, W[0], W[1], W[2], theta,
+                                                                          flag, sc, thr);
+    return cudaGetLastError();
+  }
+  static cudaError_t recon(const double *U, const Grid &g, const DevStencil *S, int mode,
+                           const uint8_t *flag, uint8_t *wset, uint8_t *applied, double *theta,
+                           double *const *F, double *src, uint32_t *heavy, DevScalars *sc,
+                           int heavy_blocks, cudaStream_t s) {
+    (void)S;
+    (void)heavy_blocks;
+    recon_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
+        U, g, mode, flag, wset, applied, theta, F[0], F[1], F[2], src, heavy, sc);
+    return cudaGetLastError();
+  }
+  static cudaError_t heavy(const double *U, const Grid &g, const DevStencil *S, double *theta,
+                           double *const *F, double *src, const uint32_t *heavy, DevScalars *sc,
+                           int heavy_blocks, cudaStream_t s) {
+    heavy_kernel<DIM, EQ><<<heavy_blocks, 128, 0, s>>>(U, g, S, theta, F[0], F[1], F[2], src, heavy, sc);
+    return cudaGetLastError();
+  }
+  static cudaError_t riemann(double *const *F, double *const *G, const Grid &g, DevScalars *sc,
+                             cudaStream_t s) {
+#pragma unroll 1
+    for (int d = 0; d < DIM; d++) {
+      dim3 grid((unsigned)((g.fdim[d][0] + kBlockX - 1) / kBlockX),
+                (unsigned)((g.fdim[d][1] + kBlockY - 1) / kBlockY), (unsigned)g.fdim[d][2]);
+      if (d == 0) riemann_kernel<DIM, EQ, 0><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(F[0], G[0], g, sc);
+      if (d == 1) riemann_kernel<DIM, EQ, 1><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(F[1], G[1], g, sc);
+      if (DIM == 3 && d == 2)
+        riemann_kernel<DIM, EQ, (DIM == 3 ? 2 : 1)><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(F[2], G[2], g, sc);
+    }
+    return cudaGetLastError();
+  }
+  static cudaError_t stage(const StageArgs &a, const Grid &g, cudaStream_t s) {
+    const dim3 grid = cell_grid(g);
+    stage_kernel<DIM, EQ><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(
+        a.U, a.Unext, a.Uprev, a.Uhat, a.Utmp, a.K, g, a.G[0], a.G[1], a.G[2], a.F[0], a.F[1],
+        a.F[2], a.src, a.theta, a.mode, a.co, a.Re, a.Pr, a.atol, a.rtol, a.part);
+    if (a.mode == STAGE_FSAL) {
+      const int64_t nblk = (int64_t)grid.x * grid.y * grid.z;
+      finalize_kernel<<<1, 1024, 0, s>>>(a.part, nblk, a.sc);
+    }
+    return cudaGetLastError();
+  }
+  static cudaError_t stage_pre(double *U1, const double *Uprev, double *Uhat, double *Utmp,
+                               const double *K, const Grid &g, double betaDt, double bhatDt,
+                               int use_tmp, cudaStream_t s) {
+    stage_pre_kernel<NV><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U1, Uprev, Uhat, Utmp, K, g,
+                                                                          betaDt, bhatDt, use_tmp);
+    return cudaGetLastError();
+  }
+  static cudaError_t copy(double *dst, const double *src, const Grid &g, cudaStream_t s) {
+    copy_interior_kernel<NV><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(dst, src, g);
+    return cudaGetLastError();
+  }
+};
+
+int64_t stage_blocks(const Grid &g) {
+  const dim3 gr = cell_grid(g);
+  return (int64_t)gr.x * gr.y * gr.z;
+}
+
+#define KFVM_DISPATCH(DIM_, EQ_, CALL)                                                  \
+  do {                                                                                \
+    if ((DIM_) == 2 && (EQ_) == EQ_HYDRO) return Launch<2, EQ_HYDRO>::CALL;           \
+    if ((DIM_) == 3 && (EQ_) == EQ_HYDRO) return Launch<3, EQ_HYDRO>::CALL;           \
+    if ((DIM_) == 2 && (EQ_) == EQ_NS) return Launch<2, EQ_NS>::CALL;                 \
+    if ((DIM_) == 3 && (EQ_) == EQ_NS) return Launch<3, EQ_NS>::CALL;                 \
+    if ((DIM_) == 2 && (EQ_) == EQ_GLM) return Launch<2, EQ_GLM>::CALL;               \
+    if ((DIM_) == 3 && (EQ_) == EQ_GLM) return Launch<3, EQ_GLM>::CALL;               \
+    return cudaErrorInvalidValue;                                                     \
+  } while (0)
+
+cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, bc(U, g, s));
+}
+cudaError_t launch_select(int dim, int eq, const double *U, const Grid &g, double *const *W,
+                          cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, select(U, g, W, s));
+}
+cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, double *const *W,
+                        const double *theta, uint8_t *flag, DevScalars *sc, double thr,
+                        cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, flag(U, g, W, theta, flag, sc, thr, s));
+}
+cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
+                         double *theta, double *const *F, double *src, const uint32_t *heavy,
+                         DevScalars *sc, int heavy_blocks, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, heavy(U, g, S, theta, F, src, heavy, sc, heavy_blocks, s));
+}
+cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
+                         int mode, const uint8_t *flag, uint8_t *wset, uint8_t *applied,
+                         double *theta, double *const *F, double *src, uint32_t *heavy,
+                         DevScalars *sc, int heavy_blocks, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, recon(U, g, S, mode, flag, wset, applied, theta, F, src, heavy, sc, heavy_blocks, s));
+}
+cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
+                           DevScalars *sc, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, riemann(F, G, g, sc, s));
+}
+cudaError_t launch_stage(int dim, int eq, const StageArgs &a, const Grid &g, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, stage(a, g, s));
+}
+cudaError_t launch_stage_pre(int dim, int eq, double *U1, const double *Uprev, double *Uhat,
+                             double *Utmp, const double *K, const Grid &g, double betaDt,
+                             double bhatDt, int use_tmp, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, stage_pre(U1, Uprev, Uhat, Utmp, K, g, betaDt, bhatDt, use_tmp, s));
+}
+cudaError_t launch_copy(int dim, int eq, double *dst, const double *src, const Grid &g,
+                        cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, copy(dst, src, g, s));
+}
+
+} // namespace kfvm

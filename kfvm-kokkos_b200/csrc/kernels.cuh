@@ -1,0 +1,341 @@
+// kernels.cuh -- sm_100a kernels of one RHS evaluation + RK stage update.
+//
+// One stage is five launches on the solver's stream:
+//   bc_fill      periodic / outflow halo of the stage state   (Solver::setCellBCs)
+//   select       linear face states of each cell and its neighbours -> KXRCF flag
+//                (KernelLinearRecon_K + setFaceBCs + WenoSelect_K; no face arrays)
+//   recon        final face states: linear, or WENO-AO for flagged cells, then the
+//                positivity limiter; writes the cell's own face slots
+//                (KernelLinearRecon_K / KernelWenoRecon_K / PositivityPreserve_K)
+//   riemann<d>   one thread per face: HLLC/HLL/LLF at every face point, quadrature
+//                weighted flux sum per face, max wave speed     (RiemannSolver*_K)
+//   stage        flux divergence (+ viscous terms, + GLM sources), fused with the
+//                low-storage FSAL register update and the error estimate
+//                (IntegrateRHS_K, Viscosity_K, SourceTerms_K, RKFSAL_*_K)
+// Reference: slug-cfd/kfvm-kokkos src/Solver.cpp:188-530 and the functors named above.
+//
+// Layouts in HBM (all FP64):
+//   U      [v][nz+2r][ny+2r][nx+2r]   padded SoA, r = 2 (2D: one z plane, no z halo)
+//   faces  [slot][q][v][face]         per direction, face = (k*fy + j)*fx + i
+//   flux   [v][face]                  quadrature-weighted flux per face
+//   K, Uhat, Utmp [v][cell]           interior SoA, cell = (k*ny + j)*nx + i
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/kfvm_b200.h"
+#include "physics.cuh"
+
+namespace kfvm {
+
+constexpr int kRad = 2;
+constexpr int kBlockX = 32, kBlockY = 4;
+
+// geometry and pointers of one solver, passed by value
+struct Grid {
+  int64_t nx, ny, nz, n;     // interior cells (nz = 1 in 2D)
+  int64_t px, py, pvol;      // padded pitch in x, rows per plane, values per variable
+  int64_t rz;                // z halo (0 in 2D)
+  int64_t fdim[3][3];        // face grid extents per direction
+  int64_t nface[3];
+  double dx, dy, dz;
+  int bc[6];
+  double gamma, ch_init;
+  int rs;
+  int64_t loff[KFVM_MAX_CELLS]; // stencil offsets in the padded array
+};
+
+// stencil on the device: weights plus linear offsets in the padded array
+struct DevStencil {
+  kfvm_stencil w;
+  int64_t loff[KFVM_MAX_CELLS];
+};
+
+// device-side scalars written by reductions
+struct DevScalars {
+  unsigned long long maxvel_bits; // max wave speed of the current step attempt
+  unsigned long long glm_lam_bits, glm_vel_bits;
+  unsigned int nflag;             // KXRCF flags of the current evaluation
+  unsigned int napplied;          // cells reconstructed with WENO
+  unsigned int nheavy;            // cells in the heavy (WENO / limiter) list
+  unsigned int pad_;
+  double err, posmin;             // error estimate outputs (finalize kernel)
+};
+
+enum ReconMode { RECON_LINEAR = 0, RECON_SPARSE = 1, RECON_FULL = 2 };
+enum StageMode { STAGE_EVAL = 0, STAGE_UPDATE = 1, STAGE_FSAL = 2 };
+
+struct StageCoef {
+  double delta, g1, g2, g3, betaDt, bhatDt;
+  int use_tmp; // delta or g2 nonzero somewhere in the scheme
+};
+
+__device__ __forceinline__ int64_t pidx(const Grid &g, int64_t i, int64_t j, int64_t k) {
+  return ((k + g.rz) * g.py + (j + kRad)) * g.px + (i + kRad);
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *a, double v) {
+  // non-negative doubles order like their bit patterns; NaN is ignored as in the
+  // reference's "vq > maxVel ? vq : maxVel"
+  if (v >= 0.0) atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <int DIM, int EQ>
+struct Cfg {
+  static constexpr int NV = Eos<EQ>::NV;
+  static constexpr int NQ = 2;
+  static constexpr int NQF = DIM == 2 ? 2 : 4;
+  static constexpr int NQC = DIM == 2 ? 4 : 8;
+  static constexpr int NF = 2 * DIM;
+  static constexpr int C = DIM == 2 ? 13 : 33;
+  static constexpr int CC = DIM == 2 ? 5 : 7;
+  static constexpr int CB = DIM == 2 ? 5 : 11;
+  static constexpr int NSUB = DIM == 2 ? 6 : 8;
+  static constexpr int NB = DIM == 2 ? 4 : 6;
+  static constexpr int NI = DIM == 2 ? 5 : 19;
+  static constexpr bool SRC = EQ == EQ_GLM;
+};
+
+// Gauss-Legendre weights on (-1/2,1/2), 2 points (src/numeric/Numeric.cpp:14-17)
+__device__ __forceinline__ double gl_wt(int) { return 1.0 / 2.0; }
+
+// ---------------------------------------------------------------------------
+// WENO-AO reconstruction of all faces (and interior points) of one cell
+// (KernelWenoRecon_K, Stencil_K.H:164-283, 416-590)
+template <int DIM, int EQ>
+__device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
+                          const DevStencil *__restrict__ S,
+                          double (&fs)[Cfg<DIM, EQ>::NF][Cfg<DIM, EQ>::NQF][Cfg<DIM, EQ>::NV],
+                          double (&cs)[Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 1][Cfg<DIM, EQ>::NV]) {
+  using T = Cfg<DIM, EQ>;
+  constexpr int NV = T::NV;
+  const kfvm_stencil &st = S->w;
+  double ref[NV];
+#pragma unroll
+  for (int v = 0; v < NV; v++) ref[v] = Uc[v * g.pvol];
+  VarConv<EQ> vc(ref, g.gamma);
+  double Vf[T::C][NV];
+  for (int c = 0; c < T::C; c++) {
+    const int64_t o = S->loff[c];
+#pragma unroll
+    for (int v = 0; v < NV; v++) Vf[c][v] = Uc[v * g.pvol + o];
+    vc.cons2LinPrim(Vf[c]);
+  }
+  // smoothness indicators beta_s[v] = sum_i (D_s V_s)_iv^2
+  double om[T::NSUB][NV];
+  for (int s = 0; s < T::NSUB; s++) {
+    const int n = s == 0 ? T::C : (s == 1 ? T::CC : T::CB);
+#pragma unroll
+    for (int v = 0; v < NV; v++) om[s][v] = 0.0;
+    for (int i = 0; i < T::NI; i++) {
+      double b[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) b[v] = 0.0;
+      for (int p = 0; p < n; p++) {
+        const int c = s < 2 ? p : (int)st.sub_idx[s - 2][p];
+        const double w = st.deriv_w[s][i][p];
+#pragma unroll
+        for (int v = 0; v < NV; v++) b[v] += w * Vf[c][v];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; v++) om[s][v] += b[v] * b[v];
+    }
+  }
+  // nonlinear weights, WENO-JS then AO form (createOmegas, Stencil_K.H:556-580)
+  constexpr double gHi = 0.7, gLo = 0.7;
+  double gam[T::NSUB];
+  gam[0] = gHi;
+  gam[1] = (1.0 - gHi) * gLo;
+#pragma unroll
+  for (int s = 2; s < T::NSUB; s++) gam[s] = (1.0 - gHi) * (1.0 - gLo) / (DIM == 2 ? 4.0 : 6.0);
+#pragma unroll
+  for (int v = 0; v < NV; v++) {
+    double tot = 0.0;
+#pragma unroll
+    for (int s = 0; s < T::NSUB; s++) {
+      om[s][v] = gam[s] / (om[s][v] * om[s][v] + 1.e-40);
+      tot += om[s][v];
+    }
+#pragma unroll
+    for (int s = 0; s < T::NSUB; s++) om[s][v] /= tot;
+    om[0][v] /= gam[0];
+#pragma unroll
+    for (int s = 1; s < T::NSUB; s++) om[s][v] -= om[0][v] * gam[s];
+  }
+  // blend the substencil reconstructions (fillRiemannStates / fillInterior)
+  auto blend = [&](const double *W, int ld, double *y, int v) {
+    double acc = 0.0;
+    for (int s = 0; s < T::NSUB; s++) {
+      const int n = s == 0 ? T::C : (s == 1 ? T::CC : T::CB);
+      const double *Ws = W + (size_t)s * ld;
+      double t = 0.0;
+      for (int p = 0; p < n; p++) {
+        const int c = s < 2 ? p : (int)st.sub_idx[s - 2][p];
+        t += Ws[p] * Vf[c][v];
+      }
+      if (s == 0) acc = 0.0;
+      if (om[s][v] != 0.0) acc += om[s][v] * t;
+    }
+    *y = acc;
+  };
+  for (int f = 0; f < T::NF; f++)
+    for (int q = 0; q < T::NQF; q++) {
+#pragma unroll
+      for (int v = 0; v < NV; v++)
+        blend(&st.face_w[0][f][q][0], 6 * KFVM_MAX_FACEQ * KFVM_MAX_CELLS, &fs[f][q][v], v);
+      vc.linPrim2Cons(fs[f][q]);
+    }
+  if constexpr (T::SRC) {
+    for (int q = 0; q < T::NQC; q++) {
+#pragma unroll
+      for (int v = 0; v < NV; v++)
+        blend(&st.cell_w[0][q][0], KFVM_MAX_CELLQ * KFVM_MAX_CELLS, &cs[q][v], v);
+      vc.linPrim2Cons(cs[q]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// positivity limiter of one cell (PositivityPreserve_K, Common_K.H:299-643), split
+// into the admissible bounds (from the 3^d neighbourhood, with the flattener) and
+// the theta scaling of the reconstructed states toward the cell average.
+struct PosBounds {
+  double rDens, minDens, maxDens, minEint;
+};
+
+template <int DIM, int EQ>
+__device__ __forceinline__ PosBounds pos_bounds(const double *__restrict__ Uc, const Grid &g) {
+  using E = Eos<EQ>;
+  constexpr int NV = Eos<EQ>::NV;
+  const double gm = g.gamma;
+  double maxDens = -1.7976931348623157e308, minDens = 1.7976931348623157e308;
+  double minEint = 1.7976931348623157e308, minSdSp = 1.7976931348623157e308;
+  constexpr int zr = DIM == 3 ? 1 : 0;
+  const int64_t sy = g.px, sz = g.px * g.py;
+#pragma unroll
+  for (int xo = -1; xo <= 1; xo++)
+#pragma unroll
+    for (int yo = -1; yo <= 1; yo++)
+#pragma unroll
+      for (int zo = -zr; zo <= zr; zo++) {
+        double s[NV];
+        const int64_t o = xo + yo * sy + zo * sz;
+#pragma unroll
+        for (int v = 0; v < NV; v++) s[v] = Uc[v * g.pvol + o];
+        maxDens = fmax(maxDens, s[DENS]);
+        minDens = fmin(minDens, s[DENS]);
+        minEint = fmin(minEint, E::eint(s));
+        minSdSp = fmin(minSdSp, E::soundspeed(gm, s));
+      }
+  auto U = [&](int64_t o, int v) { return Uc[v * g.pvol + o]; };
+  const double dxU = U(1, MOMX) / U(1, DENS) - U(-1, MOMX) / U(-1, DENS);
+  const double dyV = U(sy, MOMY) / U(sy, DENS) - U(-sy, MOMY) / U(-sy, DENS);
+  const double dzW = U(zr * sz, MOMZ) / U(zr * sz, DENS) - U(-zr * sz, MOMZ) / U(-zr * sz, DENS);
+  const double divV = (dxU + dyV + dzW) / 2.0;
+  double kappa = 0.2;
+  const double eta = fmin(1.0, fmax(0.0, -(kappa * minSdSp + divV) / (kappa * minSdSp)));
+  kappa *= (1.0 - eta);
+  PosBounds b;
+  b.rDens = Uc[DENS * g.pvol];
+  b.maxDens = maxDens * (1.0 + kappa);
+  b.minDens = minDens * (1.0 - kappa);
+  b.minEint = minEint * (1.0 - kappa);
+  return b;
+}
+
+// true when a state leaves theta at 1 in both passes of the limiter
+template <int EQ>
+__device__ __forceinline__ bool pos_inside(const PosBounds &b, const double *s) {
+  const double rho = s[DENS];
+  return rho > b.minDens && rho < b.maxDens && Eos<EQ>::eint(s) > b.minEint;
+}
+
+// the reference's theta computation and mixing on all states of a cell
+template <int DIM, int EQ>
+__device__ double pos_apply(const double *__restrict__ Uc, const Grid &g, const PosBounds &bd,
+                            double (&fs)[Cfg<DIM, EQ>::NF][Cfg<DIM, EQ>::NQF][Cfg<DIM, EQ>::NV],
+                            double (&cs)[Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 1][Cfg<DIM, EQ>::NV]) {
+  using T = Cfg<DIM, EQ>;
+  using E = Eos<EQ>;
+  constexpr int NV = T::NV;
+  double ref[NV];
+#pragma unroll
+  for (int v = 0; v < NV; v++) ref[v] = Uc[v * g.pvol];
+  const double rDens = bd.rDens, minDens = bd.minDens, maxDens = bd.maxDens, minEint = bd.minEint;
+  const double rDP = maxDens - rDens, rDM = rDens - minDens;
+  double thD = 1.0;
+  for (int q = 0; q < T::NQF; q++)
+    for (int f = 0; f < T::NF; f++) {
+      const double rho = fs[f][q][DENS];
+      thD = rho > minDens ? thD : fmin(thD, rDM / (rDens - rho));
+      thD = rho < maxDens ? thD : fmin(thD, rDP / (rho - rDens));
+    }
+  if constexpr (T::SRC) {
+    for (int q = 0; q < T::NQC; q++) {
+      const double rho = cs[q][DENS];
+      thD = rho > minDens ? thD : fmin(thD, rDM / (rDens - rho));
+      thD = rho < maxDens ? thD : fmin(thD, rDP / (rho - rDens));
+    }
+  }
+  auto mix = [&](double th) {
+    for (int f = 0; f < T::NF; f++)
+      for (int q = 0; q < T::NQF; q++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) fs[f][q][v] = ref[v] + th * (fs[f][q][v] - ref[v]);
+    if constexpr (T::SRC) {
+      for (int q = 0; q < T::NQC; q++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) cs[q][v] = ref[v] + th * (cs[q][v] - ref[v]);
+    }
+  };
+  auto replace = [&]() {
+    for (int f = 0; f < T::NF; f++)
+      for (int q = 0; q < T::NQF; q++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) fs[f][q][v] = ref[v];
+    if constexpr (T::SRC) {
+      for (int q = 0; q < T::NQC; q++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) cs[q][v] = ref[v];
+    }
+  };
+  if (thD > 0.0 && thD < 1.0) mix(thD);
+  else if (thD < 1.0) replace();
+
+  auto eintPos = [&](const double *state) {
+    double a = 0.0, b = 1.0;
+    double st[NV];
+    for (int it = 0; it < 10; it++) {
+      const double c = 0.5 * (a + b);
+#pragma unroll
+      for (int v = 0; v < NV; v++) st[v] = ref[v] + c * (state[v] - ref[v]);
+      const double dec = E::eint(st) - minEint;
+      if (dec > 0.0) a = c;
+      else b = c;
+    }
+    return a;
+  };
+  double thP = 1.0;
+  for (int q = 0; q < T::NQF; q++)
+    for (int f = 0; f < T::NF; f++) {
+      const double ei = E::eint(fs[f][q]);
+      if (!(ei > minEint)) thP = fmin(thP, eintPos(fs[f][q]));
+    }
+  if constexpr (T::SRC) {
+    for (int q = 0; q < T::NQC; q++) {
+      const double ei = E::eint(cs[q]);
+      if (!(ei > minEint)) thP = fmin(thP, eintPos(cs[q]));
+    }
+  }
+  if (thP > 0.0 && thP < 1.0) mix(thP);
+  else if (thP < 1.0) replace();
+  return fmin(thD, thP);
+}
+
+} // namespace kfvm

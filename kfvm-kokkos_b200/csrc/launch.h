@@ -1,0 +1,60 @@
+// launch.h -- host-side entry points of the kernels in kernels.cu
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace kfvm {
+
+struct StageArgs {
+  const double *U;     // stage state (padded, halo filled)
+  double *Unext;       // next stage state (padded), STAGE_UPDATE only
+  const double *Uprev; // state at the start of the step (padded)
+  double *Uhat, *Utmp, *K;
+  double *const *G;    // per-direction face fluxes
+  double *const *F;    // per-direction face states (GLM sources)
+  const double *src;   // interior point values (GLM)
+  const double *theta;
+  int mode;            // enum StageMode
+  StageCoef co;
+  double Re, Pr, atol, rtol;
+  double *part;        // block partials of the error estimate
+  DevScalars *sc;
+};
+
+int64_t stage_blocks(const Grid &g);
+cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s);
+// KXRCF selection; W are per-direction [slot][q][face] scratch arrays (the
+// face-state buffers are reused: the indicator is consumed before they are written)
+cudaError_t launch_select(int dim, int eq, const double *U, const Grid &g, double *const *W,
+                          cudaStream_t s);
+cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, double *const *W,
+                        const double *theta, uint8_t *flag, DevScalars *sc, double thr,
+                        cudaStream_t s);
+cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
+                         double *theta, double *const *F, double *src, const uint32_t *heavy,
+                         DevScalars *sc, int heavy_blocks, cudaStream_t s);
+cudaError_t upload_linear_weights(int dim, const kfvm_stencil &st, cudaStream_t s);
+// final face states: light linear pass over all cells, then the heavy pass over the
+// compacted list of WENO / limited cells (heavy holds up to one entry per cell)
+cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
+                         int mode, const uint8_t *flag, uint8_t *wset, uint8_t *applied,
+                         double *theta, double *const *F, double *src, uint32_t *heavy,
+                         DevScalars *sc, int heavy_blocks, cudaStream_t s);
+cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
+                           DevScalars *sc, cudaStream_t s);
+cudaError_t launch_stage(int dim, int eq, const StageArgs &a, const Grid &g, cudaStream_t s);
+cudaError_t launch_stage_pre(int dim, int eq, double *U1, const double *Uprev, double *Uhat,
+                             double *Utmp, const double *K, const Grid &g, double betaDt,
+                             double bhatDt, int use_tmp, cudaStream_t s);
+cudaError_t launch_copy(int dim, int eq, double *dst, const double *src, const Grid &g,
+                        cudaStream_t s);
+cudaError_t launch_ic(int dim, int eq, int ic_kind, uint64_t seed, const kfvm_config &cfg,
+                      double *U, const Grid &g, cudaStream_t s);
+
+int build_stencil(const kfvm_config *cfg, kfvm_stencil *st);
+
+} // namespace kfvm

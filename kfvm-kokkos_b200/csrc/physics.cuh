@@ -1,0 +1,274 @@
+// physics.cuh -- device-side equation-of-state, flux and Riemann-solver
+// functions for the Euler, Navier-Stokes and GLM-MHD systems, FP64.
+//
+// Restates (slug-cfd/kfvm-kokkos):
+//   src/physics/hydro/Hydro_EOS.H:22-92          EOS<Hydro>
+//   src/physics/navierstokes/NavierStokes_EOS.H   EOS<NavierStokes> (same algebra)
+//   src/physics/mhd_glm/MHD_GLM_EOS.H:22-128      EOS<MHD_GLM>
+//   src/physics/hydro/Hydro_Riemann.H:26-187      Euler flux, Batten/Roe speeds, HLLC
+//   src/physics/mhd_glm/MHD_GLM_Riemann.H:25-99   GLM flux, Davis + Wu-Shu speeds
+//   src/physics/Common_K.H:23-63                  HLL / LLF in Batten's form
+//   src/physics/Riemann.H:15-45                   HLLC star-state helpers
+//   src/physics/*/_K.H VarConvert                 linearised primitive variables
+// The arithmetic follows the reference expression by expression; nvcc may fuse
+// multiply-adds, so results agree with the CPU oracle to rounding, not bitwise.
+#pragma once
+
+#include <cstdint>
+
+namespace kfvm {
+
+enum { DENS = 0, MOMX = 1, MOMY = 2, MOMZ = 3, ETOT = 4, MAGX = 5, MAGY = 6, MAGZ = 7, PSI = 8 };
+enum { EQ_HYDRO = 0, EQ_NS = 1, EQ_GLM = 2 };
+enum { RS_LLF = 0, RS_HLL = 1, RS_HLLC = 2 };
+
+template <int EQ>
+struct Eos {
+  static constexpr int NV = EQ == EQ_GLM ? 9 : 5;
+
+  __device__ __forceinline__ static double ekin(const double *U) {
+    return 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]) / U[DENS];
+  }
+  __device__ __forceinline__ static double prsb(const double *U) {
+    return 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
+  }
+  __device__ __forceinline__ static double eint(const double *U) {
+    if constexpr (EQ == EQ_GLM) {
+      return (U[ETOT] - prsb(U) - ekin(U) - 0.5 * U[PSI] * U[PSI]);
+    } else {
+      return (U[ETOT] - ekin(U));
+    }
+  }
+  __device__ __forceinline__ static double pres(double g, const double *U) {
+    return (g - 1.0) * eint(U);
+  }
+  __device__ __forceinline__ static double soundspeed(double g, const double *U) {
+    return sqrt(g * pres(g, U) / U[DENS]);
+  }
+  // KXRCF indicator variable p / rho^gamma
+  __device__ __forceinline__ static double weno(double g, const double *U) {
+    return pres(g, U) / pow(U[DENS], g);
+  }
+  __device__ __forceinline__ static double positivity(const double *U) {
+    if constexpr (EQ == EQ_GLM) {
+#pragma unroll
+      for (int v = 0; v < NV; v++)
+        if (isnan(U[v])) return -1.0;
+    }
+    return fmin(U[DENS], eint(U));
+  }
+  __device__ __forceinline__ static void cons2prim(double g, const double *U, double *V) {
+    V[0] = U[DENS];
+    V[1] = U[MOMX] / U[DENS];
+    V[2] = U[MOMY] / U[DENS];
+    V[3] = U[MOMZ] / U[DENS];
+    V[4] = pres(g, U);
+    if constexpr (EQ == EQ_GLM) {
+      V[5] = U[MAGX];
+      V[6] = U[MAGY];
+      V[7] = U[MAGZ];
+      V[8] = U[PSI];
+    }
+  }
+  __device__ __forceinline__ static double fastMagSonic(double g, const double *U, double bl) {
+    const double asq = g * pres(g, U) / U[DENS];
+    const double bsq = 2.0 * prsb(U) / U[DENS];
+    const double blsq = bl * bl / U[DENS];
+    const double absq = asq + bsq;
+    return sqrt(0.5 * (absq + sqrt(absq * absq - 4.0 * asq * blsq)));
+  }
+
+  // physical flux in direction ord[0]
+  __device__ __forceinline__ static void flux(double ch, const int *vo, const int *bo,
+                                              const double *U, const double *V, double *F) {
+    if constexpr (EQ != EQ_GLM) {
+      (void)ch;
+      (void)bo;
+      F[DENS] = U[vo[0]];
+      F[vo[0]] = U[vo[0]] * V[vo[0]] + V[4];
+      F[vo[1]] = U[vo[0]] * V[vo[1]];
+      F[vo[2]] = U[vo[0]] * V[vo[2]];
+      F[ETOT] = V[vo[0]] * (U[ETOT] + V[4]);
+    } else {
+      const double mx = U[vo[0]];
+      const double vx = V[vo[0]], vy = V[vo[1]], vz = V[vo[2]];
+      const double bx = U[bo[0]], by = U[bo[1]], bz = U[bo[2]];
+      const double et = U[ETOT], pg = V[4];
+      const double chpsi = ch * U[PSI], hpsisq = 0.5 * U[PSI] * U[PSI];
+      const double uDb = vx * bx + vy * by + vz * bz, bsq = bx * bx + by * by + bz * bz;
+      const double pt = pg + 0.5 * bsq;
+      F[DENS] = mx;
+      F[vo[0]] = mx * vx + pt - bx * bx;
+      F[vo[1]] = mx * vy - bx * by;
+      F[vo[2]] = mx * vz - bx * bz;
+      F[ETOT] = vx * (et + pt - hpsisq) + bx * (chpsi - uDb);
+      F[bo[0]] = chpsi;
+      F[bo[1]] = vx * by - vy * bx;
+      F[bo[2]] = vx * bz - vz * bx;
+      F[PSI] = ch * bx;
+    }
+  }
+
+  __device__ __forceinline__ static double roeAvg(double rL, double rR, double qL, double qR) {
+    return (qL * sqrt(rL) + qR * sqrt(rR)) / (sqrt(rL) + sqrt(rR));
+  }
+
+  __device__ __forceinline__ static double speeds(double g, double ch, const int *vo,
+                                                  const int *bo, const double *uL,
+                                                  const double *uR, const double *vL,
+                                                  const double *vR, double &sL, double &sR) {
+    if constexpr (EQ != EQ_GLM) {
+      (void)ch;
+      (void)bo;
+      const double rhoL = uL[DENS], rhoR = uR[DENS];
+      const double hL = (uL[ETOT] + vL[4]) / rhoL, hR = (uR[ETOT] + vR[4]) / rhoR;
+      const double aL = soundspeed(g, uL), aR = soundspeed(g, uR);
+      const double uTil = roeAvg(rhoL, rhoR, vL[vo[0]], vR[vo[0]]),
+                   vTil = roeAvg(rhoL, rhoR, vL[vo[1]], vR[vo[1]]),
+                   wTil = roeAvg(rhoL, rhoR, vL[vo[2]], vR[vo[2]]),
+                   vsqTil = uTil * uTil + vTil * vTil + wTil * wTil,
+                   hTil = roeAvg(rhoL, rhoR, hL, hR),
+                   aTil = sqrt((g - 1.0) * (hTil - 0.5 * vsqTil));
+      sL = fmin(vL[vo[0]] - aL, uTil - aTil);
+      sR = fmax(vR[vo[0]] + aR, uTil + aTil);
+      return fmax(fabs(sL), fabs(sR));
+    } else {
+      const double cfL = fastMagSonic(g, uL, uL[bo[0]]);
+      const double cfR = fastMagSonic(g, uR, uR[bo[0]]);
+      const double sdL = fmin(vL[vo[0]] - fmax(ch, cfL), vR[vo[0]] - fmax(ch, cfR));
+      const double sdR = fmax(vL[vo[0]] + fmax(ch, cfL), vR[vo[0]] + fmax(ch, cfR));
+      const double rtL = sqrt(uL[DENS]), rtR = sqrt(uR[DENS]);
+      const double rtSum = rtL + rtR, vSum = (rtL * vL[vo[0]] + rtR * vR[vo[0]]) / rtSum;
+      const double b0 = uL[bo[0]] - uR[bo[0]], b1 = uL[bo[1]] - uR[bo[1]],
+                   b2 = uL[bo[2]] - uR[bo[2]];
+      const double bnDiff = sqrt(b0 * b0 + b1 * b1 + b2 * b2) / rtSum;
+      const double aL = fmin(vL[vo[0]], vSum) - cfL - bnDiff;
+      const double aR = fmin(vR[vo[0]], vSum) + cfR + bnDiff;
+      sL = fmin(sdL, aL);
+      sR = fmax(sdR, aR);
+      return fmax(fabs(sL), fabs(sR));
+    }
+  }
+
+  // Riemann solve at one face point in direction dir; returns max(|sL|,|sR|)
+  __device__ __forceinline__ static double solve(int rs, double g, double ch, int dir,
+                                                 const double *uL, const double *uR,
+                                                 double *F) {
+    const int ord[3] = {dir, (dir + 1) % 3, (dir + 2) % 3};
+    const int vo[3] = {MOMX + ord[0], MOMX + ord[1], MOMX + ord[2]};
+    const int bo[3] = {MAGX + ord[0], MAGX + ord[1], MAGX + ord[2]};
+    double vL[NV], vR[NV];
+    cons2prim(g, uL, vL);
+    cons2prim(g, uR, vR);
+    double sL, sR;
+    const double sMax = speeds(g, ch, vo, bo, uL, uR, vL, vR, sL, sR);
+    if constexpr (EQ != EQ_GLM) {
+      if (rs == RS_HLLC) {
+        const double vsqL = vL[1] * vL[1] + vL[2] * vL[2] + vL[3] * vL[3];
+        const double vsqR = vR[1] * vR[1] + vR[2] * vR[2] + vR[3] * vR[3];
+        const double aL = soundspeed(g, uL), aR = soundspeed(g, uR);
+        double M = fmax(sqrt(vsqL) / aL, sqrt(vsqR) / aR);
+        const double rhoL = vL[0], rhoR = vR[0], pL = vL[4], pR = vR[4];
+        const double uLn = vL[vo[0]], uRn = vR[vo[0]];
+        const double sS = ((pR - pL) + (rhoL * uLn * (sL - uLn) - rhoR * uRn * (sR - uRn))) /
+                          (rhoL * (sL - uLn) - rhoR * (sR - uRn));
+        const double psL = rhoL * (sL - uLn), psR = rhoR * (sR - uRn);
+        const double pS = 0.5 * ((pL + pR) + psL * (sS - uLn) + psR * (sS - uRn));
+        const double sFacL = sS / (sL - sS), sFacR = sS / (sR - sS);
+        const double uJump = vR[vo[0]] - vL[vo[0]], vJump = vR[vo[1]] - vL[vo[1]],
+                     wJump = vR[vo[2]] - vL[vo[2]];
+        const double psiL = uL[DENS] * (sL - vL[vo[0]]), psiR = uR[DENS] * (sR - vR[vo[0]]),
+                     psiFac = psiR * psiL / (psiR - psiL);
+        const double presRat = fmin(vL[4] / vR[4], vR[4] / vL[4]);
+        const double gFac = 1.0 - pow(presRat, M);
+        const double shFacL = psiFac * gFac * sL / (sL - sS),
+                     shFacR = psiFac * gFac * sR / (sR - sS);
+        M = fmin(M, 1.0);
+        const double omm = 1.0 - M * M;
+        const double fM = M * sqrt(4.0 + omm * omm) / (1.0 + M * M);
+        const double pFacL = psiFac * (fM - 1.0) * uJump + sL * pS / (sL - sS);
+        const double pFacR = psiFac * (fM - 1.0) * uJump + sR * pS / (sR - sS);
+        if (0 <= sL) {
+          flux(ch, vo, bo, uL, vL, F);
+        } else if (0 <= sS) {
+          flux(ch, vo, bo, uL, vL, F);
+          F[DENS] = sFacL * (sL * uL[DENS] - F[DENS]);
+          F[vo[0]] = sFacL * (sL * uL[vo[0]] - F[vo[0]]) + pFacL;
+          F[vo[1]] = sFacL * (sL * uL[vo[1]] - F[vo[1]]) + shFacL * vJump;
+          F[vo[2]] = sFacL * (sL * uL[vo[2]] - F[vo[2]]) + shFacL * wJump;
+          F[ETOT] = sFacL * (sL * uL[ETOT] - F[ETOT]) + sS * pFacL;
+        } else if (0 < sR) {
+          flux(ch, vo, bo, uR, vR, F);
+          F[DENS] = sFacR * (sR * uR[DENS] - F[DENS]);
+          F[vo[0]] = sFacR * (sR * uR[vo[0]] - F[vo[0]]) + pFacR;
+          F[vo[1]] = sFacR * (sR * uR[vo[1]] - F[vo[1]]) + shFacR * vJump;
+          F[vo[2]] = sFacR * (sR * uR[vo[2]] - F[vo[2]]) + shFacR * wJump;
+          F[ETOT] = sFacR * (sR * uR[ETOT] - F[ETOT]) + sS * pFacR;
+        } else {
+          flux(ch, vo, bo, uR, vR, F);
+        }
+        return sMax;
+      }
+    }
+    if (rs == RS_LLF) {
+      sL = -sMax;
+      sR = sMax;
+    }
+    const double tR = (fmin(0.0, sR) - fmin(0.0, sL)) / (sR - sL), tL = 1.0 - tR;
+    const double tD = 0.5 * (sR * fabs(sL) - sL * fabs(sR)) / (sR - sL);
+    double FR[NV];
+    flux(ch, vo, bo, uL, vL, F);
+    flux(ch, vo, bo, uR, vR, FR);
+#pragma unroll
+    for (int v = 0; v < NV; v++) F[v] = tL * F[v] + tR * FR[v] - tD * (uR[v] - uL[v]);
+    return sMax;
+  }
+};
+
+// Linearisation of the conserved variables about a reference state
+template <int EQ>
+struct VarConv {
+  double gamm, rho, u, v, w, bx, by, bz, rPsi, vsq;
+  __device__ __forceinline__ VarConv(const double *ref, double gam) {
+    gamm = gam - 1.0;
+    rho = ref[DENS];
+    u = ref[MOMX] / rho;
+    v = ref[MOMY] / rho;
+    w = ref[MOMZ] / rho;
+    if constexpr (EQ == EQ_GLM) {
+      bx = ref[MAGX];
+      by = ref[MAGY];
+      bz = ref[MAGZ];
+      rPsi = ref[PSI];
+      vsq = (u * u + v * v + w * w) / 2.0;
+    } else {
+      bx = by = bz = rPsi = 0.0;
+      vsq = 0.5 * (u * u + v * v + w * w);
+    }
+  }
+  __device__ __forceinline__ void cons2LinPrim(double *s) const {
+    if constexpr (EQ == EQ_GLM) {
+      s[ETOT] = gamm * (vsq * s[DENS] + s[ETOT] - u * s[MOMX] - v * s[MOMY] - w * s[MOMZ] -
+                        bx * s[MAGX] - by * s[MAGY] - bz * s[MAGZ] - rPsi * s[PSI]);
+    } else {
+      s[ETOT] = gamm * (vsq * s[DENS] - u * s[MOMX] - v * s[MOMY] - w * s[MOMZ] + s[ETOT]);
+    }
+    s[MOMX] = (s[MOMX] - u * s[DENS]) / rho;
+    s[MOMY] = (s[MOMY] - v * s[DENS]) / rho;
+    s[MOMZ] = (s[MOMZ] - w * s[DENS]) / rho;
+  }
+  __device__ __forceinline__ void linPrim2Cons(double *s) const {
+    if constexpr (EQ == EQ_GLM) {
+      s[ETOT] = (vsq * s[DENS] + rho * u * s[MOMX] + rho * v * s[MOMY] + rho * w * s[MOMZ] +
+                 bx * s[MAGX] + by * s[MAGY] + bz * s[MAGZ] + s[ETOT] / gamm + rPsi * s[PSI]);
+    } else {
+      s[ETOT] = (vsq * s[DENS] + rho * u * s[MOMX] + rho * v * s[MOMY] + rho * w * s[MOMZ] +
+                 s[ETOT] / gamm);
+    }
+    s[MOMX] = (rho * s[MOMX] + u * s[DENS]);
+    s[MOMY] = (rho * s[MOMY] + v * s[DENS]);
+    s[MOMZ] = (rho * s[MOMZ] + w * s[DENS]);
+  }
+};
+
+} // namespace kfvm
