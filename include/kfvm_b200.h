@@ -180,6 +180,9 @@ int kfvm_solve(kfvm_solver *s, int32_t max_steps, int64_t *n_steps_out,
 
 /* Current simulation time and dt (Solver::time, Solver::dt). */
 int kfvm_get_time(kfvm_solver *s, double *time, double *dt);
+/* Sets the simulation time and the size of the next step, as a restart from a
+ * checkpoint does (Solver::Solver reading time and dt, src/Solver.cpp:57-66). */
+int kfvm_set_time(kfvm_solver *s, double time, double dt);
 
 /* Selects the troubled-cell indicator (enum kfvm_indicator). */
 int kfvm_set_indicator(kfvm_solver *s, int32_t indicator);

@@ -734,6 +734,13 @@ int kfvm_get_time(kfvm_solver *s, double *time, double *dt) {
   return KFVM_OK;
 }
 
+int kfvm_set_time(kfvm_solver *s, double time, double dt) {
+  if (!s || !(dt > 0.0)) return fail(KFVM_ERR_ARG, "bad argument");
+  s->time = time;
+  s->dt = dt;
+  return KFVM_OK;
+}
+
 int kfvm_set_indicator(kfvm_solver *s, int32_t ind) {
   if (!s || ind < 0 || ind > KFVM_IND_NONE) return fail(KFVM_ERR_ARG, "bad indicator");
   s->indicator = ind;

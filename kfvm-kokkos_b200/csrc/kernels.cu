@@ -98,14 +98,18 @@ __device__ __forceinline__ void lin_rows(const double *__restrict__ Uc, const Gr
   for (int p = 0; p < NP; p++)
 #pragma unroll
     for (int v = 0; v < T::NV; v++) st[p][v] = 0.0;
+  // stencil cell outermost: each weight is brought into a register once and
+  // feeds all NV variables; per output the sum over cells keeps the reference's order
 #pragma unroll
-  for (int v = 0; v < T::NV; v++) {
-    const double *Uv = Uc + v * g.pvol;
+  for (int c = 0; c < T::C; c++) {
+    double u[T::NV];
 #pragma unroll
-    for (int c = 0; c < T::C; c++) {
-      const double u = __ldg(Uv + g.loff[c]);
+    for (int v = 0; v < T::NV; v++) u[v] = __ldg(Uc + v * g.pvol + g.loff[c]);
 #pragma unroll
-      for (int p = 0; p < NP; p++) st[p][v] += cw<DIM>((R0 + p) * T::C + c) * u;
+    for (int p = 0; p < NP; p++) {
+      const double w = cw<DIM>((R0 + p) * T::C + c);
+#pragma unroll
+      for (int v = 0; v < T::NV; v++) st[p][v] += w * u[v];
     }
   }
 }
@@ -251,6 +255,73 @@ __device__ __forceinline__ bool recon_group(const double *__restrict__ Uc, const
   return ok;
 }
 
+// Per-block footprint (block cells plus a one-cell ring) of the cell quantities the
+// limiter's bounds read from the 3^d neighbourhood: rho, eint, sound speed and the
+// three velocities.  Each is computed once per cell instead of once per neighbour.
+template <int DIM>
+struct PosTile {
+  static constexpr int TX = kBlockX + 2, TY = kBlockY + 2, TZ = DIM == 3 ? 3 : 1;
+  static constexpr int N = TX * TY * TZ;
+};
+
+template <int DIM, int EQ>
+__device__ __forceinline__ void pos_tile_fill(const double *__restrict__ U, const Grid &g, int64_t i0,
+                                              int64_t j0, int64_t k, double (*sm)[PosTile<DIM>::N]) {
+  using P = PosTile<DIM>;
+  using E = Eos<EQ>;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int t = tid; t < P::N; t += blockDim.x * blockDim.y) {
+    const int a = t % P::TX, b = (t / P::TX) % P::TY, cz = t / (P::TX * P::TY);
+    const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b, gk = k - (DIM == 3 ? 1 : 0) + cz;
+    if (gi > g.nx || gj > g.ny) continue; // beyond the ring of any live cell
+    const double *Uc = U + pidx(g, gi, gj, gk);
+    double st[E::NV];
+#pragma unroll
+    for (int v = 0; v < E::NV; v++) st[v] = Uc[v * g.pvol];
+    sm[0][t] = st[DENS];
+    sm[1][t] = E::eint(st);
+    sm[2][t] = E::soundspeed(g.gamma, st);
+    sm[3][t] = st[MOMX] / st[DENS];
+    sm[4][t] = st[MOMY] / st[DENS];
+    sm[5][t] = st[MOMZ] / st[DENS];
+  }
+}
+
+// PositivityPreserve_K bounds (Common_K.H:331-380) from the footprint tile
+template <int DIM, int EQ>
+__device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<DIM>::N], int tx, int ty) {
+  using P = PosTile<DIM>;
+  double maxDens = -1.7976931348623157e308, minDens = 1.7976931348623157e308;
+  double minEint = 1.7976931348623157e308, minSdSp = 1.7976931348623157e308;
+  constexpr int zr = DIM == 3 ? 1 : 0;
+  auto at = [&](int xo, int yo, int zo) { return ((zr + zo) * P::TY + (ty + 1 + yo)) * P::TX + (tx + 1 + xo); };
+#pragma unroll
+  for (int xo = -1; xo <= 1; xo++)
+#pragma unroll
+    for (int yo = -1; yo <= 1; yo++)
+#pragma unroll
+      for (int zo = -zr; zo <= zr; zo++) {
+        const int t = at(xo, yo, zo);
+        maxDens = fmax(maxDens, sm[0][t]);
+        minDens = fmin(minDens, sm[0][t]);
+        minEint = fmin(minEint, sm[1][t]);
+        minSdSp = fmin(minSdSp, sm[2][t]);
+      }
+  const double dxU = sm[3][at(1, 0, 0)] - sm[3][at(-1, 0, 0)];
+  const double dyV = sm[4][at(0, 1, 0)] - sm[4][at(0, -1, 0)];
+  const double dzW = sm[5][at(0, 0, zr)] - sm[5][at(0, 0, -zr)];
+  const double divV = (dxU + dyV + dzW) / 2.0;
+  double kappa = 0.2;
+  const double eta = fmin(1.0, fmax(0.0, -(kappa * minSdSp + divV) / (kappa * minSdSp)));
+  kappa *= (1.0 - eta);
+  PosBounds b;
+  b.rDens = sm[0][at(0, 0, 0)];
+  b.maxDens = maxDens * (1.0 + kappa);
+  b.minDens = minDens * (1.0 - kappa);
+  b.minEint = minEint * (1.0 - kappa);
+  return b;
+}
+
 template <int DIM, int EQ>
 __global__ void __launch_bounds__(128)
     recon_kernel(const double *__restrict__ U, Grid g, int mode, const uint8_t *__restrict__ flag,
@@ -263,6 +334,9 @@ __global__ void __launch_bounds__(128)
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
   const int64_t k = blockIdx.z;
+  __shared__ double tile[6][PosTile<DIM>::N];
+  pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)blockDim.x, blockIdx.y * (int64_t)blockDim.y, k, tile);
+  __syncthreads();
   bool useWeno = false, push = false;
   double lam = 0.0, vel = 0.0;
   int64_t c = 0;
@@ -285,7 +359,7 @@ __global__ void __launch_bounds__(128)
       push = true;
     } else {
       const double *Uc = U + pidx(g, i, j, k);
-      const PosBounds bd = pos_bounds<DIM, EQ>(Uc, g);
+      const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
       double *F[3] = {F0, F1, F2};
       bool ok = recon_group<DIM, EQ, 0>(Uc, g, bd, i, j, k, F, lam, vel);
       if constexpr (T::SRC) {

@@ -46,6 +46,7 @@ def lib():
         L.kfvm_take_step.argtypes = [P, C.POINTER(abi.KfvmStepInfo)]
         L.kfvm_solve.argtypes = [P, I32, C.POINTER(I64), C.POINTER(abi.KfvmStepInfo)]
         L.kfvm_get_time.argtypes = [P, P, P]
+        L.kfvm_set_time.argtypes = [P, D, D]
         L.kfvm_set_indicator.argtypes = [P, I32]
         L.kfvm_get_faces.argtypes = [P, I32, P]
         L.kfvm_get_flags.argtypes = [P, P, P]
@@ -124,6 +125,9 @@ class Solver:
         t, dt = C.c_double(), C.c_double()
         _check(lib().kfvm_get_time(self.h, C.addressof(t), C.addressof(dt)), "kfvm_get_time")
         return t.value, dt.value
+
+    def set_time(self, t, dt):
+        _check(lib().kfvm_set_time(self.h, float(t), float(dt)), "kfvm_set_time")
 
     def set_indicator(self, ind):
         _check(lib().kfvm_set_indicator(self.h, int(ind)), "kfvm_set_indicator")

@@ -29,6 +29,7 @@ int orc_eval_rhs(orc_solver *s, double t, double *rhs, double *max_vel);
 int orc_take_step(orc_solver *s, kfvm_step_info *info);
 int orc_solve(orc_solver *s, int32_t max_steps, int64_t *n_steps, kfvm_step_info *last);
 int orc_get_time(orc_solver *s, double *time, double *dt);
+int orc_set_time(orc_solver *s, double time, double dt);
 /* Keep a copy of the face states before the Riemann solve for orc_get_faces. */
 int orc_keep_faces(orc_solver *s, int32_t on);
 int orc_get_faces(orc_solver *s, int32_t dir, double *out);

@@ -47,6 +47,7 @@ def lib():
         L.orc_take_step.argtypes = [P, C.POINTER(abi.KfvmStepInfo)]
         L.orc_solve.argtypes = [P, I32, C.POINTER(I64), C.POINTER(abi.KfvmStepInfo)]
         L.orc_get_time.argtypes = [P, P, P]
+        L.orc_set_time.argtypes = [P, D, D]
         L.orc_get_faces.argtypes = [P, I32, P]
         L.orc_keep_faces.argtypes = [P, I32]
         L.orc_get_flags.argtypes = [P, P, P]
@@ -143,6 +144,9 @@ class OracleSolver:
         t, dt = C.c_double(), C.c_double()
         lib().orc_get_time(self.h, C.addressof(t), C.addressof(dt))
         return t.value, dt.value
+
+    def set_time(self, t, dt):
+        assert lib().orc_set_time(self.h, float(t), float(dt)) == 0
 
     def keep_faces(self, on=True):
         assert lib().orc_keep_faces(self.h, 1 if on else 0) == 0

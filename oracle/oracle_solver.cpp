@@ -1554,6 +1554,13 @@ int orc_solve(orc_solver *s, int32_t max_steps, int64_t *n_steps, kfvm_step_info
   return 0;
 }
 
+int orc_set_time(orc_solver *s, double time, double dt) {
+  if (!s || !(dt > 0.0)) return KFVM_ERR_ARG;
+  s->time = time;
+  s->dt = dt;
+  return 0;
+}
+
 int orc_get_time(orc_solver *s, double *time, double *dt) {
   if (!s) return KFVM_ERR_ARG;
   if (time) *time = s->time;
