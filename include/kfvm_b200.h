@@ -169,6 +169,15 @@ int kfvm_get_state(kfvm_solver *s, double *u_host);
  * SoA interior layout; max_vel (nullable) the max wave speed. */
 int kfvm_eval_rhs(kfvm_solver *s, double t, double *rhs_host, double *max_vel);
 
+/* Embedded error estimate of a state pair (RKFSAL_ErrEst_K,
+ * src/numeric/Numeric_K.H:262-290): err = sum over cells and variables of
+ * ((u-uhat)/(atol+rtol*max(|u|,|uhat|)))^2 with the solver's atol/rtol, and
+ * posmin = min over cells of the positivity function (-1 where u holds a NaN).
+ * u_dev and uhat_dev are device arrays in SoA interior layout of this solver's
+ * grid; err and posmin are host pointers.  Uses the solver's scratch memory. */
+int kfvm_err_est(kfvm_solver *s, const double *u_dev, const double *uhat_dev, double *err,
+                 double *posmin);
+
 /* One adaptive FSAL time step.  Replaces Solver::TakeStep (src/Solver.cpp:188-343). */
 int kfvm_take_step(kfvm_solver *s, kfvm_step_info *info);
 

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <string>
@@ -598,8 +599,10 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     s->heavyBlocks = (nsm > 0 ? nsm : 148) * 4; // grid-stride over the device-side count
   }
-  if ((e = dalloc((void **)&s->part, 2 * stage_blocks(g) * sizeof(double))) != cudaSuccess)
-    return cleanup(e, "alloc");
+  {
+    const int64_t nb = std::max(stage_blocks(g), errest_blocks(g.n));
+    if ((e = dalloc((void **)&s->part, 2 * nb * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
+  }
   if ((e = dalloc((void **)&s->sc, sizeof(DevScalars))) != cudaSuccess) return cleanup(e, "alloc");
   if ((e = cudaMallocHost((void **)&s->hsc, sizeof(DevScalars))) != cudaSuccess) return cleanup(e, "alloc host");
   for (int b = 0; b < 3; b++)
@@ -704,6 +707,21 @@ int kfvm_eval_rhs(kfvm_solver *s, double t, double *rhs, double *max_vel) {
   CK(cudaStreamSynchronize(s->stream));
   s->nWenoLast = s->hsc->napplied;
   if (max_vel) *max_vel = bits_to_double(s->hsc->maxvel_bits);
+  return KFVM_OK;
+}
+
+int kfvm_err_est(kfvm_solver *s, const double *u_dev, const double *uhat_dev, double *err,
+                 double *posmin) {
+  if (!s || !u_dev || !uhat_dev) return fail(KFVM_ERR_ARG, "null argument");
+  cudaError_t e = run(s, KFVM_KCLASS_OTHER, 2, [&] {
+    return kfvm::launch_errest(s->eq, u_dev, uhat_dev, s->g.n, s->cfg.atol, s->cfg.rtol, s->part, &s->sc->err,
+                               s->stream);
+  });
+  if (e != cudaSuccess) return set_err_cuda(e, "err_est");
+  CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(kfvm::DevScalars), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (err) *err = s->hsc->err;
+  if (posmin) *posmin = s->hsc->posmin;
   return KFVM_OK;
 }
 

@@ -1,0 +1,98 @@
+// errest.cu -- the embedded RK error estimate and positivity check over a state
+// pair (RKFSAL_ErrEst_K, src/numeric/Numeric_K.H:262-290 of slug-cfd/kfvm-kokkos):
+//   err    = sum over cells and variables of ((u - uhat) / (atol + rtol max(|u|,|uhat|)))^2
+//   posmin = min over cells of EOS::positivity(u), or -1 where u holds a NaN
+// Deterministic two-level reduction: one partial per block of kErrBlock cells,
+// then a fixed-order sum in one block.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "launch.h"
+
+namespace kfvm {
+
+constexpr int kErrBlock = 256;
+
+template <int EQ>
+__global__ void __launch_bounds__(kErrBlock)
+    errest_kernel(const double *__restrict__ u, const double *__restrict__ uhat, int64_t n,
+                  double atol, double rtol, double *__restrict__ part) {
+  using E = Eos<EQ>;
+  constexpr int NV = E::NV;
+  const int64_t c = blockIdx.x * (int64_t)kErrBlock + threadIdx.x;
+  double err = 0.0, pos = 1.0;
+  if (c < n) {
+    bool hasNan = false;
+    double st[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      const double a = u[v * n + c], b = uhat[v * n + c];
+      st[v] = a;
+      hasNan = hasNan || isnan(a);
+      const double e = (a - b) / (atol + rtol * fmax(fabs(a), fabs(b)));
+      err += e * e;
+    }
+    pos = hasNan ? -1.0 : E::positivity(st);
+  }
+  __shared__ double se[kErrBlock / 32], sp[kErrBlock / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    err += __shfl_xor_sync(0xffffffffu, err, o);
+    pos = fmin(pos, __shfl_xor_sync(0xffffffffu, pos, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    se[threadIdx.x >> 5] = err;
+    sp[threadIdx.x >> 5] = pos;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 1.0;
+    for (int w = 0; w < kErrBlock / 32; w++) {
+      a += se[w];
+      b = b > sp[w] ? sp[w] : b;
+    }
+    part[2 * blockIdx.x] = a;
+    part[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// fixed-order combination of the block partials into out[0] (sum) and out[1] (min)
+__global__ void __launch_bounds__(1024) errest_finalize(const double *__restrict__ part, int64_t nblk,
+                                                        double *__restrict__ out) {
+  __shared__ double se[1024], sp[1024];
+  double a = 0.0, b = 1.0;
+  for (int64_t t = threadIdx.x; t < nblk; t += blockDim.x) {
+    a += part[2 * t];
+    b = b > part[2 * t + 1] ? part[2 * t + 1] : b;
+  }
+  se[threadIdx.x] = a;
+  sp[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      se[threadIdx.x] += se[threadIdx.x + s];
+      sp[threadIdx.x] = sp[threadIdx.x] > sp[threadIdx.x + s] ? sp[threadIdx.x + s] : sp[threadIdx.x];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = se[0];
+    out[1] = sp[0];
+  }
+}
+
+int64_t errest_blocks(int64_t n) { return (n + kErrBlock - 1) / kErrBlock; }
+
+cudaError_t launch_errest(int eq, const double *u, const double *uhat, int64_t n, double atol,
+                          double rtol, double *part, double *out, cudaStream_t s) {
+  const int64_t nblk = errest_blocks(n);
+  if (nblk <= 0) return cudaErrorInvalidValue;
+  if (eq == EQ_GLM) errest_kernel<EQ_GLM><<<(unsigned)nblk, kErrBlock, 0, s>>>(u, uhat, n, atol, rtol, part);
+  else errest_kernel<EQ_HYDRO><<<(unsigned)nblk, kErrBlock, 0, s>>>(u, uhat, n, atol, rtol, part);
+  errest_finalize<<<1, 1024, 0, s>>>(part, nblk, out);
+  return cudaGetLastError();
+}
+
+} // namespace kfvm

@@ -55,6 +55,12 @@ cudaError_t launch_copy(int dim, int eq, double *dst, const double *src, const G
 cudaError_t launch_ic(int dim, int eq, int ic_kind, uint64_t seed, const kfvm_config &cfg,
                       double *U, const Grid &g, cudaStream_t s);
 
+// error estimate of a state pair: block partials into part (2 per block of 256
+// cells), fixed-order sum into out[0] (err) and out[1] (positivity minimum)
+int64_t errest_blocks(int64_t n);
+cudaError_t launch_errest(int eq, const double *u, const double *uhat, int64_t n, double atol,
+                          double rtol, double *part, double *out, cudaStream_t s);
+
 int build_stencil(const kfvm_config *cfg, kfvm_stencil *st);
 
 } // namespace kfvm

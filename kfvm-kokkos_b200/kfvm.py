@@ -44,6 +44,7 @@ def lib():
         L.kfvm_get_state.argtypes = [P, P]
         L.kfvm_eval_rhs.argtypes = [P, D, P, P]
         L.kfvm_take_step.argtypes = [P, C.POINTER(abi.KfvmStepInfo)]
+        L.kfvm_err_est.argtypes = [P, P, P, P, P]
         L.kfvm_solve.argtypes = [P, I32, C.POINTER(I64), C.POINTER(abi.KfvmStepInfo)]
         L.kfvm_get_time.argtypes = [P, P, P]
         L.kfvm_set_time.argtypes = [P, D, D]
@@ -109,6 +110,13 @@ class Solver:
         mv = C.c_double()
         _check(lib().kfvm_eval_rhs(self.h, float(t), r.ctypes.data, C.addressof(mv)), "kfvm_eval_rhs")
         return r, mv.value
+
+    def err_est(self, u_dev_ptr, uhat_dev_ptr):
+        """Error estimate of two device arrays (SoA interior): (err, posmin)."""
+        e, p = C.c_double(), C.c_double()
+        _check(lib().kfvm_err_est(self.h, C.c_void_p(u_dev_ptr), C.c_void_p(uhat_dev_ptr),
+                                  C.addressof(e), C.addressof(p)), "kfvm_err_est")
+        return e.value, p.value
 
     def take_step(self):
         info = abi.KfvmStepInfo()

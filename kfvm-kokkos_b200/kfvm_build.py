@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libkfvm_b200.so")
 
-CU_SOURCES = ["kernels.cu", "ic.cu", "capi.cu"]
+CU_SOURCES = ["kernels.cu", "ic.cu", "errest.cu", "capi.cu"]
 CXX_SOURCES = ["stencil_weights.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
