@@ -178,6 +178,28 @@ int kfvm_eval_rhs(kfvm_solver *s, double t, double *rhs_host, double *max_vel);
 int kfvm_err_est(kfvm_solver *s, const double *u_dev, const double *uhat_dev, double *err,
                  double *posmin);
 
+/* Capacity of kfvm_err_est_noalloc's fixed scratch array (cells). */
+#define KFVM_NOALLOC_MAX_CELLS (1 << 24)
+
+/* The error estimate of kfvm_err_est without any allocation and without a
+ * solver handle.  No counterpart in the reference: it serves callers that cannot
+ * call cudaMalloc -- code whose device memory is owned by another allocator (a
+ * host framework's memory pool with a fixed budget) or that runs in a setting
+ * where device allocation after start-up is not permitted.  The caller passes the
+ * inputs (u_dev, uhat_dev: n cells x NV variables, SoA, on the device) and the
+ * output (out_dev: 2 doubles on the device, receiving err and posmin as in
+ * kfvm_err_est); stream is a cudaStream_t (NULL for the legacy default stream).
+ * Its scratch is a 1 MiB file-scope device array that every GPU loading the
+ * library holds until exit; n above KFVM_NOALLOC_MAX_CELLS is rejected with
+ * KFVM_ERR_ARG.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls
+ * on one GPU share that GPU's copy of the array: calls that overlap on the same
+ * GPU (for example on two streams) race and must be serialised by the caller.
+ * Each call overwrites the scratch it reads, so no clearing is needed between
+ * calls. */
+int kfvm_err_est_noalloc(int32_t eq, const double *u_dev, const double *uhat_dev, int64_t n,
+                         double atol, double rtol, double *out_dev, void *stream);
+
 /* One adaptive FSAL time step.  Replaces Solver::TakeStep (src/Solver.cpp:188-343). */
 int kfvm_take_step(kfvm_solver *s, kfvm_step_info *info);
 

@@ -461,6 +461,8 @@ int upload_state(kfvm_solver *s, int b, const double *u) {
 
 } // namespace
 
+int kfvm::set_last_error(int code, const std::string &msg) { return fail(code, msg); }
+
 extern "C" {
 
 const char *kfvm_last_error(void) { return g_err.c_str(); }

@@ -7,7 +7,10 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
+#include <string>
 
+#include "../../include/kfvm_b200.h"
 #include "kernels.cuh"
 #include "launch.h"
 
@@ -95,4 +98,61 @@ cudaError_t launch_errest(int eq, const double *u, const double *uhat, int64_t n
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Scratch of kfvm_err_est_noalloc: one (sum, min) pair per block of kErrBlock
+// cells, for up to KFVM_NOALLOC_MAX_CELLS cells (1 MiB).  It is a file-scope
+// device array, so every GPU that loads the library holds it until exit, and all
+// calls share it.  Every block overwrites its own pair before the finalize kernel
+// reads it, so nothing has to be cleared between calls.
+static __device__ __align__(256) double g_noalloc_part[2 * (KFVM_NOALLOC_MAX_CELLS / kErrBlock)];
+
+namespace {
+std::mutex g_noalloc_mu;
+constexpr int kMaxDevices = 64;
+double *g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_part on the current device.  In host code the
+// symbol names a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, taken once per device with that device current.
+cudaError_t noalloc_scratch(double **ptr) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_part);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = static_cast<double *>(p);
+  }
+  *ptr = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+} // namespace
+
 } // namespace kfvm
+
+extern "C" int kfvm_err_est_noalloc(int32_t eq, const double *u_dev, const double *uhat_dev,
+                                    int64_t n, double atol, double rtol, double *out_dev,
+                                    void *stream) {
+  if (!u_dev || !uhat_dev || !out_dev)
+    return kfvm::set_last_error(KFVM_ERR_ARG, "kfvm_err_est_noalloc: null pointer");
+  if (eq < KFVM_EQ_HYDRO || eq > KFVM_EQ_MHD_GLM)
+    return kfvm::set_last_error(KFVM_ERR_ARG, "kfvm_err_est_noalloc: unknown equation type");
+  if (n <= 0 || n > KFVM_NOALLOC_MAX_CELLS)
+    return kfvm::set_last_error(KFVM_ERR_ARG,
+                                "kfvm_err_est_noalloc: n must be in [1, " +
+                                    std::to_string((long long)KFVM_NOALLOC_MAX_CELLS) +
+                                    "], the capacity of its fixed scratch array");
+  double *part = nullptr;
+  cudaError_t e = kfvm::noalloc_scratch(&part);
+  if (e != cudaSuccess)
+    return kfvm::set_last_error(KFVM_ERR_CUDA, std::string("kfvm_err_est_noalloc: cudaGetSymbolAddress: ") +
+                                                   cudaGetErrorString(e));
+  e = kfvm::launch_errest(eq, u_dev, uhat_dev, n, atol, rtol, part, out_dev,
+                          static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess)
+    return kfvm::set_last_error(KFVM_ERR_CUDA, std::string("kfvm_err_est_noalloc: ") + cudaGetErrorString(e));
+  return KFVM_OK;
+}

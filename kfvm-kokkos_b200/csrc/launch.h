@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 
 #include "kernels.cuh"
 
@@ -62,5 +63,8 @@ cudaError_t launch_errest(int eq, const double *u, const double *uhat, int64_t n
                           double rtol, double *part, double *out, cudaStream_t s);
 
 int build_stencil(const kfvm_config *cfg, kfvm_stencil *st);
+
+// records msg as the calling thread's kfvm_last_error() and returns code
+int set_last_error(int code, const std::string &msg);
 
 } // namespace kfvm

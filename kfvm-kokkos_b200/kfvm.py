@@ -45,6 +45,7 @@ def lib():
         L.kfvm_eval_rhs.argtypes = [P, D, P, P]
         L.kfvm_take_step.argtypes = [P, C.POINTER(abi.KfvmStepInfo)]
         L.kfvm_err_est.argtypes = [P, P, P, P, P]
+        L.kfvm_err_est_noalloc.argtypes = [I32, P, P, I64, D, D, P, P]
         L.kfvm_solve.argtypes = [P, I32, C.POINTER(I64), C.POINTER(abi.KfvmStepInfo)]
         L.kfvm_get_time.argtypes = [P, P, P]
         L.kfvm_set_time.argtypes = [P, D, D]
@@ -65,6 +66,13 @@ def _check(rc, what):
     if rc != 0:
         msg = lib().kfvm_last_error().decode(errors="replace")
         raise KfvmError(f"{what} failed ({rc}): {msg}")
+
+
+def err_est_noalloc(eq, u_dev_ptr, uhat_dev_ptr, n, atol, rtol, out_dev_ptr, stream=0):
+    """kfvm_err_est_noalloc: error estimate into out_dev (2 doubles) without allocating."""
+    _check(lib().kfvm_err_est_noalloc(int(eq), C.c_void_p(u_dev_ptr), C.c_void_p(uhat_dev_ptr),
+                                      int(n), float(atol), float(rtol), C.c_void_p(out_dev_ptr),
+                                      C.c_void_p(stream)), "kfvm_err_est_noalloc")
 
 
 def stencil(cfg):
