@@ -240,9 +240,9 @@ int kfvm_last_stage_ms(kfvm_solver *s, double *ms);
  *   (ms) and launch counts for the classes listed by KFVM_KCLASS_*.
  * kfvm_get_launch_count: kernels launched by this solver since creation. */
 enum kfvm_kernel_class {
-  KFVM_KCLASS_BC = 0, KFVM_KCLASS_SELECT = 1, KFVM_KCLASS_FLAG = 2, KFVM_KCLASS_RECON = 3,
-  KFVM_KCLASS_HEAVY = 4, KFVM_KCLASS_RIEMANN = 5, KFVM_KCLASS_STAGE = 6, KFVM_KCLASS_OTHER = 7,
-  KFVM_NUM_KCLASS = 8
+  KFVM_KCLASS_BC = 0, KFVM_KCLASS_SELECT = 1 /* WENO decision + heavy-list compaction */,
+  KFVM_KCLASS_FLAG = 2, KFVM_KCLASS_RECON = 3, KFVM_KCLASS_HEAVY = 4, KFVM_KCLASS_RIEMANN = 5,
+  KFVM_KCLASS_STAGE = 6, KFVM_KCLASS_OTHER = 7, KFVM_NUM_KCLASS = 8
 };
 int kfvm_get_stream(kfvm_solver *s, void **stream);
 int kfvm_set_timing(kfvm_solver *s, int32_t on);

@@ -112,16 +112,6 @@ bool rk_table(int rk, RKTable &r) {
   return true;
 }
 
-// The linear weights live in the constant bank, one set per (device, dimension).
-// They depend only on lfac, so solvers that share a device and dimension must
-// share lfac; the registry counts the live solvers of each slot.
-struct WeightSlot {
-  double lfac = 0.0;
-  int users = 0;
-};
-std::mutex g_slot_mu;
-std::map<std::pair<int, int>, WeightSlot> g_slots;
-
 } // namespace
 
 struct kfvm_solver {
@@ -139,6 +129,9 @@ struct kfvm_solver {
   double *src = nullptr, *theta = nullptr, *part = nullptr;
   uint8_t *flag = nullptr, *wset = nullptr, *applied = nullptr;
   uint32_t *heavy = nullptr; // compacted WENO / limiter cell list (one slot per cell)
+  double *W[3] = {nullptr, nullptr, nullptr}; // KXRCF indicator per own face slot and point
+  uint8_t *status = nullptr;                  // 1: all linear states inside the limiter bounds
+  double2 *lamvel = nullptr;                  // GLM speed maxima of each cell's linear states
   int heavyBlocks = 0;
   kfvm::DevScalars *sc = nullptr;
   kfvm::DevScalars *hsc = nullptr; // pinned host copy
@@ -150,7 +143,6 @@ struct kfvm_solver {
   int nTS = 1;
   double dmin = 0.0;
   float lastMs = 0.0f;
-  int device = -1; // device holding this solver's constant-bank weights slot
   // measurement: kernel launches, optional per-class event timing
   int64_t launches = 0;
   bool timing = false;
@@ -228,24 +220,30 @@ int eval_front(kfvm_solver *s, int b) {
     mode = RECON_LINEAR;
   } else if (s->useSparseWeno) {
     mode = RECON_SPARSE;
-    const double thr = s->cfg.weno_thresh * std::pow(s->dmin, 1.5);
-    if ((e = run(s, KFVM_KCLASS_SELECT, 1, [&] { return launch_select(dim, eq, s->Ub[b], s->g, s->F, st); })) !=
-        cudaSuccess)
-      return set_err_cuda(e, "select");
-    if ((e = run(s, KFVM_KCLASS_FLAG, 1, [&] {
-           return launch_flag(dim, eq, s->Ub[b], s->g, s->F, s->theta, s->flag, s->sc, thr, st);
-         })) != cudaSuccess)
-      return set_err_cuda(e, "flag");
   } else {
     mode = RECON_FULL;
     // after a full-WENO evaluation the sparse mode is allowed again (Solver.cpp:439-443)
     s->useSparseWeno = s->cfg.weno_thresh > 0.0 && s->indicator == KFVM_IND_KXRCF;
   }
-  if ((e = run(s, KFVM_KCLASS_RECON, 1, [&] {
-         return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, mode, s->flag, s->wset, s->applied, s->theta,
-                             s->F, s->src, s->heavy, s->sc, s->heavyBlocks, st);
+  if (mode != RECON_FULL) {
+    if ((e = run(s, KFVM_KCLASS_RECON, 1, [&] {
+           return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, mode == RECON_SPARSE, s->F, s->W, s->src,
+                               s->status, s->lamvel, st);
+         })) != cudaSuccess)
+      return set_err_cuda(e, "recon");
+  }
+  if (mode == RECON_SPARSE) {
+    const double thr = s->cfg.weno_thresh * std::pow(s->dmin, 1.5);
+    if ((e = run(s, KFVM_KCLASS_FLAG, 1, [&] {
+           return launch_flag(dim, eq, s->Ub[b], s->g, s->W, s->theta, s->flag, s->sc, thr, st);
+         })) != cudaSuccess)
+      return set_err_cuda(e, "flag");
+  }
+  if ((e = run(s, KFVM_KCLASS_SELECT, 1, [&] {
+         return launch_compact(dim, eq, s->g, mode, s->flag, s->wset, s->status, s->applied, s->theta, s->heavy,
+                               s->lamvel, s->sc, st);
        })) != cudaSuccess)
-    return set_err_cuda(e, "recon");
+    return set_err_cuda(e, "compact");
   if ((e = run(s, KFVM_KCLASS_HEAVY, 1, [&] {
          return launch_heavy(dim, eq, s->Ub[b], s->g, s->dS, s->theta, s->F, s->src, s->heavy, s->sc,
                              s->heavyBlocks, st);
@@ -562,6 +560,18 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   for (int c = 0; c < hS.w.n_cells; c++)
     hS.loff[c] = (hS.w.off[2][c] * g.py + hS.w.off[1][c]) * g.px + hS.w.off[0][c];
   for (int c = 0; c < hS.w.n_cells; c++) g.loff[c] = hS.loff[c];
+  {
+    // full-stencil linear weights as [cell][row]: face rows f*NQF+q, then interior rows
+    const int C = hS.w.n_cells, nqf = hS.w.nqf, nf = 2 * cfg->dim;
+    const int nrows = nf * nqf + (cfg->eq == KFVM_EQ_MHD_GLM ? hS.w.nqc : 0);
+    for (int c = 0; c < C; c++) {
+      int r = 0;
+      for (int f = 0; f < nf; f++)
+        for (int q = 0; q < nqf; q++) hS.lin[c * nrows + r++] = hS.w.face_w[0][f][q][c];
+      if (cfg->eq == KFVM_EQ_MHD_GLM)
+        for (int q = 0; q < hS.w.nqc; q++) hS.lin[c * nrows + r++] = hS.w.cell_w[0][q][c];
+    }
+  }
 
   auto cleanup = [&](cudaError_t e, const char *what) {
     kfvm_destroy(s);
@@ -586,6 +596,8 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
       return cleanup(e, "alloc faces");
     if ((e = dalloc((void **)&s->G[d], nv * g.nface[d] * sizeof(double))) != cudaSuccess)
       return cleanup(e, "alloc fluxes");
+    if ((e = dalloc((void **)&s->W[d], 2 * nqf * g.nface[d] * sizeof(double))) != cudaSuccess)
+      return cleanup(e, "alloc indicator");
   }
   if (cfg->eq == KFVM_EQ_MHD_GLM &&
       (e = dalloc((void **)&s->src, (size_t)nqc * nv * n * sizeof(double))) != cudaSuccess)
@@ -595,6 +607,9 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if ((e = dalloc((void **)&s->wset, n)) != cudaSuccess) return cleanup(e, "alloc");
   if ((e = dalloc((void **)&s->applied, n)) != cudaSuccess) return cleanup(e, "alloc");
   if ((e = dalloc((void **)&s->heavy, n * sizeof(uint32_t))) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->status, n)) != cudaSuccess) return cleanup(e, "alloc");
+  if (cfg->eq == KFVM_EQ_MHD_GLM && (e = dalloc((void **)&s->lamvel, n * sizeof(double2))) != cudaSuccess)
+    return cleanup(e, "alloc");
   {
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
@@ -613,22 +628,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if ((e = cudaMemcpyAsync(s->dS, &hS, sizeof(DevStencil), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess)
     return cleanup(e, "upload stencil");
   if ((e = cudaMemsetAsync(s->sc, 0, sizeof(DevScalars), s->stream)) != cudaSuccess) return cleanup(e, "memset");
-  {
-    int dev = 0;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cleanup(e, "device");
-    std::lock_guard<std::mutex> lk(g_slot_mu);
-    WeightSlot &ws = g_slots[{dev, cfg->dim}];
-    if (ws.users > 0 && ws.lfac != cfg->lfac) {
-      kfvm_destroy(s);
-      return fail(KFVM_ERR_ARG, "a live solver of this dimension on this device uses another lfac");
-    }
-    if (ws.users == 0) {
-      if ((e = upload_linear_weights(cfg->dim, hS.w, s->stream)) != cudaSuccess) return cleanup(e, "weights");
-      ws.lfac = cfg->lfac;
-    }
-    ws.users++;
-    s->device = dev;
-  }
+
   if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return cleanup(e, "sync");
   *out = s;
   return KFVM_OK;
@@ -637,10 +637,6 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
 void kfvm_destroy(kfvm_solver *s) {
   if (!s) return;
   if (s->stream) cudaStreamSynchronize(s->stream);
-  if (s->device >= 0) {
-    std::lock_guard<std::mutex> lk(g_slot_mu);
-    g_slots[{s->device, s->dim}].users--;
-  }
   cudaFree(s->dS);
   for (int b = 0; b < 3; b++) cudaFree(s->Ub[b]);
   cudaFree(s->Uhat);
@@ -649,7 +645,10 @@ void kfvm_destroy(kfvm_solver *s) {
   for (int d = 0; d < 3; d++) {
     cudaFree(s->F[d]);
     cudaFree(s->G[d]);
+    cudaFree(s->W[d]);
   }
+  cudaFree(s->status);
+  cudaFree(s->lamvel);
   cudaFree(s->src);
   cudaFree(s->theta);
   cudaFree(s->flag);

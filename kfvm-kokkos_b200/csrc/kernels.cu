@@ -59,57 +59,48 @@ __global__ void __launch_bounds__(256) bc_fill_kernel(double *__restrict__ U, Gr
 }
 
 // ---------------------------------------------------------------------------
-// Linear-reconstruction weights of the full stencil in the constant bank: face
-// points [f][q][c] followed by interior points [q][c].  They depend only on the
-// dimension and lfac (not on the grid), so one set per (device, dimension) serves
-// every solver with that lfac.  Loop indices are compile-time, so every weight is
-// an immediate constant-bank operand of its FMA.
-constexpr int kW2Face = 4 * 2 * 13, kW2Cell = 4 * 13;
-constexpr int kW3Face = 6 * 4 * 33, kW3Cell = 8 * 33;
-__constant__ double c_w2[kW2Face + kW2Cell];
-__constant__ double c_w3[kW3Face + kW3Cell];
+// Linear-reconstruction weights of the full stencil, staged per block in shared
+// memory as [cell][row] (rows: face points f*NQF+q, then interior points), so the
+// weights of consecutive rows for one stencil cell are contiguous broadcast loads.
+// The loop over stencil cells stays rolled: fully unrolled, 3960 FMAs per cell
+// overflow the instruction cache.
+template <int DIM, int EQ>
+struct LinRows {
+  static constexpr int NROWS = Cfg<DIM, EQ>::NF * Cfg<DIM, EQ>::NQF + (Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 0);
+  static constexpr int SIZE = Cfg<DIM, EQ>::C * NROWS;
+};
 
-template <int DIM>
-__device__ __forceinline__ double cw(int idx) {
-  if constexpr (DIM == 2) return c_w2[idx];
-  else return c_w3[idx];
+template <int DIM, int EQ>
+__device__ __forceinline__ void stage_lin_weights(const DevStencil *__restrict__ S, double *__restrict__ sW) {
+  using L = LinRows<DIM, EQ>;
+  for (int t = threadIdx.y * blockDim.x + threadIdx.x; t < L::SIZE; t += blockDim.x * blockDim.y)
+    sW[t] = S->lin[t];
 }
 
-cudaError_t upload_linear_weights(int dim, const kfvm_stencil &st, cudaStream_t s) {
-  const int C = st.n_cells, NQF = st.nqf, NQC = st.nqc, NF = 2 * dim;
-  double w[kW3Face + kW3Cell];
-  int n = 0;
-  for (int f = 0; f < NF; f++)
-    for (int q = 0; q < NQF; q++)
-      for (int c = 0; c < C; c++) w[n++] = st.face_w[0][f][q][c];
-  for (int q = 0; q < NQC; q++)
-    for (int c = 0; c < C; c++) w[n++] = st.cell_w[0][q][c];
-  if (dim == 2) return cudaMemcpyToSymbolAsync(c_w2, w, n * sizeof(double), 0, cudaMemcpyHostToDevice, s);
-  return cudaMemcpyToSymbolAsync(c_w3, w, n * sizeof(double), 0, cudaMemcpyHostToDevice, s);
-}
-
-// st[p][v] = sum_c W0[R0 + p][c] U[c][v] for NP consecutive weight rows starting at
-// R0 (face points are rows f*NQF + q, interior points rows NF*NQF + q)
+// st[p][v] = sum_c W0[R0 + p][c] U[c][v] for NP consecutive weight rows from R0;
+// per output the sum over stencil cells keeps the reference's order
 template <int DIM, int EQ, int R0, int NP>
 __device__ __forceinline__ void lin_rows(const double *__restrict__ Uc, const Grid &g,
+                                         const double *__restrict__ sW,
                                          double (&st)[NP][Cfg<DIM, EQ>::NV]) {
   using T = Cfg<DIM, EQ>;
+  constexpr int NR = LinRows<DIM, EQ>::NROWS;
 #pragma unroll
   for (int p = 0; p < NP; p++)
 #pragma unroll
     for (int v = 0; v < T::NV; v++) st[p][v] = 0.0;
-  // stencil cell outermost: each weight is brought into a register once and
-  // feeds all NV variables; per output the sum over cells keeps the reference's order
-#pragma unroll
+#pragma unroll 1
   for (int c = 0; c < T::C; c++) {
+    const int64_t o = g.loff[c];
     double u[T::NV];
 #pragma unroll
-    for (int v = 0; v < T::NV; v++) u[v] = __ldg(Uc + v * g.pvol + g.loff[c]);
+    for (int v = 0; v < T::NV; v++) u[v] = __ldg(Uc + v * g.pvol + o);
+    const double *w = sW + c * NR + R0;
 #pragma unroll
     for (int p = 0; p < NP; p++) {
-      const double w = cw<DIM>((R0 + p) * T::C + c);
+      const double wp = w[p];
 #pragma unroll
-      for (int v = 0; v < T::NV; v++) st[p][v] += w * u[v];
+      for (int v = 0; v < T::NV; v++) st[p][v] += wp * u[v];
     }
   }
 }
@@ -122,6 +113,21 @@ struct Groups {
   static constexpr int NG = (2 * DIM * (DIM == 2 ? 2 : 4)) / NPF;
 };
 
+
+// ---------------------------------------------------------------------------
+// Stage front end, four kernels:
+//   recon    linear face states of every cell (constant-bank weights) written to
+//            the face arrays, the KXRCF indicator p/rho^gamma at each own face point
+//            written to W, and whether every state lies strictly inside the
+//            positivity limiter's bounds (then theta = 1 exactly as in the reference)
+//   flag     KXRCF flags from W (WenoSelect_K)
+//   compact  the reference's flag-set semantics, theta = 1 for in-bounds linear
+//            cells, and the compacted heavy list (WENO cells, cells to limit)
+//   heavy    WENO-AO and/or the full limiter on the listed cells
+// theta of the previous evaluation feeds the flags, so it is rewritten only after
+// flag_kernel has read it.
+constexpr uint32_t kHeavyWeno = 0x80000000u;
+
 // face-slot address of point q, variable v of face f of cell (i,j,k) in a
 // [slot][q][v][face] array with nvv variables
 __device__ __forceinline__ int64_t face_slot_addr(const Grid &g, int f, int64_t i, int64_t j, int64_t k,
@@ -133,109 +139,18 @@ __device__ __forceinline__ int64_t face_slot_addr(const Grid &g, int f, int64_t 
   return ((int64_t)(slot * nqf + q) * nvv + v) * g.nface[d] + fidx;
 }
 
-// ---------------------------------------------------------------------------
-// KXRCF, part 1: linear face states of each cell -> indicator p/rho^gamma at its
-// own face slots (KernelLinearRecon_K + EOS::weno).  W[d] is [slot][q][face].
-template <int DIM, int EQ, int G>
-__device__ __forceinline__ void select_group(const double *__restrict__ Uc, const Grid &g,
-                                             int64_t i, int64_t j, int64_t k, double *const *W) {
-  using T = Cfg<DIM, EQ>;
-  constexpr int NP = Groups<DIM, EQ>::NPF;
-  if constexpr (G + 1 < Groups<DIM, EQ>::NG) select_group<DIM, EQ, G + 1>(Uc, g, i, j, k, W);
-  double st[NP][T::NV];
-  lin_rows<DIM, EQ, G * NP, NP>(Uc, g, st);
-#pragma unroll
-  for (int p = 0; p < NP; p++) {
-    const int f = (G * NP + p) / T::NQF, q = (G * NP + p) % T::NQF;
-    W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno(g.gamma, st[p]);
-  }
-}
-
-template <int DIM, int EQ>
-__global__ void __launch_bounds__(128)
-    select_kernel(const double *__restrict__ U, Grid g, double *W0, double *W1, double *W2) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
-  const int64_t k = blockIdx.z;
-  if (i >= g.nx || j >= g.ny) return;
-  const double *Uc = U + pidx(g, i, j, k);
-  double *W[3] = {W0, W1, W2};
-  select_group<DIM, EQ, 0>(Uc, g, i, j, k, W);
-}
-
-// KXRCF, part 2 (WenoSelect_K, Numeric_K.H:292-398): largest indicator jump across
-// the cell's faces over the cell value; the outer slot of a boundary face follows
-// setFaceBCs (periodic partner face, or the inner slot at an outflow boundary).
-template <int DIM, int EQ>
-__global__ void __launch_bounds__(128)
-    flag_kernel(const double *__restrict__ U, Grid g, const double *__restrict__ W0,
-                const double *__restrict__ W1, const double *__restrict__ W2,
-                const double *__restrict__ theta, uint8_t *__restrict__ flag,
-                DevScalars *__restrict__ sc, double wThresh) {
-  using T = Cfg<DIM, EQ>;
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
-  const int64_t k = blockIdx.z;
-  bool f = false;
-  if (i < g.nx && j < g.ny) {
-    const int64_t c = (k * g.ny + j) * g.nx + i;
-    f = theta[c] < 1.0;
-    if (!f) {
-      const double *W[3] = {W0, W1, W2};
-      double maxJump = 0.0;
-#pragma unroll
-      for (int fc = 0; fc < T::NF; fc++) {
-        const int d = fc >> 1, hi = fc & 1;
-        const int64_t fx = g.fdim[d][0], fy = g.fdim[d][1], nf = g.nface[d];
-        const int64_t fi = i + (d == 0 && hi), fj = j + (d == 1 && hi), fk = k + (d == 2 && hi);
-        int64_t fidx = (fk * fy + fj) * fx + fi, oidx = fidx;
-        const int own = hi ? 0 : 1;
-        int oth = 1 - own;
-        const int64_t m = d == 0 ? fi : (d == 1 ? fj : fk);
-        const int64_t nd = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
-        const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
-        if (m == 0 || m == nd) {
-          if (g.bc[fc] == KFVM_BC_PERIODIC) oidx = m == 0 ? fidx + nd * stride : fidx - nd * stride;
-          else oth = own;
-        }
-#pragma unroll
-        for (int q = 0; q < T::NQF; q++) {
-          const double wIn = W[d][(int64_t)(own * T::NQF + q) * nf + fidx];
-          const double wOut = W[d][(int64_t)(oth * T::NQF + q) * nf + oidx];
-          maxJump = fmax(maxJump, fabs(wOut - wIn));
-        }
-      }
-      double uAv[T::NV];
-      const double *Uc = U + pidx(g, i, j, k);
-#pragma unroll
-      for (int v = 0; v < T::NV; v++) uAv[v] = Uc[v * g.pvol];
-      const double w = maxJump / Eos<EQ>::weno(g.gamma, uAv);
-      f = w >= wThresh;
-    }
-    flag[c] = f ? 1 : 0;
-  }
-  const unsigned ball = __ballot_sync(0xffffffffu, f);
-  if ((threadIdx.x & 31) == 0 && ball) atomicAdd(&sc->nflag, (unsigned)__popc(ball));
-}
-
-// ---------------------------------------------------------------------------
-// final face states, light pass: linear reconstruction with constant-bank weights
-// for every cell that is not sent to WENO.  The positivity limiter's bounds are
-// computed first; a cell whose states all lie strictly inside them keeps theta = 1
-// exactly as in the reference.  WENO cells and cells that need the limiter are
-// appended to the heavy list (bit 31 marks WENO) for heavy_kernel.
-constexpr uint32_t kHeavyWeno = 0x80000000u;
-
 template <int DIM, int EQ, int G>
 __device__ __forceinline__ bool recon_group(const double *__restrict__ Uc, const Grid &g,
-                                            const PosBounds &bd, int64_t i, int64_t j, int64_t k,
-                                            double *const *F, double &lam, double &vel) {
+                                            const double *__restrict__ sW, const PosBounds &bd,
+                                            int64_t i, int64_t j, int64_t k, double *const *F,
+                                            double *const *W, bool wantInd, double &lam, double &vel) {
   using T = Cfg<DIM, EQ>;
   constexpr int NP = Groups<DIM, EQ>::NPF;
   bool ok = true;
-  if constexpr (G + 1 < Groups<DIM, EQ>::NG) ok = recon_group<DIM, EQ, G + 1>(Uc, g, bd, i, j, k, F, lam, vel);
+  if constexpr (G + 1 < Groups<DIM, EQ>::NG)
+    ok = recon_group<DIM, EQ, G + 1>(Uc, g, sW, bd, i, j, k, F, W, wantInd, lam, vel);
   double st[NP][T::NV];
-  lin_rows<DIM, EQ, G * NP, NP>(Uc, g, st);
+  lin_rows<DIM, EQ, G * NP, NP>(Uc, g, sW, st);
 #pragma unroll
   for (int p = 0; p < NP; p++) {
     const int f = (G * NP + p) / T::NQF, q = (G * NP + p) % T::NQF;
@@ -244,6 +159,7 @@ __device__ __forceinline__ bool recon_group(const double *__restrict__ Uc, const
     const int64_t nf = g.nface[f >> 1];
 #pragma unroll
     for (int v = 0; v < T::NV; v++) F[f >> 1][a + v * nf] = st[p][v];
+    if (wantInd) W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno(g.gamma, st[p]);
     if constexpr (T::SRC) {
       // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
       const double vv = fabs(st[p][MOMX] / st[p][DENS]);
@@ -324,29 +240,114 @@ __device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<
 
 template <int DIM, int EQ>
 __global__ void __launch_bounds__(128)
-    recon_kernel(const double *__restrict__ U, Grid g, int mode, const uint8_t *__restrict__ flag,
-                 uint8_t *__restrict__ wset, uint8_t *__restrict__ applied,
-                 double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
-                 double *__restrict__ F2, double *__restrict__ src, uint32_t *__restrict__ heavy,
-                 DevScalars *__restrict__ sc) {
+    recon_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
+                 double *__restrict__ F0,
+                 double *__restrict__ F1, double *__restrict__ F2, double *__restrict__ W0,
+                 double *__restrict__ W1, double *__restrict__ W2, double *__restrict__ src,
+                 uint8_t *__restrict__ status, double2 *__restrict__ lamvel) {
   using T = Cfg<DIM, EQ>;
   constexpr int NV = T::NV;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
   const int64_t k = blockIdx.z;
   __shared__ double tile[6][PosTile<DIM>::N];
+  __shared__ __align__(16) double sW[LinRows<DIM, EQ>::SIZE];
+  stage_lin_weights<DIM, EQ>(S, sW);
   pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)blockDim.x, blockIdx.y * (int64_t)blockDim.y, k, tile);
   __syncthreads();
+  if (i >= g.nx || j >= g.ny) return;
+  const int64_t c = (k * g.ny + j) * g.nx + i;
+  const double *Uc = U + pidx(g, i, j, k);
+  const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
+  double *F[3] = {F0, F1, F2};
+  double *W[3] = {W0, W1, W2};
+  double lam = 0.0, vel = 0.0;
+  bool ok = recon_group<DIM, EQ, 0>(Uc, g, sW, bd, i, j, k, F, W, wantInd != 0, lam, vel);
+  if constexpr (T::SRC) {
+    double cs[T::NQC][NV];
+    lin_rows<DIM, EQ, T::NF * T::NQF, T::NQC>(Uc, g, sW, cs);
+#pragma unroll
+    for (int q = 0; q < T::NQC; q++) {
+      ok = ok && pos_inside<EQ>(bd, cs[q]);
+#pragma unroll
+      for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = cs[q][v];
+    }
+    lamvel[c] = make_double2(lam, vel);
+  }
+  status[c] = ok ? 1 : 0;
+}
+
+// KXRCF flags (WenoSelect_K, Numeric_K.H:292-398): largest indicator jump across the
+// cell's faces over the cell value; the outer slot of a boundary face follows
+// setFaceBCs (periodic partner face, or the inner slot at an outflow boundary).
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(128)
+    flag_kernel(const double *__restrict__ U, Grid g, const double *__restrict__ W0,
+                const double *__restrict__ W1, const double *__restrict__ W2,
+                const double *__restrict__ theta, uint8_t *__restrict__ flag,
+                DevScalars *__restrict__ sc, double wThresh) {
+  using T = Cfg<DIM, EQ>;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  bool f = false;
+  if (i < g.nx && j < g.ny) {
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    f = theta[c] < 1.0;
+    if (!f) {
+      const double *W[3] = {W0, W1, W2};
+      double maxJump = 0.0;
+#pragma unroll
+      for (int fc = 0; fc < T::NF; fc++) {
+        const int d = fc >> 1, hi = fc & 1;
+        const int64_t fx = g.fdim[d][0], fy = g.fdim[d][1], nf = g.nface[d];
+        const int64_t fi = i + (d == 0 && hi), fj = j + (d == 1 && hi), fk = k + (d == 2 && hi);
+        int64_t fidx = (fk * fy + fj) * fx + fi, oidx = fidx;
+        const int own = hi ? 0 : 1;
+        int oth = 1 - own;
+        const int64_t m = d == 0 ? fi : (d == 1 ? fj : fk);
+        const int64_t nd = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+        const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
+        if (m == 0 || m == nd) {
+          if (g.bc[fc] == KFVM_BC_PERIODIC) oidx = m == 0 ? fidx + nd * stride : fidx - nd * stride;
+          else oth = own;
+        }
+#pragma unroll
+        for (int q = 0; q < T::NQF; q++) {
+          const double wIn = W[d][(int64_t)(own * T::NQF + q) * nf + fidx];
+          const double wOut = W[d][(int64_t)(oth * T::NQF + q) * nf + oidx];
+          maxJump = fmax(maxJump, fabs(wOut - wIn));
+        }
+      }
+      double uAv[T::NV];
+      const double *Uc = U + pidx(g, i, j, k);
+#pragma unroll
+      for (int v = 0; v < T::NV; v++) uAv[v] = Uc[v * g.pvol];
+      const double w = maxJump / Eos<EQ>::weno(g.gamma, uAv);
+      f = w >= wThresh;
+    }
+    flag[c] = f ? 1 : 0;
+  }
+  const unsigned ball = __ballot_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0 && ball) atomicAdd(&sc->nflag, (unsigned)__popc(ball));
+}
+
+// WENO decision with the flag-map semantics of WenoSelector::update
+// (Solver.cpp:687-742: the key set is replaced only when some cell was flagged),
+// theta = 1 for in-bounds linear cells, and the heavy list.
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(256)
+    compact_kernel(Grid g, int mode, const uint8_t *__restrict__ flag, uint8_t *__restrict__ wset,
+                   const uint8_t *__restrict__ status, uint8_t *__restrict__ applied,
+                   double *__restrict__ theta, uint32_t *__restrict__ heavy,
+                   const double2 *__restrict__ lamvel, DevScalars *__restrict__ sc) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool useWeno = false, push = false;
   double lam = 0.0, vel = 0.0;
-  int64_t c = 0;
-  if (i < g.nx && j < g.ny) {
-    c = (k * g.ny + j) * g.nx + i;
+  if (c < g.n) {
     if (mode == RECON_FULL) {
       useWeno = true;
     } else if (mode == RECON_SPARSE) {
-      // the flag set is replaced only when this evaluation flagged some cell
-      // (WenoSelector::update, Solver.cpp:687-742); otherwise the last set stays
       if (sc->nflag > 0) {
         useWeno = flag[c] != 0;
         wset[c] = useWeno ? 1 : 0;
@@ -355,28 +356,17 @@ __global__ void __launch_bounds__(128)
       }
     }
     applied[c] = useWeno ? 1 : 0;
-    if (useWeno) {
+    if (useWeno || !status[c]) {
       push = true;
     } else {
-      const double *Uc = U + pidx(g, i, j, k);
-      const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
-      double *F[3] = {F0, F1, F2};
-      bool ok = recon_group<DIM, EQ, 0>(Uc, g, bd, i, j, k, F, lam, vel);
-      if constexpr (T::SRC) {
-        double cs[T::NQC][NV];
-        lin_rows<DIM, EQ, T::NF * T::NQF, T::NQC>(Uc, g, cs);
-#pragma unroll
-        for (int q = 0; q < T::NQC; q++) {
-          ok = ok && pos_inside<EQ>(bd, cs[q]);
-#pragma unroll
-          for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = cs[q][v];
-        }
+      theta[c] = 1.0;
+      if constexpr (EQ == EQ_GLM) {
+        const double2 lv = lamvel[c];
+        lam = lv.x;
+        vel = lv.y;
       }
-      if (ok) theta[c] = 1.0;
-      else push = true;
     }
   }
-  // warp-aggregated append to the heavy list
   const unsigned lane = threadIdx.x & 31;
   const unsigned ball = __ballot_sync(0xffffffffu, push);
   const unsigned wball = __ballot_sync(0xffffffffu, useWeno);
@@ -385,7 +375,7 @@ __global__ void __launch_bounds__(128)
   base = __shfl_sync(0xffffffffu, base, 0);
   if (push) heavy[base + __popc(ball & ((1u << lane) - 1u))] = (uint32_t)c | (useWeno ? kHeavyWeno : 0u);
   if (lane == 0 && wball) atomicAdd(&sc->napplied, (unsigned)__popc(wball));
-  if constexpr (T::SRC) {
+  if constexpr (EQ == EQ_GLM) {
     lam = warp_max(lam);
     vel = warp_max(vel);
     if (lane == 0) {
@@ -941,8 +931,11 @@ struct Launch {
     bc_fill_kernel<DIM, NV><<<(unsigned)(blocks < 65535 * 16 ? blocks : 65535 * 16), 256, 0, s>>>(U, g);
     return cudaGetLastError();
   }
-  static cudaError_t select(const double *U, const Grid &g, double *const *W, cudaStream_t s) {
-    select_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, W[0], W[1], W[2]);
+  static cudaError_t recon(const double *U, const Grid &g, const DevStencil *S, int wantInd,
+                           double *const *F, double *const *W, double *src, uint8_t *status,
+                           double2 *lamvel, cudaStream_t s) {
+    recon_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
+        U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel);
     return cudaGetLastError();
   }
   static cudaError_t flag(const double *U, const Grid &g, double *const *W, const double *theta,
@@ -951,14 +944,11 @@ struct Launch {
                                                                           flag, sc, thr);
     return cudaGetLastError();
   }
-  static cudaError_t recon(const double *U, const Grid &g, const DevStencil *S, int mode,
-                           const uint8_t *flag, uint8_t *wset, uint8_t *applied, double *theta,
-                           double *const *F, double *src, uint32_t *heavy, DevScalars *sc,
-                           int heavy_blocks, cudaStream_t s) {
-    (void)S;
-    (void)heavy_blocks;
-    recon_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
-        U, g, mode, flag, wset, applied, theta, F[0], F[1], F[2], src, heavy, sc);
+  static cudaError_t compact(const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
+                             const uint8_t *status, uint8_t *applied, double *theta, uint32_t *heavy,
+                             const double2 *lamvel, DevScalars *sc, cudaStream_t s) {
+    compact_kernel<DIM, EQ><<<(unsigned)((g.n + 255) / 256), 256, 0, s>>>(g, mode, flag, wset, status, applied,
+                                                                           theta, heavy, lamvel, sc);
     return cudaGetLastError();
   }
   static cudaError_t heavy(const double *U, const Grid &g, const DevStencil *S, double *theta,
@@ -1023,25 +1013,25 @@ int64_t stage_blocks(const Grid &g) {
 cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s) {
   KFVM_DISPATCH(dim, eq, bc(U, g, s));
 }
-cudaError_t launch_select(int dim, int eq, const double *U, const Grid &g, double *const *W,
-                          cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, select(U, g, W, s));
+cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
+                         double *const *F, double *const *W, double *src, uint8_t *status, double2 *lamvel,
+                         cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, recon(U, g, S, wantInd, F, W, src, status, lamvel, s));
 }
 cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, double *const *W,
                         const double *theta, uint8_t *flag, DevScalars *sc, double thr,
                         cudaStream_t s) {
   KFVM_DISPATCH(dim, eq, flag(U, g, W, theta, flag, sc, thr, s));
 }
+cudaError_t launch_compact(int dim, int eq, const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
+                           const uint8_t *status, uint8_t *applied, double *theta, uint32_t *heavy,
+                           const double2 *lamvel, DevScalars *sc, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, compact(g, mode, flag, wset, status, applied, theta, heavy, lamvel, sc, s));
+}
 cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
                          double *theta, double *const *F, double *src, const uint32_t *heavy,
                          DevScalars *sc, int heavy_blocks, cudaStream_t s) {
   KFVM_DISPATCH(dim, eq, heavy(U, g, S, theta, F, src, heavy, sc, heavy_blocks, s));
-}
-cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
-                         int mode, const uint8_t *flag, uint8_t *wset, uint8_t *applied,
-                         double *theta, double *const *F, double *src, uint32_t *heavy,
-                         DevScalars *sc, int heavy_blocks, cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, recon(U, g, S, mode, flag, wset, applied, theta, F, src, heavy, sc, heavy_blocks, s));
 }
 cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
                            DevScalars *sc, cudaStream_t s) {

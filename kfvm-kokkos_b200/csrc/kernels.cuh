@@ -45,10 +45,14 @@ struct Grid {
   int64_t loff[KFVM_MAX_CELLS]; // stencil offsets in the padded array
 };
 
-// stencil on the device: weights plus linear offsets in the padded array
+// stencil on the device: weights plus linear offsets in the padded array, and the
+// full-stencil linear weights packed as [cell][row] (rows: face points f*NQF+q, then
+// interior points q) for the light reconstruction pass
+constexpr int kMaxLinRows = 6 * 4 + 8;
 struct DevStencil {
   kfvm_stencil w;
   int64_t loff[KFVM_MAX_CELLS];
+  double lin[KFVM_MAX_CELLS * kMaxLinRows];
 };
 
 // device-side scalars written by reductions

@@ -28,22 +28,19 @@ struct StageArgs {
 
 int64_t stage_blocks(const Grid &g);
 cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s);
-// KXRCF selection; W are per-direction [slot][q][face] scratch arrays (the
-// face-state buffers are reused: the indicator is consumed before they are written)
-cudaError_t launch_select(int dim, int eq, const double *U, const Grid &g, double *const *W,
-                          cudaStream_t s);
+// stage front end: linear states + KXRCF indicator + limiter bound status,
+// KXRCF flags, WENO decision / heavy-list compaction, heavy cells
+cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
+                         double *const *F, double *const *W, double *src, uint8_t *status, double2 *lamvel,
+                         cudaStream_t s);
 cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, double *const *W,
                         const double *theta, uint8_t *flag, DevScalars *sc, double thr,
                         cudaStream_t s);
+cudaError_t launch_compact(int dim, int eq, const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
+                           const uint8_t *status, uint8_t *applied, double *theta, uint32_t *heavy,
+                           const double2 *lamvel, DevScalars *sc, cudaStream_t s);
 cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
                          double *theta, double *const *F, double *src, const uint32_t *heavy,
-                         DevScalars *sc, int heavy_blocks, cudaStream_t s);
-cudaError_t upload_linear_weights(int dim, const kfvm_stencil &st, cudaStream_t s);
-// final face states: light linear pass over all cells, then the heavy pass over the
-// compacted list of WENO / limited cells (heavy holds up to one entry per cell)
-cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
-                         int mode, const uint8_t *flag, uint8_t *wset, uint8_t *applied,
-                         double *theta, double *const *F, double *src, uint32_t *heavy,
                          DevScalars *sc, int heavy_blocks, cudaStream_t s);
 cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
                            DevScalars *sc, cudaStream_t s);

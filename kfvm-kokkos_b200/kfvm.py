@@ -22,7 +22,7 @@ class KfvmError(RuntimeError):
 
 
 # kernel classes of kfvm_get_timing (enum kfvm_kernel_class)
-KCLASS = ["bc_fill", "select", "flag", "recon", "heavy", "riemann", "stage", "other"]
+KCLASS = ["bc_fill", "compact", "flag", "recon", "heavy", "riemann", "stage", "other"]
 
 
 def lib():
