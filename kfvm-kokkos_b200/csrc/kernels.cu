@@ -89,7 +89,7 @@ __device__ __forceinline__ void lin_rows(const double *__restrict__ Uc, const Gr
   for (int p = 0; p < NP; p++)
 #pragma unroll
     for (int v = 0; v < T::NV; v++) st[p][v] = 0.0;
-#pragma unroll 1
+#pragma unroll 3
   for (int c = 0; c < T::C; c++) {
     const int64_t o = g.loff[c];
     double u[T::NV];
@@ -453,21 +453,27 @@ __global__ void __launch_bounds__(128)
 }
 
 // ---------------------------------------------------------------------------
-// one thread per face of direction D: Riemann solve at every face point, the
-// quadrature-weighted flux sum per variable, and the max wave speed.
+// Riemann fluxes of direction D: one thread per face point (block = 32 faces x NQF
+// points, points along threadIdx.y), so each thread keeps only one solve live and
+// more warps hide the FP64 latency.  The quadrature-weighted sum over a face's
+// points goes through shared memory in point order, and the max wave speed
+// through a warp maximum and one atomic per warp.
 template <int DIM, int EQ, int D>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4))
     riemann_kernel(const double *__restrict__ F, double *__restrict__ G, Grid g,
                    DevScalars *__restrict__ sc) {
   using T = Cfg<DIM, EQ>;
   using E = Eos<EQ>;
-  constexpr int NV = T::NV;
+  constexpr int NV = T::NV, NQF = T::NQF;
+  __shared__ double part[NQF][NV][32];
   const int64_t fx = g.fdim[D][0], fy = g.fdim[D][1], nf = g.nface[D];
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
+  const int64_t i = blockIdx.x * (int64_t)32 + threadIdx.x;
+  const int64_t j = blockIdx.y;
   const int64_t k = blockIdx.z;
+  const int q = threadIdx.y;
   double vmax = 0.0;
-  if (i < fx && j < fy) {
+  const bool live = i < fx;
+  if (live) {
     const int64_t fidx = (k * fy + j) * fx + i;
     const int64_t m = D == 0 ? i : (D == 1 ? j : k);
     const int64_t nd = D == 0 ? g.nx : (D == 1 ? g.ny : g.nz);
@@ -486,28 +492,32 @@ __global__ void __launch_bounds__(128)
     const double ch = EQ == EQ_GLM ? __longlong_as_double((long long)sc->glm_lam_bits) -
                                          __longlong_as_double((long long)sc->glm_vel_bits)
                                    : 0.0;
-    double acc[NV];
+    double uL[NV], uR[NV], Fq[NV];
+    const double *pL = F + (int64_t)(s0 * NQF + q) * NV * nf + f0;
+    const double *pR = F + (int64_t)(s1 * NQF + q) * NV * nf + f1;
 #pragma unroll
-    for (int v = 0; v < NV; v++) acc[v] = 0.0;
-#pragma unroll
-    for (int q = 0; q < T::NQF; q++) {
-      double uL[NV], uR[NV], Fq[NV];
-#pragma unroll
-      for (int v = 0; v < NV; v++) {
-        uL[v] = __ldg(F + ((int64_t)(s0 * T::NQF + q) * NV + v) * nf + f0);
-        uR[v] = __ldg(F + ((int64_t)(s1 * T::NQF + q) * NV + v) * nf + f1);
-      }
-      const double s = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
-      vmax = s > vmax ? s : vmax;
-      const double wq = DIM == 2 ? 0.5 : 0.25; // Gauss weights 1/2 (x 1/2 in 3D)
-#pragma unroll
-      for (int v = 0; v < NV; v++) acc[v] += wq * Fq[v];
+    for (int v = 0; v < NV; v++) {
+      uL[v] = __ldg(pL + v * nf);
+      uR[v] = __ldg(pR + v * nf);
     }
+    vmax = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
+    const double wq = DIM == 2 ? 0.5 : 0.25; // Gauss weights 1/2 (x 1/2 in 3D)
 #pragma unroll
-    for (int v = 0; v < NV; v++) G[(int64_t)v * nf + fidx] = acc[v];
+    for (int v = 0; v < NV; v++) part[q][v][threadIdx.x] = wq * Fq[v];
+  }
+  __syncthreads();
+  if (live && q == 0) {
+    const int64_t fidx = (k * fy + j) * fx + i;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int p = 0; p < NQF; p++) acc += part[p][v][threadIdx.x];
+      G[(int64_t)v * nf + fidx] = acc;
+    }
   }
   vmax = warp_max(vmax);
-  if ((threadIdx.x & 31) == 0) atomic_max_pos(&sc->maxvel_bits, vmax);
+  if (threadIdx.x == 0) atomic_max_pos(&sc->maxvel_bits, vmax);
 }
 
 // ---------------------------------------------------------------------------
@@ -961,12 +971,12 @@ struct Launch {
                              cudaStream_t s) {
 #pragma unroll 1
     for (int d = 0; d < DIM; d++) {
-      dim3 grid((unsigned)((g.fdim[d][0] + kBlockX - 1) / kBlockX),
-                (unsigned)((g.fdim[d][1] + kBlockY - 1) / kBlockY), (unsigned)g.fdim[d][2]);
-      if (d == 0) riemann_kernel<DIM, EQ, 0><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(F[0], G[0], g, sc);
-      if (d == 1) riemann_kernel<DIM, EQ, 1><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(F[1], G[1], g, sc);
-      if (DIM == 3 && d == 2)
-        riemann_kernel<DIM, EQ, (DIM == 3 ? 2 : 1)><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(F[2], G[2], g, sc);
+      // one block row of 32 faces per (j, k), NQF points along threadIdx.y
+      const dim3 grid((unsigned)((g.fdim[d][0] + 31) / 32), (unsigned)g.fdim[d][1], (unsigned)g.fdim[d][2]);
+      const dim3 blk(32, Cfg<DIM, EQ>::NQF);
+      if (d == 0) riemann_kernel<DIM, EQ, 0><<<grid, blk, 0, s>>>(F[0], G[0], g, sc);
+      if (d == 1) riemann_kernel<DIM, EQ, 1><<<grid, blk, 0, s>>>(F[1], G[1], g, sc);
+      if (DIM == 3 && d == 2) riemann_kernel<DIM, EQ, (DIM == 3 ? 2 : 1)><<<grid, blk, 0, s>>>(F[2], G[2], g, sc);
     }
     return cudaGetLastError();
   }
