@@ -1,0 +1,70 @@
+// kfvm_host.hpp -- C++ host layer over the C ABI: the reference's ProblemSetup
+// (.init parsing, src/ProblemSetup.H:142-367) and Solver (src/Solver.H:118-160)
+// for one rank on one GPU.  The reference selects dimension, equations, Riemann
+// solver and RK scheme at compile time (exec/<problem>/Definitions.H); here they
+// are read from a "setup" category of the same .init file, next to the
+// reference's own categories (mesh, stencil, time, eos, user, io).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/kfvm_b200.h"
+
+namespace kfvm {
+
+struct ProblemSetup {
+  kfvm_config cfg;
+  int32_t ic = KFVM_IC_SMOOTH_WAVE;
+  uint64_t seed = 12345;
+  std::string baseName = "default", dataDir = "data";
+  int verbose = 0;
+  bool dumpState = false;
+  std::vector<std::string> warnings;
+
+  ProblemSetup();
+  // Reads "category:key value..." lines; reals go through std::stof as in the
+  // reference.  Returns false if the file cannot be opened.
+  bool setFromFile(const std::string &path);
+  std::string toJson() const;
+
+ private:
+  bool setMesh(const std::string &setting);
+  bool setStencil(const std::string &setting);
+  bool setTime(const std::string &setting);
+  bool setEos(const std::string &setting);
+  bool setIO(const std::string &setting);
+  bool setSetup(const std::string &setting);
+};
+
+// Solver::Solver / Solve / TakeStep / evalRHS over the C ABI
+class Solver {
+ public:
+  explicit Solver(const ProblemSetup &ps);
+  ~Solver();
+  Solver(const Solver &) = delete;
+  Solver &operator=(const Solver &) = delete;
+
+  void Solve();
+  void TakeStep();
+  double evalRHS(double t);
+
+  double time() const { return time_; }
+  double dt() const { return dt_; }
+  int64_t acceptedSteps() const { return accepted_; }
+  const kfvm_step_info &lastInfo() const { return info_; }
+  std::vector<double> state() const;
+
+ private:
+  void check(int rc, const char *what) const;
+  const ProblemSetup &ps_;
+  kfvm_solver *s_ = nullptr;
+  kfvm_step_info info_{};
+  double time_ = 0.0, dt_ = 0.0;
+  int64_t accepted_ = 0, nRejectThresh_ = 0, nRejectUnphys_ = 0;
+  int nTS_ = 1;
+  bool lastTimeStep_ = false;
+};
+
+} // namespace kfvm

@@ -14,6 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libkfvm_b200.so")
+RUN = os.path.join(HERE, "kfvm_run")
+HOST_SOURCES = ["host/kfvm_host.cpp", "host/kfvm_run.cpp"]
 
 CU_SOURCES = ["kernels.cu", "ic.cu", "errest.cu", "capi.cu"]
 CXX_SOURCES = ["stencil_weights.cpp"]
@@ -80,6 +82,12 @@ def build(verbose=False, ptxas_info=False):
     if _stale(LIB, objs):
         _run([nvcc, *ARCH, "-shared", "-o", LIB, *objs, blas, "-ccbin", "g++",
               f"-Xlinker=-rpath,{bdir}", "-lcudart"])
+    # C++ host driver (the counterpart of the reference's kfvm.ex)
+    host = [os.path.join(HERE, f) for f in HOST_SOURCES]
+    hdeps = host + [os.path.join(HERE, "host", "kfvm_host.hpp"), os.path.join(ROOT, "include", "kfvm_b200.h"), LIB]
+    if _stale(RUN, hdeps):
+        _run(["g++", "-O2", "-std=c++17", "-o", RUN, *host, f"-L{HERE}", "-lkfvm_b200",
+              "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 
