@@ -42,6 +42,8 @@ def parse():
     p.add_argument("--scale", type=int, default=256, help="grid cells per axis")
     p.add_argument("--e2e-steps", type=int, default=4)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"],
+                   help="arithmetic of the linear reconstruction contraction")
     return p.parse_args()
 
 
@@ -119,26 +121,48 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ roofline
-def algorithmic_bytes(cls, cfg):
-    """Algorithmic HBM bytes per launch of each kernel class (8-byte reals;
-    stencil and halo re-reads are not counted)."""
-    n = abi.ncells(cfg)
-    nv = abi.nvars(cfg)
+def _shape(cfg):
     d = cfg.dim
+    nv = abi.nvars(cfg)
     nqf = 2 if d == 2 else 4
+    nqc = 4 if d == 2 else 8
+    ncst = 13 if d == 2 else 33                         # cells of the radius-2 stencil
+    src = cfg.eq == abi.KFVM_EQ_MHD_GLM
+    return d, nv, nqf, nqc, ncst, src
+
+
+def algorithmic_bytes(cls, cfg):
+    """Algorithmic HBM bytes per launch of each kernel class (8-byte reals; every
+    array element read or written once: stencil and halo re-reads are not counted)."""
+    n = abi.ncells(cfg)
+    d, nv, nqf, nqc, ncst, src = _shape(cfg)
     nf = 2 * d
     nfaces = sum((cfg.nx + (k == 0)) * (cfg.ny + (k == 1)) * ((cfg.nz if d == 3 else 1) + (k == 2))
                  for k in range(d))
     per_cell = {
-        "select": nv * 8 + nf * nqf * 8,                  # U in, indicator per own face point out
-        "flag": 2 * nf * nqf * 8 + nv * 8 + 8 + 1,        # indicators both sides, U, theta, flag
-        "recon": nv * 8 + nf * nqf * nv * 8 + 8 + 2,       # U in, own face states out, theta, flags
-        "stage": (d * nv + 4 * nv) * 8,                   # fluxes, U, Uprev, Uhat in; U', Uhat out
+        # U in; own face states, KXRCF indicator per own face point, status out
+        "recon": nv * 8 + nf * nqf * (nv + 1) * 8 + 1 + ((nqc * nv * 8 + 16) if src else 0),
+        # indicators (each face point once), U, theta in; flag out
+        "flag": nf * nqf * 8 + nv * 8 + 8 + 1,
+        # flag, set, status in; applied out (theta / heavy-list writes are partial)
+        "compact": 4,
+        # Riemann fluxes, U, Uprev, Uhat in; U', Uhat out
+        "stage": (d * nv + 5 * nv) * 8,
         "bc_fill": 0,
     }
     if cls == "riemann":
         return nfaces * (2 * nqf * nv * 8 + nv * 8) / d   # per launch (one direction)
     return per_cell.get(cls, 0) * n
+
+
+def algorithmic_fma(cls, cfg):
+    """FP64 fused multiply-adds per launch of the linear reconstruction contraction:
+    every (stencil cell, weight row, variable) triple once per cell."""
+    if cls != "recon":
+        return None
+    d, nv, nqf, nqc, ncst, src = _shape(cfg)
+    rows = 2 * d * nqf + (nqc if src else 0)
+    return abi.ncells(cfg) * ncst * rows * nv
 
 
 def load_json(path):
@@ -167,6 +191,8 @@ def run_ours(args):
 
     cfg, ic = abi.workload(WORKLOAD, scale=args.scale, steps=args.warmup + args.steps + 10)
     solver = kfvm.Solver(cfg)
+    if args.precision == "tf32x3":
+        solver.set_precision(abi.KFVM_PREC_TF32X3)
     solver.init_ic(ic)
     n = abi.ncells(cfg)
     nv = abi.nvars(cfg)
@@ -251,12 +277,24 @@ def run_ours(args):
     avg_ms = dom_ms / max(dom_n, 1)
     algo = algorithmic_bytes(dom, cfg)
     achieved = algo / (avg_ms / 1e3) / 1e9
+    # DRAM bytes per cell of each kernel class from one ncu capture (profiles/),
+    # scaled by the cells one launch processes
     traffic_tbl = load_json(os.path.join(ROOT, "profiles", "dram_traffic.json")) or {}
-    traffic = traffic_tbl.get(dom, {}).get("bytes_per_launch_at_256") if args.scale == 256 else None
+    per_cell = traffic_tbl.get("bytes_per_cell", {}).get(dom)
+    traffic = per_cell * n if per_cell is not None else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
-                "peak_source": peak_src,
-                "note": "FP64 plain form is FP64-pipe bound, not HBM bound; see fp64 below"}
+                "algorithmic_bytes": algo, "launch_ms": avg_ms,
+                "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback"}
+    fma = algorithmic_fma(dom, cfg)
+    if fma is not None:
+        # FP64 pipe: 148 SMs x 64 FP64 FMA per clock at the maximum SM clock
+        sm_max = (peaks or {}).get("sm_max_mhz", 1965.0)
+        fp64_peak = 148 * 64 * 2 * sm_max * 1e6 / 1e12
+        fp64 = 2 * fma / (avg_ms / 1e3) / 1e12
+        roofline["fp64_pipe"] = {"achieved": fp64, "peak": fp64_peak, "unit": "TFLOP/s",
+                                 "frac": fp64 / fp64_peak, "fma_per_launch": fma,
+                                 "peak_source": "nominal (148 SMs x 64 FP64 FMA/clk x max SM clock)"}
     share = {k: round(v[0] / max(sum(x[0] for x in per_class.values()), 1e-9), 4)
              for k, v in per_class.items() if v[1] > 0}
 

@@ -47,6 +47,8 @@ enum kfvm_ts_status { KFVM_TS_ACCEPTED = 0, KFVM_TS_TOLERANCE = 1, KFVM_TS_UNPHY
  * (src/numeric/Numeric_K.H:292-398); ALL forces full WENO on every cell
  * (the reference's wenothresh < 0 path); NONE never flags (linear only). */
 enum kfvm_indicator { KFVM_IND_KXRCF = 0, KFVM_IND_ALL = 1, KFVM_IND_NONE = 2 };
+/* arithmetic of the linear reconstruction contraction */
+enum kfvm_precision { KFVM_PREC_FP64 = 0, KFVM_PREC_TF32X3 = 1 };
 /* Initial conditions built into the library (cell averages by Q^d Gauss
  * quadrature, src/numeric/Numeric_K.H:31-107). */
 enum kfvm_ic {
@@ -217,6 +219,16 @@ int kfvm_set_time(kfvm_solver *s, double time, double dt);
 
 /* Selects the troubled-cell indicator (enum kfvm_indicator). */
 int kfvm_set_indicator(kfvm_solver *s, int32_t indicator);
+
+/* Selects the arithmetic of the linear reconstruction contraction (enum
+ * kfvm_precision).  KFVM_PREC_FP64 (default) is the reference's arithmetic and
+ * summation order.  KFVM_PREC_TF32X3 computes the stencil sum of the light
+ * (non-WENO) cells on the tcgen05 tensor cores: differences to the cell average
+ * in FP32, split into two TF32 terms, three MMAs per K step, FP32 accumulation;
+ * weights precompute, WENO cells, positivity, Riemann fluxes and the RK update
+ * stay FP64.  No reference counterpart (the reference computes in FP64 only).
+ * KFVM_ERR_ARG if the device is not compute capability 10.x. */
+int kfvm_set_precision(kfvm_solver *s, int32_t precision);
 
 /* Inspection of the last RHS evaluation, for parity tests:
  * face states after the positivity limiter and face BCs, before the Riemann

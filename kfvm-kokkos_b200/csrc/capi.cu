@@ -139,6 +139,7 @@ struct kfvm_solver {
   double time = 0.0, dt = 0.0, errEst = 1.0;
   bool lastTimeStep = false, useSparseWeno = true, primed = false;
   int indicator = KFVM_IND_KXRCF;
+  int precision = KFVM_PREC_FP64;
   int64_t nRhs = 0, nWenoLast = 0;
   int nTS = 1;
   double dmin = 0.0;
@@ -157,6 +158,9 @@ struct kfvm_solver {
 };
 
 namespace {
+
+const char *const kFaultMsg =
+    "tensor-core reconstruction: a block gave up waiting for its MMA completion (bounded wait)";
 
 int set_err_cuda(cudaError_t e, const char *what) {
   return fail(KFVM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -214,7 +218,7 @@ int eval_front(kfvm_solver *s, int b) {
   if ((e = run(s, KFVM_KCLASS_BC, 1, [&] { return launch_bc(dim, eq, s->Ub[b], s->g, st); })) != cudaSuccess)
     return set_err_cuda(e, "bc");
   // reset the per-evaluation counters (nflag, napplied, nheavy) and the GLM maxima
-  CK(cudaMemsetAsync(&s->sc->glm_lam_bits, 0, 2 * sizeof(unsigned long long) + 4 * sizeof(unsigned), st));
+  CK(cudaMemsetAsync(&s->sc->glm_lam_bits, 0, 2 * sizeof(unsigned long long) + 3 * sizeof(unsigned), st));
   int mode;
   if (s->indicator == KFVM_IND_NONE) {
     mode = RECON_LINEAR;
@@ -227,6 +231,9 @@ int eval_front(kfvm_solver *s, int b) {
   }
   if (mode != RECON_FULL) {
     if ((e = run(s, KFVM_KCLASS_RECON, 1, [&] {
+           if (s->precision == KFVM_PREC_TF32X3)
+             return launch_recon_tc(dim, eq, s->Ub[b], s->g, s->dS, mode == RECON_SPARSE, s->F, s->W, s->src,
+                                    s->status, s->lamvel, s->sc, st);
            return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, mode == RECON_SPARSE, s->F, s->W, s->src,
                                s->status, s->lamvel, st);
          })) != cudaSuccess)
@@ -312,6 +319,7 @@ int prime(kfvm_solver *s) {
   if (rc) return rc;
   CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(kfvm::DevScalars), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  if (s->hsc->fault) return fail(KFVM_ERR_CUDA, kFaultMsg);
   const double maxVel = bits_to_double(s->hsc->maxvel_bits);
   s->nWenoLast = s->hsc->napplied;
   s->dt = 0.01 * s->cfg.cfl * s->dmin / maxVel;
@@ -371,6 +379,7 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
       return set_err_cuda(e, "fsal");
     CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (s->hsc->fault) return fail(KFVM_ERR_CUDA, kFaultMsg);
     maxVel = bits_to_double(s->hsc->maxvel_bits);
     s->nWenoLast = s->hsc->napplied;
     const double nDofs = (double)(s->g.n * s->nv);
@@ -571,6 +580,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
       if (cfg->eq == KFVM_EQ_MHD_GLM)
         for (int q = 0; q < hS.w.nqc; q++) hS.lin[c * nrows + r++] = hS.w.cell_w[0][q][c];
     }
+    fill_tc_weights(hS, cfg->dim, nrows);
   }
 
   auto cleanup = [&](cudaError_t e, const char *what) {
@@ -706,6 +716,7 @@ int kfvm_eval_rhs(kfvm_solver *s, double t, double *rhs, double *max_vel) {
   if (rhs)
     CK(cudaMemcpyAsync(rhs, s->K, (size_t)s->g.n * s->nv * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  if (s->hsc->fault) return fail(KFVM_ERR_CUDA, kFaultMsg);
   s->nWenoLast = s->hsc->napplied;
   if (max_vel) *max_vel = bits_to_double(s->hsc->maxvel_bits);
   return KFVM_OK;
@@ -764,6 +775,19 @@ int kfvm_set_indicator(kfvm_solver *s, int32_t ind) {
   if (!s || ind < 0 || ind > KFVM_IND_NONE) return fail(KFVM_ERR_ARG, "bad indicator");
   s->indicator = ind;
   s->useSparseWeno = s->cfg.weno_thresh > 0.0 && ind == KFVM_IND_KXRCF;
+  return KFVM_OK;
+}
+
+int kfvm_set_precision(kfvm_solver *s, int32_t precision) {
+  if (!s || precision < KFVM_PREC_FP64 || precision > KFVM_PREC_TF32X3) return fail(KFVM_ERR_ARG, "bad precision");
+  if (precision == KFVM_PREC_TF32X3) {
+    // tcgen05 exists on compute capability 10.x only
+    int dev = 0, major = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form needs an sm_100 device");
+  }
+  s->precision = precision;
   return KFVM_OK;
 }
 

@@ -1,14 +1,18 @@
 // kernels.cuh -- sm_100a kernels of one RHS evaluation + RK stage update.
 //
-// One stage is five launches on the solver's stream:
+// One stage is these launches on the solver's stream:
 //   bc_fill      periodic / outflow halo of the stage state   (Solver::setCellBCs)
-//   select       linear face states of each cell and its neighbours -> KXRCF flag
-//                (KernelLinearRecon_K + setFaceBCs + WenoSelect_K; no face arrays)
-//   recon        final face states: linear, or WENO-AO for flagged cells, then the
-//                positivity limiter; writes the cell's own face slots
-//                (KernelLinearRecon_K / KernelWenoRecon_K / PositivityPreserve_K)
-//   riemann<d>   one thread per face: HLLC/HLL/LLF at every face point, quadrature
-//                weighted flux sum per face, max wave speed     (RiemannSolver*_K)
+//   recon        linear face states of every cell written to the face arrays, the
+//                KXRCF indicator at each own face point and whether every state lies
+//                inside the positivity bounds (KernelLinearRecon_K); FP64 FMAs, or
+//                the 3xTF32 tcgen05 contraction of recon_tc.cu
+//   flag         KXRCF flags from the indicators               (WenoSelect_K)
+//   compact      the flag-set semantics of WenoSelector::update, theta = 1 for
+//                in-bounds linear cells, the compacted list of heavy cells
+//   heavy        WENO-AO and/or the full positivity limiter on the listed cells
+//                (KernelWenoRecon_K, PositivityPreserve_K)
+//   riemann<d>   one thread per face point: HLLC/HLL/LLF, quadrature weighted flux
+//                sum per face, max wave speed                 (RiemannSolver*_K)
 //   stage        flux divergence (+ viscous terms, + GLM sources), fused with the
 //                low-storage FSAL register update and the error estimate
 //                (IntegrateRHS_K, Viscosity_K, SourceTerms_K, RKFSAL_*_K)
@@ -49,10 +53,15 @@ struct Grid {
 // full-stencil linear weights packed as [cell][row] (rows: face points f*NQF+q, then
 // interior points q) for the light reconstruction pass
 constexpr int kMaxLinRows = 6 * 4 + 8;
+// The same weights for the tensor-core form: W = hi + lo, both TF32 values in FP32
+// containers, stored as the tcgen05 B operand (K-major, no swizzle): K = stencil
+// cells padded to 40, N = rows padded to 32, [cell/4][row][cell%4].
+constexpr int kTcMaxK = 40, kTcMaxN = 32;
 struct DevStencil {
   kfvm_stencil w;
   int64_t loff[KFVM_MAX_CELLS];
   double lin[KFVM_MAX_CELLS * kMaxLinRows];
+  alignas(16) float tcw[2][kTcMaxK * kTcMaxN];
 };
 
 // device-side scalars written by reductions
@@ -62,7 +71,7 @@ struct DevScalars {
   unsigned int nflag;             // KXRCF flags of the current evaluation
   unsigned int napplied;          // cells reconstructed with WENO
   unsigned int nheavy;            // cells in the heavy (WENO / limiter) list
-  unsigned int pad_;
+  unsigned int fault;              // a bounded wait in a kernel gave up (sticky)
   double err, posmin;             // error estimate outputs (finalize kernel)
 };
 

@@ -1,0 +1,107 @@
+// recon_common.cuh -- pieces shared by the FP64 and the tensor-core (3xTF32)
+// linear reconstruction kernels: the weight-row layout, the face-slot addressing
+// of the face arrays and the positivity limiter's per-block footprint tile.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace kfvm {
+
+// ---------------------------------------------------------------------------
+// Linear-reconstruction weights of the full stencil, staged per block in shared
+// memory as [cell][row] (rows: face points f*NQF+q, then interior points), so the
+// weights of consecutive rows for one stencil cell are contiguous broadcast loads.
+// The loop over stencil cells stays rolled: fully unrolled, 3960 FMAs per cell
+// overflow the instruction cache.
+template <int DIM, int EQ>
+struct LinRows {
+  static constexpr int NROWS = Cfg<DIM, EQ>::NF * Cfg<DIM, EQ>::NQF + (Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 0);
+  static constexpr int SIZE = Cfg<DIM, EQ>::C * NROWS;
+};
+
+template <int DIM, int EQ>
+__device__ __forceinline__ void stage_lin_weights(const DevStencil *__restrict__ S, double *__restrict__ sW) {
+  using L = LinRows<DIM, EQ>;
+  for (int t = threadIdx.y * blockDim.x + threadIdx.x; t < L::SIZE; t += blockDim.x * blockDim.y)
+    sW[t] = S->lin[t];
+}
+
+// face-slot address of point q, variable v of face f of cell (i,j,k) in a
+// [slot][q][v][face] array with nvv variables
+__device__ __forceinline__ int64_t face_slot_addr(const Grid &g, int f, int64_t i, int64_t j, int64_t k,
+                                                  int q, int v, int nqf, int nvv) {
+  const int d = f >> 1, hi = f & 1;
+  const int64_t fi = i + (d == 0 && hi), fj = j + (d == 1 && hi), fk = k + (d == 2 && hi);
+  const int64_t fidx = (fk * g.fdim[d][1] + fj) * g.fdim[d][0] + fi;
+  const int slot = hi ? 0 : 1;
+  return ((int64_t)(slot * nqf + q) * nvv + v) * g.nface[d] + fidx;
+}
+
+// Per-block footprint (block cells plus a one-cell ring) of the cell quantities the
+// limiter's bounds read from the 3^d neighbourhood: rho, eint, sound speed and the
+// three velocities.  Each is computed once per cell instead of once per neighbour.
+template <int DIM>
+struct PosTile {
+  static constexpr int TX = kBlockX + 2, TY = kBlockY + 2, TZ = DIM == 3 ? 3 : 1;
+  static constexpr int N = TX * TY * TZ;
+};
+
+template <int DIM, int EQ>
+__device__ __forceinline__ void pos_tile_fill(const double *__restrict__ U, const Grid &g, int64_t i0,
+                                              int64_t j0, int64_t k, double (*sm)[PosTile<DIM>::N]) {
+  using P = PosTile<DIM>;
+  using E = Eos<EQ>;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int t = tid; t < P::N; t += blockDim.x * blockDim.y) {
+    const int a = t % P::TX, b = (t / P::TX) % P::TY, cz = t / (P::TX * P::TY);
+    const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b, gk = k - (DIM == 3 ? 1 : 0) + cz;
+    if (gi > g.nx || gj > g.ny) continue; // beyond the ring of any live cell
+    const double *Uc = U + pidx(g, gi, gj, gk);
+    double st[E::NV];
+#pragma unroll
+    for (int v = 0; v < E::NV; v++) st[v] = Uc[v * g.pvol];
+    sm[0][t] = st[DENS];
+    sm[1][t] = E::eint(st);
+    sm[2][t] = E::soundspeed(g.gamma, st);
+    sm[3][t] = st[MOMX] / st[DENS];
+    sm[4][t] = st[MOMY] / st[DENS];
+    sm[5][t] = st[MOMZ] / st[DENS];
+  }
+}
+
+// PositivityPreserve_K bounds (Common_K.H:331-380) from the footprint tile
+template <int DIM, int EQ>
+__device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<DIM>::N], int tx, int ty) {
+  using P = PosTile<DIM>;
+  double maxDens = -1.7976931348623157e308, minDens = 1.7976931348623157e308;
+  double minEint = 1.7976931348623157e308, minSdSp = 1.7976931348623157e308;
+  constexpr int zr = DIM == 3 ? 1 : 0;
+  auto at = [&](int xo, int yo, int zo) { return ((zr + zo) * P::TY + (ty + 1 + yo)) * P::TX + (tx + 1 + xo); };
+#pragma unroll
+  for (int xo = -1; xo <= 1; xo++)
+#pragma unroll
+    for (int yo = -1; yo <= 1; yo++)
+#pragma unroll
+      for (int zo = -zr; zo <= zr; zo++) {
+        const int t = at(xo, yo, zo);
+        maxDens = fmax(maxDens, sm[0][t]);
+        minDens = fmin(minDens, sm[0][t]);
+        minEint = fmin(minEint, sm[1][t]);
+        minSdSp = fmin(minSdSp, sm[2][t]);
+      }
+  const double dxU = sm[3][at(1, 0, 0)] - sm[3][at(-1, 0, 0)];
+  const double dyV = sm[4][at(0, 1, 0)] - sm[4][at(0, -1, 0)];
+  const double dzW = sm[5][at(0, 0, zr)] - sm[5][at(0, 0, -zr)];
+  const double divV = (dxU + dyV + dzW) / 2.0;
+  double kappa = 0.2;
+  const double eta = fmin(1.0, fmax(0.0, -(kappa * minSdSp + divV) / (kappa * minSdSp)));
+  kappa *= (1.0 - eta);
+  PosBounds b;
+  b.rDens = sm[0][at(0, 0, 0)];
+  b.maxDens = maxDens * (1.0 + kappa);
+  b.minDens = minDens * (1.0 - kappa);
+  b.minEint = minEint * (1.0 - kappa);
+  return b;
+}
+
+} // namespace kfvm

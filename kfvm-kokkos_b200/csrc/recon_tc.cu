@@ -1,0 +1,382 @@
+// recon_tc.cu -- the linear reconstruction contraction on the tcgen05 tensor cores
+// (the FP32 form: 3xTF32 products, FP32 accumulation in tensor memory).
+//
+// Same outputs as recon_kernel (KernelLinearRecon_K, src/stencil/Stencil_K.H:56-119
+// of the reference, plus the KXRCF indicator and the positivity pre-check), with
+// the sum over stencil cells done as one MMA tile per block of 128 cells:
+//
+//   D[m][n] = sum_k A[m][k] B[k][n]      m: cell of the block (TMEM lane)
+//                                        k: stencil cell (33 in 3D, 13 in 2D, zero padded)
+//                                        n: weight row (face points, interior points)
+//   A[m][k] = u(cell m + offset k) - u(cell m)   (per variable; FP64 difference, FP32 value)
+//
+// Reconstructing the deviation from the cell average (the weights of every row sum
+// to one) keeps the FP32 rounding relative to the local variation, not to the
+// state.  Each FP32 operand x is split as x = hi + lo with hi = tf32(x),
+// lo = tf32(x - hi), and D accumulates lo_A hi_B + hi_A lo_B + hi_A hi_B, which
+// carries about 21 significant bits per product.  The face state is then
+// u(cell) + D in FP64; positivity checks, the indicator and everything after the
+// reconstruction stay FP64.
+//
+// Per block (128 threads, one cell per thread = one row of the tile):
+//   warp 0 allocates the TMEM columns (variables x N, rounded to a power of two)
+//   the split weights (B, hi and lo) are copied to shared memory once
+//   per variable: every thread writes its A row (hi and lo) into shared memory in
+//     the canonical K-major no-swizzle layout (8-row x 16-byte core matrices),
+//     thread 0 issues 3 MMAs per K step of 8 into the variable's TMEM columns and
+//     commits them to an mbarrier; the next variable waits for that mbarrier
+//     before it overwrites the A buffer
+//   epilogue: each warp reads its 32 lanes (tcgen05.ld 32x32b), adds the cell
+//     average in FP64 and writes face states, indicators, status
+// Every mbarrier wait is bounded (iteration count and a 1 s global-timer limit);
+// on timeout the block records DevScalars::fault, frees its TMEM and returns.
+// Shared memory per block is sized so that at most 512 / columns blocks are
+// resident on an SM, so a TMEM allocation never waits for another block.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include "kernels.cuh"
+#include "launch.h"
+#include "recon_common.cuh"
+
+namespace kfvm {
+
+template <int DIM, int EQ>
+struct TcShape {
+  using T = Cfg<DIM, EQ>;
+  static constexpr int NR = LinRows<DIM, EQ>::NROWS;
+  static constexpr int NP = DIM == 2 ? 16 : 32;       // MMA N (M = 128: N multiple of 16)
+  static constexpr int KP = DIM == 2 ? 16 : 40;       // stencil cells padded to K steps of 8
+  static constexpr int NKS = KP / 8;
+  static constexpr int NCH = KP / 4;                  // 16-byte core-matrix columns along K
+  static constexpr int COLS_USED = T::NV * NP;
+  static constexpr int COLS = COLS_USED <= 128 ? 128 : (COLS_USED <= 256 ? 256 : 512);
+  static constexpr int MAX_RES = 512 / COLS;          // blocks per SM that fit in TMEM
+  static constexpr int A_CH = 128 * 16;               // one K chunk of A: 128 rows x 16 B
+  static constexpr int A_PART = NCH * A_CH;           // hi or lo part of A
+  static constexpr int B_CH = NP * 16;
+  static constexpr int B_PART = NCH * B_CH;
+  static constexpr int OFF_B = 2 * A_PART;
+  static constexpr int OFF_TILE = OFF_B + 2 * B_PART;
+  static constexpr int OFF_BAR = OFF_TILE + 6 * PosTile<DIM>::N * (int)sizeof(double);
+  static constexpr int USED = OFF_BAR + 16;
+  // 228 KB of shared memory per SM: MAX_RES + 1 blocks of FLOOR bytes do not fit
+  static constexpr int FLOOR = 233472 / (MAX_RES + 1) + 256;
+  static constexpr int SMEM = USED > FLOOR ? USED : FLOOR;
+  static_assert(NR <= NP, "weight rows exceed the MMA N");
+  static_assert(T::C <= KP, "stencil exceeds the MMA K");
+  static_assert(KP <= kTcMaxK && NP <= kTcMaxN, "B table too small");
+  static_assert(SMEM <= 227 * 1024, "shared memory per block");
+  static_assert(kBlockX * kBlockY == 128, "one tile row per thread");
+  static_assert(OFF_BAR % 8 == 0, "mbarrier alignment");
+};
+
+// ---------------------------------------------------------------------------
+// tcgen05 / mbarrier helpers (inline PTX, sm_100a)
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// shared-memory matrix descriptor: start, leading (K) and stride (8-row group)
+// byte offsets, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: D f32, A and B tf32, both K-major, M = 128, N = NP
+template <int NP>
+__host__ __device__ constexpr uint32_t tf32_idesc() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NP >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, const uint32_t (&v)[4]) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v[0]), "r"(v[1]), "r"(v[2]),
+               "r"(v[3])
+               : "memory");
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, int acc) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+// bounded wait for the completion of the mbarrier phase with the given parity
+constexpr uint64_t kTcWaitNs = 1000000000ull;
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 26); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 63u) == 63u && global_ns() - t0 > kTcWaitNs) return false;
+  }
+  return false;
+}
+
+// 8 consecutive TMEM columns of this warp's 32 lanes, waited for in the same asm
+// statement so no use of the registers can move above the wait
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&r)[8]) {
+  uint32_t x0, x1, x2, x3, x4, x5, x6, x7;
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n\t"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(x0), "=r"(x1), "=r"(x2), "=r"(x3), "=r"(x4), "=r"(x5), "=r"(x6), "=r"(x7)
+      : "r"(taddr)
+      : "memory");
+  r[0] = __uint_as_float(x0);
+  r[1] = __uint_as_float(x1);
+  r[2] = __uint_as_float(x2);
+  r[3] = __uint_as_float(x3);
+  r[4] = __uint_as_float(x4);
+  r[5] = __uint_as_float(x5);
+  r[6] = __uint_as_float(x6);
+  r[7] = __uint_as_float(x7);
+}
+
+// ---------------------------------------------------------------------------
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(128)
+    recon_tc_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
+                    double *__restrict__ F0, double *__restrict__ F1, double *__restrict__ F2,
+                    double *__restrict__ W0, double *__restrict__ W1, double *__restrict__ W2,
+                    double *__restrict__ src, uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
+                    DevScalars *__restrict__ sc) {
+  using T = Cfg<DIM, EQ>;
+  using Sh = TcShape<DIM, EQ>;
+  constexpr int NV = T::NV;
+  extern __shared__ __align__(128) uint8_t smem[];
+  double(*tile)[PosTile<DIM>::N] = reinterpret_cast<double(*)[PosTile<DIM>::N]>(smem + Sh::OFF_TILE);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::OFF_BAR);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + Sh::OFF_BAR + 8);
+  const int warp = threadIdx.y;
+  const int row = warp * 32 + threadIdx.x; // tile row = TMEM lane
+  const int64_t i = blockIdx.x * (int64_t)kBlockX + threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)kBlockY + threadIdx.y;
+  const int64_t k = blockIdx.z;
+  const bool live = i < g.nx && j < g.ny;
+  const uint32_t barA = smem_u32(bar);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"((uint32_t)Sh::COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (row == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barA) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // B operand (split weights, already in core-matrix order) and the limiter tile
+  {
+    const float4 *bh = reinterpret_cast<const float4 *>(S->tcw[0]);
+    const float4 *bl = reinterpret_cast<const float4 *>(S->tcw[1]);
+    float4 *dh = reinterpret_cast<float4 *>(smem + Sh::OFF_B);
+    float4 *dl = reinterpret_cast<float4 *>(smem + Sh::OFF_B + Sh::B_PART);
+    for (int t = row; t < Sh::B_PART / 16; t += 128) {
+      dh[t] = bh[t];
+      dl[t] = bl[t];
+    }
+  }
+  pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)kBlockX, blockIdx.y * (int64_t)kBlockY, k, tile);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const double *Uc = U + pidx(g, live ? i : 0, live ? j : 0, k);
+  double uc[NV];
+#pragma unroll
+  for (int v = 0; v < NV; v++) uc[v] = live ? Uc[v * g.pvol] : 0.0;
+  const uint32_t aHi = smem_u32(smem), aLo = aHi + Sh::A_PART;
+  const uint32_t bHi = smem_u32(smem + Sh::OFF_B), bLo = bHi + Sh::B_PART;
+  constexpr uint32_t idesc = tf32_idesc<Sh::NP>();
+
+  bool ok = true;
+#pragma unroll 1
+  for (int v = 0; v < NV; v++) {
+    if (v > 0) ok = mbar_wait(barA, (uint32_t)(v - 1) & 1u);
+    if (!__syncthreads_and(ok)) break;
+    // this thread's A row for variable v: stencil differences split into hi / lo
+    const double *Uv = Uc + v * g.pvol;
+    const double ucv = live ? Uv[0] : 0.0;
+#pragma unroll
+    for (int ch = 0; ch < Sh::NCH; ch++) {
+      uint32_t hi[4], lo[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        const int c = ch * 4 + t;
+        float d = 0.0f;
+        if (c < T::C && live) d = (float)(__ldg(Uv + g.loff[c]) - ucv);
+        hi[t] = to_tf32(d);
+        lo[t] = to_tf32(d - __uint_as_float(hi[t]));
+      }
+      st_shared_v4(aHi + ch * Sh::A_CH + row * 16, hi);
+      st_shared_v4(aLo + ch * Sh::A_CH + row * 16, lo);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (row == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t d = tmem + (uint32_t)(v * Sh::NP);
+#pragma unroll
+      for (int s = 0; s < Sh::NKS; s++) {
+        const uint64_t ah = umma_desc(aHi + 2 * s * Sh::A_CH, Sh::A_CH, 128);
+        const uint64_t al = umma_desc(aLo + 2 * s * Sh::A_CH, Sh::A_CH, 128);
+        const uint64_t bh = umma_desc(bHi + 2 * s * Sh::B_CH, Sh::B_CH, 128);
+        const uint64_t bl = umma_desc(bLo + 2 * s * Sh::B_CH, Sh::B_CH, 128);
+        mma_tf32(d, al, bh, idesc, s > 0);
+        mma_tf32(d, ah, bl, idesc, 1);
+        mma_tf32(d, ah, bh, idesc, 1);
+      }
+      mma_commit(barA);
+    }
+  }
+  if (ok) ok = mbar_wait(barA, (uint32_t)(NV - 1) & 1u);
+  if (__syncthreads_and(ok)) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    PosBounds bd{};
+    if (live) bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
+    const uint32_t lane = (uint32_t)(warp * 32) << 16;
+    double *F[3] = {F0, F1, F2};
+    double *W[3] = {W0, W1, W2};
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    bool inside = true;
+    double lam = 0.0, vel = 0.0;
+#pragma unroll
+    for (int grp = 0; grp < (Sh::NR + 7) / 8; grp++) {
+      float r[NV][8];
+#pragma unroll
+      for (int v = 0; v < NV; v++) tmem_ld8(tmem + lane + (uint32_t)(v * Sh::NP + grp * 8), r[v]);
+      if (live) {
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+          const int rw = grp * 8 + p;
+          if (rw >= Sh::NR) break;
+          double st[NV];
+#pragma unroll
+          for (int v = 0; v < NV; v++) st[v] = uc[v] + (double)r[v][p];
+          inside = inside && pos_inside<EQ>(bd, st);
+          if (rw < T::NF * T::NQF) {
+            const int f = rw / T::NQF, q = rw % T::NQF;
+            const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
+            const int64_t nf = g.nface[f >> 1];
+#pragma unroll
+            for (int v = 0; v < NV; v++) F[f >> 1][a + v * nf] = st[v];
+            if (wantInd) W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno(g.gamma, st);
+            if constexpr (T::SRC) {
+              // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
+              const double vv = fabs(st[MOMX] / st[DENS]);
+              const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
+              vel = vv > vel ? vv : vel;
+              lam = l > lam ? l : lam;
+            }
+          } else if constexpr (T::SRC) {
+            const int q = rw - T::NF * T::NQF;
+#pragma unroll
+            for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
+          }
+        }
+      }
+    }
+    if (live) {
+      if constexpr (T::SRC) lamvel[c] = make_double2(lam, vel);
+      status[c] = inside ? 1 : 0;
+    }
+  } else if (row == 0) {
+    atomicExch(&sc->fault, 1u);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)Sh::COLS)
+                 : "memory");
+}
+
+template <int DIM, int EQ>
+static cudaError_t recon_tc_launch(const double *U, const Grid &g, const DevStencil *S, int wantInd,
+                                   double *const *F, double *const *W, double *src, uint8_t *status,
+                                   double2 *lamvel, DevScalars *sc, cudaStream_t s) {
+  using Sh = TcShape<DIM, EQ>;
+  static bool attr = false; // the attribute is per function and process-wide
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(recon_tc_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Sh::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const dim3 grid((unsigned)((g.nx + kBlockX - 1) / kBlockX), (unsigned)((g.ny + kBlockY - 1) / kBlockY),
+                  (unsigned)g.nz);
+  recon_tc_kernel<DIM, EQ><<<grid, dim3(kBlockX, kBlockY), Sh::SMEM, s>>>(
+      U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, sc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
+                            double *const *F, double *const *W, double *src, uint8_t *status, double2 *lamvel,
+                            DevScalars *sc, cudaStream_t s) {
+  if (dim == 2) {
+    if (eq == EQ_GLM) return recon_tc_launch<2, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
+    if (eq == EQ_NS) return recon_tc_launch<2, EQ_NS>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
+    return recon_tc_launch<2, EQ_HYDRO>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
+  }
+  if (eq == EQ_GLM) return recon_tc_launch<3, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
+  if (eq == EQ_NS) return recon_tc_launch<3, EQ_NS>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
+  return recon_tc_launch<3, EQ_HYDRO>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
+}
+
+// host: W = hi + lo split of the [cell][row] linear weights into the B layout
+void fill_tc_weights(DevStencil &S, int dim, int nrows) {
+  const int np = dim == 2 ? 16 : 32, C = S.w.n_cells;
+  auto tf32 = [](double x) {
+    float f = (float)x;
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    b = (b + 0x1000u) & 0xFFFFE000u; // round to nearest, ties away, on the magnitude
+    std::memcpy(&f, &b, 4);
+    return f;
+  };
+  std::memset(S.tcw, 0, sizeof(S.tcw));
+  for (int c = 0; c < C; c++)
+    for (int n = 0; n < nrows; n++) {
+      const double w = S.lin[c * nrows + n];
+      const float hi = tf32(w);
+      const float lo = tf32(w - (double)hi);
+      const int idx = ((c / 4) * np + n) * 4 + (c % 4);
+      S.tcw[0][idx] = hi;
+      S.tcw[1][idx] = lo;
+    }
+}
+
+} // namespace kfvm

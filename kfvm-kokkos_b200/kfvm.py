@@ -50,6 +50,7 @@ def lib():
         L.kfvm_get_time.argtypes = [P, P, P]
         L.kfvm_set_time.argtypes = [P, D, D]
         L.kfvm_set_indicator.argtypes = [P, I32]
+        L.kfvm_set_precision.argtypes = [P, I32]
         L.kfvm_get_faces.argtypes = [P, I32, P]
         L.kfvm_get_flags.argtypes = [P, P, P]
         L.kfvm_last_stage_ms.argtypes = [P, P]
@@ -147,6 +148,10 @@ class Solver:
 
     def set_indicator(self, ind):
         _check(lib().kfvm_set_indicator(self.h, int(ind)), "kfvm_set_indicator")
+
+    def set_precision(self, prec):
+        """abi.KFVM_PREC_FP64 (default) or abi.KFVM_PREC_TF32X3 (tensor-core stencil sums)."""
+        _check(lib().kfvm_set_precision(self.h, int(prec)), "kfvm_set_precision")
 
     def faces(self, d):
         c = self.cfg
