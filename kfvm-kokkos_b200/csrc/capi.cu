@@ -129,7 +129,7 @@ struct kfvm_solver {
   double *src = nullptr, *theta = nullptr, *part = nullptr;
   uint8_t *flag = nullptr, *wset = nullptr, *applied = nullptr;
   uint32_t *heavy = nullptr; // compacted WENO / limiter cell list (one slot per cell)
-  double *W[3] = {nullptr, nullptr, nullptr}; // KXRCF indicator per own face slot and point
+  float *W[3] = {nullptr, nullptr, nullptr};  // KXRCF indicator (FP32 approximation) per own face slot and point
   uint8_t *status = nullptr;                  // 1: all linear states inside the limiter bounds
   double2 *lamvel = nullptr;                  // GLM speed maxima of each cell's linear states
   int heavyBlocks = 0;
@@ -242,7 +242,7 @@ int eval_front(kfvm_solver *s, int b) {
   if (mode == RECON_SPARSE) {
     const double thr = s->cfg.weno_thresh * std::pow(s->dmin, 1.5);
     if ((e = run(s, KFVM_KCLASS_FLAG, 1, [&] {
-           return launch_flag(dim, eq, s->Ub[b], s->g, s->W, s->theta, s->flag, s->sc, thr, st);
+           return launch_flag(dim, eq, s->Ub[b], s->g, s->W, s->F, s->theta, s->flag, s->sc, thr, st);
          })) != cudaSuccess)
       return set_err_cuda(e, "flag");
   }
@@ -606,7 +606,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
       return cleanup(e, "alloc faces");
     if ((e = dalloc((void **)&s->G[d], nv * g.nface[d] * sizeof(double))) != cudaSuccess)
       return cleanup(e, "alloc fluxes");
-    if ((e = dalloc((void **)&s->W[d], 2 * nqf * g.nface[d] * sizeof(double))) != cudaSuccess)
+    if ((e = dalloc((void **)&s->W[d], 2 * nqf * g.nface[d] * sizeof(float))) != cudaSuccess)
       return cleanup(e, "alloc indicator");
   }
   if (cfg->eq == KFVM_EQ_MHD_GLM &&

@@ -114,7 +114,7 @@ template <int DIM, int EQ, int G>
 __device__ __forceinline__ bool recon_group(const double *__restrict__ Uc, const Grid &g,
                                             const double *__restrict__ sW, const PosBounds &bd,
                                             int64_t i, int64_t j, int64_t k, double *const *F,
-                                            double *const *W, bool wantInd, double &lam, double &vel) {
+                                            float *const *W, bool wantInd, double &lam, double &vel) {
   using T = Cfg<DIM, EQ>;
   constexpr int NP = Groups<DIM, EQ>::NPF;
   bool ok = true;
@@ -130,7 +130,7 @@ __device__ __forceinline__ bool recon_group(const double *__restrict__ Uc, const
     const int64_t nf = g.nface[f >> 1];
 #pragma unroll
     for (int v = 0; v < T::NV; v++) F[f >> 1][a + v * nf] = st[p][v];
-    if (wantInd) W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno(g.gamma, st[p]);
+    if (wantInd) W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno_approx(g.gamma, st[p]);
     if constexpr (T::SRC) {
       // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
       const double vv = fabs(st[p][MOMX] / st[p][DENS]);
@@ -146,8 +146,8 @@ template <int DIM, int EQ>
 __global__ void __launch_bounds__(128)
     recon_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
                  double *__restrict__ F0,
-                 double *__restrict__ F1, double *__restrict__ F2, double *__restrict__ W0,
-                 double *__restrict__ W1, double *__restrict__ W2, double *__restrict__ src,
+                 double *__restrict__ F1, double *__restrict__ F2, float *__restrict__ W0,
+                 float *__restrict__ W1, float *__restrict__ W2, double *__restrict__ src,
                  uint8_t *__restrict__ status, double2 *__restrict__ lamvel) {
   using T = Cfg<DIM, EQ>;
   constexpr int NV = T::NV;
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(128)
   const double *Uc = U + pidx(g, i, j, k);
   const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
   double *F[3] = {F0, F1, F2};
-  double *W[3] = {W0, W1, W2};
+  float *W[3] = {W0, W1, W2};
   double lam = 0.0, vel = 0.0;
   bool ok = recon_group<DIM, EQ, 0>(Uc, g, sW, bd, i, j, k, F, W, wantInd != 0, lam, vel);
   if constexpr (T::SRC) {
@@ -184,13 +184,42 @@ __global__ void __launch_bounds__(128)
 // KXRCF flags (WenoSelect_K, Numeric_K.H:292-398): largest indicator jump across the
 // cell's faces over the cell value; the outer slot of a boundary face follows
 // setFaceBCs (periodic partner face, or the inner slot at an outflow boundary).
+//
+// The face indicators arrive as FP32 approximations (Eos::weno_approx, relative
+// error < kWenoApproxEps).  The decision is taken from them only when it is certain:
+// the exact jump lies within 2 eps max|w| (+ the FP32 rounding of the difference)
+// of the approximate one, and the cell value is exact FP64.  Otherwise (a cell near
+// the threshold, or a NaN marker) every face-point indicator is recomputed exactly
+// in FP64 from the face states, as the reference computes it, so the flags are
+// the reference's.
+template <int DIM, int EQ>
+__device__ __forceinline__ void kxrcf_face(const Grid &g, int fc, int64_t i, int64_t j, int64_t k,
+                                           int64_t &fidx, int64_t &oidx, int &own, int &oth) {
+  const int d = fc >> 1, hi = fc & 1;
+  const int64_t fx = g.fdim[d][0], fy = g.fdim[d][1];
+  const int64_t fi = i + (d == 0 && hi), fj = j + (d == 1 && hi), fk = k + (d == 2 && hi);
+  fidx = (fk * fy + fj) * fx + fi;
+  oidx = fidx;
+  own = hi ? 0 : 1;
+  oth = 1 - own;
+  const int64_t m = d == 0 ? fi : (d == 1 ? fj : fk);
+  const int64_t nd = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+  const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
+  if (m == 0 || m == nd) {
+    if (g.bc[fc] == KFVM_BC_PERIODIC) oidx = m == 0 ? fidx + nd * stride : fidx - nd * stride;
+    else oth = own;
+  }
+}
+
 template <int DIM, int EQ>
 __global__ void __launch_bounds__(128)
-    flag_kernel(const double *__restrict__ U, Grid g, const double *__restrict__ W0,
-                const double *__restrict__ W1, const double *__restrict__ W2,
-                const double *__restrict__ theta, uint8_t *__restrict__ flag,
-                DevScalars *__restrict__ sc, double wThresh) {
+    flag_kernel(const double *__restrict__ U, Grid g, const float *__restrict__ W0,
+                const float *__restrict__ W1, const float *__restrict__ W2,
+                const double *__restrict__ F0, const double *__restrict__ F1,
+                const double *__restrict__ F2, const double *__restrict__ theta,
+                uint8_t *__restrict__ flag, DevScalars *__restrict__ sc, double wThresh) {
   using T = Cfg<DIM, EQ>;
+  constexpr int NV = T::NV;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
   const int64_t k = blockIdx.z;
@@ -199,36 +228,64 @@ __global__ void __launch_bounds__(128)
     const int64_t c = (k * g.ny + j) * g.nx + i;
     f = theta[c] < 1.0;
     if (!f) {
-      const double *W[3] = {W0, W1, W2};
-      double maxJump = 0.0;
+      const float *W[3] = {W0, W1, W2};
+      float jf = 0.0f, wmax = 0.0f;
+      bool bad = false;
 #pragma unroll
       for (int fc = 0; fc < T::NF; fc++) {
-        const int d = fc >> 1, hi = fc & 1;
-        const int64_t fx = g.fdim[d][0], fy = g.fdim[d][1], nf = g.nface[d];
-        const int64_t fi = i + (d == 0 && hi), fj = j + (d == 1 && hi), fk = k + (d == 2 && hi);
-        int64_t fidx = (fk * fy + fj) * fx + fi, oidx = fidx;
-        const int own = hi ? 0 : 1;
-        int oth = 1 - own;
-        const int64_t m = d == 0 ? fi : (d == 1 ? fj : fk);
-        const int64_t nd = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
-        const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
-        if (m == 0 || m == nd) {
-          if (g.bc[fc] == KFVM_BC_PERIODIC) oidx = m == 0 ? fidx + nd * stride : fidx - nd * stride;
-          else oth = own;
-        }
+        int64_t fidx, oidx;
+        int own, oth;
+        kxrcf_face<DIM, EQ>(g, fc, i, j, k, fidx, oidx, own, oth);
+        const int d = fc >> 1;
+        const int64_t nf = g.nface[d];
 #pragma unroll
         for (int q = 0; q < T::NQF; q++) {
-          const double wIn = W[d][(int64_t)(own * T::NQF + q) * nf + fidx];
-          const double wOut = W[d][(int64_t)(oth * T::NQF + q) * nf + oidx];
-          maxJump = fmax(maxJump, fabs(wOut - wIn));
+          const float wIn = W[d][(int64_t)(own * T::NQF + q) * nf + fidx];
+          const float wOut = W[d][(int64_t)(oth * T::NQF + q) * nf + oidx];
+          bad = bad || !(isfinite(wIn) && isfinite(wOut));
+          jf = fmaxf(jf, fabsf(wOut - wIn));
+          wmax = fmaxf(wmax, fmaxf(fabsf(wIn), fabsf(wOut)));
         }
       }
-      double uAv[T::NV];
+      double uAv[NV];
       const double *Uc = U + pidx(g, i, j, k);
 #pragma unroll
-      for (int v = 0; v < T::NV; v++) uAv[v] = Uc[v * g.pvol];
-      const double w = maxJump / Eos<EQ>::weno(g.gamma, uAv);
-      f = w >= wThresh;
+      for (int v = 0; v < NV; v++) uAv[v] = Uc[v * g.pvol];
+      const double wc = Eos<EQ>::weno(g.gamma, uAv);
+      bool certain = false;
+      if (!bad && wc > 0.0 && isfinite(wc)) {
+        const double margin = 2.01 * kWenoApproxEps * (double)wmax + 2e-7 * (double)jf + 1e-300;
+        const double lo = ((double)jf - margin) / wc, hi = ((double)jf + margin) / wc;
+        if (lo >= wThresh) {
+          f = true;
+          certain = true;
+        } else if (hi < wThresh) {
+          f = false;
+          certain = true;
+        }
+      }
+      if (!certain) {
+        const double *F[3] = {F0, F1, F2};
+        double maxJump = 0.0;
+        for (int fc = 0; fc < T::NF; fc++) {
+          int64_t fidx, oidx;
+          int own, oth;
+          kxrcf_face<DIM, EQ>(g, fc, i, j, k, fidx, oidx, own, oth);
+          const int d = fc >> 1;
+          const int64_t nf = g.nface[d];
+          for (int q = 0; q < T::NQF; q++) {
+            double sIn[NV], sOut[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+              sIn[v] = F[d][((int64_t)(own * T::NQF + q) * NV + v) * nf + fidx];
+              sOut[v] = F[d][((int64_t)(oth * T::NQF + q) * NV + v) * nf + oidx];
+            }
+            maxJump = fmax(maxJump, fabs(Eos<EQ>::weno(g.gamma, sOut) - Eos<EQ>::weno(g.gamma, sIn)));
+          }
+        }
+        const double w = maxJump / wc;
+        f = w >= wThresh;
+      }
     }
     flag[c] = f ? 1 : 0;
   }
@@ -846,16 +903,16 @@ struct Launch {
     return cudaGetLastError();
   }
   static cudaError_t recon(const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                           double *const *F, double *const *W, double *src, uint8_t *status,
+                           double *const *F, float *const *W, double *src, uint8_t *status,
                            double2 *lamvel, cudaStream_t s) {
     recon_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
         U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel);
     return cudaGetLastError();
   }
-  static cudaError_t flag(const double *U, const Grid &g, double *const *W, const double *theta,
-                          uint8_t *flag, DevScalars *sc, double thr, cudaStream_t s) {
-    flag_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, W[0], W[1], W[2], theta,
-                                                                          flag, sc, thr);
+  static cudaError_t flag(const double *U, const Grid &g, float *const *W, double *const *F,
+                          const double *theta, uint8_t *flag, DevScalars *sc, double thr, cudaStream_t s) {
+    flag_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, W[0], W[1], W[2], F[0], F[1],
+                                                                          F[2], theta, flag, sc, thr);
     return cudaGetLastError();
   }
   static cudaError_t compact(const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
@@ -928,14 +985,14 @@ cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s)
   KFVM_DISPATCH(dim, eq, bc(U, g, s));
 }
 cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                         double *const *F, double *const *W, double *src, uint8_t *status, double2 *lamvel,
+                         double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
                          cudaStream_t s) {
   KFVM_DISPATCH(dim, eq, recon(U, g, S, wantInd, F, W, src, status, lamvel, s));
 }
-cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, double *const *W,
+cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, float *const *W, double *const *F,
                         const double *theta, uint8_t *flag, DevScalars *sc, double thr,
                         cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, flag(U, g, W, theta, flag, sc, thr, s));
+  KFVM_DISPATCH(dim, eq, flag(U, g, W, F, theta, flag, sc, thr, s));
 }
 cudaError_t launch_compact(int dim, int eq, const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
                            const uint8_t *status, uint8_t *applied, double *theta, uint32_t *heavy,

@@ -31,16 +31,16 @@ cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s)
 // stage front end: linear states + KXRCF indicator + limiter bound status,
 // KXRCF flags, WENO decision / heavy-list compaction, heavy cells
 cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                         double *const *F, double *const *W, double *src, uint8_t *status, double2 *lamvel,
+                         double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
                          cudaStream_t s);
 // the same outputs with the stencil sum on the tcgen05 tensor cores (3xTF32);
 // a block whose wait for the MMA completion gave up sets sc->fault
 cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                            double *const *F, double *const *W, double *src, uint8_t *status, double2 *lamvel,
+                            double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
                             DevScalars *sc, cudaStream_t s);
 // host: split the [cell][row] linear weights of S into the TF32 B-operand tables
 void fill_tc_weights(DevStencil &S, int dim, int nrows);
-cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, double *const *W,
+cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, float *const *W, double *const *F,
                         const double *theta, uint8_t *flag, DevScalars *sc, double thr,
                         cudaStream_t s);
 cudaError_t launch_compact(int dim, int eq, const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,

@@ -22,6 +22,10 @@ enum { DENS = 0, MOMX = 1, MOMY = 2, MOMZ = 3, ETOT = 4, MAGX = 5, MAGY = 6, MAG
 enum { EQ_HYDRO = 0, EQ_NS = 1, EQ_GLM = 2 };
 enum { RS_LLF = 0, RS_HLL = 1, RS_HLLC = 2 };
 
+// bound on the relative error of Eos::weno_approx (exponent error <= 8e-6 from the
+// FP32 log2f / product / exp2f for |gamma log2 rho| <= 60, plus the FP32 roundings)
+constexpr double kWenoApproxEps = 2e-5;
+
 template <int EQ>
 struct Eos {
   static constexpr int NV = EQ == EQ_GLM ? 9 : 5;
@@ -48,6 +52,16 @@ struct Eos {
   // KXRCF indicator variable p / rho^gamma
   __device__ __forceinline__ static double weno(double g, const double *U) {
     return pres(g, U) / pow(U[DENS], g);
+  }
+  // The same indicator with the power taken in FP32 (the pressure stays FP64):
+  // relative error below kWenoApproxEps for densities in [2^-20, 2^20].  Outside
+  // that range, or for a non-finite pressure, it returns NaN, which tells the
+  // reader to recompute the exact value.
+  __device__ __forceinline__ static float weno_approx(double g, const double *U) {
+    const double rho = U[DENS];
+    const double p = pres(g, U);
+    if (!(rho >= 9.5367431640625e-07 && rho <= 1048576.0) || !isfinite(p)) return __int_as_float(0x7fc00000);
+    return (float)p * exp2f(-(float)g * log2f((float)rho));
   }
   __device__ __forceinline__ static double positivity(const double *U) {
     if constexpr (EQ == EQ_GLM) {

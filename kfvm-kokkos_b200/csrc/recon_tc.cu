@@ -169,7 +169,7 @@ template <int DIM, int EQ>
 __global__ void __launch_bounds__(128)
     recon_tc_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
                     double *__restrict__ F0, double *__restrict__ F1, double *__restrict__ F2,
-                    double *__restrict__ W0, double *__restrict__ W1, double *__restrict__ W2,
+                    float *__restrict__ W0, float *__restrict__ W1, float *__restrict__ W2,
                     double *__restrict__ src, uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
                     DevScalars *__restrict__ sc) {
   using T = Cfg<DIM, EQ>;
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(128)
     if (live) bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
     const uint32_t lane = (uint32_t)(warp * 32) << 16;
     double *F[3] = {F0, F1, F2};
-    double *W[3] = {W0, W1, W2};
+    float *W[3] = {W0, W1, W2};
     const int64_t c = (k * g.ny + j) * g.nx + i;
     bool inside = true;
     double lam = 0.0, vel = 0.0;
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(128)
             const int64_t nf = g.nface[f >> 1];
 #pragma unroll
             for (int v = 0; v < NV; v++) F[f >> 1][a + v * nf] = st[v];
-            if (wantInd) W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno(g.gamma, st);
+            if (wantInd) W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno_approx(g.gamma, st);
             if constexpr (T::SRC) {
               // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
               const double vv = fabs(st[MOMX] / st[DENS]);
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(128)
 
 template <int DIM, int EQ>
 static cudaError_t recon_tc_launch(const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                                   double *const *F, double *const *W, double *src, uint8_t *status,
+                                   double *const *F, float *const *W, double *src, uint8_t *status,
                                    double2 *lamvel, DevScalars *sc, cudaStream_t s) {
   using Sh = TcShape<DIM, EQ>;
   static bool attr = false; // the attribute is per function and process-wide
@@ -344,7 +344,7 @@ static cudaError_t recon_tc_launch(const double *U, const Grid &g, const DevSten
 }
 
 cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                            double *const *F, double *const *W, double *src, uint8_t *status, double2 *lamvel,
+                            double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
                             DevScalars *sc, cudaStream_t s) {
   if (dim == 2) {
     if (eq == EQ_GLM) return recon_tc_launch<2, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
