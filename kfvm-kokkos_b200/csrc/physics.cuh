@@ -127,44 +127,43 @@ struct Eos {
     return (qL * sqrt(rL) + qR * sqrt(rR)) / (sqrt(rL) + sqrt(rR));
   }
 
+  // GLM-MHD wave-speed estimates (Davis with the cleaning speed, and the Wu-Shu
+  // bound; MHD_GLM_Riemann.H:25-99)
   __device__ __forceinline__ static double speeds(double g, double ch, const int *vo,
                                                   const int *bo, const double *uL,
                                                   const double *uR, const double *vL,
                                                   const double *vR, double &sL, double &sR) {
-    if constexpr (EQ != EQ_GLM) {
-      (void)ch;
-      (void)bo;
-      const double rhoL = uL[DENS], rhoR = uR[DENS];
-      const double hL = (uL[ETOT] + vL[4]) / rhoL, hR = (uR[ETOT] + vR[4]) / rhoR;
-      const double aL = soundspeed(g, uL), aR = soundspeed(g, uR);
-      const double uTil = roeAvg(rhoL, rhoR, vL[vo[0]], vR[vo[0]]),
-                   vTil = roeAvg(rhoL, rhoR, vL[vo[1]], vR[vo[1]]),
-                   wTil = roeAvg(rhoL, rhoR, vL[vo[2]], vR[vo[2]]),
-                   vsqTil = uTil * uTil + vTil * vTil + wTil * wTil,
-                   hTil = roeAvg(rhoL, rhoR, hL, hR),
-                   aTil = sqrt((g - 1.0) * (hTil - 0.5 * vsqTil));
-      sL = fmin(vL[vo[0]] - aL, uTil - aTil);
-      sR = fmax(vR[vo[0]] + aR, uTil + aTil);
-      return fmax(fabs(sL), fabs(sR));
-    } else {
-      const double cfL = fastMagSonic(g, uL, uL[bo[0]]);
-      const double cfR = fastMagSonic(g, uR, uR[bo[0]]);
-      const double sdL = fmin(vL[vo[0]] - fmax(ch, cfL), vR[vo[0]] - fmax(ch, cfR));
-      const double sdR = fmax(vL[vo[0]] + fmax(ch, cfL), vR[vo[0]] + fmax(ch, cfR));
-      const double rtL = sqrt(uL[DENS]), rtR = sqrt(uR[DENS]);
-      const double rtSum = rtL + rtR, vSum = (rtL * vL[vo[0]] + rtR * vR[vo[0]]) / rtSum;
-      const double b0 = uL[bo[0]] - uR[bo[0]], b1 = uL[bo[1]] - uR[bo[1]],
-                   b2 = uL[bo[2]] - uR[bo[2]];
-      const double bnDiff = sqrt(b0 * b0 + b1 * b1 + b2 * b2) / rtSum;
-      const double aL = fmin(vL[vo[0]], vSum) - cfL - bnDiff;
-      const double aR = fmin(vR[vo[0]], vSum) + cfR + bnDiff;
-      sL = fmin(sdL, aL);
-      sR = fmax(sdR, aR);
-      return fmax(fabs(sL), fabs(sR));
-    }
+    const double cfL = fastMagSonic(g, uL, uL[bo[0]]);
+    const double cfR = fastMagSonic(g, uR, uR[bo[0]]);
+    const double sdL = fmin(vL[vo[0]] - fmax(ch, cfL), vR[vo[0]] - fmax(ch, cfR));
+    const double sdR = fmax(vL[vo[0]] + fmax(ch, cfL), vR[vo[0]] + fmax(ch, cfR));
+    const double rtL = sqrt(uL[DENS]), rtR = sqrt(uR[DENS]);
+    const double rtSum = rtL + rtR, vSum = (rtL * vL[vo[0]] + rtR * vR[vo[0]]) / rtSum;
+    const double b0 = uL[bo[0]] - uR[bo[0]], b1 = uL[bo[1]] - uR[bo[1]],
+                 b2 = uL[bo[2]] - uR[bo[2]];
+    const double bnDiff = sqrt(b0 * b0 + b1 * b1 + b2 * b2) / rtSum;
+    const double aL = fmin(vL[vo[0]], vSum) - cfL - bnDiff;
+    const double aR = fmin(vR[vo[0]], vSum) + cfR + bnDiff;
+    sL = fmin(sdL, aL);
+    sR = fmax(sdR, aR);
+    return fmax(fabs(sL), fabs(sR));
   }
 
-  // Riemann solve at one face point in direction dir; returns max(|sL|,|sR|)
+  // Euler / Navier-Stokes primitives with the density reciprocal taken once
+  // (the reference divides by rho at every use; the values differ by rounding only)
+  __device__ __forceinline__ static void cons2prim_r(double g, const double *U, double ir, double *V) {
+    V[0] = U[DENS];
+    V[1] = U[MOMX] * ir;
+    V[2] = U[MOMY] * ir;
+    V[3] = U[MOMZ] * ir;
+    V[4] = (g - 1.0) * (U[ETOT] - 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]) * ir);
+  }
+
+  // Riemann solve at one face point in direction dir; returns max(|sL|,|sR|).
+  // Euler / Navier-Stokes: Batten/Roe speed estimates (Hydro_Riemann.H:26-80) and,
+  // for HLLC, the low-Mach / shear-corrected star fluxes (Hydro_Riemann.H:82-187),
+  // with each repeated divisor (rho, the Roe weight sum, sL - sS, sR - sS) inverted
+  // once: about a third of the FP64 divisions of the literal form.
   __device__ __forceinline__ static double solve(int rs, double g, double ch, int dir,
                                                  const double *uL, const double *uR,
                                                  double *F) {
@@ -172,36 +171,46 @@ struct Eos {
     const int vo[3] = {MOMX + ord[0], MOMX + ord[1], MOMX + ord[2]};
     const int bo[3] = {MAGX + ord[0], MAGX + ord[1], MAGX + ord[2]};
     double vL[NV], vR[NV];
-    cons2prim(g, uL, vL);
-    cons2prim(g, uR, vR);
-    double sL, sR;
-    const double sMax = speeds(g, ch, vo, bo, uL, uR, vL, vR, sL, sR);
+    double sL, sR, sMax;
     if constexpr (EQ != EQ_GLM) {
+      const double rL = uL[DENS], rR = uR[DENS];
+      const double iL = 1.0 / rL, iR = 1.0 / rR;
+      cons2prim_r(g, uL, iL, vL);
+      cons2prim_r(g, uR, iR, vR);
+      const double pL = vL[4], pR = vR[4];
+      const double a2L = g * pL * iL, a2R = g * pR * iR;
+      const double aL = sqrt(a2L), aR = sqrt(a2R);
+      const double hL = (uL[ETOT] + pL) * iL, hR = (uR[ETOT] + pR) * iR;
+      const double sqL = sqrt(rL), sqR = sqrt(rR), isq = 1.0 / (sqL + sqR);
+      const double uTil = (vL[vo[0]] * sqL + vR[vo[0]] * sqR) * isq,
+                   vTil = (vL[vo[1]] * sqL + vR[vo[1]] * sqR) * isq,
+                   wTil = (vL[vo[2]] * sqL + vR[vo[2]] * sqR) * isq,
+                   hTil = (hL * sqL + hR * sqR) * isq;
+      const double vsqTil = uTil * uTil + vTil * vTil + wTil * wTil;
+      const double aTil = sqrt((g - 1.0) * (hTil - 0.5 * vsqTil));
+      sL = fmin(vL[vo[0]] - aL, uTil - aTil);
+      sR = fmax(vR[vo[0]] + aR, uTil + aTil);
+      sMax = fmax(fabs(sL), fabs(sR));
       if (rs == RS_HLLC) {
         const double vsqL = vL[1] * vL[1] + vL[2] * vL[2] + vL[3] * vL[3];
         const double vsqR = vR[1] * vR[1] + vR[2] * vR[2] + vR[3] * vR[3];
-        const double aL = soundspeed(g, uL), aR = soundspeed(g, uR);
         double M = fmax(sqrt(vsqL) / aL, sqrt(vsqR) / aR);
-        const double rhoL = vL[0], rhoR = vR[0], pL = vL[4], pR = vR[4];
         const double uLn = vL[vo[0]], uRn = vR[vo[0]];
-        const double sS = ((pR - pL) + (rhoL * uLn * (sL - uLn) - rhoR * uRn * (sR - uRn))) /
-                          (rhoL * (sL - uLn) - rhoR * (sR - uRn));
-        const double psL = rhoL * (sL - uLn), psR = rhoR * (sR - uRn);
+        const double psL = rL * (sL - uLn), psR = rR * (sR - uRn);
+        const double sS = ((pR - pL) + (psL * uLn - psR * uRn)) / (psL - psR);
         const double pS = 0.5 * ((pL + pR) + psL * (sS - uLn) + psR * (sS - uRn));
-        const double sFacL = sS / (sL - sS), sFacR = sS / (sR - sS);
-        const double uJump = vR[vo[0]] - vL[vo[0]], vJump = vR[vo[1]] - vL[vo[1]],
-                     wJump = vR[vo[2]] - vL[vo[2]];
-        const double psiL = uL[DENS] * (sL - vL[vo[0]]), psiR = uR[DENS] * (sR - vR[vo[0]]),
-                     psiFac = psiR * psiL / (psiR - psiL);
-        const double presRat = fmin(vL[4] / vR[4], vR[4] / vL[4]);
+        const double dL = 1.0 / (sL - sS), dR = 1.0 / (sR - sS);
+        const double sFacL = sS * dL, sFacR = sS * dR;
+        const double uJump = uRn - uLn, vJump = vR[vo[1]] - vL[vo[1]], wJump = vR[vo[2]] - vL[vo[2]];
+        const double psiFac = psR * psL / (psR - psL);
+        const double presRat = fmin(pL, pR) / fmax(pL, pR);
         const double gFac = 1.0 - pow(presRat, M);
-        const double shFacL = psiFac * gFac * sL / (sL - sS),
-                     shFacR = psiFac * gFac * sR / (sR - sS);
+        const double shFacL = psiFac * gFac * sL * dL, shFacR = psiFac * gFac * sR * dR;
         M = fmin(M, 1.0);
         const double omm = 1.0 - M * M;
         const double fM = M * sqrt(4.0 + omm * omm) / (1.0 + M * M);
-        const double pFacL = psiFac * (fM - 1.0) * uJump + sL * pS / (sL - sS);
-        const double pFacR = psiFac * (fM - 1.0) * uJump + sR * pS / (sR - sS);
+        const double pFacL = psiFac * (fM - 1.0) * uJump + sL * pS * dL;
+        const double pFacR = psiFac * (fM - 1.0) * uJump + sR * pS * dR;
         if (0 <= sL) {
           flux(ch, vo, bo, uL, vL, F);
         } else if (0 <= sS) {
@@ -223,6 +232,10 @@ struct Eos {
         }
         return sMax;
       }
+    } else {
+      cons2prim(g, uL, vL);
+      cons2prim(g, uR, vR);
+      sMax = speeds(g, ch, vo, bo, uL, uR, vL, vR, sL, sR);
     }
     if (rs == RS_LLF) {
       sL = -sMax;
