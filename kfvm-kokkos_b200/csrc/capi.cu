@@ -581,6 +581,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
         for (int q = 0; q < hS.w.nqc; q++) hS.lin[c * nrows + r++] = hS.w.cell_w[0][q][c];
     }
     fill_tc_weights(hS, cfg->dim, nrows);
+    fill_dmma_weights(hS, nrows);
   }
 
   auto cleanup = [&](cudaError_t e, const char *what) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "kernels.cuh"
 #include "launch.h"
@@ -142,6 +143,32 @@ __device__ __forceinline__ bool recon_group(const double *__restrict__ Uc, const
   return ok;
 }
 
+// Linear reconstruction of every cell on the FP64 tensor cores (mma.sync m8n8k4,
+// the FP64 MMA of sm_100a; tcgen05 has no FP64 kind).  Per warp: one row of 32 cells
+// of the block, in 4 groups of 8 cells.  For one group and variable v,
+//   D[cell][row] = sum_k A[cell][k] B[k][row],  A = U(cell + offset k), B = weights,
+// K runs over the stencil in steps of 4 (zero padded), N over the weight rows in
+// tiles of 8; each DMMA does 256 FMAs where the scalar form issues 8 DFMAs.  The
+// sum over stencil cells keeps its order in steps of four.  Lane l holds
+// D[cell l/4][rows 2(l%4), 2(l%4)+1] of every N tile, i.e. the full state (all
+// variables) of 2 NT face / interior points of its cell, and finishes them in FP64:
+// positivity pre-check, indicator, stores.  The four lanes of a cell combine their
+// in-bounds tests and GLM speed maxima by shuffles.
+template <int DIM, int EQ>
+struct DmmaShape {
+  static constexpr int NR = LinRows<DIM, EQ>::NROWS;
+  static constexpr int NT = (NR + 7) / 8;
+  static constexpr int NK = (Cfg<DIM, EQ>::C + 3) / 4;
+  static constexpr int BSIZE = NK * NT * 32;
+  static_assert(BSIZE <= kDmmaMaxB, "B fragment table too small");
+};
+
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 template <int DIM, int EQ>
 __global__ void __launch_bounds__(128)
     recon_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
@@ -150,35 +177,124 @@ __global__ void __launch_bounds__(128)
                  float *__restrict__ W1, float *__restrict__ W2, double *__restrict__ src,
                  uint8_t *__restrict__ status, double2 *__restrict__ lamvel) {
   using T = Cfg<DIM, EQ>;
-  constexpr int NV = T::NV;
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
-  const int64_t k = blockIdx.z;
+  using Sh = DmmaShape<DIM, EQ>;
+  constexpr int NV = T::NV, NT = Sh::NT, NK = Sh::NK;
   __shared__ double tile[6][PosTile<DIM>::N];
-  __shared__ __align__(16) double sW[LinRows<DIM, EQ>::SIZE];
-  stage_lin_weights<DIM, EQ>(S, sW);
-  pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)blockDim.x, blockIdx.y * (int64_t)blockDim.y, k, tile);
+  __shared__ double sB[Sh::BSIZE];
+  __shared__ int64_t sOff[NK * 4];
+  const int tid = threadIdx.y * kBlockX + threadIdx.x;
+  for (int t = tid; t < Sh::BSIZE; t += kBlockX * kBlockY) sB[t] = S->dmma_b[t];
+  if (tid < NK * 4) sOff[tid] = tid < T::C ? g.loff[tid] : 0;
+  const int64_t k = blockIdx.z;
+  pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)kBlockX, blockIdx.y * (int64_t)kBlockY, k, tile);
   __syncthreads();
-  if (i >= g.nx || j >= g.ny) return;
-  const int64_t c = (k * g.ny + j) * g.nx + i;
-  const double *Uc = U + pidx(g, i, j, k);
-  const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
+  // limiter bounds of each block cell, once (the four lanes of a cell share them)
+  __shared__ double sBd[3][kBlockX * kBlockY];
+  {
+    const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
+    sBd[0][tid] = bd.minDens;
+    sBd[1][tid] = bd.maxDens;
+    sBd[2][tid] = bd.minEint;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x;
+  const int64_t j = blockIdx.y * (int64_t)kBlockY + threadIdx.y;
+  const bool rowLive = j < g.ny;
   double *F[3] = {F0, F1, F2};
   float *W[3] = {W0, W1, W2};
-  double lam = 0.0, vel = 0.0;
-  bool ok = recon_group<DIM, EQ, 0>(Uc, g, sW, bd, i, j, k, F, W, wantInd != 0, lam, vel);
-  if constexpr (T::SRC) {
-    double cs[T::NQC][NV];
-    lin_rows<DIM, EQ, T::NF * T::NQF, T::NQC>(Uc, g, sW, cs);
+#pragma unroll 1
+  for (int grp = 0; grp < kBlockX / 8; grp++) {
+    const int cx = grp * 8 + (lane >> 2);
+    const int64_t i = blockIdx.x * (int64_t)kBlockX + cx;
+    const bool live = rowLive && i < g.nx;
+    const double *Uc = U + pidx(g, live ? i : 0, rowLive ? j : 0, k);
+    double acc[NV][NT][2];
 #pragma unroll
-    for (int q = 0; q < T::NQC; q++) {
-      ok = ok && pos_inside<EQ>(bd, cs[q]);
+    for (int v = 0; v < NV; v++)
 #pragma unroll
-      for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = cs[q][v];
+      for (int t = 0; t < NT; t++) acc[v][t][0] = acc[v][t][1] = 0.0;
+#pragma unroll 3
+    for (int ks = 0; ks < NK; ks++) {
+      const int kc = ks * 4 + (lane & 3);
+      const int64_t o = sOff[kc];
+      double a[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) a[v] = kc < T::C ? __ldg(Uc + v * g.pvol + o) : 0.0;
+#pragma unroll
+      for (int t = 0; t < NT; t++) {
+        const double b = sB[(ks * NT + t) * 32 + lane];
+#pragma unroll
+        for (int v = 0; v < NV; v++) dmma_884(acc[v][t], a[v], b);
+      }
     }
-    lamvel[c] = make_double2(lam, vel);
+    bool inside = true;
+    double lam = 0.0, vel = 0.0;
+    if (live) {
+      const int64_t c = (k * g.ny + j) * g.nx + i;
+      PosBounds bd;
+      bd.minDens = sBd[0][threadIdx.y * kBlockX + cx];
+      bd.maxDens = sBd[1][threadIdx.y * kBlockX + cx];
+      bd.minEint = sBd[2][threadIdx.y * kBlockX + cx];
+#pragma unroll
+      for (int t = 0; t < NT; t++) {
+        // rows 8t + 2(lane%4) + e: in 3D (4 points per face) the tile is direction t,
+        // face 2t + (lane%4)/2, points 2(lane%2) + e; in 2D (2 points per face)
+        // face 4t + lane%4, point e
+        const int f = DIM == 3 ? 2 * t + ((lane & 3) >> 1) : 4 * t + (lane & 3);
+        const int d = DIM == 3 ? t : (f >> 1);
+        const int hi = f & 1;
+        const int64_t nf = g.nface[d];
+        const int64_t fidx = ((k + (d == 2 && hi)) * g.fdim[d][1] + (j + (d == 1 && hi))) * g.fdim[d][0] +
+                             (i + (d == 0 && hi));
+        const int slot = hi ? 0 : 1;
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int rw = t * 8 + 2 * (lane & 3) + e;
+          if (rw < Sh::NR) {
+            double st[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) st[v] = acc[v][t][e];
+            inside = inside && pos_inside<EQ>(bd, st);
+            if (rw < T::NF * T::NQF) {
+              const int q = DIM == 3 ? 2 * (lane & 1) + e : e;
+              double *Fd = DIM == 3 ? F[t < 3 ? t : 0] : F[d];
+              const int64_t a = (int64_t)((slot * T::NQF + q) * NV) * nf + fidx;
+#pragma unroll
+              for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
+              if (wantInd)
+                (DIM == 3 ? W[t < 3 ? t : 0] : W[d])[(int64_t)(slot * T::NQF + q) * nf + fidx] =
+                    Eos<EQ>::weno_approx(g.gamma, st);
+              if constexpr (T::SRC) {
+                // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
+                const double vv = fabs(st[MOMX] / st[DENS]);
+                const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
+                vel = vv > vel ? vv : vel;
+                lam = l > lam ? l : lam;
+              }
+            } else if constexpr (T::SRC) {
+              const int q = rw - T::NF * T::NQF;
+#pragma unroll
+              for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
+            }
+          }
+        }
+      }
+    }
+    // combine the four lanes of each cell
+    inside = __shfl_xor_sync(0xffffffffu, (int)inside, 1) && inside;
+    inside = __shfl_xor_sync(0xffffffffu, (int)inside, 2) && inside;
+    if constexpr (T::SRC) {
+      lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, 1));
+      lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, 2));
+      vel = fmax(vel, __shfl_xor_sync(0xffffffffu, vel, 1));
+      vel = fmax(vel, __shfl_xor_sync(0xffffffffu, vel, 2));
+    }
+    if (live && (lane & 3) == 0) {
+      const int64_t c = (k * g.ny + j) * g.nx + i;
+      if constexpr (T::SRC) lamvel[c] = make_double2(lam, vel);
+      status[c] = inside ? 1 : 0;
+    }
   }
-  status[c] = ok ? 1 : 0;
 }
 
 // KXRCF flags (WenoSelect_K, Numeric_K.H:292-398): largest indicator jump across the
@@ -964,6 +1080,18 @@ struct Launch {
     return cudaGetLastError();
   }
 };
+
+// host: B fragments of the FP64 MMA from the [cell][row] linear weights
+void fill_dmma_weights(DevStencil &S, int nrows) {
+  const int C = S.w.n_cells, nt = (nrows + 7) / 8, nk = (C + 3) / 4;
+  std::memset(S.dmma_b, 0, sizeof(S.dmma_b));
+  for (int ks = 0; ks < nk; ks++)
+    for (int t = 0; t < nt; t++)
+      for (int l = 0; l < 32; l++) {
+        const int c = ks * 4 + (l & 3), n = t * 8 + (l >> 2);
+        if (c < C && n < nrows) S.dmma_b[(ks * nt + t) * 32 + l] = S.lin[c * nrows + n];
+      }
+}
 
 int64_t stage_blocks(const Grid &g) {
   const dim3 gr = cell_grid(g);

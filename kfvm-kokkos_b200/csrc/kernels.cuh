@@ -57,11 +57,16 @@ constexpr int kMaxLinRows = 6 * 4 + 8;
 // containers, stored as the tcgen05 B operand (K-major, no swizzle): K = stencil
 // cells padded to 40, N = rows padded to 32, [cell/4][row][cell%4].
 constexpr int kTcMaxK = 40, kTcMaxN = 32;
+// And as B fragments of the FP64 MMA m8n8k4 (4 stencil cells x 8 rows per
+// fragment, one double per lane): [k step][8-row tile][lane], lane -> (cell
+// 4 ks + lane % 4, row 8 nt + lane / 4), zero beyond the stencil or the rows.
+constexpr int kDmmaMaxB = 9 * 4 * 32;
 struct DevStencil {
   kfvm_stencil w;
   int64_t loff[KFVM_MAX_CELLS];
   double lin[KFVM_MAX_CELLS * kMaxLinRows];
   alignas(16) float tcw[2][kTcMaxK * kTcMaxN];
+  alignas(16) double dmma_b[kDmmaMaxB];
 };
 
 // device-side scalars written by reductions

@@ -40,6 +40,8 @@ cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, con
                             DevScalars *sc, cudaStream_t s);
 // host: split the [cell][row] linear weights of S into the TF32 B-operand tables
 void fill_tc_weights(DevStencil &S, int dim, int nrows);
+// host: the same weights as FP64 MMA B fragments
+void fill_dmma_weights(DevStencil &S, int nrows);
 cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, float *const *W, double *const *F,
                         const double *theta, uint8_t *flag, DevScalars *sc, double thr,
                         cudaStream_t s);

@@ -22,8 +22,11 @@ enum { DENS = 0, MOMX = 1, MOMY = 2, MOMZ = 3, ETOT = 4, MAGX = 5, MAGY = 6, MAG
 enum { EQ_HYDRO = 0, EQ_NS = 1, EQ_GLM = 2 };
 enum { RS_LLF = 0, RS_HLL = 1, RS_HLLC = 2 };
 
-// bound on the relative error of Eos::weno_approx (exponent error <= 8e-6 from the
-// FP32 log2f / product / exp2f for |gamma log2 rho| <= 60, plus the FP32 roundings)
+// bound on the relative error of Eos::weno_approx.  For |log2 rho| <= 20 and
+// gamma <= 3 the exponent -gamma lg2(rho) is off by at most gamma x 2 ulp(20)
+// = 1.2e-5 (lg2.approx) plus the FP32 roundings of gamma and of the product
+// (<= 5.5e-6), i.e. <= 1.8e-5 x ln 2 = 1.2e-5 relative after ex2; ex2.approx
+// (2^-22) and the FP32 roundings of p and rho add < 4e-7.
 constexpr double kWenoApproxEps = 2e-5;
 
 template <int EQ>
@@ -53,15 +56,20 @@ struct Eos {
   __device__ __forceinline__ static double weno(double g, const double *U) {
     return pres(g, U) / pow(U[DENS], g);
   }
-  // The same indicator with the power taken in FP32 (the pressure stays FP64):
-  // relative error below kWenoApproxEps for densities in [2^-20, 2^20].  Outside
+  // The same indicator with the power taken in FP32 by the hardware lg2 / ex2
+  // approximations (the pressure stays FP64): relative error below
+  // kWenoApproxEps for densities in [2^-20, 2^20] and 1 < gamma <= 3.  Outside
   // that range, or for a non-finite pressure, it returns NaN, which tells the
   // reader to recompute the exact value.
   __device__ __forceinline__ static float weno_approx(double g, const double *U) {
     const double rho = U[DENS];
     const double p = pres(g, U);
-    if (!(rho >= 9.5367431640625e-07 && rho <= 1048576.0) || !isfinite(p)) return __int_as_float(0x7fc00000);
-    return (float)p * exp2f(-(float)g * log2f((float)rho));
+    if (!(rho >= 9.5367431640625e-07 && rho <= 1048576.0) || !(g <= 3.0) || !isfinite(p))
+      return __int_as_float(0x7fc00000);
+    float l2, r;
+    asm("lg2.approx.f32 %0, %1;" : "=f"(l2) : "f"((float)rho));
+    asm("ex2.approx.f32 %0, %1;" : "=f"(r) : "f"(-(float)g * l2));
+    return (float)p * r;
   }
   __device__ __forceinline__ static double positivity(const double *U) {
     if constexpr (EQ == EQ_GLM) {
