@@ -60,88 +60,20 @@ __global__ void __launch_bounds__(256) bc_fill_kernel(double *__restrict__ U, Gr
   }
 }
 
-// st[p][v] = sum_c W0[R0 + p][c] U[c][v] for NP consecutive weight rows from R0;
-// per output the sum over stencil cells keeps the reference's order
-template <int DIM, int EQ, int R0, int NP>
-__device__ __forceinline__ void lin_rows(const double *__restrict__ Uc, const Grid &g,
-                                         const double *__restrict__ sW,
-                                         double (&st)[NP][Cfg<DIM, EQ>::NV]) {
-  using T = Cfg<DIM, EQ>;
-  constexpr int NR = LinRows<DIM, EQ>::NROWS;
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-#pragma unroll
-    for (int v = 0; v < T::NV; v++) st[p][v] = 0.0;
-#pragma unroll 3
-  for (int c = 0; c < T::C; c++) {
-    const int64_t o = g.loff[c];
-    double u[T::NV];
-#pragma unroll
-    for (int v = 0; v < T::NV; v++) u[v] = __ldg(Uc + v * g.pvol + o);
-    const double *w = sW + c * NR + R0;
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      const double wp = w[p];
-#pragma unroll
-      for (int v = 0; v < T::NV; v++) st[p][v] += wp * u[v];
-    }
-  }
-}
-
-// number of face points reconstructed per pass over the stencil (register budget:
-// NP x NV accumulators)
-template <int DIM, int EQ>
-struct Groups {
-  static constexpr int NPF = Eos<EQ>::NV > 5 ? 4 : 8;
-  static constexpr int NG = (2 * DIM * (DIM == 2 ? 2 : 4)) / NPF;
-};
-
-
 // ---------------------------------------------------------------------------
 // Stage front end, four kernels:
-//   recon    linear face states of every cell (shared-memory weights) written to
-//            the face arrays, the KXRCF indicator p/rho^gamma at each own face point
-//            written to W, and whether every state lies strictly inside the
-//            positivity limiter's bounds (then theta = 1 exactly as in the reference)
-//   flag     KXRCF flags from W (WenoSelect_K)
+//   recon    linear face states of every cell (FP64 MMA) written to the face
+//            arrays, the KXRCF indicator p/rho^gamma (FP32 approximation) at each
+//            own face point written to W, and whether every state lies strictly
+//            inside the positivity limiter's bounds (then theta = 1 exactly as in
+//            the reference)
+//   flag     KXRCF flags from W, exact near the threshold (WenoSelect_K)
 //   compact  the reference's flag-set semantics, theta = 1 for in-bounds linear
 //            cells, and the compacted heavy list (WENO cells, cells to limit)
 //   heavy    WENO-AO and/or the full limiter on the listed cells
 // theta of the previous evaluation feeds the flags, so it is rewritten only after
 // flag_kernel has read it.
 constexpr uint32_t kHeavyWeno = 0x80000000u;
-
-template <int DIM, int EQ, int G>
-__device__ __forceinline__ bool recon_group(const double *__restrict__ Uc, const Grid &g,
-                                            const double *__restrict__ sW, const PosBounds &bd,
-                                            int64_t i, int64_t j, int64_t k, double *const *F,
-                                            float *const *W, bool wantInd, double &lam, double &vel) {
-  using T = Cfg<DIM, EQ>;
-  constexpr int NP = Groups<DIM, EQ>::NPF;
-  bool ok = true;
-  if constexpr (G + 1 < Groups<DIM, EQ>::NG)
-    ok = recon_group<DIM, EQ, G + 1>(Uc, g, sW, bd, i, j, k, F, W, wantInd, lam, vel);
-  double st[NP][T::NV];
-  lin_rows<DIM, EQ, G * NP, NP>(Uc, g, sW, st);
-#pragma unroll
-  for (int p = 0; p < NP; p++) {
-    const int f = (G * NP + p) / T::NQF, q = (G * NP + p) % T::NQF;
-    ok = ok && pos_inside<EQ>(bd, st[p]);
-    const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, T::NV);
-    const int64_t nf = g.nface[f >> 1];
-#pragma unroll
-    for (int v = 0; v < T::NV; v++) F[f >> 1][a + v * nf] = st[p][v];
-    if (wantInd) W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno_approx(g.gamma, st[p]);
-    if constexpr (T::SRC) {
-      // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
-      const double vv = fabs(st[p][MOMX] / st[p][DENS]);
-      const double l = Eos<EQ>::fastMagSonic(g.gamma, st[p], st[p][MAGX]) + vv;
-      vel = vv > vel ? vv : vel;
-      lam = l > lam ? l : lam;
-    }
-  }
-  return ok;
-}
 
 // Linear reconstruction of every cell on the FP64 tensor cores (mma.sync m8n8k4,
 // the FP64 MMA of sm_100a; tcgen05 has no FP64 kind).  Per warp: one row of 32 cells

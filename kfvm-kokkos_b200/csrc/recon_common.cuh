@@ -8,23 +8,14 @@
 namespace kfvm {
 
 // ---------------------------------------------------------------------------
-// Linear-reconstruction weights of the full stencil, staged per block in shared
-// memory as [cell][row] (rows: face points f*NQF+q, then interior points), so the
-// weights of consecutive rows for one stencil cell are contiguous broadcast loads.
-// The loop over stencil cells stays rolled: fully unrolled, 3960 FMAs per cell
-// overflow the instruction cache.
+// Rows of the linear reconstruction: face points f*NQF+q, then (GLM sources)
+// the interior points; the full-stencil weights are [cell][row] on the host
+// and reach the kernels as MMA operand tables.
 template <int DIM, int EQ>
 struct LinRows {
   static constexpr int NROWS = Cfg<DIM, EQ>::NF * Cfg<DIM, EQ>::NQF + (Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 0);
   static constexpr int SIZE = Cfg<DIM, EQ>::C * NROWS;
 };
-
-template <int DIM, int EQ>
-__device__ __forceinline__ void stage_lin_weights(const DevStencil *__restrict__ S, double *__restrict__ sW) {
-  using L = LinRows<DIM, EQ>;
-  for (int t = threadIdx.y * blockDim.x + threadIdx.x; t < L::SIZE; t += blockDim.x * blockDim.y)
-    sW[t] = S->lin[t];
-}
 
 // face-slot address of point q, variable v of face f of cell (i,j,k) in a
 // [slot][q][v][face] array with nvv variables
