@@ -44,6 +44,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"],
                    help="arithmetic of the linear reconstruction contraction")
+    p.add_argument("--no-forms", action="store_true", help="skip timing the FP32 form")
     return p.parse_args()
 
 
@@ -174,6 +175,34 @@ def load_json(path):
 
 
 # ------------------------------------------------------------------ our arm
+def time_form(cfg, ic, prec, steps, warmup):
+    """Zone-updates/s of one arithmetic form: device time of `steps` accepted-step
+    attempts after `warmup`, CUDA events on the solver's stream."""
+    import torch
+    import kfvm
+    s = kfvm.Solver(cfg)
+    s.set_precision(prec)
+    s.init_ic(ic)
+    for _ in range(warmup):
+        s.take_step()
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    s.set_timing(True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    acc = 0
+    for _ in range(steps):
+        acc += s.take_step().accepted
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    per_class = s.timing()
+    s.close()
+    return {"value": acc * abi.ncells(cfg) / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "accepted_steps": acc,
+            "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0}}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -294,7 +323,7 @@ def run_ours(args):
         fp64 = 2 * fma / (avg_ms / 1e3) / 1e12
         roofline["fp64_pipe"] = {"achieved": fp64, "peak": fp64_peak, "unit": "TFLOP/s",
                                  "frac": fp64 / fp64_peak, "fma_per_launch": fma,
-                                 "peak_source": "nominal (148 SMs x 64 FP64 FMA/clk x max SM clock)"}
+                                 "peak_source": "nominal (148 SMs x 64 FP64 FMA/clk x max SM clock; the DMMA rate measured by ncu is the same)"}
     share = {k: round(v[0] / max(sum(x[0] for x in per_class.values()), 1e-9), 4)
              for k, v in per_class.items() if v[1] > 0}
 
@@ -310,13 +339,18 @@ def run_ours(args):
            "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0}}
     out["clocks"] = sampler.summary()
 
+    solver.close()
+    if not args.no_forms:
+        # the FP32 form (3xTF32 tensor-core reconstruction) on the same workload
+        form = time_form(cfg, ic, abi.KFVM_PREC_TF32X3, steps=max(2, args.steps // 2), warmup=2)
+        form["vs_plain"] = form["value"] / value
+        out["forms"] = {"fp32_3xtf32": form}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(sample_scale=64, sample_steps=1)
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
-    solver.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
 
