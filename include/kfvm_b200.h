@@ -46,7 +46,7 @@ enum kfvm_ts_status { KFVM_TS_ACCEPTED = 0, KFVM_TS_TOLERANCE = 1, KFVM_TS_UNPHY
 /* Troubled-cell indicator choice.  KXRCF is the reference's selector
  * (src/numeric/Numeric_K.H:292-398); ALL forces full WENO on every cell
  * (the reference's wenothresh < 0 path); NONE never flags (linear only). */
-enum kfvm_indicator { KFVM_IND_KXRCF = 0, KFVM_IND_ALL = 1, KFVM_IND_NONE = 2 };
+enum kfvm_indicator { KFVM_IND_KXRCF = 0, KFVM_IND_ALL = 1, KFVM_IND_NONE = 2, KFVM_IND_MLP = 3 };
 /* arithmetic of the linear reconstruction contraction */
 enum kfvm_precision { KFVM_PREC_FP64 = 0, KFVM_PREC_TF32X3 = 1 };
 /* Initial conditions built into the library (cell averages by Q^d Gauss
@@ -229,6 +229,51 @@ int kfvm_set_indicator(kfvm_solver *s, int32_t indicator);
  * stay FP64.  No reference counterpart (the reference computes in FP64 only).
  * KFVM_ERR_ARG if the device is not compute capability 10.x. */
 int kfvm_set_precision(kfvm_solver *s, int32_t precision);
+
+/* ---- Learned troubled-cell indicator (KFVM_IND_MLP) -----------------------
+ * No reference counterpart: it replaces the KXRCF selector (WenoSelect_K,
+ * src/numeric/Numeric_K.H:292-398) with a 2x32 MLP over the normalised 5^d
+ * density / pressure patch of a cell: inputs x = (q_k - q_c) / (max|q_k - q_c| +
+ * 1e-6 |q_c|), q = rho then p, 50 (2D) or 250 (3D); NI -> 32 -> 32 -> 1 with GELU
+ * and a sigmoid; BF16 weights, FP32 accumulation.  Weight layout (raw BF16):
+ * W1[32][NI], b1[32], W2[32][32], b2[32], w3[32], b3.
+ * Labels come from the method: a cell is troubled when the normalised WENO-JS
+ * weights of its density or pressure (createOmegas, Stencil_K.H:556-580) depart
+ * from the linear weights by more than tau somewhere.  In the stage, a hashed
+ * fraction of cells (the judge) always runs full WENO; their labels are compared
+ * with the predictions, and a step whose judged troubled cells were missed more
+ * often than miss_limit sends the next two steps to KXRCF.  The kfvm_mlp_* calls
+ * allocate the buffers they need; stepping still allocates nothing. */
+/* number of weights for dim 2 or 3 (2721 / 9121), or KFVM_ERR_ARG */
+int kfvm_mlp_num_weights(int32_t dim);
+/* Glorot-uniform initial weights (zero biases) from seed; clears Adam state */
+int kfvm_mlp_init_weights(kfvm_solver *s, uint64_t seed);
+/* load / read the BF16 weights (n = kfvm_mlp_num_weights(dim)) */
+int kfvm_mlp_set_weights(kfvm_solver *s, const uint16_t *bf16, int64_t n);
+int kfvm_mlp_get_weights(kfvm_solver *s, uint16_t *bf16_out, int64_t n);
+/* allocate (and empty) the training-sample buffer for up to capacity samples */
+int kfvm_mlp_reserve(kfvm_solver *s, int64_t capacity);
+/* append samples of the current state: every cell with departure > tau, other
+ * cells with probability keep_frac (hashed with seed); totals of the buffer */
+int kfvm_mlp_collect(kfvm_solver *s, double tau, double keep_frac, uint64_t seed, int64_t *n_samples,
+                     int64_t *n_positive);
+/* copy samples [first, first+count): BF16 features [count][NI], labels, cell index */
+int kfvm_mlp_get_samples(kfvm_solver *s, int64_t first, int64_t count, uint16_t *feats_bf16, uint8_t *labels,
+                         int64_t *cells);
+/* Adam on the weighted binary cross entropy (positives weighted pos_weight):
+ * steps minibatches of batch samples drawn from the buffer; mean loss of the
+ * first and of the last 20 steps */
+int kfvm_mlp_train(kfvm_solver *s, int32_t steps, int32_t batch, double lr, double pos_weight, uint64_t seed,
+                   double *loss_first, double *loss_last);
+/* decision threshold on the probability (default 0.5), judge fraction (1/64),
+ * label threshold tau (0.3), allowed miss rate of the judge (0.25) */
+int kfvm_mlp_config(kfvm_solver *s, double prob_threshold, double judge_frac, double tau, double miss_limit);
+/* network probability of every cell for the current state ([nz][ny][nx]);
+ * allocates a temporary device array */
+int kfvm_mlp_probability(kfvm_solver *s, float *out_host);
+/* cumulative judge counts: judged, of them troubled, troubled but missed,
+ * predicted but not troubled; fallback events; fallback steps left */
+int kfvm_mlp_stats(kfvm_solver *s, int64_t *out6);
 
 /* Inspection of the last RHS evaluation, for parity tests:
  * face states after the positivity limiter and face BCs, before the Riemann

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <random>
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -155,6 +156,25 @@ struct kfvm_solver {
   std::vector<cudaEvent_t> evPool;
   double clsMs[KFVM_NUM_KCLASS] = {0};
   int64_t clsLaunches[KFVM_NUM_KCLASS] = {0};
+  // learned troubled-cell indicator (buffers allocated by the kfvm_mlp_* calls)
+  struct Mlp {
+    bool ready = false;                 // weights set or initialised
+    int nw = 0, ni = 0;
+    uint16_t *wb = nullptr;             // BF16 weights used by inference
+    float *wq = nullptr;                // the same values as FP32 (training forward)
+    float *master = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *loss = nullptr;
+    int t = 0;                          // Adam steps taken
+    uint8_t *pred = nullptr;            // per-cell prediction of the last evaluation
+    uint16_t *feats = nullptr;          // collected samples: features, labels, cells
+    uint8_t *labels = nullptr;
+    int64_t *cells = nullptr;
+    unsigned long long *count = nullptr;
+    int64_t cap = 0, nPos = 0;
+    double logitThr = 0.0, judgeFrac = 1.0 / 64.0, tau = 0.3, missLimit = 0.25;
+    int fallbackSteps = 0;
+    int64_t fallbackEvents = 0;
+    unsigned long long lastPos = 0, lastMissed = 0;
+  } mlp;
 };
 
 namespace {
@@ -207,6 +227,12 @@ void harvest(kfvm_solver *s) {
   s->marks.clear();
 }
 
+// the reference's wenothresh sign switch: a positive threshold allows the sparse
+// (selected-cells) WENO mode, for KXRCF and for the learned indicator alike
+bool sparse_allowed(const kfvm_solver *s) {
+  return s->cfg.weno_thresh > 0.0 && (s->indicator == KFVM_IND_KXRCF || s->indicator == KFVM_IND_MLP);
+}
+
 // one RHS evaluation on buffer b: BCs, selection, reconstruction, Riemann fluxes.
 // The caller launches the stage kernel that consumes the fluxes.
 int eval_front(kfvm_solver *s, int b) {
@@ -227,32 +253,44 @@ int eval_front(kfvm_solver *s, int b) {
   } else {
     mode = RECON_FULL;
     // after a full-WENO evaluation the sparse mode is allowed again (Solver.cpp:439-443)
-    s->useSparseWeno = s->cfg.weno_thresh > 0.0 && s->indicator == KFVM_IND_KXRCF;
+    s->useSparseWeno = sparse_allowed(s);
   }
+  // the learned indicator selects the cells unless its judge has made the host
+  // fall back to KXRCF for a few steps
+  const bool mlpOn = s->indicator == KFVM_IND_MLP && s->mlp.fallbackSteps == 0;
+  const bool wantInd = mode == RECON_SPARSE && !mlpOn;
   if (mode != RECON_FULL) {
     if ((e = run(s, KFVM_KCLASS_RECON, 1, [&] {
            if (s->precision == KFVM_PREC_TF32X3)
-             return launch_recon_tc(dim, eq, s->Ub[b], s->g, s->dS, mode == RECON_SPARSE, s->F, s->W, s->src,
-                                    s->status, s->lamvel, s->sc, st);
-           return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, mode == RECON_SPARSE, s->F, s->W, s->src,
-                               s->status, s->lamvel, st);
+             return launch_recon_tc(dim, eq, s->Ub[b], s->g, s->dS, wantInd, s->F, s->W, s->src, s->status,
+                                    s->lamvel, s->sc, st);
+           return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, wantInd, s->F, s->W, s->src, s->status, s->lamvel,
+                               st);
          })) != cudaSuccess)
       return set_err_cuda(e, "recon");
   }
   if (mode == RECON_SPARSE) {
     const double thr = s->cfg.weno_thresh * std::pow(s->dmin, 1.5);
     if ((e = run(s, KFVM_KCLASS_FLAG, 1, [&] {
+           if (mlpOn)
+             return launch_mlp_flag(dim, eq, s->Ub[b], s->g, s->mlp.wb, s->theta, s->flag, s->mlp.pred, s->sc,
+                                    (float)s->mlp.logitThr, st);
            return launch_flag(dim, eq, s->Ub[b], s->g, s->W, s->F, s->theta, s->flag, s->sc, thr, st);
          })) != cudaSuccess)
       return set_err_cuda(e, "flag");
   }
+  JudgeArgs jd{0.0, 0, s->mlp.tau, s->mlp.pred};
+  if (mlpOn && mode == RECON_SPARSE) {
+    jd.frac = s->mlp.judgeFrac;
+    jd.seed = 0x6a75646765ull ^ (uint64_t)s->nRhs;
+  }
   if ((e = run(s, KFVM_KCLASS_SELECT, 1, [&] {
          return launch_compact(dim, eq, s->g, mode, s->flag, s->wset, s->status, s->applied, s->theta, s->heavy,
-                               s->lamvel, s->sc, st);
+                               s->lamvel, s->sc, jd, st);
        })) != cudaSuccess)
     return set_err_cuda(e, "compact");
   if ((e = run(s, KFVM_KCLASS_HEAVY, 1, [&] {
-         return launch_heavy(dim, eq, s->Ub[b], s->g, s->dS, s->theta, s->F, s->src, s->heavy, s->sc,
+         return launch_heavy(dim, eq, s->Ub[b], s->g, s->dS, s->theta, s->F, s->src, s->heavy, s->sc, jd,
                              s->heavyBlocks, st);
        })) != cudaSuccess)
     return set_err_cuda(e, "heavy");
@@ -309,7 +347,9 @@ int prime(kfvm_solver *s) {
   s->errEst = 1.0;
   s->lastTimeStep = false;
   s->nTS = 1;
-  s->useSparseWeno = s->cfg.weno_thresh > 0.0 && s->indicator == KFVM_IND_KXRCF;
+  s->useSparseWeno = sparse_allowed(s);
+  s->mlp.fallbackSteps = 0;
+  s->mlp.lastPos = s->mlp.lastMissed = 0;
   const int64_t n = s->g.n;
   CK(cudaMemsetAsync(s->wset, 0, n, s->stream));
   CK(cudaMemsetAsync(s->sc, 0, sizeof(kfvm::DevScalars), s->stream));
@@ -406,6 +446,19 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
       // Uprev <- U by buffer rotation instead of a copy
       s->iPrev = cur;
       s->iCur = cur;
+      // judge of the learned indicator: too many troubled cells missed in this step
+      // sends the next steps to KXRCF
+      if (s->indicator == KFVM_IND_MLP) {
+        if (s->mlp.fallbackSteps > 0) s->mlp.fallbackSteps--;
+        const unsigned long long dPos = s->hsc->mlp_pos - s->mlp.lastPos;
+        const unsigned long long dMiss = s->hsc->mlp_missed - s->mlp.lastMissed;
+        s->mlp.lastPos = s->hsc->mlp_pos;
+        s->mlp.lastMissed = s->hsc->mlp_missed;
+        if (dPos >= 8 && (double)dMiss > s->mlp.missLimit * (double)dPos) {
+          s->mlp.fallbackSteps = 2;
+          s->mlp.fallbackEvents++;
+        }
+      }
       nT++;
       break;
     } else {
@@ -669,6 +722,18 @@ void kfvm_destroy(kfvm_solver *s) {
   cudaFree(s->part);
   cudaFree(s->sc);
   if (s->hsc) cudaFreeHost(s->hsc);
+  cudaFree(s->mlp.wb);
+  cudaFree(s->mlp.wq);
+  cudaFree(s->mlp.master);
+  cudaFree(s->mlp.m);
+  cudaFree(s->mlp.v);
+  cudaFree(s->mlp.grad);
+  cudaFree(s->mlp.loss);
+  cudaFree(s->mlp.pred);
+  cudaFree(s->mlp.feats);
+  cudaFree(s->mlp.labels);
+  cudaFree(s->mlp.cells);
+  cudaFree(s->mlp.count);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   for (auto &m : s->marks) {
@@ -773,9 +838,14 @@ int kfvm_set_time(kfvm_solver *s, double time, double dt) {
 }
 
 int kfvm_set_indicator(kfvm_solver *s, int32_t ind) {
-  if (!s || ind < 0 || ind > KFVM_IND_NONE) return fail(KFVM_ERR_ARG, "bad indicator");
+  if (!s || ind < 0 || ind > KFVM_IND_MLP) return fail(KFVM_ERR_ARG, "bad indicator");
+  if (ind == KFVM_IND_MLP && !s->mlp.ready)
+    return fail(KFVM_ERR_STATE, "learned indicator: no weights (kfvm_mlp_set_weights or kfvm_mlp_init_weights + "
+                                "kfvm_mlp_train)");
+  if (ind == KFVM_IND_MLP && s->g.n > (int64_t)kfvm::kHeavyCellMax)
+    return fail(KFVM_ERR_ARG, "learned indicator: at most 2^30 cells");
   s->indicator = ind;
-  s->useSparseWeno = s->cfg.weno_thresh > 0.0 && ind == KFVM_IND_KXRCF;
+  s->useSparseWeno = sparse_allowed(s);
   return KFVM_OK;
 }
 
@@ -789,6 +859,249 @@ int kfvm_set_precision(kfvm_solver *s, int32_t precision) {
     if (major != 10) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form needs an sm_100 device");
   }
   s->precision = precision;
+  return KFVM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned troubled-cell indicator
+namespace {
+uint16_t f2bf(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0; // NaN
+  u += 0x7fffu + ((u >> 16) & 1u);                    // round to nearest even
+  return (uint16_t)(u >> 16);
+}
+float bf2f(uint16_t b) {
+  const uint32_t u = (uint32_t)b << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+int mlp_alloc(kfvm_solver *s) {
+  auto &M = s->mlp;
+  if (M.wb) return KFVM_OK;
+  M.nw = kfvm::mlp_num_weights(s->dim);
+  M.ni = kfvm::mlp_num_inputs(s->dim);
+  cudaError_t e;
+  if ((e = cudaMalloc((void **)&M.wb, M.nw * sizeof(uint16_t))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.wq, M.nw * sizeof(float))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.master, M.nw * sizeof(float))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.m, M.nw * sizeof(float))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.v, M.nw * sizeof(float))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.grad, M.nw * sizeof(float))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.loss, 4 * sizeof(float))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.pred, s->g.n)) != cudaSuccess)
+    return set_err_cuda(e, "learned indicator buffers");
+  CK(cudaMemsetAsync(M.pred, 0, s->g.n, s->stream));
+  CK(cudaMemsetAsync(M.grad, 0, M.nw * sizeof(float), s->stream));
+  return KFVM_OK;
+}
+
+// master = bf16 values, Adam state cleared
+int mlp_load(kfvm_solver *s, const std::vector<float> &w) {
+  auto &M = s->mlp;
+  std::vector<uint16_t> b(M.nw);
+  std::vector<float> q(M.nw);
+  for (int i = 0; i < M.nw; i++) {
+    b[i] = f2bf(w[i]);
+    q[i] = bf2f(b[i]);
+  }
+  CK(cudaMemcpyAsync(M.wb, b.data(), M.nw * sizeof(uint16_t), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(M.wq, q.data(), M.nw * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(M.master, q.data(), M.nw * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemsetAsync(M.m, 0, M.nw * sizeof(float), s->stream));
+  CK(cudaMemsetAsync(M.v, 0, M.nw * sizeof(float), s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  M.t = 0;
+  M.ready = true;
+  return KFVM_OK;
+}
+} // namespace
+
+int kfvm_mlp_num_weights(int32_t dim) {
+  if (dim != 2 && dim != 3) return fail(KFVM_ERR_ARG, "dim must be 2 or 3");
+  return kfvm::mlp_num_weights(dim);
+}
+
+int kfvm_mlp_init_weights(kfvm_solver *s, uint64_t seed) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  int rc = mlp_alloc(s);
+  if (rc) return rc;
+  const int ni = s->mlp.ni, nh = 32, nw = s->mlp.nw;
+  std::vector<float> w(nw, 0.0f);
+  std::mt19937_64 gen(seed);
+  auto fill = [&](int off, int fanIn, int fanOut, int count) {
+    const double a = std::sqrt(6.0 / (fanIn + fanOut)); // Glorot uniform
+    std::uniform_real_distribution<double> u(-a, a);
+    for (int i = 0; i < count; i++) w[off + i] = (float)u(gen);
+  };
+  fill(0, ni, nh, nh * ni);                            // W1
+  fill(nh * ni + nh, nh, nh, nh * nh);                 // W2
+  fill(nh * ni + nh + nh * nh + nh, nh, 1, nh);        // w3
+  return mlp_load(s, w);
+}
+
+int kfvm_mlp_set_weights(kfvm_solver *s, const uint16_t *bf16, int64_t n) {
+  if (!s || !bf16) return fail(KFVM_ERR_ARG, "null argument");
+  int rc = mlp_alloc(s);
+  if (rc) return rc;
+  if (n != s->mlp.nw) return fail(KFVM_ERR_ARG, "wrong number of learned-indicator weights");
+  std::vector<float> w(n);
+  for (int64_t i = 0; i < n; i++) w[i] = bf2f(bf16[i]);
+  return mlp_load(s, w);
+}
+
+int kfvm_mlp_get_weights(kfvm_solver *s, uint16_t *bf16, int64_t n) {
+  if (!s || !bf16) return fail(KFVM_ERR_ARG, "null argument");
+  if (!s->mlp.ready) return fail(KFVM_ERR_STATE, "learned indicator has no weights");
+  if (n != s->mlp.nw) return fail(KFVM_ERR_ARG, "wrong number of learned-indicator weights");
+  CK(cudaMemcpyAsync(bf16, s->mlp.wb, n * sizeof(uint16_t), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return KFVM_OK;
+}
+
+int kfvm_mlp_reserve(kfvm_solver *s, int64_t capacity) {
+  if (!s || capacity <= 0) return fail(KFVM_ERR_ARG, "bad capacity");
+  int rc = mlp_alloc(s);
+  if (rc) return rc;
+  auto &M = s->mlp;
+  cudaFree(M.feats);
+  cudaFree(M.labels);
+  cudaFree(M.cells);
+  M.feats = nullptr;
+  M.labels = nullptr;
+  M.cells = nullptr;
+  cudaError_t e;
+  if (!M.count && (e = cudaMalloc((void **)&M.count, sizeof(unsigned long long))) != cudaSuccess)
+    return set_err_cuda(e, "sample counter");
+  if ((e = cudaMalloc((void **)&M.feats, (size_t)capacity * M.ni * sizeof(uint16_t))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.labels, (size_t)capacity)) != cudaSuccess ||
+      (e = cudaMalloc((void **)&M.cells, (size_t)capacity * sizeof(int64_t))) != cudaSuccess) {
+    M.cap = 0;
+    return set_err_cuda(e, "sample buffer");
+  }
+  M.cap = capacity;
+  M.nPos = 0;
+  CK(cudaMemsetAsync(M.count, 0, sizeof(unsigned long long), s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return KFVM_OK;
+}
+
+int kfvm_mlp_collect(kfvm_solver *s, double tau, double keep_frac, uint64_t seed, int64_t *n_samples,
+                     int64_t *n_positive) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (!s->primed) return fail(KFVM_ERR_STATE, "collect before an initial condition was set");
+  auto &M = s->mlp;
+  if (!M.cap) return fail(KFVM_ERR_STATE, "kfvm_mlp_reserve first");
+  const int b = s->iCur;
+  cudaError_t e = run(s, KFVM_KCLASS_BC, 1, [&] { return kfvm::launch_bc(s->dim, s->eq, s->Ub[b], s->g, s->stream); });
+  if (e != cudaSuccess) return set_err_cuda(e, "bc");
+  e = run(s, KFVM_KCLASS_OTHER, 1, [&] {
+    return kfvm::launch_mlp_collect(s->dim, s->eq, s->Ub[b], s->g, s->dS, tau, keep_frac, seed, M.feats, M.labels,
+                                    M.cells, M.count, M.cap, s->stream);
+  });
+  if (e != cudaSuccess) return set_err_cuda(e, "collect");
+  unsigned long long cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, M.count, sizeof(cnt), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const int64_t have = std::min<int64_t>((int64_t)cnt, M.cap);
+  std::vector<uint8_t> lab(have);
+  if (have) CK(cudaMemcpy(lab.data(), M.labels, have, cudaMemcpyDeviceToHost));
+  int64_t pos = 0;
+  for (auto l : lab) pos += l;
+  M.nPos = pos;
+  if (n_samples) *n_samples = have;
+  if (n_positive) *n_positive = pos;
+  return KFVM_OK;
+}
+
+int kfvm_mlp_get_samples(kfvm_solver *s, int64_t first, int64_t count, uint16_t *feats, uint8_t *labels,
+                         int64_t *cells) {
+  if (!s || first < 0 || count < 0) return fail(KFVM_ERR_ARG, "bad argument");
+  auto &M = s->mlp;
+  unsigned long long cnt = 0;
+  if (M.count) CK(cudaMemcpy(&cnt, M.count, sizeof(cnt), cudaMemcpyDeviceToHost));
+  const int64_t have = std::min<int64_t>((int64_t)cnt, M.cap);
+  if (first + count > have) return fail(KFVM_ERR_ARG, "sample range beyond the collected samples");
+  if (feats && count)
+    CK(cudaMemcpy(feats, M.feats + first * M.ni, (size_t)count * M.ni * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+  if (labels && count) CK(cudaMemcpy(labels, M.labels + first, (size_t)count, cudaMemcpyDeviceToHost));
+  if (cells && count) CK(cudaMemcpy(cells, M.cells + first, (size_t)count * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  return KFVM_OK;
+}
+
+int kfvm_mlp_train(kfvm_solver *s, int32_t steps, int32_t batch, double lr, double pos_weight, uint64_t seed,
+                   double *loss_first, double *loss_last) {
+  if (!s || steps <= 0 || batch <= 0 || !(lr > 0.0) || !(pos_weight > 0.0)) return fail(KFVM_ERR_ARG, "bad argument");
+  auto &M = s->mlp;
+  if (!M.ready) return fail(KFVM_ERR_STATE, "kfvm_mlp_init_weights or kfvm_mlp_set_weights first");
+  unsigned long long cnt = 0;
+  if (M.count) CK(cudaMemcpy(&cnt, M.count, sizeof(cnt), cudaMemcpyDeviceToHost));
+  const int64_t n = std::min<int64_t>((int64_t)cnt, M.cap);
+  if (n <= 0) return fail(KFVM_ERR_STATE, "no collected samples (kfvm_mlp_collect)");
+  // loss slots: [0] mean over the first 20 steps, [1] over the last 20, [2] the rest
+  CK(cudaMemsetAsync(M.loss, 0, 4 * sizeof(float), s->stream));
+  const int win = std::min(20, steps);
+  for (int i = 0; i < steps; i++) {
+    float *slot = i < win ? M.loss : (i >= steps - win ? M.loss + 1 : M.loss + 2);
+    M.t++;
+    cudaError_t e = run(s, KFVM_KCLASS_OTHER, 2, [&] {
+      return kfvm::launch_mlp_train_step(s->dim, M.feats, M.labels, n, batch, M.master, M.m, M.v, M.grad, M.wq,
+                                         M.wb, slot, (float)pos_weight, (float)lr, M.t, seed ^ (uint64_t)M.t,
+                                         s->stream);
+    });
+    if (e != cudaSuccess) return set_err_cuda(e, "train");
+  }
+  float l[4];
+  CK(cudaMemcpyAsync(l, M.loss, sizeof(l), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  harvest(s);
+  if (loss_first) *loss_first = l[0] / win;
+  if (loss_last) *loss_last = (steps > win ? l[1] : l[0]) / win;
+  return KFVM_OK;
+}
+
+int kfvm_mlp_config(kfvm_solver *s, double prob_threshold, double judge_frac, double tau, double miss_limit) {
+  if (!s || !(prob_threshold > 0.0 && prob_threshold < 1.0) || !(judge_frac >= 0.0 && judge_frac <= 1.0) ||
+      !(tau >= 0.0) || !(miss_limit >= 0.0))
+    return fail(KFVM_ERR_ARG, "bad learned-indicator parameter");
+  s->mlp.logitThr = std::log(prob_threshold / (1.0 - prob_threshold));
+  s->mlp.judgeFrac = judge_frac;
+  s->mlp.tau = tau;
+  s->mlp.missLimit = miss_limit;
+  return KFVM_OK;
+}
+
+int kfvm_mlp_probability(kfvm_solver *s, float *out_host) {
+  if (!s || !out_host) return fail(KFVM_ERR_ARG, "null argument");
+  if (!s->mlp.ready) return fail(KFVM_ERR_STATE, "learned indicator has no weights");
+  if (!s->primed) return fail(KFVM_ERR_STATE, "no state");
+  float *d = nullptr;
+  cudaError_t e;
+  if ((e = cudaMalloc((void **)&d, s->g.n * sizeof(float))) != cudaSuccess) return set_err_cuda(e, "alloc");
+  const int b = s->iCur;
+  e = kfvm::launch_bc(s->dim, s->eq, s->Ub[b], s->g, s->stream);
+  if (e == cudaSuccess) e = kfvm::launch_mlp_prob(s->dim, s->eq, s->Ub[b], s->g, s->mlp.wb, d, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out_host, d, s->g.n * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return set_err_cuda(e, "probability");
+  return KFVM_OK;
+}
+
+int kfvm_mlp_stats(kfvm_solver *s, int64_t *out6) {
+  if (!s || !out6) return fail(KFVM_ERR_ARG, "null argument");
+  CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(kfvm::DevScalars), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  out6[0] = (int64_t)s->hsc->mlp_judged;
+  out6[1] = (int64_t)s->hsc->mlp_pos;
+  out6[2] = (int64_t)s->hsc->mlp_missed;
+  out6[3] = (int64_t)s->hsc->mlp_false;
+  out6[4] = s->mlp.fallbackEvents;
+  out6[5] = s->mlp.fallbackSteps;
   return KFVM_OK;
 }
 

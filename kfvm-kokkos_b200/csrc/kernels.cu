@@ -74,6 +74,8 @@ __global__ void __launch_bounds__(256) bc_fill_kernel(double *__restrict__ U, Gr
 // theta of the previous evaluation feeds the flags, so it is rewritten only after
 // flag_kernel has read it.
 constexpr uint32_t kHeavyWeno = 0x80000000u;
+constexpr uint32_t kHeavyJudge = 0x40000000u; // a judged cell of the learned indicator
+constexpr uint32_t kHeavyCell = 0x3fffffffu;
 
 // Linear reconstruction of every cell on the FP64 tensor cores (mma.sync m8n8k4,
 // the FP64 MMA of sm_100a; tcgen05 has no FP64 kind).  Per warp: one row of 32 cells
@@ -349,9 +351,9 @@ __global__ void __launch_bounds__(256)
     compact_kernel(Grid g, int mode, const uint8_t *__restrict__ flag, uint8_t *__restrict__ wset,
                    const uint8_t *__restrict__ status, uint8_t *__restrict__ applied,
                    double *__restrict__ theta, uint32_t *__restrict__ heavy,
-                   const double2 *__restrict__ lamvel, DevScalars *__restrict__ sc) {
+                   const double2 *__restrict__ lamvel, DevScalars *__restrict__ sc, JudgeArgs jd) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  bool useWeno = false, push = false;
+  bool useWeno = false, push = false, judged = false;
   double lam = 0.0, vel = 0.0;
   if (c < g.n) {
     if (mode == RECON_FULL) {
@@ -364,6 +366,9 @@ __global__ void __launch_bounds__(256)
         useWeno = wset[c] != 0;
       }
     }
+    // the judge's cells run full WENO whatever the flags say (they do not enter the set)
+    judged = mode == RECON_SPARSE && jd.frac > 0.0 && unit_hash(jd.seed, (uint64_t)c) < jd.frac;
+    useWeno = useWeno || judged;
     applied[c] = useWeno ? 1 : 0;
     if (useWeno || !status[c]) {
       push = true;
@@ -382,7 +387,9 @@ __global__ void __launch_bounds__(256)
   unsigned base = 0;
   if (lane == 0 && ball) base = atomicAdd(&sc->nheavy, (unsigned)__popc(ball));
   base = __shfl_sync(0xffffffffu, base, 0);
-  if (push) heavy[base + __popc(ball & ((1u << lane) - 1u))] = (uint32_t)c | (useWeno ? kHeavyWeno : 0u);
+  if (push)
+    heavy[base + __popc(ball & ((1u << lane) - 1u))] =
+        (uint32_t)c | (useWeno ? kHeavyWeno : 0u) | (judged ? kHeavyJudge : 0u);
   if (lane == 0 && wball) atomicAdd(&sc->napplied, (unsigned)__popc(wball));
   if constexpr (EQ == EQ_GLM) {
     lam = warp_max(lam);
@@ -401,7 +408,7 @@ __global__ void __launch_bounds__(128)
     heavy_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S,
                  double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
                  double *__restrict__ F2, double *__restrict__ src,
-                 const uint32_t *__restrict__ heavy, DevScalars *__restrict__ sc) {
+                 const uint32_t *__restrict__ heavy, DevScalars *__restrict__ sc, JudgeArgs jd) {
   using T = Cfg<DIM, EQ>;
   using E = Eos<EQ>;
   constexpr int NV = T::NV;
@@ -410,12 +417,21 @@ __global__ void __launch_bounds__(128)
   double lam = 0.0, vel = 0.0;
   for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
     const uint32_t e = heavy[t];
-    const int64_t c = e & ~kHeavyWeno;
+    const int64_t c = e & kHeavyCell;
     const int64_t i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
     const double *Uc = U + pidx(g, i, j, k);
     double fs[T::NF][T::NQF][NV];
     double cs[T::SRC ? T::NQC : 1][NV];
-    if (e & kHeavyWeno) {
+    if (e & kHeavyJudge) {
+      // judged cell: WENO with its label, compared with the network's prediction
+      double dep = 0.0;
+      weno_cell<DIM, EQ>(Uc, g, S, fs, cs, &dep);
+      const bool lab = dep > jd.tau, p = jd.pred[c] != 0;
+      atomicAdd(&sc->mlp_judged, 1ull);
+      if (lab) atomicAdd(&sc->mlp_pos, 1ull);
+      if (lab && !p) atomicAdd(&sc->mlp_missed, 1ull);
+      if (!lab && p) atomicAdd(&sc->mlp_false, 1ull);
+    } else if (e & kHeavyWeno) {
       weno_cell<DIM, EQ>(Uc, g, S, fs, cs);
     } else {
       for (int f = 0; f < T::NF; f++)
@@ -965,15 +981,15 @@ struct Launch {
   }
   static cudaError_t compact(const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
                              const uint8_t *status, uint8_t *applied, double *theta, uint32_t *heavy,
-                             const double2 *lamvel, DevScalars *sc, cudaStream_t s) {
+                             const double2 *lamvel, DevScalars *sc, const JudgeArgs &jd, cudaStream_t s) {
     compact_kernel<DIM, EQ><<<(unsigned)((g.n + 255) / 256), 256, 0, s>>>(g, mode, flag, wset, status, applied,
-                                                                           theta, heavy, lamvel, sc);
+                                                                           theta, heavy, lamvel, sc, jd);
     return cudaGetLastError();
   }
   static cudaError_t heavy(const double *U, const Grid &g, const DevStencil *S, double *theta,
                            double *const *F, double *src, const uint32_t *heavy, DevScalars *sc,
-                           int heavy_blocks, cudaStream_t s) {
-    heavy_kernel<DIM, EQ><<<heavy_blocks, 128, 0, s>>>(U, g, S, theta, F[0], F[1], F[2], src, heavy, sc);
+                           const JudgeArgs &jd, int heavy_blocks, cudaStream_t s) {
+    heavy_kernel<DIM, EQ><<<heavy_blocks, 128, 0, s>>>(U, g, S, theta, F[0], F[1], F[2], src, heavy, sc, jd);
     return cudaGetLastError();
   }
   static cudaError_t riemann(double *const *F, double *const *G, const Grid &g, DevScalars *sc,
@@ -1056,13 +1072,13 @@ cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, float *
 }
 cudaError_t launch_compact(int dim, int eq, const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
                            const uint8_t *status, uint8_t *applied, double *theta, uint32_t *heavy,
-                           const double2 *lamvel, DevScalars *sc, cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, compact(g, mode, flag, wset, status, applied, theta, heavy, lamvel, sc, s));
+                           const double2 *lamvel, DevScalars *sc, const JudgeArgs &jd, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, compact(g, mode, flag, wset, status, applied, theta, heavy, lamvel, sc, jd, s));
 }
 cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
                          double *theta, double *const *F, double *src, const uint32_t *heavy,
-                         DevScalars *sc, int heavy_blocks, cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, heavy(U, g, S, theta, F, src, heavy, sc, heavy_blocks, s));
+                         DevScalars *sc, const JudgeArgs &jd, int heavy_blocks, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, heavy(U, g, S, theta, F, src, heavy, sc, jd, heavy_blocks, s));
 }
 cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
                            DevScalars *sc, cudaStream_t s) {

@@ -78,6 +78,21 @@ struct DevScalars {
   unsigned int nheavy;            // cells in the heavy (WENO / limiter) list
   unsigned int fault;              // a bounded wait in a kernel gave up (sticky)
   double err, posmin;             // error estimate outputs (finalize kernel)
+  // learned indicator's judge, cumulative: judged cells, of them labelled
+  // troubled, troubled but not predicted (missed), predicted but not troubled
+  unsigned long long mlp_judged, mlp_pos, mlp_missed, mlp_false;
+};
+
+// heavy-list entries carry the cell index in the low 30 bits
+constexpr uint32_t kHeavyCellMax = 0x3fffffffu;
+
+// the learned indicator's judge: a hashed fraction of the cells runs full WENO
+// and has its label compared with the network's prediction
+struct JudgeArgs {
+  double frac;           // 0: no judge
+  uint64_t seed;         // changes every evaluation
+  double tau;            // label threshold on the WENO weight departure
+  const uint8_t *pred;   // the network's per-cell prediction
 };
 
 enum ReconMode { RECON_LINEAR = 0, RECON_SPARSE = 1, RECON_FULL = 2 };
@@ -96,6 +111,19 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *a, double v) 
   // non-negative doubles order like their bit patterns; NaN is ignored as in the
   // reference's "vq > maxVel ? vq : maxVel"
   if (v >= 0.0) atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  // splitmix64 finaliser
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// uniform in [0, 1) from two keys
+__device__ __forceinline__ double unit_hash(uint64_t a, uint64_t b) {
+  return (double)(mix64(a ^ mix64(b)) >> 11) * (1.0 / 9007199254740992.0);
 }
 
 __device__ __forceinline__ double warp_max(double v) {
@@ -130,7 +158,8 @@ template <int DIM, int EQ>
 __device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
                           const DevStencil *__restrict__ S,
                           double (&fs)[Cfg<DIM, EQ>::NF][Cfg<DIM, EQ>::NQF][Cfg<DIM, EQ>::NV],
-                          double (&cs)[Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 1][Cfg<DIM, EQ>::NV]) {
+                          double (&cs)[Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 1][Cfg<DIM, EQ>::NV],
+                          double *dep = nullptr) {
   using T = Cfg<DIM, EQ>;
   constexpr int NV = T::NV;
   const kfvm_stencil &st = S->w;
@@ -165,6 +194,17 @@ __device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
       for (int v = 0; v < NV; v++) om[s][v] += b[v] * b[v];
     }
   }
+  // significance of the density / pressure variation, for the learned indicator's
+  // label (weno_departure)
+  bool sig[2] = {false, false};
+  if (dep) {
+    double lin[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) lin[v] = ref[v];
+    vc.cons2LinPrim(lin);
+    sig[0] = sqrt(om[0][DENS]) > 1e-6 * fabs(lin[DENS]);
+    sig[1] = sqrt(om[0][ETOT]) > 1e-6 * fabs(lin[ETOT]);
+  }
   // nonlinear weights, WENO-JS then AO form (createOmegas, Stencil_K.H:556-580)
   constexpr double gHi = 0.7, gLo = 0.7;
   double gam[T::NSUB];
@@ -182,6 +222,9 @@ __device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
     }
 #pragma unroll
     for (int s = 0; s < T::NSUB; s++) om[s][v] /= tot;
+    if (dep && ((v == DENS && sig[0]) || (v == ETOT && sig[1])))
+#pragma unroll
+      for (int s = 0; s < T::NSUB; s++) *dep = fmax(*dep, fabs(om[s][v] - gam[s]));
     om[0][v] /= gam[0];
 #pragma unroll
     for (int s = 1; s < T::NSUB; s++) om[s][v] -= om[0][v] * gam[s];
@@ -223,6 +266,76 @@ __device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
 // positivity limiter of one cell (PositivityPreserve_K, Common_K.H:299-643), split
 // into the admissible bounds (from the 3^d neighbourhood, with the flattener) and
 // the theta scaling of the reconstructed states toward the cell average.
+// Label of the learned troubled-cell indicator: the largest departure of the
+// normalised WENO-JS weights (createOmegas, Stencil_K.H:556-580, before the
+// adaptive-order transform) from the linear weights gamma_s, over the substencils
+// and over density and pressure (linearised primitives 0 and 4) where their
+// variation over the stencil exceeds 1e-6 of the cell value (below that all
+// smoothness indicators are rounding noise and the weights are arbitrary).  The
+// smoothness indicators are those of weno_cell (findSmoothness, 506-554).
+template <int DIM, int EQ>
+__device__ double weno_departure(const double *__restrict__ Uc, const Grid &g,
+                                 const DevStencil *__restrict__ S) {
+  using T = Cfg<DIM, EQ>;
+  constexpr int NV = T::NV;
+  const kfvm_stencil &st = S->w;
+  double ref[NV];
+#pragma unroll
+  for (int v = 0; v < NV; v++) ref[v] = Uc[v * g.pvol];
+  VarConv<EQ> vc(ref, g.gamma);
+  double lin[NV];
+#pragma unroll
+  for (int v = 0; v < NV; v++) lin[v] = ref[v];
+  vc.cons2LinPrim(lin);
+  double Vf[T::C][2];
+  for (int c = 0; c < T::C; c++) {
+    const int64_t o = S->loff[c];
+    double u[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) u[v] = Uc[v * g.pvol + o];
+    vc.cons2LinPrim(u);
+    Vf[c][0] = u[DENS];
+    Vf[c][1] = u[ETOT];
+  }
+  double om[T::NSUB][2];
+  for (int s = 0; s < T::NSUB; s++) {
+    const int n = s == 0 ? T::C : (s == 1 ? T::CC : T::CB);
+    om[s][0] = om[s][1] = 0.0;
+    for (int i = 0; i < T::NI; i++) {
+      double b0 = 0.0, b1 = 0.0;
+      for (int q = 0; q < n; q++) {
+        const int c = s < 2 ? q : (int)st.sub_idx[s - 2][q];
+        const double w = st.deriv_w[s][i][q];
+        b0 += w * Vf[c][0];
+        b1 += w * Vf[c][1];
+      }
+      om[s][0] += b0 * b0;
+      om[s][1] += b1 * b1;
+    }
+  }
+  constexpr double gHi = 0.7, gLo = 0.7;
+  double gam[T::NSUB];
+  gam[0] = gHi;
+  gam[1] = (1.0 - gHi) * gLo;
+#pragma unroll
+  for (int s = 2; s < T::NSUB; s++) gam[s] = (1.0 - gHi) * (1.0 - gLo) / (DIM == 2 ? 4.0 : 6.0);
+  double dep = 0.0;
+#pragma unroll
+  for (int a = 0; a < 2; a++) {
+    const double r = a == 0 ? lin[DENS] : lin[ETOT];
+    if (!(sqrt(om[0][a]) > 1e-6 * fabs(r))) continue;
+    double tot = 0.0;
+#pragma unroll
+    for (int s = 0; s < T::NSUB; s++) {
+      om[s][a] = gam[s] / (om[s][a] * om[s][a] + 1.e-40);
+      tot += om[s][a];
+    }
+#pragma unroll
+    for (int s = 0; s < T::NSUB; s++) dep = fmax(dep, fabs(om[s][a] / tot - gam[s]));
+  }
+  return dep;
+}
+
 struct PosBounds {
   double rDens, minDens, maxDens, minEint;
 };

@@ -47,13 +47,28 @@ cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, float *
                         cudaStream_t s);
 cudaError_t launch_compact(int dim, int eq, const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
                            const uint8_t *status, uint8_t *applied, double *theta, uint32_t *heavy,
-                           const double2 *lamvel, DevScalars *sc, cudaStream_t s);
+                           const double2 *lamvel, DevScalars *sc, const JudgeArgs &jd, cudaStream_t s);
 cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
                          double *theta, double *const *F, double *src, const uint32_t *heavy,
-                         DevScalars *sc, int heavy_blocks, cudaStream_t s);
+                         DevScalars *sc, const JudgeArgs &jd, int heavy_blocks, cudaStream_t s);
 cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
                            DevScalars *sc, cudaStream_t s);
 cudaError_t launch_stage(int dim, int eq, const StageArgs &a, const Grid &g, cudaStream_t s);
+
+// learned troubled-cell indicator (mlp.cu)
+int mlp_num_weights(int dim);
+int mlp_num_inputs(int dim);
+cudaError_t launch_mlp_collect(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, double tau,
+                               double keep, uint64_t seed, uint16_t *feats, uint8_t *labels, int64_t *cells,
+                               unsigned long long *count, int64_t cap, cudaStream_t s);
+cudaError_t launch_mlp_flag(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
+                            const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc, float logit_thr,
+                            cudaStream_t s);
+cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb, float *out,
+                            cudaStream_t s);
+cudaError_t launch_mlp_train_step(int dim, const uint16_t *feats, const uint8_t *labels, int64_t n, int batch,
+                                  float *master, float *m, float *v, float *grad, float *wq, uint16_t *wb,
+                                  float *loss, float pos_weight, float lr, int t, uint64_t seed, cudaStream_t s);
 cudaError_t launch_stage_pre(int dim, int eq, double *U1, const double *Uprev, double *Uhat,
                              double *Utmp, const double *K, const Grid &g, double betaDt,
                              double bhatDt, int use_tmp, cudaStream_t s);

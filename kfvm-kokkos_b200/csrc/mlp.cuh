@@ -1,0 +1,87 @@
+// mlp.cuh -- the learned troubled-cell indicator: shapes, weight layout and the
+// per-block density / pressure tile its features are read from.
+//
+// Input: the normalised (2r+1)^d patch (r = 2) of density and pressure around a
+// cell, x = (q_k - q_c) / (max_k |q_k - q_c| + 1e-6 |q_c|) for q = rho, p, giving
+// 50 inputs in 2D and 250 in 3D (density first, patch cells in (z, y, x) order,
+// x fastest).  Network: NI -> 32 -> 32 -> 1, GELU after both hidden layers,
+// sigmoid output.  Weights are BF16 (raw uint16 at the C ABI), every sum
+// accumulates in FP32.  Weight layout (one flat array):
+//   W1 [32][NI], b1 [32], W2 [32][32], b2 [32], w3 [32], b3
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace kfvm {
+
+template <int DIM>
+struct MlpShape {
+  static constexpr int R = 2;
+  static constexpr int SIDE = 2 * R + 1;
+  static constexpr int P = DIM == 2 ? SIDE * SIDE : SIDE * SIDE * SIDE;
+  static constexpr int NI = 2 * P;
+  static constexpr int NH = 32;
+  static constexpr int W1 = 0, B1 = NH * NI, W2 = B1 + NH, B2 = W2 + NH * NH, W3 = B2 + NH, B3 = W3 + NH;
+  static constexpr int NW = B3 + 1;
+};
+
+// density / pressure of the block's cells plus a halo of R (padded array indices)
+template <int DIM>
+struct MlpTile {
+  static constexpr int R = MlpShape<DIM>::R;
+  static constexpr int TX = kBlockX + 2 * R, TY = kBlockY + 2 * R, TZ = DIM == 3 ? 2 * R + 1 : 1;
+  static constexpr int N = TX * TY * TZ;
+};
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+template <int DIM, int EQ>
+__device__ __forceinline__ void mlp_tile_fill(const double *__restrict__ U, const Grid &g, int64_t i0, int64_t j0,
+                                              int64_t k, double (*t)[MlpTile<DIM>::N]) {
+  using Tl = MlpTile<DIM>;
+  using E = Eos<EQ>;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int n = tid; n < Tl::N; n += blockDim.x * blockDim.y) {
+    const int a = n % Tl::TX, b = (n / Tl::TX) % Tl::TY, cz = n / (Tl::TX * Tl::TY);
+    const int64_t gi = i0 - Tl::R + a, gj = j0 - Tl::R + b, gk = k - (DIM == 3 ? Tl::R : 0) + cz;
+    if (gi > g.nx + Tl::R - 1 || gj > g.ny + Tl::R - 1) continue; // beyond the padded array
+    const double *Uc = U + pidx(g, gi, gj, gk);
+    double u[E::NV];
+#pragma unroll
+    for (int v = 0; v < E::NV; v++) u[v] = Uc[v * g.pvol];
+    t[0][n] = u[DENS];
+    t[1][n] = E::pres(g.gamma, u);
+  }
+}
+
+// patch maxima and the two scale factors of a cell at block position (tx, ty)
+template <int DIM>
+__device__ __forceinline__ void mlp_scales(const double (*t)[MlpTile<DIM>::N], int tx, int ty, double &rc,
+                                           double &pc, double &sr, double &sp) {
+  using Tl = MlpTile<DIM>;
+  constexpr int R = Tl::R, ZR = DIM == 3 ? R : 0;
+  const int c0 = (ZR * Tl::TY + ty + R) * Tl::TX + tx + R;
+  rc = t[0][c0];
+  pc = t[1][c0];
+  double mr = 0.0, mp = 0.0;
+  for (int dz = -ZR; dz <= ZR; dz++)
+    for (int dy = -R; dy <= R; dy++)
+#pragma unroll
+      for (int dx = -R; dx <= R; dx++) {
+        const int n = c0 + (dz * Tl::TY + dy) * Tl::TX + dx;
+        mr = fmax(mr, fabs(t[0][n] - rc));
+        mp = fmax(mp, fabs(t[1][n] - pc));
+      }
+  sr = 1.0 / (mr + 1e-6 * fabs(rc) + 1e-300);
+  sp = 1.0 / (mp + 1e-6 * fabs(pc) + 1e-300);
+}
+
+} // namespace kfvm

@@ -51,6 +51,17 @@ def lib():
         L.kfvm_set_time.argtypes = [P, D, D]
         L.kfvm_set_indicator.argtypes = [P, I32]
         L.kfvm_set_precision.argtypes = [P, I32]
+        L.kfvm_mlp_num_weights.argtypes = [I32]
+        L.kfvm_mlp_init_weights.argtypes = [P, C.c_uint64]
+        L.kfvm_mlp_set_weights.argtypes = [P, P, I64]
+        L.kfvm_mlp_get_weights.argtypes = [P, P, I64]
+        L.kfvm_mlp_reserve.argtypes = [P, I64]
+        L.kfvm_mlp_collect.argtypes = [P, D, D, C.c_uint64, C.POINTER(I64), C.POINTER(I64)]
+        L.kfvm_mlp_get_samples.argtypes = [P, I64, I64, P, P, P]
+        L.kfvm_mlp_train.argtypes = [P, I32, I32, D, D, C.c_uint64, C.POINTER(D), C.POINTER(D)]
+        L.kfvm_mlp_config.argtypes = [P, D, D, D, D]
+        L.kfvm_mlp_probability.argtypes = [P, P]
+        L.kfvm_mlp_stats.argtypes = [P, P]
         L.kfvm_get_faces.argtypes = [P, I32, P]
         L.kfvm_get_flags.argtypes = [P, P, P]
         L.kfvm_last_stage_ms.argtypes = [P, P]
@@ -152,6 +163,61 @@ class Solver:
     def set_precision(self, prec):
         """abi.KFVM_PREC_FP64 (default) or abi.KFVM_PREC_TF32X3 (tensor-core stencil sums)."""
         _check(lib().kfvm_set_precision(self.h, int(prec)), "kfvm_set_precision")
+
+    # ---- learned troubled-cell indicator
+    def mlp_num_weights(self):
+        return lib().kfvm_mlp_num_weights(self.cfg.dim)
+
+    def mlp_init(self, seed=1):
+        _check(lib().kfvm_mlp_init_weights(self.h, C.c_uint64(seed)), "kfvm_mlp_init_weights")
+
+    def mlp_set_weights(self, w_bf16):
+        w = np.ascontiguousarray(w_bf16, dtype=np.uint16)
+        _check(lib().kfvm_mlp_set_weights(self.h, w.ctypes.data, w.size), "kfvm_mlp_set_weights")
+
+    def mlp_weights(self):
+        w = np.empty(self.mlp_num_weights(), dtype=np.uint16)
+        _check(lib().kfvm_mlp_get_weights(self.h, w.ctypes.data, w.size), "kfvm_mlp_get_weights")
+        return w
+
+    def mlp_reserve(self, capacity):
+        _check(lib().kfvm_mlp_reserve(self.h, int(capacity)), "kfvm_mlp_reserve")
+
+    def mlp_collect(self, tau=0.3, keep=0.1, seed=7):
+        n, p = C.c_int64(), C.c_int64()
+        _check(lib().kfvm_mlp_collect(self.h, float(tau), float(keep), C.c_uint64(seed), C.byref(n), C.byref(p)),
+               "kfvm_mlp_collect")
+        return n.value, p.value
+
+    def mlp_samples(self, first, count):
+        ni = 2 * (25 if self.cfg.dim == 2 else 125)
+        f = np.empty((count, ni), dtype=np.uint16)
+        lab = np.empty(count, dtype=np.uint8)
+        cells = np.empty(count, dtype=np.int64)
+        _check(lib().kfvm_mlp_get_samples(self.h, int(first), int(count), f.ctypes.data, lab.ctypes.data,
+                                          cells.ctypes.data), "kfvm_mlp_get_samples")
+        return f, lab, cells
+
+    def mlp_train(self, steps, batch=1024, lr=3e-3, pos_weight=4.0, seed=11):
+        a, b = C.c_double(), C.c_double()
+        _check(lib().kfvm_mlp_train(self.h, int(steps), int(batch), float(lr), float(pos_weight), C.c_uint64(seed),
+                                    C.byref(a), C.byref(b)), "kfvm_mlp_train")
+        return a.value, b.value
+
+    def mlp_config(self, prob_threshold=0.5, judge_frac=1.0 / 64, tau=0.3, miss_limit=0.25):
+        _check(lib().kfvm_mlp_config(self.h, float(prob_threshold), float(judge_frac), float(tau),
+                                     float(miss_limit)), "kfvm_mlp_config")
+
+    def mlp_probability(self):
+        out = np.empty(self.n, dtype=np.float32)
+        _check(lib().kfvm_mlp_probability(self.h, out.ctypes.data), "kfvm_mlp_probability")
+        return out
+
+    def mlp_stats(self):
+        out = np.zeros(6, dtype=np.int64)
+        _check(lib().kfvm_mlp_stats(self.h, out.ctypes.data), "kfvm_mlp_stats")
+        keys = ["judged", "troubled", "missed", "false_alarm", "fallback_events", "fallback_steps_left"]
+        return dict(zip(keys, out.tolist()))
 
     def faces(self, d):
         c = self.cfg

@@ -13,7 +13,7 @@ KFVM_RS_LLF, KFVM_RS_HLL, KFVM_RS_HLLC = 0, 1, 2
 KFVM_RK_THREESTARP, KFVM_RK_FOURSTARP, KFVM_RK_SSP4_3_2, KFVM_RK_SSP10_4_3 = 0, 1, 2, 3
 KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW = 0, 1
 KFVM_TS_ACCEPTED, KFVM_TS_TOLERANCE, KFVM_TS_UNPHYSICAL = 0, 1, 2
-KFVM_IND_KXRCF, KFVM_IND_ALL, KFVM_IND_NONE = 0, 1, 2
+KFVM_IND_KXRCF, KFVM_IND_ALL, KFVM_IND_NONE, KFVM_IND_MLP = 0, 1, 2, 3
 KFVM_PREC_FP64, KFVM_PREC_TF32X3 = 0, 1
 (KFVM_IC_ISENTROPIC_VORTEX, KFVM_IC_SPHERICAL_SOD, KFVM_IC_KELVIN_HELMHOLTZ,
  KFVM_IC_TAYLOR_GREEN, KFVM_IC_ORSZAG_TANG, KFVM_IC_SMOOTH_WAVE) = range(6)

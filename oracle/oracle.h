@@ -34,6 +34,7 @@ int orc_set_time(orc_solver *s, double time, double dt);
 int orc_keep_faces(orc_solver *s, int32_t on);
 int orc_get_faces(orc_solver *s, int32_t dir, double *out);
 int orc_get_flags(orc_solver *s, uint8_t *weno_applied, double *theta);
+int orc_weno_departure(orc_solver *s, double *out);
 int orc_set_indicator(orc_solver *s, int32_t ind);
 /* Quadrature and RK coefficient tables used by the oracle. */
 int orc_tables(int32_t nq, int32_t rk, double *quad, double *rkt);

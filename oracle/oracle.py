@@ -52,6 +52,7 @@ def lib():
         L.orc_keep_faces.argtypes = [P, I32]
         L.orc_get_flags.argtypes = [P, P, P]
         L.orc_set_indicator.argtypes = [P, I32]
+        L.orc_weno_departure.argtypes = [P, P]
         L.orc_ic_cells.argtypes = [C.POINTER(abi.KfvmConfig), I32, C.c_uint64, P]
         L.orc_tables.argtypes = [I32, I32, P, P]
         _LIB = L
@@ -165,6 +166,12 @@ class OracleSolver:
         th = np.empty(self.n, dtype=np.float64)
         assert lib().orc_get_flags(self.h, a.ctypes.data, th.ctypes.data) == 0
         return a, th
+
+    def weno_departure(self):
+        """max_{s,v} |omega_{s,v} - gamma_s| of every cell (label of the learned indicator)."""
+        out = np.empty(self.n, dtype=np.float64)
+        assert lib().orc_weno_departure(self.h, out.ctypes.data) == 0
+        return out
 
     def set_indicator(self, ind):
         assert lib().orc_set_indicator(self.h, int(ind)) == 0

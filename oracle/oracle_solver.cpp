@@ -749,6 +749,71 @@ void weno_recon(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t 
   }
 }
 
+// Training label of the learned troubled-cell indicator: how far the WENO-AO
+// nonlinear weights of a cell depart from the linear ones,
+//   max over substencils s and variables v of |omega_{s,v} - gamma_s|,
+// with omega the normalised WENO-JS weights of createOmegas (Stencil_K.H:556-580,
+// before the adaptive-order transform) from the smoothness indicators of
+// findSmoothness (Stencil_K.H:506-554), exactly as weno_recon computes them.
+double weno_departure(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t j, int64_t k) {
+  const kfvm_stencil &st = S.st;
+  const int C = st.n_cells, Cc = st.n_cells_ctr, Cb = st.n_cells_bias, nv = S.nv;
+  const int nSub = st.n_sub, nBias = st.n_bias, nIndic = st.n_indic;
+  const double gHi = 0.7, gLo = 0.7;
+  double gamma[8];
+  gamma[0] = gHi;
+  gamma[1] = (1.0 - gHi) * gLo;
+  for (int s = 2; s < nSub; s++) gamma[s] = (1.0 - gHi) * (1.0 - gLo) / (S.dim == 2 ? 4.0 : 6.0);
+  double refState[9];
+  S.load(B, i, j, k, refState);
+  VarConv vc(S.cfg.eq, refState, S.cfg.gamma);
+  double Vf[KFVM_MAX_CELLS][9], Vb[KFVM_MAX_BCELLS][9], Bm[KFVM_MAX_INDIC][9];
+  for (int nC = 0; nC < C; nC++) {
+    S.load(B, i + st.off[0][nC], j + st.off[1][nC], k + (S.dim == 3 ? st.off[2][nC] : 0), Vf[nC]);
+    vc.cons2LinPrim(Vf[nC]);
+  }
+  double omega[8][9];
+  auto smooth = [&](int s, double (*V)[9], int n) {
+    for (int nI = 0; nI < nIndic; nI++)
+      for (int v = 0; v < nv; v++) {
+        double cc = 0.0;
+        for (int q = 0; q < n; q++) cc += st.deriv_w[s][nI][q] * V[q][v];
+        Bm[nI][v] = cc;
+      }
+    for (int v = 0; v < nv; v++) {
+      omega[s][v] = 0.0;
+      for (int nI = 0; nI < nIndic; nI++) omega[s][v] += Bm[nI][v] * Bm[nI][v];
+    }
+  };
+  smooth(0, Vf, C);
+  smooth(1, Vf, Cc);
+  for (int nB = 0; nB < nBias; nB++) {
+    for (int v = 0; v < nv; v++)
+      for (int c = 0; c < Cb; c++) Vb[c][v] = Vf[st.sub_idx[nB][c]][v];
+    smooth(2 + nB, Vb, Cb);
+  }
+  // density and pressure (linearised primitives 0 and 4), where their variation
+  // over the full stencil is above rounding level (1e-6 of the cell value): there
+  // all substencil indicators vanish and the normalised weights are arbitrary
+  double dep = 0.0;
+  const int vs[2] = {0, 4};
+  double lin[9];
+  for (int v = 0; v < nv; v++) lin[v] = refState[v];
+  vc.cons2LinPrim(lin);  // (rho, u, v, w, p) of the cell itself
+  const double ref[2] = {lin[0], lin[4]};
+  for (int a = 0; a < 2; a++) {
+    const int v = vs[a];
+    if (!(std::sqrt(omega[0][v]) > 1e-6 * std::fabs(ref[a]))) continue;
+    double tot = 0.0;
+    for (int s = 0; s < nSub; s++) {
+      omega[s][v] = gamma[s] / (omega[s][v] * omega[s][v] + 1.e-40);
+      tot += omega[s][v];
+    }
+    for (int s = 0; s < nSub; s++) dep = fmax(dep, fabs(omega[s][v] / tot - gamma[s]));
+  }
+  return dep;
+}
+
 // WenoSelect_K (Numeric_K.H:292-398); returns the flag
 bool kxrcf(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t j, int64_t k,
            double wThresh) {
@@ -1614,6 +1679,19 @@ int orc_get_flags(orc_solver *s, uint8_t *weno_applied, double *theta) {
   if (weno_applied) std::memcpy(weno_applied, s->applied.data(), s->n);
   if (theta) std::memcpy(theta, s->theta.data(), sizeof(double) * s->n);
   return 0;
+}
+
+// WENO weight departure of every cell of the current state ([nz][ny][nx])
+int orc_weno_departure(orc_solver *s, double *out) {
+  if (!s || !out) return KFVM_ERR_ARG;
+  std::vector<double> B = s->U;
+  set_cell_bcs(*s, B);
+  orc_solver &S = *s;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int64_t k = 0; k < S.nz; k++)
+    for (int64_t j = 0; j < S.ny; j++)
+      for (int64_t i = 0; i < S.nx; i++) out[S.ci(i, j, k)] = weno_departure(S, B, i, j, k);
+  return KFVM_OK;
 }
 
 int orc_set_indicator(orc_solver *s, int32_t ind) {
