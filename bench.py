@@ -9,6 +9,13 @@ time step (4 RHS evaluations + stage updates + error estimate) of the whole grid
 one zone-update is one cell advanced by one accepted step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload sod3d|kelvin_helmholtz|taylor_green|orszag_tang|isentropic_vortex]
+                  [--scale N] [--no-forms] [--no-cpu-baseline]
+
+Beside the plain FP64 value the line carries "forms": the same workload with the
+3xTF32 tensor-core reconstruction (fp32_3xtf32), and with the learned
+troubled-cell indicator (trained untimed on a small grid of the same problem)
+with the FP32 and with the FP64 reconstruction.
 
 With N > 1 (torchrun) every rank advances an independent replica of the grid
 (the path has no cross-GPU exchange in this scope); value is the total over ranks
@@ -28,9 +35,30 @@ sys.path.insert(0, os.path.join(ROOT, "kfvm-kokkos_b200"))
 
 import kfvm_abi as abi  # noqa: E402
 
-METRIC = "zone-updates/s on 1 B200 (3D Euler Sod blast 256^3, plain FP64)"
 UNIT = "zone-updates/s"
-WORKLOAD = "sod3d"
+# workload -> (default cells per axis, dimension, short name, description)
+WORKLOADS = {
+    "sod3d": (256, 3, "3D Euler Sod blast",
+              "3D Euler spherical Sod blast {s}^3, outflow, GP-WENO-AO r=2 + KXRCF, HLLC, SSP(4,3) FSAL "
+              "adaptive, CFL 0.8"),
+    "kelvin_helmholtz": (1024, 2, "2D Euler Kelvin-Helmholtz",
+                         "2D Euler Kelvin-Helmholtz {s}^2 periodic, seeded noise, GP-WENO-AO r=2 + KXRCF, HLLC, "
+                         "SSP(4,3) FSAL adaptive, CFL 0.8"),
+    "taylor_green": (256, 3, "3D Navier-Stokes Taylor-Green",
+                     "3D Navier-Stokes Taylor-Green {s}^3 periodic, Re 1600, Pr 0.71, Mach 0.1, GP-WENO-AO r=2 + "
+                     "KXRCF, HLLC + viscous terms, SSP(4,3) FSAL adaptive, CFL 0.8"),
+    "orszag_tang": (1024, 2, "2D GLM-MHD Orszag-Tang",
+                    "2D GLM-MHD Orszag-Tang {s}^2 periodic, GP-WENO-AO r=2 + KXRCF, HLL, SSP(4,3) FSAL adaptive, "
+                    "CFL 0.4, GLM sources"),
+    "isentropic_vortex": (128, 2, "2D Euler isentropic vortex",
+                          "2D Euler isentropic vortex {s}^2 periodic, GP-WENO-AO r=2 + KXRCF, HLLC, SSP(4,3) FSAL "
+                          "adaptive, CFL 0.8"),
+}
+
+
+def metric_name(workload, scale):
+    _, dim, short, _ = WORKLOADS[workload]
+    return f"zone-updates/s on 1 B200 ({short} {scale}^{dim}, plain FP64)"
 
 
 def parse():
@@ -39,20 +67,25 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--scale", type=int, default=256, help="grid cells per axis")
+    p.add_argument("--workload", default="sod3d", choices=sorted(WORKLOADS))
+    p.add_argument("--scale", type=int, default=None, help="grid cells per axis (default: the workload's)")
     p.add_argument("--e2e-steps", type=int, default=4)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"],
                    help="arithmetic of the linear reconstruction contraction")
-    p.add_argument("--no-forms", action="store_true", help="skip timing the FP32 form")
-    return p.parse_args()
+    p.add_argument("--no-forms", action="store_true", help="skip timing the FP32 and learned forms")
+    a = p.parse_args()
+    if a.scale is None:
+        a.scale = WORKLOADS[a.workload][0]
+    return a
 
 
-def config_block(scale, extra=None):
-    c = {"workload": f"3D Euler spherical Sod blast {scale}^3, outflow, GP-WENO-AO r=2 + KXRCF, "
-                     "HLLC, SSP(4,3) FSAL adaptive, CFL 0.8, FP64",
-         "grid": [scale, scale, scale], "cells": scale ** 3,
-         "l2": "inputs larger than L2 (state + face arrays ~GBs >> 126 MB)"}
+def config_block(workload, scale, extra=None):
+    _, dim, _, desc = WORKLOADS[workload]
+    c = {"workload": desc.format(s=scale) + ", FP64",
+         "grid": [scale] * dim, "cells": scale ** dim,
+         "l2": "inputs larger than L2 (state + face arrays ~GBs >> 126 MB)" if scale ** dim >= 2 ** 20
+         else "small grid: inputs partly L2 resident"}
     if extra:
         c.update(extra)
     return c
@@ -175,13 +208,37 @@ def load_json(path):
 
 
 # ------------------------------------------------------------------ our arm
-def time_form(cfg, ic, prec, steps, warmup):
+def train_indicator(workload, seed=1):
+    """Weights of the learned indicator for a workload: samples of a plain run of
+    the same problem on a small grid (every 6 steps of 24), 800 Adam steps."""
+    import kfvm
+    dim = WORKLOADS[workload][1]
+    cfg, ic = abi.workload(workload, scale=48 if dim == 3 else 256, steps=40)
+    s = kfvm.Solver(cfg)
+    s.init_ic(ic)
+    s.mlp_reserve(600000)
+    n = npos = 0
+    for step in range(25):
+        if step % 6 == 0:
+            n, npos = s.mlp_collect(tau=0.3, keep=0.25, seed=100 + step)
+        s.take_step()
+    s.mlp_init(seed)
+    l0, l1 = s.mlp_train(800, batch=1024, lr=3e-3, pos_weight=4.0, seed=seed)
+    w = s.mlp_weights()
+    s.close()
+    return w, {"train_grid": [cfg.nx] * dim, "samples": n, "troubled": npos, "loss_first": l0, "loss_last": l1}
+
+
+def time_form(cfg, ic, prec, steps, warmup, mlp_weights=None):
     """Zone-updates/s of one arithmetic form: device time of `steps` accepted-step
     attempts after `warmup`, CUDA events on the solver's stream."""
     import torch
     import kfvm
     s = kfvm.Solver(cfg)
     s.set_precision(prec)
+    if mlp_weights is not None:
+        s.mlp_set_weights(mlp_weights)
+        s.set_indicator(abi.KFVM_IND_MLP)
     s.init_ic(ic)
     for _ in range(warmup):
         s.take_step()
@@ -197,10 +254,13 @@ def time_form(cfg, ic, prec, steps, warmup):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     per_class = s.timing()
+    out = {"value": acc * abi.ncells(cfg) / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+           "steps": steps, "accepted_steps": acc,
+           "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0}}
+    if mlp_weights is not None:
+        out["judge"] = s.mlp_stats()
     s.close()
-    return {"value": acc * abi.ncells(cfg) / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
-            "steps": steps, "accepted_steps": acc,
-            "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0}}
+    return out
 
 
 def run_ours(args):
@@ -218,7 +278,7 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     kfvm.lib()  # raises if the CUDA library is missing: no CPU fallback
 
-    cfg, ic = abi.workload(WORKLOAD, scale=args.scale, steps=args.warmup + args.steps + 10)
+    cfg, ic = abi.workload(args.workload, scale=args.scale, steps=args.warmup + args.steps + 10)
     solver = kfvm.Solver(cfg)
     if args.precision == "tf32x3":
         solver.set_precision(abi.KFVM_PREC_TF32X3)
@@ -327,11 +387,11 @@ def run_ours(args):
     share = {k: round(v[0] / max(sum(x[0] for x in per_class.values()), 1e-9), 4)
              for k, v in per_class.items() if v[1] > 0}
 
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+    out = {"metric": metric_name(args.workload, args.scale), "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (analytic initial condition)",
-           "config": config_block(args.scale, {"parallelism": f"replicas x{ws}",
+           "config": config_block(args.workload, args.scale, {"parallelism": f"replicas x{ws}",
                                                "accepted_steps": accepted, "attempts": attempts,
                                                "weno_cells_last": nweno[-1] if nweno else None}),
            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
@@ -341,12 +401,21 @@ def run_ours(args):
 
     solver.close()
     if not args.no_forms:
-        # the FP32 form (3xTF32 tensor-core reconstruction) on the same workload
-        form = time_form(cfg, ic, abi.KFVM_PREC_TF32X3, steps=max(2, args.steps // 2), warmup=2)
+        # the FP32 form (3xTF32 tensor-core reconstruction) and the learned + FP32
+        # form (network trained untimed on a small grid of the same problem)
+        fs = max(2, args.steps // 2)
+        form = time_form(cfg, ic, abi.KFVM_PREC_TF32X3, steps=fs, warmup=2)
         form["vs_plain"] = form["value"] / value
-        out["forms"] = {"fp32_3xtf32": form}
+        w, info = train_indicator(args.workload)
+        lf = time_form(cfg, ic, abi.KFVM_PREC_TF32X3, steps=fs, warmup=2, mlp_weights=w)
+        lf["vs_plain"] = lf["value"] / value
+        lf["training"] = info
+        lf64 = time_form(cfg, ic, abi.KFVM_PREC_FP64, steps=fs, warmup=2, mlp_weights=w)
+        lf64["vs_plain"] = lf64["value"] / value
+        out["forms"] = {"fp32_3xtf32": form, "learned_fp32": lf, "learned_fp64": lf64}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(sample_scale=64, sample_steps=1)
+        out["cpu_baseline"] = cpu_baseline(args.workload, sample_scale=cpu_sample_scale(args.workload),
+                                           sample_steps=1)
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -363,13 +432,18 @@ def _oracle():
     return oracle
 
 
-def cpu_baseline(sample_scale, sample_steps, warmup=0):
+def cpu_sample_scale(workload):
+    """Grid of the bounded CPU sample (about 10-30 s of host work)."""
+    return 64 if WORKLOADS[workload][1] == 3 else 512
+
+
+def cpu_baseline(workload, sample_scale, sample_steps, warmup=0):
     """The oracle (CPU restatement of the reference path, OpenMP over cells) timed
     on the host cores on a bounded sample of the workload."""
     oracle = _oracle()
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
-    cfg, ic = abi.workload(WORKLOAD, scale=sample_scale, steps=sample_steps + warmup + 2)
+    cfg, ic = abi.workload(workload, scale=sample_scale, steps=sample_steps + warmup + 2)
     s = oracle.OracleSolver(cfg)
     s.init_ic(ic)
     for _ in range(warmup):
@@ -381,7 +455,7 @@ def cpu_baseline(sample_scale, sample_steps, warmup=0):
     dt = time.perf_counter() - t0
     n = abi.ncells(cfg)
     return {"value": acc * n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{sample_steps} accepted step(s) of the same problem on a {sample_scale}^3 grid "
+            "sample": f"{sample_steps} accepted step(s) of the same problem on a {sample_scale}^{cfg.dim} grid "
                       f"({acc * n} zone-updates in {dt:.1f} s)"}
 
 
@@ -392,8 +466,8 @@ def run_reference(args):
     oracle = _oracle()
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
-    sample = 48
-    cfg, ic = abi.workload(WORKLOAD, scale=sample, steps=args.warmup + args.steps + 2)
+    sample = 48 if WORKLOADS[args.workload][1] == 3 else 192
+    cfg, ic = abi.workload(args.workload, scale=sample, steps=args.warmup + args.steps + 2)
     s = oracle.OracleSolver(cfg)
     s.init_ic(ic)
     for _ in range(args.warmup):
@@ -405,13 +479,13 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     n = abi.ncells(cfg)
     value = acc * n / dt
-    desc = (f"each step: one accepted time step of the same problem on a {sample}^3 grid "
+    desc = (f"each step: one accepted time step of the same problem on a {sample}^{cfg.dim} grid "
             f"(the reference build is unavailable here; this is the CPU restatement of its path)")
-    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+    out = {"impl": "reference", "metric": metric_name(args.workload, args.scale), "value": value, "unit": UNIT, "n_gpus": ws,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (analytic initial condition)",
-           "config": config_block(args.scale, {"sample_grid": [sample] * 3}),
+           "config": config_block(args.workload, args.scale, {"sample_grid": [sample] * cfg.dim}),
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                             "sample": desc},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
