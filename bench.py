@@ -210,17 +210,18 @@ def load_json(path):
 # ------------------------------------------------------------------ our arm
 def train_indicator(workload, seed=1):
     """Weights of the learned indicator for a workload: samples of a plain run of
-    the same problem on a small grid (every 6 steps of 24), 800 Adam steps."""
+    the same problem (3D on a 128^3 grid), every 6 steps of 24, all troubled
+    cells and 5 % of the others; 800 Adam steps."""
     import kfvm
     dim = WORKLOADS[workload][1]
-    cfg, ic = abi.workload(workload, scale=48 if dim == 3 else 256, steps=40)
+    cfg, ic = abi.workload(workload, scale=128 if dim == 3 else WORKLOADS[workload][0], steps=40)
     s = kfvm.Solver(cfg)
     s.init_ic(ic)
-    s.mlp_reserve(600000)
+    s.mlp_reserve(1500000)
     n = npos = 0
     for step in range(25):
         if step % 6 == 0:
-            n, npos = s.mlp_collect(tau=0.3, keep=0.25, seed=100 + step)
+            n, npos = s.mlp_collect(tau=0.3, keep=0.05, seed=100 + step)
         s.take_step()
     s.mlp_init(seed)
     l0, l1 = s.mlp_train(800, batch=1024, lr=3e-3, pos_weight=4.0, seed=seed)

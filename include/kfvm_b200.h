@@ -234,7 +234,7 @@ int kfvm_set_precision(kfvm_solver *s, int32_t precision);
  * No reference counterpart: it replaces the KXRCF selector (WenoSelect_K,
  * src/numeric/Numeric_K.H:292-398) with a 2x32 MLP over the normalised 5^d
  * density / pressure patch of a cell: inputs x = (q_k - q_c) / (max|q_k - q_c| +
- * 1e-6 |q_c|), q = rho then p, 50 (2D) or 250 (3D); NI -> 32 -> 32 -> 1 with GELU
+ * 1e-4 |q_c|), q = rho then p, 50 (2D) or 250 (3D); NI -> 32 -> 32 -> 1 with GELU
  * and a sigmoid; BF16 weights, FP32 accumulation.  Weight layout (raw BF16):
  * W1[32][NI], b1[32], W2[32][32], b2[32], w3[32], b3.
  * Labels come from the method: a cell is troubled when the normalised WENO-JS
@@ -265,7 +265,7 @@ int kfvm_mlp_get_samples(kfvm_solver *s, int64_t first, int64_t count, uint16_t 
  * first and of the last 20 steps */
 int kfvm_mlp_train(kfvm_solver *s, int32_t steps, int32_t batch, double lr, double pos_weight, uint64_t seed,
                    double *loss_first, double *loss_last);
-/* decision threshold on the probability (default 0.5), judge fraction (1/64),
+/* decision threshold on the probability (default 0.5), judge fraction (1/256),
  * label threshold tau (0.3), allowed miss rate of the judge (0.25) */
 int kfvm_mlp_config(kfvm_solver *s, double prob_threshold, double judge_frac, double tau, double miss_limit);
 /* network probability of every cell for the current state ([nz][ny][nx]);

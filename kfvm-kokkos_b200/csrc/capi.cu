@@ -170,7 +170,7 @@ struct kfvm_solver {
     int64_t *cells = nullptr;
     unsigned long long *count = nullptr;
     int64_t cap = 0, nPos = 0;
-    double logitThr = 0.0, judgeFrac = 1.0 / 64.0, tau = 0.3, missLimit = 0.25;
+    double logitThr = 0.0, judgeFrac = 1.0 / 256.0, tau = 0.3, missLimit = 0.25;
     int fallbackSteps = 0;
     int64_t fallbackEvents = 0;
     unsigned long long lastPos = 0, lastMissed = 0;

@@ -86,6 +86,10 @@ struct DevScalars {
 // heavy-list entries carry the cell index in the low 30 bits
 constexpr uint32_t kHeavyCellMax = 0x3fffffffu;
 
+// variations below this fraction of a cell's density / pressure count as smooth for
+// the learned indicator (labels and the normalisation of its features)
+constexpr double kMlpFloor = 1e-4;
+
 // the learned indicator's judge: a hashed fraction of the cells runs full WENO
 // and has its label compared with the network's prediction
 struct JudgeArgs {
@@ -202,8 +206,8 @@ __device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
 #pragma unroll
     for (int v = 0; v < NV; v++) lin[v] = ref[v];
     vc.cons2LinPrim(lin);
-    sig[0] = sqrt(om[0][DENS]) > 1e-6 * fabs(lin[DENS]);
-    sig[1] = sqrt(om[0][ETOT]) > 1e-6 * fabs(lin[ETOT]);
+    sig[0] = sqrt(om[0][DENS]) > kMlpFloor * fabs(lin[DENS]);
+    sig[1] = sqrt(om[0][ETOT]) > kMlpFloor * fabs(lin[ETOT]);
   }
   // nonlinear weights, WENO-JS then AO form (createOmegas, Stencil_K.H:556-580)
   constexpr double gHi = 0.7, gLo = 0.7;
@@ -270,8 +274,9 @@ __device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
 // normalised WENO-JS weights (createOmegas, Stencil_K.H:556-580, before the
 // adaptive-order transform) from the linear weights gamma_s, over the substencils
 // and over density and pressure (linearised primitives 0 and 4) where their
-// variation over the stencil exceeds 1e-6 of the cell value (below that all
-// smoothness indicators are rounding noise and the weights are arbitrary).  The
+// variation over the stencil exceeds kMlpFloor = 1e-4 of the cell value (below
+// that the weights of noise-level variations are arbitrary, and the linear
+// reconstruction of such variations is harmless).  The
 // smoothness indicators are those of weno_cell (findSmoothness, 506-554).
 template <int DIM, int EQ>
 __device__ double weno_departure(const double *__restrict__ Uc, const Grid &g,
@@ -323,7 +328,7 @@ __device__ double weno_departure(const double *__restrict__ Uc, const Grid &g,
 #pragma unroll
   for (int a = 0; a < 2; a++) {
     const double r = a == 0 ? lin[DENS] : lin[ETOT];
-    if (!(sqrt(om[0][a]) > 1e-6 * fabs(r))) continue;
+    if (!(sqrt(om[0][a]) > kMlpFloor * fabs(r))) continue;
     double tot = 0.0;
 #pragma unroll
     for (int s = 0; s < T::NSUB; s++) {

@@ -2,7 +2,7 @@
 // per-block density / pressure tile its features are read from.
 //
 // Input: the normalised (2r+1)^d patch (r = 2) of density and pressure around a
-// cell, x = (q_k - q_c) / (max_k |q_k - q_c| + 1e-6 |q_c|) for q = rho, p, giving
+// cell, x = (q_k - q_c) / (max_k |q_k - q_c| + 1e-4 |q_c|) for q = rho, p, giving
 // 50 inputs in 2D and 250 in 3D (density first, patch cells in (z, y, x) order,
 // x fastest).  Network: NI -> 32 -> 32 -> 1, GELU after both hidden layers,
 // sigmoid output.  Weights are BF16 (raw uint16 at the C ABI), every sum
@@ -80,8 +80,8 @@ __device__ __forceinline__ void mlp_scales(const double (*t)[MlpTile<DIM>::N], i
         mr = fmax(mr, fabs(t[0][n] - rc));
         mp = fmax(mp, fabs(t[1][n] - pc));
       }
-  sr = 1.0 / (mr + 1e-6 * fabs(rc) + 1e-300);
-  sp = 1.0 / (mp + 1e-6 * fabs(pc) + 1e-300);
+  sr = 1.0 / (mr + kMlpFloor * fabs(rc) + 1e-300);
+  sp = 1.0 / (mp + kMlpFloor * fabs(pc) + 1e-300);
 }
 
 } // namespace kfvm

@@ -18,16 +18,19 @@
 // u(cell) + D in FP64; positivity checks, the indicator and everything after the
 // reconstruction stay FP64.
 //
-// Per block (128 threads, one cell per thread = one row of the tile):
+// Per block (256 threads, two per cell = per row of the tile, 128 cells):
 //   warp 0 allocates the TMEM columns (variables x N, rounded to a power of two)
-//   the split weights (B, hi and lo) are copied to shared memory once
-//   per variable: every thread writes its A row (hi and lo) into shared memory in
-//     the canonical K-major no-swizzle layout (8-row x 16-byte core matrices),
-//     thread 0 issues 3 MMAs per K step of 8 into the variable's TMEM columns and
-//     commits them to an mbarrier; the next variable waits for that mbarrier
-//     before it overwrites the A buffer
-//   epilogue: each warp reads its 32 lanes (tcgen05.ld 32x32b), adds the cell
-//     average in FP64 and writes face states, indicators, status
+//   the split weights (B, hi and lo) and the limiter footprint tile are loaded,
+//     and the limiter bounds of each cell are computed once
+//   per variable: the two threads of a row write its A row (hi and lo, half of
+//     the K chunks each) into shared memory in the canonical K-major no-swizzle
+//     layout (8-row x 16-byte core matrices); thread 0 issues 3 MMAs per K step
+//     of 8 into the variable's TMEM columns and commits them to an mbarrier; the
+//     next variable waits for that mbarrier before it overwrites the A buffer
+//   epilogue: each warp reads its 32 lanes (tcgen05.ld 32x32b), the two threads
+//     of a row take half of its face / interior points each, add the cell
+//     average in FP64 and write face states and indicators; the in-bounds test
+//     and the GLM speeds of a cell are combined in shared memory
 // Every mbarrier wait is bounded (iteration count and a 1 s global-timer limit);
 // on timeout the block records DevScalars::fault, frees its TMEM and returns.
 // Shared memory per block is sized so that at most 512 / columns blocks are
@@ -43,6 +46,11 @@
 
 namespace kfvm {
 
+// Two threads per tile row (cell): threads 0..127 are part 0, 128..255 part 1;
+// warp w reads TMEM lanes 32 (w % 4) .. +31, so both parts reach every row.
+constexpr int kTcParts = 2;
+constexpr int kTcThreads = 128 * kTcParts;
+
 template <int DIM, int EQ>
 struct TcShape {
   using T = Cfg<DIM, EQ>;
@@ -51,6 +59,8 @@ struct TcShape {
   static constexpr int KP = DIM == 2 ? 16 : 40;       // stencil cells padded to K steps of 8
   static constexpr int NKS = KP / 8;
   static constexpr int NCH = KP / 4;                  // 16-byte core-matrix columns along K
+  // epilogue rows per part, even (TMEM loads of column pairs)
+  static constexpr int RPP = (((NR + kTcParts - 1) / kTcParts) + 1) / 2 * 2;
   static constexpr int COLS_USED = T::NV * NP;
   static constexpr int COLS = COLS_USED <= 128 ? 128 : (COLS_USED <= 256 ? 256 : 512);
   static constexpr int MAX_RES = 512 / COLS;          // blocks per SM that fit in TMEM
@@ -60,17 +70,20 @@ struct TcShape {
   static constexpr int B_PART = NCH * B_CH;
   static constexpr int OFF_B = 2 * A_PART;
   static constexpr int OFF_TILE = OFF_B + 2 * B_PART;
-  static constexpr int OFF_BAR = OFF_TILE + 6 * PosTile<DIM>::N * (int)sizeof(double);
+  static constexpr int OFF_BD = OFF_TILE + 6 * PosTile<DIM>::N * (int)sizeof(double); // bounds [3][128]
+  static constexpr int OFF_RED = OFF_BD + 3 * 128 * (int)sizeof(double);              // lam, vel [2][128], in-bounds [128]
+  static constexpr int OFF_BAR = OFF_RED + 2 * 128 * 8 + 128 * 4;
   static constexpr int USED = OFF_BAR + 16;
   // 228 KB of shared memory per SM: MAX_RES + 1 blocks of FLOOR bytes do not fit
   static constexpr int FLOOR = 233472 / (MAX_RES + 1) + 256;
   static constexpr int SMEM = USED > FLOOR ? USED : FLOOR;
   static_assert(NR <= NP, "weight rows exceed the MMA N");
+  static_assert(kTcParts * RPP <= NP, "epilogue rows beyond the MMA N");
   static_assert(T::C <= KP, "stencil exceeds the MMA K");
   static_assert(KP <= kTcMaxK && NP <= kTcMaxN, "B table too small");
   static_assert(SMEM <= 227 * 1024, "shared memory per block");
-  static_assert(kBlockX * kBlockY == 128, "one tile row per thread");
-  static_assert(OFF_BAR % 8 == 0, "mbarrier alignment");
+  static_assert(kBlockX * kBlockY == 128, "one tile row per cell");
+  static_assert(OFF_BAR % 8 == 0 && OFF_BD % 8 == 0, "alignment");
 };
 
 // ---------------------------------------------------------------------------
@@ -144,6 +157,20 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
+// 2 consecutive TMEM columns (an even column) of this warp's 32 lanes, waited for
+// in the same asm statement
+__device__ __forceinline__ void tmem_ld2(uint32_t taddr, float &r0, float &r1) {
+  uint32_t x0, x1;
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];\n\t"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(x0), "=r"(x1)
+      : "r"(taddr)
+      : "memory");
+  r0 = __uint_as_float(x0);
+  r1 = __uint_as_float(x1);
+}
+
 // 8 consecutive TMEM columns of this warp's 32 lanes, waited for in the same asm
 // statement so no use of the registers can move above the wait
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&r)[8]) {
@@ -166,7 +193,7 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&r)[8]) {
 
 // ---------------------------------------------------------------------------
 template <int DIM, int EQ>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kTcThreads, 2)
     recon_tc_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
                     double *__restrict__ F0, double *__restrict__ F1, double *__restrict__ F2,
                     float *__restrict__ W0, float *__restrict__ W1, float *__restrict__ W2,
@@ -177,12 +204,18 @@ __global__ void __launch_bounds__(128)
   constexpr int NV = T::NV;
   extern __shared__ __align__(128) uint8_t smem[];
   double(*tile)[PosTile<DIM>::N] = reinterpret_cast<double(*)[PosTile<DIM>::N]>(smem + Sh::OFF_TILE);
+  double(*sBd)[128] = reinterpret_cast<double(*)[128]>(smem + Sh::OFF_BD);
+  unsigned long long *sLam = reinterpret_cast<unsigned long long *>(smem + Sh::OFF_RED);
+  unsigned long long *sVel = sLam + 128;
+  int *sIn = reinterpret_cast<int *>(smem + Sh::OFF_RED + 2 * 128 * 8);
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::OFF_BAR);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + Sh::OFF_BAR + 8);
-  const int warp = threadIdx.y;
-  const int row = warp * 32 + threadIdx.x; // tile row = TMEM lane
-  const int64_t i = blockIdx.x * (int64_t)kBlockX + threadIdx.x;
-  const int64_t j = blockIdx.y * (int64_t)kBlockY + threadIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quarter = warp & 3, part = warp >> 2;
+  const int row = quarter * 32 + lane;     // tile row = TMEM lane = cell (lane, quarter) of the block
+  const int tid = threadIdx.x;
+  const int64_t i = blockIdx.x * (int64_t)kBlockX + lane;
+  const int64_t j = blockIdx.y * (int64_t)kBlockY + quarter;
   const int64_t k = blockIdx.z;
   const bool live = i < g.nx && j < g.ny;
   const uint32_t barA = smem_u32(bar);
@@ -193,7 +226,7 @@ __global__ void __launch_bounds__(128)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (row == 0) {
+  if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barA) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -203,22 +236,49 @@ __global__ void __launch_bounds__(128)
     const float4 *bl = reinterpret_cast<const float4 *>(S->tcw[1]);
     float4 *dh = reinterpret_cast<float4 *>(smem + Sh::OFF_B);
     float4 *dl = reinterpret_cast<float4 *>(smem + Sh::OFF_B + Sh::B_PART);
-    for (int t = row; t < Sh::B_PART / 16; t += 128) {
+    for (int t = tid; t < Sh::B_PART / 16; t += kTcThreads) {
       dh[t] = bh[t];
       dl[t] = bl[t];
     }
   }
-  pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)kBlockX, blockIdx.y * (int64_t)kBlockY, k, tile);
+  {
+    // the footprint tile, filled by all threads (pos_tile_fill strides by blockDim)
+    using P = PosTile<DIM>;
+    const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY;
+    for (int t = tid; t < P::N; t += kTcThreads) {
+      const int a = t % P::TX, b = (t / P::TX) % P::TY, cz = t / (P::TX * P::TY);
+      const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b, gk = k - (DIM == 3 ? 1 : 0) + cz;
+      if (gi > g.nx || gj > g.ny) continue;
+      const double *Uq = U + pidx(g, gi, gj, gk);
+      double st[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) st[v] = Uq[v * g.pvol];
+      tile[0][t] = st[DENS];
+      tile[1][t] = Eos<EQ>::eint(st);
+      tile[2][t] = Eos<EQ>::soundspeed(g.gamma, st);
+      tile[3][t] = st[MOMX] / st[DENS];
+      tile[4][t] = st[MOMY] / st[DENS];
+      tile[5][t] = st[MOMZ] / st[DENS];
+    }
+  }
+  if (part == 0) {
+    sIn[row] = 1;
+    sLam[row] = 0ull;
+    sVel[row] = 0ull;
+  }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
+  if (part == 0 && live) {
+    const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, lane, quarter);
+    sBd[0][row] = bd.minDens;
+    sBd[1][row] = bd.maxDens;
+    sBd[2][row] = bd.minEint;
+  }
 
   const double *Uc = U + pidx(g, live ? i : 0, live ? j : 0, k);
-  double uc[NV];
-#pragma unroll
-  for (int v = 0; v < NV; v++) uc[v] = live ? Uc[v * g.pvol] : 0.0;
   const uint32_t aHi = smem_u32(smem), aLo = aHi + Sh::A_PART;
   const uint32_t bHi = smem_u32(smem + Sh::OFF_B), bLo = bHi + Sh::B_PART;
   constexpr uint32_t idesc = tf32_idesc<Sh::NP>();
@@ -228,11 +288,11 @@ __global__ void __launch_bounds__(128)
   for (int v = 0; v < NV; v++) {
     if (v > 0) ok = mbar_wait(barA, (uint32_t)(v - 1) & 1u);
     if (!__syncthreads_and(ok)) break;
-    // this thread's A row for variable v: stencil differences split into hi / lo
+    // this thread's share of the A row for variable v: chunks part, part + 2, ...
     const double *Uv = Uc + v * g.pvol;
     const double ucv = live ? Uv[0] : 0.0;
 #pragma unroll
-    for (int ch = 0; ch < Sh::NCH; ch++) {
+    for (int ch = part; ch < Sh::NCH; ch += kTcParts) {
       uint32_t hi[4], lo[4];
 #pragma unroll
       for (int t = 0; t < 4; t++) {
@@ -247,7 +307,7 @@ __global__ void __launch_bounds__(128)
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (row == 0) {
+    if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t d = tmem + (uint32_t)(v * Sh::NP);
 #pragma unroll
@@ -266,55 +326,73 @@ __global__ void __launch_bounds__(128)
   if (ok) ok = mbar_wait(barA, (uint32_t)(NV - 1) & 1u);
   if (__syncthreads_and(ok)) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    PosBounds bd{};
-    if (live) bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
-    const uint32_t lane = (uint32_t)(warp * 32) << 16;
+    PosBounds bd;
+    bd.minDens = sBd[0][row];
+    bd.maxDens = sBd[1][row];
+    bd.minEint = sBd[2][row];
+    double uc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) uc[v] = live ? Uc[v * g.pvol] : 0.0;
+    const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
     double *F[3] = {F0, F1, F2};
     float *W[3] = {W0, W1, W2};
     const int64_t c = (k * g.ny + j) * g.nx + i;
     bool inside = true;
     double lam = 0.0, vel = 0.0;
+    const int r0 = part * Sh::RPP;
 #pragma unroll
-    for (int grp = 0; grp < (Sh::NR + 7) / 8; grp++) {
-      float r[NV][8];
+    for (int rp = 0; rp < Sh::RPP; rp += 2) {
+      float a0[NV], a1[NV];
 #pragma unroll
-      for (int v = 0; v < NV; v++) tmem_ld8(tmem + lane + (uint32_t)(v * Sh::NP + grp * 8), r[v]);
+      for (int v = 0; v < NV; v++) tmem_ld2(tmem + lanes + (uint32_t)(v * Sh::NP + r0 + rp), a0[v], a1[v]);
       if (live) {
 #pragma unroll
-        for (int p = 0; p < 8; p++) {
-          const int rw = grp * 8 + p;
-          if (rw >= Sh::NR) break;
-          double st[NV];
+        for (int e = 0; e < 2; e++) {
+          const int rw = r0 + rp + e;
+          if (rw < Sh::NR) {
+            double st[NV];
 #pragma unroll
-          for (int v = 0; v < NV; v++) st[v] = uc[v] + (double)r[v][p];
-          inside = inside && pos_inside<EQ>(bd, st);
-          if (rw < T::NF * T::NQF) {
-            const int f = rw / T::NQF, q = rw % T::NQF;
-            const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
-            const int64_t nf = g.nface[f >> 1];
+            for (int v = 0; v < NV; v++) st[v] = uc[v] + (double)(e ? a1[v] : a0[v]);
+            inside = inside && pos_inside<EQ>(bd, st);
+            if (rw < T::NF * T::NQF) {
+              const int f = rw / T::NQF, q = rw % T::NQF;
+              const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
+              const int64_t nf = g.nface[f >> 1];
 #pragma unroll
-            for (int v = 0; v < NV; v++) F[f >> 1][a + v * nf] = st[v];
-            if (wantInd) W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno_approx(g.gamma, st);
-            if constexpr (T::SRC) {
-              // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
-              const double vv = fabs(st[MOMX] / st[DENS]);
-              const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
-              vel = vv > vel ? vv : vel;
-              lam = l > lam ? l : lam;
+              for (int v = 0; v < NV; v++) F[f >> 1][a + v * nf] = st[v];
+              if (wantInd)
+                W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno_approx(g.gamma, st);
+              if constexpr (T::SRC) {
+                // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
+                const double vv = fabs(st[MOMX] / st[DENS]);
+                const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
+                vel = vv > vel ? vv : vel;
+                lam = l > lam ? l : lam;
+              }
+            } else if constexpr (T::SRC) {
+              const int q = rw - T::NF * T::NQF;
+#pragma unroll
+              for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
             }
-          } else if constexpr (T::SRC) {
-            const int q = rw - T::NF * T::NQF;
-#pragma unroll
-            for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
           }
         }
       }
     }
-    if (live) {
-      if constexpr (T::SRC) lamvel[c] = make_double2(lam, vel);
-      status[c] = inside ? 1 : 0;
+    // combine the two parts of each cell
+    if (live && !inside) atomicAnd(&sIn[row], 0);
+    if constexpr (T::SRC) {
+      if (live) {
+        if (lam >= 0.0) atomicMax(&sLam[row], (unsigned long long)__double_as_longlong(lam));
+        if (vel >= 0.0) atomicMax(&sVel[row], (unsigned long long)__double_as_longlong(vel));
+      }
     }
-  } else if (row == 0) {
+    __syncthreads();
+    if (live && part == 0) {
+      if constexpr (T::SRC)
+        lamvel[c] = make_double2(__longlong_as_double((long long)sLam[row]), __longlong_as_double((long long)sVel[row]));
+      status[c] = sIn[row] ? 1 : 0;
+    }
+  } else if (tid == 0) {
     atomicExch(&sc->fault, 1u);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -338,7 +416,7 @@ static cudaError_t recon_tc_launch(const double *U, const Grid &g, const DevSten
   }
   const dim3 grid((unsigned)((g.nx + kBlockX - 1) / kBlockX), (unsigned)((g.ny + kBlockY - 1) / kBlockY),
                   (unsigned)g.nz);
-  recon_tc_kernel<DIM, EQ><<<grid, dim3(kBlockX, kBlockY), Sh::SMEM, s>>>(
+  recon_tc_kernel<DIM, EQ><<<grid, kTcThreads, Sh::SMEM, s>>>(
       U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, sc);
   return cudaGetLastError();
 }

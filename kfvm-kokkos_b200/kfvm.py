@@ -204,7 +204,7 @@ class Solver:
                                     C.byref(a), C.byref(b)), "kfvm_mlp_train")
         return a.value, b.value
 
-    def mlp_config(self, prob_threshold=0.5, judge_frac=1.0 / 64, tau=0.3, miss_limit=0.25):
+    def mlp_config(self, prob_threshold=0.5, judge_frac=1.0 / 256, tau=0.3, miss_limit=0.25):
         _check(lib().kfvm_mlp_config(self.h, float(prob_threshold), float(judge_frac), float(tau),
                                      float(miss_limit)), "kfvm_mlp_config")
 

@@ -793,8 +793,8 @@ double weno_departure(orc_solver &S, const std::vector<double> &B, int64_t i, in
     smooth(2 + nB, Vb, Cb);
   }
   // density and pressure (linearised primitives 0 and 4), where their variation
-  // over the full stencil is above rounding level (1e-6 of the cell value): there
-  // all substencil indicators vanish and the normalised weights are arbitrary
+  // over the full stencil is above 1e-4 of the cell value: below that the weights
+  // of noise-level variations are arbitrary and their linear reconstruction harmless
   double dep = 0.0;
   const int vs[2] = {0, 4};
   double lin[9];
@@ -803,7 +803,7 @@ double weno_departure(orc_solver &S, const std::vector<double> &B, int64_t i, in
   const double ref[2] = {lin[0], lin[4]};
   for (int a = 0; a < 2; a++) {
     const int v = vs[a];
-    if (!(std::sqrt(omega[0][v]) > 1e-6 * std::fabs(ref[a]))) continue;
+    if (!(std::sqrt(omega[0][v]) > 1e-4 * std::fabs(ref[a]))) continue;
     double tot = 0.0;
     for (int s = 0; s < nSub; s++) {
       omega[s][v] = gamma[s] / (omega[s][v] * omega[s][v] + 1.e-40);

@@ -62,8 +62,8 @@ def features(state, cfg, cells):
         pr, pq = rp[sl].ravel(), pp[sl].ravel()
         rc, pc = rho[k, j, i], p[k, j, i]
         dr, dq = pr - rc, pq - pc
-        sr = 1.0 / (np.abs(dr).max() + 1e-6 * abs(rc) + 1e-300)
-        sq = 1.0 / (np.abs(dq).max() + 1e-6 * abs(pc) + 1e-300)
+        sr = 1.0 / (np.abs(dr).max() + 1e-4 * abs(rc) + 1e-300)
+        sq = 1.0 / (np.abs(dq).max() + 1e-4 * abs(pc) + 1e-300)
         out[n] = np.concatenate([(dr * sr).astype(np.float32), (dq * sq).astype(np.float32)])
     return out.astype(np.float32)
 

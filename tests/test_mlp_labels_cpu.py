@@ -47,5 +47,7 @@ def test_bf16_helpers_and_features():
     u[4] = 2.5
     f = mlp_ref.features(u, cfg, [3 * 8 + 4])[0]
     fr = f[:25].reshape(5, 5)
-    assert np.allclose(fr[2], [-1.0, -0.5, 0.0, 0.5, 1.0], atol=1e-3)
+    # max |drho| = 0.02 at rho_c = 1.04: scale 1 / (0.02 + 1e-4 * 1.04)
+    s = 0.02 / (0.02 + 1e-4 * 1.04)
+    assert np.allclose(fr[2], s * np.array([-1.0, -0.5, 0.0, 0.5, 1.0]), atol=1e-6)
     assert np.allclose(f[25:], 0.0, atol=1e-6)
