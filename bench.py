@@ -91,6 +91,20 @@ def config_block(workload, scale, extra=None):
     return c
 
 
+def replica_totals(elapsed, work, world_size, device):
+    """Replicas only: every rank advances its own copy of the grid, so the job's
+    time is the slowest rank's and its work the sum over ranks."""
+    if world_size <= 1:
+        return elapsed, work
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(elapsed)], device=device, dtype=torch.float64)
+    w = torch.tensor([float(work)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return t.item(), w.item()
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -286,8 +300,9 @@ def run_ours(args):
     solver.init_ic(ic)
     n = abi.ncells(cfg)
     nv = abi.nvars(cfg)
+    rhs0 = 1  # the FSAL priming evaluation
     for _ in range(args.warmup):
-        solver.take_step()
+        rhs0 = solver.take_step().n_rhs
 
     stream = torch.cuda.ExternalStream(solver.stream_handle())
     solver.set_timing(True)
@@ -307,6 +322,7 @@ def run_ours(args):
         accepted += info.accepted
         attempts += info.attempts
         nweno.append(info.n_weno)
+    n_rhs = info.n_rhs - rhs0 if args.steps else 0
     e1.record(stream)
     torch.cuda.synchronize()
     if ws > 1:
@@ -318,14 +334,7 @@ def run_ours(args):
     solver.set_timing(False)
 
     # max over ranks of the device time, sum of the work
-    t_max, work = ms, accepted * n
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        w = torch.tensor([float(work)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(w, op=dist.ReduceOp.SUM)
-        t_max, work = t.item(), w.item()
+    t_max, work = replica_totals(ms, accepted * n, ws, "cuda")
     value = work / (t_max / 1e3)
 
     # end to end through the public API with host buffers: per step upload the
@@ -345,14 +354,7 @@ def run_ours(args):
         solver.get_state(host)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_work = e2e_acc * n
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        w = torch.tensor([float(e2e_work)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(w, op=dist.ReduceOp.SUM)
-        e2e_s, e2e_work = t.item(), w.item()
+    e2e_s, e2e_work = replica_totals(e2e_s, e2e_acc * n, ws, "cuda")
     e2e = {"value": e2e_work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(nv * n * 8),
            "d2h_bytes_per_step": int(nv * n * 8),
            "how": "per step: kfvm_set_state from pinned host (re-primes FSAL), kfvm_take_step, "
@@ -385,6 +387,23 @@ def run_ours(args):
         roofline["fp64_pipe"] = {"achieved": fp64, "peak": fp64_peak, "unit": "TFLOP/s",
                                  "frac": fp64 / fp64_peak, "fma_per_launch": fma,
                                  "peak_source": "nominal (148 SMs x 64 FP64 FMA/clk x max SM clock; the DMMA rate measured by ncu is the same)"}
+    # the whole path: attainable zone-updates/s = min(HBM / B_zu, FP64 / F_zu)
+    # B_zu: per stage U, Uprev, Utmp, Uhat in and U', Utmp, Uhat out (7 NV reals),
+    #       plus the error pass (2 NV reals); F_zu: per RHS evaluation and cell the
+    #       linear contraction (2 rows C NV), d NQF Riemann solves at ~200 flops and
+    #       ~300 flops of divergence / update, 4 evaluations per step (WENO cells extra)
+    d_, nv_, nqf_, nqc_, ncst_, src_ = _shape(cfg)
+    rows_ = 2 * d_ * nqf_ + (nqc_ if src_ else 0)
+    b_zu = 4 * 7 * nv_ * 8 + 2 * nv_ * 8
+    f_zu = 4 * (2 * rows_ * ncst_ * nv_ + d_ * nqf_ * 200 + 300)
+    sm_max_ = (peaks or {}).get("sm_max_mhz", 1965.0)
+    fp64_peak_ = 148 * 64 * 2 * sm_max_ * 1e6
+    att_hbm, att_fp64 = hbm_peak * 1e9 / b_zu, fp64_peak_ / f_zu
+    path_roofline = {"bytes_per_zone_update": b_zu, "flops_per_zone_update": f_zu,
+                     "attainable_hbm": att_hbm, "attainable_fp64": att_fp64,
+                     "binding": "fp64" if att_fp64 < att_hbm else "hbm",
+                     "frac_hbm": value / att_hbm, "frac_fp64": value / att_fp64,
+                     "frac_binding": value / min(att_hbm, att_fp64), "unit": UNIT}
     share = {k: round(v[0] / max(sum(x[0] for x in per_class.values()), 1e-9), 4)
              for k, v in per_class.items() if v[1] > 0}
 
@@ -395,7 +414,8 @@ def run_ours(args):
            "config": config_block(args.workload, args.scale, {"parallelism": f"replicas x{ws}",
                                                "accepted_steps": accepted, "attempts": attempts,
                                                "weno_cells_last": nweno[-1] if nweno else None}),
-           "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+           "rhs_evals": int(n_rhs), "rhs_cell_rate": n_rhs * n / (t_max / 1e3) if n_rhs else None,
+           "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "path_roofline": path_roofline,
            "kernel_share": share,
            "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0}}
     out["clocks"] = sampler.summary()
@@ -433,6 +453,17 @@ def _oracle():
     return oracle
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_sample_scale(workload):
     """Grid of the bounded CPU sample (about 10-30 s of host work)."""
     return 64 if WORKLOADS[workload][1] == 3 else 512
@@ -455,7 +486,7 @@ def cpu_baseline(workload, sample_scale, sample_steps, warmup=0):
         acc += s.take_step().accepted
     dt = time.perf_counter() - t0
     n = abi.ncells(cfg)
-    return {"value": acc * n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+    return {"value": acc * n / dt, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": "port",
             "sample": f"{sample_steps} accepted step(s) of the same problem on a {sample_scale}^{cfg.dim} grid "
                       f"({acc * n} zone-updates in {dt:.1f} s)"}
 
@@ -487,7 +518,7 @@ def run_reference(args):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (analytic initial condition)",
            "config": config_block(args.workload, args.scale, {"sample_grid": [sample] * cfg.dim}),
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": "port",
                             "sample": desc},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
