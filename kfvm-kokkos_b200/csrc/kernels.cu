@@ -188,7 +188,9 @@ __global__ void __launch_bounds__(128)
             double st[NV];
 #pragma unroll
             for (int v = 0; v < NV; v++) st[v] = acc[v][t][e];
-            inside = inside && pos_inside<EQ>(bd, st);
+            // pos_inside, with the internal energy kept for the indicator's pressure
+            const double ei = Eos<EQ>::eint(st);
+            inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
             if (rw < T::NF * T::NQF) {
               const int q = DIM == 3 ? 2 * (lane & 1) + e : e;
               double *Fd = DIM == 3 ? F[t < 3 ? t : 0] : F[d];
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(128)
               for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
               if (wantInd)
                 (DIM == 3 ? W[t < 3 ? t : 0] : W[d])[(int64_t)(slot * T::NQF + q) * nf + fidx] =
-                    Eos<EQ>::weno_approx(g.gamma, st);
+                    Eos<EQ>::weno_approx_rp(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
               if constexpr (T::SRC) {
                 // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
                 const double vv = fabs(st[MOMX] / st[DENS]);
@@ -401,78 +403,288 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// heavy pass over the listed cells: WENO-AO reconstruction (KernelWenoRecon_K) or the
-// linear states already written, then the full positivity procedure
+// ---------------------------------------------------------------------------
+// Heavy pass, split by variable.  WENO-AO (KernelWenoRecon_K, Stencil_K.H:164-283,
+// 416-590) works variable by variable on the linearised primitives: smoothness
+// indicators, nonlinear weights and the blend of the substencil reconstructions
+// of variable v need only that variable.  So a block takes 32 listed cells and one
+// thread per (cell, variable) (threadIdx.x = cell, threadIdx.y = variable, one warp
+// per variable) computes that variable at every face / interior point into
+// shared memory, with all WENO weights staged in shared memory once per block;
+// then one thread per cell converts back to conserved variables and runs the
+// positivity procedure (PositivityPreserve_K) and the stores.  Each sum keeps the
+// reference's order.
 template <int DIM, int EQ>
-__global__ void __launch_bounds__(128)
-    heavy_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S,
-                 double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
-                 double *__restrict__ F2, double *__restrict__ src,
-                 const uint32_t *__restrict__ heavy, DevScalars *__restrict__ sc, JudgeArgs jd) {
+struct HeavyShape {
+  using T = Cfg<DIM, EQ>;
+  static constexpr int NR = LinRows<DIM, EQ>::NROWS;          // face points, then interior points
+  static constexpr int NSUM = T::C + T::CC + T::NB * T::CB;   // stencil cells over all substencils
+  static constexpr int DER = T::NI * NSUM;                    // derivative weights
+  static constexpr int FW = NR * NSUM;                        // reconstruction weights
+  static constexpr int CELLS = 32;
+  static constexpr size_t BYTES = (size_t)(DER + FW + CELLS * NR * T::NV + CELLS * 2) * sizeof(double) +
+                                  (size_t)T::NB * T::CB * sizeof(int);
+  __host__ __device__ static constexpr int n(int s) { return s == 0 ? T::C : (s == 1 ? T::CC : T::CB); }
+  __host__ __device__ static constexpr int off(int s) {
+    return s == 0 ? 0 : (s == 1 ? T::C : T::C + T::CC + (s - 2) * T::CB);
+  }
+};
+
+// PositivityPreserve_K's theta procedure on a cell's states held as [row][v]
+// (rows: face points f*NQF+q, then interior points); Common_K.H:299-643
+template <int DIM, int EQ>
+__device__ double pos_apply_rows(const double *__restrict__ ref, const PosBounds &bd, double *__restrict__ rs) {
   using T = Cfg<DIM, EQ>;
   using E = Eos<EQ>;
-  constexpr int NV = T::NV;
+  constexpr int NV = T::NV, NR = LinRows<DIM, EQ>::NROWS;
+  const double rDens = bd.rDens, minDens = bd.minDens, maxDens = bd.maxDens, minEint = bd.minEint;
+  const double rDP = maxDens - rDens, rDM = rDens - minDens;
+  double thD = 1.0;
+  for (int r = 0; r < NR; r++) {
+    const double rho = rs[r * NV + DENS];
+    thD = rho > minDens ? thD : fmin(thD, rDM / (rDens - rho));
+    thD = rho < maxDens ? thD : fmin(thD, rDP / (rho - rDens));
+  }
+  auto mix = [&](double th) {
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+      for (int v = 0; v < NV; v++) rs[r * NV + v] = ref[v] + th * (rs[r * NV + v] - ref[v]);
+  };
+  auto replace = [&]() {
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+      for (int v = 0; v < NV; v++) rs[r * NV + v] = ref[v];
+  };
+  if (thD > 0.0 && thD < 1.0) mix(thD);
+  else if (thD < 1.0) replace();
+  double thP = 1.0;
+  for (int r = 0; r < NR; r++) {
+    double st[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) st[v] = rs[r * NV + v];
+    if (!(E::eint(st) > minEint)) {
+      double a = 0.0, b = 1.0;
+      for (int it = 0; it < 10; it++) {
+        const double c = 0.5 * (a + b);
+        double sm[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) sm[v] = ref[v] + c * (st[v] - ref[v]);
+        if (E::eint(sm) - minEint > 0.0) a = c;
+        else b = c;
+      }
+      thP = fmin(thP, a);
+    }
+  }
+  if (thP > 0.0 && thP < 1.0) mix(thP);
+  else if (thP < 1.0) replace();
+  return fmin(thD, thP);
+}
+
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(32 * Eos<EQ>::NV)
+    heavy_var_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S,
+                     double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
+                     double *__restrict__ F2, double *__restrict__ src, const uint32_t *__restrict__ heavy,
+                     DevScalars *__restrict__ sc, JudgeArgs jd) {
+  using T = Cfg<DIM, EQ>;
+  using H = HeavyShape<DIM, EQ>;
+  using E = Eos<EQ>;
+  constexpr int NV = T::NV, NR = H::NR;
+  extern __shared__ __align__(16) double hsm[];
+  double *sDer = hsm;                       // [s][i][p]
+  double *sFw = sDer + H::DER;              // [s][row][p]
+  double *sFs = sFw + H::FW;                // [cell][row][v]
+  double *sDep = sFs + H::CELLS * NR * NV;  // [cell][2]
+  int *sSub = reinterpret_cast<int *>(sDep + H::CELLS * 2);
+  const kfvm_stencil &st = S->w;
+  const int tid = threadIdx.y * 32 + threadIdx.x, nt = 32 * NV;
+  for (int t = tid; t < H::DER; t += nt) {
+    int s = 0;
+    while (s + 1 < T::NSUB && t >= T::NI * H::off(s + 1)) s++;
+    const int r = t - T::NI * H::off(s), i = r / H::n(s), p = r % H::n(s);
+    sDer[t] = st.deriv_w[s][i][p];
+  }
+  for (int t = tid; t < H::FW; t += nt) {
+    int s = 0;
+    while (s + 1 < T::NSUB && t >= NR * H::off(s + 1)) s++;
+    const int r = t - NR * H::off(s), row = r / H::n(s), p = r % H::n(s);
+    const int nfq = T::NF * T::NQF;
+    sFw[t] = row < nfq ? st.face_w[s][row / T::NQF][row % T::NQF][p] : st.cell_w[s][row - nfq][p];
+  }
+  for (int t = tid; t < T::NB * T::CB; t += nt) sSub[t] = (int)st.sub_idx[t / T::CB][t % T::CB];
+  __syncthreads();
+
   const unsigned count = sc->nheavy;
+  const int x = threadIdx.x, v = threadIdx.y;
   double *F[3] = {F0, F1, F2};
   double lam = 0.0, vel = 0.0;
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
-    const uint32_t e = heavy[t];
+  for (unsigned base = blockIdx.x * H::CELLS; base < count; base += gridDim.x * H::CELLS) {
+    const unsigned t = base + x;
+    const bool have = t < count;
+    const uint32_t e = have ? heavy[t] : 0u;
     const int64_t c = e & kHeavyCell;
     const int64_t i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
     const double *Uc = U + pidx(g, i, j, k);
-    double fs[T::NF][T::NQF][NV];
-    double cs[T::SRC ? T::NQC : 1][NV];
-    if (e & kHeavyJudge) {
-      // judged cell: WENO with its label, compared with the network's prediction
-      double dep = 0.0;
-      weno_cell<DIM, EQ>(Uc, g, S, fs, cs, &dep);
-      const bool lab = dep > jd.tau, p = jd.pred[c] != 0;
-      atomicAdd(&sc->mlp_judged, 1ull);
-      if (lab) atomicAdd(&sc->mlp_pos, 1ull);
-      if (lab && !p) atomicAdd(&sc->mlp_missed, 1ull);
-      if (!lab && p) atomicAdd(&sc->mlp_false, 1ull);
-    } else if (e & kHeavyWeno) {
-      weno_cell<DIM, EQ>(Uc, g, S, fs, cs);
-    } else {
-      for (int f = 0; f < T::NF; f++)
-        for (int q = 0; q < T::NQF; q++) {
-          const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
+    double *rs = sFs + x * NR * NV;
+    if (have && (e & kHeavyWeno)) {
+      // ---- variable v of WENO-AO on the linearised primitives
+      double ref[NV];
 #pragma unroll
-          for (int v = 0; v < NV; v++) fs[f][q][v] = F[f >> 1][a + v * g.nface[f >> 1]];
+      for (int w = 0; w < NV; w++) ref[w] = Uc[w * g.pvol];
+      VarConv<EQ> vc(ref, g.gamma);
+      double Vf[T::C];
+      for (int q = 0; q < T::C; q++) {
+        const int64_t o = S->loff[q];
+        double u[NV];
+#pragma unroll
+        for (int w = 0; w < NV; w++) u[w] = Uc[w * g.pvol + o];
+        vc.cons2LinPrim(u);
+        double uv = u[0];
+#pragma unroll
+        for (int w = 1; w < NV; w++) uv = v == w ? u[w] : uv;
+        Vf[q] = uv;
+      }
+      auto cellOf = [&](int s, int p) { return s < 2 ? p : sSub[(s - 2) * T::CB + p]; };
+      // smoothness indicators: each stencil value is read once and feeds all
+      // NI derivative rows (per row the sum over p keeps its order)
+      double om[T::NSUB];
+#pragma unroll 1
+      for (int s = 0; s < T::NSUB; s++) {
+        const int n = H::n(s);
+        const double *D = sDer + T::NI * H::off(s);
+        double b[T::NI];
+#pragma unroll
+        for (int ii = 0; ii < T::NI; ii++) b[ii] = 0.0;
+        for (int p = 0; p < n; p++) {
+          const double val = Vf[cellOf(s, p)];
+#pragma unroll
+          for (int ii = 0; ii < T::NI; ii++) b[ii] += D[ii * n + p] * val;
         }
-      if constexpr (T::SRC) {
-        for (int q = 0; q < T::NQC; q++)
+        double beta = 0.0;
 #pragma unroll
-          for (int v = 0; v < NV; v++) cs[q][v] = src[(q * NV + v) * g.n + c];
+        for (int ii = 0; ii < T::NI; ii++) beta += b[ii] * b[ii];
+        om[s] = beta;
+      }
+      bool sig = false;
+      if (jd.frac > 0.0 && (e & kHeavyJudge) && (v == DENS || v == ETOT)) {
+        double lin[NV];
+#pragma unroll
+        for (int w = 0; w < NV; w++) lin[w] = ref[w];
+        vc.cons2LinPrim(lin);
+        sig = sqrt(om[0]) > kMlpFloor * fabs(v == DENS ? lin[DENS] : lin[ETOT]);
+      }
+      constexpr double gHi = 0.7, gLo = 0.7;
+      double gam[T::NSUB];
+      gam[0] = gHi;
+      gam[1] = (1.0 - gHi) * gLo;
+#pragma unroll
+      for (int s = 2; s < T::NSUB; s++) gam[s] = (1.0 - gHi) * (1.0 - gLo) / (DIM == 2 ? 4.0 : 6.0);
+      double tot = 0.0;
+#pragma unroll
+      for (int s = 0; s < T::NSUB; s++) {
+        om[s] = gam[s] / (om[s] * om[s] + 1.e-40);
+        tot += om[s];
+      }
+#pragma unroll
+      for (int s = 0; s < T::NSUB; s++) om[s] /= tot;
+      double dep = 0.0;
+      if (sig)
+#pragma unroll
+        for (int s = 0; s < T::NSUB; s++) dep = fmax(dep, fabs(om[s] - gam[s]));
+      if (v == DENS) sDep[x * 2] = dep;
+      if (v == ETOT) sDep[x * 2 + 1] = dep;
+      om[0] /= gam[0];
+#pragma unroll
+      for (int s = 1; s < T::NSUB; s++) om[s] -= om[0] * gam[s];
+      // blend of the substencil reconstructions at every row; each stencil value
+      // feeds all rows of its substencil (per row the sum over p keeps its order)
+      double acc[NR];
+#pragma unroll
+      for (int r = 0; r < NR; r++) acc[r] = 0.0;
+#pragma unroll 1
+      for (int s = 0; s < T::NSUB; s++) {
+        const int n = H::n(s);
+        const double *Wr = sFw + NR * H::off(s);
+        double tt[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) tt[r] = 0.0;
+        for (int p = 0; p < n; p++) {
+          const double val = Vf[cellOf(s, p)];
+#pragma unroll
+          for (int r = 0; r < NR; r++) tt[r] += Wr[r * n + p] * val;
+        }
+        if (om[s] != 0.0)
+#pragma unroll
+          for (int r = 0; r < NR; r++) acc[r] += om[s] * tt[r];
+      }
+#pragma unroll
+      for (int r = 0; r < NR; r++) rs[r * NV + v] = acc[r];
+    } else if (have) {
+      // limiter only: the linear states already written
+      for (int r = 0; r < NR; r++) {
+        double val;
+        if (r < T::NF * T::NQF) {
+          const int f = r / T::NQF, q = r % T::NQF;
+          val = F[f >> 1][face_slot_addr(g, f, i, j, k, q, v, T::NQF, NV)];
+        } else {
+          val = src[((r - T::NF * T::NQF) * NV + v) * g.n + c];
+        }
+        rs[r * NV + v] = val;
       }
     }
-    const PosBounds bd = pos_bounds<DIM, EQ>(Uc, g);
-    theta[c] = pos_apply<DIM, EQ>(Uc, g, bd, fs, cs);
-    for (int f = 0; f < T::NF; f++)
-      for (int q = 0; q < T::NQF; q++) {
-        const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
+    __syncthreads();
+    // ---- back to conserved variables and PositivityPreserve_K, one thread per cell
+    if (v == 0 && have) {
+      double ref[NV];
 #pragma unroll
-        for (int v = 0; v < NV; v++) F[f >> 1][a + v * g.nface[f >> 1]] = fs[f][q][v];
-        if constexpr (T::SRC) {
-          const double *u = fs[f][q];
+      for (int w = 0; w < NV; w++) ref[w] = Uc[w * g.pvol];
+      if (e & kHeavyWeno) {
+        VarConv<EQ> vc(ref, g.gamma);
+        for (int r = 0; r < NR; r++) vc.linPrim2Cons(rs + r * NV);
+        if (e & kHeavyJudge) {
+          const double dep = fmax(sDep[x * 2], sDep[x * 2 + 1]);
+          const bool lab = dep > jd.tau, p = jd.pred[c] != 0;
+          atomicAdd(&sc->mlp_judged, 1ull);
+          if (lab) atomicAdd(&sc->mlp_pos, 1ull);
+          if (lab && !p) atomicAdd(&sc->mlp_missed, 1ull);
+          if (!lab && p) atomicAdd(&sc->mlp_false, 1ull);
+        }
+      }
+      const PosBounds bd = pos_bounds<DIM, EQ>(Uc, g);
+      theta[c] = pos_apply_rows<DIM, EQ>(ref, bd, rs);
+      if constexpr (T::SRC) {
+        for (int r = 0; r < T::NF * T::NQF; r++) {
+          const double *u = rs + r * NV;
           const double vv = fabs(u[MOMX] / u[DENS]);
           const double l = E::fastMagSonic(g.gamma, u, u[MAGX]) + vv;
           vel = vv > vel ? vv : vel;
           lam = l > lam ? l : lam;
         }
       }
-    if constexpr (T::SRC) {
-      for (int q = 0; q < T::NQC; q++)
-#pragma unroll
-        for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = cs[q][v];
     }
+    __syncthreads();
+    // stores: thread (cell, v) writes variable v of every row
+    if (have) {
+      for (int r = 0; r < NR; r++) {
+        const double val = rs[r * NV + v];
+        if (r < T::NF * T::NQF) {
+          const int f = r / T::NQF, q = r % T::NQF;
+          F[f >> 1][face_slot_addr(g, f, i, j, k, q, v, T::NQF, NV)] = val;
+        } else {
+          src[((r - T::NF * T::NQF) * NV + v) * g.n + c] = val;
+        }
+      }
+    }
+    __syncthreads();
   }
   if constexpr (T::SRC) {
-    lam = warp_max(lam);
-    vel = warp_max(vel);
-    if ((threadIdx.x & 31) == 0) {
-      atomic_max_pos(&sc->glm_lam_bits, lam);
-      atomic_max_pos(&sc->glm_vel_bits, vel);
+    if (threadIdx.y == 0) {
+      lam = warp_max(lam);
+      vel = warp_max(vel);
+      if (threadIdx.x == 0) {
+        atomic_max_pos(&sc->glm_lam_bits, lam);
+        atomic_max_pos(&sc->glm_vel_bits, vel);
+      }
     }
   }
 }
@@ -989,7 +1201,15 @@ struct Launch {
   static cudaError_t heavy(const double *U, const Grid &g, const DevStencil *S, double *theta,
                            double *const *F, double *src, const uint32_t *heavy, DevScalars *sc,
                            const JudgeArgs &jd, int heavy_blocks, cudaStream_t s) {
-    heavy_kernel<DIM, EQ><<<heavy_blocks, 128, 0, s>>>(U, g, S, theta, F[0], F[1], F[2], src, heavy, sc, jd);
+    static bool attr = false;
+    if (!attr) {
+      cudaError_t e = cudaFuncSetAttribute(heavy_var_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)HeavyShape<DIM, EQ>::BYTES);
+      if (e != cudaSuccess) return e;
+      attr = true;
+    }
+    heavy_var_kernel<DIM, EQ><<<heavy_blocks, dim3(32, NV), HeavyShape<DIM, EQ>::BYTES, s>>>(
+        U, g, S, theta, F[0], F[1], F[2], src, heavy, sc, jd);
     return cudaGetLastError();
   }
   static cudaError_t riemann(double *const *F, double *const *G, const Grid &g, DevScalars *sc,

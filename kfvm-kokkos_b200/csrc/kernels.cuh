@@ -155,121 +155,6 @@ struct Cfg {
 // Gauss-Legendre weights on (-1/2,1/2), 2 points (src/numeric/Numeric.cpp:14-17)
 __device__ __forceinline__ double gl_wt(int) { return 1.0 / 2.0; }
 
-// ---------------------------------------------------------------------------
-// WENO-AO reconstruction of all faces (and interior points) of one cell
-// (KernelWenoRecon_K, Stencil_K.H:164-283, 416-590)
-template <int DIM, int EQ>
-__device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
-                          const DevStencil *__restrict__ S,
-                          double (&fs)[Cfg<DIM, EQ>::NF][Cfg<DIM, EQ>::NQF][Cfg<DIM, EQ>::NV],
-                          double (&cs)[Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 1][Cfg<DIM, EQ>::NV],
-                          double *dep = nullptr) {
-  using T = Cfg<DIM, EQ>;
-  constexpr int NV = T::NV;
-  const kfvm_stencil &st = S->w;
-  double ref[NV];
-#pragma unroll
-  for (int v = 0; v < NV; v++) ref[v] = Uc[v * g.pvol];
-  VarConv<EQ> vc(ref, g.gamma);
-  double Vf[T::C][NV];
-  for (int c = 0; c < T::C; c++) {
-    const int64_t o = S->loff[c];
-#pragma unroll
-    for (int v = 0; v < NV; v++) Vf[c][v] = Uc[v * g.pvol + o];
-    vc.cons2LinPrim(Vf[c]);
-  }
-  // smoothness indicators beta_s[v] = sum_i (D_s V_s)_iv^2
-  double om[T::NSUB][NV];
-  for (int s = 0; s < T::NSUB; s++) {
-    const int n = s == 0 ? T::C : (s == 1 ? T::CC : T::CB);
-#pragma unroll
-    for (int v = 0; v < NV; v++) om[s][v] = 0.0;
-    for (int i = 0; i < T::NI; i++) {
-      double b[NV];
-#pragma unroll
-      for (int v = 0; v < NV; v++) b[v] = 0.0;
-      for (int p = 0; p < n; p++) {
-        const int c = s < 2 ? p : (int)st.sub_idx[s - 2][p];
-        const double w = st.deriv_w[s][i][p];
-#pragma unroll
-        for (int v = 0; v < NV; v++) b[v] += w * Vf[c][v];
-      }
-#pragma unroll
-      for (int v = 0; v < NV; v++) om[s][v] += b[v] * b[v];
-    }
-  }
-  // significance of the density / pressure variation, for the learned indicator's
-  // label (weno_departure)
-  bool sig[2] = {false, false};
-  if (dep) {
-    double lin[NV];
-#pragma unroll
-    for (int v = 0; v < NV; v++) lin[v] = ref[v];
-    vc.cons2LinPrim(lin);
-    sig[0] = sqrt(om[0][DENS]) > kMlpFloor * fabs(lin[DENS]);
-    sig[1] = sqrt(om[0][ETOT]) > kMlpFloor * fabs(lin[ETOT]);
-  }
-  // nonlinear weights, WENO-JS then AO form (createOmegas, Stencil_K.H:556-580)
-  constexpr double gHi = 0.7, gLo = 0.7;
-  double gam[T::NSUB];
-  gam[0] = gHi;
-  gam[1] = (1.0 - gHi) * gLo;
-#pragma unroll
-  for (int s = 2; s < T::NSUB; s++) gam[s] = (1.0 - gHi) * (1.0 - gLo) / (DIM == 2 ? 4.0 : 6.0);
-#pragma unroll
-  for (int v = 0; v < NV; v++) {
-    double tot = 0.0;
-#pragma unroll
-    for (int s = 0; s < T::NSUB; s++) {
-      om[s][v] = gam[s] / (om[s][v] * om[s][v] + 1.e-40);
-      tot += om[s][v];
-    }
-#pragma unroll
-    for (int s = 0; s < T::NSUB; s++) om[s][v] /= tot;
-    if (dep && ((v == DENS && sig[0]) || (v == ETOT && sig[1])))
-#pragma unroll
-      for (int s = 0; s < T::NSUB; s++) *dep = fmax(*dep, fabs(om[s][v] - gam[s]));
-    om[0][v] /= gam[0];
-#pragma unroll
-    for (int s = 1; s < T::NSUB; s++) om[s][v] -= om[0][v] * gam[s];
-  }
-  // blend the substencil reconstructions (fillRiemannStates / fillInterior)
-  auto blend = [&](const double *W, int ld, double *y, int v) {
-    double acc = 0.0;
-    for (int s = 0; s < T::NSUB; s++) {
-      const int n = s == 0 ? T::C : (s == 1 ? T::CC : T::CB);
-      const double *Ws = W + (size_t)s * ld;
-      double t = 0.0;
-      for (int p = 0; p < n; p++) {
-        const int c = s < 2 ? p : (int)st.sub_idx[s - 2][p];
-        t += Ws[p] * Vf[c][v];
-      }
-      if (s == 0) acc = 0.0;
-      if (om[s][v] != 0.0) acc += om[s][v] * t;
-    }
-    *y = acc;
-  };
-  for (int f = 0; f < T::NF; f++)
-    for (int q = 0; q < T::NQF; q++) {
-#pragma unroll
-      for (int v = 0; v < NV; v++)
-        blend(&st.face_w[0][f][q][0], 6 * KFVM_MAX_FACEQ * KFVM_MAX_CELLS, &fs[f][q][v], v);
-      vc.linPrim2Cons(fs[f][q]);
-    }
-  if constexpr (T::SRC) {
-    for (int q = 0; q < T::NQC; q++) {
-#pragma unroll
-      for (int v = 0; v < NV; v++)
-        blend(&st.cell_w[0][q][0], KFVM_MAX_CELLQ * KFVM_MAX_CELLS, &cs[q][v], v);
-      vc.linPrim2Cons(cs[q]);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// positivity limiter of one cell (PositivityPreserve_K, Common_K.H:299-643), split
-// into the admissible bounds (from the 3^d neighbourhood, with the flattener) and
-// the theta scaling of the reconstructed states toward the cell average.
 // Label of the learned troubled-cell indicator: the largest departure of the
 // normalised WENO-JS weights (createOmegas, Stencil_K.H:556-580, before the
 // adaptive-order transform) from the linear weights gamma_s, over the substencils
@@ -277,7 +162,7 @@ __device__ void weno_cell(const double *__restrict__ Uc, const Grid &g,
 // variation over the stencil exceeds kMlpFloor = 1e-4 of the cell value (below
 // that the weights of noise-level variations are arbitrary, and the linear
 // reconstruction of such variations is harmless).  The
-// smoothness indicators are those of weno_cell (findSmoothness, 506-554).
+// smoothness indicators are those of heavy_var_kernel (findSmoothness, 506-554).
 template <int DIM, int EQ>
 __device__ double weno_departure(const double *__restrict__ Uc, const Grid &g,
                                  const DevStencil *__restrict__ S) {
@@ -390,88 +275,6 @@ template <int EQ>
 __device__ __forceinline__ bool pos_inside(const PosBounds &b, const double *s) {
   const double rho = s[DENS];
   return rho > b.minDens && rho < b.maxDens && Eos<EQ>::eint(s) > b.minEint;
-}
-
-// the reference's theta computation and mixing on all states of a cell
-template <int DIM, int EQ>
-__device__ double pos_apply(const double *__restrict__ Uc, const Grid &g, const PosBounds &bd,
-                            double (&fs)[Cfg<DIM, EQ>::NF][Cfg<DIM, EQ>::NQF][Cfg<DIM, EQ>::NV],
-                            double (&cs)[Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 1][Cfg<DIM, EQ>::NV]) {
-  using T = Cfg<DIM, EQ>;
-  using E = Eos<EQ>;
-  constexpr int NV = T::NV;
-  double ref[NV];
-#pragma unroll
-  for (int v = 0; v < NV; v++) ref[v] = Uc[v * g.pvol];
-  const double rDens = bd.rDens, minDens = bd.minDens, maxDens = bd.maxDens, minEint = bd.minEint;
-  const double rDP = maxDens - rDens, rDM = rDens - minDens;
-  double thD = 1.0;
-  for (int q = 0; q < T::NQF; q++)
-    for (int f = 0; f < T::NF; f++) {
-      const double rho = fs[f][q][DENS];
-      thD = rho > minDens ? thD : fmin(thD, rDM / (rDens - rho));
-      thD = rho < maxDens ? thD : fmin(thD, rDP / (rho - rDens));
-    }
-  if constexpr (T::SRC) {
-    for (int q = 0; q < T::NQC; q++) {
-      const double rho = cs[q][DENS];
-      thD = rho > minDens ? thD : fmin(thD, rDM / (rDens - rho));
-      thD = rho < maxDens ? thD : fmin(thD, rDP / (rho - rDens));
-    }
-  }
-  auto mix = [&](double th) {
-    for (int f = 0; f < T::NF; f++)
-      for (int q = 0; q < T::NQF; q++)
-#pragma unroll
-        for (int v = 0; v < NV; v++) fs[f][q][v] = ref[v] + th * (fs[f][q][v] - ref[v]);
-    if constexpr (T::SRC) {
-      for (int q = 0; q < T::NQC; q++)
-#pragma unroll
-        for (int v = 0; v < NV; v++) cs[q][v] = ref[v] + th * (cs[q][v] - ref[v]);
-    }
-  };
-  auto replace = [&]() {
-    for (int f = 0; f < T::NF; f++)
-      for (int q = 0; q < T::NQF; q++)
-#pragma unroll
-        for (int v = 0; v < NV; v++) fs[f][q][v] = ref[v];
-    if constexpr (T::SRC) {
-      for (int q = 0; q < T::NQC; q++)
-#pragma unroll
-        for (int v = 0; v < NV; v++) cs[q][v] = ref[v];
-    }
-  };
-  if (thD > 0.0 && thD < 1.0) mix(thD);
-  else if (thD < 1.0) replace();
-
-  auto eintPos = [&](const double *state) {
-    double a = 0.0, b = 1.0;
-    double st[NV];
-    for (int it = 0; it < 10; it++) {
-      const double c = 0.5 * (a + b);
-#pragma unroll
-      for (int v = 0; v < NV; v++) st[v] = ref[v] + c * (state[v] - ref[v]);
-      const double dec = E::eint(st) - minEint;
-      if (dec > 0.0) a = c;
-      else b = c;
-    }
-    return a;
-  };
-  double thP = 1.0;
-  for (int q = 0; q < T::NQF; q++)
-    for (int f = 0; f < T::NF; f++) {
-      const double ei = E::eint(fs[f][q]);
-      if (!(ei > minEint)) thP = fmin(thP, eintPos(fs[f][q]));
-    }
-  if constexpr (T::SRC) {
-    for (int q = 0; q < T::NQC; q++) {
-      const double ei = E::eint(cs[q]);
-      if (!(ei > minEint)) thP = fmin(thP, eintPos(cs[q]));
-    }
-  }
-  if (thP > 0.0 && thP < 1.0) mix(thP);
-  else if (thP < 1.0) replace();
-  return fmin(thD, thP);
 }
 
 } // namespace kfvm

@@ -7,7 +7,7 @@
 // Numeric_K.H:292-398 of the reference): it writes the same per-cell flags that
 // compact_kernel turns into the WENO set, with the positivity-history rule
 // (theta < 1 flags a cell) kept.  A sampled fraction of cells (the judge) always
-// runs full WENO; heavy_kernel computes their labels on the way and counts the
+// runs full WENO; heavy_var_kernel computes their labels on the way and counts the
 // cells the network missed, which the host uses to fall back to KXRCF.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>

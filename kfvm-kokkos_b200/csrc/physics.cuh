@@ -62,8 +62,10 @@ struct Eos {
   // that range, or for a non-finite pressure, it returns NaN, which tells the
   // reader to recompute the exact value.
   __device__ __forceinline__ static float weno_approx(double g, const double *U) {
-    const double rho = U[DENS];
-    const double p = pres(g, U);
+    return weno_approx_rp(g, U[DENS], pres(g, U));
+  }
+  // the same from density and pressure
+  __device__ __forceinline__ static float weno_approx_rp(double g, double rho, double p) {
     if (!(rho >= 9.5367431640625e-07 && rho <= 1048576.0) || !(g <= 3.0) || !isfinite(p))
       return __int_as_float(0x7fc00000);
     float l2, r;
