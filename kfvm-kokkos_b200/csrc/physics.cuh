@@ -204,7 +204,8 @@ struct Eos {
       if (rs == RS_HLLC) {
         const double vsqL = vL[1] * vL[1] + vL[2] * vL[2] + vL[3] * vL[3];
         const double vsqR = vR[1] * vR[1] + vR[2] * vR[2] + vR[3] * vR[3];
-        double M = fmax(sqrt(vsqL) / aL, sqrt(vsqR) / aR);
+        // max of the two Mach numbers: sqrt is monotone, so one root of the larger square
+        double M = sqrt(fmax(vsqL / a2L, vsqR / a2R));
         const double uLn = vL[vo[0]], uRn = vR[vo[0]];
         const double psL = rL * (sL - uLn), psR = rR * (sR - uRn);
         const double sS = ((pR - pL) + (psL * uLn - psR * uRn)) / (psL - psR);
@@ -214,7 +215,8 @@ struct Eos {
         const double uJump = uRn - uLn, vJump = vR[vo[1]] - vL[vo[1]], wJump = vR[vo[2]] - vL[vo[2]];
         const double psiFac = psR * psL / (psR - psL);
         const double presRat = fmin(pL, pR) / fmax(pL, pR);
-        const double gFac = 1.0 - pow(presRat, M);
+        // presRat^M (pressure ratio in (0, 1]) as exp(M log presRat); exactly 0 for equal pressures
+        const double gFac = presRat == 1.0 ? 0.0 : 1.0 - exp(M * log(presRat));
         const double shFacL = psiFac * gFac * sL * dL, shFacR = psiFac * gFac * sR * dR;
         M = fmin(M, 1.0);
         const double omm = 1.0 - M * M;
