@@ -39,6 +39,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "launch.h"
@@ -334,50 +335,59 @@ __global__ void __launch_bounds__(kTcThreads, 2)
 #pragma unroll
     for (int v = 0; v < NV; v++) uc[v] = live ? Uc[v * g.pvol] : 0.0;
     const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
-    double *F[3] = {F0, F1, F2};
-    float *W[3] = {W0, W1, W2};
     const int64_t c = (k * g.ny + j) * g.nx + i;
     bool inside = true;
     double lam = 0.0, vel = 0.0;
-    const int r0 = part * Sh::RPP;
+    // the rows of each part are known at compile time (face, direction, point)
+    auto epilogue = [&](auto partTag) {
+      constexpr int PART = decltype(partTag)::value;
+      constexpr int R0 = PART * Sh::RPP;
 #pragma unroll
-    for (int rp = 0; rp < Sh::RPP; rp += 2) {
-      float a0[NV], a1[NV];
+      for (int rp = 0; rp < Sh::RPP; rp += 2) {
+        float a0[NV], a1[NV];
 #pragma unroll
-      for (int v = 0; v < NV; v++) tmem_ld2(tmem + lanes + (uint32_t)(v * Sh::NP + r0 + rp), a0[v], a1[v]);
-      if (live) {
+        for (int v = 0; v < NV; v++) tmem_ld2(tmem + lanes + (uint32_t)(v * Sh::NP + R0 + rp), a0[v], a1[v]);
+        if (live) {
 #pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int rw = r0 + rp + e;
-          if (rw < Sh::NR) {
-            double st[NV];
+          for (int e = 0; e < 2; e++) {
+            const int rw = R0 + rp + e;
+            if (rw < Sh::NR) {
+              double st[NV];
 #pragma unroll
-            for (int v = 0; v < NV; v++) st[v] = uc[v] + (double)(e ? a1[v] : a0[v]);
-            inside = inside && pos_inside<EQ>(bd, st);
-            if (rw < T::NF * T::NQF) {
-              const int f = rw / T::NQF, q = rw % T::NQF;
-              const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
-              const int64_t nf = g.nface[f >> 1];
+              for (int v = 0; v < NV; v++) st[v] = uc[v] + (double)(e ? a1[v] : a0[v]);
+              // pos_inside, with the internal energy kept for the indicator's pressure
+              const double ei = Eos<EQ>::eint(st);
+              inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
+              if (rw < T::NF * T::NQF) {
+                const int f = rw / T::NQF, q = rw % T::NQF, d = f >> 1;
+                double *Fd = d == 0 ? F0 : (d == 1 ? F1 : F2);
+                const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
+                const int64_t nf = g.nface[d];
 #pragma unroll
-              for (int v = 0; v < NV; v++) F[f >> 1][a + v * nf] = st[v];
-              if (wantInd)
-                W[f >> 1][face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] = Eos<EQ>::weno_approx(g.gamma, st);
-              if constexpr (T::SRC) {
-                // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
-                const double vv = fabs(st[MOMX] / st[DENS]);
-                const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
-                vel = vv > vel ? vv : vel;
-                lam = l > lam ? l : lam;
+                for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
+                if (wantInd)
+                  (d == 0 ? W0 : (d == 1 ? W1 : W2))[face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] =
+                      Eos<EQ>::weno_approx_rp(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
+                if constexpr (T::SRC) {
+                  // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
+                  const double vv = fabs(st[MOMX] / st[DENS]);
+                  const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
+                  vel = vv > vel ? vv : vel;
+                  lam = l > lam ? l : lam;
+                }
+              } else if constexpr (T::SRC) {
+                const int q = rw - T::NF * T::NQF;
+#pragma unroll
+                for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
               }
-            } else if constexpr (T::SRC) {
-              const int q = rw - T::NF * T::NQF;
-#pragma unroll
-              for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
             }
           }
         }
       }
-    }
+    };
+    static_assert(kTcParts == 2, "epilogue specialised for two parts");
+    if (part == 0) epilogue(std::integral_constant<int, 0>{});
+    else epilogue(std::integral_constant<int, 1>{});
     // combine the two parts of each cell
     if (live && !inside) atomicAnd(&sIn[row], 0);
     if constexpr (T::SRC) {
