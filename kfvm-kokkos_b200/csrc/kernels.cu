@@ -868,18 +868,19 @@ __device__ void glm_sources(const double *__restrict__ Uc, const Grid &g, int64_
 
 // compact viscous stress and heat flux (Viscosity_K<NavierStokes>, NavierStokes_K.H:190-407)
 template <int DIM>
-__device__ void viscous(const double *__restrict__ Uc, const Grid &g, double Re, double Pr,
-                        double *rhs) {
-  using E = Eos<EQ_NS>;
-  const int64_t sy = g.px, sz = g.px * g.py;
-  auto prim = [&](int64_t o, double &u, double &v, double &w, double &T) {
-    double Uo[5];
-#pragma unroll
-    for (int q = 0; q < 5; q++) Uo[q] = Uc[q * g.pvol + o];
-    u = Uo[MOMX] / Uo[DENS];
-    v = Uo[MOMY] / Uo[DENS];
-    w = Uo[MOMZ] / Uo[DENS];
-    T = E::pres(g.gamma, Uo) / Uo[DENS];
+__device__ void viscous(const double (*vt)[PosTile<DIM>::N], const Grid &g, int tx, int ty, double Re,
+                        double Pr, double *rhs) {
+  // velocities and temperature of the 3^d neighbourhood from the block's tile
+  using P = PosTile<DIM>;
+  constexpr int zr = DIM == 3 ? 1 : 0;
+  // the reference's divisions by 3 and 6 as products with the rounded reciprocals
+  constexpr double kThird = 1.0 / 3.0, kSixth = 1.0 / 6.0;
+  auto prim = [&](int xo, int yo, int zo, double &u, double &v, double &w, double &T) {
+    const int t = ((zr + zo) * P::TY + (ty + 1 + yo)) * P::TX + (tx + 1 + xo);
+    u = vt[0][t];
+    v = vt[1][t];
+    w = vt[2][t];
+    T = vt[3][t];
   };
   if constexpr (DIM == 2) {
     const double rdx = 1.0 / g.dx, rdy = 1.0 / g.dy;
@@ -888,27 +889,27 @@ __device__ void viscous(const double *__restrict__ Uc, const Grid &g, double Re,
     for (int xo = -1; xo <= 1; xo++)
 #pragma unroll
       for (int yo = -1; yo <= 1; yo++)
-        prim(xo + yo * sy, u[xo + 1][yo + 1], v[xo + 1][yo + 1], w[xo + 1][yo + 1], T[xo + 1][yo + 1]);
+        prim(xo, yo, 0, u[xo + 1][yo + 1], v[xo + 1][yo + 1], w[xo + 1][yo + 1], T[xo + 1][yo + 1]);
     double px[4], mx[4], py[4], my[4];
-    px[0] = 4.0 * rdx * (u[2][1] - u[1][1]) / 3.0;
-    px[0] -= rdy * (v[1][2] + v[2][2] - v[1][0] - v[2][0]) / 6.0;
-    px[1] = rdy * (u[1][2] + u[2][2] - u[1][0] - u[2][0]) / 4.0;
+    px[0] = 4.0 * rdx * (u[2][1] - u[1][1]) * kThird;
+    px[0] -= rdy * (v[1][2] + v[2][2] - v[1][0] - v[2][0]) * kSixth;
+    px[1] = rdy * (u[1][2] + u[2][2] - u[1][0] - u[2][0]) * 0.25;
     px[1] += rdx * (v[2][1] - v[1][1]);
     px[2] = rdx * (w[2][1] - w[1][1]);
-    mx[0] = 4.0 * rdx * (u[1][1] - u[0][1]) / 3.0;
-    mx[0] -= rdy * (v[0][2] + v[1][2] - v[0][0] - v[1][0]) / 6.0;
-    mx[1] = rdy * (u[0][2] + u[1][2] - u[0][0] - u[1][0]) / 4.0;
+    mx[0] = 4.0 * rdx * (u[1][1] - u[0][1]) * kThird;
+    mx[0] -= rdy * (v[0][2] + v[1][2] - v[0][0] - v[1][0]) * kSixth;
+    mx[1] = rdy * (u[0][2] + u[1][2] - u[0][0] - u[1][0]) * 0.25;
     mx[1] += rdx * (v[1][1] - v[0][1]);
     mx[2] = rdx * (w[1][1] - w[0][1]);
-    py[0] = rdx * (v[2][2] + v[2][1] - v[0][2] - v[0][1]) / 4.0;
+    py[0] = rdx * (v[2][2] + v[2][1] - v[0][2] - v[0][1]) * 0.25;
     py[0] += rdy * (u[1][2] - u[1][1]);
-    py[1] = 4.0 * rdy * (v[1][2] - v[1][1]) / 3.0;
-    py[1] -= rdx * (u[2][2] + u[2][1] - u[0][2] - u[0][1]) / 6.0;
+    py[1] = 4.0 * rdy * (v[1][2] - v[1][1]) * kThird;
+    py[1] -= rdx * (u[2][2] + u[2][1] - u[0][2] - u[0][1]) * kSixth;
     py[2] = rdy * (w[1][2] - w[1][1]);
-    my[0] = rdx * (v[2][1] + v[2][0] - v[0][1] - v[0][0]) / 4.0;
+    my[0] = rdx * (v[2][1] + v[2][0] - v[0][1] - v[0][0]) * 0.25;
     my[0] += rdy * (u[1][1] - u[1][0]);
-    my[1] = 4.0 * rdy * (v[1][1] - v[1][0]) / 3.0;
-    my[1] -= rdx * (u[2][1] + u[2][0] - u[0][1] - u[0][0]) / 6.0;
+    my[1] = 4.0 * rdy * (v[1][1] - v[1][0]) * kThird;
+    my[1] -= rdx * (u[2][1] + u[2][0] - u[0][1] - u[0][0]) * kSixth;
     my[2] = rdy * (w[1][1] - w[1][0]);
     px[3] = rdx * (T[2][1] - T[1][1]);
     mx[3] = rdx * (T[1][1] - T[0][1]);
@@ -933,51 +934,51 @@ __device__ void viscous(const double *__restrict__ Uc, const Grid &g, double Re,
       for (int yo = -1; yo <= 1; yo++)
 #pragma unroll
         for (int zo = -1; zo <= 1; zo++)
-          prim(xo + yo * sy + zo * sz, u[xo + 1][yo + 1][zo + 1], v[xo + 1][yo + 1][zo + 1],
+          prim(xo, yo, zo, u[xo + 1][yo + 1][zo + 1], v[xo + 1][yo + 1][zo + 1],
                w[xo + 1][yo + 1][zo + 1], T[xo + 1][yo + 1][zo + 1]);
     double px[4], mx[4], py[4], my[4], pz[4], mz[4];
-    px[0] = 4.0 * rdx * (u[2][1][1] - u[1][1][1]) / 3.0;
-    px[0] -= rdy * (v[1][2][1] + v[2][2][1] - v[1][0][1] - v[2][0][1]) / 6.0;
-    px[0] -= rdz * (w[1][1][2] + w[2][1][2] - w[1][1][0] - w[2][1][0]) / 6.0;
-    px[1] = rdy * (u[1][2][1] + u[2][2][1] - u[1][0][1] - u[2][0][1]) / 4.0;
+    px[0] = 4.0 * rdx * (u[2][1][1] - u[1][1][1]) * kThird;
+    px[0] -= rdy * (v[1][2][1] + v[2][2][1] - v[1][0][1] - v[2][0][1]) * kSixth;
+    px[0] -= rdz * (w[1][1][2] + w[2][1][2] - w[1][1][0] - w[2][1][0]) * kSixth;
+    px[1] = rdy * (u[1][2][1] + u[2][2][1] - u[1][0][1] - u[2][0][1]) * 0.25;
     px[1] += rdx * (v[2][1][1] - v[1][1][1]);
-    px[2] = rdz * (u[2][1][2] + u[1][1][2] - u[2][1][0] - u[1][1][0]) / 4.0;
+    px[2] = rdz * (u[2][1][2] + u[1][1][2] - u[2][1][0] - u[1][1][0]) * 0.25;
     px[2] += rdx * (w[2][1][1] - w[1][1][1]);
-    mx[0] = 4.0 * rdx * (u[1][1][1] - u[0][1][1]) / 3.0;
-    mx[0] -= rdy * (v[0][2][1] + v[1][2][1] - v[0][0][1] - v[1][0][1]) / 6.0;
-    mx[0] -= rdz * (w[0][1][2] + w[1][1][2] - w[0][1][0] - w[1][1][0]) / 6.0;
-    mx[1] = rdy * (u[0][2][1] + u[1][2][1] - u[0][0][1] - u[1][0][1]) / 4.0;
+    mx[0] = 4.0 * rdx * (u[1][1][1] - u[0][1][1]) * kThird;
+    mx[0] -= rdy * (v[0][2][1] + v[1][2][1] - v[0][0][1] - v[1][0][1]) * kSixth;
+    mx[0] -= rdz * (w[0][1][2] + w[1][1][2] - w[0][1][0] - w[1][1][0]) * kSixth;
+    mx[1] = rdy * (u[0][2][1] + u[1][2][1] - u[0][0][1] - u[1][0][1]) * 0.25;
     mx[1] += rdx * (v[1][1][1] - v[0][1][1]);
-    mx[2] = rdz * (u[1][1][2] + u[0][1][2] - u[1][1][0] - u[0][1][0]) / 4.0;
+    mx[2] = rdz * (u[1][1][2] + u[0][1][2] - u[1][1][0] - u[0][1][0]) * 0.25;
     mx[2] += rdx * (w[1][1][1] - w[0][1][1]);
-    py[0] = rdx * (v[2][2][1] + v[2][1][1] - v[0][2][1] - v[0][1][1]) / 4.0;
+    py[0] = rdx * (v[2][2][1] + v[2][1][1] - v[0][2][1] - v[0][1][1]) * 0.25;
     py[0] += rdy * (u[1][2][1] - u[1][1][1]);
-    py[1] = 4.0 * rdy * (v[1][2][1] - v[1][1][1]) / 3.0;
-    py[1] -= rdx * (u[2][2][1] + u[2][1][1] - u[0][2][1] - u[0][1][1]) / 6.0;
-    py[1] -= rdz * (w[1][2][2] + w[1][1][2] - w[1][2][0] - w[1][1][0]) / 6.0;
-    py[2] = rdz * (v[1][2][2] + v[1][1][2] - v[1][2][0] - v[1][1][0]) / 4.0;
+    py[1] = 4.0 * rdy * (v[1][2][1] - v[1][1][1]) * kThird;
+    py[1] -= rdx * (u[2][2][1] + u[2][1][1] - u[0][2][1] - u[0][1][1]) * kSixth;
+    py[1] -= rdz * (w[1][2][2] + w[1][1][2] - w[1][2][0] - w[1][1][0]) * kSixth;
+    py[2] = rdz * (v[1][2][2] + v[1][1][2] - v[1][2][0] - v[1][1][0]) * 0.25;
     py[2] += rdy * (w[1][2][1] - w[1][1][1]);
-    my[0] = rdx * (v[2][1][1] + v[2][0][1] - v[0][1][1] - v[0][0][1]) / 4.0;
+    my[0] = rdx * (v[2][1][1] + v[2][0][1] - v[0][1][1] - v[0][0][1]) * 0.25;
     my[0] += rdy * (u[1][1][1] - u[1][0][1]);
-    my[1] = 4.0 * rdy * (v[1][1][1] - v[1][0][1]) / 3.0;
-    my[1] -= rdx * (u[2][1][1] + u[2][0][1] - u[0][1][1] - u[0][0][1]) / 6.0;
-    my[1] -= rdz * (w[1][1][2] + w[1][0][2] - w[1][1][0] - w[1][0][0]) / 6.0;
-    my[2] = rdz * (v[1][1][2] + v[1][0][2] - v[1][1][0] - v[1][0][0]) / 4.0;
+    my[1] = 4.0 * rdy * (v[1][1][1] - v[1][0][1]) * kThird;
+    my[1] -= rdx * (u[2][1][1] + u[2][0][1] - u[0][1][1] - u[0][0][1]) * kSixth;
+    my[1] -= rdz * (w[1][1][2] + w[1][0][2] - w[1][1][0] - w[1][0][0]) * kSixth;
+    my[2] = rdz * (v[1][1][2] + v[1][0][2] - v[1][1][0] - v[1][0][0]) * 0.25;
     my[2] += rdy * (w[1][1][1] - w[1][0][1]);
-    pz[0] = rdx * (w[2][2][1] + w[2][1][1] - w[0][2][1] - w[0][1][1]) / 4.0;
+    pz[0] = rdx * (w[2][2][1] + w[2][1][1] - w[0][2][1] - w[0][1][1]) * 0.25;
     pz[0] += rdz * (u[1][1][2] - u[1][1][1]);
-    pz[1] = rdy * (w[1][2][2] + w[1][2][1] - w[1][0][2] - w[1][0][1]) / 4.0;
+    pz[1] = rdy * (w[1][2][2] + w[1][2][1] - w[1][0][2] - w[1][0][1]) * 0.25;
     pz[1] += rdz * (v[1][1][2] - v[1][1][1]);
-    pz[2] = 4.0 * rdz * (w[1][1][2] - w[1][1][1]) / 3.0;
-    pz[2] -= rdx * (u[2][2][1] + u[2][1][1] - u[0][2][1] - u[0][1][1]) / 6.0;
-    pz[2] -= rdy * (v[1][2][2] + v[1][2][1] - v[1][0][2] - v[1][0][1]) / 6.0;
-    mz[0] = rdx * (w[2][2][0] + w[2][1][0] - w[0][2][0] - w[0][1][0]) / 4.0;
+    pz[2] = 4.0 * rdz * (w[1][1][2] - w[1][1][1]) * kThird;
+    pz[2] -= rdx * (u[2][2][1] + u[2][1][1] - u[0][2][1] - u[0][1][1]) * kSixth;
+    pz[2] -= rdy * (v[1][2][2] + v[1][2][1] - v[1][0][2] - v[1][0][1]) * kSixth;
+    mz[0] = rdx * (w[2][2][0] + w[2][1][0] - w[0][2][0] - w[0][1][0]) * 0.25;
     mz[0] += rdz * (u[1][1][1] - u[1][1][0]);
-    mz[1] = rdy * (w[1][2][1] + w[1][2][0] - w[1][0][1] - w[1][0][0]) / 4.0;
+    mz[1] = rdy * (w[1][2][1] + w[1][2][0] - w[1][0][1] - w[1][0][0]) * 0.25;
     mz[1] += rdz * (v[1][1][1] - v[1][1][0]);
-    mz[2] = 4.0 * rdz * (w[1][1][1] - w[1][1][0]) / 3.0;
-    mz[2] -= rdx * (u[2][2][0] + u[2][1][0] - u[0][2][0] - u[0][1][0]) / 6.0;
-    mz[2] -= rdy * (v[1][2][1] + v[1][2][0] - v[1][0][1] - v[1][0][0]) / 6.0;
+    mz[2] = 4.0 * rdz * (w[1][1][1] - w[1][1][0]) * kThird;
+    mz[2] -= rdx * (u[2][2][0] + u[2][1][0] - u[0][2][0] - u[0][1][0]) * kSixth;
+    mz[2] -= rdy * (v[1][2][1] + v[1][2][0] - v[1][0][1] - v[1][0][0]) * kSixth;
     px[3] = rdx * (T[2][1][1] - T[1][1][1]);
     mx[3] = rdx * (T[1][1][1] - T[0][1][1]);
     py[3] = rdy * (T[1][2][1] - T[1][1][1]);
@@ -1017,6 +1018,31 @@ __global__ void __launch_bounds__(128)
   const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
   const int64_t k = blockIdx.z;
   double err = 0.0, pos = 1.0;
+  // Navier-Stokes: velocities and temperature of the block's cells and a
+  // one-cell ring, once per cell (one reciprocal of the density each)
+  constexpr int NVT = EQ == EQ_NS ? 4 : 1, NTT = EQ == EQ_NS ? PosTile<DIM>::N : 1;
+  __shared__ double vt[NVT][NTT];
+  if constexpr (EQ == EQ_NS) {
+    using P = PosTile<DIM>;
+    const int64_t i0 = blockIdx.x * (int64_t)blockDim.x, j0 = blockIdx.y * (int64_t)blockDim.y;
+    for (int t = threadIdx.y * blockDim.x + threadIdx.x; t < P::N; t += blockDim.x * blockDim.y) {
+      const int a = t % P::TX, b = (t / P::TX) % P::TY, cz = t / (P::TX * P::TY);
+      const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b, gk = k - (DIM == 3 ? 1 : 0) + cz;
+      if (gi > g.nx || gj > g.ny) continue; // beyond the ring of any live cell
+      const double *Uq = U + pidx(g, gi, gj, gk);
+      double uq[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) uq[v] = Uq[v * g.pvol];
+      const double ir = 1.0 / uq[DENS];
+      const double pr = (g.gamma - 1.0) * (uq[ETOT] - 0.5 * (uq[MOMX] * uq[MOMX] + uq[MOMY] * uq[MOMY] +
+                                                               uq[MOMZ] * uq[MOMZ]) * ir);
+      vt[0][t] = uq[MOMX] * ir;
+      vt[1][t] = uq[MOMY] * ir;
+      vt[2][t] = uq[MOMZ] * ir;
+      vt[3][t] = pr * ir;
+    }
+    __syncthreads();
+  }
   if (i < g.nx && j < g.ny) {
     const int64_t c = (k * g.ny + j) * g.nx + i;
     const int64_t p = pidx(g, i, j, k);
@@ -1038,7 +1064,7 @@ __global__ void __launch_bounds__(128)
       }
     }
     if constexpr (EQ == EQ_GLM) glm_sources<DIM>(Uc, g, i, j, k, c, F0, F1, F2, src, theta[c], r);
-    if constexpr (EQ == EQ_NS) viscous<DIM>(Uc, g, Re, Pr, r);
+    if constexpr (EQ == EQ_NS) viscous<DIM>(vt, g, threadIdx.x, threadIdx.y, Re, Pr, r);
 
     if (mode == STAGE_EVAL) {
 #pragma unroll
