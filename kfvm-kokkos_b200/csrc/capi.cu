@@ -607,6 +607,9 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   g.dx = (cfg->xup - cfg->xlo) / cfg->nx;
   g.dy = (cfg->yup - cfg->ylo) / cfg->ny;
   g.dz = (cfg->zup - cfg->zlo) / nz;
+  g.rdx = 1.0 / g.dx;
+  g.rdy = 1.0 / g.dy;
+  g.rdz = 1.0 / g.dz;
   for (int f = 0; f < 6; f++) g.bc[f] = cfg->bc[f];
   g.gamma = cfg->gamma;
   g.rs = cfg->rs;

@@ -883,7 +883,7 @@ __device__ void viscous(const double (*vt)[PosTile<DIM>::N], const Grid &g, int 
     T = vt[3][t];
   };
   if constexpr (DIM == 2) {
-    const double rdx = 1.0 / g.dx, rdy = 1.0 / g.dy;
+    const double rdx = g.rdx, rdy = g.rdy;
     double u[3][3], v[3][3], w[3][3], T[3][3];
 #pragma unroll
     for (int xo = -1; xo <= 1; xo++)
@@ -926,7 +926,7 @@ __device__ void viscous(const double (*vt)[PosTile<DIM>::N], const Grid &g, int 
     rhs[MOMZ] += srw;
     rhs[ETOT] += ste + u[1][1] * sru + v[1][1] * srv + w[1][1] * srw;
   } else {
-    const double rdx = 1.0 / g.dx, rdy = 1.0 / g.dy, rdz = 1.0 / g.dz;
+    const double rdx = g.rdx, rdy = g.rdy, rdz = g.rdz;
     double u[3][3][3], v[3][3][3], w[3][3][3], T[3][3][3];
 #pragma unroll
     for (int xo = -1; xo <= 1; xo++)
@@ -1053,14 +1053,14 @@ __global__ void __launch_bounds__(128)
       const int64_t f1 = (k * g.fdim[1][1] + j) * g.fdim[1][0] + i;
 #pragma unroll
       for (int v = 0; v < NV; v++) {
-        r[v] = (G0[v * g.nface[0] + f0] - G0[v * g.nface[0] + f0 + 1]) / g.dx;
-        r[v] += (G1[v * g.nface[1] + f1] - G1[v * g.nface[1] + f1 + g.fdim[1][0]]) / g.dy;
+        r[v] = (G0[v * g.nface[0] + f0] - G0[v * g.nface[0] + f0 + 1]) * g.rdx;
+        r[v] += (G1[v * g.nface[1] + f1] - G1[v * g.nface[1] + f1 + g.fdim[1][0]]) * g.rdy;
       }
       if constexpr (DIM == 3) {
         const int64_t f2 = (k * g.fdim[2][1] + j) * g.fdim[2][0] + i;
         const int64_t sz = g.fdim[2][0] * g.fdim[2][1];
 #pragma unroll
-        for (int v = 0; v < NV; v++) r[v] += (G2[v * g.nface[2] + f2] - G2[v * g.nface[2] + f2 + sz]) / g.dz;
+        for (int v = 0; v < NV; v++) r[v] += (G2[v * g.nface[2] + f2] - G2[v * g.nface[2] + f2 + sz]) * g.rdz;
       }
     }
     if constexpr (EQ == EQ_GLM) glm_sources<DIM>(Uc, g, i, j, k, c, F0, F1, F2, src, theta[c], r);

@@ -43,6 +43,7 @@ struct Grid {
   int64_t fdim[3][3];        // face grid extents per direction
   int64_t nface[3];
   double dx, dy, dz;
+  double rdx, rdy, rdz;      // 1 / dx, 1 / dy, 1 / dz
   int bc[6];
   double gamma, ch_init;
   int rs;
