@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "launch.h"
@@ -481,7 +482,7 @@ __device__ double pos_apply_rows(const double *__restrict__ ref, const PosBounds
 }
 
 template <int DIM, int EQ>
-__global__ void __launch_bounds__(32 * Eos<EQ>::NV)
+__global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
     heavy_var_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S,
                      double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
                      double *__restrict__ F2, double *__restrict__ src, const uint32_t *__restrict__ heavy,
@@ -532,17 +533,29 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV)
 #pragma unroll
       for (int w = 0; w < NV; w++) ref[w] = Uc[w * g.pvol];
       VarConv<EQ> vc(ref, g.gamma);
+      // component v of the linearised primitives on the stencil (the variable is
+      // uniform in the warp, so each case loads only what its component needs)
       double Vf[T::C];
-      for (int q = 0; q < T::C; q++) {
-        const int64_t o = S->loff[q];
-        double u[NV];
+      auto lin = [&](auto cTag) {
+        constexpr int CV = decltype(cTag)::value;
+#pragma unroll 4
+        for (int q = 0; q < T::C; q++) {
+          const int64_t o = S->loff[q];
+          double u[NV];
 #pragma unroll
-        for (int w = 0; w < NV; w++) u[w] = Uc[w * g.pvol + o];
-        vc.cons2LinPrim(u);
-        double uv = u[0];
-#pragma unroll
-        for (int w = 1; w < NV; w++) uv = v == w ? u[w] : uv;
-        Vf[q] = uv;
+          for (int w = 0; w < NV; w++)
+            u[w] = (CV == ETOT || w == CV || w == DENS) ? Uc[w * g.pvol + o] : 0.0;
+          Vf[q] = vc.lin1(u, CV);
+        }
+      };
+      switch (v) {
+        case DENS: lin(std::integral_constant<int, DENS>{}); break;
+        case MOMX: lin(std::integral_constant<int, MOMX>{}); break;
+        case MOMY: lin(std::integral_constant<int, MOMY>{}); break;
+        case MOMZ: lin(std::integral_constant<int, MOMZ>{}); break;
+        case ETOT: lin(std::integral_constant<int, ETOT>{}); break;
+        default:
+          for (int q = 0; q < T::C; q++) Vf[q] = Uc[v * g.pvol + S->loff[q]]; // magnetic field, psi
       }
       auto cellOf = [&](int s, int p) { return s < 2 ? p : sSub[(s - 2) * T::CB + p]; };
       // smoothness indicators: each stencil value is read once and feeds all

@@ -250,15 +250,17 @@ __device__ __forceinline__ PosBounds pos_bounds(const double *__restrict__ Uc, c
         const int64_t o = xo + yo * sy + zo * sz;
 #pragma unroll
         for (int v = 0; v < NV; v++) s[v] = Uc[v * g.pvol + o];
+        const double ir = 1.0 / s[DENS];
+        const double ei = E::eint_r(s, ir);
         maxDens = fmax(maxDens, s[DENS]);
         minDens = fmin(minDens, s[DENS]);
-        minEint = fmin(minEint, E::eint(s));
-        minSdSp = fmin(minSdSp, E::soundspeed(gm, s));
+        minEint = fmin(minEint, ei);
+        minSdSp = fmin(minSdSp, sqrt(gm * ((gm - 1.0) * ei) * ir));
       }
   auto U = [&](int64_t o, int v) { return Uc[v * g.pvol + o]; };
   const double dxU = U(1, MOMX) / U(1, DENS) - U(-1, MOMX) / U(-1, DENS);
   const double dyV = U(sy, MOMY) / U(sy, DENS) - U(-sy, MOMY) / U(-sy, DENS);
-  const double dzW = U(zr * sz, MOMZ) / U(zr * sz, DENS) - U(-zr * sz, MOMZ) / U(-zr * sz, DENS);
+  const double dzW = DIM == 3 ? U(sz, MOMZ) / U(sz, DENS) - U(-sz, MOMZ) / U(-sz, DENS) : 0.0;
   const double divV = (dxU + dyV + dzW) / 2.0;
   double kappa = 0.2;
   const double eta = fmin(1.0, fmax(0.0, -(kappa * minSdSp + divV) / (kappa * minSdSp)));

@@ -46,6 +46,16 @@ struct Eos {
       return (U[ETOT] - ekin(U));
     }
   }
+  // internal energy with the reciprocal density given (one division shared by
+  // the quantities of a state)
+  __device__ __forceinline__ static double eint_r(const double *U, double ir) {
+    const double ke = 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]) * ir;
+    if constexpr (EQ == EQ_GLM) {
+      return (U[ETOT] - prsb(U) - ke - 0.5 * U[PSI] * U[PSI]);
+    } else {
+      return (U[ETOT] - ke);
+    }
+  }
   __device__ __forceinline__ static double pres(double g, const double *U) {
     return (g - 1.0) * eint(U);
   }
@@ -184,7 +194,7 @@ struct Eos {
     double sL, sR, sMax;
     if constexpr (EQ != EQ_GLM) {
       const double rL = uL[DENS], rR = uR[DENS];
-      const double iL = 1.0 / rL, iR = 1.0 / rR;
+      const double iLR = 1.0 / (rL * rR), iL = rR * iLR, iR = rL * iLR;
       cons2prim_r(g, uL, iL, vL);
       cons2prim_r(g, uR, iR, vR);
       const double pL = vL[4], pR = vR[4];
@@ -210,7 +220,7 @@ struct Eos {
         const double psL = rL * (sL - uLn), psR = rR * (sR - uRn);
         const double sS = ((pR - pL) + (psL * uLn - psR * uRn)) / (psL - psR);
         const double pS = 0.5 * ((pL + pR) + psL * (sS - uLn) + psR * (sS - uRn));
-        const double dL = 1.0 / (sL - sS), dR = 1.0 / (sR - sS);
+        const double dLR = 1.0 / ((sL - sS) * (sR - sS)), dL = (sR - sS) * dLR, dR = (sL - sS) * dLR;
         const double sFacL = sS * dL, sFacR = sS * dR;
         const double uJump = uRn - uLn, vJump = vR[vo[1]] - vL[vo[1]], wJump = vR[vo[2]] - vL[vo[2]];
         const double psiFac = psR * psL / (psR - psL);
@@ -267,10 +277,11 @@ struct Eos {
 // Linearisation of the conserved variables about a reference state
 template <int EQ>
 struct VarConv {
-  double gamm, rho, u, v, w, bx, by, bz, rPsi, vsq;
+  double gamm, rho, irho, u, v, w, bx, by, bz, rPsi, vsq;
   __device__ __forceinline__ VarConv(const double *ref, double gam) {
     gamm = gam - 1.0;
     rho = ref[DENS];
+    irho = 1.0 / rho;
     u = ref[MOMX] / rho;
     v = ref[MOMY] / rho;
     w = ref[MOMZ] / rho;
@@ -295,6 +306,22 @@ struct VarConv {
     s[MOMX] = (s[MOMX] - u * s[DENS]) / rho;
     s[MOMY] = (s[MOMY] - v * s[DENS]) / rho;
     s[MOMZ] = (s[MOMZ] - w * s[DENS]) / rho;
+  }
+  // component c of cons2LinPrim(s), the momenta scaled by the reciprocal density
+  __device__ __forceinline__ double lin1(const double *s, int c) const {
+    if (c == DENS) return s[DENS];
+    if (c == MOMX) return (s[MOMX] - u * s[DENS]) * irho;
+    if (c == MOMY) return (s[MOMY] - v * s[DENS]) * irho;
+    if (c == MOMZ) return (s[MOMZ] - w * s[DENS]) * irho;
+    if (c == ETOT) {
+      if constexpr (EQ == EQ_GLM) {
+        return gamm * (vsq * s[DENS] + s[ETOT] - u * s[MOMX] - v * s[MOMY] - w * s[MOMZ] - bx * s[MAGX] -
+                       by * s[MAGY] - bz * s[MAGZ] - rPsi * s[PSI]);
+      } else {
+        return gamm * (vsq * s[DENS] - u * s[MOMX] - v * s[MOMY] - w * s[MOMZ] + s[ETOT]);
+      }
+    }
+    return s[c];
   }
   __device__ __forceinline__ void linPrim2Cons(double *s) const {
     if constexpr (EQ == EQ_GLM) {

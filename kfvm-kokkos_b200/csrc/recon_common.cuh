@@ -51,12 +51,14 @@ __device__ __forceinline__ void pos_tile_fill(const double *__restrict__ U, cons
     double st[E::NV];
 #pragma unroll
     for (int v = 0; v < E::NV; v++) st[v] = Uc[v * g.pvol];
+    const double ir = 1.0 / st[DENS];
+    const double ei = E::eint_r(st, ir);
     sm[0][t] = st[DENS];
-    sm[1][t] = E::eint(st);
-    sm[2][t] = E::soundspeed(g.gamma, st);
-    sm[3][t] = st[MOMX] / st[DENS];
-    sm[4][t] = st[MOMY] / st[DENS];
-    sm[5][t] = st[MOMZ] / st[DENS];
+    sm[1][t] = ei;
+    sm[2][t] = sqrt(g.gamma * ((g.gamma - 1.0) * ei) * ir);
+    sm[3][t] = st[MOMX] * ir;
+    sm[4][t] = st[MOMY] * ir;
+    sm[5][t] = st[MOMZ] * ir;
   }
 }
 

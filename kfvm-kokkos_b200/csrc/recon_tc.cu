@@ -254,12 +254,14 @@ __global__ void __launch_bounds__(kTcThreads, 2)
       double st[NV];
 #pragma unroll
       for (int v = 0; v < NV; v++) st[v] = Uq[v * g.pvol];
+      const double ir = 1.0 / st[DENS];
+      const double ei = Eos<EQ>::eint_r(st, ir);
       tile[0][t] = st[DENS];
-      tile[1][t] = Eos<EQ>::eint(st);
-      tile[2][t] = Eos<EQ>::soundspeed(g.gamma, st);
-      tile[3][t] = st[MOMX] / st[DENS];
-      tile[4][t] = st[MOMY] / st[DENS];
-      tile[5][t] = st[MOMZ] / st[DENS];
+      tile[1][t] = ei;
+      tile[2][t] = sqrt(g.gamma * ((g.gamma - 1.0) * ei) * ir);
+      tile[3][t] = st[MOMX] * ir;
+      tile[4][t] = st[MOMY] * ir;
+      tile[5][t] = st[MOMZ] * ir;
     }
   }
   if (part == 0) {
