@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 // points goes through shared memory in point order, and the max wave speed
 // through a warp maximum and one atomic per warp.
 template <int DIM, int EQ, int D>
-__global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4))
+__global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4), EQ == EQ_GLM ? 1 : (DIM == 2 ? 16 : 8))
     riemann_kernel(const double *__restrict__ F, double *__restrict__ G, Grid g,
                    DevScalars *__restrict__ sc) {
   using T = Cfg<DIM, EQ>;
