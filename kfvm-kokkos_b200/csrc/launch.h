@@ -61,11 +61,15 @@ int mlp_num_inputs(int dim);
 cudaError_t launch_mlp_collect(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, double tau,
                                double keep, uint64_t seed, uint16_t *feats, uint8_t *labels, int64_t *cells,
                                unsigned long long *count, int64_t cap, cudaStream_t s);
+// inference: first layer on tcgen05 (BF16, FP32 accumulation) with the W1^T image
+// of launch_mlp_pack, the rest in FP32 on the CUDA cores
 cudaError_t launch_mlp_flag(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
-                            const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc, float logit_thr,
-                            cudaStream_t s);
-cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb, float *out,
-                            cudaStream_t s);
+                            const uint16_t *w1img, const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc,
+                            float logit_thr, cudaStream_t s);
+cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
+                            const uint16_t *w1img, float *out, DevScalars *sc, cudaStream_t s);
+int mlp_w1_image_size(int dim);
+cudaError_t launch_mlp_pack(int dim, const uint16_t *wb, uint16_t *img, cudaStream_t s);
 cudaError_t launch_mlp_train_step(int dim, const uint16_t *feats, const uint8_t *labels, int64_t n, int batch,
                                   float *master, float *m, float *v, float *grad, float *wq, uint16_t *wb,
                                   float *loss, float pos_weight, float lr, int t, uint64_t seed, cudaStream_t s);

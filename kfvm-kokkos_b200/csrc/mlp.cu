@@ -17,6 +17,7 @@
 #include "kernels.cuh"
 #include "launch.h"
 #include "mlp.cuh"
+#include "tcgen05.cuh"
 
 namespace kfvm {
 
@@ -188,117 +189,211 @@ __global__ void __launch_bounds__(256)
   wq[t] = __bfloat162float(b);
 }
 
-// BF16 weights -> FP32, W1 transposed to [input][hidden] for the per-cell pass
-template <int DIM>
-__device__ __forceinline__ void mlp_stage_weights(const uint16_t *__restrict__ wb, float *__restrict__ sw) {
-  using M = MlpShape<DIM>;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
-  for (int t = tid; t < M::NW; t += nt) {
-    const float x = __bfloat162float(__ushort_as_bfloat16(wb[t]));
-    if (t < M::B1) sw[(t % M::NI) * M::NH + t / M::NI] = x;
-    else sw[t] = x;
-  }
-}
+// ---------------------------------------------------------------------------
+// Inference with the first layer on the tcgen05 tensor cores: per block of 128
+// cells (two threads per cell = per row of the tile) the BF16 feature rows form
+// A [128 x KP], W1^T in BF16 forms B [KP x 32], and D = A B accumulates in FP32
+// in 32 TMEM columns (M128 N32 K16 MMAs, kind::f16).  The features are written
+// in halves of K into one shared-memory buffer (two blocks fit an SM).  Then
+// bias + GELU, the 32 x 32 second layer and the output on the CUDA cores in FP32
+// (as in training).  Every mbarrier wait is bounded; on timeout the block sets
+// DevScalars::fault and returns after freeing its TMEM.
+constexpr int kMlpThreads = 256;
 
-// network logit of the cell at block position (tx, ty), features from the tile;
-// the first layer sums the density inputs, then the pressure inputs, in order
 template <int DIM>
-__device__ __forceinline__ float mlp_cell_logit(const double (*t)[MlpTile<DIM>::N], int tx, int ty,
-                                                const float *__restrict__ sw) {
+struct MlpTc {
   using M = MlpShape<DIM>;
   using Tl = MlpTile<DIM>;
-  constexpr int R = Tl::R, ZR = DIM == 3 ? R : 0;
-  double rc, pc, sr, sp;
-  mlp_scales<DIM>(t, tx, ty, rc, pc, sr, sp);
-  const int c0 = (ZR * Tl::TY + ty + R) * Tl::TX + tx + R;
-  float z[M::NH];
-#pragma unroll
-  for (int h = 0; h < M::NH; h++) z[h] = sw[M::B1 + h];
-#pragma unroll 1
-  for (int a = 0; a < 2; a++) {
-    const double ref = a == 0 ? rc : pc, sc = a == 0 ? sr : sp;
-    int q = a * M::P;
-    for (int dz = -ZR; dz <= ZR; dz++)
-      for (int dy = -R; dy <= R; dy++)
-#pragma unroll
-        for (int dx = -R; dx <= R; dx++, q++) {
-          const float x = (float)((t[a][c0 + (dz * Tl::TY + dy) * Tl::TX + dx] - ref) * sc);
-          const float4 *wr = reinterpret_cast<const float4 *>(sw + q * M::NH);
-#pragma unroll
-          for (int h4 = 0; h4 < M::NH / 4; h4++) {
-            const float4 wv = wr[h4];
-            z[4 * h4 + 0] = fmaf(wv.x, x, z[4 * h4 + 0]);
-            z[4 * h4 + 1] = fmaf(wv.y, x, z[4 * h4 + 1]);
-            z[4 * h4 + 2] = fmaf(wv.z, x, z[4 * h4 + 2]);
-            z[4 * h4 + 3] = fmaf(wv.w, x, z[4 * h4 + 3]);
-          }
-        }
-  }
-#pragma unroll
-  for (int h = 0; h < M::NH; h++) z[h] = gelu(z[h]);
-  float out = sw[M::B3];
-#pragma unroll 4
-  for (int o = 0; o < M::NH; o++) {
-    float a = sw[M::B2 + o];
-    const float *wr = sw + M::W2 + o * M::NH;
-#pragma unroll
-    for (int h = 0; h < M::NH; h++) a = fmaf(wr[h], z[h], a);
-    out = fmaf(sw[M::W3 + o], gelu(a), out);
-  }
-  return out;
-}
-
-template <int DIM>
-struct FlagSmem {
-  static constexpr size_t TILE = 2 * MlpTile<DIM>::N * sizeof(double);
-  static constexpr size_t BYTES = TILE + MlpShape<DIM>::NW * sizeof(float);
+  static constexpr int KP = (M::NI + 15) / 16 * 16;        // K padded to the MMA K of 16
+  static constexpr int NCH = KP / 8;                       // 16-byte chunks of 8 BF16
+  static constexpr int HALVES = DIM == 3 ? 2 : 1;
+  static constexpr int NCHH = NCH / HALVES;                // chunks per half
+  static constexpr int A_CH = 128 * 16;
+  static constexpr int B_CH = 32 * 16;
+  static constexpr int OFF_B = NCHH * A_CH;                // A: one half
+  static constexpr int OFF_TILE = OFF_B + NCH * B_CH;      // B: all of W1^T
+  static constexpr int OFF_H = OFF_TILE + 2 * Tl::N * 8;   // H1 [128][33] floats
+  static constexpr int OFF_W = OFF_H + 128 * 33 * 4;       // b1, W2, b2, w3, b3 (floats)
+  static constexpr int NW2 = M::NW - M::B1;
+  static constexpr int OFF_SC = OFF_W + (NW2 + 3) / 4 * 16; // scales [128][4] doubles
+  static constexpr int OFF_OFS = OFF_SC + 128 * 4 * 8;     // patch offsets [P] int
+  static constexpr int OFF_BAR = OFF_OFS + (M::P + 3) / 4 * 16;
+  static constexpr int SMEM = OFF_BAR + 16;
+  static_assert(NCH % HALVES == 0 && NCHH % 2 == 0, "K halves of whole MMA steps");
+  static_assert(SMEM <= 113 * 1024, "two blocks per SM");
 };
 
-// inference in the stage: flag = network says troubled, or theta < 1 (the
-// positivity history rule of WenoSelect_K); pred keeps the network's answer for
-// the judge; the flagged count feeds the flag-set semantics as in flag_kernel
-template <int DIM, int EQ>
-__global__ void __launch_bounds__(128)
-    mlp_flag_kernel(const double *__restrict__ U, Grid g, const uint16_t *__restrict__ wb,
-                    const double *__restrict__ theta, uint8_t *__restrict__ flag, uint8_t *__restrict__ pred,
-                    DevScalars *__restrict__ sc, float logit_thr) {
-  using Tl = MlpTile<DIM>;
-  extern __shared__ __align__(16) unsigned char fsm[];
-  double(*tile)[Tl::N] = reinterpret_cast<double(*)[Tl::N]>(fsm);
-  float *sw = reinterpret_cast<float *>(fsm + FlagSmem<DIM>::TILE);
-  const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY, k = blockIdx.z;
-  mlp_stage_weights<DIM>(wb, sw);
-  mlp_tile_fill<DIM, EQ>(U, g, i0, j0, k, tile);
-  __syncthreads();
-  const int64_t i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-  bool f = false;
-  if (i < g.nx && j < g.ny) {
-    const int64_t c = (k * g.ny + j) * g.nx + i;
-    const bool p = mlp_cell_logit<DIM>(tile, threadIdx.x, threadIdx.y, sw) > logit_thr;
-    pred[c] = p ? 1 : 0;
-    f = p || theta[c] < 1.0;
-    flag[c] = f ? 1 : 0;
-  }
-  const unsigned ball = __ballot_sync(0xffffffffu, f);
-  if ((threadIdx.x & 31) == 0 && ball) atomicAdd(&sc->nflag, (unsigned)__popc(ball));
+template <int DIM>
+__global__ void __launch_bounds__(256) mlp_pack_kernel(const uint16_t *__restrict__ wb, uint16_t *__restrict__ img) {
+  using M = MlpShape<DIM>;
+  using C = MlpTc<DIM>;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 32 * C::KP) return;
+  const int n = t / C::KP, k = t % C::KP;
+  img[(k / 8) * 256 + n * 8 + (k % 8)] = k < M::NI ? wb[M::W1 + n * M::NI + k] : (uint16_t)0;
 }
 
-// probability of every cell (inspection and tests)
-template <int DIM, int EQ>
-__global__ void __launch_bounds__(128)
-    mlp_prob_kernel(const double *__restrict__ U, Grid g, const uint16_t *__restrict__ wb, float *__restrict__ out) {
+// mode 0: flags (+ prediction, flagged count); mode 1: probabilities
+template <int DIM, int EQ, int MODE>
+__global__ void __launch_bounds__(kMlpThreads, 2)
+    mlp_tc_kernel(const double *__restrict__ U, Grid g, const uint16_t *__restrict__ wb,
+                  const uint16_t *__restrict__ w1img, const double *__restrict__ theta, uint8_t *__restrict__ flag,
+                  uint8_t *__restrict__ pred, float *__restrict__ prob, DevScalars *__restrict__ sc, float logit_thr) {
+  using M = MlpShape<DIM>;
   using Tl = MlpTile<DIM>;
-  extern __shared__ __align__(16) unsigned char fsm[];
-  double(*tile)[Tl::N] = reinterpret_cast<double(*)[Tl::N]>(fsm);
-  float *sw = reinterpret_cast<float *>(fsm + FlagSmem<DIM>::TILE);
+  using C = MlpTc<DIM>;
+  extern __shared__ __align__(128) uint8_t msm[];
+  double(*tile)[Tl::N] = reinterpret_cast<double(*)[Tl::N]>(msm + C::OFF_TILE);
+  float(*sH)[33] = reinterpret_cast<float(*)[33]>(msm + C::OFF_H);
+  float *sW = reinterpret_cast<float *>(msm + C::OFF_W);   // layout of the flat weights from B1 on
+  double(*sSc)[4] = reinterpret_cast<double(*)[4]>(msm + C::OFF_SC);
+  int *sOfs = reinterpret_cast<int *>(msm + C::OFF_OFS);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(msm + C::OFF_BAR);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(msm + C::OFF_BAR + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quarter = warp & 3, part = warp >> 2;
+  const int row = quarter * 32 + lane;
   const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY, k = blockIdx.z;
-  mlp_stage_weights<DIM>(wb, sw);
-  mlp_tile_fill<DIM, EQ>(U, g, i0, j0, k, tile);
+  const int64_t i = i0 + lane, j = j0 + quarter;
+  const bool live = i < g.nx && j < g.ny;
+  const uint32_t barA = smem_u32(bar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(32u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barA) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  {
+    const uint4 *src = reinterpret_cast<const uint4 *>(w1img);
+    uint4 *dst = reinterpret_cast<uint4 *>(msm + C::OFF_B);
+    for (int t = tid; t < C::NCH * C::B_CH / 16; t += kMlpThreads) dst[t] = src[t];
+    for (int t = tid; t < C::NW2; t += kMlpThreads) sW[t] = __bfloat162float(__ushort_as_bfloat16(wb[M::B1 + t]));
+    constexpr int ZR = DIM == 3 ? Tl::R : 0;
+    for (int q = tid; q < M::P; q += kMlpThreads) {
+      const int dx = q % M::SIDE - Tl::R, dy = (q / M::SIDE) % M::SIDE - Tl::R, dz = q / (M::SIDE * M::SIDE) - ZR;
+      sOfs[q] = (dz * Tl::TY + dy) * Tl::TX + dx;
+    }
+  }
+  for (int t = tid; t < Tl::N; t += kMlpThreads) {
+    const int a = t % Tl::TX, b = (t / Tl::TX) % Tl::TY, cz = t / (Tl::TX * Tl::TY);
+    const int64_t gi = i0 - Tl::R + a, gj = j0 - Tl::R + b, gk = k - (DIM == 3 ? Tl::R : 0) + cz;
+    if (gi > g.nx + Tl::R - 1 || gj > g.ny + Tl::R - 1) continue;
+    const double *Uq = U + pidx(g, gi, gj, gk);
+    double u[Eos<EQ>::NV];
+#pragma unroll
+    for (int v = 0; v < Eos<EQ>::NV; v++) u[v] = Uq[v * g.pvol];
+    tile[0][t] = u[DENS];
+    tile[1][t] = Eos<EQ>::pres(g.gamma, u);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  const int64_t i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-  if (i >= g.nx || j >= g.ny) return;
-  const float z = mlp_cell_logit<DIM>(tile, threadIdx.x, threadIdx.y, sw);
-  out[(k * g.ny + j) * g.nx + i] = 1.0f / (1.0f + expf(-z));
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  // scales of the two patches: part 0 density, part 1 pressure
+  constexpr int ZR = DIM == 3 ? Tl::R : 0;
+  const int c0 = (ZR * Tl::TY + quarter + Tl::R) * Tl::TX + lane + Tl::R;
+  {
+    const double ref = tile[part][c0];
+    double mx = 0.0;
+    for (int q = 0; q < M::P; q++) mx = fmax(mx, fabs(tile[part][c0 + sOfs[q]] - ref));
+    sSc[row][part] = ref;
+    sSc[row][2 + part] = 1.0 / (mx + kMlpFloor * fabs(ref) + 1e-300);
+  }
+  __syncthreads();
+  const double rc = sSc[row][0], pc = sSc[row][1], sr = sSc[row][2], sp = sSc[row][3];
+  const uint32_t aB = smem_u32(msm), bB = smem_u32(msm + C::OFF_B);
+  constexpr uint32_t idesc = bf16_idesc<32>();
+  bool ok = true;
+#pragma unroll 1
+  for (int h = 0; h < C::HALVES; h++) {
+    // this thread's chunks of the half: features k = 8 ch .. 8 ch + 7
+    for (int cl = part; cl < C::NCHH; cl += 2) {
+      const int ch = h * C::NCHH + cl;
+      uint32_t pk[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        float x2[2];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int kk = ch * 8 + 2 * t + e;
+          float x = 0.0f;
+          if (kk < M::P) x = (float)((tile[0][c0 + sOfs[kk]] - rc) * sr);
+          else if (kk < M::NI) x = (float)((tile[1][c0 + sOfs[kk - M::P]] - pc) * sp);
+          x2[e] = live ? x : 0.0f;
+        }
+        pk[t] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x2[0])) |
+                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x2[1])) << 16);
+      }
+      st_shared_v4(aB + cl * C::A_CH + row * 16, pk);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+      for (int s = 0; s < C::NCHH / 2; s++) {
+        const uint64_t ad = umma_desc(aB + 2 * s * C::A_CH, C::A_CH, 128);
+        const uint64_t bd = umma_desc(bB + (h * C::NCHH + 2 * s) * C::B_CH, C::B_CH, 128);
+        mma_bf16(tmem, ad, bd, idesc, (h > 0 || s > 0) ? 1 : 0);
+      }
+      mma_commit(barA);
+    }
+    ok = mbar_wait(barA, (uint32_t)h & 1u);
+    if (!__syncthreads_and(ok)) break;
+  }
+  if (__syncthreads_and(ok)) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // first layer: bias + GELU of this part's 16 hidden units
+    const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+    float z[16];
+    tmem_ld8(tmem + lanes + (uint32_t)(16 * part), *reinterpret_cast<float(*)[8]>(z));
+    tmem_ld8(tmem + lanes + (uint32_t)(16 * part + 8), *reinterpret_cast<float(*)[8]>(z + 8));
+#pragma unroll
+    for (int t = 0; t < 16; t++) sH[row][16 * part + t] = gelu(z[t] + sW[16 * part + t]);
+    __syncthreads();
+    // second layer and output on the CUDA cores, 16 outputs per part
+    float acc = 0.0f;
+#pragma unroll 4
+    for (int o = 16 * part; o < 16 * part + 16; o++) {
+      float a = sW[M::B2 - M::B1 + o];
+      const float *wr = sW + (M::W2 - M::B1) + o * M::NH;
+#pragma unroll
+      for (int hh = 0; hh < M::NH; hh++) a = fmaf(wr[hh], sH[row][hh], a);
+      acc = fmaf(sW[M::W3 - M::B1 + o], gelu(a), acc);
+    }
+    __syncthreads();
+    if (part == 1) sH[row][32] = acc;   // the second half's sum, read by part 0
+    __syncthreads();
+    if (part == 0 && live) {
+      const float logit = sW[M::B3 - M::B1] + acc + sH[row][32];
+      const int64_t c = (k * g.ny + j) * g.nx + i;
+      if (MODE == 0) {
+        const bool p = logit > logit_thr;
+        pred[c] = p ? 1 : 0;
+        const bool f = p || theta[c] < 1.0;
+        flag[c] = f ? 1 : 0;
+      } else {
+        prob[c] = 1.0f / (1.0f + expf(-logit));
+      }
+    }
+    if (MODE == 0 && part == 0) {
+      bool f = false;
+      if (live) f = flag[(k * g.ny + j) * g.nx + i] != 0;
+      const unsigned ball = __ballot_sync(0xffffffffu, f);
+      if (lane == 0 && ball) atomicAdd(&sc->nflag, (unsigned)__popc(ball));
+    }
+  } else if (tid == 0) {
+    atomicExch(&sc->fault, 1u);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u) : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -320,32 +415,32 @@ static cudaError_t collect_t(const double *U, const Grid &g, const DevStencil *S
   return cudaGetLastError();
 }
 
-template <int DIM, int EQ>
-static cudaError_t flag_t(const double *U, const Grid &g, const uint16_t *wb, const double *theta, uint8_t *flag,
-                          uint8_t *pred, DevScalars *sc, float thr, cudaStream_t s) {
+template <int DIM, int EQ, int MODE>
+static cudaError_t tc_t(const double *U, const Grid &g, const uint16_t *wb, const uint16_t *img, const double *theta,
+                        uint8_t *flag, uint8_t *pred, float *prob, DevScalars *sc, float thr, cudaStream_t s) {
+  using C = MlpTc<DIM>;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(mlp_flag_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)FlagSmem<DIM>::BYTES);
+    cudaError_t e = cudaFuncSetAttribute(mlp_tc_kernel<DIM, EQ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         C::SMEM);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  mlp_flag_kernel<DIM, EQ><<<mlp_cell_grid(g), dim3(kBlockX, kBlockY), FlagSmem<DIM>::BYTES, s>>>(
-      U, g, wb, theta, flag, pred, sc, thr);
+  mlp_tc_kernel<DIM, EQ, MODE><<<mlp_cell_grid(g), kMlpThreads, C::SMEM, s>>>(U, g, wb, img, theta, flag, pred, prob,
+                                                                            sc, thr);
   return cudaGetLastError();
 }
 
 template <int DIM, int EQ>
-static cudaError_t prob_t(const double *U, const Grid &g, const uint16_t *wb, float *out, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(mlp_prob_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)FlagSmem<DIM>::BYTES);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  mlp_prob_kernel<DIM, EQ><<<mlp_cell_grid(g), dim3(kBlockX, kBlockY), FlagSmem<DIM>::BYTES, s>>>(U, g, wb, out);
-  return cudaGetLastError();
+static cudaError_t flag_t(const double *U, const Grid &g, const uint16_t *wb, const uint16_t *img,
+                          const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc, float thr, cudaStream_t s) {
+  return tc_t<DIM, EQ, 0>(U, g, wb, img, theta, flag, pred, nullptr, sc, thr, s);
+}
+
+template <int DIM, int EQ>
+static cudaError_t prob_t(const double *U, const Grid &g, const uint16_t *wb, const uint16_t *img, float *out,
+                          DevScalars *sc, cudaStream_t s) {
+  return tc_t<DIM, EQ, 1>(U, g, wb, img, nullptr, nullptr, nullptr, out, sc, 0.0f, s);
 }
 
 #define KFVM_MLP_DISPATCH(DIM_, EQ_, FN, ...)                                      \
@@ -366,14 +461,23 @@ cudaError_t launch_mlp_collect(int dim, int eq, const double *U, const Grid &g, 
 }
 
 cudaError_t launch_mlp_flag(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
-                            const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc, float logit_thr,
-                            cudaStream_t s) {
-  KFVM_MLP_DISPATCH(dim, eq, flag_t, U, g, wb, theta, flag, pred, sc, logit_thr, s);
+                            const uint16_t *w1img, const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc,
+                            float logit_thr, cudaStream_t s) {
+  KFVM_MLP_DISPATCH(dim, eq, flag_t, U, g, wb, w1img, theta, flag, pred, sc, logit_thr, s);
 }
 
-cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb, float *out,
-                            cudaStream_t s) {
-  KFVM_MLP_DISPATCH(dim, eq, prob_t, U, g, wb, out, s);
+cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
+                            const uint16_t *w1img, float *out, DevScalars *sc, cudaStream_t s) {
+  KFVM_MLP_DISPATCH(dim, eq, prob_t, U, g, wb, w1img, out, sc, s);
+}
+
+int mlp_w1_image_size(int dim) { return dim == 2 ? 32 * MlpTc<2>::KP : 32 * MlpTc<3>::KP; }
+
+cudaError_t launch_mlp_pack(int dim, const uint16_t *wb, uint16_t *img, cudaStream_t s) {
+  const int n = mlp_w1_image_size(dim);
+  if (dim == 2) mlp_pack_kernel<2><<<(n + 255) / 256, 256, 0, s>>>(wb, img);
+  else mlp_pack_kernel<3><<<(n + 255) / 256, 256, 0, s>>>(wb, img);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_mlp_train_step(int dim, const uint16_t *feats, const uint8_t *labels, int64_t n, int batch,

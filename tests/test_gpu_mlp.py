@@ -2,8 +2,9 @@
 
 * labels (WENO weight departure > tau) against the oracle's restatement,
 * features (normalised density / pressure patch, BF16) against numpy,
-* the network's probability (BF16 weights, FP32 accumulation) against a
-  float64 numpy forward pass with the same BF16 weights,
+* the network's probability (first layer on the tensor cores with BF16 features
+  and weights, FP32 accumulation) against a float64 numpy forward pass with the
+  same BF16 values,
 * training (loss falls, troubled cells are recalled on the collected set),
 * a run with the indicator in the stage (the judge counts, no failure) whose
   state stays close to the KXRCF run, and, on the isentropic vortex after one
@@ -74,7 +75,9 @@ def test_probability_matches_numpy(name, scale, product_lib, gpu):
     prob = s.mlp_probability()
     u = s.get_state()
     cells = np.arange(0, abi.ncells(cfg), 7)
-    ref = mlp_ref.probability(w, mlp_ref.features(u, cfg, cells))
+    # the kernel feeds the tensor cores BF16 features, as training sees them
+    x = mlp_ref.bf16_to_f32(mlp_ref.f32_to_bf16(mlp_ref.features(u, cfg, cells)))
+    ref = mlp_ref.probability(w, x)
     assert np.abs(prob[cells] - ref).max() < 2e-4, name
     # weights round-trip through the ABI
     s.mlp_set_weights(w)
