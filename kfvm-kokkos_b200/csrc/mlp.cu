@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(128)
                        int64_t *__restrict__ cells, unsigned long long *__restrict__ count, int64_t cap) {
   using M = MlpShape<DIM>;
   using Tl = MlpTile<DIM>;
-  __shared__ double tile[2][Tl::N];
+  __shared__ float tile[2][Tl::N];
   const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY, k = blockIdx.z;
   mlp_tile_fill<DIM, EQ>(U, g, i0, j0, k, tile);
   __syncthreads();
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(128)
   if (!pos && !(unit_hash(seed, (uint64_t)c) < keep_frac)) return;
   const unsigned long long idx = atomicAdd(count, 1ull);
   if ((int64_t)idx >= cap) return;
-  double rc, pc, sr, sp;
+  float rc, pc, sr, sp;
   mlp_scales<DIM>(tile, threadIdx.x, threadIdx.y, rc, pc, sr, sp);
   constexpr int R = Tl::R, ZR = DIM == 3 ? R : 0;
   const int c0 = (ZR * Tl::TY + threadIdx.y + R) * Tl::TX + threadIdx.x + R;
@@ -53,8 +53,8 @@ __global__ void __launch_bounds__(128)
     for (int dy = -R; dy <= R; dy++)
       for (int dx = -R; dx <= R; dx++, q++) {
         const int n = c0 + (dz * Tl::TY + dy) * Tl::TX + dx;
-        x[q] = __bfloat16_as_ushort(__float2bfloat16_rn((float)((tile[0][n] - rc) * sr)));
-        x[M::P + q] = __bfloat16_as_ushort(__float2bfloat16_rn((float)((tile[1][n] - pc) * sp)));
+        x[q] = __bfloat16_as_ushort(__float2bfloat16_rn(mlp_feature(tile[0][n], rc, sr)));
+        x[M::P + q] = __bfloat16_as_ushort(__float2bfloat16_rn(mlp_feature(tile[1][n], pc, sp)));
       }
   labels[idx] = pos ? 1 : 0;
   cells[idx] = c;
@@ -212,11 +212,11 @@ struct MlpTc {
   static constexpr int B_CH = 32 * 16;
   static constexpr int OFF_B = NCHH * A_CH;                // A: one half
   static constexpr int OFF_TILE = OFF_B + NCH * B_CH;      // B: all of W1^T
-  static constexpr int OFF_H = OFF_TILE + 2 * Tl::N * 8;   // H1 [128][33] floats
+  static constexpr int OFF_H = OFF_TILE + (2 * Tl::N * 4 + 15) / 16 * 16; // H1 [128][33] floats
   static constexpr int OFF_W = OFF_H + 128 * 33 * 4;       // b1, W2, b2, w3, b3 (floats)
   static constexpr int NW2 = M::NW - M::B1;
-  static constexpr int OFF_SC = OFF_W + (NW2 + 3) / 4 * 16; // scales [128][4] doubles
-  static constexpr int OFF_OFS = OFF_SC + 128 * 4 * 8;     // patch offsets [P] int
+  static constexpr int OFF_SC = OFF_W + (NW2 + 3) / 4 * 16; // centers and scales [128][4] floats
+  static constexpr int OFF_OFS = OFF_SC + 128 * 4 * 4;     // patch offsets [P] int
   static constexpr int OFF_BAR = OFF_OFS + (M::P + 3) / 4 * 16;
   static constexpr int SMEM = OFF_BAR + 16;
   static_assert(NCH % HALVES == 0 && NCHH % 2 == 0, "K halves of whole MMA steps");
@@ -243,10 +243,10 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
   using Tl = MlpTile<DIM>;
   using C = MlpTc<DIM>;
   extern __shared__ __align__(128) uint8_t msm[];
-  double(*tile)[Tl::N] = reinterpret_cast<double(*)[Tl::N]>(msm + C::OFF_TILE);
+  float(*tile)[Tl::N] = reinterpret_cast<float(*)[Tl::N]>(msm + C::OFF_TILE);
   float(*sH)[33] = reinterpret_cast<float(*)[33]>(msm + C::OFF_H);
   float *sW = reinterpret_cast<float *>(msm + C::OFF_W);   // layout of the flat weights from B1 on
-  double(*sSc)[4] = reinterpret_cast<double(*)[4]>(msm + C::OFF_SC);
+  float(*sSc)[4] = reinterpret_cast<float(*)[4]>(msm + C::OFF_SC);
   int *sOfs = reinterpret_cast<int *>(msm + C::OFF_OFS);
   uint64_t *bar = reinterpret_cast<uint64_t *>(msm + C::OFF_BAR);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(msm + C::OFF_BAR + 8);
@@ -286,8 +286,8 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
     double u[Eos<EQ>::NV];
 #pragma unroll
     for (int v = 0; v < Eos<EQ>::NV; v++) u[v] = Uq[v * g.pvol];
-    tile[0][t] = u[DENS];
-    tile[1][t] = Eos<EQ>::pres(g.gamma, u);
+    tile[0][t] = (float)u[DENS];
+    tile[1][t] = (float)Eos<EQ>::pres(g.gamma, u);
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -298,14 +298,14 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
   constexpr int ZR = DIM == 3 ? Tl::R : 0;
   const int c0 = (ZR * Tl::TY + quarter + Tl::R) * Tl::TX + lane + Tl::R;
   {
-    const double ref = tile[part][c0];
-    double mx = 0.0;
-    for (int q = 0; q < M::P; q++) mx = fmax(mx, fabs(tile[part][c0 + sOfs[q]] - ref));
+    const float ref = tile[part][c0];
+    float mx = 0.0f;
+    for (int q = 0; q < M::P; q++) mx = fmaxf(mx, fabsf(__fsub_rn(tile[part][c0 + sOfs[q]], ref)));
     sSc[row][part] = ref;
-    sSc[row][2 + part] = 1.0 / (mx + kMlpFloor * fabs(ref) + 1e-300);
+    sSc[row][2 + part] = mlp_scale(mx, ref);
   }
   __syncthreads();
-  const double rc = sSc[row][0], pc = sSc[row][1], sr = sSc[row][2], sp = sSc[row][3];
+  const float rc = sSc[row][0], pc = sSc[row][1], sr = sSc[row][2], sp = sSc[row][3];
   const uint32_t aB = smem_u32(msm), bB = smem_u32(msm + C::OFF_B);
   constexpr uint32_t idesc = bf16_idesc<32>();
   bool ok = true;
@@ -322,12 +322,12 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
         for (int e = 0; e < 2; e++) {
           const int kk = ch * 8 + 2 * t + e;
           float x = 0.0f;
-          if (kk < M::P) x = (float)((tile[0][c0 + sOfs[kk]] - rc) * sr);
-          else if (kk < M::NI) x = (float)((tile[1][c0 + sOfs[kk - M::P]] - pc) * sp);
+          if (kk < M::P) x = mlp_feature(tile[0][c0 + sOfs[kk]], rc, sr);
+          else if (kk < M::NI) x = mlp_feature(tile[1][c0 + sOfs[kk - M::P]], pc, sp);
           x2[e] = live ? x : 0.0f;
         }
-        pk[t] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x2[0])) |
-                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x2[1])) << 16);
+        const __nv_bfloat162 b2 = __floats2bfloat162_rn(x2[0], x2[1]); // .x low half, .y high half
+        pk[t] = *reinterpret_cast<const uint32_t *>(&b2);
       }
       st_shared_v4(aB + cl * C::A_CH + row * 16, pk);
     }

@@ -2,9 +2,11 @@
 // per-block density / pressure tile its features are read from.
 //
 // Input: the normalised (2r+1)^d patch (r = 2) of density and pressure around a
-// cell, x = (q_k - q_c) / (max_k |q_k - q_c| + 1e-4 |q_c|) for q = rho, p, giving
-// 50 inputs in 2D and 250 in 3D (density first, patch cells in (z, y, x) order,
-// x fastest).  Network: NI -> 32 -> 32 -> 1, GELU after both hidden layers,
+// cell, giving 50 inputs in 2D and 250 in 3D (density first, patch cells in
+// (z, y, x) order, x fastest).  With q = rho or p (computed in FP64, rounded to
+// FP32) and every operation below in FP32:
+//   d_k = q_k - q_c,  s = 1 / (max_k |d_k| + 1e-4 |q_c|),  x_k = d_k s,
+// then rounded to BF16, the operand type of the network.  Network: NI -> 32 -> 32 -> 1, GELU after both hidden layers,
 // sigmoid output.  Weights are BF16 (raw uint16 at the C ABI), every sum
 // accumulates in FP32.  Weight layout (one flat array):
 //   W1 [32][NI], b1 [32], W2 [32][32], b2 [32], w3 [32], b3
@@ -45,7 +47,7 @@ __device__ __forceinline__ float gelu_grad(float x) {
 
 template <int DIM, int EQ>
 __device__ __forceinline__ void mlp_tile_fill(const double *__restrict__ U, const Grid &g, int64_t i0, int64_t j0,
-                                              int64_t k, double (*t)[MlpTile<DIM>::N]) {
+                                              int64_t k, float (*t)[MlpTile<DIM>::N]) {
   using Tl = MlpTile<DIM>;
   using E = Eos<EQ>;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -57,31 +59,40 @@ __device__ __forceinline__ void mlp_tile_fill(const double *__restrict__ U, cons
     double u[E::NV];
 #pragma unroll
     for (int v = 0; v < E::NV; v++) u[v] = Uc[v * g.pvol];
-    t[0][n] = u[DENS];
-    t[1][n] = E::pres(g.gamma, u);
+    t[0][n] = (float)u[DENS];
+    t[1][n] = (float)E::pres(g.gamma, u);
   }
 }
 
-// patch maxima and the two scale factors of a cell at block position (tx, ty)
+// 1 / (m + 1e-4 |q_c|), every operation rounded on its own (no contraction), so
+// the value is reproducible off the GPU
+__device__ __forceinline__ float mlp_scale(float m, float qc) {
+  return __fdiv_rn(1.0f, __fadd_rn(__fadd_rn(m, __fmul_rn(1e-4f, fabsf(qc))), 1e-30f));
+}
+
+// a feature: (q - q_c) s
+__device__ __forceinline__ float mlp_feature(float q, float qc, float s) { return __fmul_rn(__fsub_rn(q, qc), s); }
+
+// center values and scale factors of the two patches of a cell at block position (tx, ty)
 template <int DIM>
-__device__ __forceinline__ void mlp_scales(const double (*t)[MlpTile<DIM>::N], int tx, int ty, double &rc,
-                                           double &pc, double &sr, double &sp) {
+__device__ __forceinline__ void mlp_scales(const float (*t)[MlpTile<DIM>::N], int tx, int ty, float &rc,
+                                           float &pc, float &sr, float &sp) {
   using Tl = MlpTile<DIM>;
   constexpr int R = Tl::R, ZR = DIM == 3 ? R : 0;
   const int c0 = (ZR * Tl::TY + ty + R) * Tl::TX + tx + R;
   rc = t[0][c0];
   pc = t[1][c0];
-  double mr = 0.0, mp = 0.0;
+  float mr = 0.0f, mp = 0.0f;
   for (int dz = -ZR; dz <= ZR; dz++)
     for (int dy = -R; dy <= R; dy++)
 #pragma unroll
       for (int dx = -R; dx <= R; dx++) {
         const int n = c0 + (dz * Tl::TY + dy) * Tl::TX + dx;
-        mr = fmax(mr, fabs(t[0][n] - rc));
-        mp = fmax(mp, fabs(t[1][n] - pc));
+        mr = fmaxf(mr, fabsf(__fsub_rn(t[0][n], rc)));
+        mp = fmaxf(mp, fabsf(__fsub_rn(t[1][n], pc)));
       }
-  sr = 1.0 / (mr + kMlpFloor * fabs(rc) + 1e-300);
-  sp = 1.0 / (mp + kMlpFloor * fabs(pc) + 1e-300);
+  sr = mlp_scale(mr, rc);
+  sp = mlp_scale(mp, pc);
 }
 
 } // namespace kfvm

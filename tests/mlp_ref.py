@@ -28,7 +28,9 @@ def pressure(u, gamma, glm=False):
 
 
 def features(state, cfg, cells):
-    """Features of the given cells from an interior state (nv, n)."""
+    """Features of the given cells from an interior state (nv, n): density and
+    pressure in float64 rounded to float32, differences, maxima, scales and
+    products in float32 (the kernels' definition)."""
     dim = cfg.dim
     nz = cfg.nz if dim == 3 else 1
     shape = (nz, cfg.ny, cfg.nx)
@@ -51,21 +53,24 @@ def features(state, cfg, cells):
             w[ax] = (R, R)
             a = np.pad(a, w, mode=m)
         return a
-    rp, pp = pad(rho), pad(p)
+    # density and pressure in FP64, rounded to FP32; the rest in FP32
+    rp, pp = pad(rho).astype(np.float32), pad(p).astype(np.float32)
     zr = R if dim == 3 else 0
-    out = np.empty((len(cells), 2 * (2 * R + 1) ** dim))
+    out = np.empty((len(cells), 2 * (2 * R + 1) ** dim), dtype=np.float32)
+    f4 = np.float32(1e-4)
+    tiny = np.float32(1e-30)
     for n, c in enumerate(cells):
         k, rem = divmod(int(c), cfg.nx * cfg.ny)
         j, i = divmod(rem, cfg.nx)
         kk = k + zr
         sl = (slice(kk - zr, kk + zr + 1), slice(j, j + 2 * R + 1), slice(i, i + 2 * R + 1))
         pr, pq = rp[sl].ravel(), pp[sl].ravel()
-        rc, pc = rho[k, j, i], p[k, j, i]
+        rc, pc = rp[kk, j + R, i + R], pp[kk, j + R, i + R]
         dr, dq = pr - rc, pq - pc
-        sr = 1.0 / (np.abs(dr).max() + 1e-4 * abs(rc) + 1e-300)
-        sq = 1.0 / (np.abs(dq).max() + 1e-4 * abs(pc) + 1e-300)
-        out[n] = np.concatenate([(dr * sr).astype(np.float32), (dq * sq).astype(np.float32)])
-    return out.astype(np.float32)
+        sr = np.float32(1.0) / (np.abs(dr).max() + f4 * np.abs(rc) + tiny)
+        sq = np.float32(1.0) / (np.abs(dq).max() + f4 * np.abs(pc) + tiny)
+        out[n] = np.concatenate([dr * sr, dq * sq])
+    return out
 
 
 def unpack(w_bf16, ni):
