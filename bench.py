@@ -188,10 +188,11 @@ def algorithmic_bytes(cls, cfg):
     nfaces = sum((cfg.nx + (k == 0)) * (cfg.ny + (k == 1)) * ((cfg.nz if d == 3 else 1) + (k == 2))
                  for k in range(d))
     per_cell = {
-        # U in; own face states, KXRCF indicator per own face point, status out
-        "recon": nv * 8 + nf * nqf * (nv + 1) * 8 + 1 + ((nqc * nv * 8 + 16) if src else 0),
+        # U in; own face states (8-byte reals), KXRCF indicator (4-byte) per own face
+        # point, status out
+        "recon": nv * 8 + nf * nqf * (nv * 8 + 4) + 1 + ((nqc * nv * 8 + 16) if src else 0),
         # indicators (each face point once), U, theta in; flag out
-        "flag": nf * nqf * 8 + nv * 8 + 8 + 1,
+        "flag": nf * nqf * 4 + nv * 8 + 8 + 1,
         # flag, set, status in; applied out (theta / heavy-list writes are partial)
         "compact": 4,
         # Riemann fluxes, U, Uprev, Uhat in; U', Uhat out
