@@ -230,6 +230,13 @@ int kfvm_set_indicator(kfvm_solver *s, int32_t indicator);
  * KFVM_ERR_ARG if the device is not compute capability 10.x. */
 int kfvm_set_precision(kfvm_solver *s, int32_t precision);
 
+/* Self-test of the bounded waits of the tensor-core kernels (no reference
+ * counterpart): one thread waits on an mbarrier that nothing completes, with a
+ * limit of limit_s seconds (0 < limit_s <= 1), and reports that it gave up and
+ * how long it waited.  The tensor-core kernels use the same wait (1 s limit) and
+ * turn a timeout into KFVM_ERR_CUDA on the host instead of a hang. */
+int kfvm_selftest_wait(double limit_s, int32_t *gave_up, double *waited_s);
+
 /* ---- Learned troubled-cell indicator (KFVM_IND_MLP) -----------------------
  * No reference counterpart: it replaces the KXRCF selector (WenoSelect_K,
  * src/numeric/Numeric_K.H:292-398) with a 2x32 MLP over the normalised 5^d

@@ -1118,6 +1118,19 @@ int kfvm_mlp_stats(kfvm_solver *s, int64_t *out6) {
   return KFVM_OK;
 }
 
+int kfvm_selftest_wait(double limit_s, int32_t *gave_up, double *waited_s) {
+  if (!(limit_s > 0.0 && limit_s <= 1.0) || !gave_up || !waited_s) return fail(KFVM_ERR_ARG, "bad argument");
+  unsigned long long *d = nullptr, h[2] = {0, 0};
+  cudaError_t e = cudaMalloc((void **)&d, sizeof(h));
+  if (e == cudaSuccess) e = kfvm::launch_wait_probe((uint64_t)(limit_s * 1e9), d, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return set_err_cuda(e, "wait probe");
+  *gave_up = (int32_t)h[0];
+  *waited_s = (double)h[1] * 1e-9;
+  return KFVM_OK;
+}
+
 int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
   if (!s || !out || dir < 0 || dir >= s->dim) return fail(KFVM_ERR_ARG, "bad argument");
   const kfvm::Grid &g = s->g;

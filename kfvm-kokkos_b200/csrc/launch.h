@@ -38,6 +38,8 @@ cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const 
 cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
                             double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
                             DevScalars *sc, cudaStream_t s);
+// self-test of the bounded mbarrier wait: out[0] = gave up, out[1] = ns waited
+cudaError_t launch_wait_probe(uint64_t limit_ns, unsigned long long *out, cudaStream_t s);
 // host: split the [cell][row] linear weights of S into the TF32 B-operand tables
 void fill_tc_weights(DevStencil &S, int dim, int nrows);
 // host: the same weights as FP64 MMA B fragments

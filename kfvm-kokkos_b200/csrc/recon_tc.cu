@@ -310,6 +310,25 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                  : "memory");
 }
 
+// Self-test of the bounded wait: one block waits on an mbarrier that nothing
+// arrives on, with the given limit, and records whether it gave up and how long
+// it waited.  The kernel always returns.
+__global__ void wait_probe_kernel(uint64_t limit_ns, unsigned long long *out) {
+  __shared__ uint64_t bar;
+  const uint32_t b = smem_u32(&bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  const uint64_t t0 = global_ns();
+  const bool done = mbar_wait(b, 0u, limit_ns);
+  out[0] = done ? 0ull : 1ull;
+  out[1] = global_ns() - t0;
+}
+
+cudaError_t launch_wait_probe(uint64_t limit_ns, unsigned long long *out, cudaStream_t s) {
+  wait_probe_kernel<<<1, 1, 0, s>>>(limit_ns, out);
+  return cudaGetLastError();
+}
+
 template <int DIM, int EQ>
 static cudaError_t recon_tc_launch(const double *U, const Grid &g, const DevStencil *S, int wantInd,
                                    double *const *F, float *const *W, double *src, uint8_t *status,

@@ -61,7 +61,7 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 
 // bounded wait for the completion of the mbarrier phase with the given parity
 constexpr uint64_t kTcWaitNs = 1000000000ull;
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns = kTcWaitNs) {
   const uint64_t t0 = global_ns();
   for (uint32_t it = 0; it < (1u << 26); ++it) {
     uint32_t done;
@@ -73,7 +73,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((it & 63u) == 63u && global_ns() - t0 > kTcWaitNs) return false;
+    if ((it & 63u) == 63u && global_ns() - t0 > limit_ns) return false;
   }
   return false;
 }

@@ -51,6 +51,7 @@ def lib():
         L.kfvm_set_time.argtypes = [P, D, D]
         L.kfvm_set_indicator.argtypes = [P, I32]
         L.kfvm_set_precision.argtypes = [P, I32]
+        L.kfvm_selftest_wait.argtypes = [D, C.POINTER(I32), C.POINTER(D)]
         L.kfvm_mlp_num_weights.argtypes = [I32]
         L.kfvm_mlp_init_weights.argtypes = [P, C.c_uint64]
         L.kfvm_mlp_set_weights.argtypes = [P, P, I64]
@@ -85,6 +86,13 @@ def err_est_noalloc(eq, u_dev_ptr, uhat_dev_ptr, n, atol, rtol, out_dev_ptr, str
     _check(lib().kfvm_err_est_noalloc(int(eq), C.c_void_p(u_dev_ptr), C.c_void_p(uhat_dev_ptr),
                                       int(n), float(atol), float(rtol), C.c_void_p(out_dev_ptr),
                                       C.c_void_p(stream)), "kfvm_err_est_noalloc")
+
+
+def selftest_wait(limit_s):
+    """kfvm_selftest_wait: (gave_up, seconds waited) of a bounded wait that cannot complete."""
+    g, w = C.c_int32(), C.c_double()
+    _check(lib().kfvm_selftest_wait(float(limit_s), C.byref(g), C.byref(w)), "kfvm_selftest_wait")
+    return bool(g.value), w.value
 
 
 def stencil(cfg):
