@@ -707,7 +707,7 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 // points, points along threadIdx.y), so each thread keeps only one solve live and
 // more warps hide the FP64 latency.  The quadrature-weighted sum over a face's
 // points goes through shared memory in point order, and the max wave speed
-// through a warp maximum and one atomic per warp.
+// through a warp maximum and an atomic only from warps that raise it.
 template <int DIM, int EQ, int D>
 __global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4), EQ == EQ_GLM ? 1 : (DIM == 2 ? 16 : 8))
     riemann_kernel(const double *__restrict__ F, double *__restrict__ G, Grid g,

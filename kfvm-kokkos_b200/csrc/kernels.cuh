@@ -114,8 +114,15 @@ __device__ __forceinline__ int64_t pidx(const Grid &g, int64_t i, int64_t j, int
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long *a, double v) {
   // non-negative doubles order like their bit patterns; NaN is ignored as in the
-  // reference's "vq > maxVel ? vq : maxVel"
-  if (v >= 0.0) atomicMax(a, (unsigned long long)__double_as_longlong(v));
+  // reference's "vq > maxVel ? vq : maxVel".  The maximum only grows during a
+  // launch, so a value not above a plain read of it cannot raise it: skipping
+  // those spares the same-address atomics that serialise in L2 (one per warp over
+  // millions of warps doubled the Riemann kernel's time once the wave speeds
+  // varied from warp to warp).
+  if (v >= 0.0) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    if (b > *(volatile const unsigned long long *)a) atomicMax(a, b);
+  }
 }
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
