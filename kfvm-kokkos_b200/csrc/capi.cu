@@ -128,6 +128,7 @@ struct kfvm_solver {
   double *Uhat = nullptr, *Utmp = nullptr, *K = nullptr;
   double *F[3] = {nullptr, nullptr, nullptr}, *G[3] = {nullptr, nullptr, nullptr};
   double *src = nullptr, *theta = nullptr, *part = nullptr;
+  double *io = nullptr; // host-order interior state for set/get (allocated at first use)
   uint8_t *flag = nullptr, *wset = nullptr, *applied = nullptr;
   uint32_t *heavy = nullptr; // compacted WENO / limiter cell list (one slot per cell)
   float *W[3] = {nullptr, nullptr, nullptr};  // KXRCF indicator (FP32 approximation) per own face slot and point
@@ -354,8 +355,7 @@ int prime(kfvm_solver *s) {
   const int64_t n = s->g.n;
   CK(cudaMemsetAsync(s->wset, 0, n, s->stream));
   CK(cudaMemsetAsync(s->sc, 0, sizeof(kfvm::DevScalars), s->stream));
-  std::vector<double> one(n, 1.0);
-  CK(cudaMemcpyAsync(s->theta, one.data(), n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(kfvm::launch_fill(s->theta, n, 1.0, s->stream));
   int rc = eval_into_K(s, s->iPrev);
   if (rc) return rc;
   CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(kfvm::DevScalars), cudaMemcpyDeviceToHost, s->stream));
@@ -489,34 +489,18 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
   return KFVM_OK;
 }
 
-// host SoA interior <-> padded device buffer, one strided 3D copy per variable
-cudaMemcpy3DParms interior_copy(kfvm_solver *s, int b, int v, double *host, bool toDevice) {
-  const kfvm::Grid &g = s->g;
-  cudaMemcpy3DParms p;
-  std::memset(&p, 0, sizeof(p));
-  cudaPitchedPtr hp = make_cudaPitchedPtr(host + (size_t)v * g.n, g.nx * sizeof(double), g.nx, g.ny);
-  cudaPitchedPtr dp = make_cudaPitchedPtr(s->Ub[b] + (size_t)v * g.pvol, g.px * sizeof(double), g.px, g.py);
-  const cudaPos dpos = make_cudaPos(kfvm::kRad * sizeof(double), kfvm::kRad, g.rz);
-  if (toDevice) {
-    p.srcPtr = hp;
-    p.dstPtr = dp;
-    p.dstPos = dpos;
-    p.kind = cudaMemcpyHostToDevice;
-  } else {
-    p.srcPtr = dp;
-    p.srcPos = dpos;
-    p.dstPtr = hp;
-    p.kind = cudaMemcpyDeviceToHost;
-  }
-  p.extent = make_cudaExtent(g.nx * sizeof(double), g.ny, g.nz);
-  return p;
+// the host-order interior state (variable, k, j, i) travels as one contiguous copy
+// through a device staging buffer; a kernel moves it to or from the padded layout
+// (strided 3D copies of 2 KB rows ran at a fraction of the link bandwidth)
+int ensure_io(kfvm_solver *s) {
+  if (!s->io) CK(cudaMalloc(&s->io, (size_t)s->g.n * s->nv * sizeof(double)));
+  return KFVM_OK;
 }
 
 int upload_state(kfvm_solver *s, int b, const double *u) {
-  for (int v = 0; v < s->nv; v++) {
-    cudaMemcpy3DParms p = interior_copy(s, b, v, const_cast<double *>(u), true);
-    CK(cudaMemcpy3DAsync(&p, s->stream));
-  }
+  if (int rc = ensure_io(s)) return rc;
+  CK(cudaMemcpyAsync(s->io, u, (size_t)s->g.n * s->nv * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(kfvm::launch_interior(s->Ub[b], s->io, s->g, s->nv, true, s->stream));
   return KFVM_OK;
 }
 
@@ -719,6 +703,7 @@ void kfvm_destroy(kfvm_solver *s) {
   cudaFree(s->lamvel);
   cudaFree(s->src);
   cudaFree(s->theta);
+  cudaFree(s->io);
   cudaFree(s->flag);
   cudaFree(s->wset);
   cudaFree(s->applied);
@@ -769,10 +754,9 @@ int kfvm_set_state(kfvm_solver *s, const double *u) {
 
 int kfvm_get_state(kfvm_solver *s, double *u) {
   if (!s || !u) return fail(KFVM_ERR_ARG, "null argument");
-  for (int v = 0; v < s->nv; v++) {
-    cudaMemcpy3DParms p = interior_copy(s, s->iCur, v, u, false);
-    CK(cudaMemcpy3DAsync(&p, s->stream));
-  }
+  if (int rc = ensure_io(s)) return rc;
+  CK(kfvm::launch_interior(s->Ub[s->iCur], s->io, s->g, s->nv, false, s->stream));
+  CK(cudaMemcpyAsync(u, s->io, (size_t)s->g.n * s->nv * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return KFVM_OK;
 }

@@ -2,6 +2,7 @@
 // See kernels.cuh for the stage structure and the HBM layouts.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <type_traits>
@@ -1315,6 +1316,37 @@ int64_t stage_blocks(const Grid &g) {
     if ((DIM_) == 3 && (EQ_) == EQ_GLM) return Launch<3, EQ_GLM>::CALL;               \
     return cudaErrorInvalidValue;                                                     \
   } while (0)
+
+// host-order interior (variable, k, j, i; i fastest) <-> padded device layout:
+// one thread per cell of a row, rows (j, k) and variables over the grid
+template <bool TO_PADDED>
+__global__ void __launch_bounds__(256) interior_kernel(double *__restrict__ Up, double *__restrict__ flat, Grid g) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= g.nx) return;
+  const int64_t j = blockIdx.y, k = blockIdx.z % g.nz, v = blockIdx.z / g.nz;
+  const int64_t f = v * g.n + (k * g.ny + j) * g.nx + i;
+  const int64_t p = v * g.pvol + pidx(g, i, j, k);
+  if (TO_PADDED) Up[p] = flat[f];
+  else flat[f] = Up[p];
+}
+
+__global__ void __launch_bounds__(256) fill_kernel(double *__restrict__ p, int64_t n, double val) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    p[t] = val;
+}
+
+cudaError_t launch_interior(double *Up, double *flat, const Grid &g, int nv, bool toPadded, cudaStream_t s) {
+  const dim3 grid((unsigned)((g.nx + 255) / 256), (unsigned)g.ny, (unsigned)(g.nz * nv));
+  if (toPadded) interior_kernel<true><<<grid, 256, 0, s>>>(Up, flat, g);
+  else interior_kernel<false><<<grid, 256, 0, s>>>(Up, flat, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill(double *p, int64_t n, double val, cudaStream_t s) {
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);
+  fill_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, s>>>(p, n, val);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s) {
   KFVM_DISPATCH(dim, eq, bc(U, g, s));

@@ -28,6 +28,10 @@ struct StageArgs {
 
 int64_t stage_blocks(const Grid &g);
 cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s);
+// interior state between the host order (variable, k, j, i) in a flat device
+// buffer and the padded layout; one launch for all variables
+cudaError_t launch_interior(double *Up, double *flat, const Grid &g, int nv, bool toPadded, cudaStream_t s);
+cudaError_t launch_fill(double *p, int64_t n, double val, cudaStream_t s);
 // stage front end: linear states + KXRCF indicator + limiter bound status,
 // KXRCF flags, WENO decision / heavy-list compaction, heavy cells
 cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
