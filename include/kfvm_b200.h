@@ -237,6 +237,13 @@ int kfvm_set_precision(kfvm_solver *s, int32_t precision);
  * turn a timeout into KFVM_ERR_CUDA on the host instead of a hang. */
 int kfvm_selftest_wait(double limit_s, int32_t *gave_up, double *waited_s);
 
+/* Self-test of the FP64 reciprocal used by the Riemann solvers (Newton-Raphson
+ * refinement of the hardware approximation): over n pseudo-random doubles with
+ * exponents in [-300, 300] and both signs, the largest distance in ulps between
+ * it and the IEEE quotient 1/y, and the largest relative difference between
+ * x * rcp(y) and x / y.  No reference counterpart (the reference divides). */
+int kfvm_selftest_rcp(int64_t n, uint64_t seed, int64_t *max_ulp, double *max_rel_quot);
+
 /* ---- Learned troubled-cell indicator (KFVM_IND_MLP) -----------------------
  * No reference counterpart: it replaces the KXRCF selector (WenoSelect_K,
  * src/numeric/Numeric_K.H:292-398) with a 2x32 MLP over the normalised 5^d

@@ -1115,6 +1115,22 @@ int kfvm_selftest_wait(double limit_s, int32_t *gave_up, double *waited_s) {
   return KFVM_OK;
 }
 
+int kfvm_selftest_rcp(int64_t n, uint64_t seed, int64_t *max_ulp, double *max_rel_quot) {
+  if (n <= 0 || n > ((int64_t)1 << 32) || !max_ulp || !max_rel_quot) return fail(KFVM_ERR_ARG, "bad argument");
+  unsigned long long *d = nullptr, h[2] = {0, 0};
+  cudaError_t e = cudaMalloc((void **)&d, sizeof(h));
+  if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(h));
+  if (e == cudaSuccess) e = kfvm::launch_rcp_probe(n, seed, d, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return set_err_cuda(e, "reciprocal probe");
+  *max_ulp = (int64_t)h[0];
+  double q;
+  std::memcpy(&q, &h[1], sizeof(q));
+  *max_rel_quot = q;
+  return KFVM_OK;
+}
+
 int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
   if (!s || !out || dir < 0 || dir >= s->dim) return fail(KFVM_ERR_ARG, "bad argument");
   const kfvm::Grid &g = s->g;

@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(128)
               for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
               if (wantInd)
                 (DIM == 3 ? W[t < 3 ? t : 0] : W[d])[(int64_t)(slot * T::NQF + q) * nf + fidx] =
-                    Eos<EQ>::weno_approx_rp(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
+                    Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
               if constexpr (T::SRC) {
                 // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
                 const double vv = fabs(st[MOMX] / st[DENS]);
@@ -239,8 +239,9 @@ __global__ void __launch_bounds__(128)
 // cell's faces over the cell value; the outer slot of a boundary face follows
 // setFaceBCs (periodic partner face, or the inner slot at an outflow boundary).
 //
-// The face indicators arrive as FP32 approximations (Eos::weno_approx, relative
-// error < kWenoApproxEps).  The decision is taken from them only when it is certain:
+// The face indicators arrive in FP32 (Eos::weno_store: in 3D the hardware
+// approximation, relative error < kWenoApproxEps; in 2D the FP64 value rounded,
+// < kWenoRoundEps).  The decision is taken from them only when it is certain:
 // the exact jump lies within 2 eps max|w| (+ the FP32 rounding of the difference)
 // of the approximate one, and the cell value is exact FP64.  Otherwise (a cell near
 // the threshold, or a NaN marker) every face-point indicator is recomputed exactly
@@ -308,7 +309,8 @@ __global__ void __launch_bounds__(128)
       const double wc = Eos<EQ>::weno(g.gamma, uAv);
       bool certain = false;
       if (!bad && wc > 0.0 && isfinite(wc)) {
-        const double margin = 2.01 * kWenoApproxEps * (double)wmax + 2e-7 * (double)jf + 1e-300;
+        const double eps = DIM == 2 ? kWenoRoundEps : kWenoApproxEps;
+        const double margin = 2.01 * eps * (double)wmax + 2e-7 * (double)jf + 1e-300;
         const double lo = ((double)jf - margin) / wc, hi = ((double)jf + margin) / wc;
         if (lo >= wThresh) {
           f = true;
@@ -1333,6 +1335,33 @@ __global__ void __launch_bounds__(256) interior_kernel(double *__restrict__ Up, 
 __global__ void __launch_bounds__(256) fill_kernel(double *__restrict__ p, int64_t n, double val) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
     p[t] = val;
+}
+
+// accuracy probe of rcp_nr against the IEEE reciprocal and quotient
+__global__ void __launch_bounds__(256) rcp_probe_kernel(int64_t n, uint64_t seed, unsigned long long *out) {
+  unsigned long long worst = 0, worstQ = 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t h = mix64(seed ^ (uint64_t)t), h2 = mix64(h);
+    // mantissa from the hash, exponent uniform in [-300, 300], random sign
+    const double m = 1.0 + (double)(h >> 12) * 0x1.0p-52;
+    const int ex = (int)(h2 % 601) - 300;
+    const double y = ((h2 >> 32) & 1 ? -1.0 : 1.0) * scalbn(m, ex);
+    const double x = 1.0 + (double)(h2 >> 12) * 0x1.0p-52;
+    const double r = rcp_nr(y), q = 1.0 / y;
+    const long long d = __double_as_longlong(r) - __double_as_longlong(q);
+    const unsigned long long du = (unsigned long long)(d < 0 ? -d : d);
+    worst = du > worst ? du : worst;
+    const double rel = fabs(x * r - x / y) / fabs(x / y);
+    const unsigned long long rq = (unsigned long long)__double_as_longlong(rel);
+    worstQ = rq > worstQ ? rq : worstQ;
+  }
+  atomicMax(&out[0], worst);
+  atomicMax(&out[1], worstQ);
+}
+
+cudaError_t launch_rcp_probe(int64_t n, uint64_t seed, unsigned long long *out, cudaStream_t s) {
+  rcp_probe_kernel<<<148 * 4, 256, 0, s>>>(n, seed, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_interior(double *Up, double *flat, const Grid &g, int nv, bool toPadded, cudaStream_t s) {

@@ -32,6 +32,9 @@ cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s)
 // buffer and the padded layout; one launch for all variables
 cudaError_t launch_interior(double *Up, double *flat, const Grid &g, int nv, bool toPadded, cudaStream_t s);
 cudaError_t launch_fill(double *p, int64_t n, double val, cudaStream_t s);
+// rcp_nr accuracy probe: out[0] = max ulp distance to 1/y, out[1] = bits of the
+// largest relative difference of x * rcp_nr(y) from x / y
+cudaError_t launch_rcp_probe(int64_t n, uint64_t seed, unsigned long long *out, cudaStream_t s);
 // stage front end: linear states + KXRCF indicator + limiter bound status,
 // KXRCF flags, WENO decision / heavy-list compaction, heavy cells
 cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,

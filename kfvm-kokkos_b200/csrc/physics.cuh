@@ -28,6 +28,24 @@ enum { RS_LLF = 0, RS_HLL = 1, RS_HLLC = 2 };
 // (<= 5.5e-6), i.e. <= 1.8e-5 x ln 2 = 1.2e-5 relative after ex2; ex2.approx
 // (2^-22) and the FP32 roundings of p and rho add < 4e-7.
 constexpr double kWenoApproxEps = 2e-5;
+// bound on the relative error of Eos::weno_round: one rounding to FP32 (2^-24)
+// plus a few FP64 ulps of the pressure, the power and the quotient
+constexpr double kWenoRoundEps = 6.0e-8;
+
+// Reciprocal by Newton-Raphson refinement (Flynn 1970; Markstein 1990) of the
+// hardware's approximate FP64 reciprocal (PTX rcp.approx.ftz.f64): each step
+// e = 1 - y r, r = r + r e squares the relative error, and two steps bring the
+// seed to within about one ulp of 1/y for normal y (tests compare it with the
+// IEEE quotient).  It has no special-case branches: y = 0, infinite or subnormal
+// gives NaN or infinity, which only states that are already unphysical reach.
+__device__ __forceinline__ double rcp_nr(double y) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(y));
+  double e = fma(-y, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-y, r, 1.0);
+  return fma(r, e, r);
+}
 
 template <int EQ>
 struct Eos {
@@ -81,7 +99,24 @@ struct Eos {
     float l2, r;
     asm("lg2.approx.f32 %0, %1;" : "=f"(l2) : "f"((float)rho));
     asm("ex2.approx.f32 %0, %1;" : "=f"(r) : "f"(-(float)g * l2));
-    return (float)p * r;
+    const float w = (float)p * r;
+    // an FP32 underflow (or overflow) of the product voids the bound
+    return fabsf(w) >= 1.17549435e-38f ? w : __int_as_float(0x7fc00000);
+  }
+  // The indicator computed in FP64 as the reference does and rounded once to FP32
+  // (relative error below kWenoRoundEps), or NaN where FP32 cannot hold it
+  __device__ __forceinline__ static float weno_round_rp(double g, double rho, double p) {
+    const float w = __double2float_rn(p / pow(rho, g));
+    return fabsf(w) >= 1.17549435e-38f && fabsf(w) <= 3.0e38f ? w : __int_as_float(0x7fc00000);
+  }
+  // the FP32 form the reconstruction stores: in 2D (8 face points per cell, where
+  // the power is cheap next to the rest and fine grids put smooth cells' jumps
+  // close to the threshold) the rounded FP64 value; in 3D (24 points) the
+  // hardware approximation
+  template <int DIM>
+  __device__ __forceinline__ static float weno_store(double g, double rho, double p) {
+    if constexpr (DIM == 2) return weno_round_rp(g, rho, p);
+    else return weno_approx_rp(g, rho, p);
   }
   __device__ __forceinline__ static double positivity(const double *U) {
     if constexpr (EQ == EQ_GLM) {
@@ -182,8 +217,10 @@ struct Eos {
   // Riemann solve at one face point in direction dir; returns max(|sL|,|sR|).
   // Euler / Navier-Stokes: Batten/Roe speed estimates (Hydro_Riemann.H:26-80) and,
   // for HLLC, the low-Mach / shear-corrected star fluxes (Hydro_Riemann.H:82-187),
-  // with each repeated divisor (rho, the Roe weight sum, sL - sS, sR - sS) inverted
-  // once: about a third of the FP64 divisions of the literal form.
+  // with each repeated divisor (rho, the Roe weight sum, sL - sS, sR - sS, psL - psR)
+  // inverted once by rcp_nr, the Roe weights from one root of rR / rL and the Mach
+  // estimate from one root: 7 reciprocals and 6 roots where the literal form
+  // divides about 30 times.
   __device__ __forceinline__ static double solve(int rs, double g, double ch, int dir,
                                                  const double *uL, const double *uR,
                                                  double *F) {
@@ -194,18 +231,18 @@ struct Eos {
     double sL, sR, sMax;
     if constexpr (EQ != EQ_GLM) {
       const double rL = uL[DENS], rR = uR[DENS];
-      const double iLR = 1.0 / (rL * rR), iL = rR * iLR, iR = rL * iLR;
+      const double iLR = rcp_nr(rL * rR), iL = rR * iLR, iR = rL * iLR;
       cons2prim_r(g, uL, iL, vL);
       cons2prim_r(g, uR, iR, vR);
       const double pL = vL[4], pR = vR[4];
       const double a2L = g * pL * iL, a2R = g * pR * iR;
       const double aL = sqrt(a2L), aR = sqrt(a2R);
       const double hL = (uL[ETOT] + pL) * iL, hR = (uR[ETOT] + pR) * iR;
-      const double sqL = sqrt(rL), sqR = sqrt(rR), isq = 1.0 / (sqL + sqR);
-      const double uTil = (vL[vo[0]] * sqL + vR[vo[0]] * sqR) * isq,
-                   vTil = (vL[vo[1]] * sqL + vR[vo[1]] * sqR) * isq,
-                   wTil = (vL[vo[2]] * sqL + vR[vo[2]] * sqR) * isq,
-                   hTil = (hL * sqL + hR * sqR) * isq;
+      // Roe weights sqrt(rL) / (sqrt(rL) + sqrt(rR)) = 1 / (1 + sqrt(rR / rL)) and
+      // sqrt(rR) / (...) = sqrt(rR / rL) / (1 + sqrt(rR / rL)): one root, one reciprocal
+      const double tq = sqrt(rR * iL), wL = rcp_nr(1.0 + tq), wR = tq * wL;
+      const double uTil = vL[vo[0]] * wL + vR[vo[0]] * wR, vTil = vL[vo[1]] * wL + vR[vo[1]] * wR,
+                   wTil = vL[vo[2]] * wL + vR[vo[2]] * wR, hTil = hL * wL + hR * wR;
       const double vsqTil = uTil * uTil + vTil * vTil + wTil * wTil;
       const double aTil = sqrt((g - 1.0) * (hTil - 0.5 * vsqTil));
       sL = fmin(vL[vo[0]] - aL, uTil - aTil);
@@ -214,23 +251,26 @@ struct Eos {
       if (rs == RS_HLLC) {
         const double vsqL = vL[1] * vL[1] + vL[2] * vL[2] + vL[3] * vL[3];
         const double vsqR = vR[1] * vR[1] + vR[2] * vR[2] + vR[3] * vR[3];
-        // max of the two Mach numbers: sqrt is monotone, so one root of the larger square
-        double M = sqrt(fmax(vsqL / a2L, vsqR / a2R));
+        // max of the two Mach numbers max(|v|^2 / a^2) = max(vsqL a2R, vsqR a2L) / (a2L a2R):
+        // one root and one reciprocal of aL aR
+        double M = sqrt(fmax(vsqL * a2R, vsqR * a2L)) * rcp_nr(aL * aR);
         const double uLn = vL[vo[0]], uRn = vR[vo[0]];
         const double psL = rL * (sL - uLn), psR = rR * (sR - uRn);
-        const double sS = ((pR - pL) + (psL * uLn - psR * uRn)) / (psL - psR);
+        // sS and psR psL / (psR - psL) share the reciprocal of psL - psR
+        const double iD = rcp_nr(psL - psR);
+        const double sS = ((pR - pL) + (psL * uLn - psR * uRn)) * iD;
         const double pS = 0.5 * ((pL + pR) + psL * (sS - uLn) + psR * (sS - uRn));
-        const double dLR = 1.0 / ((sL - sS) * (sR - sS)), dL = (sR - sS) * dLR, dR = (sL - sS) * dLR;
+        const double dLR = rcp_nr((sL - sS) * (sR - sS)), dL = (sR - sS) * dLR, dR = (sL - sS) * dLR;
         const double sFacL = sS * dL, sFacR = sS * dR;
         const double uJump = uRn - uLn, vJump = vR[vo[1]] - vL[vo[1]], wJump = vR[vo[2]] - vL[vo[2]];
-        const double psiFac = psR * psL / (psR - psL);
-        const double presRat = fmin(pL, pR) / fmax(pL, pR);
+        const double psiFac = -(psR * psL) * iD;
+        const double presRat = fmin(1.0, fmin(pL, pR) * rcp_nr(fmax(pL, pR)));
         // presRat^M (pressure ratio in (0, 1]) as exp(M log presRat); exactly 0 for equal pressures
-        const double gFac = presRat == 1.0 ? 0.0 : 1.0 - exp(M * log(presRat));
+        const double gFac = pL == pR ? 0.0 : 1.0 - exp(M * log(presRat));
         const double shFacL = psiFac * gFac * sL * dL, shFacR = psiFac * gFac * sR * dR;
         M = fmin(M, 1.0);
         const double omm = 1.0 - M * M;
-        const double fM = M * sqrt(4.0 + omm * omm) / (1.0 + M * M);
+        const double fM = M * sqrt(4.0 + omm * omm) * rcp_nr(1.0 + M * M);
         const double pFacL = psiFac * (fM - 1.0) * uJump + sL * pS * dL;
         const double pFacR = psiFac * (fM - 1.0) * uJump + sR * pS * dR;
         if (0 <= sL) {
@@ -263,8 +303,9 @@ struct Eos {
       sL = -sMax;
       sR = sMax;
     }
-    const double tR = (fmin(0.0, sR) - fmin(0.0, sL)) / (sR - sL), tL = 1.0 - tR;
-    const double tD = 0.5 * (sR * fabs(sL) - sL * fabs(sR)) / (sR - sL);
+    const double iS = rcp_nr(sR - sL);
+    const double tR = (fmin(0.0, sR) - fmin(0.0, sL)) * iS, tL = 1.0 - tR;
+    const double tD = 0.5 * (sR * fabs(sL) - sL * fabs(sR)) * iS;
     double FR[NV];
     flux(ch, vo, bo, uL, vL, F);
     flux(ch, vo, bo, uR, vR, FR);

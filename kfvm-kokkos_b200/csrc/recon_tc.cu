@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                 for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
                 if (wantInd)
                   (d == 0 ? W0 : (d == 1 ? W1 : W2))[face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] =
-                      Eos<EQ>::weno_approx_rp(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
+                      Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
                 if constexpr (T::SRC) {
                   // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
                   const double vv = fabs(st[MOMX] / st[DENS]);

@@ -52,6 +52,7 @@ def lib():
         L.kfvm_set_indicator.argtypes = [P, I32]
         L.kfvm_set_precision.argtypes = [P, I32]
         L.kfvm_selftest_wait.argtypes = [D, C.POINTER(I32), C.POINTER(D)]
+        L.kfvm_selftest_rcp.argtypes = [I64, C.c_uint64, C.POINTER(I64), C.POINTER(D)]
         L.kfvm_mlp_num_weights.argtypes = [I32]
         L.kfvm_mlp_init_weights.argtypes = [P, C.c_uint64]
         L.kfvm_mlp_set_weights.argtypes = [P, P, I64]
@@ -93,6 +94,14 @@ def selftest_wait(limit_s):
     g, w = C.c_int32(), C.c_double()
     _check(lib().kfvm_selftest_wait(float(limit_s), C.byref(g), C.byref(w)), "kfvm_selftest_wait")
     return bool(g.value), w.value
+
+
+def selftest_rcp(n=1 << 24, seed=5):
+    """kfvm_selftest_rcp: (max ulp distance of the Riemann reciprocal from 1/y,
+    max relative difference of x * rcp(y) from x / y) over n random doubles."""
+    u, q = C.c_int64(), C.c_double()
+    _check(lib().kfvm_selftest_rcp(int(n), int(seed), C.byref(u), C.byref(q)), "kfvm_selftest_rcp")
+    return u.value, q.value
 
 
 def stencil(cfg):
