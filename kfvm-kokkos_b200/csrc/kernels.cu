@@ -83,19 +83,23 @@ constexpr uint32_t kHeavyCell = 0x3fffffffu;
 // the FP64 MMA of sm_100a; tcgen05 has no FP64 kind).  Per warp: one row of 32 cells
 // of the block, in 4 groups of 8 cells.  For one group and variable v,
 //   D[cell][row] = sum_k A[cell][k] B[k][row],  A = U(cell + offset k), B = weights,
-// K runs over the stencil in steps of 4 (zero padded), N over the weight rows in
-// tiles of 8; each DMMA does 256 FMAs where the scalar form issues 8 DFMAs.  The
-// sum over stencil cells keeps its order in steps of four.  Lane l holds
+// K runs over the stencil in steps of 4, N over the weight rows in tiles of 8;
+// each DMMA does 256 FMAs where the scalar form issues 8 DFMAs.  The sum over
+// stencil cells keeps its order in steps of four.  Lane l holds
 // D[cell l/4][rows 2(l%4), 2(l%4)+1] of every N tile, i.e. the full state (all
 // variables) of 2 NT face / interior points of its cell, and finishes them in FP64:
 // positivity pre-check, indicator, stores.  The four lanes of a cell combine their
 // in-bounds tests and GLM speed maxima by shuffles.
+// The stencil has 4m + 1 cells (13 in 2D, 33 in 3D): the first 4m go through the
+// MMAs in m K-steps and the last one is added in the epilogue by one FMA per row
+// and variable, which spares a K-step that would be three quarters padding.
 template <int DIM, int EQ>
 struct DmmaShape {
   static constexpr int NR = LinRows<DIM, EQ>::NROWS;
   static constexpr int NT = (NR + 7) / 8;
-  static constexpr int NK = (Cfg<DIM, EQ>::C + 3) / 4;
+  static constexpr int NK = (Cfg<DIM, EQ>::C - 1) / 4;
   static constexpr int BSIZE = NK * NT * 32;
+  static_assert((Cfg<DIM, EQ>::C - 1) % 4 == 0, "stencil of 4m + 1 cells");
   static_assert(BSIZE <= kDmmaMaxB, "B fragment table too small");
 };
 
@@ -118,9 +122,12 @@ __global__ void __launch_bounds__(128)
   __shared__ double tile[6][PosTile<DIM>::N];
   __shared__ double sB[Sh::BSIZE];
   __shared__ int64_t sOff[NK * 4];
+  __shared__ double sWl[NT * 8]; // weights of the last stencil cell per row
   const int tid = threadIdx.y * kBlockX + threadIdx.x;
   for (int t = tid; t < Sh::BSIZE; t += kBlockX * kBlockY) sB[t] = S->dmma_b[t];
-  if (tid < NK * 4) sOff[tid] = tid < T::C ? g.loff[tid] : 0;
+  if (tid < NK * 4) sOff[tid] = g.loff[tid];
+  if (tid < NT * 8) sWl[tid] = tid < Sh::NR ? S->lin[(T::C - 1) * Sh::NR + tid] : 0.0;
+  const int64_t oLast = g.loff[T::C - 1];
   const int64_t k = blockIdx.z;
   pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)kBlockX, blockIdx.y * (int64_t)kBlockY, k, tile);
   __syncthreads();
@@ -149,19 +156,33 @@ __global__ void __launch_bounds__(128)
     for (int v = 0; v < NV; v++)
 #pragma unroll
       for (int t = 0; t < NT; t++) acc[v][t][0] = acc[v][t][1] = 0.0;
-#pragma unroll 3
+#pragma unroll 4
     for (int ks = 0; ks < NK; ks++) {
       const int kc = ks * 4 + (lane & 3);
       const int64_t o = sOff[kc];
       double a[NV];
 #pragma unroll
-      for (int v = 0; v < NV; v++) a[v] = kc < T::C ? __ldg(Uc + v * g.pvol + o) : 0.0;
+      for (int v = 0; v < NV; v++) a[v] = __ldg(Uc + v * g.pvol + o);
 #pragma unroll
       for (int t = 0; t < NT; t++) {
         const double b = sB[(ks * NT + t) * 32 + lane];
 #pragma unroll
         for (int v = 0; v < NV; v++) dmma_884(acc[v][t], a[v], b);
       }
+    }
+    {
+      // the last stencil cell
+      double ul[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) ul[v] = __ldg(Uc + v * g.pvol + oLast);
+#pragma unroll
+      for (int t = 0; t < NT; t++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const double wl = sWl[t * 8 + 2 * (lane & 3) + e];
+#pragma unroll
+          for (int v = 0; v < NV; v++) acc[v][t][e] = fma(wl, ul[v], acc[v][t][e]);
+        }
     }
     bool inside = true;
     double lam = 0.0, vel = 0.0;
@@ -1293,7 +1314,8 @@ struct Launch {
 
 // host: B fragments of the FP64 MMA from the [cell][row] linear weights
 void fill_dmma_weights(DevStencil &S, int nrows) {
-  const int C = S.w.n_cells, nt = (nrows + 7) / 8, nk = (C + 3) / 4;
+  // all stencil cells but the last (added in the kernel's epilogue)
+  const int C = S.w.n_cells - 1, nt = (nrows + 7) / 8, nk = (C + 3) / 4;
   std::memset(S.dmma_b, 0, sizeof(S.dmma_b));
   for (int ks = 0; ks < nk; ks++)
     for (int t = 0; t < nt; t++)
