@@ -373,7 +373,8 @@ def run_ours(args):
     # DRAM bytes per cell of each kernel class from one ncu capture (profiles/),
     # scaled by the cells one launch processes
     traffic_tbl = load_json(os.path.join(ROOT, "profiles", "dram_traffic.json")) or {}
-    per_cell = traffic_tbl.get("bytes_per_cell", {}).get(dom)
+    case = f"{cfg.dim}d_{('hydro', 'ns', 'glm')[cfg.eq]}"
+    per_cell = traffic_tbl.get("cases", {}).get(case, {}).get("bytes_per_cell", {}).get(dom)
     traffic = per_cell * n if per_cell is not None else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak,
                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
