@@ -444,8 +444,10 @@ struct HeavyShape {
   using T = Cfg<DIM, EQ>;
   static constexpr int NR = LinRows<DIM, EQ>::NROWS;          // face points, then interior points
   static constexpr int NSUM = T::C + T::CC + T::NB * T::CB;   // stencil cells over all substencils
-  static constexpr int DER = T::NI * NSUM;                    // derivative weights
-  static constexpr int FW = NR * NSUM;                        // reconstruction weights
+  static constexpr int NIP = (T::NI + 1) & ~1;                // derivative rows padded to pairs
+  static constexpr int DER = NIP * NSUM;                      // derivative weights [s][p][i]
+  static constexpr int FW = NR * NSUM;                        // reconstruction weights [s][p][row]
+  static_assert(NR % 2 == 0, "rows in pairs");
   static constexpr int CELLS = 32;
   static constexpr size_t BYTES = (size_t)(DER + FW + CELLS * NR * T::NV + CELLS * 2) * sizeof(double) +
                                   (size_t)T::NB * T::CB * sizeof(int);
@@ -516,23 +518,25 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
   using E = Eos<EQ>;
   constexpr int NV = T::NV, NR = H::NR;
   extern __shared__ __align__(16) double hsm[];
-  double *sDer = hsm;                       // [s][i][p]
-  double *sFw = sDer + H::DER;              // [s][row][p]
+  double *sDer = hsm;                       // [s][p][i], i padded to NIP
+  double *sFw = sDer + H::DER;              // [s][p][row]
   double *sFs = sFw + H::FW;                // [cell][row][v]
   double *sDep = sFs + H::CELLS * NR * NV;  // [cell][2]
   int *sSub = reinterpret_cast<int *>(sDep + H::CELLS * 2);
   const kfvm_stencil &st = S->w;
   const int tid = threadIdx.y * 32 + threadIdx.x, nt = 32 * NV;
+  // weights transposed so that the rows of one stencil value are adjacent and
+  // load as 16-byte pairs
   for (int t = tid; t < H::DER; t += nt) {
     int s = 0;
-    while (s + 1 < T::NSUB && t >= T::NI * H::off(s + 1)) s++;
-    const int r = t - T::NI * H::off(s), i = r / H::n(s), p = r % H::n(s);
-    sDer[t] = st.deriv_w[s][i][p];
+    while (s + 1 < T::NSUB && t >= H::NIP * H::off(s + 1)) s++;
+    const int r = t - H::NIP * H::off(s), p = r / H::NIP, i = r % H::NIP;
+    sDer[t] = i < T::NI ? st.deriv_w[s][i][p] : 0.0;
   }
   for (int t = tid; t < H::FW; t += nt) {
     int s = 0;
     while (s + 1 < T::NSUB && t >= NR * H::off(s + 1)) s++;
-    const int r = t - NR * H::off(s), row = r / H::n(s), p = r % H::n(s);
+    const int r = t - NR * H::off(s), p = r / NR, row = r % NR;
     const int nfq = T::NF * T::NQF;
     sFw[t] = row < nfq ? st.face_w[s][row / T::NQF][row % T::NQF][p] : st.cell_w[s][row - nfq][p];
   }
@@ -588,14 +592,19 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 #pragma unroll 1
       for (int s = 0; s < T::NSUB; s++) {
         const int n = H::n(s);
-        const double *D = sDer + T::NI * H::off(s);
+        const double *D = sDer + H::NIP * H::off(s);
         double b[T::NI];
 #pragma unroll
         for (int ii = 0; ii < T::NI; ii++) b[ii] = 0.0;
         for (int p = 0; p < n; p++) {
           const double val = Vf[cellOf(s, p)];
+          const double2 *D2 = reinterpret_cast<const double2 *>(D + p * H::NIP);
 #pragma unroll
-          for (int ii = 0; ii < T::NI; ii++) b[ii] += D[ii * n + p] * val;
+          for (int i2 = 0; i2 < H::NIP / 2; i2++) {
+            const double2 d = D2[i2];
+            b[2 * i2] += d.x * val;
+            if (2 * i2 + 1 < T::NI) b[2 * i2 + 1] += d.y * val;
+          }
         }
         double beta = 0.0;
 #pragma unroll
@@ -647,8 +656,13 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
         for (int r = 0; r < NR; r++) tt[r] = 0.0;
         for (int p = 0; p < n; p++) {
           const double val = Vf[cellOf(s, p)];
+          const double2 *W2 = reinterpret_cast<const double2 *>(Wr + p * NR);
 #pragma unroll
-          for (int r = 0; r < NR; r++) tt[r] += Wr[r * n + p] * val;
+          for (int r2 = 0; r2 < NR / 2; r2++) {
+            const double2 w = W2[r2];
+            tt[2 * r2] += w.x * val;
+            tt[2 * r2 + 1] += w.y * val;
+          }
         }
         if (om[s] != 0.0)
 #pragma unroll
