@@ -128,6 +128,7 @@ struct kfvm_solver {
   double *Uhat = nullptr, *Utmp = nullptr, *K = nullptr;
   double *F[3] = {nullptr, nullptr, nullptr}, *G[3] = {nullptr, nullptr, nullptr};
   double *src = nullptr, *theta = nullptr, *part = nullptr;
+  double *bnd = nullptr; // limiter bounds per cell from the reconstruction pass, 3 x n
   double *io = nullptr; // host-order interior state for set/get (allocated at first use)
   uint8_t *flag = nullptr, *wset = nullptr, *applied = nullptr;
   uint32_t *heavy = nullptr; // compacted WENO / limiter cell list (one slot per cell)
@@ -265,9 +266,9 @@ int eval_front(kfvm_solver *s, int b) {
     if ((e = run(s, KFVM_KCLASS_RECON, 1, [&] {
            if (s->precision == KFVM_PREC_TF32X3)
              return launch_recon_tc(dim, eq, s->Ub[b], s->g, s->dS, wantInd, s->F, s->W, s->src, s->status,
-                                    s->lamvel, s->sc, st);
+                                    s->lamvel, s->bnd, s->sc, st);
            return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, wantInd, s->F, s->W, s->src, s->status, s->lamvel,
-                               st);
+                               s->bnd, st);
          })) != cudaSuccess)
       return set_err_cuda(e, "recon");
   }
@@ -292,8 +293,8 @@ int eval_front(kfvm_solver *s, int b) {
        })) != cudaSuccess)
     return set_err_cuda(e, "compact");
   if ((e = run(s, KFVM_KCLASS_HEAVY, 1, [&] {
-         return launch_heavy(dim, eq, s->Ub[b], s->g, s->dS, s->theta, s->F, s->src, s->heavy, s->sc, jd,
-                             s->heavyBlocks, st);
+         return launch_heavy(dim, eq, s->Ub[b], s->g, s->dS, s->theta, s->F, s->src, s->heavy,
+                             mode == RECON_FULL ? nullptr : s->bnd, s->sc, jd, s->heavyBlocks, st);
        })) != cudaSuccess)
     return set_err_cuda(e, "heavy");
   if ((e = run(s, KFVM_KCLASS_RIEMANN, dim, [&] { return launch_riemann(dim, eq, s->F, s->G, s->g, s->sc, st); })) !=
@@ -655,6 +656,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
       (e = dalloc((void **)&s->src, (size_t)nqc * nv * n * sizeof(double))) != cudaSuccess)
     return cleanup(e, "alloc");
   if ((e = dalloc((void **)&s->theta, n * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->bnd, 3 * n * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
   if ((e = dalloc((void **)&s->flag, n)) != cudaSuccess) return cleanup(e, "alloc");
   if ((e = dalloc((void **)&s->wset, n)) != cudaSuccess) return cleanup(e, "alloc");
   if ((e = dalloc((void **)&s->applied, n)) != cudaSuccess) return cleanup(e, "alloc");
@@ -703,6 +705,7 @@ void kfvm_destroy(kfvm_solver *s) {
   cudaFree(s->lamvel);
   cudaFree(s->src);
   cudaFree(s->theta);
+  cudaFree(s->bnd);
   cudaFree(s->io);
   cudaFree(s->flag);
   cudaFree(s->wset);

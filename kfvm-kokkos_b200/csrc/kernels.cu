@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128)
                  double *__restrict__ F0,
                  double *__restrict__ F1, double *__restrict__ F2, float *__restrict__ W0,
                  float *__restrict__ W1, float *__restrict__ W2, double *__restrict__ src,
-                 uint8_t *__restrict__ status, double2 *__restrict__ lamvel) {
+                 uint8_t *__restrict__ status, double2 *__restrict__ lamvel, double *__restrict__ bnd) {
   using T = Cfg<DIM, EQ>;
   using Sh = DmmaShape<DIM, EQ>;
   constexpr int NV = T::NV, NT = Sh::NT, NK = Sh::NK;
@@ -138,6 +138,14 @@ __global__ void __launch_bounds__(128)
     sBd[0][tid] = bd.minDens;
     sBd[1][tid] = bd.maxDens;
     sBd[2][tid] = bd.minEint;
+    // and for the heavy pass
+    const int64_t bi = blockIdx.x * (int64_t)kBlockX + threadIdx.x, bj = blockIdx.y * (int64_t)kBlockY + threadIdx.y;
+    if (bi < g.nx && bj < g.ny) {
+      const int64_t c = (k * g.ny + bj) * g.nx + bi;
+      bnd[c] = bd.minDens;
+      bnd[g.n + c] = bd.maxDens;
+      bnd[2 * g.n + c] = bd.minEint;
+    }
   }
   __syncthreads();
   const int lane = threadIdx.x;
@@ -512,7 +520,7 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
     heavy_var_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S,
                      double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
                      double *__restrict__ F2, double *__restrict__ src, const uint32_t *__restrict__ heavy,
-                     DevScalars *__restrict__ sc, JudgeArgs jd) {
+                     const double *__restrict__ bnd, DevScalars *__restrict__ sc, JudgeArgs jd) {
   using T = Cfg<DIM, EQ>;
   using H = HeavyShape<DIM, EQ>;
   using E = Eos<EQ>;
@@ -701,7 +709,16 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
           if (!lab && p) atomicAdd(&sc->mlp_false, 1ull);
         }
       }
-      const PosBounds bd = pos_bounds<DIM, EQ>(Uc, g);
+      PosBounds bd;
+      if (bnd) {
+        // the reconstruction pass computed them (pos_bounds_tile)
+        bd.rDens = ref[DENS];
+        bd.minDens = bnd[c];
+        bd.maxDens = bnd[g.n + c];
+        bd.minEint = bnd[2 * g.n + c];
+      } else {
+        bd = pos_bounds<DIM, EQ>(Uc, g);
+      }
       theta[c] = pos_apply_rows<DIM, EQ>(ref, bd, rs);
       if constexpr (T::SRC) {
         for (int r = 0; r < T::NF * T::NQF; r++) {
@@ -1257,9 +1274,9 @@ struct Launch {
   }
   static cudaError_t recon(const double *U, const Grid &g, const DevStencil *S, int wantInd,
                            double *const *F, float *const *W, double *src, uint8_t *status,
-                           double2 *lamvel, cudaStream_t s) {
+                           double2 *lamvel, double *bnd, cudaStream_t s) {
     recon_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
-        U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel);
+        U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd);
     return cudaGetLastError();
   }
   static cudaError_t flag(const double *U, const Grid &g, float *const *W, double *const *F,
@@ -1276,8 +1293,8 @@ struct Launch {
     return cudaGetLastError();
   }
   static cudaError_t heavy(const double *U, const Grid &g, const DevStencil *S, double *theta,
-                           double *const *F, double *src, const uint32_t *heavy, DevScalars *sc,
-                           const JudgeArgs &jd, int heavy_blocks, cudaStream_t s) {
+                           double *const *F, double *src, const uint32_t *heavy, const double *bnd,
+                           DevScalars *sc, const JudgeArgs &jd, int heavy_blocks, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
       cudaError_t e = cudaFuncSetAttribute(heavy_var_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1286,7 +1303,7 @@ struct Launch {
       attr = true;
     }
     heavy_var_kernel<DIM, EQ><<<heavy_blocks, dim3(32, NV), HeavyShape<DIM, EQ>::BYTES, s>>>(
-        U, g, S, theta, F[0], F[1], F[2], src, heavy, sc, jd);
+        U, g, S, theta, F[0], F[1], F[2], src, heavy, bnd, sc, jd);
     return cudaGetLastError();
   }
   static cudaError_t riemann(double *const *F, double *const *G, const Grid &g, DevScalars *sc,
@@ -1418,8 +1435,8 @@ cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s)
 }
 cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
                          double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
-                         cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, recon(U, g, S, wantInd, F, W, src, status, lamvel, s));
+                         double *bnd, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, recon(U, g, S, wantInd, F, W, src, status, lamvel, bnd, s));
 }
 cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, float *const *W, double *const *F,
                         const double *theta, uint8_t *flag, DevScalars *sc, double thr,
@@ -1433,8 +1450,9 @@ cudaError_t launch_compact(int dim, int eq, const Grid &g, int mode, const uint8
 }
 cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
                          double *theta, double *const *F, double *src, const uint32_t *heavy,
-                         DevScalars *sc, const JudgeArgs &jd, int heavy_blocks, cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, heavy(U, g, S, theta, F, src, heavy, sc, jd, heavy_blocks, s));
+                         const double *bnd, DevScalars *sc, const JudgeArgs &jd, int heavy_blocks,
+                         cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, heavy(U, g, S, theta, F, src, heavy, bnd, sc, jd, heavy_blocks, s));
 }
 cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
                            DevScalars *sc, cudaStream_t s) {

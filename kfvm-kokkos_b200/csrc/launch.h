@@ -37,14 +37,15 @@ cudaError_t launch_fill(double *p, int64_t n, double val, cudaStream_t s);
 cudaError_t launch_rcp_probe(int64_t n, uint64_t seed, unsigned long long *out, cudaStream_t s);
 // stage front end: linear states + KXRCF indicator + limiter bound status,
 // KXRCF flags, WENO decision / heavy-list compaction, heavy cells
+// bnd: the limiter bounds of every cell, [minDens | maxDens | minEint][cell], for the heavy pass
 cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
                          double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
-                         cudaStream_t s);
+                         double *bnd, cudaStream_t s);
 // the same outputs with the stencil sum on the tcgen05 tensor cores (3xTF32);
 // a block whose wait for the MMA completion gave up sets sc->fault
 cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
                             double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
-                            DevScalars *sc, cudaStream_t s);
+                            double *bnd, DevScalars *sc, cudaStream_t s);
 // self-test of the bounded mbarrier wait: out[0] = gave up, out[1] = ns waited
 cudaError_t launch_wait_probe(uint64_t limit_ns, unsigned long long *out, cudaStream_t s);
 // host: split the [cell][row] linear weights of S into the TF32 B-operand tables
@@ -57,9 +58,12 @@ cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, float *
 cudaError_t launch_compact(int dim, int eq, const Grid &g, int mode, const uint8_t *flag, uint8_t *wset,
                            const uint8_t *status, uint8_t *applied, double *theta, uint32_t *heavy,
                            const double2 *lamvel, DevScalars *sc, const JudgeArgs &jd, cudaStream_t s);
+// bnd: the reconstruction's limiter bounds, or null (full-WENO evaluations, where
+// no reconstruction pass ran) to compute them from the state
 cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const DevStencil *S,
                          double *theta, double *const *F, double *src, const uint32_t *heavy,
-                         DevScalars *sc, const JudgeArgs &jd, int heavy_blocks, cudaStream_t s);
+                         const double *bnd, DevScalars *sc, const JudgeArgs &jd, int heavy_blocks,
+                         cudaStream_t s);
 cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
                            DevScalars *sc, cudaStream_t s);
 cudaError_t launch_stage(int dim, int eq, const StageArgs &a, const Grid &g, cudaStream_t s);

@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                     double *__restrict__ F0, double *__restrict__ F1, double *__restrict__ F2,
                     float *__restrict__ W0, float *__restrict__ W1, float *__restrict__ W2,
                     double *__restrict__ src, uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
-                    DevScalars *__restrict__ sc) {
+                    double *__restrict__ bnd, DevScalars *__restrict__ sc) {
   using T = Cfg<DIM, EQ>;
   using Sh = TcShape<DIM, EQ>;
   constexpr int NV = T::NV;
@@ -175,6 +175,10 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     sBd[0][row] = bd.minDens;
     sBd[1][row] = bd.maxDens;
     sBd[2][row] = bd.minEint;
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    bnd[c] = bd.minDens;
+    bnd[g.n + c] = bd.maxDens;
+    bnd[2 * g.n + c] = bd.minEint;
   }
 
   const double *Uc = U + pidx(g, live ? i : 0, live ? j : 0, k);
@@ -332,7 +336,7 @@ cudaError_t launch_wait_probe(uint64_t limit_ns, unsigned long long *out, cudaSt
 template <int DIM, int EQ>
 static cudaError_t recon_tc_launch(const double *U, const Grid &g, const DevStencil *S, int wantInd,
                                    double *const *F, float *const *W, double *src, uint8_t *status,
-                                   double2 *lamvel, DevScalars *sc, cudaStream_t s) {
+                                   double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s) {
   using Sh = TcShape<DIM, EQ>;
   static bool attr = false; // the attribute is per function and process-wide
   if (!attr) {
@@ -344,21 +348,21 @@ static cudaError_t recon_tc_launch(const double *U, const Grid &g, const DevSten
   const dim3 grid((unsigned)((g.nx + kBlockX - 1) / kBlockX), (unsigned)((g.ny + kBlockY - 1) / kBlockY),
                   (unsigned)g.nz);
   recon_tc_kernel<DIM, EQ><<<grid, kTcThreads, Sh::SMEM, s>>>(
-      U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, sc);
+      U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd, sc);
   return cudaGetLastError();
 }
 
 cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
                             double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
-                            DevScalars *sc, cudaStream_t s) {
+                            double *bnd, DevScalars *sc, cudaStream_t s) {
   if (dim == 2) {
-    if (eq == EQ_GLM) return recon_tc_launch<2, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
-    if (eq == EQ_NS) return recon_tc_launch<2, EQ_NS>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
-    return recon_tc_launch<2, EQ_HYDRO>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
+    if (eq == EQ_GLM) return recon_tc_launch<2, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+    if (eq == EQ_NS) return recon_tc_launch<2, EQ_NS>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+    return recon_tc_launch<2, EQ_HYDRO>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
   }
-  if (eq == EQ_GLM) return recon_tc_launch<3, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
-  if (eq == EQ_NS) return recon_tc_launch<3, EQ_NS>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
-  return recon_tc_launch<3, EQ_HYDRO>(U, g, S, wantInd, F, W, src, status, lamvel, sc, s);
+  if (eq == EQ_GLM) return recon_tc_launch<3, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+  if (eq == EQ_NS) return recon_tc_launch<3, EQ_NS>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+  return recon_tc_launch<3, EQ_HYDRO>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
 }
 
 // host: W = hi + lo split of the [cell][row] linear weights into the B layout
