@@ -67,6 +67,7 @@ enum kfvm_ic {
 #define KFVM_ERR_LAPACK (-3)   /* dgetrf/dgetrs reported a singular system   */
 #define KFVM_ERR_NOMEM (-4)    /* device or host allocation failed           */
 #define KFVM_ERR_STATE (-5)    /* call out of order (e.g. step before IC)    */
+#define KFVM_ERR_IO (-6)       /* a plot / checkpoint file cannot be written or read */
 
 /* ---- sizes -------------------------------------------------------------- */
 #define KFVM_RAD 2          /* stencil radius (STENCIL_RADIUS)                 */
@@ -133,6 +134,9 @@ typedef struct kfvm_step_info {
   int32_t last_step; /* 1 if the solver decided to stop                    */
   int64_t n_weno;    /* cells sent to WENO in the last RHS evaluation      */
   int64_t n_rhs;     /* total RHS evaluations so far                       */
+  int32_t write_plot; /* 1 if the step ended on a plot time or the final time
+                         (Solver.cpp:197-205); reported once               */
+  int32_t reserved;
 } kfvm_step_info;
 
 typedef struct kfvm_solver kfvm_solver;
@@ -300,6 +304,38 @@ int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out_host);
  * applied to the cell) and positivity theta (wenoFlag(.,1)); either pointer may
  * be null.  Layout [nz][ny][nx]. */
 int kfvm_get_flags(kfvm_solver *s, uint8_t *weno_applied, double *theta);
+
+/* ---- Plot and checkpoint files (src/io/WriterPDI.cpp, user/pdi_*_xdmf.yml) ----
+ * XDMF 2 descriptions with raw little-endian FP64 datasets ([z][y][x], x fastest)
+ * where the reference writes HDF5 through PDI; the dataset names, the 3DRectMesh
+ * of nodal coordinates and the attribute list follow WriterPDI::writeXML.  A file
+ * set is <dir>/<base>_<num:07d>.xmf, .<dataset>.bin per dataset and .meta (time,
+ * time step, time step size, gamma, grid).  Conserved datasets always, the
+ * auxiliary ones (vel*, eint, pres | prsg prsb) only for plots (ckpt = 0), and
+ * weno / fomx (the two components of the WENO flag view: WENO applied, positivity
+ * theta) in both.  u is the host-order state [v][z][y][x] of kfvm_get_state.
+ * The directory is created if missing.  KFVM_ERR_IO if a file cannot be written. */
+int kfvm_plotfile_write(const kfvm_config *cfg, const char *dir, const char *base, int32_t num, int32_t ckpt,
+                        int32_t time_step, double time, double dt, const double *u, const uint8_t *weno,
+                        const double *theta);
+/* Reads a file set written by kfvm_plotfile_write (path of the .xmf).  The grid,
+ * dimension and equations recorded in its .meta must match cfg (KFVM_ERR_ARG
+ * otherwise); a missing or short dataset is KFVM_ERR_IO. */
+int kfvm_plotfile_read(const kfvm_config *cfg, const char *xmf_path, double *u, uint8_t *weno, double *theta,
+                       int32_t *time_step, double *time, double *dt);
+/* The solver's current state, flags, time and step size written as above
+ * (WriterPDI::writePlot / writeCkpt, Solver.cpp:113-122). */
+int kfvm_write_plotfile(kfvm_solver *s, const char *dir, const char *base, int32_t num, int32_t ckpt,
+                        int32_t time_step);
+/* Restart from a checkpoint (Solver::Solver with ps.restart, Solver.cpp:60-80):
+ * state, WENO flags and positivity theta from the file, the FSAL priming
+ * evaluation with those flags, then time and step size from the file; returns
+ * the file's time step (the caller continues at time_step + 1). */
+int kfvm_restart(kfvm_solver *s, const char *xmf_path, int32_t *time_step);
+/* Plot times for the step-size limit of kfvm_take_step: with plot_freq > 0 a step
+ * that would pass plot_num * plot_freq is shortened to end on it and reports
+ * write_plot (Solver.cpp:202-205).  The caller advances plot_num after writing. */
+int kfvm_set_plot_freq(kfvm_solver *s, double plot_freq, int32_t plot_num);
 
 /* Device time of the last kfvm_take_step call, for measurement (ms). */
 int kfvm_last_stage_ms(kfvm_solver *s, double *ms);

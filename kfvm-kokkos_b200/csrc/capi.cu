@@ -141,6 +141,9 @@ struct kfvm_solver {
   RKTable rk;
   double time = 0.0, dt = 0.0, errEst = 1.0;
   bool lastTimeStep = false, useSparseWeno = true, primed = false;
+  double plotFreq = 0.0; // plot times for the step-size limit (kfvm_set_plot_freq)
+  int32_t plotNum = 0;
+  bool writePlot = false;
   int indicator = KFVM_IND_KXRCF;
   int precision = KFVM_PREC_FP64;
   int64_t nRhs = 0, nWenoLast = 0;
@@ -375,9 +378,14 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
   if (!s->primed) return fail(KFVM_ERR_STATE, "take_step before an initial condition was set");
   const RKTable &rk = s->rk;
   cudaStream_t st = s->stream;
+  // limit dt to hit the final time or the next plot time (Solver.cpp:197-205)
   if (s->time + s->dt > s->cfg.final_time) {
     s->dt = s->cfg.final_time - s->time;
     s->lastTimeStep = true;
+    s->writePlot = true;
+  } else if (s->plotFreq > 0.0 && s->time + s->dt > s->plotNum * s->plotFreq) {
+    s->dt = s->plotNum * s->plotFreq - s->time;
+    s->writePlot = true;
   }
   bool accepted = false, firstUnphys = true;
   double maxVel = 0.0, errNew = 0.0, dtTaken = 0.0;
@@ -437,7 +445,10 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
       s->dt = firstUnphys ? std::fmin(0.25 * s->cfg.cfl * s->dmin / maxVel, s->dt / 4.0) : s->dt / 2.0;
       firstUnphys = false;
       s->useSparseWeno = false; // force full WENO on the retry
-      if (s->lastTimeStep) s->lastTimeStep = false;
+      if (s->lastTimeStep) {
+        s->lastTimeStep = false;
+        s->writePlot = false;
+      }
     } else if (lStat == KFVM_TS_ACCEPTED) {
       accepted = true;
       dtTaken = s->dt;
@@ -465,7 +476,10 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
       break;
     } else {
       s->dt = s->dt * dtfac;
-      if (s->lastTimeStep) s->lastTimeStep = false;
+      if (s->lastTimeStep) {
+        s->lastTimeStep = false;
+        s->writePlot = false;
+      }
     }
   }
   CK(cudaEventRecord(s->ev1, st));
@@ -486,7 +500,9 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
     info->last_step = s->lastTimeStep ? 1 : 0;
     info->n_weno = s->nWenoLast;
     info->n_rhs = s->nRhs;
+    info->write_plot = s->writePlot ? 1 : 0;
   }
+  s->writePlot = false; // reported once
   return KFVM_OK;
 }
 
@@ -1173,6 +1189,54 @@ int kfvm_get_flags(kfvm_solver *s, uint8_t *weno_applied, double *theta) {
   if (weno_applied) CK(cudaMemcpyAsync(weno_applied, s->applied, s->g.n, cudaMemcpyDeviceToHost, s->stream));
   if (theta) CK(cudaMemcpyAsync(theta, s->theta, s->g.n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  return KFVM_OK;
+}
+
+int kfvm_set_plot_freq(kfvm_solver *s, double plot_freq, int32_t plot_num) {
+  if (!s || !(plot_freq >= 0.0) || plot_num < 0) return fail(KFVM_ERR_ARG, "bad argument");
+  s->plotFreq = plot_freq;
+  s->plotNum = plot_num;
+  return KFVM_OK;
+}
+
+int kfvm_write_plotfile(kfvm_solver *s, const char *dir, const char *base, int32_t num, int32_t ckpt,
+                        int32_t time_step) {
+  if (!s || !dir || !base) return fail(KFVM_ERR_ARG, "null argument");
+  const int64_t n = s->g.n;
+  std::vector<double> u((size_t)n * s->nv), th((size_t)n);
+  std::vector<uint8_t> w((size_t)n);
+  int rc = kfvm_get_state(s, u.data());
+  if (rc) return rc;
+  if ((rc = kfvm_get_flags(s, w.data(), th.data()))) return rc;
+  return kfvm_plotfile_write(&s->cfg, dir, base, num, ckpt, time_step, s->time, s->dt, u.data(), w.data(),
+                             th.data());
+}
+
+int kfvm_restart(kfvm_solver *s, const char *xmf_path, int32_t *time_step) {
+  if (!s || !xmf_path || !time_step) return fail(KFVM_ERR_ARG, "null argument");
+  const int64_t n = s->g.n;
+  std::vector<double> u((size_t)n * s->nv), th((size_t)n);
+  std::vector<uint8_t> w((size_t)n);
+  double t = 0.0, h = 0.0;
+  int32_t ts = 0;
+  int rc = kfvm_plotfile_read(&s->cfg, xmf_path, u.data(), w.data(), th.data(), &ts, &t, &h);
+  if (rc) return rc;
+  if (!(h > 0.0)) return fail(KFVM_ERR_IO, "kfvm_restart: the file holds no time step size (a plot file?)");
+  // state and both components of the WENO flag view, then the FSAL priming
+  // evaluation; time, time step and step size come from the file (Solver.cpp:60-80)
+  if ((rc = upload_state(s, s->iPrev, u.data()))) return rc;
+  if ((rc = prime(s))) return rc;
+  CK(cudaMemcpyAsync(s->theta, th.data(), n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->wset, w.data(), n, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->applied, w.data(), n, cudaMemcpyHostToDevice, s->stream));
+  // the priming evaluation again, now with the restored flags
+  CK(cudaMemsetAsync(&s->sc->maxvel_bits, 0, sizeof(unsigned long long), s->stream));
+  if ((rc = eval_into_K(s, s->iPrev))) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  s->time = t;
+  s->dt = h;
+  s->nTS = ts + 1;
+  *time_step = ts;
   return KFVM_OK;
 }
 

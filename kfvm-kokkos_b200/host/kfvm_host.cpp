@@ -1,6 +1,7 @@
 // kfvm_host.cpp -- ProblemSetup (.init parsing) and Solver over the C ABI.
 #include "kfvm_host.hpp"
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -129,7 +130,16 @@ bool ProblemSetup::setIO(const std::string &setting) {
   else if (w[0] == "datadir" && w.size() >= 2) dataDir = w[1];
   else if (w[0] == "verbose" && w.size() >= 2) verbose = std::stoi(w[1]);
   else if (w[0] == "dumpstate" && w.size() >= 2) dumpState = std::stoi(w[1]) != 0;
-  else return true; // plot/checkpoint settings have no effect in this build
+  else if (w[0] == "plotfreq" && w.size() >= 2) plotFreq = rf(w[1]);
+  else if (w[0] == "ckptfreq" && w.size() >= 2) ckptFreq = std::stoi(w[1]);
+  else if (w[0] == "restartfile" && w.size() >= 2) {
+    restartFile = w[1];
+    restart = true;
+  } else if (w[0] == "statsfreq" || w[0] == "pdiconf") {
+    warnings.push_back("io:" + w[0] + " has no effect in this build (flow statistics and PDI are not built)");
+  } else {
+    return false;
+  }
   return true;
 }
 
@@ -193,21 +203,58 @@ std::string ProblemSetup::toJson() const {
                 "\"prandtl\": %.17g, \"weno_thresh\": %.17g, \"lfac\": %.17g, \"cfl\": %.17g, \"atol\": "
                 "%.17g, \"rtol\": %.17g, \"rejection_thresh\": %.17g, \"min_dt\": %.17g, \"final_time\": "
                 "%.17g, \"rejection_limit\": %d, \"max_steps\": %d, \"have_sources\": %d, \"ic\": %d, "
-                "\"seed\": %llu, \"warnings\": %d}",
+                "\"seed\": %llu, \"warnings\": %d, \"plot_freq\": %.17g, \"ckpt_freq\": %d, \"restart\": %d}",
                 cfg.dim, cfg.eq, cfg.rs, cfg.rk, cfg.nq, cfg.indicator, (long long)cfg.nx,
                 (long long)cfg.ny, (long long)cfg.nz, cfg.xlo, cfg.xup, cfg.ylo, cfg.yup, cfg.zlo, cfg.zup,
                 cfg.bc[0], cfg.bc[1], cfg.bc[2], cfg.bc[3], cfg.bc[4], cfg.bc[5], cfg.gamma, cfg.reynolds,
                 cfg.prandtl, cfg.weno_thresh, cfg.lfac, cfg.cfl, cfg.atol, cfg.rtol, cfg.rejection_thresh,
                 cfg.min_dt, cfg.final_time, cfg.rejection_limit, cfg.max_steps, cfg.have_sources, ic,
-                (unsigned long long)seed, (int)warnings.size());
+                (unsigned long long)seed, (int)warnings.size(), plotFreq, ckptFreq, restart ? 1 : 0);
   return b;
 }
 
 // ---------------------------------------------------------------------------
 Solver::Solver(const ProblemSetup &ps) : ps_(ps) {
   check(kfvm_create(&ps.cfg, &s_), "kfvm_create");
-  check(kfvm_init_ic(s_, ps.ic, ps.seed), "kfvm_init_ic"); // setIC + FSAL priming + first dt
+  if (!ps.restart) {
+    check(kfvm_init_ic(s_, ps.ic, ps.seed), "kfvm_init_ic"); // setIC + FSAL priming + first dt
+    if (ps.plotFreq > 0.0) {
+      writePlot();
+      plotNum_++;
+    }
+    if (ps.ckptFreq > 0) writeCkpt(0);
+  } else {
+    std::printf("Restarting from: %s\n", ps.restartFile.c_str());
+    int32_t step = 0;
+    check(kfvm_restart(s_, ps.restartFile.c_str(), &step), "kfvm_restart");
+    nTS_ = step + 1;
+  }
   check(kfvm_get_time(s_, &time_, &dt_), "kfvm_get_time");
+  if (ps.restart && ps.plotFreq > 0.0) plotNum_ = static_cast<int>(std::ceil(time_ / ps.plotFreq));
+  check(kfvm_set_plot_freq(s_, ps.plotFreq, plotNum_), "kfvm_set_plot_freq");
+}
+
+std::string Solver::outputPrefix() const {
+  const kfvm_config &c = ps_.cfg;
+  std::string p = ps_.dataDir + "/R2_NX" + std::to_string(c.nx) + "_NY" + std::to_string(c.ny);
+  if (c.dim == 3) p += "_NZ" + std::to_string(c.nz);
+  return p + "/";
+}
+
+void Solver::writePlot() {
+  const std::string dir = outputPrefix() + "plot";
+  char b[32];
+  std::snprintf(b, sizeof(b), "_%07d.xmf", plotNum_);
+  std::printf("Writing file: %s/%s%s\n", dir.c_str(), ps_.baseName.c_str(), b);
+  check(kfvm_write_plotfile(s_, dir.c_str(), ps_.baseName.c_str(), plotNum_, 0, plotNum_), "kfvm_write_plotfile");
+}
+
+void Solver::writeCkpt(int step) {
+  const std::string dir = outputPrefix() + "ckpt";
+  char b[32];
+  std::snprintf(b, sizeof(b), "_%07d.xmf", step);
+  std::printf("Writing file: %s/%s%s\n", dir.c_str(), ps_.baseName.c_str(), b);
+  check(kfvm_write_plotfile(s_, dir.c_str(), ps_.baseName.c_str(), step, 1, step), "kfvm_write_plotfile");
 }
 
 Solver::~Solver() { kfvm_destroy(s_); }
@@ -229,11 +276,18 @@ void Solver::TakeStep() {
   }
 }
 
-// Solver::Solve (src/Solver.cpp:84-140) without plot/checkpoint output
+// Solver::Solve (src/Solver.cpp:84-140) with its plot and checkpoint cadence
 void Solver::Solve() {
-  for (; nTS_ < ps_.cfg.max_steps && !lastTimeStep_; ++nTS_) {
+  const int maxSteps = ps_.cfg.max_steps;
+  for (; nTS_ < maxSteps && !lastTimeStep_; ++nTS_) {
     if (ps_.verbose > 0) std::printf("Step %d: time = %.4g\n", nTS_, time_);
     TakeStep();
+    if (ps_.plotFreq > 0.0 && (info_.write_plot || lastTimeStep_ || nTS_ == maxSteps - 1)) {
+      writePlot();
+      plotNum_++;
+      check(kfvm_set_plot_freq(s_, ps_.plotFreq, plotNum_), "kfvm_set_plot_freq");
+    }
+    if (ps_.ckptFreq > 0 && (nTS_ % ps_.ckptFreq == 0 || lastTimeStep_ || nTS_ == maxSteps - 1)) writeCkpt(nTS_);
   }
   std::printf("Time stepping completed\n  %lld RHS evals and %lld/%lld rejected (accuracy/unphysical) steps\n",
               (long long)info_.n_rhs, (long long)nRejectThresh_, (long long)nRejectUnphys_);

@@ -19,6 +19,11 @@ struct ProblemSetup {
   int32_t ic = KFVM_IC_SMOOTH_WAVE;
   uint64_t seed = 12345;
   std::string baseName = "default", dataDir = "data";
+  // plot / checkpoint output and restart (ProblemSetup.H:333-367)
+  double plotFreq = 0.0;
+  int ckptFreq = 0;
+  std::string restartFile;
+  bool restart = false;
   int verbose = 0;
   bool dumpState = false;
   std::vector<std::string> warnings;
@@ -41,6 +46,8 @@ struct ProblemSetup {
 // Solver::Solver / Solve / TakeStep / evalRHS over the C ABI
 class Solver {
  public:
+  // Solver::Solver: initial condition (plus the first plot and checkpoint) or a
+  // restart from ps.restartFile, then the FSAL priming evaluation
   explicit Solver(const ProblemSetup &ps);
   ~Solver();
   Solver(const Solver &) = delete;
@@ -58,12 +65,17 @@ class Solver {
 
  private:
   void check(int rc, const char *what) const;
+  // <dataDir>/R2_NX.._NY..[_NZ..]/ (WriterPDI.cpp:20-33)
+  std::string outputPrefix() const;
+  void writePlot();
+  void writeCkpt(int step);
   const ProblemSetup &ps_;
   kfvm_solver *s_ = nullptr;
   kfvm_step_info info_{};
   double time_ = 0.0, dt_ = 0.0;
   int64_t accepted_ = 0, nRejectThresh_ = 0, nRejectUnphys_ = 0;
   int nTS_ = 1;
+  int plotNum_ = 0;
   bool lastTimeStep_ = false;
 };
 

@@ -66,6 +66,13 @@ def lib():
         L.kfvm_mlp_stats.argtypes = [P, P]
         L.kfvm_get_faces.argtypes = [P, I32, P]
         L.kfvm_get_flags.argtypes = [P, P, P]
+        L.kfvm_plotfile_write.argtypes = [C.POINTER(abi.KfvmConfig), C.c_char_p, C.c_char_p, I32, I32, I32, D, D,
+                                          P, P, P]
+        L.kfvm_plotfile_read.argtypes = [C.POINTER(abi.KfvmConfig), C.c_char_p, P, P, P, C.POINTER(I32),
+                                         C.POINTER(D), C.POINTER(D)]
+        L.kfvm_write_plotfile.argtypes = [P, C.c_char_p, C.c_char_p, I32, I32, I32]
+        L.kfvm_restart.argtypes = [P, C.c_char_p, C.POINTER(I32)]
+        L.kfvm_set_plot_freq.argtypes = [P, D, I32]
         L.kfvm_last_stage_ms.argtypes = [P, P]
         L.kfvm_get_stream.argtypes = [P, C.POINTER(C.c_void_p)]
         L.kfvm_set_timing.argtypes = [P, I32]
@@ -102,6 +109,30 @@ def selftest_rcp(n=1 << 24, seed=5):
     u, q = C.c_int64(), C.c_double()
     _check(lib().kfvm_selftest_rcp(int(n), int(seed), C.byref(u), C.byref(q)), "kfvm_selftest_rcp")
     return u.value, q.value
+
+
+def plotfile_write(cfg, directory, base, num, u, weno, theta, time=0.0, time_step=0, dt=0.0, ckpt=False):
+    """kfvm_plotfile_write from host arrays: u [nv][n] float64, weno [n] 0/1, theta [n]."""
+    nv, n = abi.nvars(cfg), abi.ncells(cfg)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(nv, n)
+    w = np.ascontiguousarray(weno, dtype=np.uint8).reshape(n)
+    th = np.ascontiguousarray(theta, dtype=np.float64).reshape(n)
+    _check(lib().kfvm_plotfile_write(C.byref(cfg), str(directory).encode(), str(base).encode(), int(num),
+                                     1 if ckpt else 0, int(time_step), float(time), float(dt), u.ctypes.data,
+                                     w.ctypes.data, th.ctypes.data), "kfvm_plotfile_write")
+    return os.path.join(str(directory), f"{base}_{int(num):07d}.xmf")
+
+
+def plotfile_read(cfg, xmf_path):
+    """kfvm_plotfile_read: dict with u [nv][n], weno [n], theta [n], time_step, time, dt."""
+    nv, n = abi.nvars(cfg), abi.ncells(cfg)
+    u = np.empty((nv, n), dtype=np.float64)
+    w = np.empty(n, dtype=np.uint8)
+    th = np.empty(n, dtype=np.float64)
+    ts, t, h = C.c_int32(), C.c_double(), C.c_double()
+    _check(lib().kfvm_plotfile_read(C.byref(cfg), str(xmf_path).encode(), u.ctypes.data, w.ctypes.data,
+                                    th.ctypes.data, C.byref(ts), C.byref(t), C.byref(h)), "kfvm_plotfile_read")
+    return {"u": u, "weno": w, "theta": th, "time_step": ts.value, "time": t.value, "dt": h.value}
 
 
 def stencil(cfg):
@@ -244,6 +275,21 @@ class Solver:
         out = np.empty((2, nqf, self.nv, fd[0] * fd[1] * fd[2]), dtype=np.float64)
         _check(lib().kfvm_get_faces(self.h, int(d), out.ctypes.data), "kfvm_get_faces")
         return out
+
+    def write_plotfile(self, directory, base, num, ckpt=False, time_step=0):
+        """kfvm_write_plotfile: the current state as an XDMF + binary file set; returns the .xmf path."""
+        _check(lib().kfvm_write_plotfile(self.h, str(directory).encode(), str(base).encode(), int(num),
+                                         1 if ckpt else 0, int(time_step)), "kfvm_write_plotfile")
+        return os.path.join(str(directory), f"{base}_{int(num):07d}.xmf")
+
+    def restart(self, xmf_path):
+        """kfvm_restart from a checkpoint; returns its time step."""
+        ts = C.c_int32()
+        _check(lib().kfvm_restart(self.h, str(xmf_path).encode(), C.byref(ts)), "kfvm_restart")
+        return ts.value
+
+    def set_plot_freq(self, plot_freq, plot_num):
+        _check(lib().kfvm_set_plot_freq(self.h, float(plot_freq), int(plot_num)), "kfvm_set_plot_freq")
 
     def flags(self):
         a = np.empty(self.n, dtype=np.uint8)

@@ -60,6 +60,7 @@ class KfvmStepInfo(C.Structure):
         ("max_vel", C.c_double), ("err_est", C.c_double),
         ("status", C.c_int32), ("attempts", C.c_int32), ("accepted", C.c_int32),
         ("last_step", C.c_int32), ("n_weno", C.c_int64), ("n_rhs", C.c_int64),
+        ("write_plot", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
