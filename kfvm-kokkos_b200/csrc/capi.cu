@@ -188,6 +188,18 @@ namespace {
 const char *const kFaultMsg =
     "tensor-core reconstruction: a block gave up waiting for its MMA completion (bounded wait)";
 
+// the -1 entries of the wall coefficient tables as a bit mask over the variables
+// (src/physics/hydro/Hydro_BCCoeffs.H, navierstokes/NavierStokes_BCCoeffs.H,
+// mhd_glm/MHD_GLM_BCCoeffs.H): reflecting negates the normal momentum (and the
+// normal magnetic field), no-slip every momentum component (and the normal field)
+unsigned wall_flip(int bc, int d, bool glm) {
+  using namespace kfvm;
+  const unsigned bn = glm ? 1u << (MAGX + d) : 0u;
+  if (bc == KFVM_BC_REFLECTING) return (1u << (MOMX + d)) | bn;
+  if (bc == KFVM_BC_NOSLIP) return (1u << MOMX) | (1u << MOMY) | (1u << MOMZ) | bn;
+  return 0u;
+}
+
 int set_err_cuda(cudaError_t e, const char *what) {
   return fail(KFVM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -576,9 +588,13 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if (cfg->nx * cfg->ny * nz >= (int64_t)0x80000000LL) return fail(KFVM_ERR_ARG, "more than 2^31 cells");
   if (cfg->nx < 3 || cfg->ny < 3 || nz < (cfg->dim == 3 ? 3 : 1))
     return fail(KFVM_ERR_ARG, "grid too small for a radius-2 stencil");
-  for (int d = 0; d < cfg->dim; d++)
+  for (int d = 0; d < cfg->dim; d++) {
     if ((cfg->bc[2 * d] == KFVM_BC_PERIODIC) != (cfg->bc[2 * d + 1] == KFVM_BC_PERIODIC))
       return fail(KFVM_ERR_ARG, "periodic boundaries must come in pairs");
+    for (int f = 2 * d; f < 2 * d + 2; f++)
+      if (cfg->bc[f] < KFVM_BC_PERIODIC || cfg->bc[f] > KFVM_BC_NOSLIP)
+        return fail(KFVM_ERR_ARG, "unknown boundary condition (periodic, outflow, reflecting, noslip)");
+  }
   kfvm_solver *s = new kfvm_solver();
   s->cfg = *cfg;
   s->cfg.nz = nz;
@@ -612,7 +628,10 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   g.rdx = 1.0 / g.dx;
   g.rdy = 1.0 / g.dy;
   g.rdz = 1.0 / g.dz;
-  for (int f = 0; f < 6; f++) g.bc[f] = cfg->bc[f];
+  for (int f = 0; f < 6; f++) {
+    g.bc[f] = cfg->bc[f];
+    g.bflip[f] = wall_flip(cfg->bc[f], f / 2, cfg->eq == KFVM_EQ_MHD_GLM);
+  }
   g.gamma = cfg->gamma;
   g.rs = cfg->rs;
   s->dmin = cfg->dim == 2 ? std::fmin(g.dx, g.dy) : std::fmin(g.dx, std::fmin(g.dy, g.dz));
@@ -1163,6 +1182,7 @@ int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
   const int64_t nd = dir == 0 ? g.nx : (dir == 1 ? g.ny : g.nz);
   const int64_t stride = dir == 0 ? 1 : (dir == 1 ? fx : fx * fy);
   const bool per = g.bc[2 * dir] == KFVM_BC_PERIODIC;
+  const unsigned flo = g.bflip[2 * dir], fhi = g.bflip[2 * dir + 1];
   for (int64_t k = 0; k < fz; k++)
     for (int64_t j = 0; j < fy; j++)
       for (int64_t i = 0; i < fx; i++) {
@@ -1176,8 +1196,8 @@ int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
               out[s0 + lo] = out[s0 + hi];
               out[s1 + hi] = out[s1 + lo];
             } else {
-              out[s0 + lo] = out[s1 + lo];
-              out[s1 + hi] = out[s0 + hi];
+              out[s0 + lo] = (flo >> v) & 1u ? -out[s1 + lo] : out[s1 + lo];
+              out[s1 + hi] = (fhi >> v) & 1u ? -out[s0 + hi] : out[s0 + hi];
             }
           }
       }

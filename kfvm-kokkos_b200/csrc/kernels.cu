@@ -57,8 +57,16 @@ __global__ void __launch_bounds__(256) bc_fill_kernel(double *__restrict__ U, Gr
     const int64_t sj = axis_map(j, g.ny, g.bc[2], g.bc[3]);
     const int64_t sk = DIM == 3 ? axis_map(k, g.nz, g.bc[4], g.bc[5]) : k;
     const int64_t dst = pidx(g, i, j, k), src = pidx(g, si, sj, sk);
+    // wall mirrors flip signs; the sequential x, y, z fills of the reference
+    // multiply a corner by the coefficients of every wall it lies beyond
+    unsigned flip = (i < 0 ? g.bflip[0] : (i >= g.nx ? g.bflip[1] : 0u)) ^
+                    (j < 0 ? g.bflip[2] : (j >= g.ny ? g.bflip[3] : 0u));
+    if (DIM == 3) flip ^= k < 0 ? g.bflip[4] : (k >= g.nz ? g.bflip[5] : 0u);
 #pragma unroll
-    for (int v = 0; v < NV; v++) U[v * g.pvol + dst] = U[v * g.pvol + src];
+    for (int v = 0; v < NV; v++) {
+      const double x = U[v * g.pvol + src];
+      U[v * g.pvol + dst] = (flip >> v) & 1u ? -x : x;
+    }
   }
 }
 
@@ -786,13 +794,20 @@ __global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4), EQ == EQ_GLM ? 1 : (D
     // periodic partner face, or copy the interior slot at an outflow boundary
     int64_t f0 = fidx, f1 = fidx;
     int s0 = 0, s1 = 1;
+    unsigned flipL = 0u, flipR = 0u; // wall mirrors (reflecting / no-slip)
     const int64_t stride = D == 0 ? 1 : (D == 1 ? fx : fx * fy);
     if (m == 0) {
       if (g.bc[2 * D] == KFVM_BC_PERIODIC) f0 = fidx + nd * stride;
-      else s0 = 1;
+      else {
+        s0 = 1;
+        flipL = g.bflip[2 * D];
+      }
     } else if (m == nd) {
       if (g.bc[2 * D + 1] == KFVM_BC_PERIODIC) f1 = fidx - nd * stride;
-      else s1 = 0;
+      else {
+        s1 = 0;
+        flipR = g.bflip[2 * D + 1];
+      }
     }
     const double ch = EQ == EQ_GLM ? __longlong_as_double((long long)sc->glm_lam_bits) -
                                          __longlong_as_double((long long)sc->glm_vel_bits)
@@ -804,6 +819,8 @@ __global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4), EQ == EQ_GLM ? 1 : (D
     for (int v = 0; v < NV; v++) {
       uL[v] = __ldg(pL + v * nf);
       uR[v] = __ldg(pR + v * nf);
+      if ((flipL >> v) & 1u) uL[v] = -uL[v];
+      if ((flipR >> v) & 1u) uR[v] = -uR[v];
     }
     vmax = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
     const double wq = DIM == 2 ? 0.5 : 0.25; // Gauss weights 1/2 (x 1/2 in 3D)
@@ -848,14 +865,22 @@ __device__ void glm_sources(const double *__restrict__ Uc, const Grid &g, int64_
     const int64_t nd = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
     const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
     int64_t fidx = (fk * fy + fj) * fx + fi;
+    unsigned flip = 0u;
     if (m == 0 && s == 0) {
       if (g.bc[2 * d] == KFVM_BC_PERIODIC) fidx += nd * stride;
-      else s = 1;
+      else {
+        s = 1;
+        flip = g.bflip[2 * d];
+      }
     } else if (m == nd && s == 1) {
       if (g.bc[2 * d + 1] == KFVM_BC_PERIODIC) fidx -= nd * stride;
-      else s = 0;
+      else {
+        s = 0;
+        flip = g.bflip[2 * d + 1];
+      }
     }
-    return Fd[d][((int64_t)(s * NQF + q) * NV + v) * g.nface[d] + fidx];
+    const double x = Fd[d][((int64_t)(s * NQF + q) * NV + v) * g.nface[d] + fidx];
+    return (flip >> v) & 1u ? -x : x;
   };
   const double wt[2] = {0.5, 0.5};
   double divB = 0.0;

@@ -45,6 +45,9 @@ struct Grid {
   double dx, dy, dz;
   double rdx, rdy, rdz;      // 1 / dx, 1 / dy, 1 / dz
   int bc[6];
+  // variables whose sign the wall mirror flips, bit v per face (reflecting and
+  // no-slip coefficient tables of <Eq>_BCCoeffs.H; 0 for periodic / outflow)
+  unsigned bflip[6];
   double gamma, ch_init;
   int rs;
   int64_t loff[KFVM_MAX_CELLS]; // stencil offsets in the padded array

@@ -171,6 +171,8 @@ bool ProblemSetup::setSetup(const std::string &setting) {
       const std::string &b = w[1 + (nf == 1 ? 0 : std::min(f, nf - 1))];
       if (b == "periodic") cfg.bc[f] = KFVM_BC_PERIODIC;
       else if (b == "outflow") cfg.bc[f] = KFVM_BC_OUTFLOW;
+      else if (b == "reflecting") cfg.bc[f] = KFVM_BC_REFLECTING;
+      else if (b == "noslip") cfg.bc[f] = KFVM_BC_NOSLIP;
       else return false;
     }
   } else if (k == "ic") {

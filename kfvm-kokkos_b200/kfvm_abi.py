@@ -11,7 +11,7 @@ import struct
 KFVM_EQ_HYDRO, KFVM_EQ_NAVIERSTOKES, KFVM_EQ_MHD_GLM = 0, 1, 2
 KFVM_RS_LLF, KFVM_RS_HLL, KFVM_RS_HLLC = 0, 1, 2
 KFVM_RK_THREESTARP, KFVM_RK_FOURSTARP, KFVM_RK_SSP4_3_2, KFVM_RK_SSP10_4_3 = 0, 1, 2, 3
-KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW = 0, 1
+KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW, KFVM_BC_REFLECTING, KFVM_BC_NOSLIP = 0, 1, 2, 3
 KFVM_TS_ACCEPTED, KFVM_TS_TOLERANCE, KFVM_TS_UNPHYSICAL = 0, 1, 2
 KFVM_IND_KXRCF, KFVM_IND_ALL, KFVM_IND_NONE, KFVM_IND_MLP = 0, 1, 2, 3
 KFVM_PREC_FP64, KFVM_PREC_TF32X3 = 0, 1
@@ -98,9 +98,12 @@ def make_config(dim, eq, nx, ny, nz=1, extent=(0, 1, 0, 1, 0, 1), bc="periodic",
     c.xlo, c.xup, c.ylo, c.yup = e[0], e[1], e[2], e[3]
     if dim == 3:
         c.zlo, c.zup = e[4], e[5]
-    code = KFVM_BC_PERIODIC if bc == "periodic" else KFVM_BC_OUTFLOW
+    codes = {"periodic": KFVM_BC_PERIODIC, "outflow": KFVM_BC_OUTFLOW, "reflecting": KFVM_BC_REFLECTING,
+             "noslip": KFVM_BC_NOSLIP}
+    # one name for all faces, or one per face (west east south north bottom top)
+    names = [bc] * 6 if isinstance(bc, str) else list(bc) + [bc[-1]] * (6 - len(bc))
     for f in range(6):
-        c.bc[f] = code
+        c.bc[f] = codes[names[f]]
     c.gamma, c.cfl, c.weno_thresh, c.lfac = stof(gamma), stof(cfl), stof(weno_thresh), stof(lfac)
     c.reynolds, c.prandtl = stof(reynolds), stof(prandtl)
     c.atol, c.rtol, c.final_time = stof(atol), stof(rtol), stof(final_time)

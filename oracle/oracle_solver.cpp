@@ -508,7 +508,28 @@ struct orc_solver {
 
 namespace {
 
-// ---------------- BCs (Solver.cpp:744-830, BoundaryConditions_K.H:53-72, 529-546) ----
+// ---------------- BCs (Solver.cpp:744-830, 1460-1946; BoundaryConditions_K.H:53-95,
+// 529-570) ----
+// Wall coefficient of variable v at face f: the reflecting and no-slip tables of
+// src/physics/{hydro,navierstokes,mhd_glm}/*_BCCoeffs.H (1 for outflow).
+double wall_coef(const orc_solver &S, int f, int v) {
+  const int bc = S.cfg.bc[f], d = f / 2;
+  const bool glm = S.nv == 9;
+  if (bc == KFVM_BC_REFLECTING) {
+    static const double hy[3][5] = {{1, -1, 1, 1, 1}, {1, 1, -1, 1, 1}, {1, 1, 1, -1, 1}};
+    static const double mh[3][9] = {{1, -1, 1, 1, 1, -1, 1, 1, 1}, {1, 1, -1, 1, 1, 1, -1, 1, 1},
+                                    {1, 1, 1, -1, 1, 1, 1, -1, 1}};
+    return glm ? mh[d][v] : hy[d][v];
+  }
+  if (bc == KFVM_BC_NOSLIP) {
+    static const double hy[5] = {1, -1, -1, -1, 1};
+    static const double mh[3][9] = {{1, -1, -1, -1, 1, -1, 1, 1, 1}, {1, -1, -1, -1, 1, 1, -1, 1, 1},
+                                    {1, -1, -1, -1, 1, 1, 1, -1, 1}};
+    return glm ? mh[d][v] : hy[v];
+  }
+  return 1.0;
+}
+
 void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
   const int r = KFVM_RAD;
   auto &c = S.cfg;
@@ -521,9 +542,9 @@ void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
             B[S.ui(-r + h, j, k, v)] = B[S.ui(S.nx - r + h, j, k, v)];
             B[S.ui(S.nx + h, j, k, v)] = B[S.ui(h, j, k, v)];
           } else {
-            B[S.ui(-h - 1, j, k, v)] = B[S.ui(h, j, k, v)];
+            B[S.ui(-h - 1, j, k, v)] = wall_coef(S, 0, v) * B[S.ui(h, j, k, v)];
+            B[S.ui(S.nx + h, j, k, v)] = wall_coef(S, 1, v) * B[S.ui(S.nx - h - 1, j, k, v)];
           }
-          if (c.bc[1] != KFVM_BC_PERIODIC) B[S.ui(S.nx + h, j, k, v)] = B[S.ui(S.nx - h - 1, j, k, v)];
         }
   // y: i over the full halo range, k interior
   for (int64_t k = 0; k < S.nz; k++)
@@ -534,9 +555,9 @@ void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
             B[S.ui(i, -r + h, k, v)] = B[S.ui(i, S.ny - r + h, k, v)];
             B[S.ui(i, S.ny + h, k, v)] = B[S.ui(i, h, k, v)];
           } else {
-            B[S.ui(i, -h - 1, k, v)] = B[S.ui(i, h, k, v)];
+            B[S.ui(i, -h - 1, k, v)] = wall_coef(S, 2, v) * B[S.ui(i, h, k, v)];
+            B[S.ui(i, S.ny + h, k, v)] = wall_coef(S, 3, v) * B[S.ui(i, S.ny - h - 1, k, v)];
           }
-          if (c.bc[3] != KFVM_BC_PERIODIC) B[S.ui(i, S.ny + h, k, v)] = B[S.ui(i, S.ny - h - 1, k, v)];
         }
   if (S.dim == 3) {
     for (int64_t j = -r; j < S.ny + r; j++)
@@ -547,9 +568,9 @@ void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
               B[S.ui(i, j, -r + h, v)] = B[S.ui(i, j, S.nz - r + h, v)];
               B[S.ui(i, j, S.nz + h, v)] = B[S.ui(i, j, h, v)];
             } else {
-              B[S.ui(i, j, -h - 1, v)] = B[S.ui(i, j, h, v)];
+              B[S.ui(i, j, -h - 1, v)] = wall_coef(S, 4, v) * B[S.ui(i, j, h, v)];
+              B[S.ui(i, j, S.nz + h, v)] = wall_coef(S, 5, v) * B[S.ui(i, j, S.nz - h - 1, v)];
             }
-            if (c.bc[5] != KFVM_BC_PERIODIC) B[S.ui(i, j, S.nz + h, v)] = B[S.ui(i, j, S.nz - h - 1, v)];
           }
   }
 }
@@ -561,14 +582,20 @@ void set_face_bcs(orc_solver &S) {
   auto cp = [&](double *dst, const double *src) {
     for (int q = 0; q < nqf * nv; q++) dst[q] = src[q];
   };
+  // wall faces: the outer slot is the inner one times the face's coefficients
+  // (FaceBc*_K<outflow / reflecting>, BoundaryConditions_K.H:529-570)
+  auto cpw = [&](double *dst, const double *src, int f) {
+    for (int q = 0; q < nqf; q++)
+      for (int v = 0; v < nv; v++) dst[q * nv + v] = wall_coef(S, f, v) * src[q * nv + v];
+  };
   for (int64_t k = 0; k < S.nz; k++)
     for (int64_t j = 0; j < S.ny; j++) {
       if (c.bc[0] == KFVM_BC_PERIODIC) {
         cp(S.fs(0, S.nx, j, k, 1, 0), S.fs(0, 0, j, k, 1, 0));
         cp(S.fs(0, 0, j, k, 0, 0), S.fs(0, S.nx, j, k, 0, 0));
       } else {
-        cp(S.fs(0, 0, j, k, 0, 0), S.fs(0, 0, j, k, 1, 0));
-        cp(S.fs(0, S.nx, j, k, 1, 0), S.fs(0, S.nx, j, k, 0, 0));
+        cpw(S.fs(0, 0, j, k, 0, 0), S.fs(0, 0, j, k, 1, 0), 0);
+        cpw(S.fs(0, S.nx, j, k, 1, 0), S.fs(0, S.nx, j, k, 0, 0), 1);
       }
     }
   for (int64_t k = 0; k < S.nz; k++)
@@ -577,8 +604,8 @@ void set_face_bcs(orc_solver &S) {
         cp(S.fs(1, i, S.ny, k, 1, 0), S.fs(1, i, 0, k, 1, 0));
         cp(S.fs(1, i, 0, k, 0, 0), S.fs(1, i, S.ny, k, 0, 0));
       } else {
-        cp(S.fs(1, i, 0, k, 0, 0), S.fs(1, i, 0, k, 1, 0));
-        cp(S.fs(1, i, S.ny, k, 1, 0), S.fs(1, i, S.ny, k, 0, 0));
+        cpw(S.fs(1, i, 0, k, 0, 0), S.fs(1, i, 0, k, 1, 0), 2);
+        cpw(S.fs(1, i, S.ny, k, 1, 0), S.fs(1, i, S.ny, k, 0, 0), 3);
       }
     }
   if (S.dim == 3) {
@@ -588,8 +615,8 @@ void set_face_bcs(orc_solver &S) {
           cp(S.fs(2, i, j, S.nz, 1, 0), S.fs(2, i, j, 0, 1, 0));
           cp(S.fs(2, i, j, 0, 0, 0), S.fs(2, i, j, S.nz, 0, 0));
         } else {
-          cp(S.fs(2, i, j, 0, 0, 0), S.fs(2, i, j, 0, 1, 0));
-          cp(S.fs(2, i, j, S.nz, 1, 0), S.fs(2, i, j, S.nz, 0, 0));
+          cpw(S.fs(2, i, j, 0, 0, 0), S.fs(2, i, j, 0, 1, 0), 4);
+          cpw(S.fs(2, i, j, S.nz, 1, 0), S.fs(2, i, j, S.nz, 0, 0), 5);
         }
       }
   }
