@@ -135,6 +135,11 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi's start-up (NVML initialisation) stalls the device for some
+        # milliseconds: let it finish before the timed region begins
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < 3.0 and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -245,6 +250,19 @@ def train_indicator(workload, seed=1):
     return w, {"train_grid": [cfg.nx] * dim, "samples": n, "troubled": npos, "loss_first": l0, "loss_last": l1}
 
 
+def kernel_breakdown(solver, steps):
+    """Device time per kernel class (CUDA events around each launch on the solver's
+    stream) over `steps` more steps: {class: (ms, launches)}."""
+    import torch
+    solver.set_timing(True)
+    for _ in range(steps):
+        solver.take_step()
+    torch.cuda.synchronize()
+    per_class = solver.timing()
+    solver.set_timing(False)
+    return per_class
+
+
 def time_form(cfg, ic, prec, steps, warmup, mlp_weights=None):
     """Zone-updates/s of one arithmetic form: device time of `steps` accepted-step
     attempts after `warmup`, CUDA events on the solver's stream."""
@@ -259,7 +277,6 @@ def time_form(cfg, ic, prec, steps, warmup, mlp_weights=None):
     for _ in range(warmup):
         s.take_step()
     stream = torch.cuda.ExternalStream(s.stream_handle())
-    s.set_timing(True)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -269,7 +286,7 @@ def time_form(cfg, ic, prec, steps, warmup, mlp_weights=None):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    per_class = s.timing()
+    per_class = kernel_breakdown(s, min(steps, 2))
     out = {"value": acc * abi.ncells(cfg) / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
            "steps": steps, "accepted_steps": acc,
            "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0}}
@@ -306,7 +323,6 @@ def run_ours(args):
         rhs0 = solver.take_step().n_rhs
 
     stream = torch.cuda.ExternalStream(solver.stream_handle())
-    solver.set_timing(True)
     launches0 = solver.launch_count()
     sampler = ClockSampler(local)
     if ws > 1:
@@ -331,8 +347,10 @@ def run_ours(args):
     sampler.stop()
     ms = e0.elapsed_time(e1)
     launches = solver.launch_count() - launches0
-    per_class = solver.timing()
-    solver.set_timing(False)
+    # the per-class breakdown comes from further steps: its events around every
+    # launch would take launch slots inside the timed steps
+    breakdown_steps = max(1, min(args.steps, 4))
+    per_class = kernel_breakdown(solver, breakdown_steps)
 
     # max over ranks of the device time, sum of the work
     t_max, work = replica_totals(ms, accepted * n, ws, "cuda")
@@ -419,7 +437,8 @@ def run_ours(args):
            "rhs_evals": int(n_rhs), "rhs_cell_rate": n_rhs * n / (t_max / 1e3) if n_rhs else None,
            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "path_roofline": path_roofline,
            "kernel_share": share,
-           "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0}}
+           "kernel_ms": {k: round(v[0], 3) for k, v in per_class.items() if v[1] > 0},
+           "kernel_breakdown_steps": breakdown_steps}
     out["clocks"] = sampler.summary()
 
     solver.close()

@@ -159,7 +159,11 @@ class Solver:
             self.h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter shutdown the module globals may already be gone
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def init_ic(self, ic_kind, seed=12345):
         _check(lib().kfvm_init_ic(self.h, int(ic_kind), C.c_uint64(seed)), "kfvm_init_ic")
