@@ -43,7 +43,7 @@ enum kfvm_rk {
 /* BCType (src/Types.H:40) without "user": a reflecting wall mirrors the state
  * and negates the normal momentum (and the normal magnetic field for GLM-MHD); a
  * no-slip wall negates every momentum component (and the normal magnetic field),
- * with the coefficient tables of src/physics/*\/<Eq>_BCCoeffs.H. */
+ * with the coefficient tables of src/physics/<eq>/<Eq>_BCCoeffs.H. */
 enum kfvm_bc { KFVM_BC_PERIODIC = 0, KFVM_BC_OUTFLOW = 1, KFVM_BC_REFLECTING = 2, KFVM_BC_NOSLIP = 3 };
 /* src/Types.H:40 */
 enum kfvm_ts_status { KFVM_TS_ACCEPTED = 0, KFVM_TS_TOLERANCE = 1, KFVM_TS_UNPHYSICAL = 2 };

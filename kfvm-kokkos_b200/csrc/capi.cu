@@ -579,7 +579,8 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if (!cfg || !out) return fail(KFVM_ERR_ARG, "null argument");
   *out = nullptr;
   if (cfg->dim != 2 && cfg->dim != 3) return fail(KFVM_ERR_ARG, "dim must be 2 or 3");
-  if (cfg->nq != 2) return fail(KFVM_ERR_ARG, "the GPU path supports NUM_QUAD_PTS = 2");
+  if (!(cfg->nq == 2 || (cfg->nq == 3 && cfg->dim == 2)))
+    return fail(KFVM_ERR_ARG, "the GPU path supports NUM_QUAD_PTS = 2, and 3 in 2D");
   if (cfg->eq < 0 || cfg->eq > 2) return fail(KFVM_ERR_ARG, "unknown equation type");
   if (cfg->rs < 0 || cfg->rs > 2) return fail(KFVM_ERR_ARG, "unknown Riemann solver");
   if (cfg->eq == KFVM_EQ_MHD_GLM && cfg->rs == KFVM_RS_HLLC)
@@ -634,6 +635,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   }
   g.gamma = cfg->gamma;
   g.rs = cfg->rs;
+  g.nq = cfg->nq;
   s->dmin = cfg->dim == 2 ? std::fmin(g.dx, g.dy) : std::fmin(g.dx, std::fmin(g.dy, g.dz));
 
   DevStencil hS;
@@ -670,7 +672,8 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if ((e = cudaEventCreate(&s->ev0)) != cudaSuccess) return cleanup(e, "event");
   if ((e = cudaEventCreate(&s->ev1)) != cudaSuccess) return cleanup(e, "event");
   const size_t nv = s->nv, n = g.n;
-  const int nqf = cfg->dim == 2 ? 2 : 4, nqc = cfg->dim == 2 ? 4 : 8;
+  const int nqf = cfg->dim == 2 ? cfg->nq : cfg->nq * cfg->nq;
+  const int nqc = cfg->dim == 2 ? cfg->nq * cfg->nq : cfg->nq * cfg->nq * cfg->nq;
   auto dalloc = [&](void **p, size_t bytes) { return cudaMalloc(p, bytes); };
   if ((e = dalloc((void **)&s->dS, sizeof(DevStencil))) != cudaSuccess) return cleanup(e, "alloc");
   for (int b = 0; b < 3; b++)
@@ -884,6 +887,7 @@ int kfvm_set_precision(kfvm_solver *s, int32_t precision) {
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
     if (major != 10) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form needs an sm_100 device");
+    if (s->g.nq != 2) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form is built for 2 Gauss points");
   }
   s->precision = precision;
   return KFVM_OK;
@@ -1172,7 +1176,7 @@ int kfvm_selftest_rcp(int64_t n, uint64_t seed, int64_t *max_ulp, double *max_re
 int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
   if (!s || !out || dir < 0 || dir >= s->dim) return fail(KFVM_ERR_ARG, "bad argument");
   const kfvm::Grid &g = s->g;
-  const int nqf = s->dim == 2 ? 2 : 4, nv = s->nv;
+  const int nqf = s->dim == 2 ? s->g.nq : s->g.nq * s->g.nq, nv = s->nv;
   const int64_t nf = g.nface[dir];
   CK(cudaMemcpyAsync(out, s->F[dir], (size_t)2 * nqf * nv * nf * sizeof(double), cudaMemcpyDeviceToHost,
                      s->stream));

@@ -1,4 +1,4 @@
-// ic.cu -- initial conditions as cell averages by Q^d Gauss quadrature
+// ic.cu -- initial conditions as cell averages by Q^d Gauss quadrature (Q = 2 or 3)
 // (IntegrateIC_K, src/numeric/Numeric_K.H:31-107 of slug-cfd/kfvm-kokkos) for
 // the built-in problems.  The pointwise formulas are the problem library's
 // InitialCondition.H functions with the benchmark problems' parameters:
@@ -125,8 +125,23 @@ __global__ void __launch_bounds__(128) ic_kernel(IcParams p, uint64_t seed, doub
   const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
   const int64_t k = blockIdx.z;
   if (i >= g.nx || j >= g.ny) return;
-  const double ab[2] = {-0.577350269189625764509148 / 2.0, 0.577350269189625764509148 / 2.0};
-  const double wt[2] = {1.0 / 2.0, 1.0 / 2.0};
+  // Gauss-Legendre rule on (-1/2, 1/2) in the reference's point order
+  // (src/numeric/Numeric.cpp:14-27), g.nq = 2 or 3 points per direction
+  const int nq = g.nq;
+  double ab[3], wt[3];
+  if (nq == 3) {
+    ab[0] = 0.0;
+    ab[1] = -0.7745966692414833770358530 / 2.0;
+    ab[2] = 0.7745966692414833770358530 / 2.0;
+    wt[0] = 0.8888888888888888888888888 / 2.0;
+    wt[1] = wt[2] = 0.5555555555555555555555555 / 2.0;
+  } else {
+    ab[0] = -0.577350269189625764509148 / 2.0;
+    ab[1] = 0.577350269189625764509148 / 2.0;
+    ab[2] = 0.0;
+    wt[0] = wt[1] = 1.0 / 2.0;
+    wt[2] = 0.0;
+  }
   const double xc = g.dx * (double(i) + 0.5) + p.xlo, yc = g.dy * (double(j) + 0.5) + p.ylo;
   const double zc = g.dz * (double(k) + 0.5) + p.zlo;
   double noise = 0.0;
@@ -138,9 +153,9 @@ __global__ void __launch_bounds__(128) ic_kernel(IcParams p, uint64_t seed, doub
   double acc[NV];
 #pragma unroll
   for (int v = 0; v < NV; v++) acc[v] = 0.0;
-  const int nzq = DIM == 3 ? 2 : 1;
-  for (int a = 0; a < 2; a++)
-    for (int b = 0; b < 2; b++)
+  const int nzq = DIM == 3 ? nq : 1;
+  for (int a = 0; a < nq; a++)
+    for (int b = 0; b < nq; b++)
       for (int e = 0; e < nzq; e++) {
         const double x = ab[a] * g.dx + xc, y = ab[b] * g.dy + yc;
         const double z = DIM == 3 ? ab[e] * g.dz + zc : p.zlo;

@@ -101,13 +101,13 @@ constexpr uint32_t kHeavyCell = 0x3fffffffu;
 // The stencil has 4m + 1 cells (13 in 2D, 33 in 3D): the first 4m go through the
 // MMAs in m K-steps and the last one is added in the epilogue by one FMA per row
 // and variable, which spares a K-step that would be three quarters padding.
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ = 2>
 struct DmmaShape {
-  static constexpr int NR = LinRows<DIM, EQ>::NROWS;
+  static constexpr int NR = LinRows<DIM, EQ, NQ>::NROWS;
   static constexpr int NT = (NR + 7) / 8;
-  static constexpr int NK = (Cfg<DIM, EQ>::C - 1) / 4;
+  static constexpr int NK = (Cfg<DIM, EQ, NQ>::C - 1) / 4;
   static constexpr int BSIZE = NK * NT * 32;
-  static_assert((Cfg<DIM, EQ>::C - 1) % 4 == 0, "stencil of 4m + 1 cells");
+  static_assert((Cfg<DIM, EQ, NQ>::C - 1) % 4 == 0, "stencil of 4m + 1 cells");
   static_assert(BSIZE <= kDmmaMaxB, "B fragment table too small");
 };
 
@@ -117,15 +117,15 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ>
 __global__ void __launch_bounds__(128)
     recon_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
                  double *__restrict__ F0,
                  double *__restrict__ F1, double *__restrict__ F2, float *__restrict__ W0,
                  float *__restrict__ W1, float *__restrict__ W2, double *__restrict__ src,
                  uint8_t *__restrict__ status, double2 *__restrict__ lamvel, double *__restrict__ bnd) {
-  using T = Cfg<DIM, EQ>;
-  using Sh = DmmaShape<DIM, EQ>;
+  using T = Cfg<DIM, EQ, NQ>;
+  using Sh = DmmaShape<DIM, EQ, NQ>;
   constexpr int NV = T::NV, NT = Sh::NT, NK = Sh::NK;
   __shared__ double tile[6][PosTile<DIM>::N];
   __shared__ double sB[Sh::BSIZE];
@@ -210,19 +210,21 @@ __global__ void __launch_bounds__(128)
       bd.minEint = sBd[2][threadIdx.y * kBlockX + cx];
 #pragma unroll
       for (int t = 0; t < NT; t++) {
-        // rows 8t + 2(lane%4) + e: in 3D (4 points per face) the tile is direction t,
-        // face 2t + (lane%4)/2, points 2(lane%2) + e; in 2D (2 points per face)
-        // face 4t + lane%4, point e
-        const int f = DIM == 3 ? 2 * t + ((lane & 3) >> 1) : 4 * t + (lane & 3);
-        const int d = DIM == 3 ? t : (f >> 1);
-        const int hi = f & 1;
-        const int64_t nf = g.nface[d];
-        const int64_t fidx = ((k + (d == 2 && hi)) * g.fdim[d][1] + (j + (d == 1 && hi))) * g.fdim[d][0] +
-                             (i + (d == 0 && hi));
-        const int slot = hi ? 0 : 1;
+        const int rw0 = t * 8 + 2 * (lane & 3);
 #pragma unroll
         for (int e = 0; e < 2; e++) {
-          const int rw = t * 8 + 2 * (lane & 3) + e;
+          // row 8t + 2(lane%4) + e: face point q = row % NQF of face f = row / NQF
+          // (rows past the face points are interior points); with an even NQF both
+          // rows of a lane lie on one face, which the compiler then computes once
+          const int rw = rw0 + e;
+          const int fr = (T::NQF % 2 == 0 ? rw0 : rw) / T::NQF;
+          const int f = fr < T::NF ? fr : 0;
+          const int d = f >> 1;
+          const int hi = f & 1;
+          const int64_t nf = g.nface[d];
+          const int64_t fidx = ((k + (d == 2 && hi)) * g.fdim[d][1] + (j + (d == 1 && hi))) * g.fdim[d][0] +
+                               (i + (d == 0 && hi));
+          const int slot = hi ? 0 : 1;
           if (rw < Sh::NR) {
             double st[NV];
 #pragma unroll
@@ -231,13 +233,13 @@ __global__ void __launch_bounds__(128)
             const double ei = Eos<EQ>::eint(st);
             inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
             if (rw < T::NF * T::NQF) {
-              const int q = DIM == 3 ? 2 * (lane & 1) + e : e;
-              double *Fd = DIM == 3 ? F[t < 3 ? t : 0] : F[d];
+              const int q = rw % T::NQF;
+              double *Fd = F[d];
               const int64_t a = (int64_t)((slot * T::NQF + q) * NV) * nf + fidx;
 #pragma unroll
               for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
               if (wantInd)
-                (DIM == 3 ? W[t < 3 ? t : 0] : W[d])[(int64_t)(slot * T::NQF + q) * nf + fidx] =
+                W[d][(int64_t)(slot * T::NQF + q) * nf + fidx] =
                     Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
               if constexpr (T::SRC) {
                 // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
@@ -303,14 +305,14 @@ __device__ __forceinline__ void kxrcf_face(const Grid &g, int fc, int64_t i, int
   }
 }
 
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ>
 __global__ void __launch_bounds__(128)
     flag_kernel(const double *__restrict__ U, Grid g, const float *__restrict__ W0,
                 const float *__restrict__ W1, const float *__restrict__ W2,
                 const double *__restrict__ F0, const double *__restrict__ F1,
                 const double *__restrict__ F2, const double *__restrict__ theta,
                 uint8_t *__restrict__ flag, DevScalars *__restrict__ sc, double wThresh) {
-  using T = Cfg<DIM, EQ>;
+  using T = Cfg<DIM, EQ, NQ>;
   constexpr int NV = T::NV;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t j = blockIdx.y * (int64_t)blockDim.y + threadIdx.y;
@@ -455,15 +457,15 @@ __global__ void __launch_bounds__(256)
 // then one thread per cell converts back to conserved variables and runs the
 // positivity procedure (PositivityPreserve_K) and the stores.  Each sum keeps the
 // reference's order.
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ = 2>
 struct HeavyShape {
-  using T = Cfg<DIM, EQ>;
-  static constexpr int NR = LinRows<DIM, EQ>::NROWS;          // face points, then interior points
+  using T = Cfg<DIM, EQ, NQ>;
+  static constexpr int NR = LinRows<DIM, EQ, NQ>::NROWS;      // face points, then interior points
   static constexpr int NSUM = T::C + T::CC + T::NB * T::CB;   // stencil cells over all substencils
   static constexpr int NIP = (T::NI + 1) & ~1;                // derivative rows padded to pairs
   static constexpr int DER = NIP * NSUM;                      // derivative weights [s][p][i]
-  static constexpr int FW = NR * NSUM;                        // reconstruction weights [s][p][row]
-  static_assert(NR % 2 == 0, "rows in pairs");
+  static constexpr int NRP = (NR + 1) & ~1;                  // rows padded to pairs
+  static constexpr int FW = NRP * NSUM;                       // reconstruction weights [s][p][row]
   static constexpr int CELLS = 32;
   static constexpr size_t BYTES = (size_t)(DER + FW + CELLS * NR * T::NV + CELLS * 2) * sizeof(double) +
                                   (size_t)T::NB * T::CB * sizeof(int);
@@ -475,11 +477,11 @@ struct HeavyShape {
 
 // PositivityPreserve_K's theta procedure on a cell's states held as [row][v]
 // (rows: face points f*NQF+q, then interior points); Common_K.H:299-643
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ>
 __device__ double pos_apply_rows(const double *__restrict__ ref, const PosBounds &bd, double *__restrict__ rs) {
-  using T = Cfg<DIM, EQ>;
+  using T = Cfg<DIM, EQ, NQ>;
   using E = Eos<EQ>;
-  constexpr int NV = T::NV, NR = LinRows<DIM, EQ>::NROWS;
+  constexpr int NV = T::NV, NR = LinRows<DIM, EQ, NQ>::NROWS;
   const double rDens = bd.rDens, minDens = bd.minDens, maxDens = bd.maxDens, minEint = bd.minEint;
   const double rDP = maxDens - rDens, rDM = rDens - minDens;
   double thD = 1.0;
@@ -523,14 +525,14 @@ __device__ double pos_apply_rows(const double *__restrict__ ref, const PosBounds
   return fmin(thD, thP);
 }
 
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ>
 __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
     heavy_var_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S,
                      double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
                      double *__restrict__ F2, double *__restrict__ src, const uint32_t *__restrict__ heavy,
                      const double *__restrict__ bnd, DevScalars *__restrict__ sc, JudgeArgs jd) {
-  using T = Cfg<DIM, EQ>;
-  using H = HeavyShape<DIM, EQ>;
+  using T = Cfg<DIM, EQ, NQ>;
+  using H = HeavyShape<DIM, EQ, NQ>;
   using E = Eos<EQ>;
   constexpr int NV = T::NV, NR = H::NR;
   extern __shared__ __align__(16) double hsm[];
@@ -551,10 +553,10 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
   }
   for (int t = tid; t < H::FW; t += nt) {
     int s = 0;
-    while (s + 1 < T::NSUB && t >= NR * H::off(s + 1)) s++;
-    const int r = t - NR * H::off(s), p = r / NR, row = r % NR;
+    while (s + 1 < T::NSUB && t >= H::NRP * H::off(s + 1)) s++;
+    const int r = t - H::NRP * H::off(s), p = r / H::NRP, row = r % H::NRP;
     const int nfq = T::NF * T::NQF;
-    sFw[t] = row < nfq ? st.face_w[s][row / T::NQF][row % T::NQF][p] : st.cell_w[s][row - nfq][p];
+    sFw[t] = row >= NR ? 0.0 : (row < nfq ? st.face_w[s][row / T::NQF][row % T::NQF][p] : st.cell_w[s][row - nfq][p]);
   }
   for (int t = tid; t < T::NB * T::CB; t += nt) sSub[t] = (int)st.sub_idx[t / T::CB][t % T::CB];
   __syncthreads();
@@ -666,15 +668,15 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 #pragma unroll 1
       for (int s = 0; s < T::NSUB; s++) {
         const int n = H::n(s);
-        const double *Wr = sFw + NR * H::off(s);
-        double tt[NR];
+        const double *Wr = sFw + H::NRP * H::off(s);
+        double tt[H::NRP];
 #pragma unroll
-        for (int r = 0; r < NR; r++) tt[r] = 0.0;
+        for (int r = 0; r < H::NRP; r++) tt[r] = 0.0;
         for (int p = 0; p < n; p++) {
           const double val = Vf[cellOf(s, p)];
-          const double2 *W2 = reinterpret_cast<const double2 *>(Wr + p * NR);
+          const double2 *W2 = reinterpret_cast<const double2 *>(Wr + p * H::NRP);
 #pragma unroll
-          for (int r2 = 0; r2 < NR / 2; r2++) {
+          for (int r2 = 0; r2 < H::NRP / 2; r2++) {
             const double2 w = W2[r2];
             tt[2 * r2] += w.x * val;
             tt[2 * r2 + 1] += w.y * val;
@@ -727,7 +729,7 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
       } else {
         bd = pos_bounds<DIM, EQ>(Uc, g);
       }
-      theta[c] = pos_apply_rows<DIM, EQ>(ref, bd, rs);
+      theta[c] = pos_apply_rows<DIM, EQ, NQ>(ref, bd, rs);
       if constexpr (T::SRC) {
         for (int r = 0; r < T::NF * T::NQF; r++) {
           const double *u = rs + r * NV;
@@ -771,11 +773,11 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 // more warps hide the FP64 latency.  The quadrature-weighted sum over a face's
 // points goes through shared memory in point order, and the max wave speed
 // through a warp maximum and an atomic only from warps that raise it.
-template <int DIM, int EQ, int D>
-__global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4), EQ == EQ_GLM ? 1 : (DIM == 2 ? 16 : 8))
+template <int DIM, int EQ, int D, int NQ>
+__global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF, EQ == EQ_GLM ? 1 : (DIM == 2 ? 16 : 8))
     riemann_kernel(const double *__restrict__ F, double *__restrict__ G, Grid g,
                    DevScalars *__restrict__ sc) {
-  using T = Cfg<DIM, EQ>;
+  using T = Cfg<DIM, EQ, NQ>;
   using E = Eos<EQ>;
   constexpr int NV = T::NV, NQF = T::NQF;
   __shared__ double part[NQF][NV][32];
@@ -794,20 +796,13 @@ __global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4), EQ == EQ_GLM ? 1 : (D
     // periodic partner face, or copy the interior slot at an outflow boundary
     int64_t f0 = fidx, f1 = fidx;
     int s0 = 0, s1 = 1;
-    unsigned flipL = 0u, flipR = 0u; // wall mirrors (reflecting / no-slip)
     const int64_t stride = D == 0 ? 1 : (D == 1 ? fx : fx * fy);
     if (m == 0) {
       if (g.bc[2 * D] == KFVM_BC_PERIODIC) f0 = fidx + nd * stride;
-      else {
-        s0 = 1;
-        flipL = g.bflip[2 * D];
-      }
+      else s0 = 1;
     } else if (m == nd) {
       if (g.bc[2 * D + 1] == KFVM_BC_PERIODIC) f1 = fidx - nd * stride;
-      else {
-        s1 = 0;
-        flipR = g.bflip[2 * D + 1];
-      }
+      else s1 = 0;
     }
     const double ch = EQ == EQ_GLM ? __longlong_as_double((long long)sc->glm_lam_bits) -
                                          __longlong_as_double((long long)sc->glm_vel_bits)
@@ -819,11 +814,19 @@ __global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4), EQ == EQ_GLM ? 1 : (D
     for (int v = 0; v < NV; v++) {
       uL[v] = __ldg(pL + v * nf);
       uR[v] = __ldg(pR + v * nf);
-      if ((flipL >> v) & 1u) uL[v] = -uL[v];
-      if ((flipR >> v) & 1u) uR[v] = -uR[v];
+    }
+    if (s0 == 1 || s1 == 0) {
+      // a wall face (reflecting / no-slip) mirrors the inner state with sign flips
+      const unsigned flipL = s0 == 1 ? g.bflip[2 * D] : 0u, flipR = s1 == 0 ? g.bflip[2 * D + 1] : 0u;
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        if ((flipL >> v) & 1u) uL[v] = -uL[v];
+        if ((flipR >> v) & 1u) uR[v] = -uR[v];
+      }
     }
     vmax = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
-    const double wq = DIM == 2 ? 0.5 : 0.25; // Gauss weights 1/2 (x 1/2 in 3D)
+    // Gauss weight of point q (3D: the product of the two transverse weights)
+    const double wq = DIM == 2 ? gl_wt<NQ>(q) : gl_wt<NQ>(q / NQ) * gl_wt<NQ>(q % NQ);
 #pragma unroll
     for (int v = 0; v < NV; v++) part[q][v][threadIdx.x] = wq * Fq[v];
   }
@@ -845,18 +848,28 @@ __global__ void __launch_bounds__(32 * (DIM == 2 ? 2 : 4), EQ == EQ_GLM ? 1 : (D
 // ---------------------------------------------------------------------------
 // GLM source terms at the interior points of a cell (SourceTerms_K<MHD_GLM>,
 // MHD_GLM_K.H:316-547, zero user forcing), added to rhs with the cell quadrature
-template <int DIM>
+template <int DIM, int NQ>
 __device__ void glm_sources(const double *__restrict__ Uc, const Grid &g, int64_t i, int64_t j,
                             int64_t k, int64_t c, const double *__restrict__ F0,
                             const double *__restrict__ F1, const double *__restrict__ F2,
                             const double *__restrict__ src, double th, double *rhs) {
-  using T = Cfg<DIM, EQ_GLM>;
-  constexpr int NV = 9, NQ = 2, NQF = T::NQF;
+  using T = Cfg<DIM, EQ_GLM, NQ>;
+  constexpr int NV = 9, NQF = T::NQF;
   constexpr int nzq = DIM == 3 ? NQ : 1;
-  // LGL -> GL differentiation matrix, 2 points (Numeric.cpp:50-52)
-  const double Dm[2][4] = {
+  static_assert(NQ == 2 || NQ == 3, "differentiation matrices for 2 and 3 points");
+  // LGL -> GL differentiation matrix, row-major NQ x (NQ + 2): output point, inputs
+  // [left face, interior points in abscissa order, right face] (Numeric.cpp:50-70)
+  constexpr double D2[2][4] = {
       {-2.7320508075688767, 1.732050807568877, 1.7320508075688767, -0.7320508075688767},
       {0.7320508075688767, -1.7320508075688767, -1.732050807568877, 2.7320508075688767}};
+  constexpr double D3[3][5] = {
+      {1.5, 0.0, -3.2274861218395139, 3.2274861218395148, -1.5},
+      {-5.323790007724451, 2.06559111797729, 3.872983346207419, -1.2909944487358063, 0.6762099922755506},
+      {-0.6762099922755498, -2.0655911179772883, 1.2909944487358065, -3.8729833462074184, 5.323790007724451}};
+  auto Dm = [&](int r, int col) {
+    if constexpr (NQ == 3) return D3[r][col];
+    else return D2[r][col];
+  };
   const double *Fd[3] = {F0, F1, F2};
   // face value of variable v at point q of face (d, index fi,fj,fk), slot s with face BCs
   auto fv = [&](int d, int64_t fi, int64_t fj, int64_t fk, int s, int q, int v) {
@@ -882,7 +895,9 @@ __device__ void glm_sources(const double *__restrict__ Uc, const Grid &g, int64_
     const double x = Fd[d][((int64_t)(s * NQF + q) * NV + v) * g.nface[d] + fidx];
     return (flip >> v) & 1u ? -x : x;
   };
-  const double wt[2] = {0.5, 0.5};
+  double wt[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; q++) wt[q] = gl_wt<NQ>(q);
   double divB = 0.0;
   for (int nQ = 0; nQ < NQ; nQ++)
     for (int nS = 0; nS < nzq; nS++) {
@@ -924,20 +939,20 @@ __device__ void glm_sources(const double *__restrict__ Uc, const Grid &g, int64_
         } else {
           {
             const int fIdx = DIM == 2 ? nR : nR * NQ + nS;
-            double d = Dm[nQ][0] * fv(0, i, j, k, 1, fIdx, PSI) + Dm[nQ][NQ + 1] * fv(0, i + 1, j, k, 0, fIdx, PSI);
-            for (int m = 1; m <= NQ; m++) d += Dm[nQ][m] * cv(m - 1, nR, nS, PSI);
+            double d = Dm(nQ, 0) * fv(0, i, j, k, 1, fIdx, PSI) + Dm(nQ, NQ + 1) * fv(0, i + 1, j, k, 0, fIdx, PSI);
+            for (int m = 1; m <= NQ; m++) d += Dm(nQ, m) * cv(m - 1, nR, nS, PSI);
             dpx = d / g.dx;
           }
           {
             const int fIdx = DIM == 2 ? nQ : nQ * NQ + nS;
-            double d = Dm[nR][0] * fv(1, i, j, k, 1, fIdx, PSI) + Dm[nR][NQ + 1] * fv(1, i, j + 1, k, 0, fIdx, PSI);
-            for (int m = 1; m <= NQ; m++) d += Dm[nR][m] * cv(nQ, m - 1, nS, PSI);
+            double d = Dm(nR, 0) * fv(1, i, j, k, 1, fIdx, PSI) + Dm(nR, NQ + 1) * fv(1, i, j + 1, k, 0, fIdx, PSI);
+            for (int m = 1; m <= NQ; m++) d += Dm(nR, m) * cv(nQ, m - 1, nS, PSI);
             dpy = d / g.dy;
           }
           if (DIM == 3) {
             const int fIdx = nQ * NQ + nR;
-            double d = Dm[nS][0] * fv(2, i, j, k, 1, fIdx, PSI) + Dm[nS][NQ + 1] * fv(2, i, j, k + 1, 0, fIdx, PSI);
-            for (int m = 1; m <= NQ; m++) d += Dm[nS][m] * cv(nQ, nR, m - 1, PSI);
+            double d = Dm(nS, 0) * fv(2, i, j, k, 1, fIdx, PSI) + Dm(nS, NQ + 1) * fv(2, i, j, k + 1, 0, fIdx, PSI);
+            for (int m = 1; m <= NQ; m++) d += Dm(nS, m) * cv(nQ, nR, m - 1, PSI);
             dpz = d / g.dz;
           }
         }
@@ -1093,7 +1108,7 @@ __device__ void viscous(const double (*vt)[PosTile<DIM>::N], const Grid &g, int 
 
 // ---------------------------------------------------------------------------
 // flux divergence (+ viscous, + GLM sources) fused with the RK register update
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ>
 __global__ void __launch_bounds__(128)
     stage_kernel(const double *__restrict__ U, double *__restrict__ Unext,
                  const double *__restrict__ Uprev, double *__restrict__ Uhat,
@@ -1104,7 +1119,7 @@ __global__ void __launch_bounds__(128)
                  const double *__restrict__ src, const double *__restrict__ theta, int mode,
                  StageCoef co, double Re, double Pr, double atol, double rtol,
                  double *__restrict__ part) {
-  using T = Cfg<DIM, EQ>;
+  using T = Cfg<DIM, EQ, NQ>;
   using E = Eos<EQ>;
   constexpr int NV = T::NV;
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1156,7 +1171,7 @@ __global__ void __launch_bounds__(128)
         for (int v = 0; v < NV; v++) r[v] += (G2[v * g.nface[2] + f2] - G2[v * g.nface[2] + f2 + sz]) * g.rdz;
       }
     }
-    if constexpr (EQ == EQ_GLM) glm_sources<DIM>(Uc, g, i, j, k, c, F0, F1, F2, src, theta[c], r);
+    if constexpr (EQ == EQ_GLM) glm_sources<DIM, NQ>(Uc, g, i, j, k, c, F0, F1, F2, src, theta[c], r);
     if constexpr (EQ == EQ_NS) viscous<DIM>(vt, g, threadIdx.x, threadIdx.y, Re, Pr, r);
 
     if (mode == STAGE_EVAL) {
@@ -1287,7 +1302,7 @@ static dim3 cell_grid(const Grid &g) {
               (unsigned)g.nz);
 }
 
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ>
 struct Launch {
   static constexpr int NV = Eos<EQ>::NV;
   static cudaError_t bc(double *U, const Grid &g, cudaStream_t s) {
@@ -1300,13 +1315,13 @@ struct Launch {
   static cudaError_t recon(const double *U, const Grid &g, const DevStencil *S, int wantInd,
                            double *const *F, float *const *W, double *src, uint8_t *status,
                            double2 *lamvel, double *bnd, cudaStream_t s) {
-    recon_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
+    recon_kernel<DIM, EQ, NQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
         U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd);
     return cudaGetLastError();
   }
   static cudaError_t flag(const double *U, const Grid &g, float *const *W, double *const *F,
                           const double *theta, uint8_t *flag, DevScalars *sc, double thr, cudaStream_t s) {
-    flag_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, W[0], W[1], W[2], F[0], F[1],
+    flag_kernel<DIM, EQ, NQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, W[0], W[1], W[2], F[0], F[1],
                                                                           F[2], theta, flag, sc, thr);
     return cudaGetLastError();
   }
@@ -1322,12 +1337,12 @@ struct Launch {
                            DevScalars *sc, const JudgeArgs &jd, int heavy_blocks, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
-      cudaError_t e = cudaFuncSetAttribute(heavy_var_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)HeavyShape<DIM, EQ>::BYTES);
+      cudaError_t e = cudaFuncSetAttribute(heavy_var_kernel<DIM, EQ, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)HeavyShape<DIM, EQ, NQ>::BYTES);
       if (e != cudaSuccess) return e;
       attr = true;
     }
-    heavy_var_kernel<DIM, EQ><<<heavy_blocks, dim3(32, NV), HeavyShape<DIM, EQ>::BYTES, s>>>(
+    heavy_var_kernel<DIM, EQ, NQ><<<heavy_blocks, dim3(32, NV), HeavyShape<DIM, EQ, NQ>::BYTES, s>>>(
         U, g, S, theta, F[0], F[1], F[2], src, heavy, bnd, sc, jd);
     return cudaGetLastError();
   }
@@ -1337,16 +1352,16 @@ struct Launch {
     for (int d = 0; d < DIM; d++) {
       // one block row of 32 faces per (j, k), NQF points along threadIdx.y
       const dim3 grid((unsigned)((g.fdim[d][0] + 31) / 32), (unsigned)g.fdim[d][1], (unsigned)g.fdim[d][2]);
-      const dim3 blk(32, Cfg<DIM, EQ>::NQF);
-      if (d == 0) riemann_kernel<DIM, EQ, 0><<<grid, blk, 0, s>>>(F[0], G[0], g, sc);
-      if (d == 1) riemann_kernel<DIM, EQ, 1><<<grid, blk, 0, s>>>(F[1], G[1], g, sc);
-      if (DIM == 3 && d == 2) riemann_kernel<DIM, EQ, (DIM == 3 ? 2 : 1)><<<grid, blk, 0, s>>>(F[2], G[2], g, sc);
+      const dim3 blk(32, Cfg<DIM, EQ, NQ>::NQF);
+      if (d == 0) riemann_kernel<DIM, EQ, 0, NQ><<<grid, blk, 0, s>>>(F[0], G[0], g, sc);
+      if (d == 1) riemann_kernel<DIM, EQ, 1, NQ><<<grid, blk, 0, s>>>(F[1], G[1], g, sc);
+      if (DIM == 3 && d == 2) riemann_kernel<DIM, EQ, (DIM == 3 ? 2 : 1), NQ><<<grid, blk, 0, s>>>(F[2], G[2], g, sc);
     }
     return cudaGetLastError();
   }
   static cudaError_t stage(const StageArgs &a, const Grid &g, cudaStream_t s) {
     const dim3 grid = cell_grid(g);
-    stage_kernel<DIM, EQ><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(
+    stage_kernel<DIM, EQ, NQ><<<grid, dim3(kBlockX, kBlockY), 0, s>>>(
         a.U, a.Unext, a.Uprev, a.Uhat, a.Utmp, a.K, g, a.G[0], a.G[1], a.G[2], a.F[0], a.F[1],
         a.F[2], a.src, a.theta, a.mode, a.co, a.Re, a.Pr, a.atol, a.rtol, a.part);
     if (a.mode == STAGE_FSAL) {
@@ -1386,14 +1401,22 @@ int64_t stage_blocks(const Grid &g) {
   return (int64_t)gr.x * gr.y * gr.z;
 }
 
+// one instantiation per (dimension, equations, Gauss points): 2 points for both
+// dimensions, 3 points for 2D; the grid's nq selects
 #define KFVM_DISPATCH(DIM_, EQ_, CALL)                                                  \
   do {                                                                                \
-    if ((DIM_) == 2 && (EQ_) == EQ_HYDRO) return Launch<2, EQ_HYDRO>::CALL;           \
-    if ((DIM_) == 3 && (EQ_) == EQ_HYDRO) return Launch<3, EQ_HYDRO>::CALL;           \
-    if ((DIM_) == 2 && (EQ_) == EQ_NS) return Launch<2, EQ_NS>::CALL;                 \
-    if ((DIM_) == 3 && (EQ_) == EQ_NS) return Launch<3, EQ_NS>::CALL;                 \
-    if ((DIM_) == 2 && (EQ_) == EQ_GLM) return Launch<2, EQ_GLM>::CALL;               \
-    if ((DIM_) == 3 && (EQ_) == EQ_GLM) return Launch<3, EQ_GLM>::CALL;               \
+    if (g.nq == 2) {                                                                  \
+      if ((DIM_) == 2 && (EQ_) == EQ_HYDRO) return Launch<2, EQ_HYDRO, 2>::CALL;      \
+      if ((DIM_) == 3 && (EQ_) == EQ_HYDRO) return Launch<3, EQ_HYDRO, 2>::CALL;      \
+      if ((DIM_) == 2 && (EQ_) == EQ_NS) return Launch<2, EQ_NS, 2>::CALL;            \
+      if ((DIM_) == 3 && (EQ_) == EQ_NS) return Launch<3, EQ_NS, 2>::CALL;            \
+      if ((DIM_) == 2 && (EQ_) == EQ_GLM) return Launch<2, EQ_GLM, 2>::CALL;          \
+      if ((DIM_) == 3 && (EQ_) == EQ_GLM) return Launch<3, EQ_GLM, 2>::CALL;          \
+    } else if (g.nq == 3 && (DIM_) == 2) {                                            \
+      if ((EQ_) == EQ_HYDRO) return Launch<2, EQ_HYDRO, 3>::CALL;                     \
+      if ((EQ_) == EQ_NS) return Launch<2, EQ_NS, 3>::CALL;                           \
+      if ((EQ_) == EQ_GLM) return Launch<2, EQ_GLM, 3>::CALL;                         \
+    }                                                                                 \
     return cudaErrorInvalidValue;                                                     \
   } while (0)
 

@@ -44,6 +44,7 @@ struct Grid {
   int64_t nface[3];
   double dx, dy, dz;
   double rdx, rdy, rdz;      // 1 / dx, 1 / dy, 1 / dz
+  int nq;                    // Gauss points per direction
   int bc[6];
   // variables whose sign the wall mirror flips, bit v per face (reflecting and
   // no-slip coefficient tables of <Eq>_BCCoeffs.H; 0 for periodic / outflow)
@@ -147,12 +148,13 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-template <int DIM, int EQ>
+// NQ_: Gauss points per direction (NUM_QUAD_PTS of the reference's Definitions.H)
+template <int DIM, int EQ, int NQ_ = 2>
 struct Cfg {
   static constexpr int NV = Eos<EQ>::NV;
-  static constexpr int NQ = 2;
-  static constexpr int NQF = DIM == 2 ? 2 : 4;
-  static constexpr int NQC = DIM == 2 ? 4 : 8;
+  static constexpr int NQ = NQ_;
+  static constexpr int NQF = DIM == 2 ? NQ_ : NQ_ * NQ_;
+  static constexpr int NQC = DIM == 2 ? NQ_ * NQ_ : NQ_ * NQ_ * NQ_;
   static constexpr int NF = 2 * DIM;
   static constexpr int C = DIM == 2 ? 13 : 33;
   static constexpr int CC = DIM == 2 ? 5 : 7;
@@ -163,8 +165,13 @@ struct Cfg {
   static constexpr bool SRC = EQ == EQ_GLM;
 };
 
-// Gauss-Legendre weights on (-1/2,1/2), 2 points (src/numeric/Numeric.cpp:14-17)
-__device__ __forceinline__ double gl_wt(int) { return 1.0 / 2.0; }
+// Gauss-Legendre weights on (-1/2,1/2) in the reference's point order
+// (src/numeric/Numeric.cpp:14-27: 2 points (1/2, 1/2); 3 points, centre first)
+template <int NQ>
+__device__ __forceinline__ double gl_wt(int q) {
+  if constexpr (NQ == 3) return q == 0 ? 0.8888888888888888888888888 / 2.0 : 0.5555555555555555555555555 / 2.0;
+  else return 1.0 / 2.0;
+}
 
 // Label of the learned troubled-cell indicator: the largest departure of the
 // normalised WENO-JS weights (createOmegas, Stencil_K.H:556-580, before the

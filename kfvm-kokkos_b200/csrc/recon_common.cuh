@@ -11,10 +11,11 @@ namespace kfvm {
 // Rows of the linear reconstruction: face points f*NQF+q, then (GLM sources)
 // the interior points; the full-stencil weights are [cell][row] on the host
 // and reach the kernels as MMA operand tables.
-template <int DIM, int EQ>
+template <int DIM, int EQ, int NQ = 2>
 struct LinRows {
-  static constexpr int NROWS = Cfg<DIM, EQ>::NF * Cfg<DIM, EQ>::NQF + (Cfg<DIM, EQ>::SRC ? Cfg<DIM, EQ>::NQC : 0);
-  static constexpr int SIZE = Cfg<DIM, EQ>::C * NROWS;
+  using T = Cfg<DIM, EQ, NQ>;
+  static constexpr int NROWS = T::NF * T::NQF + (T::SRC ? T::NQC : 0);
+  static constexpr int SIZE = T::C * NROWS;
 };
 
 // face-slot address of point q, variable v of face f of cell (i,j,k) in a

@@ -121,10 +121,20 @@ RKC rk_table(int rk) {
   return r;
 }
 
-// LGL -> GL differentiation matrix, NQ = 2 (src/numeric/Numeric.cpp:50-52)
-const double kDiffMat2[2][4] = {
-    {-2.7320508075688767, 1.732050807568877, 1.7320508075688767, -0.7320508075688767},
-    {0.7320508075688767, -1.7320508075688767, -1.732050807568877, 2.7320508075688767}};
+// LGL -> GL differentiation matrices, row-major NQ x (NQ + 2): output point nQ,
+// inputs [left face, the NQ interior points in abscissa order, right face]
+// (src/numeric/Numeric.cpp:47-70, Numeric.H:55-61)
+const double kDiffMat1[3] = {-1.0, 0.0, 1.0};
+const double kDiffMat2[8] = {-2.7320508075688767, 1.732050807568877,   1.7320508075688767, -0.7320508075688767,
+                             0.7320508075688767,  -1.7320508075688767, -1.732050807568877, 2.7320508075688767};
+const double kDiffMat3[15] = {1.5,  0.0,  -3.2274861218395139, 3.2274861218395148, -1.5,
+                              -5.323790007724451, 2.06559111797729, 3.872983346207419, -1.2909944487358063,
+                              0.6762099922755506, -0.6762099922755498, -2.0655911179772883, 1.2909944487358065,
+                              -3.8729833462074184, 5.323790007724451};
+inline double diff_mat(int nq, int r, int c) {
+  const double *D = nq == 1 ? kDiffMat1 : (nq == 2 ? kDiffMat2 : kDiffMat3);
+  return D[r * (nq + 2) + c];
+}
 
 // ---------------- EOS (Hydro_EOS.H, NavierStokes_EOS.H, MHD_GLM_EOS.H) ----------------
 enum { DENS = 0, MOMX = 1, MOMY = 2, MOMZ = 3, ETOT = 4, MAGX = 5, MAGY = 6, MAGZ = 7, PSI = 8 };
@@ -1011,28 +1021,28 @@ void glm_sources(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t
             dpz = tdz * (B[S.ui(i, j, k + 1, PSI)] - B[S.ui(i, j, k - 1, PSI)]);
           }
         } else {
-          // diffX / diffY / diffZ with the LGL->GL matrix D (NQ = 2)
+          // diffX / diffY / diffZ with the LGL->GL matrix D
           {
             const int fIdx = S.dim == 2 ? nR : nR * nq + nS;
-            double d = kDiffMat2[nQ][0] * S.fs(0, i, j, k, 1, fIdx)[PSI] +
-                       kDiffMat2[nQ][nq + 1] * S.fs(0, i + 1, j, k, 0, fIdx)[PSI];
-            for (int m = 1; m <= nq; m++) d += kDiffMat2[nQ][m] * cellv(m - 1, nR, nS, PSI);
+            double d = diff_mat(nq, nQ, 0) * S.fs(0, i, j, k, 1, fIdx)[PSI] +
+                       diff_mat(nq, nQ, nq + 1) * S.fs(0, i + 1, j, k, 0, fIdx)[PSI];
+            for (int m = 1; m <= nq; m++) d += diff_mat(nq, nQ, m) * cellv(m - 1, nR, nS, PSI);
             d /= S.dx;
             dpx = d;
           }
           {
             const int fIdx = S.dim == 2 ? nQ : nQ * nq + nS;
-            double d = kDiffMat2[nR][0] * S.fs(1, i, j, k, 1, fIdx)[PSI] +
-                       kDiffMat2[nR][nq + 1] * S.fs(1, i, j + 1, k, 0, fIdx)[PSI];
-            for (int m = 1; m <= nq; m++) d += kDiffMat2[nR][m] * cellv(nQ, m - 1, nS, PSI);
+            double d = diff_mat(nq, nR, 0) * S.fs(1, i, j, k, 1, fIdx)[PSI] +
+                       diff_mat(nq, nR, nq + 1) * S.fs(1, i, j + 1, k, 0, fIdx)[PSI];
+            for (int m = 1; m <= nq; m++) d += diff_mat(nq, nR, m) * cellv(nQ, m - 1, nS, PSI);
             d /= S.dy;
             dpy = d;
           }
           if (S.dim == 3) {
             const int fIdx = nQ * nq + nR;
-            double d = kDiffMat2[nS][0] * S.fs(2, i, j, k, 1, fIdx)[PSI] +
-                       kDiffMat2[nS][nq + 1] * S.fs(2, i, j, k + 1, 0, fIdx)[PSI];
-            for (int m = 1; m <= nq; m++) d += kDiffMat2[nS][m] * cellv(nQ, nR, m - 1, PSI);
+            double d = diff_mat(nq, nS, 0) * S.fs(2, i, j, k, 1, fIdx)[PSI] +
+                       diff_mat(nq, nS, nq + 1) * S.fs(2, i, j, k + 1, 0, fIdx)[PSI];
+            for (int m = 1; m <= nq; m++) d += diff_mat(nq, nS, m) * cellv(nQ, nR, m - 1, PSI);
             d /= S.dz;
             dpz = d;
           }
@@ -1513,7 +1523,7 @@ int orc_set_threads(int n) {
 }
 
 orc_solver *orc_create(const kfvm_config *cfg) {
-  if (!cfg || (cfg->dim != 2 && cfg->dim != 3) || cfg->nq != 2) return nullptr;
+  if (!cfg || (cfg->dim != 2 && cfg->dim != 3) || cfg->nq < 1 || cfg->nq > 3) return nullptr;
   orc_solver *S = new orc_solver();
   S->cfg = *cfg;
   if (S->cfg.dim == 2) S->cfg.nz = 1;

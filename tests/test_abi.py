@@ -58,7 +58,8 @@ def test_default_config(product_lib):
 
 @pytest.mark.parametrize("mutate,msg", [
     (lambda c: setattr(c, "dim", 4), "dim"),
-    (lambda c: setattr(c, "nq", 3), "NUM_QUAD_PTS"),
+    (lambda c: setattr(c, "nq", 4), "NUM_QUAD_PTS"),
+    (lambda c: (setattr(c, "dim", 3), setattr(c, "nz", 16), setattr(c, "nq", 3)), "NUM_QUAD_PTS"),
     (lambda c: (setattr(c, "eq", abi.KFVM_EQ_MHD_GLM), setattr(c, "rs", abi.KFVM_RS_HLLC)), "HLLC"),
     (lambda c: c.bc.__setitem__(1, abi.KFVM_BC_OUTFLOW), "pairs"),
     (lambda c: setattr(c, "rk", 9), "RK"),

@@ -172,3 +172,40 @@ def test_walls_against_oracle(name, scale, steps, walls, gpu, product_lib, oracl
     assert np.all(err <= STEP_TOL), err
     if cfg.eq != abi.KFVM_EQ_MHD_GLM:  # the GLM HLL fan is not symmetric (MHD_GLM_Riemann.H:87)
         assert abs(ug[0].sum() - m0) <= 1e-12 * abs(m0)
+
+
+# the reference's 3-point Gauss rule (NUM_QUAD_PTS 3, 18 of its problems): 2D
+Q3_CASES = [
+    ("isentropic_vortex", 32, 4),
+    ("kelvin_helmholtz", 32, 4),
+    ("orszag_tang", 32, 4),
+]
+
+
+@pytest.mark.parametrize("name,scale,steps", Q3_CASES)
+def test_three_point_quadrature(name, scale, steps, gpu, product_lib, oracle_lib):
+    """NUM_QUAD_PTS = 3 (points ordered centre, minus, plus as in Numeric.cpp:21):
+    initial condition, one RHS evaluation with its face states and WENO flags, and
+    N steps against the oracle."""
+    cfg, ic = abi.workload(name, scale=scale, steps=steps)
+    cfg.nq = 3
+    g = product_lib.Solver(cfg)
+    o = oracle_lib.OracleSolver(cfg)
+    g.init_ic(ic)
+    o.init_ic(ic)
+    assert np.all(rel_l1(g.get_state(), o.get_state()) <= 1e-14)
+    o.keep_faces(True)
+    rg, vg = g.eval_rhs(0.0)
+    ro, vo = o.eval_rhs(0.0)
+    assert np.all(rel_l1(rg, ro) <= RHS_TOL), rel_l1(rg, ro)
+    assert abs(vg - vo) <= 1e-13 * abs(vo)
+    ag, _ = g.flags()
+    ao, _ = o.flags()
+    assert np.array_equal(ag, ao), (ag.sum(), ao.sum())
+    for d in range(cfg.dim):
+        fg, fo = g.faces(d), o.faces(d)
+        assert fg.shape[1] == 3
+        assert np.abs(fg - fo).max() <= 1e-12 * np.abs(fo).max(), d
+    step_pair(g, o, steps)
+    err = rel_l1(g.get_state(), o.get_state())
+    assert np.all(err <= STEP_TOL), err
