@@ -190,12 +190,15 @@ def _vortex_exact(cfg, t):
     return avg  # [y][x]
 
 
-def test_isentropic_vortex_convergence(oracle_lib):
+@pytest.mark.parametrize("nq", [2, 3])
+def test_isentropic_vortex_convergence(nq, oracle_lib):
     """Density L1 error against the advected exact solution drops at high order
-    (the reference's convergence sweep, exec/Hydro/IsenVort/sweepN.sh)."""
+    (the reference's convergence sweep, exec/Hydro/IsenVort/sweepN.sh), with the
+    2- and the 3-point Gauss rule."""
     errs = []
     for n in (32, 64):
         cfg, ic = abi.workload("isentropic_vortex", scale=n, steps=10000)
+        cfg.nq = nq
         cfg.final_time = 0.5
         cfg.atol = cfg.rtol = 1e-8
         s = oracle_lib.OracleSolver(cfg)
