@@ -38,7 +38,7 @@ int fail(int code, const std::string &msg) {
       return fail(KFVM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
   } while (0)
 
-// RK coefficient tables (src/numeric/Numeric.H:111-203)
+// RK coefficient tables (src/numeric/Numeric.H:111-282)
 struct RKTable {
   int nStages;
   double gam1[10], gam2[10], gam3[10], delta[10], beta[10], bhat[10], c[10];
@@ -106,6 +106,108 @@ bool rk_table(int rk, RKTable &r) {
     r.bhatfsal = 1.020760551185952388626787099944507877e-01;
     r.ep1 = 0.7 / 3.0;
     r.ep2 = -0.23 / 3.0;
+  } else if (rk == KFVM_RK_SSP10_4_3) {
+    // SSP(10,4) of Ketcheson with the embedded pair and PI values of Conde et al.
+    r.nStages = 10;
+    const double g1[] = {0.0, 1.0, 1.0, 1.0, 2.0 / 5.0, 1.0, 1.0, 1.0, 1.0, 3.0 / 5.0};
+    const double g2[] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0};
+    const double g3[] = {0.0, 0.0, 0.0, 0.0, 3.0 / 5.0, 0.0, 0.0, 0.0, 0.0, -3.0 / 2.0};
+    const double de[] = {0.0, 0.0, 0.0, 0.0, 0.0, 9.0 / 10.0, 0.0, 0.0, 0.0, 0.0};
+    const double be[] = {1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0, 1.0 / 15.0,
+                         1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0, 1.0 / 10.0};
+    const double bh[] = {0.0, 2.0 / 9.0, 0.0, 0.0, 5.0 / 18.0, 1.0 / 3.0, 0.0, 0.0, 0.0, 1.0 / 6.0};
+    const double cc[] = {0.0, 1.0 / 6.0, 1.0 / 3.0, 1.0 / 2.0, 2.0 / 3.0, 1.0 / 3.0, 1.0 / 2.0, 2.0 / 3.0,
+                         5.0 / 6.0, 1.0};
+    for (int i = 0; i < 10; i++) {
+      r.gam1[i] = g1[i];
+      r.gam2[i] = g2[i];
+      r.gam3[i] = g3[i];
+      r.delta[i] = de[i];
+      r.beta[i] = be[i];
+      r.bhat[i] = bh[i];
+      r.c[i] = cc[i];
+    }
+    r.bhatfsal = 0.0;
+    r.ep1 = 0.8 / 3.0;
+    r.ep2 = -0.31 / 3.0;
+  } else if (rk == KFVM_RK_FOURSTARP) {
+    // fourth-order adaptive method of Ranocha et al.
+    r.nStages = 9;
+    const double g1[] = {0.0,
+                         -4.655641447335068552684422206224169103e+00,
+                         -7.720265099645871829248487209517314217e-01,
+                         -4.024436690519806086742256154738379161e+00,
+                         -2.129676284018530966221583708648634733e-02,
+                         -2.435022509790109546199372365866450709e+00,
+                         1.985627297131987000579523283542615256e-02,
+                         -2.810791146791038566946663374735713961e-01,
+                         1.689434168754859644351230590422137972e-01};
+    const double g2[] = {0.0,
+                         2.499262792574495009336242992898153462e+00,
+                         5.866820377718875577451517985847920081e-01,
+                         1.205146086523094569925592464380295241e+00,
+                         3.474793722186732780030762737753849272e-01,
+                         1.321346060965113109321230804210670518e+00,
+                         3.119636464694193615946633676950358444e-01,
+                         4.351419539684379261368971206040518552e-01,
+                         2.359698130028753572503744518147537768e-01};
+    const double g3[] = {0.0,
+                         0.0,
+                         0.0,
+                         7.621006678721315291614677352949377871e-01,
+                         -1.981182504339400567765766904309673119e-01,
+                         -6.228959218699007450469629366684127462e-01,
+                         -3.752248380775956442989480369774937099e-01,
+                         -3.355438309135169811915662336248989661e-01,
+                         -4.560955005031121479972862973705108039e-02};
+    const double de[] = {1.0,
+                         1.262923876648114432874834923838556100e+00,
+                         7.574967189685911558308119415539596711e-01,
+                         5.163589453140728104667573195005629833e-01,
+                         -2.746327421802609557034437892013640319e-02,
+                         -4.382673178127944142238606608356542890e-01,
+                         1.273587294602656522645691372699677063e+00,
+                         -6.294740283927400326554066998751383342e-01,
+                         0.0};
+    const double be[] = {2.836343005184365275160654678626695428e-01,
+                         9.736500104654741223716056170419660217e-01,
+                         3.382359225242515288768487569778320563e-01,
+                         -3.584943611106183357043212309791897386e-01,
+                         -4.113944068471528211627210454497620358e-03,
+                         1.427968894048586363415504654313371031e+00,
+                         1.808470948394314017665968411915568633e-02,
+                         1.605770645946802213926893453819236685e-01,
+                         2.952227015964591648775833803635147962e-01};
+    const double bh[] = {2.483675912451591196775756814283216443e-02,
+                         1.866327774562103796990092260942180726e-01,
+                         5.671080795936984495604436622517631183e-02,
+                         -3.447695439149287702616943808570747099e-03,
+                         3.602245056516636472203469198006404016e-03,
+                         4.545570622145088936800484247980581766e-01,
+                         -2.434665289427612407531544765622888855e-04,
+                         6.642755361103549971517945063138312147e-02,
+                         1.613697079523505006226025497715177578e-01};
+    const double cc[] = {0.0,
+                         2.836343005184365275160654678626695428e-01,
+                         5.484076570002894365286665352032296535e-01,
+                         3.687228761669438493478872632332010073e-01,
+                         -6.806126440140844191258463830024463902e-01,
+                         3.518526124230705801739919476290327750e-01,
+                         1.665941994879593315477304663913129942e+00,
+                         9.715279295934715835299192116436237065e-01,
+                         9.051569840159589594903399929316959062e-01};
+    for (int i = 0; i < 9; i++) {
+      r.gam1[i] = g1[i];
+      r.gam2[i] = g2[i];
+      r.gam3[i] = g3[i];
+      r.delta[i] = de[i];
+      r.beta[i] = be[i];
+      r.bhat[i] = bh[i];
+      r.c[i] = cc[i];
+    }
+    r.bhatfsal = 4.955424859358438183052504342394102722e-02;
+    r.ep1 = 0.38 / 4.0;
+    r.ep2 = -0.18 / 4.0;
   } else {
     return false;
   }

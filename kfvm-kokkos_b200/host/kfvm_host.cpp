@@ -163,6 +163,8 @@ bool ProblemSetup::setSetup(const std::string &setting) {
   } else if (k == "rk") {
     if (v == "ssp4_3_2") cfg.rk = KFVM_RK_SSP4_3_2;
     else if (v == "threestarp") cfg.rk = KFVM_RK_THREESTARP;
+    else if (v == "fourstarp") cfg.rk = KFVM_RK_FOURSTARP;
+    else if (v == "ssp10_4_3") cfg.rk = KFVM_RK_SSP10_4_3;
     else return false;
   } else if (k == "bc") {
     // one word per face (west east south north [bottom top]) or one for all

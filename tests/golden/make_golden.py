@@ -2,7 +2,7 @@
 
 Reads (as text, nothing is compiled or run) the Gauss-Legendre tables of
 src/numeric/Numeric.cpp:9-46 and the RK coefficient tables of
-src/numeric/Numeric.H:111-203 of slug-cfd/kfvm-kokkos, evaluates the literal
+src/numeric/Numeric.H:111-282 of slug-cfd/kfvm-kokkos, evaluates the literal
 expressions (e.g. "1.0 / 3.0") in double precision, and writes them as JSON.
 Usage: python tests/golden/make_golden.py /root/reference
 """
@@ -32,7 +32,7 @@ for nq in (1, 2, 3):
     for name in ("ab", "wt"):
         m = re.search(r"QuadRuleLUT<%d>::%s\s*(?:=\s*)?\{([^}]*)\}" % (nq, name), cpp)
         out["quad"].setdefault(str(nq), {})[name] = arr(m.group(1))
-for scheme in ("SSP4_3_2", "ThreeStarP"):
+for scheme in ("SSP4_3_2", "SSP10_4_3", "ThreeStarP", "FourStarP"):
     m = re.search(r"struct RKCoeff<RKType::%s> \{(.*?)\n\};" % scheme, hdr, re.S)
     body = m.group(1)
     tab = {}

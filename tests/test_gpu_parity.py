@@ -209,3 +209,36 @@ def test_three_point_quadrature(name, scale, steps, gpu, product_lib, oracle_lib
     step_pair(g, o, steps)
     err = rel_l1(g.get_state(), o.get_state())
     assert np.all(err <= STEP_TOL), err
+
+
+# the other Riemann solvers and RK scheme of the reference's compile-time choices
+VARIANTS = [
+    ("isentropic_vortex", 32, 4, {"rs": abi.KFVM_RS_HLL}),
+    ("isentropic_vortex", 32, 4, {"rs": abi.KFVM_RS_LLF}),
+    ("orszag_tang", 32, 4, {"rs": abi.KFVM_RS_LLF}),
+    ("kelvin_helmholtz", 32, 4, {"rk": abi.KFVM_RK_THREESTARP}),
+    ("kelvin_helmholtz", 32, 3, {"rk": abi.KFVM_RK_FOURSTARP}),
+    ("isentropic_vortex", 32, 3, {"rk": abi.KFVM_RK_SSP10_4_3}),
+    ("sod3d", 16, 3, {"rs": abi.KFVM_RS_HLL}),
+]
+
+
+@pytest.mark.parametrize("name,scale,steps,over", VARIANTS)
+def test_solver_variants(name, scale, steps, over, gpu, product_lib, oracle_lib):
+    """HLL and LLF fluxes (Common_K.H:23-63) and the ThreeStarP, FourStarP and
+    SSP(10,4) schemes (Numeric.H:134-282) against the oracle: one RHS evaluation
+    and N steps."""
+    cfg, ic = abi.workload(name, scale=scale, steps=steps)
+    for k, v in over.items():
+        setattr(cfg, k, v)
+    g = product_lib.Solver(cfg)
+    o = oracle_lib.OracleSolver(cfg)
+    g.init_ic(ic)
+    o.init_ic(ic)
+    rg, vg = g.eval_rhs(0.0)
+    ro, vo = o.eval_rhs(0.0)
+    assert np.all(rel_l1(rg, ro) <= RHS_TOL), rel_l1(rg, ro)
+    assert abs(vg - vo) <= 1e-13 * abs(vo)
+    step_pair(g, o, steps)
+    err = rel_l1(g.get_state(), o.get_state())
+    assert np.all(err <= STEP_TOL), err

@@ -29,7 +29,9 @@ def test_quadrature_tables(nq, oracle_lib):
 
 
 @pytest.mark.parametrize("rk,name", [(abi.KFVM_RK_SSP4_3_2, "SSP4_3_2"),
-                                     (abi.KFVM_RK_THREESTARP, "ThreeStarP")])
+                                     (abi.KFVM_RK_SSP10_4_3, "SSP10_4_3"),
+                                     (abi.KFVM_RK_THREESTARP, "ThreeStarP"),
+                                     (abi.KFVM_RK_FOURSTARP, "FourStarP")])
 def test_rk_tables(rk, name, oracle_lib):
     _, _, t = oracle_lib.tables(2, rk)
     g = GOLD["rk"][name]
