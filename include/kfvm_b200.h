@@ -29,7 +29,10 @@ extern "C" {
 /* ---- enumerations (values match the reference's enums) ------------------ */
 
 /* src/physics/EquationTypes.H:8-16 */
-enum kfvm_eq { KFVM_EQ_HYDRO = 0, KFVM_EQ_NAVIERSTOKES = 1, KFVM_EQ_MHD_GLM = 2 };
+/* KFVM_EQ_SRHYDRO: special-relativistic hydrodynamics (src/physics/srhydro):
+ * conserved D = rho W, S = rho h W^2 v, E = rho h W^2 - p; the primitives are
+ * recovered by Newton iteration on the pressure; HLL or LLF fluxes only */
+enum kfvm_eq { KFVM_EQ_HYDRO = 0, KFVM_EQ_NAVIERSTOKES = 1, KFVM_EQ_MHD_GLM = 2, KFVM_EQ_SRHYDRO = 3 };
 /* src/physics/RSTypes.H:6 */
 enum kfvm_rs { KFVM_RS_LLF = 0, KFVM_RS_HLL = 1, KFVM_RS_HLLC = 2 };
 /* src/numeric/RKTypes.H:6 (SSP4_3_2 is the only third-order SSP method there) */
@@ -61,7 +64,11 @@ enum kfvm_ic {
   KFVM_IC_KELVIN_HELMHOLTZ = 2,  /* 2D Euler shear layer + seeded noise         */
   KFVM_IC_TAYLOR_GREEN = 3,      /* 3D Navier-Stokes Taylor-Green vortex        */
   KFVM_IC_ORSZAG_TANG = 4,       /* 2D GLM-MHD Orszag-Tang vortex               */
-  KFVM_IC_SMOOTH_WAVE = 5        /* any dim/eq: smooth density/velocity wave     */
+  KFVM_IC_SMOOTH_WAVE = 5,       /* any dim/eq: smooth density/velocity wave     */
+  KFVM_IC_SR_SHOCK_TUBE = 6,     /* SR hydro: rho,p = 10,40/3 for |x|<1/2 else 1,1e-6
+                                    (exec/SRHydro/SRShockTube)                    */
+  KFVM_IC_SR_RIEMANN_2D = 7      /* SR hydro 2D four-quadrant Riemann problem
+                                    (exec/SRHydro/SRRiem2d)                       */
 };
 
 /* ---- error codes -------------------------------------------------------- */

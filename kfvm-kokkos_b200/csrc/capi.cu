@@ -683,10 +683,14 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if (cfg->dim != 2 && cfg->dim != 3) return fail(KFVM_ERR_ARG, "dim must be 2 or 3");
   if (!(cfg->nq == 2 || (cfg->nq == 3 && cfg->dim == 2)))
     return fail(KFVM_ERR_ARG, "the GPU path supports NUM_QUAD_PTS = 2, and 3 in 2D");
-  if (cfg->eq < 0 || cfg->eq > 2) return fail(KFVM_ERR_ARG, "unknown equation type");
+  if (cfg->eq < KFVM_EQ_HYDRO || cfg->eq > KFVM_EQ_SRHYDRO) return fail(KFVM_ERR_ARG, "unknown equation type");
   if (cfg->rs < 0 || cfg->rs > 2) return fail(KFVM_ERR_ARG, "unknown Riemann solver");
   if (cfg->eq == KFVM_EQ_MHD_GLM && cfg->rs == KFVM_RS_HLLC)
     return fail(KFVM_ERR_ARG, "HLLC is not defined for MHD_GLM");
+  if (cfg->eq == KFVM_EQ_SRHYDRO && cfg->rs == KFVM_RS_HLLC)
+    return fail(KFVM_ERR_ARG, "the SRHydro Riemann solvers are HLL and LLF");
+  if (cfg->eq == KFVM_EQ_SRHYDRO && cfg->indicator == KFVM_IND_MLP)
+    return fail(KFVM_ERR_ARG, "the learned indicator is trained for the Euler / GLM-MHD paths");
   const int64_t nz = cfg->dim == 3 ? cfg->nz : 1;
   if (cfg->nx * cfg->ny * nz >= (int64_t)0x80000000LL) return fail(KFVM_ERR_ARG, "more than 2^31 cells");
   if (cfg->nx < 3 || cfg->ny < 3 || nz < (cfg->dim == 3 ? 3 : 1))
@@ -880,7 +884,7 @@ void kfvm_destroy(kfvm_solver *s) {
 
 int kfvm_init_ic(kfvm_solver *s, int32_t ic_kind, uint64_t seed) {
   if (!s) return fail(KFVM_ERR_ARG, "null solver");
-  if (ic_kind < 0 || ic_kind > KFVM_IC_SMOOTH_WAVE) return fail(KFVM_ERR_ARG, "unknown initial condition");
+  if (ic_kind < 0 || ic_kind > KFVM_IC_SR_RIEMANN_2D) return fail(KFVM_ERR_ARG, "unknown initial condition");
   cudaError_t e = run(s, KFVM_KCLASS_OTHER, 1, [&] {
     return kfvm::launch_ic(s->dim, s->eq, ic_kind, seed, s->cfg, s->Ub[s->iPrev], s->g, s->stream);
   });
@@ -974,6 +978,8 @@ int kfvm_set_indicator(kfvm_solver *s, int32_t ind) {
   if (ind == KFVM_IND_MLP && !s->mlp.ready)
     return fail(KFVM_ERR_STATE, "learned indicator: no weights (kfvm_mlp_set_weights or kfvm_mlp_init_weights + "
                                 "kfvm_mlp_train)");
+  if (ind == KFVM_IND_MLP && s->eq == KFVM_EQ_SRHYDRO)
+    return fail(KFVM_ERR_ARG, "the learned indicator is trained for the Euler / GLM-MHD paths");
   if (ind == KFVM_IND_MLP && s->g.n > (int64_t)kfvm::kHeavyCellMax)
     return fail(KFVM_ERR_ARG, "learned indicator: at most 2^30 cells");
   s->indicator = ind;
@@ -990,6 +996,7 @@ int kfvm_set_precision(kfvm_solver *s, int32_t precision) {
     CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
     if (major != 10) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form needs an sm_100 device");
     if (s->g.nq != 2) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form is built for 2 Gauss points");
+    if (s->eq == KFVM_EQ_SRHYDRO) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form is built for the Euler / GLM-MHD paths");
   }
   s->precision = precision;
   return KFVM_OK;

@@ -93,6 +93,7 @@ cudaError_t launch_errest(int eq, const double *u, const double *uhat, int64_t n
   const int64_t nblk = errest_blocks(n);
   if (nblk <= 0) return cudaErrorInvalidValue;
   if (eq == EQ_GLM) errest_kernel<EQ_GLM><<<(unsigned)nblk, kErrBlock, 0, s>>>(u, uhat, n, atol, rtol, part);
+  else if (eq == EQ_SR) errest_kernel<EQ_SR><<<(unsigned)nblk, kErrBlock, 0, s>>>(u, uhat, n, atol, rtol, part);
   else errest_kernel<EQ_HYDRO><<<(unsigned)nblk, kErrBlock, 0, s>>>(u, uhat, n, atol, rtol, part);
   errest_finalize<<<1, 1024, 0, s>>>(part, nblk, out);
   return cudaGetLastError();
@@ -138,7 +139,7 @@ extern "C" int kfvm_err_est_noalloc(int32_t eq, const double *u_dev, const doubl
                                     void *stream) {
   if (!u_dev || !uhat_dev || !out_dev)
     return kfvm::set_last_error(KFVM_ERR_ARG, "kfvm_err_est_noalloc: null pointer");
-  if (eq < KFVM_EQ_HYDRO || eq > KFVM_EQ_MHD_GLM)
+  if (eq < KFVM_EQ_HYDRO || eq > KFVM_EQ_SRHYDRO)
     return kfvm::set_last_error(KFVM_ERR_ARG, "kfvm_err_est_noalloc: unknown equation type");
   if (n <= 0 || n > KFVM_NOALLOC_MAX_CELLS)
     return kfvm::set_last_error(KFVM_ERR_ARG,

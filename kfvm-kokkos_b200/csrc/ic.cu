@@ -93,6 +93,34 @@ __device__ void ic_point(const IcParams &p, double x, double y, double z, double
     s[ETOT] = pr / gm + rho * (u * u + v * v + w * w) / 2.0 + (bx * bx + by * by + bz * bz) / 2.0;
     break;
   }
+  case KFVM_IC_SR_SHOCK_TUBE: {
+    // exec/SRHydro/SRShockTube: at rest, rho, p = 10, 40/3 for |x| < 1/2, else 1, 1e-6
+    const double gR = g / gm, ax = fabs(x);
+    const double rho = ax < 0.5 ? 10.0 : 1.0, pr = ax < 0.5 ? 40.0 / 3.0 : 1.e-6;
+    const double h = 1.0 + pr * gR / rho;
+    s[DENS] = rho;
+    s[ETOT] = rho * h - pr;
+    break;
+  }
+  case KFVM_IC_SR_RIEMANN_2D: {
+    // exec/SRHydro/SRRiem2d: four quadrants, two of them moving at 0.99 c
+    const double gR = g / gm, v0 = 0.99;
+    double rho = 0.5, vx = 0.0, vy = 0.0, pr = 1.0;
+    if (x > 0.0) {
+      rho = 0.1;
+      if (y > 0.0) pr = 0.01;
+      else vy = v0;
+    } else if (y > 0.0) {
+      rho = 0.1;
+      vx = v0;
+    }
+    const double W = 1.0 / sqrt(1.0 - vx * vx - vy * vy), h = 1.0 + pr * gR / rho;
+    s[DENS] = rho * W;
+    s[MOMX] = rho * W * W * h * vx;
+    s[MOMY] = rho * W * W * h * vy;
+    s[ETOT] = rho * W * W * h - pr;
+    break;
+  }
   default: { // KFVM_IC_SMOOTH_WAVE: periodic smooth flow on the box
     const double X = 2.0 * pi * (x - p.xlo) / (p.xup - p.xlo);
     const double Y = 2.0 * pi * (y - p.ylo) / (p.yup - p.ylo);
@@ -100,6 +128,16 @@ __device__ void ic_point(const IcParams &p, double x, double y, double z, double
     const double rho = 1.0 + 0.2 * sin(X) * cos(Y) * cos(Z);
     const double u = 0.5 + 0.1 * sin(Y), v = 0.3 * cos(X), w = 0.1 * sin(X + Y);
     const double pr = 1.0 + 0.1 * cos(X - Y + Z);
+    if (p.eq == KFVM_EQ_SRHYDRO) {
+      // the same primitives as a special-relativistic state
+      const double W = 1.0 / sqrt(1.0 - (u * u + v * v + w * w)), h = 1.0 + pr * g / (gm * rho);
+      s[DENS] = rho * W;
+      s[MOMX] = rho * W * W * h * u;
+      s[MOMY] = rho * W * W * h * v;
+      s[MOMZ] = rho * W * W * h * w;
+      s[ETOT] = rho * W * W * h - pr;
+      break;
+    }
     s[DENS] = rho;
     s[MOMX] = rho * u;
     s[MOMY] = rho * v;

@@ -230,17 +230,25 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
             for (int v = 0; v < NV; v++) st[v] = acc[v][t][e];
             // pos_inside, with the internal energy kept for the indicator's pressure
-            const double ei = Eos<EQ>::eint(st);
-            inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
+            double ei = 0.0;
+            if constexpr (EQ == EQ_SR) {
+              inside = inside && pos_inside<EQ>(bd, st);
+            } else {
+              ei = Eos<EQ>::eint(st);
+              inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
+            }
             if (rw < T::NF * T::NQF) {
               const int q = rw % T::NQF;
               double *Fd = F[d];
               const int64_t a = (int64_t)((slot * T::NQF + q) * NV) * nf + fidx;
 #pragma unroll
               for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
-              if (wantInd)
-                W[d][(int64_t)(slot * T::NQF + q) * nf + fidx] =
-                    Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
+              if (wantInd) {
+                // SR: the indicator is the density itself, stored rounded
+                const float wv = EQ == EQ_SR ? __double2float_rn(st[DENS])
+                                             : Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
+                W[d][(int64_t)(slot * T::NQF + q) * nf + fidx] = wv;
+              }
               if constexpr (T::SRC) {
                 // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
                 const double vv = fabs(st[MOMX] / st[DENS]);
@@ -348,7 +356,7 @@ __global__ void __launch_bounds__(128)
       const double wc = Eos<EQ>::weno(g.gamma, uAv);
       bool certain = false;
       if (!bad && wc > 0.0 && isfinite(wc)) {
-        const double eps = DIM == 2 ? kWenoRoundEps : kWenoApproxEps;
+        const double eps = (DIM == 2 || EQ == EQ_SR) ? kWenoRoundEps : kWenoApproxEps;
         const double margin = 2.01 * eps * (double)wmax + 2e-7 * (double)jf + 1e-300;
         const double lo = ((double)jf - margin) / wc, hi = ((double)jf + margin) / wc;
         if (lo >= wThresh) {
@@ -484,6 +492,31 @@ __device__ double pos_apply_rows(const double *__restrict__ ref, const PosBounds
   constexpr int NV = T::NV, NR = LinRows<DIM, EQ, NQ>::NROWS;
   const double rDens = bd.rDens, minDens = bd.minDens, maxDens = bd.maxDens, minEint = bd.minEint;
   const double rDP = maxDens - rDens, rDM = rDens - minDens;
+  if constexpr (EQ == EQ_SR) {
+    // PositivityPreserve_K<SRHydro> (SRHydro_K.H:248-437): density theta, mixed in;
+    // then the theta of the bound on E - sqrt(D^2 + S^2), mixed in; both applied
+    // also when they are 1
+    auto mixr = [&](double th) {
+      for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) rs[r * NV + v] = ref[v] + th * (rs[r * NV + v] - ref[v]);
+    };
+    double thD = 1.0;
+    for (int r = 0; r < NR; r++) {
+      const double rho = rs[r * NV + DENS];
+      thD = rho < minDens ? fmin(thD, rDM / (rDens - rho)) : thD;
+      thD = rho > maxDens ? fmin(thD, rDP / (rho - rDens)) : thD;
+    }
+    mixr(thD);
+    const double edRef = sr::ediff(ref), edd = edRef - minEint;
+    double thE = 1.0;
+    for (int r = 0; r < NR; r++) {
+      const double ed = sr::ediff(rs + r * NV);
+      thE = ed < minEint ? fmin(thE, edd / (edRef - ed)) : thE;
+    }
+    mixr(thE);
+    return fmin(thE, thD);
+  }
   double thD = 1.0;
   for (int r = 0; r < NR; r++) {
     const double rho = rs[r * NV + DENS];
@@ -774,7 +807,8 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 // points goes through shared memory in point order, and the max wave speed
 // through a warp maximum and an atomic only from warps that raise it.
 template <int DIM, int EQ, int D, int NQ>
-__global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF, EQ == EQ_GLM ? 1 : (DIM == 2 ? 16 : 8))
+__global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
+                                  EQ == EQ_GLM ? 1 : (EQ == EQ_SR ? (DIM == 2 ? 8 : 4) : (DIM == 2 ? 16 : 8)))
     riemann_kernel(const double *__restrict__ F, double *__restrict__ G, Grid g,
                    DevScalars *__restrict__ sc) {
   using T = Cfg<DIM, EQ, NQ>;
@@ -1412,10 +1446,13 @@ int64_t stage_blocks(const Grid &g) {
       if ((DIM_) == 3 && (EQ_) == EQ_NS) return Launch<3, EQ_NS, 2>::CALL;            \
       if ((DIM_) == 2 && (EQ_) == EQ_GLM) return Launch<2, EQ_GLM, 2>::CALL;          \
       if ((DIM_) == 3 && (EQ_) == EQ_GLM) return Launch<3, EQ_GLM, 2>::CALL;          \
+      if ((DIM_) == 2 && (EQ_) == EQ_SR) return Launch<2, EQ_SR, 2>::CALL;            \
+      if ((DIM_) == 3 && (EQ_) == EQ_SR) return Launch<3, EQ_SR, 2>::CALL;            \
     } else if (g.nq == 3 && (DIM_) == 2) {                                            \
       if ((EQ_) == EQ_HYDRO) return Launch<2, EQ_HYDRO, 3>::CALL;                     \
       if ((EQ_) == EQ_NS) return Launch<2, EQ_NS, 3>::CALL;                           \
       if ((EQ_) == EQ_GLM) return Launch<2, EQ_GLM, 3>::CALL;                         \
+      if ((EQ_) == EQ_SR) return Launch<2, EQ_SR, 3>::CALL;                           \
     }                                                                                 \
     return cudaErrorInvalidValue;                                                     \
   } while (0)

@@ -244,6 +244,7 @@ __device__ double weno_departure(const double *__restrict__ Uc, const Grid &g,
   return dep;
 }
 
+// limiter bounds of a cell; minEint holds the bound on E - sqrt(D^2 + S^2) for SR
 struct PosBounds {
   double rDens, minDens, maxDens, minEint;
 };
@@ -257,6 +258,24 @@ __device__ __forceinline__ PosBounds pos_bounds(const double *__restrict__ Uc, c
   double minEint = 1.7976931348623157e308, minSdSp = 1.7976931348623157e308;
   constexpr int zr = DIM == 3 ? 1 : 0;
   const int64_t sy = g.px, sz = g.px * g.py;
+  if constexpr (EQ == EQ_SR) {
+    // PositivityPreserve_K<SRHydro> (SRHydro_K.H:224-246): no flattening
+#pragma unroll
+    for (int xo = -1; xo <= 1; xo++)
+#pragma unroll
+      for (int yo = -1; yo <= 1; yo++)
+#pragma unroll
+        for (int zo = -zr; zo <= zr; zo++) {
+          double s[NV];
+          const int64_t o = xo + yo * sy + zo * sz;
+#pragma unroll
+          for (int v = 0; v < NV; v++) s[v] = Uc[v * g.pvol + o];
+          maxDens = fmax(maxDens, s[DENS]);
+          minDens = fmin(minDens, s[DENS]);
+          minEint = fmin(minEint, sr::ediff(s));
+        }
+    return PosBounds{Uc[DENS * g.pvol], minDens, maxDens, minEint};
+  }
 #pragma unroll
   for (int xo = -1; xo <= 1; xo++)
 #pragma unroll
@@ -291,10 +310,12 @@ __device__ __forceinline__ PosBounds pos_bounds(const double *__restrict__ Uc, c
 }
 
 // true when a state leaves theta at 1 in both passes of the limiter
+// (SR: the comparisons are strict the other way, SRHydro_K.H:256-257, 372)
 template <int EQ>
 __device__ __forceinline__ bool pos_inside(const PosBounds &b, const double *s) {
   const double rho = s[DENS];
-  return rho > b.minDens && rho < b.maxDens && Eos<EQ>::eint(s) > b.minEint;
+  if constexpr (EQ == EQ_SR) return rho >= b.minDens && rho <= b.maxDens && sr::ediff(s) >= b.minEint;
+  else return rho > b.minDens && rho < b.maxDens && Eos<EQ>::eint(s) > b.minEint;
 }
 
 } // namespace kfvm

@@ -10,16 +10,20 @@
 //   src/physics/Common_K.H:23-63                  HLL / LLF in Batten's form
 //   src/physics/Riemann.H:15-45                   HLLC star-state helpers
 //   src/physics/*/_K.H VarConvert                 linearised primitive variables
+//   src/physics/srhydro/SRHydro_{EOS,Riemann}.H  special-relativistic EOS (sr_eos.h),
+//                                                 flux and wave speeds (HLL / LLF)
 // The arithmetic follows the reference expression by expression; nvcc may fuse
 // multiply-adds, so results agree with the CPU oracle to rounding, not bitwise.
 #pragma once
 
 #include <cstdint>
 
+#include "sr_eos.h"
+
 namespace kfvm {
 
 enum { DENS = 0, MOMX = 1, MOMY = 2, MOMZ = 3, ETOT = 4, MAGX = 5, MAGY = 6, MAGZ = 7, PSI = 8 };
-enum { EQ_HYDRO = 0, EQ_NS = 1, EQ_GLM = 2 };
+enum { EQ_HYDRO = 0, EQ_NS = 1, EQ_GLM = 2, EQ_SR = 3 };
 enum { RS_LLF = 0, RS_HLL = 1, RS_HLLC = 2 };
 
 // bound on the relative error of Eos::weno_approx.  For |log2 rho| <= 20 and
@@ -50,6 +54,8 @@ __device__ __forceinline__ double rcp_nr(double y) {
 template <int EQ>
 struct Eos {
   static constexpr int NV = EQ == EQ_GLM ? 9 : 5;
+  // primitives: SR keeps the Lorentz factor after the pressure
+  static constexpr int NVP = EQ == EQ_SR ? 6 : NV;
 
   __device__ __forceinline__ static double ekin(const double *U) {
     return 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]) / U[DENS];
@@ -80,9 +86,10 @@ struct Eos {
   __device__ __forceinline__ static double soundspeed(double g, const double *U) {
     return sqrt(g * pres(g, U) / U[DENS]);
   }
-  // KXRCF indicator variable p / rho^gamma
+  // KXRCF indicator variable p / rho^gamma (SR: the density D, SRHydro_EOS.H:225-228)
   __device__ __forceinline__ static double weno(double g, const double *U) {
-    return pres(g, U) / pow(U[DENS], g);
+    if constexpr (EQ == EQ_SR) return U[DENS];
+    else return pres(g, U) / pow(U[DENS], g);
   }
   // The same indicator with the power taken in FP32 by the hardware lg2 / ex2
   // approximations (the pressure stays FP64): relative error below
@@ -119,6 +126,7 @@ struct Eos {
     else return weno_approx_rp(g, rho, p);
   }
   __device__ __forceinline__ static double positivity(const double *U) {
+    if constexpr (EQ == EQ_SR) return sr::positivity(U);
     if constexpr (EQ == EQ_GLM) {
 #pragma unroll
       for (int v = 0; v < NV; v++)
@@ -127,6 +135,10 @@ struct Eos {
     return fmin(U[DENS], eint(U));
   }
   __device__ __forceinline__ static void cons2prim(double g, const double *U, double *V) {
+    if constexpr (EQ == EQ_SR) {
+      sr::cons2prim(g, U, V);
+      return;
+    }
     V[0] = U[DENS];
     V[1] = U[MOMX] / U[DENS];
     V[2] = U[MOMY] / U[DENS];
@@ -150,7 +162,16 @@ struct Eos {
   // physical flux in direction ord[0]
   __device__ __forceinline__ static void flux(double ch, const int *vo, const int *bo,
                                               const double *U, const double *V, double *F) {
-    if constexpr (EQ != EQ_GLM) {
+    if constexpr (EQ == EQ_SR) {
+      // SRHydro_Riemann.H:24-37
+      (void)ch;
+      (void)bo;
+      F[DENS] = U[DENS] * V[vo[0]];
+      F[vo[0]] = U[vo[0]] * V[vo[0]] + V[4];
+      F[vo[1]] = U[vo[1]] * V[vo[0]];
+      F[vo[2]] = U[vo[2]] * V[vo[0]];
+      F[ETOT] = U[vo[0]];
+    } else if constexpr (EQ != EQ_GLM) {
       (void)ch;
       (void)bo;
       F[DENS] = U[vo[0]];
@@ -227,9 +248,24 @@ struct Eos {
     const int ord[3] = {dir, (dir + 1) % 3, (dir + 2) % 3};
     const int vo[3] = {MOMX + ord[0], MOMX + ord[1], MOMX + ord[2]};
     const int bo[3] = {MAGX + ord[0], MAGX + ord[1], MAGX + ord[2]};
-    double vL[NV], vR[NV];
+    double vL[NVP], vR[NVP];
     double sL, sR, sMax;
-    if constexpr (EQ != EQ_GLM) {
+    if constexpr (EQ == EQ_SR) {
+      // SRHydro_Riemann.H:39-77: bounds of the relativistic characteristic speeds
+      sr::cons2prim(g, uL, vL);
+      sr::cons2prim(g, uR, vR);
+      const double aL = sr::soundspeed(g, vL), aLsq = aL * aL;
+      const double aR = sr::soundspeed(g, vR), aRsq = aR * aR;
+      const double wL = vL[5], sigL = aLsq / (wL * wL * (1.0 - aLsq));
+      const double sqrtL = sqrt(sigL * (1.0 + sigL - vL[vo[0]] * vL[vo[0]]));
+      const double wR = vR[5], sigR = aRsq / (wR * wR * (1.0 - aRsq));
+      const double sqrtR = sqrt(sigR * (1.0 + sigR - vR[vo[0]] * vR[vo[0]]));
+      const double sLm = (vL[vo[0]] - sqrtL) / (1.0 + sigL), sRm = (vR[vo[0]] - sqrtR) / (1.0 + sigR);
+      const double sLp = (vL[vo[0]] + sqrtL) / (1.0 + sigL), sRp = (vR[vo[0]] + sqrtR) / (1.0 + sigR);
+      sL = fmin(sLm, sRm);
+      sR = fmax(sLp, sRp);
+      sMax = fmax(fabs(sL), fabs(sR));
+    } else if constexpr (EQ != EQ_GLM) {
       const double rL = uL[DENS], rR = uR[DENS];
       const double iLR = rcp_nr(rL * rR), iL = rR * iLR, iR = rL * iLR;
       cons2prim_r(g, uL, iL, vL);
@@ -320,6 +356,18 @@ template <int EQ>
 struct VarConv {
   double gamm, rho, irho, u, v, w, bx, by, bz, rPsi, vsq;
   __device__ __forceinline__ VarConv(const double *ref, double gam) {
+    if constexpr (EQ == EQ_SR) {
+      // SRHydro_K.H:22-56: the momenta over D, linearised about (D, S) of the cell;
+      // (rho, u, v, w) hold (D, Sx, Sy, Sz)
+      gamm = gam - 1.0;
+      rho = ref[DENS];
+      irho = 1.0 / rho;
+      u = ref[MOMX];
+      v = ref[MOMY];
+      w = ref[MOMZ];
+      bx = by = bz = rPsi = vsq = 0.0;
+      return;
+    }
     gamm = gam - 1.0;
     rho = ref[DENS];
     irho = 1.0 / rho;
@@ -338,6 +386,12 @@ struct VarConv {
     }
   }
   __device__ __forceinline__ void cons2LinPrim(double *s) const {
+    if constexpr (EQ == EQ_SR) {
+      s[MOMX] = s[MOMX] / rho - s[DENS] * u / (rho * rho);
+      s[MOMY] = s[MOMY] / rho - s[DENS] * v / (rho * rho);
+      s[MOMZ] = s[MOMZ] / rho - s[DENS] * w / (rho * rho);
+      return;
+    }
     if constexpr (EQ == EQ_GLM) {
       s[ETOT] = gamm * (vsq * s[DENS] + s[ETOT] - u * s[MOMX] - v * s[MOMY] - w * s[MOMZ] -
                         bx * s[MAGX] - by * s[MAGY] - bz * s[MAGZ] - rPsi * s[PSI]);
@@ -350,6 +404,12 @@ struct VarConv {
   }
   // component c of cons2LinPrim(s), the momenta scaled by the reciprocal density
   __device__ __forceinline__ double lin1(const double *s, int c) const {
+    if constexpr (EQ == EQ_SR) {
+      if (c == MOMX) return s[MOMX] / rho - s[DENS] * u / (rho * rho);
+      if (c == MOMY) return s[MOMY] / rho - s[DENS] * v / (rho * rho);
+      if (c == MOMZ) return s[MOMZ] / rho - s[DENS] * w / (rho * rho);
+      return s[c];
+    }
     if (c == DENS) return s[DENS];
     if (c == MOMX) return (s[MOMX] - u * s[DENS]) * irho;
     if (c == MOMY) return (s[MOMY] - v * s[DENS]) * irho;
@@ -365,6 +425,12 @@ struct VarConv {
     return s[c];
   }
   __device__ __forceinline__ void linPrim2Cons(double *s) const {
+    if constexpr (EQ == EQ_SR) {
+      s[MOMX] = s[DENS] * u / rho + rho * s[MOMX];
+      s[MOMY] = s[DENS] * v / rho + rho * s[MOMY];
+      s[MOMZ] = s[DENS] * w / rho + rho * s[MOMZ];
+      return;
+    }
     if constexpr (EQ == EQ_GLM) {
       s[ETOT] = (vsq * s[DENS] + rho * u * s[MOMX] + rho * v * s[MOMY] + rho * w * s[MOMZ] +
                  bx * s[MAGX] + by * s[MAGY] + bz * s[MAGZ] + s[ETOT] / gamm + rPsi * s[PSI]);

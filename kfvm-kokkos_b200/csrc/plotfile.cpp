@@ -8,9 +8,10 @@
 // <base>_<num:07d>.meta (time, time step, time step size, gamma and the grid, the
 // scalars the reference stores in the HDF5 file).  Datasets:
 //   conserved   dens momx momy momz etot (+ magx magy magz psi for GLM-MHD)
-//   plot only   velx vely velz eint pres (GLM-MHD: eint prsg prsb), as AuxVars
-//               computes them (src/physics/hydro/Hydro_K.H:66-97,
-//               src/physics/mhd_glm/MHD_GLM_K.H:71-106)
+//   plot only   velx vely velz eint pres (GLM-MHD: eint prsg prsb; SRHydro: rho
+//               velx vely velz lorz pres), as AuxVars computes them
+//               (src/physics/hydro/Hydro_K.H:66-97, src/physics/mhd_glm/MHD_GLM_K.H:71-106,
+//               src/physics/srhydro/SRHydro_K.H:59-88; WriterPDI.cpp:268-278)
 //   both        weno (WENO applied, 0 or 1) and fomx (the positivity theta), the
 //               two components of the reference's wenoFlag view
 // Host code only; the solver-level calls in capi.cu download the state first.
@@ -27,6 +28,7 @@
 #include <vector>
 
 #include "../../include/kfvm_b200.h"
+#include "sr_eos.h"
 
 namespace kfvm {
 int set_last_error(int code, const std::string &msg);
@@ -37,7 +39,7 @@ namespace {
 struct Grid3 {
   int64_t nx, ny, nz, n;
   int nv;
-  bool glm;
+  bool glm, sr;
 };
 
 Grid3 grid_of(const kfvm_config *c) {
@@ -47,6 +49,7 @@ Grid3 grid_of(const kfvm_config *c) {
   g.nz = c->dim == 3 ? c->nz : 1;
   g.n = g.nx * g.ny * g.nz;
   g.glm = c->eq == KFVM_EQ_MHD_GLM;
+  g.sr = c->eq == KFVM_EQ_SRHYDRO;
   g.nv = g.glm ? 9 : 5;
   return g;
 }
@@ -130,7 +133,18 @@ int plotfile_write(const kfvm_config *cfg, const char *dir, const char *base, in
     ok = ok && write_raw(stem + ".weno.bin", w.data(), n);
     ok = ok && write_raw(stem + ".fomx.bin", theta, n);
   }
-  if (!ckpt && ok) {
+  if (!ckpt && ok && g.sr) {
+    // AuxVars<SRHydro>: the primitives by the pressure recovery
+    std::vector<double> V(6 * n);
+    for (size_t c = 0; c < n; c++) {
+      double U[5], v[6];
+      for (int q = 0; q < 5; q++) U[q] = u[(size_t)q * n + c];
+      kfvm::sr::cons2prim(cfg->gamma, U, v);
+      for (int q = 0; q < 6; q++) V[(size_t)q * n + c] = v[q];
+    }
+    const char *an[6] = {".rho.bin", ".velx.bin", ".vely.bin", ".velz.bin", ".pres.bin", ".lorz.bin"};
+    for (int q = 0; q < 6 && ok; q++) ok = write_raw(stem + an[q], V.data() + (size_t)q * n, n);
+  } else if (!ckpt && ok) {
     // auxiliary variables (AuxVars<Hydro> / AuxVars<MHD_GLM>)
     const double gm = cfg->gamma;
     std::vector<double> a(n);
@@ -192,7 +206,12 @@ int plotfile_write(const kfvm_config *cfg, const char *dir, const char *base, in
     if (g.glm) attr_vector(o, g, stem, "B", "magx", "magy", "magz");
     attr_scalar(o, g, stem, "etot");
     if (g.glm) attr_scalar(o, g, stem, "psi");
-    if (!ckpt) {
+    if (!ckpt && g.sr) {
+      attr_scalar(o, g, stem, "rho");
+      attr_vector(o, g, stem, "vel", "velx", "vely", "velz");
+      attr_scalar(o, g, stem, "lorz");
+      attr_scalar(o, g, stem, "pres");
+    } else if (!ckpt) {
       attr_vector(o, g, stem, "vel", "velx", "vely", "velz");
       attr_scalar(o, g, stem, "eint");
       if (g.glm) {

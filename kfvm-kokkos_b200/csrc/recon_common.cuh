@@ -52,6 +52,12 @@ __device__ __forceinline__ void pos_tile_fill(const double *__restrict__ U, cons
     double st[E::NV];
 #pragma unroll
     for (int v = 0; v < E::NV; v++) st[v] = Uc[v * g.pvol];
+    if constexpr (EQ == EQ_SR) {
+      // density and E - sqrt(D^2 + S^2); SR bounds need nothing else
+      sm[0][t] = st[DENS];
+      sm[1][t] = sr::ediff(st);
+      continue;
+    }
     const double ir = 1.0 / st[DENS];
     const double ei = E::eint_r(st, ir);
     sm[0][t] = st[DENS];
@@ -63,7 +69,8 @@ __device__ __forceinline__ void pos_tile_fill(const double *__restrict__ U, cons
   }
 }
 
-// PositivityPreserve_K bounds (Common_K.H:331-380) from the footprint tile
+// PositivityPreserve_K bounds (Common_K.H:331-380; SR: SRHydro_K.H:224-246, no
+// flattening) from the footprint tile
 template <int DIM, int EQ>
 __device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<DIM>::N], int tx, int ty) {
   using P = PosTile<DIM>;
@@ -71,6 +78,20 @@ __device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<
   double minEint = 1.7976931348623157e308, minSdSp = 1.7976931348623157e308;
   constexpr int zr = DIM == 3 ? 1 : 0;
   auto at = [&](int xo, int yo, int zo) { return ((zr + zo) * P::TY + (ty + 1 + yo)) * P::TX + (tx + 1 + xo); };
+  if constexpr (EQ == EQ_SR) {
+#pragma unroll
+    for (int xo = -1; xo <= 1; xo++)
+#pragma unroll
+      for (int yo = -1; yo <= 1; yo++)
+#pragma unroll
+        for (int zo = -zr; zo <= zr; zo++) {
+          const int t = at(xo, yo, zo);
+          maxDens = fmax(maxDens, sm[0][t]);
+          minDens = fmin(minDens, sm[0][t]);
+          minEint = fmin(minEint, sm[1][t]);
+        }
+    return PosBounds{sm[0][at(0, 0, 0)], minDens, maxDens, minEint};
+  }
 #pragma unroll
   for (int xo = -1; xo <= 1; xo++)
 #pragma unroll

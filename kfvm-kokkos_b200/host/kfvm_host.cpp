@@ -154,6 +154,7 @@ bool ProblemSetup::setSetup(const std::string &setting) {
     if (v == "hydro") cfg.eq = KFVM_EQ_HYDRO;
     else if (v == "navierstokes") cfg.eq = KFVM_EQ_NAVIERSTOKES;
     else if (v == "mhd_glm") cfg.eq = KFVM_EQ_MHD_GLM;
+    else if (v == "srhydro") cfg.eq = KFVM_EQ_SRHYDRO;
     else return false;
   } else if (k == "riemann") {
     if (v == "llf") cfg.rs = KFVM_RS_LLF;
@@ -184,6 +185,8 @@ bool ProblemSetup::setSetup(const std::string &setting) {
     else if (v == "taylor_green") ic = KFVM_IC_TAYLOR_GREEN;
     else if (v == "orszag_tang") ic = KFVM_IC_ORSZAG_TANG;
     else if (v == "smooth_wave") ic = KFVM_IC_SMOOTH_WAVE;
+    else if (v == "sr_shock_tube") ic = KFVM_IC_SR_SHOCK_TUBE;
+    else if (v == "sr_riemann_2d") ic = KFVM_IC_SR_RIEMANN_2D;
     else return false;
   } else if (k == "seed") {
     seed = (uint64_t)std::stoull(v);

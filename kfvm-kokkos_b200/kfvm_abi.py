@@ -8,7 +8,7 @@ through float32 here.
 import ctypes as C
 import struct
 
-KFVM_EQ_HYDRO, KFVM_EQ_NAVIERSTOKES, KFVM_EQ_MHD_GLM = 0, 1, 2
+KFVM_EQ_HYDRO, KFVM_EQ_NAVIERSTOKES, KFVM_EQ_MHD_GLM, KFVM_EQ_SRHYDRO = 0, 1, 2, 3
 KFVM_RS_LLF, KFVM_RS_HLL, KFVM_RS_HLLC = 0, 1, 2
 KFVM_RK_THREESTARP, KFVM_RK_FOURSTARP, KFVM_RK_SSP4_3_2, KFVM_RK_SSP10_4_3 = 0, 1, 2, 3
 KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW, KFVM_BC_REFLECTING, KFVM_BC_NOSLIP = 0, 1, 2, 3
@@ -16,7 +16,8 @@ KFVM_TS_ACCEPTED, KFVM_TS_TOLERANCE, KFVM_TS_UNPHYSICAL = 0, 1, 2
 KFVM_IND_KXRCF, KFVM_IND_ALL, KFVM_IND_NONE, KFVM_IND_MLP = 0, 1, 2, 3
 KFVM_PREC_FP64, KFVM_PREC_TF32X3 = 0, 1
 (KFVM_IC_ISENTROPIC_VORTEX, KFVM_IC_SPHERICAL_SOD, KFVM_IC_KELVIN_HELMHOLTZ,
- KFVM_IC_TAYLOR_GREEN, KFVM_IC_ORSZAG_TANG, KFVM_IC_SMOOTH_WAVE) = range(6)
+ KFVM_IC_TAYLOR_GREEN, KFVM_IC_ORSZAG_TANG, KFVM_IC_SMOOTH_WAVE,
+ KFVM_IC_SR_SHOCK_TUBE, KFVM_IC_SR_RIEMANN_2D) = range(8)
 
 KFVM_MAX_CELLS, KFVM_MAX_SUB, KFVM_MAX_BIAS, KFVM_MAX_BCELLS = 33, 8, 6, 11
 KFVM_MAX_INDIC, KFVM_MAX_FACEQ, KFVM_MAX_CELLQ = 19, 9, 27
@@ -145,6 +146,20 @@ def workload(name, scale=None, steps=None):
         c = make_config(2, KFVM_EQ_MHD_GLM, n, n, extent=(0, 1, 0, 1),
                         gamma=5.0 / 3.0, rs=KFVM_RS_HLL, cfl=0.4, steps=steps or 1000)
         return c, KFVM_IC_ORSZAG_TANG
+    # special-relativistic hydro (exec/SRHydro/SRShockTube, exec/SRHydro/SRRiem2d)
+    if name == "sr_shock_tube":
+        n = scale or 2000
+        c = make_config(3, KFVM_EQ_SRHYDRO, n, 4, 4, extent=(0, 1, 0, 0.002, 0, 0.002),
+                        bc=["outflow", "outflow", "periodic", "periodic", "periodic", "periodic"],
+                        gamma=1.66666666666666, rs=KFVM_RS_HLL, cfl=1.25, steps=steps or 100,
+                        atol=1e-3, rtol=1e-3)
+        return c, KFVM_IC_SR_SHOCK_TUBE
+    if name == "sr_riemann_2d":
+        n = scale or 512
+        c = make_config(2, KFVM_EQ_SRHYDRO, n, n, extent=(-1, 1, -1, 1), bc="outflow",
+                        gamma=1.66666666666666, rs=KFVM_RS_LLF, cfl=1.0, steps=steps or 200,
+                        atol=1e-3, rtol=1e-3)
+        return c, KFVM_IC_SR_RIEMANN_2D
     raise ValueError(name)
 
 

@@ -245,6 +245,74 @@ struct Phys {
   int eq, nv, rs;
   double gamma, ch;
 
+  // ---- special-relativistic hydro (SRHydro_EOS.H:30-260) ----
+  static double sr_ssq(const double *U) { return U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]; }
+  static double sr_lorenz(double p, const double *U) {
+    const double DhW = U[ETOT] + p, DhWsq = DhW * DhW;
+    return 1.0 / sqrt(1.0 - sr_ssq(U) / DhWsq);
+  }
+  // initial guess (eqs 2.21 / 2.16 of arXiv:2305.14805, as SRHydro_EOS.H:75-91)
+  double sr_pres_guess(const double *U) const {
+    const double ESsq = U[ETOT] * U[ETOT] - sr_ssq(U);
+    if (U[DENS] >= ESsq / U[ETOT]) return 0.0;
+    const double gm2E = (gamma - 2.0) * U[ETOT], gm = gamma - 1.0;
+    return (gm2E + sqrt(gm2E * gm2E - 4.0 * gm * (U[DENS] * sqrt(ESsq) - ESsq))) / 2.0;
+  }
+  // the stable Newton iteration (algorithm 2.3)
+  double sr_pres_stable(double rtol, const double *U, double p) const {
+    const double gm = gamma - 1.0, gm2 = gamma - 2.0, D = U[DENS], E = U[ETOT], Ssq = sr_ssq(U);
+    for (int n = 0; n < 200; n++) {
+      const double EP = E + p, rt = sqrt(EP * EP - Ssq);
+      const double psiP = Ssq + EP * (p / gm - E) + D * rt;
+      const double dpsiP = (2.0 * p - gm2 * E) / gm + D * EP / rt;
+      const double dp = -psiP / dpsiP;
+      if (fabs(dp) / p < rtol) break;
+      p += dp;
+    }
+    return p;
+  }
+  // pressure recovery (algorithm 2.1 with the switch to 2.3), SRHydro_EOS.H:118-175
+  double sr_pres(const double *U) const {
+    const double eps1 = 0.01, eps2 = 1.e-4, rtol = 1.e-9;
+    double p = sr_pres_guess(U);
+    const double Dsq = U[DENS] * U[DENS], Esq = U[ETOT] * U[ETOT], Ssq = sr_ssq(U), ESsq = Esq - Ssq;
+    if (Dsq / ESsq < eps2) return sr_pres_stable(rtol, U, p);
+    const double gm = gamma - 1.0, gm2 = gamma - 2.0;
+    const double c0 = -ESsq * (Dsq - ESsq) * gm * gm;
+    const double c1 = 2.0 * U[ETOT] * (gm2 * ESsq * gm - Dsq * gm * gm);
+    const double c2 = Esq * (gamma * gamma - 6.0 * gm) + 2.0 * Ssq * gm - Dsq * gm * gm;
+    const double c3 = -2.0 * U[ETOT] * gm2;
+    for (int n = 0; n < 200; n++) {
+      const double W = sr_lorenz(p, U);
+      if (W < 1.0 + eps1) return sr_pres_stable(rtol, U, p);
+      const double phiP = c0 + p * (c1 + p * (c2 + p * (c3 + p)));
+      const double dphiP = c1 + p * (2.0 * c2 + p * (3.0 * c3 + p));
+      const double dp = -phiP / dphiP;
+      if (fabs(dp) / p < rtol) break;
+      p += dp;
+    }
+    return p;
+  }
+  // cons2prim (SRHydro_EOS.H:30-48): V = rho, vx, vy, vz, p, and W in V[5]
+  void sr_cons2prim(const double *U, double *V) const {
+    const double p = sr_pres(U);
+    const double W = sr_lorenz(p, U);
+    const double rho = U[DENS] / W;
+    const double ei = p / ((gamma - 1.0) * (U[DENS] / sr_lorenz(p, U))), h = 1.0 + gamma * ei;
+    V[0] = rho;
+    V[1] = U[MOMX] / (rho * W * W * h);
+    V[2] = U[MOMY] / (rho * W * W * h);
+    V[3] = U[MOMZ] / (rho * W * W * h);
+    V[4] = p;
+    V[5] = W;
+  }
+  double sr_soundspeed(const double *V) const {
+    const double h = 1.0 + gamma * V[4] / ((gamma - 1.0) * V[0]);
+    return sqrt(gamma * V[4] / (V[0] * h));
+  }
+  // E - sqrt(D^2 + S^2), the quantity the SR limiter bounds (SRHydro_K.H:440-450)
+  static double sr_ediff(const double *U) { return U[ETOT] - sqrt(U[DENS] * U[DENS] + sr_ssq(U)); }
+
   double ekin(const double *U) const {
     return 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]) / U[DENS];
   }
@@ -257,8 +325,16 @@ struct Phys {
   }
   double pres(const double *U) const { return (gamma - 1.0) * eint(U); }
   double soundspeed(const double *U) const { return sqrt(gamma * pres(U) / U[DENS]); }
-  double weno(const double *U) const { return pres(U) / std::pow(U[DENS], gamma); }
+  double weno(const double *U) const {
+    if (eq == KFVM_EQ_SRHYDRO) return U[DENS]; // SRHydro_EOS.H:225-228
+    return pres(U) / std::pow(U[DENS], gamma);
+  }
   double positivity(const double *U) const {
+    if (eq == KFVM_EQ_SRHYDRO) {
+      // SRHydro_EOS.H:238-250: the bound on E also keeps p > 0 and |v| < 1
+      const double etotDiff = U[ETOT] * U[ETOT] - (U[DENS] * U[DENS] + sr_ssq(U));
+      return fmin(U[DENS], etotDiff);
+    }
     if (eq == KFVM_EQ_MHD_GLM) {
       for (int v = 0; v < nv; v++)
         if (std::isnan(U[v])) return -1.0;
@@ -266,6 +342,10 @@ struct Phys {
     return fmin(U[DENS], eint(U));
   }
   void cons2prim(const double *U, double *V) const {
+    if (eq == KFVM_EQ_SRHYDRO) {
+      sr_cons2prim(U, V);
+      return;
+    }
     V[0] = U[DENS];
     V[1] = U[MOMX] / U[DENS];
     V[2] = U[MOMY] / U[DENS];
@@ -289,6 +369,15 @@ struct Phys {
   // ---- fluxes (Hydro_Riemann.H:26-37, MHD_GLM_Riemann.H:25-53) ----
   void flux(const int ord[3], const double *U, const double *V, double *F) const {
     const int vo[3] = {MOMX + ord[0], MOMX + ord[1], MOMX + ord[2]};
+    if (eq == KFVM_EQ_SRHYDRO) {
+      // SRHydro_Riemann.H:24-36
+      F[DENS] = U[DENS] * V[vo[0]];
+      F[vo[0]] = U[vo[0]] * V[vo[0]] + V[4];
+      F[vo[1]] = U[vo[1]] * V[vo[0]];
+      F[vo[2]] = U[vo[2]] * V[vo[0]];
+      F[ETOT] = U[vo[0]];
+      return;
+    }
     if (eq != KFVM_EQ_MHD_GLM) {
       F[DENS] = U[vo[0]];
       F[vo[0]] = U[vo[0]] * V[vo[0]] + V[4];
@@ -324,6 +413,22 @@ struct Phys {
   double speeds(const int ord[3], const double *uL, const double *uR, const double *vL,
                 const double *vR, double &sL, double &sR) const {
     const int vo[3] = {MOMX + ord[0], MOMX + ord[1], MOMX + ord[2]};
+    if (eq == KFVM_EQ_SRHYDRO) {
+      // SRHydro_Riemann.H:39-77
+      const double aL = sr_soundspeed(vL), aLsq = aL * aL;
+      const double aR = sr_soundspeed(vR), aRsq = aR * aR;
+      const double wL = vL[5], sigL = aLsq / (wL * wL * (1.0 - aLsq));
+      const double sqrtL = sqrt(sigL * (1.0 + sigL - vL[vo[0]] * vL[vo[0]]));
+      const double wR = vR[5], sigR = aRsq / (wR * wR * (1.0 - aRsq));
+      const double sqrtR = sqrt(sigR * (1.0 + sigR - vR[vo[0]] * vR[vo[0]]));
+      const double sLm = (vL[vo[0]] - sqrtL) / (1.0 + sigL);
+      const double sRm = (vR[vo[0]] - sqrtR) / (1.0 + sigR);
+      const double sLp = (vL[vo[0]] + sqrtL) / (1.0 + sigL);
+      const double sRp = (vR[vo[0]] + sqrtR) / (1.0 + sigR);
+      sL = fmin(sLm, sRm);
+      sR = fmax(sLp, sRp);
+      return fmax(fabs(sL), fabs(sR));
+    }
     if (eq != KFVM_EQ_MHD_GLM) {
       const double rhoL = uL[DENS], rhoR = uR[DENS];
       const double hL = (uL[ETOT] + vL[4]) / rhoL, hR = (uR[ETOT] + vR[4]) / rhoR;
@@ -426,7 +531,14 @@ struct Phys {
 struct VarConv {
   int eq;
   double gamm, rho, u, v, w, bx, by, bz, rPsi, vsq;
+  double D = 0.0, Sx = 0.0, Sy = 0.0, Sz = 0.0; // SRHydro_K.H:28-58
   VarConv(int eq_, const double *ref, double gam) : eq(eq_) {
+    if (eq == KFVM_EQ_SRHYDRO) {
+      D = ref[DENS];
+      Sx = ref[MOMX];
+      Sy = ref[MOMY];
+      Sz = ref[MOMZ];
+    }
     gamm = gam - 1.0;
     rho = ref[DENS];
     u = ref[MOMX] / rho;
@@ -444,6 +556,12 @@ struct VarConv {
     }
   }
   void cons2LinPrim(double *s) const {
+    if (eq == KFVM_EQ_SRHYDRO) {
+      s[MOMX] = s[MOMX] / D - s[DENS] * Sx / (D * D);
+      s[MOMY] = s[MOMY] / D - s[DENS] * Sy / (D * D);
+      s[MOMZ] = s[MOMZ] / D - s[DENS] * Sz / (D * D);
+      return;
+    }
     if (eq == KFVM_EQ_MHD_GLM) {
       s[ETOT] = gamm * (vsq * s[DENS] + s[ETOT] - u * s[MOMX] - v * s[MOMY] - w * s[MOMZ] -
                         bx * s[MAGX] - by * s[MAGY] - bz * s[MAGZ] - rPsi * s[PSI]);
@@ -455,6 +573,12 @@ struct VarConv {
     s[MOMZ] = (s[MOMZ] - w * s[DENS]) / rho;
   }
   void linPrim2Cons(double *s) const {
+    if (eq == KFVM_EQ_SRHYDRO) {
+      s[MOMX] = s[DENS] * Sx / D + D * s[MOMX];
+      s[MOMY] = s[DENS] * Sy / D + D * s[MOMY];
+      s[MOMZ] = s[DENS] * Sz / D + D * s[MOMZ];
+      return;
+    }
     if (eq == KFVM_EQ_MHD_GLM) {
       s[ETOT] = (vsq * s[DENS] + rho * u * s[MOMX] + rho * v * s[MOMY] + rho * w * s[MOMZ] +
                  bx * s[MAGX] + by * s[MAGY] + bz * s[MAGZ] + s[ETOT] / gamm + rPsi * s[PSI]);
@@ -543,6 +667,34 @@ void ic_point(int kind, const kfvm_config &c, double x, double y, double z, doub
     s[ETOT] = p / gm + rho * (u * u + v * v + w * w) / 2.0 + (bx * bx + by * by + bz * bz) / 2.0;
     break;
   }
+  case KFVM_IC_SR_SHOCK_TUBE: {
+    // exec/SRHydro/SRShockTube/InitialCondition.H
+    const double gR = c.gamma / (c.gamma - 1.0), ax = fabs(x), W = 1.0;
+    const double rho = ax < 0.5 ? 10.0 : 1.0, p = ax < 0.5 ? 40.0 / 3.0 : 1.e-6;
+    const double h = 1.0 + p * gR / rho;
+    s[DENS] = rho * W;
+    s[ETOT] = rho * h * W * W - p;
+    break;
+  }
+  case KFVM_IC_SR_RIEMANN_2D: {
+    // exec/SRHydro/SRRiem2d/InitialCondition.H
+    const double gR = c.gamma / (c.gamma - 1.0), v0 = 0.99;
+    double rho, vx, vy, p;
+    if (x > 0.0) {
+      if (y > 0.0) { rho = 0.1; vx = 0.0; vy = 0.0; p = 0.01; }
+      else { rho = 0.1; vx = 0.0; vy = v0; p = 1.0; }
+    } else {
+      if (y > 0.0) { rho = 0.1; vx = v0; vy = 0.0; p = 1.0; }
+      else { rho = 0.5; vx = 0.0; vy = 0.0; p = 1.0; }
+    }
+    const double W = 1.0 / sqrt(1.0 - vx * vx - vy * vy), h = 1.0 + p * gR / rho;
+    s[DENS] = rho * W;
+    s[MOMX] = rho * W * W * h * vx;
+    s[MOMY] = rho * W * W * h * vy;
+    s[MOMZ] = 0.0;
+    s[ETOT] = rho * W * W * h - p;
+    break;
+  }
   default: { // KFVM_IC_SMOOTH_WAVE
     const double X = 2.0 * M_PI * (x - c.xlo) / (c.xup - c.xlo);
     const double Y = 2.0 * M_PI * (y - c.ylo) / (c.yup - c.ylo);
@@ -550,6 +702,16 @@ void ic_point(int kind, const kfvm_config &c, double x, double y, double z, doub
     const double rho = 1.0 + 0.2 * std::sin(X) * std::cos(Y) * std::cos(Z);
     const double u = 0.5 + 0.1 * std::sin(Y), v = 0.3 * std::cos(X), w = 0.1 * std::sin(X + Y);
     const double p = 1.0 + 0.1 * std::cos(X - Y + Z);
+    if (c.eq == KFVM_EQ_SRHYDRO) {
+      // the same primitives as a special-relativistic state
+      const double W = 1.0 / sqrt(1.0 - (u * u + v * v + w * w)), h = 1.0 + p * c.gamma / (gm * rho);
+      s[DENS] = rho * W;
+      s[MOMX] = rho * W * W * h * u;
+      s[MOMY] = rho * W * W * h * v;
+      s[MOMZ] = rho * W * W * h * w;
+      s[ETOT] = rho * W * W * h - p;
+      break;
+    }
     s[DENS] = rho;
     s[MOMX] = rho * u;
     s[MOMY] = rho * v;
@@ -975,6 +1137,62 @@ bool kxrcf(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t j, in
   return (w >= wThresh || S.theta[S.ci(i, j, k)] < 1.0);
 }
 
+// PositivityPreserve_K<SRHydro> (SRHydro_K.H:193-452): the density bounds of the
+// 3^d neighbours (no flattening), then a lower bound on E - sqrt(D^2 + S^2); each
+// theta is applied to every face and source point, also when it is 1
+void positivity_sr(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t j,
+                   int64_t k, const double *ref) {
+  const int nv = S.nv, nqf = S.nqf;
+  const double rDens = ref[DENS], edRef = Phys::sr_ediff(ref);
+  double maxDens = -std::numeric_limits<double>::max(), minDens = std::numeric_limits<double>::max();
+  double minED = std::numeric_limits<double>::max();
+  const int zr = S.dim == 3 ? 1 : 0;
+  for (int xo = -1; xo <= 1; xo++)
+    for (int yo = -1; yo <= 1; yo++)
+      for (int zo = -zr; zo <= zr; zo++) {
+        double s[9];
+        S.load(B, i + xo, j + yo, k + zo, s);
+        maxDens = fmax(maxDens, s[DENS]);
+        minDens = fmin(minDens, s[DENS]);
+        minED = fmin(minED, Phys::sr_ediff(s));
+      }
+  double *rsF[6];
+  own_faces(S, i, j, k, rsF);
+  const int nF = 2 * S.dim;
+  const int64_t c = S.ci(i, j, k);
+  auto mix = [&](double th) {
+    for (int q = 0; q < nqf; q++)
+      for (int v = 0; v < nv; v++)
+        for (int f = 0; f < nF; f++) rsF[f][q * nv + v] = ref[v] + th * (rsF[f][q * nv + v] - ref[v]);
+    if (S.haveSources)
+      for (int q = 0; q < S.nqc; q++)
+        for (int v = 0; v < nv; v++) S.sp(c, q)[v] = ref[v] + th * (S.sp(c, q)[v] - ref[v]);
+  };
+  const double rDP = maxDens - rDens, rDM = rDens - minDens;
+  double thD = 1.0;
+  auto dth = [&](double rho) {
+    thD = rho < minDens ? fmin(thD, rDM / (rDens - rho)) : thD;
+    thD = rho > maxDens ? fmin(thD, rDP / (rho - rDens)) : thD;
+  };
+  for (int q = 0; q < nqf; q++)
+    for (int f = 0; f < nF; f++) dth(rsF[f][q * nv + DENS]);
+  if (S.haveSources)
+    for (int q = 0; q < S.nqc; q++) dth(S.sp(c, q)[DENS]);
+  mix(thD);
+  const double edd = edRef - minED;
+  double thE = 1.0;
+  auto eth = [&](const double *state) {
+    const double ed = Phys::sr_ediff(state);
+    thE = ed < minED ? fmin(thE, edd / (edRef - ed)) : thE;
+  };
+  for (int q = 0; q < nqf; q++)
+    for (int f = 0; f < nF; f++) eth(&rsF[f][q * nv]);
+  if (S.haveSources)
+    for (int q = 0; q < S.nqc; q++) eth(S.sp(c, q));
+  mix(thE);
+  S.theta[c] = fmin(thE, thD);
+}
+
 // PositivityPreserve_K (Common_K.H:299-643)
 void positivity(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t j,
                 int64_t k) {
@@ -983,6 +1201,10 @@ void positivity(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t 
   double ref[9];
   S.load(B, i, j, k, ref);
   const double rDens = ref[DENS];
+  if (S.cfg.eq == KFVM_EQ_SRHYDRO) {
+    positivity_sr(S, B, i, j, k, ref);
+    return;
+  }
   double maxDens = -std::numeric_limits<double>::max(), minDens = std::numeric_limits<double>::max();
   double minEint = std::numeric_limits<double>::max(), minSdSp = std::numeric_limits<double>::max();
   const int zr = S.dim == 3 ? 1 : 0;
@@ -1626,6 +1848,9 @@ int orc_set_threads(int n) {
 
 orc_solver *orc_create(const kfvm_config *cfg) {
   if (!cfg || (cfg->dim != 2 && cfg->dim != 3) || cfg->nq < 1 || cfg->nq > 3) return nullptr;
+  if (cfg->eq < KFVM_EQ_HYDRO || cfg->eq > KFVM_EQ_SRHYDRO) return nullptr;
+  // the SR Riemann solvers are HLL and LLF only (SRHydro_Riemann.H)
+  if (cfg->eq == KFVM_EQ_SRHYDRO && cfg->rs == KFVM_RS_HLLC) return nullptr;
   orc_solver *S = new orc_solver();
   S->cfg = *cfg;
   if (S->cfg.dim == 2) S->cfg.nz = 1;

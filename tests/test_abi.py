@@ -61,6 +61,10 @@ def test_default_config(product_lib):
     (lambda c: setattr(c, "nq", 4), "NUM_QUAD_PTS"),
     (lambda c: (setattr(c, "dim", 3), setattr(c, "nz", 16), setattr(c, "nq", 3)), "NUM_QUAD_PTS"),
     (lambda c: (setattr(c, "eq", abi.KFVM_EQ_MHD_GLM), setattr(c, "rs", abi.KFVM_RS_HLLC)), "HLLC"),
+    (lambda c: (setattr(c, "eq", abi.KFVM_EQ_SRHYDRO), setattr(c, "rs", abi.KFVM_RS_HLLC)), "HLL and LLF"),
+    (lambda c: (setattr(c, "eq", abi.KFVM_EQ_SRHYDRO), setattr(c, "rs", abi.KFVM_RS_HLL),
+                setattr(c, "indicator", abi.KFVM_IND_MLP)), "learned"),
+    (lambda c: setattr(c, "eq", 4), "equation"),
     (lambda c: c.bc.__setitem__(1, abi.KFVM_BC_OUTFLOW), "pairs"),
     (lambda c: setattr(c, "rk", 9), "RK"),
     (lambda c: setattr(c, "nx", 2), "small"),

@@ -242,3 +242,82 @@ def test_solver_variants(name, scale, steps, over, gpu, product_lib, oracle_lib)
     step_pair(g, o, steps)
     err = rel_l1(g.get_state(), o.get_state())
     assert np.all(err <= STEP_TOL), err
+
+
+# special-relativistic hydro (src/physics/srhydro): the reference's shock tube and
+# four-quadrant Riemann problem at small sizes, and a smooth periodic flow
+def sr_smooth(dim, n, steps, rs):
+    cfg = abi.make_config(dim, abi.KFVM_EQ_SRHYDRO, n, n, n, gamma=5.0 / 3.0, rs=rs, cfl=0.8,
+                          steps=steps)
+    return cfg, abi.KFVM_IC_SMOOTH_WAVE
+
+
+def face_departure(cfg, faces, u):
+    """Per cell: the largest |face state - cell mean| over its face points and
+    variables, relative to the largest |component| of the cell mean."""
+    nz = cfg.nz if cfg.dim == 3 else 1
+    n = cfg.nx * cfg.ny * nz
+    k, j, i = np.unravel_index(np.arange(n), (nz, cfg.ny, cfg.nx))
+    dep = np.zeros(n)
+    for d in range(cfg.dim):
+        f = faces[d]                                  # [slot][q][v][face]
+        fx, fy = cfg.nx + (d == 0), cfg.ny + (d == 1)
+        lo = (k * fy + j) * fx + i
+        hi = ((k + (d == 2)) * fy + (j + (d == 1))) * fx + (i + (d == 0))
+        for slot, idx in ((1, lo), (0, hi)):
+            s_ = f[slot][:, :, idx]                   # [q][v][cell]
+            dep = np.maximum(dep, np.abs(s_ - u[None]).max(axis=(0, 1)))
+    return dep / np.abs(u).max(axis=0)
+
+
+SR_CASES = [
+    ("sr_shock_tube", 48, 5, 2),
+    ("sr_riemann_2d", 32, 5, 2),
+    ("sr_riemann_2d", 32, 4, 3),
+    ("sr_smooth_2d", 24, 4, 2),
+    ("sr_smooth_3d", 12, 3, 2),
+]
+
+
+@pytest.mark.parametrize("name,scale,steps,nq", SR_CASES)
+def test_srhydro_against_oracle(name, scale, steps, nq, gpu, product_lib, oracle_lib):
+    """SRHydro: Newton pressure recovery, HLL / LLF fluxes with the relativistic
+    speed bounds, the density + E - |(D, S)| limiter: initial condition, one RHS
+    evaluation with its face states, flags and max wave speed, and N steps."""
+    if name == "sr_smooth_2d":
+        cfg, ic = sr_smooth(2, scale, steps, abi.KFVM_RS_LLF)
+    elif name == "sr_smooth_3d":
+        cfg, ic = sr_smooth(3, scale, steps, abi.KFVM_RS_HLL)
+    else:
+        cfg, ic = abi.workload(name, scale=scale, steps=steps)
+    cfg.nq = nq
+    g = product_lib.Solver(cfg)
+    o = oracle_lib.OracleSolver(cfg)
+    g.init_ic(ic)
+    o.init_ic(ic)
+    assert np.all(rel_l1(g.get_state(), o.get_state()) <= 1e-14)
+    o.keep_faces(True)
+    rg, vg = g.eval_rhs(0.0)
+    ro, vo = o.eval_rhs(0.0)
+    assert np.all(rel_l1(rg, ro) <= RHS_TOL), rel_l1(rg, ro)
+    assert abs(vg - vo) <= 1e-13 * abs(vo)
+    ag, thg = g.flags()
+    ao, tho = o.flags()
+    assert np.array_equal(ag, ao), (ag.sum(), ao.sum())
+    fg = [g.faces(d) for d in range(cfg.dim)]
+    fo = [o.faces(d) for d in range(cfg.dim)]
+    for d in range(cfg.dim):
+        assert np.abs(fg[d] - fo[d]).max() <= 1e-12 * np.abs(fo[d]).max(), d
+    # theta may differ only where it changes nothing.  SR's limiter compares
+    # strictly against neighbourhood bounds that include the cell itself
+    # (SRHydro_K.H:224-257, no flattening margin), so where the reconstruction
+    # returns the cell mean to rounding (a uniform stencil, or WENO-AO choosing a
+    # uniform substencil next to a jump) theta is 0 or 1 by the sign of the
+    # rounding; the limited states are then the cell mean on both sides.
+    diff = np.abs(thg - tho) > 1e-12
+    u0 = o.get_state()
+    assert np.all(face_departure(cfg, fg, u0)[diff] <= 1e-12)
+    assert np.all(face_departure(cfg, fo, u0)[diff] <= 1e-12)
+    step_pair(g, o, steps)
+    err = rel_l1(g.get_state(), o.get_state())
+    assert np.all(err <= STEP_TOL), err

@@ -243,3 +243,41 @@ def test_oracle_walls_conserve_mass(name, scale, walls, oracle_lib):
     u1 = s.get_state()
     assert np.all(np.isfinite(u1))
     assert abs(u1[0].sum() - m0) <= 1e-12 * abs(m0)
+
+
+@pytest.mark.parametrize("dim,n,rs", [(2, 16, abi.KFVM_RS_LLF), (3, 8, abi.KFVM_RS_HLL)])
+def test_oracle_srhydro_conserves_periodic(dim, n, rs, oracle_lib):
+    """SRHydro on a periodic smooth flow: D, S and E are conserved to rounding (the
+    flux differences telescope) and every state stays admissible: D > 0 and
+    E^2 > D^2 + |S|^2 (SRHydro_EOS.H:238-250)."""
+    cfg = abi.make_config(dim, abi.KFVM_EQ_SRHYDRO, n, n, n, gamma=5.0 / 3.0, rs=rs, cfl=0.8, steps=4)
+    s = oracle_lib.OracleSolver(cfg)
+    s.init_ic(abi.KFVM_IC_SMOOTH_WAVE)
+    u0 = s.get_state()
+    s.solve(cfg.max_steps)
+    u1 = s.get_state()
+    assert np.all(np.isfinite(u1))
+    tot0, tot1 = u0.sum(axis=1), u1.sum(axis=1)
+    scale = np.abs(u0).sum(axis=1)
+    assert np.all(np.abs(tot1 - tot0) <= 1e-12 * scale), (tot1 - tot0) / scale
+    assert np.all(u1[0] > 0.0)
+    assert np.all(u1[4] ** 2 > u1[0] ** 2 + (u1[1:4] ** 2).sum(axis=0))
+
+
+def test_oracle_sr_shock_tube_plateaus(oracle_lib):
+    """SRShockTube (exec/SRHydro/SRShockTube) before the waves reach the outflow
+    ends: mass is conserved, the undisturbed states keep their initial values, and
+    D stays between the two initial densities (the limiter bounds face values, so
+    cell averages may cross the bounds by rounding-sized amounts of the RK stages)."""
+    cfg, ic = abi.workload("sr_shock_tube", scale=64, steps=12)
+    s = oracle_lib.OracleSolver(cfg)
+    s.init_ic(ic)
+    u0 = s.get_state()
+    s.solve(cfg.max_steps)
+    u1 = s.get_state().reshape(5, 4, 4, 64)
+    assert abs(u1[0].sum() - u0[0].sum()) <= 1e-12 * u0[0].sum()
+    d = u1[0, 0, 0]
+    assert np.all(u1[0] == u1[0, :1, :1])           # uniform across y and z
+    assert d[0] == 10.0 and d[-1] == 1.0
+    assert d.min() >= 1.0 - 1e-6 and d.max() <= 10.0 + 1e-6
+    assert np.all(np.diff(d) <= 1e-6)               # D falls from left to right

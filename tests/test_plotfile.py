@@ -178,3 +178,36 @@ def test_driver_plots_on_plot_times_and_restarts(tmp_path, gpu, product_lib):
     assert np.array_equal(a.get_state(), b.get_state())
     a.close()
     b.close()
+
+
+def test_plot_srhydro_aux_recovers_primitives(tmp_path, product_lib):
+    """AuxVars<SRHydro> (SRHydro_K.H:59-88, WriterPDI.cpp:268-278): rho, vel, lorz and
+    pres from the Newton pressure recovery of SRHydro_EOS.H, checked against the
+    primitives the conserved state was built from, over both branches of the
+    recovery (D^2 / (E^2 - S^2) above and below 1e-4) and Lorentz factors up to 22."""
+    kfvm = product_lib
+    cfg = small_cfg(2, abi.KFVM_EQ_SRHYDRO)
+    cfg.gamma = abi.stof(5.0 / 3.0)
+    g = cfg.gamma
+    rng = np.random.default_rng(11)
+    n = abi.ncells(cfg)
+    rho = 10.0 ** rng.uniform(-3, 1, n)
+    p = 10.0 ** rng.uniform(-3, 2, n)
+    speed = np.concatenate([rng.uniform(0, 0.999, n - 4), [0.0, 0.5, 0.99, 0.999]])
+    ang = rng.uniform(0, 2 * np.pi, n)
+    vx, vy, vz = speed * np.cos(ang), speed * np.sin(ang) * 0.8, speed * np.sin(ang) * 0.6
+    W = 1.0 / np.sqrt(1.0 - (vx * vx + vy * vy + vz * vz))
+    h = 1.0 + g * p / ((g - 1.0) * rho)
+    u = np.stack([rho * W, rho * W * W * h * vx, rho * W * W * h * vy, rho * W * W * h * vz,
+                  rho * W * W * h - p])
+    weno = np.zeros(n, np.uint8)
+    theta = np.ones(n)
+    xmf = kfvm.plotfile_write(cfg, tmp_path, "sr", 2, u, weno, theta)
+    _, attrs, _ = items(xmf)
+    assert list(attrs) == ["dens", "mom", "etot", "rho", "vel", "lorz", "pres", "weno", "fomx"]
+    rd = lambda name: np.fromfile(tmp_path / f"sr_0000002.{name}.bin", dtype="<f8")
+    assert np.allclose(rd("pres"), p, rtol=1e-8, atol=0)
+    assert np.allclose(rd("rho"), rho, rtol=1e-8, atol=0)
+    assert np.allclose(rd("lorz"), W, rtol=1e-8, atol=0)
+    for name, v in (("velx", vx), ("vely", vy), ("velz", vz)):
+        assert np.allclose(rd(name), v, rtol=1e-8, atol=1e-12)
