@@ -53,6 +53,9 @@ WORKLOADS = {
     "isentropic_vortex": (128, 2, "2D Euler isentropic vortex",
                           "2D Euler isentropic vortex {s}^2 periodic, GP-WENO-AO r=2 + KXRCF, HLLC, SSP(4,3) FSAL "
                           "adaptive, CFL 0.8"),
+    "sr_riemann_2d": (512, 2, "2D SR-hydro four-quadrant Riemann",
+                      "2D special-relativistic hydro four-quadrant Riemann problem {s}^2 outflow, GP-WENO-AO r=2 + "
+                      "KXRCF, LLF, SSP(4,3) FSAL adaptive, CFL 1.0, Newton pressure recovery"),
 }
 
 
@@ -391,7 +394,7 @@ def run_ours(args):
     # DRAM bytes per cell of each kernel class from one ncu capture (profiles/),
     # scaled by the cells one launch processes
     traffic_tbl = load_json(os.path.join(ROOT, "profiles", "dram_traffic.json")) or {}
-    case = f"{cfg.dim}d_{('hydro', 'ns', 'glm')[cfg.eq]}"
+    case = f"{cfg.dim}d_{('hydro', 'ns', 'glm', 'sr')[cfg.eq]}"
     per_cell = traffic_tbl.get("cases", {}).get(case, {}).get("bytes_per_cell", {}).get(dom)
     traffic = per_cell * n if per_cell is not None else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak,
@@ -442,7 +445,7 @@ def run_ours(args):
     out["clocks"] = sampler.summary()
 
     solver.close()
-    if not args.no_forms:
+    if not args.no_forms and cfg.eq != abi.KFVM_EQ_SRHYDRO:
         # the FP32 form (3xTF32 tensor-core reconstruction) and the learned + FP32
         # form (network trained untimed on a small grid of the same problem)
         fs = max(2, args.steps // 2)

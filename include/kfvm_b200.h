@@ -13,7 +13,8 @@
  * State exchange format ("SoA interior"): double[NV][nz][ny][nx], x fastest,
  * interior cells only (no halo).  nz == 1 in 2D.  The conserved-variable order
  * is the reference's (src/physics/SimVar.H:12-66):
- *   Euler / Navier-Stokes: dens, momx, momy, momz, etot            (NV = 5)
+ *   Euler / Navier-Stokes / SRHydro: dens, momx, momy, momz, etot  (NV = 5;
+ *                          SRHydro: D, Sx, Sy, Sz, E)
  *   GLM-MHD:               dens, momx, momy, momz, etot,
  *                          magx, magy, magz, psi                    (NV = 9)
  */
@@ -67,8 +68,11 @@ enum kfvm_ic {
   KFVM_IC_SMOOTH_WAVE = 5,       /* any dim/eq: smooth density/velocity wave     */
   KFVM_IC_SR_SHOCK_TUBE = 6,     /* SR hydro: rho,p = 10,40/3 for |x|<1/2 else 1,1e-6
                                     (exec/SRHydro/SRShockTube)                    */
-  KFVM_IC_SR_RIEMANN_2D = 7      /* SR hydro 2D four-quadrant Riemann problem
+  KFVM_IC_SR_RIEMANN_2D = 7,     /* SR hydro 2D four-quadrant Riemann problem
                                     (exec/SRHydro/SRRiem2d)                       */
+  KFVM_IC_STIR_TURB = 8          /* gas at rest, rho = 1, p = 1/gamma (GLM-MHD:
+                                    plus bx = sqrt(2p/beta), user:beta 0.1), for
+                                    random forcing (exec/{Hydro,NavierStokes,MHD}/StirTurb) */
 };
 
 /* ---- error codes -------------------------------------------------------- */
@@ -366,6 +370,42 @@ int kfvm_get_stream(kfvm_solver *s, void **stream);
 int kfvm_set_timing(kfvm_solver *s, int32_t on);
 int kfvm_get_timing(kfvm_solver *s, double *ms_per_class, int64_t *launches_per_class);
 int kfvm_get_launch_count(kfvm_solver *s, int64_t *launches);
+
+/* ---- random forcing (stirred turbulence) ----
+ * The reference's ENABLE_RANDOM_FORCING path (src/ParameterStructs.H:20-74,
+ * src/ParameterStructs.cpp:41-88, src/physics/Common_K.H:645-784,
+ * src/Solver.cpp:99-103, 365-409).  Modes: the wavevectors k of the half space with
+ * 0 < |k|^2 <= 9 (14 in 2D, 57 in 3D) in the reference's order; per mode and
+ * direction a complex amplitude drawn as sigma N(0,1), sigma = sqrt(|k| (4 - |k|)).
+ * The kick f (a Helmholtz mix of the modes, weight `ratio` on the compressive part)
+ * is scaled so that it injects edot dt of kinetic energy into the domain, and is
+ * added to the momenta (rho f) and the total energy; the stored FSAL stage is kept,
+ * as in the reference.
+ * A mode table is double[n_modes][dim][3]: (k_d, real amplitude, imaginary
+ * amplitude) for each direction d. */
+#define KFVM_FORCING_MAX_MODES 57
+typedef struct kfvm_forcing {
+  double edot;   /* eos:forceedot, energy injection rate */
+  double ratio;  /* eos:forceratio, compressive-to-solenoidal weight */
+  double t_off;  /* eos:forcetoff, no forcing from this time on */
+  uint64_t seed; /* generator seed; the reference seeds each draw from std::random_device */
+} kfvm_forcing;
+
+/* number of forcing modes for dim (14 or 57), or KFVM_ERR_ARG */
+int kfvm_forcing_num_modes(int32_t dim);
+/* One draw of the mode table (EosParameters::updateForcing with its generator,
+ * std::mt19937 + std::normal_distribution, seeded by seed32): host only. */
+int kfvm_forcing_draw(int32_t dim, uint32_t seed32, double *modes);
+/* Enables forcing on a solver (f NULL disables it).  kfvm_solve then forces before
+ * every step while time < t_off (Solver::Solve, Solver.cpp:99-103).  Allocates the
+ * solver's device mode table. */
+int kfvm_set_forcing(kfvm_solver *s, const kfvm_forcing *f);
+/* Solver::applyForcing: forces the current state once with the table modes_in, or
+ * (modes_in NULL) with the next draw of the solver's generator, at the current step
+ * size.  modes_out (optional) receives the table used, force_str (optional) the
+ * strength.  Synchronises the solver's stream (the strength needs the domain
+ * integrals). */
+int kfvm_apply_forcing(kfvm_solver *s, const double *modes_in, double *modes_out, double *force_str);
 
 /* Human-readable text for the last error on this thread. */
 const char *kfvm_last_error(void);

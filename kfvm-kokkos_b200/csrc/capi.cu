@@ -243,6 +243,12 @@ struct kfvm_solver {
   RKTable rk;
   double time = 0.0, dt = 0.0, errEst = 1.0;
   bool lastTimeStep = false, useSparseWeno = true, primed = false;
+  // random forcing (kfvm_set_forcing): parameters, draws so far, device mode table
+  // and integrals
+  bool forcing = false;
+  kfvm_forcing fpar{};
+  uint64_t fdraws = 0;
+  double *fmodes = nullptr, *fsums = nullptr;
   double plotFreq = 0.0; // plot times for the step-size limit (kfvm_set_plot_freq)
   int32_t plotNum = 0;
   bool writePlot = false;
@@ -815,7 +821,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
     s->heavyBlocks = (nsm > 0 ? nsm : 148) * 4; // grid-stride over the device-side count
   }
   {
-    const int64_t nb = std::max(stage_blocks(g), errest_blocks(g.n));
+    const int64_t nb = std::max(std::max(stage_blocks(g), errest_blocks(g.n)), forcing_blocks(g));
     if ((e = dalloc((void **)&s->part, 2 * nb * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
   }
   if ((e = dalloc((void **)&s->sc, sizeof(DevScalars))) != cudaSuccess) return cleanup(e, "alloc");
@@ -856,6 +862,8 @@ void kfvm_destroy(kfvm_solver *s) {
   cudaFree(s->applied);
   cudaFree(s->heavy);
   cudaFree(s->part);
+  cudaFree(s->fmodes);
+  cudaFree(s->fsums);
   cudaFree(s->sc);
   if (s->hsc) cudaFreeHost(s->hsc);
   cudaFree(s->mlp.wb);
@@ -884,7 +892,7 @@ void kfvm_destroy(kfvm_solver *s) {
 
 int kfvm_init_ic(kfvm_solver *s, int32_t ic_kind, uint64_t seed) {
   if (!s) return fail(KFVM_ERR_ARG, "null solver");
-  if (ic_kind < 0 || ic_kind > KFVM_IC_SR_RIEMANN_2D) return fail(KFVM_ERR_ARG, "unknown initial condition");
+  if (ic_kind < 0 || ic_kind > KFVM_IC_STIR_TURB) return fail(KFVM_ERR_ARG, "unknown initial condition");
   cudaError_t e = run(s, KFVM_KCLASS_OTHER, 1, [&] {
     return kfvm::launch_ic(s->dim, s->eq, ic_kind, seed, s->cfg, s->Ub[s->iPrev], s->g, s->stream);
   });
@@ -950,6 +958,11 @@ int kfvm_solve(kfvm_solver *s, int32_t max_steps, int64_t *n_steps_out, kfvm_ste
   std::memset(&info, 0, sizeof(info));
   int64_t acc = 0;
   for (; s->nTS < max_steps && !s->lastTimeStep; ++s->nTS) {
+    // Solver::Solve (Solver.cpp:99-103): force before the step while time < t_off
+    if (s->forcing && s->time < s->fpar.t_off) {
+      int rc = kfvm_apply_forcing(s, nullptr, nullptr, nullptr);
+      if (rc) return rc;
+    }
     int rc = take_step(s, &info);
     if (rc) return rc;
     acc += info.accepted;
@@ -1370,6 +1383,75 @@ int kfvm_restart(kfvm_solver *s, const char *xmf_path, int32_t *time_step) {
   s->dt = h;
   s->nTS = ts + 1;
   *time_step = ts;
+  return KFVM_OK;
+}
+
+int kfvm_forcing_num_modes(int32_t dim) {
+  const int n = kfvm::forcing_num_modes(dim);
+  return n < 0 ? fail(KFVM_ERR_ARG, "dim must be 2 or 3") : n;
+}
+
+int kfvm_forcing_draw(int32_t dim, uint32_t seed32, double *modes) {
+  if (!modes) return fail(KFVM_ERR_ARG, "null argument");
+  if (dim != 2 && dim != 3) return fail(KFVM_ERR_ARG, "dim must be 2 or 3");
+  kfvm::forcing_draw(dim, seed32, modes);
+  return KFVM_OK;
+}
+
+int kfvm_set_forcing(kfvm_solver *s, const kfvm_forcing *f) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (!f) {
+    s->forcing = false;
+    return KFVM_OK;
+  }
+  if (s->eq == KFVM_EQ_SRHYDRO) return fail(KFVM_ERR_ARG, "random forcing acts on Newtonian momenta (Hydro, NS, GLM-MHD)");
+  if (!(f->edot >= 0.0) || !std::isfinite(f->ratio)) return fail(KFVM_ERR_ARG, "forcing: edot >= 0 and a finite ratio");
+  if (!s->fmodes) {
+    CK(cudaMalloc((void **)&s->fmodes, KFVM_FORCING_MAX_MODES * 3 * 3 * sizeof(double)));
+    CK(cudaMalloc((void **)&s->fsums, 2 * sizeof(double)));
+  }
+  s->fpar = *f;
+  s->fdraws = 0;
+  s->forcing = true;
+  return KFVM_OK;
+}
+
+int kfvm_apply_forcing(kfvm_solver *s, const double *modes_in, double *modes_out, double *force_str) {
+  using namespace kfvm;
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (!s->forcing || !s->fmodes) return fail(KFVM_ERR_STATE, "forcing not enabled (kfvm_set_forcing)");
+  if (!s->primed) return fail(KFVM_ERR_STATE, "no state yet (kfvm_init_ic / kfvm_set_state / kfvm_restart)");
+  const int nm = forcing_num_modes(s->dim);
+  std::vector<double> m((size_t)nm * s->dim * 3);
+  if (modes_in) {
+    std::copy(modes_in, modes_in + m.size(), m.begin());
+  } else {
+    // a fresh generator per draw, as updateForcing makes one per call; its seed from
+    // the solver's seed and the draw count (SplitMix64 finaliser)
+    uint64_t x = s->fpar.seed + 0x9E3779B97F4A7C15ull * (++s->fdraws);
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    forcing_draw(s->dim, (uint32_t)(x >> 32), m.data());
+  }
+  const double lo[3] = {s->cfg.xlo, s->cfg.ylo, s->cfg.zlo};
+  double *U = s->Ub[s->iCur];
+  CK(cudaMemcpyAsync(s->fmodes, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(launch_forcing_integrate(s->dim, U, s->g, s->fmodes, nm, s->fpar.ratio, lo, s->part, s->fsums, s->stream));
+  s->launches += 2;
+  double ab[2];
+  CK(cudaMemcpyAsync(ab, s->fsums, sizeof(ab), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  // Solver::forceStrComm (Solver.cpp:395-409): the root of A s^2 + B s + C = 0 with
+  // C = -edot dt / dvol
+  const double dvol = s->dim == 2 ? s->g.dx * s->g.dy : s->g.dx * s->g.dy * s->g.dz;
+  const double A = ab[0], B = ab[1], C = -s->fpar.edot * s->dt / dvol;
+  const double str = (-B + std::sqrt(std::fmax(0.0, B * B - 4.0 * A * C))) / (2.0 * A);
+  CK(launch_forcing_apply(s->dim, U, s->g, s->fmodes, nm, s->fpar.ratio, str, lo, s->stream));
+  s->launches += 1;
+  CK(cudaStreamSynchronize(s->stream));
+  if (modes_out) std::copy(m.begin(), m.end(), modes_out);
+  if (force_str) *force_str = str;
   return KFVM_OK;
 }
 

@@ -121,6 +121,19 @@ __device__ void ic_point(const IcParams &p, double x, double y, double z, double
     s[ETOT] = rho * W * W * h - pr;
     break;
   }
+  case KFVM_IC_STIR_TURB: {
+    // exec/{Hydro,NavierStokes,MHD}/StirTurb: at rest with unit sound speed; GLM-MHD
+    // adds a uniform bx of plasma beta 0.1 (user:beta, read through std::stof)
+    const double pr = 1.0 / g;
+    s[DENS] = 1.0;
+    s[ETOT] = pr / gm;
+    if (p.eq == KFVM_EQ_MHD_GLM) {
+      const double bx = sqrt(2.0 * pr / (double)0.1f);
+      s[ETOT] += 0.5 * bx * bx;
+      s[MAGX] = bx;
+    }
+    break;
+  }
   default: { // KFVM_IC_SMOOTH_WAVE: periodic smooth flow on the box
     const double X = 2.0 * pi * (x - p.xlo) / (p.xup - p.xlo);
     const double Y = 2.0 * pi * (y - p.ylo) / (p.yup - p.ylo);

@@ -97,6 +97,16 @@ cudaError_t launch_ic(int dim, int eq, int ic_kind, uint64_t seed, const kfvm_co
 // error estimate of a state pair: block partials into part (2 per block of 256
 // cells), fixed-order sum into out[0] (err) and out[1] (positivity minimum)
 int64_t errest_blocks(int64_t n);
+
+// random forcing (forcing.cu): mode table on the host, integrals and kick on the device
+int forcing_num_modes(int dim);
+void forcing_draw(int dim, uint32_t seed32, double *modes);
+int64_t forcing_blocks(const Grid &g);
+cudaError_t launch_forcing_integrate(int dim, const double *U, const Grid &g, const double *modes, int nm,
+                                     double ratio, const double lo[3], double *part, double *sums,
+                                     cudaStream_t s);
+cudaError_t launch_forcing_apply(int dim, double *U, const Grid &g, const double *modes, int nm, double ratio,
+                                 double str, const double lo[3], cudaStream_t s);
 cudaError_t launch_errest(int eq, const double *u, const double *uhat, int64_t n, double atol,
                           double rtol, double *part, double *out, cudaStream_t s);
 

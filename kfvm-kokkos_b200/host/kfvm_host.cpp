@@ -58,6 +58,8 @@ bool ProblemSetup::setFromFile(const std::string &path) {
   }
   if (cfg.dim == 2) cfg.nz = 1;
   if (cfg.eq == KFVM_EQ_MHD_GLM) cfg.have_sources = 1; // ProblemSetup.H:81
+  if (forcing && !forceTOffSet)
+    warnings.push_back("setup:forcing on without eos:forcetoff: no step is forced (forcetoff = 0)");
   return true;
 }
 
@@ -119,6 +121,12 @@ bool ProblemSetup::setEos(const std::string &setting) {
   else if (k == "reynolds") cfg.reynolds = rf(v);
   else if (k == "prandtl") cfg.prandtl = rf(v);
   else if (k == "wenothresh") cfg.weno_thresh = rf(v);
+  else if (k == "forceedot") force.edot = rf(v);
+  else if (k == "forceratio") force.ratio = rf(v);
+  else if (k == "forcetoff") {
+    force.t_off = rf(v);
+    forceTOffSet = true;
+  } else if (k == "forcestr") (void)rf(v); // computed every step, the value read is not used
   else return false;
   return true;
 }
@@ -187,9 +195,15 @@ bool ProblemSetup::setSetup(const std::string &setting) {
     else if (v == "smooth_wave") ic = KFVM_IC_SMOOTH_WAVE;
     else if (v == "sr_shock_tube") ic = KFVM_IC_SR_SHOCK_TUBE;
     else if (v == "sr_riemann_2d") ic = KFVM_IC_SR_RIEMANN_2D;
+    else if (v == "stir_turb") ic = KFVM_IC_STIR_TURB;
+    else return false;
+  } else if (k == "forcing") {
+    if (v == "on") forcing = true;
+    else if (v == "off") forcing = false;
     else return false;
   } else if (k == "seed") {
     seed = (uint64_t)std::stoull(v);
+    force.seed = seed;
   } else if (k == "indicator") {
     if (v == "kxrcf") cfg.indicator = KFVM_IND_KXRCF;
     else if (v == "all") cfg.indicator = KFVM_IND_ALL;
@@ -210,13 +224,15 @@ std::string ProblemSetup::toJson() const {
                 "\"prandtl\": %.17g, \"weno_thresh\": %.17g, \"lfac\": %.17g, \"cfl\": %.17g, \"atol\": "
                 "%.17g, \"rtol\": %.17g, \"rejection_thresh\": %.17g, \"min_dt\": %.17g, \"final_time\": "
                 "%.17g, \"rejection_limit\": %d, \"max_steps\": %d, \"have_sources\": %d, \"ic\": %d, "
-                "\"seed\": %llu, \"warnings\": %d, \"plot_freq\": %.17g, \"ckpt_freq\": %d, \"restart\": %d}",
+                "\"seed\": %llu, \"warnings\": %d, \"plot_freq\": %.17g, \"ckpt_freq\": %d, \"restart\": %d, "
+                "\"forcing\": %d, \"force_edot\": %.17g, \"force_ratio\": %.17g, \"force_t_off\": %.17g}",
                 cfg.dim, cfg.eq, cfg.rs, cfg.rk, cfg.nq, cfg.indicator, (long long)cfg.nx,
                 (long long)cfg.ny, (long long)cfg.nz, cfg.xlo, cfg.xup, cfg.ylo, cfg.yup, cfg.zlo, cfg.zup,
                 cfg.bc[0], cfg.bc[1], cfg.bc[2], cfg.bc[3], cfg.bc[4], cfg.bc[5], cfg.gamma, cfg.reynolds,
                 cfg.prandtl, cfg.weno_thresh, cfg.lfac, cfg.cfl, cfg.atol, cfg.rtol, cfg.rejection_thresh,
                 cfg.min_dt, cfg.final_time, cfg.rejection_limit, cfg.max_steps, cfg.have_sources, ic,
-                (unsigned long long)seed, (int)warnings.size(), plotFreq, ckptFreq, restart ? 1 : 0);
+                (unsigned long long)seed, (int)warnings.size(), plotFreq, ckptFreq, restart ? 1 : 0, forcing ? 1 : 0,
+                force.edot, force.ratio, force.t_off);
   return b;
 }
 
@@ -236,6 +252,7 @@ Solver::Solver(const ProblemSetup &ps) : ps_(ps) {
     check(kfvm_restart(s_, ps.restartFile.c_str(), &step), "kfvm_restart");
     nTS_ = step + 1;
   }
+  if (ps.forcing) check(kfvm_set_forcing(s_, &ps.force), "kfvm_set_forcing");
   check(kfvm_get_time(s_, &time_, &dt_), "kfvm_get_time");
   if (ps.restart && ps.plotFreq > 0.0) plotNum_ = static_cast<int>(std::ceil(time_ / ps.plotFreq));
   check(kfvm_set_plot_freq(s_, ps.plotFreq, plotNum_), "kfvm_set_plot_freq");
@@ -288,6 +305,8 @@ void Solver::Solve() {
   const int maxSteps = ps_.cfg.max_steps;
   for (; nTS_ < maxSteps && !lastTimeStep_; ++nTS_) {
     if (ps_.verbose > 0) std::printf("Step %d: time = %.4g\n", nTS_, time_);
+    // random forcing before the step while time < forcetoff (Solver.cpp:99-103)
+    if (ps_.forcing && time_ < ps_.force.t_off) check(kfvm_apply_forcing(s_, nullptr, nullptr, nullptr), "kfvm_apply_forcing");
     TakeStep();
     if (ps_.plotFreq > 0.0 && (info_.write_plot || lastTimeStep_ || nTS_ == maxSteps - 1)) {
       writePlot();

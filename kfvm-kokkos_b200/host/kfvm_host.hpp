@@ -24,6 +24,10 @@ struct ProblemSetup {
   int ckptFreq = 0;
   std::string restartFile;
   bool restart = false;
+  // random forcing (ENABLE_RANDOM_FORCING of the reference's Definitions.H as
+  // setup:forcing on; eos:forceedot / forceratio / forcetoff, ParameterStructs.cpp:15-38)
+  bool forcing = false, forceTOffSet = false;
+  kfvm_forcing force{2.0, 1.0, 0.0, 12345};
   int verbose = 0;
   bool dumpState = false;
   std::vector<std::string> warnings;

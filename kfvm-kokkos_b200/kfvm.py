@@ -78,6 +78,10 @@ def lib():
         L.kfvm_set_timing.argtypes = [P, I32]
         L.kfvm_get_timing.argtypes = [P, P, P]
         L.kfvm_get_launch_count.argtypes = [P, C.POINTER(I64)]
+        L.kfvm_forcing_num_modes.argtypes = [I32]
+        L.kfvm_forcing_draw.argtypes = [I32, C.c_uint32, P]
+        L.kfvm_set_forcing.argtypes = [P, C.POINTER(abi.KfvmForcing)]
+        L.kfvm_apply_forcing.argtypes = [P, P, P, P]
         L.kfvm_last_error.restype = C.c_char_p
         _LIB = L
     return _LIB
@@ -109,6 +113,20 @@ def selftest_rcp(n=1 << 24, seed=5):
     u, q = C.c_int64(), C.c_double()
     _check(lib().kfvm_selftest_rcp(int(n), int(seed), C.byref(u), C.byref(q)), "kfvm_selftest_rcp")
     return u.value, q.value
+
+
+def forcing_num_modes(dim):
+    n = lib().kfvm_forcing_num_modes(int(dim))
+    if n < 0:
+        _check(n, "kfvm_forcing_num_modes")
+    return n
+
+
+def forcing_draw(dim, seed32):
+    """kfvm_forcing_draw: one mode table [n][dim][3] = (k_d, real, imaginary)."""
+    m = np.empty((forcing_num_modes(dim), dim, 3), dtype=np.float64)
+    _check(lib().kfvm_forcing_draw(int(dim), int(seed32) & 0xFFFFFFFF, m.ctypes.data), "kfvm_forcing_draw")
+    return m
 
 
 def plotfile_write(cfg, directory, base, num, u, weno, theta, time=0.0, time_step=0, dt=0.0, ckpt=False):
@@ -291,6 +309,22 @@ class Solver:
         ts = C.c_int32()
         _check(lib().kfvm_restart(self.h, str(xmf_path).encode(), C.byref(ts)), "kfvm_restart")
         return ts.value
+
+    def set_forcing(self, forcing):
+        """kfvm_set_forcing with an abi.KfvmForcing (None disables)."""
+        _check(lib().kfvm_set_forcing(self.h, C.byref(forcing) if forcing is not None else None),
+               "kfvm_set_forcing")
+
+    def apply_forcing(self, modes=None):
+        """kfvm_apply_forcing: force the current state once (a new draw when modes is
+        None); returns (mode table used, strength)."""
+        dim = self.cfg.dim
+        out = np.empty((forcing_num_modes(dim), dim, 3), dtype=np.float64)
+        mi = None if modes is None else np.ascontiguousarray(modes, dtype=np.float64)
+        s = C.c_double()
+        _check(lib().kfvm_apply_forcing(self.h, None if mi is None else mi.ctypes.data, out.ctypes.data,
+                                        C.byref(s)), "kfvm_apply_forcing")
+        return out, s.value
 
     def set_plot_freq(self, plot_freq, plot_num):
         _check(lib().kfvm_set_plot_freq(self.h, float(plot_freq), int(plot_num)), "kfvm_set_plot_freq")

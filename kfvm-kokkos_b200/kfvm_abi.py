@@ -17,7 +17,8 @@ KFVM_IND_KXRCF, KFVM_IND_ALL, KFVM_IND_NONE, KFVM_IND_MLP = 0, 1, 2, 3
 KFVM_PREC_FP64, KFVM_PREC_TF32X3 = 0, 1
 (KFVM_IC_ISENTROPIC_VORTEX, KFVM_IC_SPHERICAL_SOD, KFVM_IC_KELVIN_HELMHOLTZ,
  KFVM_IC_TAYLOR_GREEN, KFVM_IC_ORSZAG_TANG, KFVM_IC_SMOOTH_WAVE,
- KFVM_IC_SR_SHOCK_TUBE, KFVM_IC_SR_RIEMANN_2D) = range(8)
+ KFVM_IC_SR_SHOCK_TUBE, KFVM_IC_SR_RIEMANN_2D, KFVM_IC_STIR_TURB) = range(9)
+KFVM_FORCING_MAX_MODES = 57
 
 KFVM_MAX_CELLS, KFVM_MAX_SUB, KFVM_MAX_BIAS, KFVM_MAX_BCELLS = 33, 8, 6, 11
 KFVM_MAX_INDIC, KFVM_MAX_FACEQ, KFVM_MAX_CELLQ = 19, 9, 27
@@ -53,6 +54,10 @@ class KfvmStencil(C.Structure):
         ("cell_w", ((C.c_double * KFVM_MAX_CELLS) * KFVM_MAX_CELLQ) * KFVM_MAX_SUB),
         ("deriv_w", ((C.c_double * KFVM_MAX_CELLS) * KFVM_MAX_INDIC) * KFVM_MAX_SUB),
     ]
+
+
+class KfvmForcing(C.Structure):
+    _fields_ = [("edot", C.c_double), ("ratio", C.c_double), ("t_off", C.c_double), ("seed", C.c_uint64)]
 
 
 class KfvmStepInfo(C.Structure):
@@ -160,7 +165,19 @@ def workload(name, scale=None, steps=None):
                         gamma=1.66666666666666, rs=KFVM_RS_LLF, cfl=1.0, steps=steps or 200,
                         atol=1e-3, rtol=1e-3)
         return c, KFVM_IC_SR_RIEMANN_2D
+    # randomly forced turbulence (exec/Hydro/StirTurb/stirturb3d.init; forcing
+    # parameters: eos:forceedot 60, forceratio 1, forcetoff 1.5)
+    if name == "stir_turb":
+        n = scale or 128
+        c = make_config(3, KFVM_EQ_HYDRO, n, n, n, extent=(0, 1, 0, 1, 0, 1), gamma=1.001, rs=KFVM_RS_HLL,
+                        cfl=1.25, weno_thresh=-1.0, steps=steps or 100, atol=1e-3, rtol=1e-3)
+        return c, KFVM_IC_STIR_TURB
     raise ValueError(name)
+
+
+def stir_turb_forcing(seed=1):
+    """eos:forceedot 60, eos:forceratio 1, eos:forcetoff 1.5 of stirturb3d.init (stof-rounded)."""
+    return KfvmForcing(stof(60.0), stof(1.0), stof(1.5), seed)
 
 
 def nvars(cfg):

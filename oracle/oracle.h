@@ -30,6 +30,9 @@ int orc_take_step(orc_solver *s, kfvm_step_info *info);
 int orc_solve(orc_solver *s, int32_t max_steps, int64_t *n_steps, kfvm_step_info *last);
 int orc_get_time(orc_solver *s, double *time, double *dt);
 int orc_set_time(orc_solver *s, double time, double dt);
+/* Random forcing with a given mode table (n_modes x dim x 3). */
+int orc_apply_forcing(orc_solver *s, const double *modes, int32_t n_modes, double edot, double ratio,
+                      double *force_str);
 /* Keep a copy of the face states before the Riemann solve for orc_get_faces. */
 int orc_keep_faces(orc_solver *s, int32_t on);
 int orc_get_faces(orc_solver *s, int32_t dir, double *out);

@@ -48,6 +48,7 @@ def lib():
         L.orc_solve.argtypes = [P, I32, C.POINTER(I64), C.POINTER(abi.KfvmStepInfo)]
         L.orc_get_time.argtypes = [P, P, P]
         L.orc_set_time.argtypes = [P, D, D]
+        L.orc_apply_forcing.argtypes = [P, P, I32, D, D, P]
         L.orc_get_faces.argtypes = [P, I32, P]
         L.orc_keep_faces.argtypes = [P, I32]
         L.orc_get_flags.argtypes = [P, P, P]
@@ -145,6 +146,14 @@ class OracleSolver:
         t, dt = C.c_double(), C.c_double()
         lib().orc_get_time(self.h, C.addressof(t), C.addressof(dt))
         return t.value, dt.value
+
+    def apply_forcing(self, modes, edot, ratio):
+        """Random forcing with the given mode table [n][dim][3]; returns the strength."""
+        m = np.ascontiguousarray(modes, dtype=np.float64)
+        s = C.c_double()
+        assert lib().orc_apply_forcing(self.h, m.ctypes.data, m.shape[0], float(edot), float(ratio),
+                                       C.addressof(s)) == 0
+        return s.value
 
     def set_time(self, t, dt):
         assert lib().orc_set_time(self.h, float(t), float(dt)) == 0

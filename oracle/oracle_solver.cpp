@@ -695,6 +695,18 @@ void ic_point(int kind, const kfvm_config &c, double x, double y, double z, doub
     s[ETOT] = rho * W * W * h - p;
     break;
   }
+  case KFVM_IC_STIR_TURB: {
+    // exec/{Hydro,NavierStokes,MHD}/StirTurb/InitialCondition.H (user:beta 0.1)
+    const double p = 1.0 / c.gamma;
+    s[DENS] = 1.0;
+    s[ETOT] = p / gm;
+    if (c.eq == KFVM_EQ_MHD_GLM) {
+      const double bx = sqrt(2.0 * p / (double)0.1f);
+      s[ETOT] += 0.5 * bx * bx;
+      s[MAGX] = bx;
+    }
+    break;
+  }
   default: { // KFVM_IC_SMOOTH_WAVE
     const double X = 2.0 * M_PI * (x - c.xlo) / (c.xup - c.xlo);
     const double Y = 2.0 * M_PI * (y - c.ylo) / (c.yup - c.ylo);
@@ -1980,6 +1992,70 @@ int orc_solve(orc_solver *s, int32_t max_steps, int64_t *n_steps, kfvm_step_info
   }
   if (n_steps) *n_steps = acc;
   if (last) *last = info;
+  return 0;
+}
+
+// Solver::applyForcing with a given mode table (Solver.cpp:365-409,
+// RandForcingIntegrate_K / RandForcingApply_K, Common_K.H:645-784): domain integrals
+// in cell order, the strength that injects edot dt, the kick on U, Uprev = U.
+// modes: [n][dim][3] = (k_d, real, imaginary); n = 14 (2D) or 57 (3D).
+int orc_apply_forcing(orc_solver *s, const double *modes, int32_t n_modes, double edot, double ratio,
+                      double *force_str) {
+  if (!s || !modes || n_modes <= 0) return KFVM_ERR_ARG;
+  orc_solver &S = *s;
+  const int dim = S.dim;
+  const double fr = ratio, mfr = 1.0 - 2.0 * fr;
+  auto force = [&](int64_t i, int64_t j, int64_t k, double str, bool scaled, double &fu, double &fv,
+                   double &fw) {
+    fu = fv = fw = 0.0;
+    const double x = S.dx * (double(i) + 0.5) + S.cfg.xlo, y = S.dy * (double(j) + 0.5) + S.cfg.ylo;
+    const double z = dim == 2 ? S.dz * 0.5 + S.cfg.zlo : S.dz * (double(k) + 0.5) + S.cfg.zlo;
+    for (int n = 0; n < n_modes; n++) {
+      auto A = [&](int d, int c) { return modes[((size_t)n * dim + d) * 3 + c]; };
+      const double k1 = A(0, 0), k2 = A(1, 0), k3 = dim == 3 ? A(2, 0) : 0.0;
+      const double kdx = k1 * x + k2 * y + k3 * z;
+      const double cs = std::cos(2.0 * M_PI * kdx), sn = std::sin(2.0 * M_PI * kdx);
+      const double fun = A(0, 1) * cs - A(0, 2) * sn;
+      const double fvn = A(1, 1) * cs - A(1, 2) * sn;
+      const double fwn = dim == 3 ? A(2, 1) * cs - A(2, 2) * sn : 0.0;
+      const double ksq = k1 * k1 + k2 * k2 + k3 * k3, iksq = 1.0 / ksq;
+      const double du = (fr + mfr * iksq * k1 * k1) * fun + mfr * iksq * (k1 * k2 * fvn + k1 * k3 * fwn);
+      const double dv = (fr + mfr * iksq * k2 * k2) * fvn + mfr * iksq * (k1 * k2 * fun + k2 * k3 * fwn);
+      const double dw = (fr + mfr * iksq * k3 * k3) * fwn + mfr * iksq * (k1 * k3 * fun + k2 * k3 * fvn);
+      fu += scaled ? str * du : du;
+      fv += scaled ? str * dv : dv;
+      fw += scaled ? str * dw : dw;
+    }
+  };
+  double intA = 0.0, intB = 0.0;
+  for (int64_t k = 0; k < S.nz; k++)
+    for (int64_t j = 0; j < S.ny; j++)
+      for (int64_t i = 0; i < S.nx; i++) {
+        double fu, fv, fw;
+        force(i, j, k, 1.0, false, fu, fv, fw);
+        const double rho = S.U[S.ui(i, j, k, DENS)];
+        intA += 0.5 * rho * (fu * fu + fv * fv + fw * fw);
+        intB += S.U[S.ui(i, j, k, MOMX)] * fu + S.U[S.ui(i, j, k, MOMY)] * fv + S.U[S.ui(i, j, k, MOMZ)] * fw;
+      }
+  const double dvol = dim == 2 ? S.dx * S.dy : S.dx * S.dy * S.dz;
+  const double A = intA, B = intB, C = -edot * S.dt / dvol;
+  const double str = (-B + std::sqrt(std::fmax(0.0, B * B - 4.0 * A * C))) / (2.0 * A);
+  for (int64_t k = 0; k < S.nz; k++)
+    for (int64_t j = 0; j < S.ny; j++)
+      for (int64_t i = 0; i < S.nx; i++) {
+        double fu, fv, fw;
+        force(i, j, k, str, true, fu, fv, fw);
+        const double rho = S.U[S.ui(i, j, k, DENS)];
+        double &mx = S.U[S.ui(i, j, k, MOMX)], &my = S.U[S.ui(i, j, k, MOMY)], &mz = S.U[S.ui(i, j, k, MOMZ)];
+        double ePert = 0.5 * rho * (fu * fu + fv * fv + fw * fw);
+        ePert += mx * fu + my * fv + mz * fw;
+        mx += rho * fu;
+        my += rho * fv;
+        mz += rho * fw;
+        S.U[S.ui(i, j, k, ETOT)] += ePert;
+      }
+  S.Uprev = S.U;
+  if (force_str) *force_str = str;
   return 0;
 }
 
