@@ -243,6 +243,11 @@ struct kfvm_solver {
   RKTable rk;
   double time = 0.0, dt = 0.0, errEst = 1.0;
   bool lastTimeStep = false, useSparseWeno = true, primed = false;
+  // equal-state Riemann variant (Euler / Navier-Stokes): on while at least a quarter
+  // of its sampled faces qualify; when off, probed again after kSameProbeSteps steps
+  bool sameOn = true;
+  int sameProbe = 0;
+  unsigned long long sameSeen = 0, sampSeen = 0;
   // random forcing (kfvm_set_forcing): parameters, draws so far, device mode table
   // and integrals
   bool forcing = false;
@@ -353,6 +358,24 @@ void harvest(kfvm_solver *s) {
   s->marks.clear();
 }
 
+// Keeps the equal-state Riemann variant while at least a quarter of the faces it
+// samples qualify (where few do, its heavier general path costs a few per cent);
+// otherwise uses the plain variant and probes again after kSameProbeSteps steps.
+constexpr int kSameProbeSteps = 4;
+void update_same_mode(kfvm_solver *s) {
+  const unsigned long long dS = s->hsc->nsame - s->sameSeen, dN = s->hsc->nsamp - s->sampSeen;
+  s->sameSeen = s->hsc->nsame;
+  s->sampSeen = s->hsc->nsamp;
+  if (s->sameOn) {
+    if (dN > 0 && 4 * dS < dN) {
+      s->sameOn = false;
+      s->sameProbe = kSameProbeSteps;
+    }
+  } else if (--s->sameProbe <= 0) {
+    s->sameOn = true;
+  }
+}
+
 // the reference's wenothresh sign switch: a positive threshold allows the sparse
 // (selected-cells) WENO mode, for KXRCF and for the learned indicator alike
 bool sparse_allowed(const kfvm_solver *s) {
@@ -420,7 +443,8 @@ int eval_front(kfvm_solver *s, int b) {
                              mode == RECON_FULL ? nullptr : s->bnd, s->sc, jd, s->heavyBlocks, st);
        })) != cudaSuccess)
     return set_err_cuda(e, "heavy");
-  if ((e = run(s, KFVM_KCLASS_RIEMANN, dim, [&] { return launch_riemann(dim, eq, s->F, s->G, s->g, s->sc, st); })) !=
+  if ((e = run(s, KFVM_KCLASS_RIEMANN, dim,
+               [&] { return launch_riemann(dim, eq, s->F, s->G, s->g, s->sc, s->sameOn, st); })) !=
       cudaSuccess)
     return set_err_cuda(e, "riemann");
   return KFVM_OK;
@@ -552,6 +576,7 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
     if (s->hsc->fault) return fail(KFVM_ERR_CUDA, kFaultMsg);
     maxVel = bits_to_double(s->hsc->maxvel_bits);
     s->nWenoLast = s->hsc->napplied;
+    update_same_mode(s);
     const double nDofs = (double)(s->g.n * s->nv);
     const double posFlag = s->hsc->posmin;
     errNew = 1.0 / std::sqrt(s->hsc->err / nDofs);

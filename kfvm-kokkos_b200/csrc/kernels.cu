@@ -806,7 +806,13 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 // more warps hide the FP64 latency.  The quadrature-weighted sum over a face's
 // points goes through shared memory in point order, and the max wave speed
 // through a warp maximum and an atomic only from warps that raise it.
-template <int DIM, int EQ, int D, int NQ>
+// SAME: Euler / Navier-Stokes faces whose two states agree to kSameTol take the
+// consistent flux F(u) without the wave fan (Eos::solve_same); one block in
+// kSameSample counts such faces so that the host can fall back to the plain
+// variant where few faces qualify (its slow path spills more registers).
+constexpr int kSameSample = 1024;
+
+template <int DIM, int EQ, int D, int NQ, bool SAME>
 __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
                                   EQ == EQ_GLM ? 1 : (EQ == EQ_SR ? (DIM == 2 ? 8 : 4) : (DIM == 2 ? 16 : 8)))
     riemann_kernel(const double *__restrict__ F, double *__restrict__ G, Grid g,
@@ -822,6 +828,7 @@ __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
   const int q = threadIdx.y;
   double vmax = 0.0;
   const bool live = i < fx;
+  bool same = false;
   if (live) {
     const int64_t fidx = (k * fy + j) * fx + i;
     const int64_t m = D == 0 ? i : (D == 1 ? j : k);
@@ -858,13 +865,30 @@ __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
         if ((flipR >> v) & 1u) uR[v] = -uR[v];
       }
     }
-    vmax = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
+    if constexpr (SAME && (EQ == EQ_HYDRO || EQ == EQ_NS)) {
+      // a face inside a uniform region needs no wave fan (kSameTol)
+      same = E::same_state(uL, uR);
+      if (same) vmax = E::solve_same(g.gamma, D, uL, Fq);
+      else vmax = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
+    } else {
+      vmax = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
+    }
     // Gauss weight of point q (3D: the product of the two transverse weights)
     const double wq = DIM == 2 ? gl_wt<NQ>(q) : gl_wt<NQ>(q / NQ) * gl_wt<NQ>(q % NQ);
 #pragma unroll
     for (int v = 0; v < NV; v++) part[q][v][threadIdx.x] = wq * Fq[v];
   }
+  __shared__ unsigned cnt[2];
+  const bool sampled = SAME && (blockIdx.x + 5u * blockIdx.y + 11u * blockIdx.z) % kSameSample == 0;
+  if (sampled && threadIdx.x == 0 && q == 0) cnt[0] = cnt[1] = 0u;
   __syncthreads();
+  if (sampled) {
+    const unsigned bs = __ballot_sync(0xffffffffu, same), bl = __ballot_sync(0xffffffffu, live);
+    if (threadIdx.x == 0) {
+      atomicAdd(&cnt[0], (unsigned)__popc(bs));
+      atomicAdd(&cnt[1], (unsigned)__popc(bl));
+    }
+  }
   if (live && q == 0) {
     const int64_t fidx = (k * fy + j) * fx + i;
 #pragma unroll
@@ -877,6 +901,13 @@ __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
   }
   vmax = warp_max(vmax);
   if (threadIdx.x == 0) atomic_max_pos(&sc->maxvel_bits, vmax);
+  if (sampled) {
+    __syncthreads();
+    if (threadIdx.x == 0 && q == 0) {
+      atomicAdd(&sc->nsame, (unsigned long long)cnt[0]);
+      atomicAdd(&sc->nsamp, (unsigned long long)cnt[1]);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1380,16 +1411,27 @@ struct Launch {
         U, g, S, theta, F[0], F[1], F[2], src, heavy, bnd, sc, jd);
     return cudaGetLastError();
   }
-  static cudaError_t riemann(double *const *F, double *const *G, const Grid &g, DevScalars *sc,
-                             cudaStream_t s) {
+  template <bool SAME>
+  static void riemann_dirs(double *const *F, double *const *G, const Grid &g, DevScalars *sc, cudaStream_t s) {
 #pragma unroll 1
     for (int d = 0; d < DIM; d++) {
       // one block row of 32 faces per (j, k), NQF points along threadIdx.y
       const dim3 grid((unsigned)((g.fdim[d][0] + 31) / 32), (unsigned)g.fdim[d][1], (unsigned)g.fdim[d][2]);
       const dim3 blk(32, Cfg<DIM, EQ, NQ>::NQF);
-      if (d == 0) riemann_kernel<DIM, EQ, 0, NQ><<<grid, blk, 0, s>>>(F[0], G[0], g, sc);
-      if (d == 1) riemann_kernel<DIM, EQ, 1, NQ><<<grid, blk, 0, s>>>(F[1], G[1], g, sc);
-      if (DIM == 3 && d == 2) riemann_kernel<DIM, EQ, (DIM == 3 ? 2 : 1), NQ><<<grid, blk, 0, s>>>(F[2], G[2], g, sc);
+      if (d == 0) riemann_kernel<DIM, EQ, 0, NQ, SAME><<<grid, blk, 0, s>>>(F[0], G[0], g, sc);
+      if (d == 1) riemann_kernel<DIM, EQ, 1, NQ, SAME><<<grid, blk, 0, s>>>(F[1], G[1], g, sc);
+      if (DIM == 3 && d == 2)
+        riemann_kernel<DIM, EQ, (DIM == 3 ? 2 : 1), NQ, SAME><<<grid, blk, 0, s>>>(F[2], G[2], g, sc);
+    }
+  }
+  static cudaError_t riemann(double *const *F, double *const *G, const Grid &g, DevScalars *sc, bool same,
+                             cudaStream_t s) {
+    if constexpr (EQ == EQ_HYDRO || EQ == EQ_NS) {
+      if (same) riemann_dirs<true>(F, G, g, sc, s);
+      else riemann_dirs<false>(F, G, g, sc, s);
+    } else {
+      (void)same;
+      riemann_dirs<false>(F, G, g, sc, s);
     }
     return cudaGetLastError();
   }
@@ -1540,8 +1582,8 @@ cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const 
   KFVM_DISPATCH(dim, eq, heavy(U, g, S, theta, F, src, heavy, bnd, sc, jd, heavy_blocks, s));
 }
 cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
-                           DevScalars *sc, cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, riemann(F, G, g, sc, s));
+                           DevScalars *sc, bool same, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, riemann(F, G, g, sc, same, s));
 }
 cudaError_t launch_stage(int dim, int eq, const StageArgs &a, const Grid &g, cudaStream_t s) {
   KFVM_DISPATCH(dim, eq, stage(a, g, s));

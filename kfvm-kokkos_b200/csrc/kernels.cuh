@@ -86,6 +86,9 @@ struct DevScalars {
   // learned indicator's judge, cumulative: judged cells, of them labelled
   // troubled, troubled but not predicted (missed), predicted but not troubled
   unsigned long long mlp_judged, mlp_pos, mlp_missed, mlp_false;
+  // Riemann faces with equal states in the sampled blocks of the equal-state
+  // variant, and the faces sampled, cumulative
+  unsigned long long nsame, nsamp;
 };
 
 // heavy-list entries carry the cell index in the low 30 bits

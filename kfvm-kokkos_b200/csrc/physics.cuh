@@ -32,6 +32,13 @@ enum { RS_LLF = 0, RS_HLL = 1, RS_HLLC = 2 };
 // (<= 5.5e-6), i.e. <= 1.8e-5 x ln 2 = 1.2e-5 relative after ex2; ex2.approx
 // (2^-22) and the FP32 roundings of p and rho add < 4e-7.
 constexpr double kWenoApproxEps = 2e-5;
+// Two face states whose components differ by at most kSameTol x their largest
+// component are treated as one state by the Riemann kernel (Eos::same_state): every
+// solver here is consistent, F(u, u) = F(u), and differs from F(u) by about
+// (wave speed) x |uR - uL| for nearby states, so the flux changes by less than
+// 1e-14 of its scale.  The reconstruction of a uniform region leaves such
+// rounding-level differences between the two sides of a face.
+constexpr double kSameTol = 1e-14;
 // bound on the relative error of Eos::weno_round: one rounding to FP32 (2^-24)
 // plus a few FP64 ulps of the pressure, the power and the quotient
 constexpr double kWenoRoundEps = 6.0e-8;
@@ -57,8 +64,13 @@ struct Eos {
   // primitives: SR keeps the Lorentz factor after the pressure
   static constexpr int NVP = EQ == EQ_SR ? 6 : NV;
 
+  // kinetic energy; gas at rest (all momenta exactly 0, common in undisturbed
+  // regions) skips the division, whose zero-dividend case leaves the hardware's
+  // fast path: the value is the same +0 the quotient gives for a positive density
   __device__ __forceinline__ static double ekin(const double *U) {
-    return 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]) / U[DENS];
+    const double m2 = 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]);
+    if (m2 == 0.0 && U[DENS] > 0.0) return 0.0;
+    return m2 / U[DENS];
   }
   __device__ __forceinline__ static double prsb(const double *U) {
     return 0.5 * (U[MAGX] * U[MAGX] + U[MAGY] * U[MAGY] + U[MAGZ] * U[MAGZ]);
@@ -235,6 +247,32 @@ struct Eos {
     V[4] = (g - 1.0) * (U[ETOT] - 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]) * ir);
   }
 
+  // uL, uR equal to kSameTol (false when either holds a NaN)
+  __device__ __forceinline__ static bool same_state(const double *uL, const double *uR) {
+    double s = 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; v++) s = fmax(s, fabs(uL[v]));
+    bool same = true;
+#pragma unroll
+    for (int v = 0; v < NV; v++) same = same && fabs(uR[v] - uL[v]) <= kSameTol * s;
+    return same;
+  }
+
+  // Euler / Navier-Stokes face with equal states (kSameTol): the physical flux, and
+  // the speed bound max(|sL|, |sR|) = |u_n| + a that the Batten/Roe estimates give
+  // for equal states (Hydro_Riemann.H:41-81 with uTil = u, aTil = a)
+  __device__ __forceinline__ static double solve_same(double g, int dir, const double *u, double *F) {
+    static_assert(EQ == EQ_HYDRO || EQ == EQ_NS, "Euler / Navier-Stokes only");
+    const int ord[3] = {dir, (dir + 1) % 3, (dir + 2) % 3};
+    const int vo[3] = {MOMX + ord[0], MOMX + ord[1], MOMX + ord[2]};
+    const int bo[3] = {MAGX + ord[0], MAGX + ord[1], MAGX + ord[2]};
+    const double ir = 1.0 / u[DENS];
+    double V[NV];
+    cons2prim_r(g, u, ir, V);
+    flux(0.0, vo, bo, u, V, F);
+    return fabs(V[vo[0]]) + sqrt(g * V[4] * ir);
+  }
+
   // Riemann solve at one face point in direction dir; returns max(|sL|,|sR|).
   // Euler / Navier-Stokes: Batten/Roe speed estimates (Hydro_Riemann.H:26-80) and,
   // for HLLC, the low-Mach / shear-corrected star fluxes (Hydro_Riemann.H:82-187),
@@ -273,6 +311,7 @@ struct Eos {
       const double pL = vL[4], pR = vR[4];
       const double a2L = g * pL * iL, a2R = g * pR * iR;
       const double aL = sqrt(a2L), aR = sqrt(a2R);
+
       const double hL = (uL[ETOT] + pL) * iL, hR = (uR[ETOT] + pR) * iR;
       // Roe weights sqrt(rL) / (sqrt(rL) + sqrt(rR)) = 1 / (1 + sqrt(rR / rL)) and
       // sqrt(rR) / (...) = sqrt(rR / rL) / (1 + sqrt(rR / rL)): one root, one reciprocal
