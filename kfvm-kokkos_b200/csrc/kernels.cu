@@ -234,7 +234,10 @@ __global__ void __launch_bounds__(128)
             if constexpr (EQ == EQ_SR) {
               inside = inside && pos_inside<EQ>(bd, st);
             } else {
-              ei = Eos<EQ>::eint(st);
+              // Euler / Navier-Stokes: without the IEEE division (GLM-MHD, whose
+              // kernel it slowed, keeps the plain expression)
+              if constexpr (EQ == EQ_GLM) ei = Eos<EQ>::eint(st);
+              else ei = Eos<EQ>::eint_vs(st, bd.minEint);
               inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
             }
             if (rw < T::NF * T::NQF) {

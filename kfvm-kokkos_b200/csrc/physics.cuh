@@ -82,6 +82,20 @@ struct Eos {
       return (U[ETOT] - ekin(U));
     }
   }
+  // Internal energy for a comparison with the bound b: the kinetic energy by the
+  // Newton-refined reciprocal (within 2 ulp of the quotient), and the exact
+  // expression wherever the approximate value lies within 2^-50 (|ke| + |eint|)
+  // of b, so that eint > b is decided as the exact expression decides it.
+  // Non-finite or non-positive densities fall through to the exact expression.
+  __device__ __forceinline__ static double eint_vs(const double *U, double b) {
+    const double m2 = 0.5 * (U[MOMX] * U[MOMX] + U[MOMY] * U[MOMY] + U[MOMZ] * U[MOMZ]);
+    const double ke = m2 * rcp_nr(U[DENS]);
+    double ei;
+    if constexpr (EQ == EQ_GLM) ei = U[ETOT] - prsb(U) - ke - 0.5 * U[PSI] * U[PSI];
+    else ei = U[ETOT] - ke;
+    if (!(fabs(ei - b) > 8.9e-16 * (fabs(ke) + fabs(ei)) + 1e-300) || !(U[DENS] > 0.0)) ei = eint(U);
+    return ei;
+  }
   // internal energy with the reciprocal density given (one division shared by
   // the quantities of a state)
   __device__ __forceinline__ static double eint_r(const double *U, double ir) {
