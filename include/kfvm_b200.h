@@ -407,6 +407,15 @@ int kfvm_set_forcing(kfvm_solver *s, const kfvm_forcing *f);
  * integrals). */
 int kfvm_apply_forcing(kfvm_solver *s, const double *modes_in, double *modes_out, double *force_str);
 
+/* Solver::evalFlowStats (src/Solver.cpp:153-185; FlowStats<Eq>, src/physics/hydro/
+ * Hydro_K.H:103-178, navierstokes/NavierStokes_K.H:102-175, mhd_glm/MHD_GLM_K.H:108-211):
+ * volume averages of the current state's kinetic energy and enstrophy (velocity
+ * gradients by central differences over the boundary-filled halo), and for
+ * GLM-MHD the current helicity B . curl B.  stats receives n_stats values (2; GLM-MHD
+ * 3; SRHydro 1, always 0 as in the reference), n_stats may be NULL.  Synchronises
+ * the solver's stream. */
+int kfvm_flow_stats(kfvm_solver *s, double *stats, int32_t *n_stats);
+
 /* Human-readable text for the last error on this thread. */
 const char *kfvm_last_error(void);
 

@@ -254,6 +254,8 @@ struct kfvm_solver {
   kfvm_forcing fpar{};
   uint64_t fdraws = 0;
   double *fmodes = nullptr, *fsums = nullptr;
+  // flow statistics: block partials and the three sums
+  double *spart = nullptr, *ssum = nullptr;
   double plotFreq = 0.0; // plot times for the step-size limit (kfvm_set_plot_freq)
   int32_t plotNum = 0;
   bool writePlot = false;
@@ -849,6 +851,8 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
     const int64_t nb = std::max(std::max(stage_blocks(g), errest_blocks(g.n)), forcing_blocks(g));
     if ((e = dalloc((void **)&s->part, 2 * nb * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
   }
+  if ((e = dalloc((void **)&s->spart, 3 * stats_blocks(g) * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
+  if ((e = dalloc((void **)&s->ssum, 3 * sizeof(double))) != cudaSuccess) return cleanup(e, "alloc");
   if ((e = dalloc((void **)&s->sc, sizeof(DevScalars))) != cudaSuccess) return cleanup(e, "alloc");
   if ((e = cudaMallocHost((void **)&s->hsc, sizeof(DevScalars))) != cudaSuccess) return cleanup(e, "alloc host");
   for (int b = 0; b < 3; b++)
@@ -888,6 +892,8 @@ void kfvm_destroy(kfvm_solver *s) {
   cudaFree(s->heavy);
   cudaFree(s->part);
   cudaFree(s->fmodes);
+  cudaFree(s->spart);
+  cudaFree(s->ssum);
   cudaFree(s->fsums);
   cudaFree(s->sc);
   if (s->hsc) cudaFreeHost(s->hsc);
@@ -1408,6 +1414,29 @@ int kfvm_restart(kfvm_solver *s, const char *xmf_path, int32_t *time_step) {
   s->dt = h;
   s->nTS = ts + 1;
   *time_step = ts;
+  return KFVM_OK;
+}
+
+int kfvm_flow_stats(kfvm_solver *s, double *stats, int32_t *n_stats) {
+  using namespace kfvm;
+  if (!s || !stats) return fail(KFVM_ERR_ARG, "null argument");
+  if (!s->primed) return fail(KFVM_ERR_STATE, "no state yet (kfvm_init_ic / kfvm_set_state / kfvm_restart)");
+  const kfvm_config &c = s->cfg;
+  const double volume = s->dim == 2 ? (c.xup - c.xlo) * (c.yup - c.ylo)
+                                    : (c.xup - c.xlo) * (c.yup - c.ylo) * (c.zup - c.zlo);
+  const double dvol = s->dim == 2 ? s->g.dx * s->g.dy : s->g.dx * s->g.dy * s->g.dz;
+  double *U = s->Ub[s->iCur];
+  // the halo as the boundary conditions set it (the reference relies on the last
+  // evaluation having set it; filling again gives the same values)
+  CK(launch_bc(s->dim, s->eq, U, s->g, s->stream));
+  CK(launch_stats(s->dim, s->eq, U, s->g, dvol / volume, s->spart, s->ssum, s->stream));
+  s->launches += s->eq == KFVM_EQ_SRHYDRO ? 1 : 3;
+  double h[3];
+  CK(cudaMemcpyAsync(h, s->ssum, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const int n = stats_count(s->eq);
+  for (int q = 0; q < n; q++) stats[q] = h[q];
+  if (n_stats) *n_stats = n;
   return KFVM_OK;
 }
 

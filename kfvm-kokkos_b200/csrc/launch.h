@@ -99,6 +99,12 @@ cudaError_t launch_ic(int dim, int eq, int ic_kind, uint64_t seed, const kfvm_co
 // cells), fixed-order sum into out[0] (err) and out[1] (positivity minimum)
 int64_t errest_blocks(int64_t n);
 
+// flow statistics (stats.cu): 3 partials per block, the sums into out[0..2]
+int64_t stats_blocks(const Grid &g);
+int stats_count(int eq);
+cudaError_t launch_stats(int dim, int eq, const double *U, const Grid &g, double ifac, double *part, double *out,
+                         cudaStream_t s);
+
 // random forcing (forcing.cu): mode table on the host, integrals and kick on the device
 int forcing_num_modes(int dim);
 void forcing_draw(int dim, uint32_t seed32, double *modes);

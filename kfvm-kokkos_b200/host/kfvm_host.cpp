@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
@@ -143,8 +144,10 @@ bool ProblemSetup::setIO(const std::string &setting) {
   else if (w[0] == "restartfile" && w.size() >= 2) {
     restartFile = w[1];
     restart = true;
-  } else if (w[0] == "statsfreq" || w[0] == "pdiconf") {
-    warnings.push_back("io:" + w[0] + " has no effect in this build (flow statistics and PDI are not built)");
+  } else if (w[0] == "statsfreq" && w.size() >= 2) {
+    statsFreq = std::stoi(w[1]);
+  } else if (w[0] == "pdiconf") {
+    warnings.push_back("io:pdiconf has no effect in this build (PDI is not built; files are XDMF + raw binary)");
   } else {
     return false;
   }
@@ -225,14 +228,15 @@ std::string ProblemSetup::toJson() const {
                 "%.17g, \"rtol\": %.17g, \"rejection_thresh\": %.17g, \"min_dt\": %.17g, \"final_time\": "
                 "%.17g, \"rejection_limit\": %d, \"max_steps\": %d, \"have_sources\": %d, \"ic\": %d, "
                 "\"seed\": %llu, \"warnings\": %d, \"plot_freq\": %.17g, \"ckpt_freq\": %d, \"restart\": %d, "
-                "\"forcing\": %d, \"force_edot\": %.17g, \"force_ratio\": %.17g, \"force_t_off\": %.17g}",
+                "\"forcing\": %d, \"force_edot\": %.17g, \"force_ratio\": %.17g, \"force_t_off\": %.17g, "
+                "\"stats_freq\": %d}",
                 cfg.dim, cfg.eq, cfg.rs, cfg.rk, cfg.nq, cfg.indicator, (long long)cfg.nx,
                 (long long)cfg.ny, (long long)cfg.nz, cfg.xlo, cfg.xup, cfg.ylo, cfg.yup, cfg.zlo, cfg.zup,
                 cfg.bc[0], cfg.bc[1], cfg.bc[2], cfg.bc[3], cfg.bc[4], cfg.bc[5], cfg.gamma, cfg.reynolds,
                 cfg.prandtl, cfg.weno_thresh, cfg.lfac, cfg.cfl, cfg.atol, cfg.rtol, cfg.rejection_thresh,
                 cfg.min_dt, cfg.final_time, cfg.rejection_limit, cfg.max_steps, cfg.have_sources, ic,
                 (unsigned long long)seed, (int)warnings.size(), plotFreq, ckptFreq, restart ? 1 : 0, forcing ? 1 : 0,
-                force.edot, force.ratio, force.t_off);
+                force.edot, force.ratio, force.t_off, statsFreq);
   return b;
 }
 
@@ -273,6 +277,21 @@ void Solver::writePlot() {
   check(kfvm_write_plotfile(s_, dir.c_str(), ps_.baseName.c_str(), plotNum_, 0, plotNum_), "kfvm_write_plotfile");
 }
 
+void Solver::evalFlowStats() {
+  double st[3];
+  int32_t n = 0;
+  check(kfvm_flow_stats(s_, st, &n), "kfvm_flow_stats");
+  const std::string dir = outputPrefix();
+  std::filesystem::create_directories(dir);
+  FILE *f = std::fopen((dir + ps_.baseName + "_stats.dat").c_str(), statsRows_ == 0 ? "w" : "a");
+  if (!f) throw std::runtime_error("cannot write " + dir + ps_.baseName + "_stats.dat");
+  std::fprintf(f, "%.17g", time_);
+  for (int q = 0; q < n; q++) std::fprintf(f, " %.17g", st[q]);
+  std::fprintf(f, "\n");
+  std::fclose(f);
+  statsRows_++;
+}
+
 void Solver::writeCkpt(int step) {
   const std::string dir = outputPrefix() + "ckpt";
   char b[32];
@@ -303,17 +322,22 @@ void Solver::TakeStep() {
 // Solver::Solve (src/Solver.cpp:84-140) with its plot and checkpoint cadence
 void Solver::Solve() {
   const int maxSteps = ps_.cfg.max_steps;
+  // flow statistics before stepping, every statsfreq steps and after the last
+  // (Solver.cpp:87-91, 108-111, 124-126)
+  if (ps_.statsFreq > 0) evalFlowStats();
   for (; nTS_ < maxSteps && !lastTimeStep_; ++nTS_) {
     if (ps_.verbose > 0) std::printf("Step %d: time = %.4g\n", nTS_, time_);
     // random forcing before the step while time < forcetoff (Solver.cpp:99-103)
     if (ps_.forcing && time_ < ps_.force.t_off) check(kfvm_apply_forcing(s_, nullptr, nullptr, nullptr), "kfvm_apply_forcing");
     TakeStep();
+    if (ps_.statsFreq > 0 && nTS_ % ps_.statsFreq == 0) evalFlowStats();
     if (ps_.plotFreq > 0.0 && (info_.write_plot || lastTimeStep_ || nTS_ == maxSteps - 1)) {
       writePlot();
       plotNum_++;
       check(kfvm_set_plot_freq(s_, ps_.plotFreq, plotNum_), "kfvm_set_plot_freq");
     }
     if (ps_.ckptFreq > 0 && (nTS_ % ps_.ckptFreq == 0 || lastTimeStep_ || nTS_ == maxSteps - 1)) writeCkpt(nTS_);
+    if (lastTimeStep_ && ps_.statsFreq > 0) evalFlowStats();
   }
   std::printf("Time stepping completed\n  %lld RHS evals and %lld/%lld rejected (accuracy/unphysical) steps\n",
               (long long)info_.n_rhs, (long long)nRejectThresh_, (long long)nRejectUnphys_);

@@ -22,6 +22,7 @@ struct ProblemSetup {
   // plot / checkpoint output and restart (ProblemSetup.H:333-367)
   double plotFreq = 0.0;
   int ckptFreq = 0;
+  int statsFreq = 0; // io:statsfreq: flow statistics every statsFreq steps
   std::string restartFile;
   bool restart = false;
   // random forcing (ENABLE_RANDOM_FORCING of the reference's Definitions.H as
@@ -73,6 +74,9 @@ class Solver {
   std::string outputPrefix() const;
   void writePlot();
   void writeCkpt(int step);
+  // Solver::evalFlowStats: one row "time stats..." appended to <prefix><base>_stats.dat
+  // (the reference appends the same row to <prefix><base>_stats.h5)
+  void evalFlowStats();
   const ProblemSetup &ps_;
   kfvm_solver *s_ = nullptr;
   kfvm_step_info info_{};
@@ -80,6 +84,7 @@ class Solver {
   int64_t accepted_ = 0, nRejectThresh_ = 0, nRejectUnphys_ = 0;
   int nTS_ = 1;
   int plotNum_ = 0;
+  int statsRows_ = 0;
   bool lastTimeStep_ = false;
 };
 

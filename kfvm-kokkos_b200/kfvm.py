@@ -78,6 +78,7 @@ def lib():
         L.kfvm_set_timing.argtypes = [P, I32]
         L.kfvm_get_timing.argtypes = [P, P, P]
         L.kfvm_get_launch_count.argtypes = [P, C.POINTER(I64)]
+        L.kfvm_flow_stats.argtypes = [P, P, C.POINTER(I32)]
         L.kfvm_forcing_num_modes.argtypes = [I32]
         L.kfvm_forcing_draw.argtypes = [I32, C.c_uint32, P]
         L.kfvm_set_forcing.argtypes = [P, C.POINTER(abi.KfvmForcing)]
@@ -309,6 +310,14 @@ class Solver:
         ts = C.c_int32()
         _check(lib().kfvm_restart(self.h, str(xmf_path).encode(), C.byref(ts)), "kfvm_restart")
         return ts.value
+
+    def flow_stats(self):
+        """kfvm_flow_stats: volume-averaged kinetic energy, enstrophy (GLM-MHD: and
+        current helicity) of the current state."""
+        out = np.zeros(3, dtype=np.float64)
+        n = C.c_int32()
+        _check(lib().kfvm_flow_stats(self.h, out.ctypes.data, C.byref(n)), "kfvm_flow_stats")
+        return out[:n.value].copy()
 
     def set_forcing(self, forcing):
         """kfvm_set_forcing with an abi.KfvmForcing (None disables)."""

@@ -30,6 +30,8 @@ int orc_take_step(orc_solver *s, kfvm_step_info *info);
 int orc_solve(orc_solver *s, int32_t max_steps, int64_t *n_steps, kfvm_step_info *last);
 int orc_get_time(orc_solver *s, double *time, double *dt);
 int orc_set_time(orc_solver *s, double time, double dt);
+/* Flow statistics of the current state (n_stats = 2, GLM-MHD 3, SRHydro 1). */
+int orc_flow_stats(orc_solver *s, double *stats, int32_t *n_stats);
 /* Random forcing with a given mode table (n_modes x dim x 3). */
 int orc_apply_forcing(orc_solver *s, const double *modes, int32_t n_modes, double edot, double ratio,
                       double *force_str);

@@ -49,6 +49,7 @@ def lib():
         L.orc_get_time.argtypes = [P, P, P]
         L.orc_set_time.argtypes = [P, D, D]
         L.orc_apply_forcing.argtypes = [P, P, I32, D, D, P]
+        L.orc_flow_stats.argtypes = [P, P, P]
         L.orc_get_faces.argtypes = [P, I32, P]
         L.orc_keep_faces.argtypes = [P, I32]
         L.orc_get_flags.argtypes = [P, P, P]
@@ -146,6 +147,12 @@ class OracleSolver:
         t, dt = C.c_double(), C.c_double()
         lib().orc_get_time(self.h, C.addressof(t), C.addressof(dt))
         return t.value, dt.value
+
+    def flow_stats(self):
+        out = np.zeros(3, dtype=np.float64)
+        n = C.c_int32()
+        assert lib().orc_flow_stats(self.h, out.ctypes.data, C.addressof(n)) == 0
+        return out[:n.value].copy()
 
     def apply_forcing(self, modes, edot, ratio):
         """Random forcing with the given mode table [n][dim][3]; returns the strength."""

@@ -1995,6 +1995,60 @@ int orc_solve(orc_solver *s, int32_t max_steps, int64_t *n_steps, kfvm_step_info
   return 0;
 }
 
+// Solver::evalFlowStats (FlowStats<Eq>, Hydro_K.H:103-178, NavierStokes_K.H:102-175,
+// MHD_GLM_K.H:108-211): volume averages, cell by cell in index order, over the
+// state with its boundary halo set
+int orc_flow_stats(orc_solver *s, double *stats, int32_t *n_stats) {
+  if (!s || !stats) return KFVM_ERR_ARG;
+  orc_solver &S = *s;
+  const int eq = S.cfg.eq;
+  const int n = eq == KFVM_EQ_MHD_GLM ? 3 : (eq == KFVM_EQ_SRHYDRO ? 1 : 2);
+  if (n_stats) *n_stats = n;
+  for (int q = 0; q < n; q++) stats[q] = 0.0;
+  if (eq == KFVM_EQ_SRHYDRO) return 0;
+  set_cell_bcs(S, S.U);
+  const std::vector<double> &B = S.U;
+  auto U = [&](int64_t i, int64_t j, int64_t k, int v) { return B[S.ui(i, j, k, v)]; };
+  auto vel = [&](int64_t i, int64_t j, int64_t k, int v) { return U(i, j, k, v) / U(i, j, k, DENS); };
+  const double volume = S.dim == 2 ? (S.cfg.xup - S.cfg.xlo) * (S.cfg.yup - S.cfg.ylo)
+                                   : (S.cfg.xup - S.cfg.xlo) * (S.cfg.yup - S.cfg.ylo) * (S.cfg.zup - S.cfg.zlo);
+  const double dvol = S.dim == 2 ? S.dx * S.dy : S.dx * S.dy * S.dz;
+  const double ifac = dvol / volume;
+  for (int64_t k = 0; k < S.nz; k++)
+    for (int64_t j = 0; j < S.ny; j++)
+      for (int64_t i = 0; i < S.nx; i++) {
+        const double ek = 0.5 * (U(i, j, k, MOMX) * U(i, j, k, MOMX) + U(i, j, k, MOMY) * U(i, j, k, MOMY) +
+                                 U(i, j, k, MOMZ) * U(i, j, k, MOMZ)) / U(i, j, k, DENS);
+        const double dyu = 0.5 * (vel(i, j + 1, k, MOMX) - vel(i, j - 1, k, MOMX)) / S.dy;
+        const double dxv = 0.5 * (vel(i + 1, j, k, MOMY) - vel(i - 1, j, k, MOMY)) / S.dx;
+        double dzu = 0.0, dzv = 0.0, dxw = 0.0, dyw = 0.0;
+        if (S.dim == 3) {
+          dzu = 0.5 * (vel(i, j, k + 1, MOMX) - vel(i, j, k - 1, MOMX)) / S.dz;
+          dzv = 0.5 * (vel(i, j, k + 1, MOMY) - vel(i, j, k - 1, MOMY)) / S.dz;
+          dxw = 0.5 * (vel(i + 1, j, k, MOMZ) - vel(i - 1, j, k, MOMZ)) / S.dx;
+          dyw = 0.5 * (vel(i, j + 1, k, MOMZ) - vel(i, j - 1, k, MOMZ)) / S.dy;
+        }
+        const double omx = dyw - dzv, omy = dzu - dxw, omz = dxv - dyu;
+        const double et = 0.5 * U(i, j, k, DENS) * (omx * omx + omy * omy + omz * omz);
+        stats[0] += ifac * ek;
+        stats[1] += ifac * et;
+        if (eq == KFVM_EQ_MHD_GLM) {
+          const double dybx = 0.5 * (U(i, j + 1, k, MAGX) - U(i, j - 1, k, MAGX)) / S.dy;
+          const double dxby = 0.5 * (U(i + 1, j, k, MAGY) - U(i - 1, j, k, MAGY)) / S.dx;
+          double dzbx = 0.0, dzby = 0.0, dxbz = 0.0, dybz = 0.0;
+          if (S.dim == 3) {
+            dzbx = 0.5 * (U(i, j, k + 1, MAGX) - U(i, j, k - 1, MAGX)) / S.dz;
+            dzby = 0.5 * (U(i, j, k + 1, MAGY) - U(i, j, k - 1, MAGY)) / S.dz;
+            dxbz = 0.5 * (U(i + 1, j, k, MAGZ) - U(i - 1, j, k, MAGZ)) / S.dx;
+            dybz = 0.5 * (U(i, j + 1, k, MAGZ) - U(i, j - 1, k, MAGZ)) / S.dy;
+          }
+          const double cbx = dybz - dzby, cby = dzbx - dxbz, cbz = dxby - dybx;
+          stats[2] += ifac * (U(i, j, k, MAGX) * cbx + U(i, j, k, MAGY) * cby + U(i, j, k, MAGZ) * cbz);
+        }
+      }
+  return 0;
+}
+
 // Solver::applyForcing with a given mode table (Solver.cpp:365-409,
 // RandForcingIntegrate_K / RandForcingApply_K, Common_K.H:645-784): domain integrals
 // in cell order, the strength that injects edot dt, the kick on U, Uprev = U.
