@@ -272,14 +272,26 @@ struct Eos {
     return same;
   }
 
-  // Euler / Navier-Stokes face with equal states (kSameTol): the physical flux, and
-  // the speed bound max(|sL|, |sR|) = |u_n| + a that the Batten/Roe estimates give
-  // for equal states (Hydro_Riemann.H:41-81 with uTil = u, aTil = a)
+  // Face with equal states (kSameTol): the physical flux, and the speed bound
+  // max(|sL|, |sR|) that the estimates give for equal states.  Euler / Navier-Stokes:
+  // |u_n| + a (Hydro_Riemann.H:41-81 with uTil = u, aTil = a); SRHydro: the larger
+  // magnitude of the state's two characteristic bounds (SRHydro_Riemann.H:39-77),
+  // with one pressure recovery instead of two
   __device__ __forceinline__ static double solve_same(double g, int dir, const double *u, double *F) {
-    static_assert(EQ == EQ_HYDRO || EQ == EQ_NS, "Euler / Navier-Stokes only");
+    static_assert(EQ == EQ_HYDRO || EQ == EQ_NS || EQ == EQ_SR, "Euler / Navier-Stokes / SRHydro");
     const int ord[3] = {dir, (dir + 1) % 3, (dir + 2) % 3};
     const int vo[3] = {MOMX + ord[0], MOMX + ord[1], MOMX + ord[2]};
     const int bo[3] = {MAGX + ord[0], MAGX + ord[1], MAGX + ord[2]};
+    if constexpr (EQ == EQ_SR) {
+      double V[NVP];
+      sr::cons2prim(g, u, V);
+      flux(0.0, vo, bo, u, V, F);
+      const double a = sr::soundspeed(g, V), asq = a * a;
+      const double w = V[5], sig = asq / (w * w * (1.0 - asq));
+      const double rt = sqrt(sig * (1.0 + sig - V[vo[0]] * V[vo[0]]));
+      const double sm = (V[vo[0]] - rt) / (1.0 + sig), sp = (V[vo[0]] + rt) / (1.0 + sig);
+      return fmax(fabs(sm), fabs(sp));
+    }
     const double ir = 1.0 / u[DENS];
     double V[NV];
     cons2prim_r(g, u, ir, V);
