@@ -1481,7 +1481,8 @@ int64_t stage_blocks(const Grid &g) {
 }
 
 // one instantiation per (dimension, equations, Gauss points): 2 points for both
-// dimensions, 3 points for 2D; the grid's nq selects
+// dimensions, 3 points for 2D and for 3D Euler / Navier-Stokes (3D GLM-MHD with 3
+// points would need 81 rows per cell); the grid's nq selects
 #define KFVM_DISPATCH(DIM_, EQ_, CALL)                                                  \
   do {                                                                                \
     if (g.nq == 2) {                                                                  \
@@ -1498,6 +1499,9 @@ int64_t stage_blocks(const Grid &g) {
       if ((EQ_) == EQ_NS) return Launch<2, EQ_NS, 3>::CALL;                           \
       if ((EQ_) == EQ_GLM) return Launch<2, EQ_GLM, 3>::CALL;                         \
       if ((EQ_) == EQ_SR) return Launch<2, EQ_SR, 3>::CALL;                           \
+    } else if (g.nq == 3 && (DIM_) == 3) {                                            \
+      if ((EQ_) == EQ_HYDRO) return Launch<3, EQ_HYDRO, 3>::CALL;                     \
+      if ((EQ_) == EQ_NS) return Launch<3, EQ_NS, 3>::CALL;                           \
     }                                                                                 \
     return cudaErrorInvalidValue;                                                     \
   } while (0)

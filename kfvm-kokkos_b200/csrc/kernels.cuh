@@ -57,7 +57,7 @@ struct Grid {
 // stencil on the device: weights plus linear offsets in the padded array, and the
 // full-stencil linear weights packed as [cell][row] (rows: face points f*NQF+q, then
 // interior points q) for the light reconstruction pass
-constexpr int kMaxLinRows = 6 * 4 + 8;
+constexpr int kMaxLinRows = 6 * 9; // 3D, 3 Gauss points: 6 faces x 9 points
 // The same weights for the tensor-core form: W = hi + lo, both TF32 values in FP32
 // containers, stored as the tcgen05 B operand (K-major, no swizzle): K = stencil
 // cells padded to 40, N = rows padded to 32, [cell/4][row][cell%4].
@@ -65,7 +65,7 @@ constexpr int kTcMaxK = 40, kTcMaxN = 32;
 // And as B fragments of the FP64 MMA m8n8k4 (4 stencil cells x 8 rows per
 // fragment, one double per lane): [k step][8-row tile][lane], lane -> (cell
 // 4 ks + lane % 4, row 8 nt + lane / 4), zero beyond the stencil or the rows.
-constexpr int kDmmaMaxB = 9 * 4 * 32;
+constexpr int kDmmaMaxB = 8 * 7 * 32; // 8 K-steps x 7 row tiles (54 rows)
 struct DevStencil {
   kfvm_stencil w;
   int64_t loff[KFVM_MAX_CELLS];
