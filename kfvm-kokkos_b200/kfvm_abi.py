@@ -119,7 +119,8 @@ def make_config(dim, eq, nx, ny, nz=1, extent=(0, 1, 0, 1, 0, 1), bc="periodic",
 
 
 def workload(name, scale=None, steps=None):
-    """The five benchmark workloads (configs of the north-star problem list).
+    """The benchmark workloads (Sod 3D, Kelvin-Helmholtz, Taylor-Green, Orszag-Tang,
+    isentropic vortex) and the SR-hydro and stirred-turbulence problems.
 
     scale, if given, replaces the grid resolution per axis (for small parity runs).
     Returns (config, ic_kind)."""

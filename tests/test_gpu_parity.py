@@ -2,7 +2,7 @@
 
 Each case runs the same configuration, initial condition and weights on both
 sides.  The bar: relative L1 error <= 1e-12 per conserved variable for the
-state after N accepted steps, and close agreement of
+state after N accepted steps (the FP64 parity bar), and close agreement of
 a single RHS evaluation, its face states, WENO flags and max wave speed.
 The GPU fuses multiply-adds, the oracle does not, so agreement is to rounding.
 """
