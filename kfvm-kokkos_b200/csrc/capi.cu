@@ -243,7 +243,7 @@ struct kfvm_solver {
   RKTable rk;
   double time = 0.0, dt = 0.0, errEst = 1.0;
   bool lastTimeStep = false, useSparseWeno = true, primed = false;
-  // equal-state Riemann variant (Euler / Navier-Stokes / SRHydro): on while at least a quarter
+  // equal-state Riemann variant: on while at least a quarter
   // of its sampled faces qualify; when off, probed again after kSameProbeSteps steps
   bool sameOn = true;
   int sameProbe = 0;

@@ -809,8 +809,8 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 // more warps hide the FP64 latency.  The quadrature-weighted sum over a face's
 // points goes through shared memory in point order, and the max wave speed
 // through a warp maximum and an atomic only from warps that raise it.
-// SAME: Euler / Navier-Stokes / SRHydro faces whose two states agree to kSameTol take
-// the consistent flux F(u) without the wave fan (Eos::solve_same); one block in
+// SAME: faces whose two states agree to kSameTol take the consistent flux F(u)
+// without the wave fan (Eos::solve_same); one block in
 // kSameSample counts such faces so that the host can fall back to the plain
 // variant where few faces qualify (its slow path spills more registers).
 constexpr int kSameSample = 1024;
@@ -868,10 +868,10 @@ __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
         if ((flipR >> v) & 1u) uR[v] = -uR[v];
       }
     }
-    if constexpr (SAME && EQ != EQ_GLM) {
+    if constexpr (SAME) {
       // a face inside a uniform region needs no wave fan (kSameTol)
       same = E::same_state(uL, uR);
-      if (same) vmax = E::solve_same(g.gamma, D, uL, Fq);
+      if (same) vmax = E::solve_same(g.gamma, ch, D, uL, Fq);
       else vmax = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
     } else {
       vmax = E::solve(g.rs, g.gamma, ch, D, uL, uR, Fq);
@@ -1429,13 +1429,8 @@ struct Launch {
   }
   static cudaError_t riemann(double *const *F, double *const *G, const Grid &g, DevScalars *sc, bool same,
                              cudaStream_t s) {
-    if constexpr (EQ != EQ_GLM) {
-      if (same) riemann_dirs<true>(F, G, g, sc, s);
-      else riemann_dirs<false>(F, G, g, sc, s);
-    } else {
-      (void)same;
-      riemann_dirs<false>(F, G, g, sc, s);
-    }
+    if (same) riemann_dirs<true>(F, G, g, sc, s);
+    else riemann_dirs<false>(F, G, g, sc, s);
     return cudaGetLastError();
   }
   static cudaError_t stage(const StageArgs &a, const Grid &g, cudaStream_t s) {

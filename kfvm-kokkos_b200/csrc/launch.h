@@ -64,7 +64,7 @@ cudaError_t launch_heavy(int dim, int eq, const double *U, const Grid &g, const 
                          double *theta, double *const *F, double *src, const uint32_t *heavy,
                          const double *bnd, DevScalars *sc, const JudgeArgs &jd, int heavy_blocks,
                          cudaStream_t s);
-// same: the equal-state variant of the Euler / Navier-Stokes / SRHydro kernels
+// same: the equal-state variant of the Riemann kernels
 cudaError_t launch_riemann(int dim, int eq, double *const *F, double *const *G, const Grid &g,
                            DevScalars *sc, bool same, cudaStream_t s);
 cudaError_t launch_stage(int dim, int eq, const StageArgs &a, const Grid &g, cudaStream_t s);

@@ -276,12 +276,18 @@ struct Eos {
   // max(|sL|, |sR|) that the estimates give for equal states.  Euler / Navier-Stokes:
   // |u_n| + a (Hydro_Riemann.H:41-81 with uTil = u, aTil = a); SRHydro: the larger
   // magnitude of the state's two characteristic bounds (SRHydro_Riemann.H:39-77),
-  // with one pressure recovery instead of two
-  __device__ __forceinline__ static double solve_same(double g, int dir, const double *u, double *F) {
-    static_assert(EQ == EQ_HYDRO || EQ == EQ_NS || EQ == EQ_SR, "Euler / Navier-Stokes / SRHydro");
+  // with one pressure recovery instead of two; GLM-MHD: |u_n| + max(ch, cf), what
+  // the Davis and Wu-Shu bounds (MHD_GLM_Riemann.H:55-99) give with no jump in B
+  __device__ __forceinline__ static double solve_same(double g, double ch, int dir, const double *u, double *F) {
     const int ord[3] = {dir, (dir + 1) % 3, (dir + 2) % 3};
     const int vo[3] = {MOMX + ord[0], MOMX + ord[1], MOMX + ord[2]};
     const int bo[3] = {MAGX + ord[0], MAGX + ord[1], MAGX + ord[2]};
+    if constexpr (EQ == EQ_GLM) {
+      double V[NV];
+      cons2prim(g, u, V);
+      flux(ch, vo, bo, u, V, F);
+      return fabs(V[vo[0]]) + fmax(ch, fastMagSonic(g, u, u[bo[0]]));
+    }
     if constexpr (EQ == EQ_SR) {
       double V[NVP];
       sr::cons2prim(g, u, V);
