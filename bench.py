@@ -460,7 +460,7 @@ def run_ours(args):
         out["forms"] = {"fp32_3xtf32": form, "learned_fp32": lf, "learned_fp64": lf64}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.workload, sample_scale=cpu_sample_scale(args.workload),
-                                           sample_steps=1)
+                                           sample_steps=3)
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -489,61 +489,88 @@ def cpu_model():
 
 
 def cpu_sample_scale(workload):
-    """Grid of the bounded CPU sample (about 10-30 s of host work)."""
+    """Grid of the bounded CPU sample (about 10-30 s of host work for 3 steps)."""
     return 64 if WORKLOADS[workload][1] == 3 else 512
 
 
-def cpu_baseline(workload, sample_scale, sample_steps, warmup=0):
-    """The oracle (CPU restatement of the reference path, OpenMP over cells) timed
-    on the host cores on a bounded sample of the workload."""
+def _refrun():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    return refrun
+
+
+def reference_build_rate(workload, sample_scale, steps, cores, warmup=0):
+    """The reference's own CPU code, timed: its src/ compiled unchanged against the
+    host stand-ins of oracle/refshim (OpenMP over cells), one process per run.
+    Seconds per accepted step = (wall time of a run of `steps` steps - wall time of
+    a run of 0 steps) / steps: both runs pay the same set-up (weights, initial
+    condition, FSAL priming evaluation) and write no files.  Returns
+    (zone-updates/s, seconds per step) or None where no build exists."""
+    refrun = _refrun()
+    if refrun.binary(workload) is None:
+        return None
+    cfg, _ = abi.workload(workload, scale=sample_scale, steps=steps)
+    if warmup:
+        refrun.run(workload, cfg, warmup, threads=cores, ckpt=False)
+    sec = refrun.time_steps(workload, cfg, steps, threads=cores)
+    return abi.ncells(cfg) / sec, sec
+
+
+def oracle_rate(workload, sample_scale, steps, cores, warmup=0):
+    """The oracle (this repository's CPU restatement of the path, OpenMP over cells)."""
     oracle = _oracle()
-    cores = os.cpu_count() or 1
     oracle.set_threads(cores)
-    cfg, ic = abi.workload(workload, scale=sample_scale, steps=sample_steps + warmup + 2)
+    cfg, ic = abi.workload(workload, scale=sample_scale, steps=steps + warmup + 2)
     s = oracle.OracleSolver(cfg)
     s.init_ic(ic)
     for _ in range(warmup):
         s.take_step()
     t0 = time.perf_counter()
     acc = 0
-    for _ in range(sample_steps):
+    for _ in range(steps):
         acc += s.take_step().accepted
     dt = time.perf_counter() - t0
-    n = abi.ncells(cfg)
-    return {"value": acc * n / dt, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": "port",
-            "sample": f"{sample_steps} accepted step(s) of the same problem on a {sample_scale}^{cfg.dim} grid "
-                      f"({acc * n} zone-updates in {dt:.1f} s)"}
+    return acc * abi.ncells(cfg) / dt, dt / max(steps, 1)
+
+
+def cpu_rate(workload, sample_scale, steps, cores, warmup=0):
+    """(value, seconds per step, kind, what): the reference build where it exists
+    (kind "reference"), else the oracle port (kind "port")."""
+    dim = WORKLOADS[workload][1]
+    r = reference_build_rate(workload, sample_scale, steps, cores, warmup)
+    if r is not None:
+        return r[0], r[1], "reference", (
+            f"the reference's own CPU code (its src/ compiled unchanged against host-only Kokkos/MPI/PDI "
+            f"stand-ins, OpenMP on {cores} threads), {steps} accepted steps of the same problem on a "
+            f"{sample_scale}^{dim} grid, stepping loop only (run of {steps} steps minus run of 0 steps)")
+    v, sec = oracle_rate(workload, sample_scale, steps, cores, warmup)
+    return v, sec, "port", (
+        f"the oracle (CPU restatement of the reference path, OpenMP on {cores} threads; no reference build "
+        f"present), {steps} accepted steps of the same problem on a {sample_scale}^{dim} grid")
+
+
+def cpu_baseline(workload, sample_scale, sample_steps=3):
+    """The reference's CPU code timed on the host cores on a bounded sample of the workload."""
+    cores = os.cpu_count() or 1
+    v, sec, kind, what = cpu_rate(workload, sample_scale, sample_steps, cores)
+    return {"value": v, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": kind, "sample": what}
 
 
 def run_reference(args):
     ws, rank, local = dist_init()
     if rank != 0:
         return
-    oracle = _oracle()
     cores = os.cpu_count() or 1
-    oracle.set_threads(cores)
-    sample = 48 if WORKLOADS[args.workload][1] == 3 else 192
-    cfg, ic = abi.workload(args.workload, scale=sample, steps=args.warmup + args.steps + 2)
-    s = oracle.OracleSolver(cfg)
-    s.init_ic(ic)
-    for _ in range(args.warmup):
-        s.take_step()
-    t0 = time.perf_counter()
-    acc = 0
-    for _ in range(args.steps):
-        acc += s.take_step().accepted
-    dt = time.perf_counter() - t0
-    n = abi.ncells(cfg)
-    value = acc * n / dt
-    desc = (f"each step: one accepted time step of the same problem on a {sample}^{cfg.dim} grid "
-            f"(the reference build is unavailable here; this is the CPU restatement of its path)")
-    out = {"impl": "reference", "metric": metric_name(args.workload, args.scale), "value": value, "unit": UNIT, "n_gpus": ws,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+    sample = cpu_sample_scale(args.workload)
+    dim = WORKLOADS[args.workload][1]
+    value, sec, kind, what = cpu_rate(args.workload, sample, args.steps, cores, warmup=args.warmup)
+    out = {"impl": "reference", "metric": metric_name(args.workload, args.scale), "value": value, "unit": UNIT,
+           "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (analytic initial condition)",
-           "config": config_block(args.workload, args.scale, {"sample_grid": [sample] * cfg.dim}),
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": "port",
-                            "sample": desc},
+           "config": config_block(args.workload, args.scale, {"sample_grid": [sample] * dim}),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": kind,
+                            "sample": "each step: " + what},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 

@@ -1,0 +1,2 @@
+// TEST INFRASTRUCTURE ONLY: see KokkosBatched_Gemv_Decl.hpp
+#include "KokkosBatched_Gemv_Decl.hpp"

@@ -1,0 +1,2 @@
+// TEST INFRASTRUCTURE ONLY: see Kokkos_Core.hpp
+#include "Kokkos_Core.hpp"

@@ -4,14 +4,16 @@ Reads (as text, nothing is compiled or run) the Gauss-Legendre tables of
 src/numeric/Numeric.cpp:9-46 and the RK coefficient tables of
 src/numeric/Numeric.H:111-282 of slug-cfd/kfvm-kokkos, evaluates the literal
 expressions (e.g. "1.0 / 3.0") in double precision, and writes them as JSON.
-Usage: python tests/golden/make_golden.py /root/reference
+Usage: python tests/golden/make_golden.py <path of the reference checkout>
 """
 import json
 import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py <path of the reference checkout>")
+ref = sys.argv[1]
 cpp = open(os.path.join(ref, "src/numeric/Numeric.cpp")).read()
 hdr = open(os.path.join(ref, "src/numeric/Numeric.H")).read()
 

@@ -1,0 +1,71 @@
+"""Regenerate tests/golden/ref/*.npz: states from the reference's own run.
+
+Builds the reference solver from its sources (oracle/build_ref.py: the
+reference's src/ compiled unchanged against the host stand-ins of
+oracle/refshim/), runs each case below with a checkpoint after every step, and
+stores per case: the configuration (workload, grid, steps, indicator), the time
+and proposed step size after every step, the WENO cell count of every step, the
+per-variable sums of the state after every step, and the final state and WENO
+flags in full.  The tests replay the same steps in the oracle and in the CUDA
+path with the reference's step sizes imposed and compare with these states.
+
+Usage: python tests/golden/make_ref_fixtures.py <path of the reference checkout>
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+for p in (os.path.join(ROOT, "oracle"), os.path.join(ROOT, "kfvm-kokkos_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import build_ref  # noqa: E402
+import kfvm_abi as abi  # noqa: E402
+import refrun  # noqa: E402
+
+# (case, workload, grid per axis, accepted steps, wenothresh override or None)
+CASES = [
+    ("vortex_128_c1", "isentropic_vortex", 128, 20, None),     # the problem list's C1, as stated
+    ("sod3d_24", "sod3d", 24, 5, None),
+    ("sod3d_16_fullweno", "sod3d", 16, 3, -1.0),               # wenothresh < 0: WENO everywhere
+    ("kelvin_helmholtz_64", "kelvin_helmholtz", 64, 10, None),
+    ("taylor_green_16", "taylor_green", 16, 4, None),
+    ("orszag_tang_64", "orszag_tang", 64, 10, None),
+]
+
+
+def case_config(workload, scale, steps, thresh):
+    cfg, ic = abi.workload(workload, scale=scale, steps=steps)
+    if thresh is not None:
+        cfg.weno_thresh = abi.stof(thresh)
+        cfg.indicator = abi.KFVM_IND_ALL if thresh < 0 else abi.KFVM_IND_KXRCF
+    return cfg, ic
+
+
+def main():
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_ref_fixtures.py <path of the reference checkout>")
+    build_ref.build_all(sys.argv[1], sorted({c[1] for c in CASES}))
+    out = os.path.join(HERE, "ref")
+    os.makedirs(out, exist_ok=True)
+    for case, workload, scale, steps, thresh in CASES:
+        cfg, ic = case_config(workload, scale, steps, thresh)
+        cks, _ = refrun.run(workload, cfg, steps)
+        assert len(cks) == steps + 1, (case, len(cks))
+        np.savez_compressed(
+            os.path.join(out, case + ".npz"),
+            workload=workload, scale=scale, steps=steps,
+            weno_thresh=np.nan if thresh is None else thresh,
+            times=np.array([c[1] for c in cks]), dts=np.array([c[2] for c in cks]),
+            weno_counts=np.array([int((c[4][0] > 0).sum()) for c in cks]),
+            sums=np.array([c[3].sum(axis=1) for c in cks]),
+            abs_sums=np.array([np.abs(c[3]).sum(axis=1) for c in cks]),
+            state=cks[-1][3], flags=cks[-1][4])
+        print(case, "steps", steps, "weno cells last", int((cks[-1][4][0] > 0).sum()))
+
+
+if __name__ == "__main__":
+    main()
