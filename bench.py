@@ -296,7 +296,35 @@ def time_form(cfg, ic, prec, steps, warmup, mlp_weights=None):
     if mlp_weights is not None:
         out["judge"] = s.mlp_stats()
     s.close()
+    out["l1_vs_plain"] = form_difference(cfg, ic, prec, mlp_weights)
     return out
+
+
+def form_difference(cfg, ic, prec, mlp_weights=None, steps=3):
+    """Relative L1 difference per conserved variable between a form and plain FP64
+    after `steps` accepted steps from the initial condition, the form driven with
+    plain FP64's step sizes (so both states are at the same time levels)."""
+    import numpy as np
+    import kfvm
+    a = kfvm.Solver(cfg)
+    a.init_ic(ic)
+    b = kfvm.Solver(cfg)
+    b.set_precision(prec)
+    if mlp_weights is not None:
+        b.mlp_set_weights(mlp_weights)
+        b.set_indicator(abi.KFVM_IND_MLP)
+    b.init_ic(ic)
+    for _ in range(steps):
+        b.set_time(*a.time_dt())
+        a.take_step()
+        b.take_step()
+    ua, ub = a.get_state(), b.get_state()
+    a.close()
+    b.close()
+    den = np.maximum(np.abs(ua).sum(axis=1), 1e-300)
+    rel = np.abs(ub - ua).sum(axis=1) / den
+    names = ["dens", "momx", "momy", "momz", "etot", "magx", "magy", "magz", "psi"]
+    return {"steps": steps, "per_variable": {names[v]: float(rel[v]) for v in range(len(rel))}}
 
 
 def run_ours(args):

@@ -726,7 +726,8 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if (cfg->eq == KFVM_EQ_SRHYDRO && cfg->indicator == KFVM_IND_MLP)
     return fail(KFVM_ERR_ARG, "the learned indicator is trained for the Euler / GLM-MHD paths");
   const int64_t nz = cfg->dim == 3 ? cfg->nz : 1;
-  if (cfg->nx * cfg->ny * nz >= (int64_t)0x80000000LL) return fail(KFVM_ERR_ARG, "more than 2^31 cells");
+  if (cfg->nx * cfg->ny * nz > (int64_t)kfvm::kHeavyCellMax + 1)
+    return fail(KFVM_ERR_ARG, "more than 2^29 cells (the WENO cell list packs a cell index in 29 bits)");
   if (cfg->nx < 3 || cfg->ny < 3 || nz < (cfg->dim == 3 ? 3 : 1))
     return fail(KFVM_ERR_ARG, "grid too small for a radius-2 stencil");
   for (int d = 0; d < cfg->dim; d++) {
@@ -1025,8 +1026,6 @@ int kfvm_set_indicator(kfvm_solver *s, int32_t ind) {
                                 "kfvm_mlp_train)");
   if (ind == KFVM_IND_MLP && s->eq == KFVM_EQ_SRHYDRO)
     return fail(KFVM_ERR_ARG, "the learned indicator is trained for the Euler / GLM-MHD paths");
-  if (ind == KFVM_IND_MLP && s->g.n > (int64_t)kfvm::kHeavyCellMax)
-    return fail(KFVM_ERR_ARG, "learned indicator: at most 2^30 cells");
   s->indicator = ind;
   s->useSparseWeno = sparse_allowed(s);
   return KFVM_OK;

@@ -83,9 +83,12 @@ __global__ void __launch_bounds__(256) bc_fill_kernel(double *__restrict__ U, Gr
 //   heavy    WENO-AO and/or the full limiter on the listed cells
 // theta of the previous evaluation feeds the flags, so it is rewritten only after
 // flag_kernel has read it.
-constexpr uint32_t kHeavyWeno = 0x80000000u;
-constexpr uint32_t kHeavyJudge = 0x40000000u; // a judged cell of the learned indicator
-constexpr uint32_t kHeavyCell = 0x3fffffffu;
+constexpr uint32_t kHeavyWeno = 0x80000000u;      // WENO-AO is computed for the cell
+constexpr uint32_t kHeavyJudge = 0x40000000u;     // a judged cell of the learned indicator
+constexpr uint32_t kHeavyJudgeOnly = 0x20000000u; // judged but outside the WENO set: it keeps
+                                                  // its linear states unless the judge's label
+                                                  // says troubled (the cell-level fallback)
+constexpr uint32_t kHeavyCell = kHeavyCellMax;
 
 // Linear reconstruction of every cell on the FP64 tensor cores (mma.sync m8n8k4,
 // the FP64 MMA of sm_100a; tcgen05 has no FP64 kind).  Per warp: one row of 32 cells
@@ -409,7 +412,7 @@ __global__ void __launch_bounds__(256)
                    double *__restrict__ theta, uint32_t *__restrict__ heavy,
                    const double2 *__restrict__ lamvel, DevScalars *__restrict__ sc, JudgeArgs jd) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  bool useWeno = false, push = false, judged = false;
+  bool useWeno = false, push = false, judged = false, judgeOnly = false;
   double lam = 0.0, vel = 0.0;
   if (c < g.n) {
     if (mode == RECON_FULL) {
@@ -422,8 +425,10 @@ __global__ void __launch_bounds__(256)
         useWeno = wset[c] != 0;
       }
     }
-    // the judge's cells run full WENO whatever the flags say (they do not enter the set)
+    // the judge's cells compute full WENO whatever the flags say (they do not enter
+    // the set); one outside the set keeps its linear states unless judged troubled
     judged = mode == RECON_SPARSE && jd.frac > 0.0 && unit_hash(jd.seed, (uint64_t)c) < jd.frac;
+    judgeOnly = judged && !useWeno;
     useWeno = useWeno || judged;
     applied[c] = useWeno ? 1 : 0;
     if (useWeno || !status[c]) {
@@ -445,7 +450,8 @@ __global__ void __launch_bounds__(256)
   base = __shfl_sync(0xffffffffu, base, 0);
   if (push)
     heavy[base + __popc(ball & ((1u << lane) - 1u))] =
-        (uint32_t)c | (useWeno ? kHeavyWeno : 0u) | (judged ? kHeavyJudge : 0u);
+        (uint32_t)c | (useWeno ? kHeavyWeno : 0u) | (judged ? kHeavyJudge : 0u) |
+        (judgeOnly ? kHeavyJudgeOnly : 0u);
   if (lane == 0 && wball) atomicAdd(&sc->napplied, (unsigned)__popc(wball));
   if constexpr (EQ == EQ_GLM) {
     lam = warp_max(lam);
@@ -724,8 +730,9 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
       }
 #pragma unroll
       for (int r = 0; r < NR; r++) rs[r * NV + v] = acc[r];
-    } else if (have) {
-      // limiter only: the linear states already written
+    }
+    auto load_linear = [&]() {
+      // the linear states the reconstruction pass wrote
       for (int r = 0; r < NR; r++) {
         double val;
         if (r < T::NF * T::NQF) {
@@ -736,7 +743,13 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
         }
         rs[r * NV + v] = val;
       }
-    }
+    };
+    if (have && !(e & kHeavyWeno)) load_linear();  // limiter only
+    __syncthreads();
+    // a judged cell outside the WENO set that the judge finds smooth keeps its
+    // linear states: the judge measures the network without perturbing the flow
+    const bool keepLinear = have && (e & kHeavyJudgeOnly) && !(fmax(sDep[x * 2], sDep[x * 2 + 1]) > jd.tau);
+    if (keepLinear) load_linear();
     __syncthreads();
     // ---- back to conserved variables and PositivityPreserve_K, one thread per cell
     if (v == 0 && have) {
@@ -745,7 +758,8 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
       for (int w = 0; w < NV; w++) ref[w] = Uc[w * g.pvol];
       if (e & kHeavyWeno) {
         VarConv<EQ> vc(ref, g.gamma);
-        for (int r = 0; r < NR; r++) vc.linPrim2Cons(rs + r * NV);
+        if (!keepLinear)
+          for (int r = 0; r < NR; r++) vc.linPrim2Cons(rs + r * NV);
         if (e & kHeavyJudge) {
           const double dep = fmax(sDep[x * 2], sDep[x * 2 + 1]);
           const bool lab = dep > jd.tau, p = jd.pred[c] != 0;

@@ -91,8 +91,9 @@ struct DevScalars {
   unsigned long long nsame, nsamp;
 };
 
-// heavy-list entries carry the cell index in the low 30 bits
-constexpr uint32_t kHeavyCellMax = 0x3fffffffu;
+// heavy-list entries carry the cell index in the low 29 bits (grids of at most 2^29
+// cells: 180 GB holds about 1.4e8 cells of the 3D path's arrays)
+constexpr uint32_t kHeavyCellMax = 0x1fffffffu;
 
 // variations below this fraction of a cell's density / pressure count as smooth for
 // the learned indicator (labels and the normalisation of its features)

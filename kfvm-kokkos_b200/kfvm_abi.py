@@ -152,6 +152,12 @@ def workload(name, scale=None, steps=None):
         c = make_config(2, KFVM_EQ_MHD_GLM, n, n, extent=(0, 1, 0, 1),
                         gamma=5.0 / 3.0, rs=KFVM_RS_HLL, cfl=0.4, steps=steps or 1000)
         return c, KFVM_IC_ORSZAG_TANG
+    # 3D GLM-MHD: the Orszag-Tang vortex extruded in z (exec/MHD/OrszagTang/orsztang3d.init)
+    if name == "orszag_tang_3d":
+        n = scale or 128
+        c = make_config(3, KFVM_EQ_MHD_GLM, n, n, n, extent=(0, 1, 0, 1, 0, 1),
+                        gamma=5.0 / 3.0, rs=KFVM_RS_HLL, cfl=0.4, steps=steps or 100)
+        return c, KFVM_IC_ORSZAG_TANG
     # special-relativistic hydro (exec/SRHydro/SRShockTube, exec/SRHydro/SRRiem2d)
     if name == "sr_shock_tube":
         n = scale or 2000

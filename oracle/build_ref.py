@@ -138,6 +138,7 @@ PROBLEMS = {
     "kelvin_helmholtz": (2, "Hydro", "HLLC", "SSP4_3_2", 2, "periodic", False, IC_KH),
     "taylor_green": (3, "NavierStokes", "HLLC", "SSP4_3_2", 2, "periodic", False, IC_TGV),
     "orszag_tang": (2, "MHD_GLM", "HLL", "SSP4_3_2", 2, "periodic", True, IC_OT),
+    "orszag_tang_3d": (3, "MHD_GLM", "HLL", "SSP4_3_2", 2, "periodic", True, IC_OT),
 }
 
 

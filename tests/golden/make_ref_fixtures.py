@@ -34,6 +34,7 @@ CASES = [
     ("kelvin_helmholtz_64", "kelvin_helmholtz", 64, 10, None),
     ("taylor_green_16", "taylor_green", 16, 4, None),
     ("orszag_tang_64", "orszag_tang", 64, 10, None),
+    ("orszag_tang_3d_16", "orszag_tang_3d", 16, 3, None),     # 3D GLM-MHD sources at Q^3 points
 ]
 
 
