@@ -281,11 +281,12 @@ struct kfvm_solver {
     bool ready = false;                 // weights set or initialised
     int nw = 0, ni = 0;
     uint16_t *wb = nullptr;             // BF16 weights used by inference
-    uint16_t *w1img = nullptr;          // W1^T in the tcgen05 B-operand layout
+    uint8_t *img = nullptr;             // the inference kernel's weight image (tcgen05 B operands, biases)
     float *wq = nullptr;                // the same values as FP32 (training forward)
     float *master = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *loss = nullptr;
     int t = 0;                          // Adam steps taken
     uint8_t *pred = nullptr;            // per-cell prediction of the last evaluation
+    kfvm::MlpTileBuf tiles;             // (density, pressure) pairs and their TMA tile map
     uint16_t *feats = nullptr;          // collected samples: features, labels, cells
     uint8_t *labels = nullptr;
     int64_t *cells = nullptr;
@@ -422,10 +423,10 @@ int eval_front(kfvm_solver *s, int b) {
   }
   if (mode == RECON_SPARSE) {
     const double thr = s->cfg.weno_thresh * std::pow(s->dmin, 1.5);
-    if ((e = run(s, KFVM_KCLASS_FLAG, 1, [&] {
+    if ((e = run(s, KFVM_KCLASS_FLAG, mlpOn ? 2 : 1, [&] {
            if (mlpOn)
-             return launch_mlp_flag(dim, eq, s->Ub[b], s->g, s->mlp.wb, s->mlp.w1img, s->theta, s->flag,
-                                    s->mlp.pred, s->sc, (float)s->mlp.logitThr, st);
+             return launch_mlp_flag(dim, eq, s->Ub[b], s->g, s->mlp.tiles, s->mlp.img, s->theta,
+                                    s->flag, s->mlp.pred, s->sc, (float)s->mlp.logitThr, st);
            return launch_flag(dim, eq, s->Ub[b], s->g, s->W, s->F, s->theta, s->flag, s->sc, thr, st);
          })) != cudaSuccess)
       return set_err_cuda(e, "flag");
@@ -907,7 +908,8 @@ void kfvm_destroy(kfvm_solver *s) {
   cudaFree(s->mlp.grad);
   cudaFree(s->mlp.loss);
   cudaFree(s->mlp.pred);
-  cudaFree(s->mlp.w1img);
+  cudaFree(s->mlp.img);
+  cudaFree(s->mlp.tiles.rp);
   cudaFree(s->mlp.feats);
   cudaFree(s->mlp.labels);
   cudaFree(s->mlp.cells);
@@ -1077,7 +1079,8 @@ int mlp_alloc(kfvm_solver *s) {
       (e = cudaMalloc((void **)&M.grad, M.nw * sizeof(float))) != cudaSuccess ||
       (e = cudaMalloc((void **)&M.loss, 4 * sizeof(float))) != cudaSuccess ||
       (e = cudaMalloc((void **)&M.pred, s->g.n)) != cudaSuccess ||
-      (e = cudaMalloc((void **)&M.w1img, kfvm::mlp_w1_image_size(s->dim) * sizeof(uint16_t))) != cudaSuccess)
+      (e = cudaMalloc((void **)&M.img, kfvm::mlp_image_bytes(s->dim))) != cudaSuccess ||
+      (e = kfvm::mlp_tile_buf_init(s->dim, s->g, M.tiles)) != cudaSuccess)
     return set_err_cuda(e, "learned indicator buffers");
   CK(cudaMemsetAsync(M.pred, 0, s->g.n, s->stream));
   CK(cudaMemsetAsync(M.grad, 0, M.nw * sizeof(float), s->stream));
@@ -1098,7 +1101,7 @@ int mlp_load(kfvm_solver *s, const std::vector<float> &w) {
   CK(cudaMemcpyAsync(M.master, q.data(), M.nw * sizeof(float), cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemsetAsync(M.m, 0, M.nw * sizeof(float), s->stream));
   CK(cudaMemsetAsync(M.v, 0, M.nw * sizeof(float), s->stream));
-  cudaError_t e = kfvm::launch_mlp_pack(s->dim, M.wb, M.w1img, s->stream);
+  cudaError_t e = kfvm::launch_mlp_pack(s->dim, M.wb, M.wq, M.img, s->stream);
   if (e != cudaSuccess) return set_err_cuda(e, "pack");
   CK(cudaStreamSynchronize(s->stream));
   M.t = 0;
@@ -1241,7 +1244,7 @@ int kfvm_mlp_train(kfvm_solver *s, int32_t steps, int32_t batch, double lr, doub
     });
     if (e != cudaSuccess) return set_err_cuda(e, "train");
   }
-  cudaError_t ep = kfvm::launch_mlp_pack(s->dim, M.wb, M.w1img, s->stream);
+  cudaError_t ep = kfvm::launch_mlp_pack(s->dim, M.wb, M.wq, M.img, s->stream);
   if (ep != cudaSuccess) return set_err_cuda(ep, "pack");
   float l[4];
   CK(cudaMemcpyAsync(l, M.loss, sizeof(l), cudaMemcpyDeviceToHost, s->stream));
@@ -1273,7 +1276,8 @@ int kfvm_mlp_probability(kfvm_solver *s, float *out_host) {
   const int b = s->iCur;
   e = kfvm::launch_bc(s->dim, s->eq, s->Ub[b], s->g, s->stream);
   if (e == cudaSuccess)
-    e = kfvm::launch_mlp_prob(s->dim, s->eq, s->Ub[b], s->g, s->mlp.wb, s->mlp.w1img, d, s->sc, s->stream);
+    e = kfvm::launch_mlp_prob(s->dim, s->eq, s->Ub[b], s->g, s->mlp.tiles, s->mlp.img, d, s->sc,
+                              s->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(out_host, d, s->g.n * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);

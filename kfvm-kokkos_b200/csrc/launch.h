@@ -1,6 +1,7 @@
 // launch.h -- host-side entry points of the kernels in kernels.cu
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -75,15 +76,26 @@ int mlp_num_inputs(int dim);
 cudaError_t launch_mlp_collect(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, double tau,
                                double keep, uint64_t seed, uint16_t *feats, uint8_t *labels, int64_t *cells,
                                unsigned long long *count, int64_t cap, cudaStream_t s);
-// inference: first layer on tcgen05 (BF16, FP32 accumulation) with the W1^T image
-// of launch_mlp_pack, the rest in FP32 on the CUDA cores
-cudaError_t launch_mlp_flag(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
-                            const uint16_t *w1img, const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc,
-                            float logit_thr, cudaStream_t s);
-cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
-                            const uint16_t *w1img, float *out, DevScalars *sc, cudaStream_t s);
-int mlp_w1_image_size(int dim);
-cudaError_t launch_mlp_pack(int dim, const uint16_t *wb, uint16_t *img, cudaStream_t s);
+// inference: the (density, pressure) pairs of every padded cell (one kernel), then
+// per block a TMA load of its halo tile of pairs plus bulk loads of the weight image,
+// and the network with both matrix layers on tcgen05 (layer 1 BF16, layer 2 split
+// TF32; FP32 accumulation), bias, GELU and output in FP32 (a second kernel)
+struct MlpTileBuf {
+  CUtensorMap map;         // halo tiles of rp (TMA box TX x TY x TZ of 8-byte pairs)
+  float2 *rp = nullptr;    // [plane][row][x] pairs, row pitch rpx
+  int64_t rpx = 0;
+};
+cudaError_t mlp_tile_buf_init(int dim, const Grid &g, MlpTileBuf &tb);
+// img: the weight image of launch_mlp_pack
+cudaError_t launch_mlp_flag(int dim, int eq, const double *U, const Grid &g, const MlpTileBuf &tb, const uint8_t *img,
+                            const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc, float logit_thr,
+                            cudaStream_t s);
+cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const MlpTileBuf &tb, const uint8_t *img,
+                            float *out, DevScalars *sc, cudaStream_t s);
+// the inference kernel's weight image (W1^T BF16, W2^T FP32, biases) from the BF16
+// weights wb and their FP32 values wq, after every change of the weights
+int mlp_image_bytes(int dim);
+cudaError_t launch_mlp_pack(int dim, const uint16_t *wb, const float *wq, uint8_t *img, cudaStream_t s);
 cudaError_t launch_mlp_train_step(int dim, const uint16_t *feats, const uint8_t *labels, int64_t n, int batch,
                                   float *master, float *m, float *v, float *grad, float *wq, uint16_t *wb,
                                   float *loss, float pos_weight, float lr, int t, uint64_t seed, cudaStream_t s);

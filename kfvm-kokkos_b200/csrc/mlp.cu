@@ -12,12 +12,14 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "kernels.cuh"
 #include "launch.h"
 #include "mlp.cuh"
 #include "tcgen05.cuh"
+#include "tma.cuh"
 
 namespace kfvm {
 
@@ -190,63 +192,121 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
-// Inference with the first layer on the tcgen05 tensor cores: per block of 128
-// cells (two threads per cell = per row of the tile) the BF16 feature rows form
-// A [128 x KP], W1^T in BF16 forms B [KP x 32], and D = A B accumulates in FP32
-// in 32 TMEM columns (M128 N32 K16 MMAs, kind::f16).  The features are written
-// in halves of K into one shared-memory buffer (two blocks fit an SM).  Then
-// bias + GELU, the 32 x 32 second layer and the output on the CUDA cores in FP32
-// (as in training).  Every mbarrier wait is bounded; on timeout the block sets
-// DevScalars::fault and returns after freeing its TMEM.
+// Density and pressure of every padded cell as an FP32 pair (the values the
+// features are made of), row pitch rpx (even, so that rows of 8-byte pairs start
+// on 16-byte boundaries for the TMA loads of the inference kernel).  Computed
+// once per evaluation; every block of the inference kernel then loads its
+// 36 x 8 x 5 halo tile of pairs (11.5 KB) instead of five FP64 variables.
+template <int EQ>
+__global__ void __launch_bounds__(256)
+    mlp_rp_kernel(const double *__restrict__ U, Grid g, int64_t planes, int64_t rpx, float2 *__restrict__ rp) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= g.px * g.py * planes) return;
+  const int64_t a = t % g.px, r = t / g.px;   // r = plane * py + row
+  double u[Eos<EQ>::NV];
+#pragma unroll
+  for (int v = 0; v < Eos<EQ>::NV; v++) u[v] = U[v * g.pvol + t];
+  rp[r * rpx + a] = make_float2((float)u[DENS], (float)Eos<EQ>::pres(g.gamma, u));
+}
+
+// ---------------------------------------------------------------------------
+// Inference with both matrix layers on the tcgen05 tensor cores, per block of 128
+// cells (two threads per cell = per row of the tiles, part 0 and part 1):
+//   layer 1  D1 = A1 B1, A1 [128 x KP] the BF16 features, B1 = W1^T in BF16,
+//            M128 N32 K16 MMAs (kind::f16), FP32 accumulation in TMEM columns 0-31.
+//            The GEMM places density feature q in column q and pressure feature q
+//            in column PAD + q (PAD = 32 in 2D, 128 in 3D), so that one 8-byte
+//            read of the (density, pressure) pair of a patch cell gives both.
+//   layer 2  D2 = A2 B2, A2 [128 x 32] = H1 = gelu(D1 + b1) split as tf32 hi + lo,
+//            B2 = W2^T (BF16 values, exact in TF32), M128 N32 K8 MMAs (kind::tf32,
+//            two per K step: hi and lo), FP32 accumulation in TMEM columns 32-63;
+//            the product carries about 21 bits of H1, as the FP32 layer of
+//            training does.
+//   output   gelu(D2 + b2) . w3 + b3, each part summing 16 hidden units.
+// The block's halo tile of pairs arrives by one TMA load.  Every mbarrier wait is
+// bounded; on timeout the block sets DevScalars::fault, waits (bounded) for its
+// tile load, frees its TMEM and returns.
 constexpr int kMlpThreads = 256;
 
 template <int DIM>
 struct MlpTc {
   using M = MlpShape<DIM>;
   using Tl = MlpTile<DIM>;
-  static constexpr int KP = (M::NI + 15) / 16 * 16;        // K padded to the MMA K of 16
-  static constexpr int NCH = KP / 8;                       // 16-byte chunks of 8 BF16
-  static constexpr int HALVES = DIM == 3 ? 2 : 1;
-  static constexpr int NCHH = NCH / HALVES;                // chunks per half
-  static constexpr int A_CH = 128 * 16;
-  static constexpr int B_CH = 32 * 16;
-  static constexpr int OFF_B = NCHH * A_CH;                // A: one half
-  static constexpr int OFF_TILE = OFF_B + NCH * B_CH;      // B: all of W1^T
-  static constexpr int OFF_H = OFF_TILE + (2 * Tl::N * 4 + 15) / 16 * 16; // H1 [128][33] floats
-  static constexpr int OFF_W = OFF_H + 128 * 33 * 4;       // b1, W2, b2, w3, b3 (floats)
-  static constexpr int NW2 = M::NW - M::B1;
-  static constexpr int OFF_SC = OFF_W + (NW2 + 3) / 4 * 16; // centers and scales [128][4] floats
-  static constexpr int OFF_OFS = OFF_SC + 128 * 4 * 4;     // patch offsets [P] int
+  static constexpr int PAD = DIM == 2 ? 32 : 128;          // GEMM column of the first pressure feature
+  static constexpr int KP = 2 * PAD;                       // layer-1 K
+  static constexpr int NCH = KP / 8;                       // 16-byte chunks of 8 BF16 along K
+  static constexpr int NQC = PAD / 8;                      // chunks of one quantity
+  static constexpr int A_CH = 128 * 16;                    // one K chunk of a 128-row operand
+  static constexpr int B_CH = 32 * 16;                     // one K chunk of a 32-row operand
+  static constexpr int A1 = NCH * A_CH;
+  static constexpr int A2 = 2 * 8 * A_CH;                  // H1 hi and lo: 32 K = 8 chunks of 4 tf32
+  // the weight image in global memory (launch_mlp_pack), copied as two bulk loads:
+  //   W1^T [k / 8][n][k % 8] BF16 | W2^T [k / 4][n][k % 4] FP32 | b1 b2 w3 b3 (+ 3 pad) FP32
+  static constexpr int W1B = NCH * B_CH;
+  static constexpr int W2B = 8 * B_CH;
+  static constexpr int PRMB = 100 * 4;
+  static constexpr int IMG_BYTES = W1B + W2B + PRMB;
+  static constexpr int OFF_B1 = A1 > A2 ? A1 : A2;         // A1, then A2 in the same bytes
+  static constexpr int OFF_B2 = OFF_B1 + W1B;
+  static constexpr int OFF_W = OFF_B2 + W2B;
+  static constexpr int OFF_TILE = (OFF_W + PRMB + 127) / 128 * 128;
+  static constexpr int OFF_MX = OFF_TILE + (Tl::N * 8 + 15) / 16 * 16; // patch maxima [2 parts][128][2]
+  static constexpr int OFF_SUM = OFF_MX + 2 * 128 * 2 * 4; // part 1's share of the output sum [128]
+  static constexpr int OFF_OFS = OFF_SUM + 128 * 4;        // patch offsets [P] int
   static constexpr int OFF_BAR = OFF_OFS + (M::P + 3) / 4 * 16;
-  static constexpr int SMEM = OFF_BAR + 16;
-  static_assert(NCH % HALVES == 0 && NCHH % 2 == 0, "K halves of whole MMA steps");
+  static constexpr int SMEM = OFF_BAR + 32;                // MMA barrier, TMEM slot, load barrier
+  static_assert(M::P <= PAD && NQC % 2 == 0, "pressure features start past the density ones");
+  static_assert(OFF_TILE % 128 == 0 && OFF_B1 % 16 == 0 && OFF_B2 % 16 == 0, "TMA destination alignment");
+  static_assert((W2B + PRMB) % 16 == 0 && W1B % 16 == 0, "bulk copy sizes");
+  static_assert((Tl::TX * 8) % 16 == 0, "TMA box inner extent");
   static_assert(SMEM <= 113 * 1024, "two blocks per SM");
 };
 
+// the weight image of the inference kernel: W1^T in the layer-1 B layout
+// [k / 8][n][k % 8] (k the GEMM column), then W2^T as FP32 in the layer-2 B layout
+// [k / 4][n][k % 4], then b1, b2, w3, b3 as FP32
 template <int DIM>
-__global__ void __launch_bounds__(256) mlp_pack_kernel(const uint16_t *__restrict__ wb, uint16_t *__restrict__ img) {
+__global__ void __launch_bounds__(256)
+    mlp_pack_kernel(const uint16_t *__restrict__ wb, const float *__restrict__ wq, uint8_t *__restrict__ img) {
   using M = MlpShape<DIM>;
   using C = MlpTc<DIM>;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 32 * C::KP) return;
-  const int n = t / C::KP, k = t % C::KP;
-  img[(k / 8) * 256 + n * 8 + (k % 8)] = k < M::NI ? wb[M::W1 + n * M::NI + k] : (uint16_t)0;
+  if (t < 32 * C::KP) {
+    const int n = t / C::KP, k = t % C::KP;
+    const int q = k < C::PAD ? k : k - C::PAD;
+    const int f = k < C::PAD ? q : M::P + q;               // network input of this column
+    reinterpret_cast<uint16_t *>(img)[(k / 8) * 256 + n * 8 + (k % 8)] =
+        q < M::P ? wb[M::W1 + n * M::NI + f] : (uint16_t)0;
+  }
+  float *w2 = reinterpret_cast<float *>(img + C::W1B);
+  if (t < M::NH * M::NH) {
+    const int n = t / M::NH, kk = t % M::NH;
+    w2[(kk / 4) * 128 + n * 4 + (kk % 4)] = wq[M::W2 + n * M::NH + kk];
+  }
+  float *prm = reinterpret_cast<float *>(img + C::W1B + C::W2B);
+  if (t < 32) {
+    prm[t] = wq[M::B1 + t];
+    prm[32 + t] = wq[M::B2 + t];
+    prm[64 + t] = wq[M::W3 + t];
+  }
+  if (t < 4) prm[96 + t] = t == 0 ? wq[M::B3] : 0.0f;
 }
 
 // mode 0: flags (+ prediction, flagged count); mode 1: probabilities
 template <int DIM, int EQ, int MODE>
 __global__ void __launch_bounds__(kMlpThreads, 2)
-    mlp_tc_kernel(const double *__restrict__ U, Grid g, const uint16_t *__restrict__ wb,
-                  const uint16_t *__restrict__ w1img, const double *__restrict__ theta, uint8_t *__restrict__ flag,
-                  uint8_t *__restrict__ pred, float *__restrict__ prob, DevScalars *__restrict__ sc, float logit_thr) {
+    mlp_tc_kernel(const __grid_constant__ CUtensorMap rpMap, Grid g, const uint8_t *__restrict__ img,
+                  const double *__restrict__ theta, uint8_t *__restrict__ flag, uint8_t *__restrict__ pred,
+                  float *__restrict__ prob, DevScalars *__restrict__ sc, float logit_thr) {
   using M = MlpShape<DIM>;
   using Tl = MlpTile<DIM>;
   using C = MlpTc<DIM>;
   extern __shared__ __align__(128) uint8_t msm[];
-  float(*tile)[Tl::N] = reinterpret_cast<float(*)[Tl::N]>(msm + C::OFF_TILE);
-  float(*sH)[33] = reinterpret_cast<float(*)[33]>(msm + C::OFF_H);
-  float *sW = reinterpret_cast<float *>(msm + C::OFF_W);   // layout of the flat weights from B1 on
-  float(*sSc)[4] = reinterpret_cast<float(*)[4]>(msm + C::OFF_SC);
+  // the block's halo tile of (density, pressure) pairs, [z][y][x] as the TMA box lands
+  const float2 *tile = reinterpret_cast<const float2 *>(msm + C::OFF_TILE);
+  const float *sW = reinterpret_cast<const float *>(msm + C::OFF_W);   // b1 [32], b2 [32], w3 [32], b3
+  float(*sMx)[128][2] = reinterpret_cast<float(*)[128][2]>(msm + C::OFF_MX);
+  float *sSum = reinterpret_cast<float *>(msm + C::OFF_SUM);
   int *sOfs = reinterpret_cast<int *>(msm + C::OFF_OFS);
   uint64_t *bar = reinterpret_cast<uint64_t *>(msm + C::OFF_BAR);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(msm + C::OFF_BAR + 8);
@@ -256,144 +316,177 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
   const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY, k = blockIdx.z;
   const int64_t i = i0 + lane, j = j0 + quarter;
   const bool live = i < g.nx && j < g.ny;
-  const uint32_t barA = smem_u32(bar);
+  const uint32_t barA = smem_u32(bar), barL = barA + 16;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                 "r"(32u)
+                 "r"(64u)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barA) : "memory");
+    mbar_init(barA, 1);
+    mbar_init(barL, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    // the halo tile (padded coordinates of its first cell: i0 - R, j0 - R, k - R in
+    // cells) and the weight image, all on one barrier
+    mbar_arrive_expect_tx(barL, (uint32_t)(Tl::N * sizeof(float2) + C::IMG_BYTES));
+    tma_load_3d(smem_u32(msm + C::OFF_TILE), &rpMap, (int)i0, (int)j0, (int)k, barL);
+    bulk_load(smem_u32(msm + C::OFF_B1), img, C::W1B, barL);
+    bulk_load(smem_u32(msm + C::OFF_B2), img + C::W1B, C::W2B + C::PRMB, barL);
   }
   {
-    const uint4 *src = reinterpret_cast<const uint4 *>(w1img);
-    uint4 *dst = reinterpret_cast<uint4 *>(msm + C::OFF_B);
-    for (int t = tid; t < C::NCH * C::B_CH / 16; t += kMlpThreads) dst[t] = src[t];
-    for (int t = tid; t < C::NW2; t += kMlpThreads) sW[t] = __bfloat162float(__ushort_as_bfloat16(wb[M::B1 + t]));
     constexpr int ZR = DIM == 3 ? Tl::R : 0;
     for (int q = tid; q < M::P; q += kMlpThreads) {
       const int dx = q % M::SIDE - Tl::R, dy = (q / M::SIDE) % M::SIDE - Tl::R, dz = q / (M::SIDE * M::SIDE) - ZR;
       sOfs[q] = (dz * Tl::TY + dy) * Tl::TX + dx;
     }
   }
-  for (int t = tid; t < Tl::N; t += kMlpThreads) {
-    const int a = t % Tl::TX, b = (t / Tl::TX) % Tl::TY, cz = t / (Tl::TX * Tl::TY);
-    const int64_t gi = i0 - Tl::R + a, gj = j0 - Tl::R + b, gk = k - (DIM == 3 ? Tl::R : 0) + cz;
-    if (gi > g.nx + Tl::R - 1 || gj > g.ny + Tl::R - 1) continue;
-    const double *Uq = U + pidx(g, gi, gj, gk);
-    double u[Eos<EQ>::NV];
-#pragma unroll
-    for (int v = 0; v < Eos<EQ>::NV; v++) u[v] = Uq[v * g.pvol];
-    tile[0][t] = (float)u[DENS];
-    tile[1][t] = (float)Eos<EQ>::pres(g.gamma, u);
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
-  // scales of the two patches: part 0 density, part 1 pressure
+  bool ok = __syncthreads_and(mbar_wait(barL, 0u));
   constexpr int ZR = DIM == 3 ? Tl::R : 0;
   const int c0 = (ZR * Tl::TY + quarter + Tl::R) * Tl::TX + lane + Tl::R;
-  {
-    const float ref = tile[part][c0];
-    float mx = 0.0f;
-    for (int q = 0; q < M::P; q++) mx = fmaxf(mx, fabsf(__fsub_rn(tile[part][c0 + sOfs[q]], ref)));
-    sSc[row][part] = ref;
-    sSc[row][2 + part] = mlp_scale(mx, ref);
+  const uint32_t aB = smem_u32(msm), b1B = smem_u32(msm + C::OFF_B1), b2B = smem_u32(msm + C::OFF_B2);
+  const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+  if (ok) {
+    // patch maxima of |q - q_c|, each part over half the patch
+    const float2 ref = tile[c0];
+    float mr = 0.0f, mp = 0.0f;
+    const int q0 = part * ((M::P + 1) / 2), q1 = part ? M::P : (M::P + 1) / 2;
+    for (int q = q0; q < q1; q++) {
+      const float2 v = tile[c0 + sOfs[q]];
+      mr = fmaxf(mr, fabsf(__fsub_rn(v.x, ref.x)));
+      mp = fmaxf(mp, fabsf(__fsub_rn(v.y, ref.y)));
+    }
+    sMx[part][row][0] = mr;
+    sMx[part][row][1] = mp;
   }
   __syncthreads();
-  const float rc = sSc[row][0], pc = sSc[row][1], sr = sSc[row][2], sp = sSc[row][3];
-  const uint32_t aB = smem_u32(msm), bB = smem_u32(msm + C::OFF_B);
-  constexpr uint32_t idesc = bf16_idesc<32>();
-  bool ok = true;
-#pragma unroll 1
-  for (int h = 0; h < C::HALVES; h++) {
-    // this thread's chunks of the half: features k = 8 ch .. 8 ch + 7
-    for (int cl = part; cl < C::NCHH; cl += 2) {
-      const int ch = h * C::NCHH + cl;
-      uint32_t pk[4];
+  if (ok) {
+    const float2 ref = tile[c0];
+    const float sr = mlp_scale(fmaxf(sMx[0][row][0], sMx[1][row][0]), ref.x);
+    const float sp = mlp_scale(fmaxf(sMx[0][row][1], sMx[1][row][1]), ref.y);
+    // features: chunk cq of 8 patch cells gives density chunk cq and pressure
+    // chunk NQC + cq; the parts take alternate chunks
+    for (int cq = part; cq < C::NQC; cq += 2) {
+      uint32_t pr[4], pp[4];
 #pragma unroll
-      for (int t = 0; t < 4; t++) {
-        float x2[2];
+      for (int u = 0; u < 4; u++) {
+        float xr[2], xp[2];
 #pragma unroll
         for (int e = 0; e < 2; e++) {
-          const int kk = ch * 8 + 2 * t + e;
-          float x = 0.0f;
-          if (kk < M::P) x = mlp_feature(tile[0][c0 + sOfs[kk]], rc, sr);
-          else if (kk < M::NI) x = mlp_feature(tile[1][c0 + sOfs[kk - M::P]], pc, sp);
-          x2[e] = live ? x : 0.0f;
+          const int q = cq * 8 + 2 * u + e;
+          xr[e] = xp[e] = 0.0f;
+          if (q < M::P && live) {
+            const float2 v = tile[c0 + sOfs[q]];
+            xr[e] = mlp_feature(v.x, ref.x, sr);
+            xp[e] = mlp_feature(v.y, ref.y, sp);
+          }
         }
-        const __nv_bfloat162 b2 = __floats2bfloat162_rn(x2[0], x2[1]); // .x low half, .y high half
-        pk[t] = *reinterpret_cast<const uint32_t *>(&b2);
+        const __nv_bfloat162 br = __floats2bfloat162_rn(xr[0], xr[1]); // .x low half, .y high half
+        const __nv_bfloat162 bp = __floats2bfloat162_rn(xp[0], xp[1]);
+        pr[u] = *reinterpret_cast<const uint32_t *>(&br);
+        pp[u] = *reinterpret_cast<const uint32_t *>(&bp);
       }
-      st_shared_v4(aB + cl * C::A_CH + row * 16, pk);
+      st_shared_v4(aB + cq * C::A_CH + row * 16, pr);
+      st_shared_v4(aB + (C::NQC + cq) * C::A_CH + row * 16, pp);
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll 1
-      for (int s = 0; s < C::NCHH / 2; s++) {
-        const uint64_t ad = umma_desc(aB + 2 * s * C::A_CH, C::A_CH, 128);
-        const uint64_t bd = umma_desc(bB + (h * C::NCHH + 2 * s) * C::B_CH, C::B_CH, 128);
-        mma_bf16(tmem, ad, bd, idesc, (h > 0 || s > 0) ? 1 : 0);
-      }
-      mma_commit(barA);
-    }
-    ok = mbar_wait(barA, (uint32_t)h & 1u);
-    if (!__syncthreads_and(ok)) break;
   }
-  if (__syncthreads_and(ok)) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  if (ok && tid == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // first layer: bias + GELU of this part's 16 hidden units
-    const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+    constexpr uint32_t idesc1 = bf16_idesc<32>();
+#pragma unroll 1
+    for (int s = 0; s < C::NCH / 2; s++) {
+      const uint64_t ad = umma_desc(aB + 2 * s * C::A_CH, C::A_CH, 128);
+      const uint64_t bd = umma_desc(b1B + 2 * s * C::B_CH, C::B_CH, 128);
+      mma_bf16(tmem, ad, bd, idesc1, s > 0 ? 1 : 0);
+    }
+    mma_commit(barA);
+  }
+  if (ok) ok = mbar_wait(barA, 0u);
+  ok = __syncthreads_and(ok);
+  if (ok) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // H1 = gelu(D1 + b1) of this part's 16 hidden units, split hi + lo into A2
     float z[16];
     tmem_ld8(tmem + lanes + (uint32_t)(16 * part), *reinterpret_cast<float(*)[8]>(z));
     tmem_ld8(tmem + lanes + (uint32_t)(16 * part + 8), *reinterpret_cast<float(*)[8]>(z + 8));
+    const uint32_t aHi = aB, aLo = aB + 8 * C::A_CH;
 #pragma unroll
-    for (int t = 0; t < 16; t++) sH[row][16 * part + t] = gelu(z[t] + sW[16 * part + t]);
-    __syncthreads();
-    // second layer and output on the CUDA cores, 16 outputs per part
-    float acc = 0.0f;
-#pragma unroll 4
-    for (int o = 16 * part; o < 16 * part + 16; o++) {
-      float a = sW[M::B2 - M::B1 + o];
-      const float *wr = sW + (M::W2 - M::B1) + o * M::NH;
+    for (int c = 0; c < 4; c++) {
+      uint32_t hi[4], lo[4];
 #pragma unroll
-      for (int hh = 0; hh < M::NH; hh++) a = fmaf(wr[hh], sH[row][hh], a);
-      acc = fmaf(sW[M::W3 - M::B1 + o], gelu(a), acc);
-    }
-    __syncthreads();
-    if (part == 1) sH[row][32] = acc;   // the second half's sum, read by part 0
-    __syncthreads();
-    if (part == 0 && live) {
-      const float logit = sW[M::B3 - M::B1] + acc + sH[row][32];
-      const int64_t c = (k * g.ny + j) * g.nx + i;
-      if (MODE == 0) {
-        const bool p = logit > logit_thr;
-        pred[c] = p ? 1 : 0;
-        const bool f = p || theta[c] < 1.0;
-        flag[c] = f ? 1 : 0;
-      } else {
-        prob[c] = 1.0f / (1.0f + expf(-logit));
+      for (int u = 0; u < 4; u++) {
+        const int h = 16 * part + 4 * c + u;
+        const float x = gelu(z[4 * c + u] + sW[h]);
+        hi[u] = to_tf32(x);
+        lo[u] = to_tf32(x - __uint_as_float(hi[u]));
       }
+      st_shared_v4(aHi + (4 * part + c) * C::A_CH + row * 16, hi);
+      st_shared_v4(aLo + (4 * part + c) * C::A_CH + row * 16, lo);
     }
-    if (MODE == 0 && part == 0) {
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (ok && tid == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    constexpr uint32_t idesc2 = tf32_idesc<32>();
+    const uint32_t aHi = aB, aLo = aB + 8 * C::A_CH;
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const uint64_t bd = umma_desc(b2B + 2 * s * C::B_CH, C::B_CH, 128);
+      mma_tf32(tmem + 32, umma_desc(aLo + 2 * s * C::A_CH, C::A_CH, 128), bd, idesc2, s > 0 ? 1 : 0);
+      mma_tf32(tmem + 32, umma_desc(aHi + 2 * s * C::A_CH, C::A_CH, 128), bd, idesc2, 1);
+    }
+    mma_commit(barA);
+  }
+  if (ok) ok = mbar_wait(barA, 1u);
+  ok = __syncthreads_and(ok);
+  if (ok) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float z[16];
+    tmem_ld8(tmem + lanes + (uint32_t)(32 + 16 * part), *reinterpret_cast<float(*)[8]>(z));
+    tmem_ld8(tmem + lanes + (uint32_t)(32 + 16 * part + 8), *reinterpret_cast<float(*)[8]>(z + 8));
+    float acc = 0.0f;
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int o = 16 * part + u;
+      acc = fmaf(sW[64 + o], gelu(z[u] + sW[32 + o]), acc);
+    }
+    if (part == 1) sSum[row] = acc;
+    __syncthreads();
+    if (part == 0) {
       bool f = false;
-      if (live) f = flag[(k * g.ny + j) * g.nx + i] != 0;
-      const unsigned ball = __ballot_sync(0xffffffffu, f);
-      if (lane == 0 && ball) atomicAdd(&sc->nflag, (unsigned)__popc(ball));
+      if (live) {
+        const float logit = sW[96] + acc + sSum[row];
+        const int64_t c = (k * g.ny + j) * g.nx + i;
+        if (MODE == 0) {
+          const bool p = logit > logit_thr;
+          pred[c] = p ? 1 : 0;
+          f = p || theta[c] < 1.0;
+          flag[c] = f ? 1 : 0;
+        } else {
+          prob[c] = 1.0f / (1.0f + expf(-logit));
+        }
+      }
+      if (MODE == 0) {
+        const unsigned ball = __ballot_sync(0xffffffffu, f);
+        if (lane == 0 && ball) atomicAdd(&sc->nflag, (unsigned)__popc(ball));
+      }
     }
   } else if (tid == 0) {
     atomicExch(&sc->fault, 1u);
+    mbar_wait(barL, 0u);   // loads still in flight land before the block leaves
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u) : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -416,8 +509,9 @@ static cudaError_t collect_t(const double *U, const Grid &g, const DevStencil *S
 }
 
 template <int DIM, int EQ, int MODE>
-static cudaError_t tc_t(const double *U, const Grid &g, const uint16_t *wb, const uint16_t *img, const double *theta,
-                        uint8_t *flag, uint8_t *pred, float *prob, DevScalars *sc, float thr, cudaStream_t s) {
+static cudaError_t tc_t(const double *U, const Grid &g, float2 *rp, int64_t rpx, const CUtensorMap &map,
+                        const uint8_t *img, const double *theta, uint8_t *flag, uint8_t *pred, float *prob,
+                        DevScalars *sc, float thr, cudaStream_t s) {
   using C = MlpTc<DIM>;
   static bool attr = false;
   if (!attr) {
@@ -426,21 +520,25 @@ static cudaError_t tc_t(const double *U, const Grid &g, const uint16_t *wb, cons
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  mlp_tc_kernel<DIM, EQ, MODE><<<mlp_cell_grid(g), kMlpThreads, C::SMEM, s>>>(U, g, wb, img, theta, flag, pred, prob,
+  const int64_t planes = DIM == 3 ? g.nz + 2 * kRad : 1;
+  const int64_t np = g.px * g.py * planes;
+  mlp_rp_kernel<EQ><<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, g, planes, rpx, rp);
+  mlp_tc_kernel<DIM, EQ, MODE><<<mlp_cell_grid(g), kMlpThreads, C::SMEM, s>>>(map, g, img, theta, flag, pred, prob,
                                                                             sc, thr);
   return cudaGetLastError();
 }
 
 template <int DIM, int EQ>
-static cudaError_t flag_t(const double *U, const Grid &g, const uint16_t *wb, const uint16_t *img,
-                          const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc, float thr, cudaStream_t s) {
-  return tc_t<DIM, EQ, 0>(U, g, wb, img, theta, flag, pred, nullptr, sc, thr, s);
+static cudaError_t flag_t(const double *U, const Grid &g, float2 *rp, int64_t rpx, const CUtensorMap &map,
+                          const uint8_t *img, const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc,
+                          float thr, cudaStream_t s) {
+  return tc_t<DIM, EQ, 0>(U, g, rp, rpx, map, img, theta, flag, pred, nullptr, sc, thr, s);
 }
 
 template <int DIM, int EQ>
-static cudaError_t prob_t(const double *U, const Grid &g, const uint16_t *wb, const uint16_t *img, float *out,
-                          DevScalars *sc, cudaStream_t s) {
-  return tc_t<DIM, EQ, 1>(U, g, wb, img, nullptr, nullptr, nullptr, out, sc, 0.0f, s);
+static cudaError_t prob_t(const double *U, const Grid &g, float2 *rp, int64_t rpx, const CUtensorMap &map,
+                          const uint8_t *img, float *out, DevScalars *sc, cudaStream_t s) {
+  return tc_t<DIM, EQ, 1>(U, g, rp, rpx, map, img, nullptr, nullptr, nullptr, out, sc, 0.0f, s);
 }
 
 #define KFVM_MLP_DISPATCH(DIM_, EQ_, FN, ...)                                      \
@@ -460,23 +558,73 @@ cudaError_t launch_mlp_collect(int dim, int eq, const double *U, const Grid &g, 
   KFVM_MLP_DISPATCH(dim, eq, collect_t, U, g, S, tau, keep, seed, feats, labels, cells, count, cap, s);
 }
 
-cudaError_t launch_mlp_flag(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
-                            const uint16_t *w1img, const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc,
-                            float logit_thr, cudaStream_t s) {
-  KFVM_MLP_DISPATCH(dim, eq, flag_t, U, g, wb, w1img, theta, flag, pred, sc, logit_thr, s);
+cudaError_t launch_mlp_flag(int dim, int eq, const double *U, const Grid &g, const MlpTileBuf &tb, const uint8_t *img,
+                            const double *theta, uint8_t *flag, uint8_t *pred, DevScalars *sc, float logit_thr,
+                            cudaStream_t s) {
+  KFVM_MLP_DISPATCH(dim, eq, flag_t, U, g, tb.rp, tb.rpx, tb.map, img, theta, flag, pred, sc, logit_thr, s);
 }
 
-cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const uint16_t *wb,
-                            const uint16_t *w1img, float *out, DevScalars *sc, cudaStream_t s) {
-  KFVM_MLP_DISPATCH(dim, eq, prob_t, U, g, wb, w1img, out, sc, s);
+cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, const MlpTileBuf &tb, const uint8_t *img,
+                            float *out, DevScalars *sc, cudaStream_t s) {
+  KFVM_MLP_DISPATCH(dim, eq, prob_t, U, g, tb.rp, tb.rpx, tb.map, img, out, sc, s);
 }
 
-int mlp_w1_image_size(int dim) { return dim == 2 ? 32 * MlpTc<2>::KP : 32 * MlpTc<3>::KP; }
+// ---------------------------------------------------------------------------
+// the (density, pressure) pair array and the tensor map of its halo tiles
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-cudaError_t launch_mlp_pack(int dim, const uint16_t *wb, uint16_t *img, cudaStream_t s) {
-  const int n = mlp_w1_image_size(dim);
-  if (dim == 2) mlp_pack_kernel<2><<<(n + 255) / 256, 256, 0, s>>>(wb, img);
-  else mlp_pack_kernel<3><<<(n + 255) / 256, 256, 0, s>>>(wb, img);
+int encode_tensor_map_8b(CUtensorMap *map, const void *base, int rank, const uint64_t *dims,
+                         const uint64_t *strides_bytes, const uint32_t *box) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      return -1;
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return -2;
+  cuuint64_t d[5], st[4];
+  cuuint32_t bx[5], es[5];
+  for (int r = 0; r < rank; r++) {
+    d[r] = dims[r];
+    bx[r] = box[r];
+    es[r] = 1;
+    if (r > 0) {
+      if (strides_bytes[r - 1] % 16 != 0) return -3;
+      st[r - 1] = strides_bytes[r - 1];
+    }
+  }
+  if ((box[0] * 8) % 16 != 0) return -4;
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void *>(base), d, st, bx,
+                        es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -5;
+}
+
+cudaError_t mlp_tile_buf_init(int dim, const Grid &g, MlpTileBuf &tb) {
+  const int64_t planes = dim == 3 ? g.nz + 2 * kRad : 1;
+  tb.rpx = (g.px + 1) / 2 * 2;  // even: every row starts on a 16-byte boundary
+  cudaError_t e = cudaMalloc((void **)&tb.rp, (size_t)(tb.rpx * g.py * planes) * sizeof(float2));
+  if (e != cudaSuccess) return e;
+  const uint64_t dims[3] = {(uint64_t)g.px, (uint64_t)g.py, (uint64_t)planes};
+  const uint64_t strides[2] = {(uint64_t)(tb.rpx * 8), (uint64_t)(tb.rpx * g.py * 8)};
+  const uint32_t box[3] = {dim == 3 ? (uint32_t)MlpTile<3>::TX : (uint32_t)MlpTile<2>::TX,
+                           dim == 3 ? (uint32_t)MlpTile<3>::TY : (uint32_t)MlpTile<2>::TY,
+                           dim == 3 ? (uint32_t)MlpTile<3>::TZ : (uint32_t)MlpTile<2>::TZ};
+  if (encode_tensor_map_8b(&tb.map, tb.rp, 3, dims, strides, box) != 0) return cudaErrorInvalidValue;
+  return cudaSuccess;
+}
+
+int mlp_image_bytes(int dim) { return dim == 2 ? MlpTc<2>::IMG_BYTES : MlpTc<3>::IMG_BYTES; }
+
+cudaError_t launch_mlp_pack(int dim, const uint16_t *wb, const float *wq, uint8_t *img, cudaStream_t s) {
+  const int n = dim == 2 ? 32 * MlpTc<2>::KP : 32 * MlpTc<3>::KP;   // at least the 1024 W2 entries
+  if (dim == 2) mlp_pack_kernel<2><<<(n + 255) / 256, 256, 0, s>>>(wb, wq, img);
+  else mlp_pack_kernel<3><<<(n + 255) / 256, 256, 0, s>>>(wb, wq, img);
   return cudaGetLastError();
 }
 

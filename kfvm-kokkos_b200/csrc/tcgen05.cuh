@@ -59,10 +59,12 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
                : "memory");
 }
 
-// bounded wait for the completion of the mbarrier phase with the given parity
+// bounded wait for the completion of the mbarrier phase with the given parity: an
+// iteration cap and a time limit, the clock read first after 64 polls (a wait
+// that completes quickly never reads the global timer)
 constexpr uint64_t kTcWaitNs = 1000000000ull;
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns = kTcWaitNs) {
-  const uint64_t t0 = global_ns();
+  uint64_t t0 = 0;
   for (uint32_t it = 0; it < (1u << 26); ++it) {
     uint32_t done;
     asm volatile(
@@ -73,7 +75,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((it & 63u) == 63u && global_ns() - t0 > limit_ns) return false;
+    if ((it & 63u) == 63u) {
+      const uint64_t now = global_ns();
+      if (it == 63u) t0 = now;
+      else if (now - t0 > limit_ns) return false;
+    }
   }
   return false;
 }
