@@ -261,6 +261,10 @@ struct kfvm_solver {
   bool writePlot = false;
   int indicator = KFVM_IND_KXRCF;
   int precision = KFVM_PREC_FP64;
+  // TMA maps of the three state buffers for the tensor-core reconstruction's halo
+  // tiles (built when the FP32 form is selected; unused where the pitch is odd)
+  CUtensorMap umap[3];
+  bool umapOk = false;
   int64_t nRhs = 0, nWenoLast = 0;
   int nTS = 1;
   double dmin = 0.0;
@@ -283,7 +287,7 @@ struct kfvm_solver {
     uint16_t *wb = nullptr;             // BF16 weights used by inference
     uint8_t *img = nullptr;             // the inference kernel's weight image (tcgen05 B operands, biases)
     float *wq = nullptr;                // the same values as FP32 (training forward)
-    float *master = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *loss = nullptr;
+    float *master = nullptr, *m = nullptr, *v = nullptr, *loss = nullptr;
     int t = 0;                          // Adam steps taken
     uint8_t *pred = nullptr;            // per-cell prediction of the last evaluation
     kfvm::MlpTileBuf tiles;             // (density, pressure) pairs and their TMA tile map
@@ -291,7 +295,13 @@ struct kfvm_solver {
     uint8_t *labels = nullptr;
     int64_t *cells = nullptr;
     unsigned long long *count = nullptr;
-    int64_t cap = 0, nPos = 0;
+    int64_t cap = 0, nPos = 0, have = 0;
+    uint8_t *flags = nullptr;           // collection scratch: per-cell keep / label flags,
+    int64_t *sel = nullptr, *nsel = nullptr;  // the kept cells in cell order and their count
+    void *selTemp = nullptr;            // device scratch of the stable select
+    size_t selBytes = 0;
+    float *gpart = nullptr, *lpart = nullptr;  // training: per-block gradient rows and losses
+    int gpartBlocks = 0;
     double logitThr = 0.0, judgeFrac = 1.0 / 256.0, tau = 0.3, missLimit = 0.25;
     int fallbackSteps = 0;
     int64_t fallbackEvents = 0;
@@ -412,10 +422,15 @@ int eval_front(kfvm_solver *s, int b) {
   const bool mlpOn = s->indicator == KFVM_IND_MLP && s->mlp.fallbackSteps == 0;
   const bool wantInd = mode == RECON_SPARSE && !mlpOn;
   if (mode != RECON_FULL) {
-    if ((e = run(s, KFVM_KCLASS_RECON, 1, [&] {
-           if (s->precision == KFVM_PREC_TF32X3)
-             return launch_recon_tc(dim, eq, s->Ub[b], s->g, s->dS, wantInd, s->F, s->W, s->src, s->status,
+    if ((e = run(s, KFVM_KCLASS_RECON, s->precision == KFVM_PREC_TF32X3 ? 2 : 1, [&] {
+           if (s->precision == KFVM_PREC_TF32X3) {
+             // the limiter bounds of every cell, then the linear states
+             cudaError_t eb = launch_bounds(dim, eq, s->Ub[b], s->g, s->bnd, st);
+             if (eb != cudaSuccess) return eb;
+             return launch_recon_tc(dim, eq, s->Ub[b], s->umapOk ? &s->umap[b] : nullptr, s->g, s->dS, wantInd,
+                                    s->F, s->W, s->src, s->status,
                                     s->lamvel, s->bnd, s->sc, st);
+           }
            return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, wantInd, s->F, s->W, s->src, s->status, s->lamvel,
                                s->bnd, st);
          })) != cudaSuccess)
@@ -905,7 +920,12 @@ void kfvm_destroy(kfvm_solver *s) {
   cudaFree(s->mlp.master);
   cudaFree(s->mlp.m);
   cudaFree(s->mlp.v);
-  cudaFree(s->mlp.grad);
+  cudaFree(s->mlp.gpart);
+  cudaFree(s->mlp.lpart);
+  cudaFree(s->mlp.flags);
+  cudaFree(s->mlp.sel);
+  cudaFree(s->mlp.nsel);
+  cudaFree(s->mlp.selTemp);
   cudaFree(s->mlp.loss);
   cudaFree(s->mlp.pred);
   cudaFree(s->mlp.img);
@@ -1043,6 +1063,12 @@ int kfvm_set_precision(kfvm_solver *s, int32_t precision) {
     if (major != 10) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form needs an sm_100 device");
     if (s->g.nq != 2) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form is built for 2 Gauss points");
     if (s->eq == KFVM_EQ_SRHYDRO) return fail(KFVM_ERR_ARG, "the TF32 tensor-core form is built for the Euler / GLM-MHD paths");
+    if (!s->umapOk) {
+      bool all = true;
+      for (int b = 0; b < 3; b++)
+        all = all && kfvm::recon_tc_state_map(&s->umap[b], s->Ub[b], s->g, s->dim, s->nv) == 0;
+      s->umapOk = all;
+    }
   }
   s->precision = precision;
   return KFVM_OK;
@@ -1076,14 +1102,12 @@ int mlp_alloc(kfvm_solver *s) {
       (e = cudaMalloc((void **)&M.master, M.nw * sizeof(float))) != cudaSuccess ||
       (e = cudaMalloc((void **)&M.m, M.nw * sizeof(float))) != cudaSuccess ||
       (e = cudaMalloc((void **)&M.v, M.nw * sizeof(float))) != cudaSuccess ||
-      (e = cudaMalloc((void **)&M.grad, M.nw * sizeof(float))) != cudaSuccess ||
       (e = cudaMalloc((void **)&M.loss, 4 * sizeof(float))) != cudaSuccess ||
       (e = cudaMalloc((void **)&M.pred, s->g.n)) != cudaSuccess ||
       (e = cudaMalloc((void **)&M.img, kfvm::mlp_image_bytes(s->dim))) != cudaSuccess ||
       (e = kfvm::mlp_tile_buf_init(s->dim, s->g, M.tiles)) != cudaSuccess)
     return set_err_cuda(e, "learned indicator buffers");
   CK(cudaMemsetAsync(M.pred, 0, s->g.n, s->stream));
-  CK(cudaMemsetAsync(M.grad, 0, M.nw * sizeof(float), s->stream));
   return KFVM_OK;
 }
 
@@ -1172,8 +1196,17 @@ int kfvm_mlp_reserve(kfvm_solver *s, int64_t capacity) {
     M.cap = 0;
     return set_err_cuda(e, "sample buffer");
   }
+  if (!M.flags) {
+    M.selBytes = kfvm::mlp_select_temp_bytes(s->g.n);
+    if ((e = cudaMalloc((void **)&M.flags, (size_t)s->g.n)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&M.sel, (size_t)s->g.n * sizeof(int64_t))) != cudaSuccess ||
+        (e = cudaMalloc((void **)&M.nsel, sizeof(int64_t))) != cudaSuccess ||
+        (e = cudaMalloc(&M.selTemp, M.selBytes > 0 ? M.selBytes : 16)) != cudaSuccess)
+      return set_err_cuda(e, "sample selection scratch");
+  }
   M.cap = capacity;
   M.nPos = 0;
+  M.have = 0;
   CK(cudaMemsetAsync(M.count, 0, sizeof(unsigned long long), s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return KFVM_OK;
@@ -1188,15 +1221,27 @@ int kfvm_mlp_collect(kfvm_solver *s, double tau, double keep_frac, uint64_t seed
   const int b = s->iCur;
   cudaError_t e = run(s, KFVM_KCLASS_BC, 1, [&] { return kfvm::launch_bc(s->dim, s->eq, s->Ub[b], s->g, s->stream); });
   if (e != cudaSuccess) return set_err_cuda(e, "bc");
-  e = run(s, KFVM_KCLASS_OTHER, 1, [&] {
-    return kfvm::launch_mlp_collect(s->dim, s->eq, s->Ub[b], s->g, s->dS, tau, keep_frac, seed, M.feats, M.labels,
-                                    M.cells, M.count, M.cap, s->stream);
+  // labels, pairs, then the kept cells in cell order (a stable select)
+  e = run(s, KFVM_KCLASS_OTHER, 3, [&] {
+    return kfvm::launch_mlp_select(s->dim, s->eq, s->Ub[b], s->g, s->dS, tau, keep_frac, seed, M.tiles, M.flags,
+                                   M.sel, M.nsel, M.selTemp, M.selBytes, s->stream);
   });
   if (e != cudaSuccess) return set_err_cuda(e, "collect");
-  unsigned long long cnt = 0;
-  CK(cudaMemcpyAsync(&cnt, M.count, sizeof(cnt), cudaMemcpyDeviceToHost, s->stream));
+  int64_t nsel = 0;
+  CK(cudaMemcpyAsync(&nsel, M.nsel, sizeof(nsel), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
-  const int64_t have = std::min<int64_t>((int64_t)cnt, M.cap);
+  // appended after the samples of earlier calls, up to the capacity
+  const int64_t take = std::min<int64_t>(nsel, M.cap - M.have);
+  e = run(s, KFVM_KCLASS_OTHER, 1, [&] {
+    return kfvm::launch_mlp_features(s->dim, s->g, M.tiles, M.sel, take, M.flags, M.feats + M.have * M.ni,
+                                     M.labels + M.have, M.cells + M.have, s->stream);
+  });
+  if (e != cudaSuccess) return set_err_cuda(e, "collect features");
+  M.have += take;
+  const unsigned long long cnt = (unsigned long long)M.have;
+  CK(cudaMemcpyAsync(M.count, &cnt, sizeof(cnt), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const int64_t have = M.have;
   std::vector<uint8_t> lab(have);
   if (have) CK(cudaMemcpy(lab.data(), M.labels, have, cudaMemcpyDeviceToHost));
   int64_t pos = 0;
@@ -1231,6 +1276,18 @@ int kfvm_mlp_train(kfvm_solver *s, int32_t steps, int32_t batch, double lr, doub
   if (M.count) CK(cudaMemcpy(&cnt, M.count, sizeof(cnt), cudaMemcpyDeviceToHost));
   const int64_t n = std::min<int64_t>((int64_t)cnt, M.cap);
   if (n <= 0) return fail(KFVM_ERR_STATE, "no collected samples (kfvm_mlp_collect)");
+  const int blocks = kfvm::mlp_train_blocks(batch);
+  if (M.gpartBlocks < blocks) {
+    cudaFree(M.gpart);
+    cudaFree(M.lpart);
+    M.gpart = M.lpart = nullptr;
+    M.gpartBlocks = 0;
+    cudaError_t ea;
+    if ((ea = cudaMalloc((void **)&M.gpart, (size_t)blocks * M.nw * sizeof(float))) != cudaSuccess ||
+        (ea = cudaMalloc((void **)&M.lpart, (size_t)blocks * sizeof(float))) != cudaSuccess)
+      return set_err_cuda(ea, "training scratch");
+    M.gpartBlocks = blocks;
+  }
   // loss slots: [0] mean over the first 20 steps, [1] over the last 20, [2] the rest
   CK(cudaMemsetAsync(M.loss, 0, 4 * sizeof(float), s->stream));
   const int win = std::min(20, steps);
@@ -1238,9 +1295,9 @@ int kfvm_mlp_train(kfvm_solver *s, int32_t steps, int32_t batch, double lr, doub
     float *slot = i < win ? M.loss : (i >= steps - win ? M.loss + 1 : M.loss + 2);
     M.t++;
     cudaError_t e = run(s, KFVM_KCLASS_OTHER, 2, [&] {
-      return kfvm::launch_mlp_train_step(s->dim, M.feats, M.labels, n, batch, M.master, M.m, M.v, M.grad, M.wq,
-                                         M.wb, slot, (float)pos_weight, (float)lr, M.t, seed ^ (uint64_t)M.t,
-                                         s->stream);
+      return kfvm::launch_mlp_train_step(s->dim, M.feats, M.labels, n, batch, M.master, M.m, M.v, M.gpart, M.lpart,
+                                         M.wq, M.wb, slot, (float)pos_weight, (float)lr, M.t,
+                                         seed ^ (uint64_t)M.t, s->stream);
     });
     if (e != cudaSuccess) return set_err_cuda(e, "train");
   }

@@ -142,7 +142,8 @@ __global__ void __launch_bounds__(128)
   const int64_t k = blockIdx.z;
   pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)kBlockX, blockIdx.y * (int64_t)kBlockY, k, tile);
   __syncthreads();
-  // limiter bounds of each block cell, once (the four lanes of a cell share them)
+  // limiter bounds of each block cell, once (the four lanes of a cell share them);
+  // computed here, where the other resident blocks' contraction hides their loads
   __shared__ double sBd[3][kBlockX * kBlockY];
   {
     const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
@@ -285,6 +286,26 @@ __global__ void __launch_bounds__(128)
       if constexpr (T::SRC) lamvel[c] = make_double2(lam, vel);
       status[c] = inside ? 1 : 0;
     }
+  }
+}
+
+// PositivityPreserve_K bounds of every cell (Common_K.H:331-380; SR: SRHydro_K.H:224-246)
+// from a per-block footprint tile: [minDens | maxDens | minEint][cell], the same
+// values recon_kernel computes in its own prologue.  The pre-pass of the tensor-core
+// reconstruction, whose shared memory holds the halo tiles instead.
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(128) bounds_kernel(const double *__restrict__ U, Grid g, double *__restrict__ bnd) {
+  __shared__ double tile[6][PosTile<DIM>::N];
+  const int64_t k = blockIdx.z;
+  pos_tile_fill<DIM, EQ>(U, g, blockIdx.x * (int64_t)kBlockX, blockIdx.y * (int64_t)kBlockY, k, tile);
+  __syncthreads();
+  const int64_t i = blockIdx.x * (int64_t)kBlockX + threadIdx.x, j = blockIdx.y * (int64_t)kBlockY + threadIdx.y;
+  if (i < g.nx && j < g.ny) {
+    const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, threadIdx.x, threadIdx.y);
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    bnd[c] = bd.minDens;
+    bnd[g.n + c] = bd.maxDens;
+    bnd[2 * g.n + c] = bd.minEint;
   }
 }
 
@@ -1394,6 +1415,10 @@ struct Launch {
     bc_fill_kernel<DIM, NV><<<(unsigned)(blocks < 65535 * 16 ? blocks : 65535 * 16), 256, 0, s>>>(U, g);
     return cudaGetLastError();
   }
+  static cudaError_t bounds(const double *U, const Grid &g, double *bnd, cudaStream_t s) {
+    bounds_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, bnd);
+    return cudaGetLastError();
+  }
   static cudaError_t recon(const double *U, const Grid &g, const DevStencil *S, int wantInd,
                            double *const *F, float *const *W, double *src, uint8_t *status,
                            double2 *lamvel, double *bnd, cudaStream_t s) {
@@ -1576,6 +1601,10 @@ cudaError_t launch_fill(double *p, int64_t n, double val, cudaStream_t s) {
 cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s) {
   KFVM_DISPATCH(dim, eq, bc(U, g, s));
 }
+cudaError_t launch_bounds(int dim, int eq, const double *U, const Grid &g, double *bnd, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, bounds(U, g, bnd, s));
+}
+
 cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
                          double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
                          double *bnd, cudaStream_t s) {

@@ -36,17 +36,22 @@ cudaError_t launch_fill(double *p, int64_t n, double val, cudaStream_t s);
 // rcp_nr accuracy probe: out[0] = max ulp distance to 1/y, out[1] = bits of the
 // largest relative difference of x * rcp_nr(y) from x / y
 cudaError_t launch_rcp_probe(int64_t n, uint64_t seed, unsigned long long *out, cudaStream_t s);
+// limiter bounds of every cell, [minDens | maxDens | minEint][cell] (the pre-pass
+// of the reconstruction kernels, which read them)
+cudaError_t launch_bounds(int dim, int eq, const double *U, const Grid &g, double *bnd, cudaStream_t s);
 // stage front end: linear states + KXRCF indicator + limiter bound status,
 // KXRCF flags, WENO decision / heavy-list compaction, heavy cells
-// bnd: the limiter bounds of every cell, [minDens | maxDens | minEint][cell], for the heavy pass
+// bnd: the limiter bounds of every cell from launch_bounds
 cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
                          double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
                          double *bnd, cudaStream_t s);
 // the same outputs with the stencil sum on the tcgen05 tensor cores (3xTF32);
-// a block whose wait for the MMA completion gave up sets sc->fault
-cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                            double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
-                            double *bnd, DevScalars *sc, cudaStream_t s);
+// umap (recon_tc_state_map of U) stages the halo tiles by TMA, null loads them
+// with plain global loads; a block whose wait gave up sets sc->fault
+cudaError_t launch_recon_tc(int dim, int eq, const double *U, const CUtensorMap *umap, const Grid &g,
+                            const DevStencil *S, int wantInd, double *const *F, float *const *W, double *src,
+                            uint8_t *status, double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s);
+int recon_tc_state_map(CUtensorMap *map, const double *U, const Grid &g, int dim, int nv);
 // self-test of the bounded mbarrier wait: out[0] = gave up, out[1] = ns waited
 cudaError_t launch_wait_probe(uint64_t limit_ns, unsigned long long *out, cudaStream_t s);
 // host: split the [cell][row] linear weights of S into the TF32 B-operand tables
@@ -73,9 +78,18 @@ cudaError_t launch_stage(int dim, int eq, const StageArgs &a, const Grid &g, cud
 // learned troubled-cell indicator (mlp.cu)
 int mlp_num_weights(int dim);
 int mlp_num_inputs(int dim);
-cudaError_t launch_mlp_collect(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, double tau,
-                               double keep, uint64_t seed, uint16_t *feats, uint8_t *labels, int64_t *cells,
-                               unsigned long long *count, int64_t cap, cudaStream_t s);
+// sample collection in cell order: labels and keep decisions of every cell into
+// flags, the (density, pressure) pairs into tb, and the kept cells' indices
+// compacted into sel (*nsel of them; temp: mlp_select_temp_bytes(g.n) bytes of
+// device scratch); then the features of the first `count` of them
+size_t mlp_select_temp_bytes(int64_t n);
+struct MlpTileBuf;
+cudaError_t launch_mlp_select(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, double tau,
+                              double keep, uint64_t seed, const MlpTileBuf &tb, uint8_t *flags, int64_t *sel,
+                              int64_t *nsel, void *temp, size_t temp_bytes, cudaStream_t s);
+cudaError_t launch_mlp_features(int dim, const Grid &g, const MlpTileBuf &tb, const int64_t *sel, int64_t count,
+                                const uint8_t *flags, uint16_t *feats, uint8_t *labels, int64_t *cells,
+                                cudaStream_t s);
 // inference: the (density, pressure) pairs of every padded cell (one kernel), then
 // per block a TMA load of its halo tile of pairs plus bulk loads of the weight image,
 // and the network with both matrix layers on tcgen05 (layer 1 BF16, layer 2 split
@@ -96,9 +110,13 @@ cudaError_t launch_mlp_prob(int dim, int eq, const double *U, const Grid &g, con
 // weights wb and their FP32 values wq, after every change of the weights
 int mlp_image_bytes(int dim);
 cudaError_t launch_mlp_pack(int dim, const uint16_t *wb, const float *wq, uint8_t *img, cudaStream_t s);
+// one training step: per-block gradient rows in gpart (mlp_train_blocks(batch) x
+// weights) and losses in lpart, summed in block order by the Adam update
+int mlp_train_blocks(int batch);
 cudaError_t launch_mlp_train_step(int dim, const uint16_t *feats, const uint8_t *labels, int64_t n, int batch,
-                                  float *master, float *m, float *v, float *grad, float *wq, uint16_t *wb,
-                                  float *loss, float pos_weight, float lr, int t, uint64_t seed, cudaStream_t s);
+                                  float *master, float *m, float *v, float *gpart, float *lpart, float *wq,
+                                  uint16_t *wb, float *loss, float pos_weight, float lr, int t, uint64_t seed,
+                                  cudaStream_t s);
 cudaError_t launch_stage_pre(int dim, int eq, double *U1, const double *Uprev, double *Uhat,
                              double *Utmp, const double *K, const Grid &g, double betaDt,
                              double bhatDt, int use_tmp, cudaStream_t s);

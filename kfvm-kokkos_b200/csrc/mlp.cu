@@ -12,8 +12,11 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <thrust/iterator/counting_iterator.h>
+
 #include <algorithm>
 #include <cstdint>
+#include <cub/device/device_select.cuh>
 
 #include "kernels.cuh"
 #include "launch.h"
@@ -24,48 +27,65 @@
 namespace kfvm {
 
 // ---------------------------------------------------------------------------
-// sample collection: every cell's label; positives always kept, negatives with
-// probability keep_frac; features stored as BF16
+// sample collection, in a fixed order: (1) every cell's label and keep decision
+// (positives always kept, negatives with probability keep_frac by a hash of the
+// cell); (2) the kept cells compacted in cell order (a stable select); (3) their
+// features from the (density, pressure) pairs, stored as BF16.  The set and its
+// order repeat exactly, so training on it does too.
 template <int DIM, int EQ>
-__global__ void __launch_bounds__(128)
-    mlp_collect_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, double tau,
-                       double keep_frac, uint64_t seed, uint16_t *__restrict__ feats, uint8_t *__restrict__ labels,
-                       int64_t *__restrict__ cells, unsigned long long *__restrict__ count, int64_t cap) {
-  using M = MlpShape<DIM>;
-  using Tl = MlpTile<DIM>;
-  __shared__ float tile[2][Tl::N];
-  const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY, k = blockIdx.z;
-  mlp_tile_fill<DIM, EQ>(U, g, i0, j0, k, tile);
-  __syncthreads();
-  const int64_t i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-  if (i >= g.nx || j >= g.ny) return;
-  const int64_t c = (k * g.ny + j) * g.nx + i;
+__global__ void __launch_bounds__(256)
+    mlp_label_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, double tau,
+                     double keep_frac, uint64_t seed, uint8_t *__restrict__ flags) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= g.n) return;
+  const int64_t i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
   const double dep = weno_departure<DIM, EQ>(U + pidx(g, i, j, k), g, S);
   const bool pos = dep > tau;
-  if (!pos && !(unit_hash(seed, (uint64_t)c) < keep_frac)) return;
-  const unsigned long long idx = atomicAdd(count, 1ull);
-  if ((int64_t)idx >= cap) return;
-  float rc, pc, sr, sp;
-  mlp_scales<DIM>(tile, threadIdx.x, threadIdx.y, rc, pc, sr, sp);
-  constexpr int R = Tl::R, ZR = DIM == 3 ? R : 0;
-  const int c0 = (ZR * Tl::TY + threadIdx.y + R) * Tl::TX + threadIdx.x + R;
-  uint16_t *x = feats + (int64_t)idx * M::NI;
+  const bool keep = pos || unit_hash(seed, (uint64_t)c) < keep_frac;
+  flags[c] = keep ? (pos ? 3 : 1) : 0;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128)
+    mlp_feature_kernel(const float2 *__restrict__ rp, int64_t rpx, Grid g, const int64_t *__restrict__ sel,
+                       int64_t count, const uint8_t *__restrict__ flags, uint16_t *__restrict__ feats,
+                       uint8_t *__restrict__ labels, int64_t *__restrict__ cells) {
+  using M = MlpShape<DIM>;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const int64_t c = sel[t];
+  const int64_t i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+  const float2 *p0 = rp + ((k + g.rz) * g.py + j + kRad) * rpx + i + kRad;
+  constexpr int R = M::R, ZR = DIM == 3 ? R : 0;
+  const float rc = p0->x, pc = p0->y;
+  float mr = 0.0f, mp = 0.0f;
+  for (int dz = -ZR; dz <= ZR; dz++)
+    for (int dy = -R; dy <= R; dy++)
+      for (int dx = -R; dx <= R; dx++) {
+        const float2 q = p0[(dz * g.py + dy) * rpx + dx];
+        mr = fmaxf(mr, fabsf(__fsub_rn(q.x, rc)));
+        mp = fmaxf(mp, fabsf(__fsub_rn(q.y, pc)));
+      }
+  const float sr = mlp_scale(mr, rc), sp = mlp_scale(mp, pc);
+  uint16_t *x = feats + t * M::NI;
   int q = 0;
   for (int dz = -ZR; dz <= ZR; dz++)
     for (int dy = -R; dy <= R; dy++)
       for (int dx = -R; dx <= R; dx++, q++) {
-        const int n = c0 + (dz * Tl::TY + dy) * Tl::TX + dx;
-        x[q] = __bfloat16_as_ushort(__float2bfloat16_rn(mlp_feature(tile[0][n], rc, sr)));
-        x[M::P + q] = __bfloat16_as_ushort(__float2bfloat16_rn(mlp_feature(tile[1][n], pc, sp)));
+        const float2 v = p0[(dz * g.py + dy) * rpx + dx];
+        x[q] = __bfloat16_as_ushort(__float2bfloat16_rn(mlp_feature(v.x, rc, sr)));
+        x[M::P + q] = __bfloat16_as_ushort(__float2bfloat16_rn(mlp_feature(v.y, pc, sp)));
       }
-  labels[idx] = pos ? 1 : 0;
-  cells[idx] = c;
+  labels[t] = flags[c] >> 1;
+  cells[t] = c;
 }
 
 // ---------------------------------------------------------------------------
 // training: one block = kTrainB samples drawn uniformly (with replacement) from
-// the collected set; forward and backward in FP32 with the BF16-rounded weights,
-// gradients of the weighted binary cross entropy summed into grad
+// the collected set; forward and backward in FP32 with the BF16-rounded weights;
+// the block's gradient of the weighted binary cross entropy goes to its own row
+// of gpart and its loss to lpart (summed in block order by the Adam kernel, so a
+// training run repeats bit for bit)
 constexpr int kTrainB = 64;
 
 template <int DIM>
@@ -88,7 +108,7 @@ struct TrainSmem {
 template <int DIM>
 __global__ void __launch_bounds__(256)
     mlp_train_kernel(const uint16_t *__restrict__ feats, const uint8_t *__restrict__ labels, int64_t n,
-                     const float *__restrict__ w, float *__restrict__ grad, float *__restrict__ loss,
+                     const float *__restrict__ w, float *__restrict__ gpart, float *__restrict__ lpart,
                      float pos_weight, float inv_batch, uint64_t seed, int64_t step) {
   using M = MlpShape<DIM>;
   using L = TrainSmem<DIM>;
@@ -133,7 +153,7 @@ __global__ void __launch_bounds__(256)
     const float p = 1.0f / (1.0f + expf(-z));
     // weighted BCE on the logit: wt (softplus(z) - y z)
     const float sp = z > 0.0f ? z + log1pf(expf(-z)) : log1pf(expf(z));
-    atomicAdd(loss, wt * (sp - y * z) * inv_batch);
+    LB[tid] = wt * (sp - y * z) * inv_batch;   // the label is not read again
     DY[tid] = wt * (p - y) * inv_batch;
   }
   __syncthreads();
@@ -168,19 +188,31 @@ __global__ void __launch_bounds__(256)
     } else {
       for (int s = 0; s < kTrainB; s++) a += DY[s];
     }
-    atomicAdd(grad + t, a);
+    gpart[(int64_t)blockIdx.x * M::NW + t] = a;
+  }
+  if (tid == 0) {
+    float l = 0.0f;
+    for (int q = 0; q < kTrainB; q++) l += LB[q];
+    lpart[blockIdx.x] = l;
   }
 }
 
-// Adam on the FP32 master weights; the forward passes use their BF16 rounding
+// Adam on the FP32 master weights with the gradient summed over the blocks'
+// rows in block order; the forward passes use the weights' BF16 rounding
 __global__ void __launch_bounds__(256)
     mlp_adam_kernel(float *__restrict__ master, float *__restrict__ m, float *__restrict__ v,
-                    float *__restrict__ grad, float *__restrict__ wq, uint16_t *__restrict__ wb, int nw, float lr,
+                    const float *__restrict__ gpart, const float *__restrict__ lpart, int blocks,
+                    float *__restrict__ loss, float *__restrict__ wq, uint16_t *__restrict__ wb, int nw, float lr,
                     float c1, float c2) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    float l = 0.0f;
+    for (int b = 0; b < blocks; b++) l += lpart[b];
+    *loss += l;
+  }
   if (t >= nw) return;
-  const float gr = grad[t];
-  grad[t] = 0.0f;
+  float gr = 0.0f;
+  for (int b = 0; b < blocks; b++) gr += gpart[(int64_t)b * nw + t];
   const float mt = 0.9f * m[t] + 0.1f * gr, vt = 0.999f * v[t] + 0.001f * gr * gr;
   m[t] = mt;
   v[t] = vt;
@@ -500,11 +532,17 @@ int mlp_num_weights(int dim) { return dim == 2 ? MlpShape<2>::NW : MlpShape<3>::
 int mlp_num_inputs(int dim) { return dim == 2 ? MlpShape<2>::NI : MlpShape<3>::NI; }
 
 template <int DIM, int EQ>
-static cudaError_t collect_t(const double *U, const Grid &g, const DevStencil *S, double tau, double keep,
-                             uint64_t seed, uint16_t *feats, uint8_t *labels, int64_t *cells,
-                             unsigned long long *count, int64_t cap, cudaStream_t s) {
-  mlp_collect_kernel<DIM, EQ><<<mlp_cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, S, tau, keep, seed, feats,
-                                                                                   labels, cells, count, cap);
+static cudaError_t label_t(const double *U, const Grid &g, const DevStencil *S, double tau, double keep,
+                           uint64_t seed, uint8_t *flags, cudaStream_t s) {
+  mlp_label_kernel<DIM, EQ><<<(unsigned)((g.n + 255) / 256), 256, 0, s>>>(U, g, S, tau, keep, seed, flags);
+  return cudaGetLastError();
+}
+
+template <int DIM, int EQ>
+static cudaError_t rp_t(const double *U, const Grid &g, float2 *rp, int64_t rpx, cudaStream_t s) {
+  const int64_t planes = DIM == 3 ? g.nz + 2 * kRad : 1;
+  const int64_t np = g.px * g.py * planes;
+  mlp_rp_kernel<EQ><<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, g, planes, rpx, rp);
   return cudaGetLastError();
 }
 
@@ -552,10 +590,32 @@ static cudaError_t prob_t(const double *U, const Grid &g, float2 *rp, int64_t rp
     return cudaErrorInvalidValue;                                                \
   } while (0)
 
-cudaError_t launch_mlp_collect(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, double tau,
-                               double keep, uint64_t seed, uint16_t *feats, uint8_t *labels, int64_t *cells,
-                               unsigned long long *count, int64_t cap, cudaStream_t s) {
-  KFVM_MLP_DISPATCH(dim, eq, collect_t, U, g, S, tau, keep, seed, feats, labels, cells, count, cap, s);
+size_t mlp_select_temp_bytes(int64_t n) {
+  size_t bytes = 0;
+  cub::DeviceSelect::Flagged(nullptr, bytes, thrust::counting_iterator<int64_t>(0), (const uint8_t *)nullptr,
+                             (int64_t *)nullptr, (int64_t *)nullptr, n);
+  return bytes;
+}
+
+cudaError_t launch_mlp_select(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, double tau,
+                              double keep, uint64_t seed, const MlpTileBuf &tb, uint8_t *flags, int64_t *sel,
+                              int64_t *nsel, void *temp, size_t temp_bytes, cudaStream_t s) {
+  cudaError_t e;
+  auto labels = [&]() -> cudaError_t { KFVM_MLP_DISPATCH(dim, eq, label_t, U, g, S, tau, keep, seed, flags, s); };
+  auto pairs = [&]() -> cudaError_t { KFVM_MLP_DISPATCH(dim, eq, rp_t, U, g, tb.rp, tb.rpx, s); };
+  if ((e = labels()) != cudaSuccess || (e = pairs()) != cudaSuccess) return e;
+  return cub::DeviceSelect::Flagged(temp, temp_bytes, thrust::counting_iterator<int64_t>(0), flags, sel, nsel, g.n,
+                                    s);
+}
+
+cudaError_t launch_mlp_features(int dim, const Grid &g, const MlpTileBuf &tb, const int64_t *sel, int64_t count,
+                                const uint8_t *flags, uint16_t *feats, uint8_t *labels, int64_t *cells,
+                                cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)((count + 127) / 128);
+  if (dim == 2) mlp_feature_kernel<2><<<blocks, 128, 0, s>>>(tb.rp, tb.rpx, g, sel, count, flags, feats, labels, cells);
+  else mlp_feature_kernel<3><<<blocks, 128, 0, s>>>(tb.rp, tb.rpx, g, sel, count, flags, feats, labels, cells);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_mlp_flag(int dim, int eq, const double *U, const Grid &g, const MlpTileBuf &tb, const uint8_t *img,
@@ -629,9 +689,10 @@ cudaError_t launch_mlp_pack(int dim, const uint16_t *wb, const float *wq, uint8_
 }
 
 cudaError_t launch_mlp_train_step(int dim, const uint16_t *feats, const uint8_t *labels, int64_t n, int batch,
-                                  float *master, float *m, float *v, float *grad, float *wq, uint16_t *wb,
-                                  float *loss, float pos_weight, float lr, int t, uint64_t seed, cudaStream_t s) {
-  const int blocks = (batch + kTrainB - 1) / kTrainB;
+                                  float *master, float *m, float *v, float *gpart, float *lpart, float *wq,
+                                  uint16_t *wb, float *loss, float pos_weight, float lr, int t, uint64_t seed,
+                                  cudaStream_t s) {
+  const int blocks = mlp_train_blocks(batch);
   const float inv = 1.0f / (float)(blocks * kTrainB);
   cudaError_t e;
   if (dim == 2) {
@@ -640,22 +701,25 @@ cudaError_t launch_mlp_train_step(int dim, const uint16_t *feats, const uint8_t 
                                            (int)TrainSmem<2>::BYTES)) != cudaSuccess)
       return e;
     attr = true;
-    mlp_train_kernel<2><<<blocks, 256, TrainSmem<2>::BYTES, s>>>(feats, labels, n, wq, grad, loss, pos_weight, inv,
-                                                                 seed, t);
+    mlp_train_kernel<2><<<blocks, 256, TrainSmem<2>::BYTES, s>>>(feats, labels, n, wq, gpart, lpart, pos_weight,
+                                                                 inv, seed, t);
   } else {
     static bool attr = false;
     if (!attr && (e = cudaFuncSetAttribute(mlp_train_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)TrainSmem<3>::BYTES)) != cudaSuccess)
       return e;
     attr = true;
-    mlp_train_kernel<3><<<blocks, 256, TrainSmem<3>::BYTES, s>>>(feats, labels, n, wq, grad, loss, pos_weight, inv,
-                                                                 seed, t);
+    mlp_train_kernel<3><<<blocks, 256, TrainSmem<3>::BYTES, s>>>(feats, labels, n, wq, gpart, lpart, pos_weight,
+                                                                 inv, seed, t);
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int nw = mlp_num_weights(dim);
   const float c1 = 1.0f / (1.0f - powf(0.9f, (float)t)), c2 = 1.0f / (1.0f - powf(0.999f, (float)t));
-  mlp_adam_kernel<<<(nw + 255) / 256, 256, 0, s>>>(master, m, v, grad, wq, wb, nw, lr, c1, c2);
+  mlp_adam_kernel<<<(nw + 255) / 256, 256, 0, s>>>(master, m, v, gpart, lpart, blocks, loss, wq, wb, nw, lr, c1,
+                                                   c2);
   return cudaGetLastError();
 }
+
+int mlp_train_blocks(int batch) { return (batch + kTrainB - 1) / kTrainB; }
 
 } // namespace kfvm

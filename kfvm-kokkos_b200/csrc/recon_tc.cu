@@ -20,8 +20,8 @@
 //
 // Per block (256 threads, two per cell = per row of the tile, 128 cells):
 //   warp 0 allocates the TMEM columns (variables x N, rounded to a power of two)
-//   the split weights (B, hi and lo) and the limiter footprint tile are loaded,
-//     and the limiter bounds of each cell are computed once
+//   the split weights (B, hi and lo) are loaded and each cell's limiter bounds
+//     read (bounds_kernel computed them)
 //   per variable: the two threads of a row write its A row (hi and lo, half of
 //     the K chunks each) into shared memory in the canonical K-major no-swizzle
 //     layout (8-row x 16-byte core matrices); thread 0 issues 3 MMAs per K step
@@ -45,6 +45,7 @@
 #include "launch.h"
 #include "recon_common.cuh"
 #include "tcgen05.cuh"
+#include "tma.cuh"
 
 namespace kfvm {
 
@@ -71,8 +72,7 @@ struct TcShape {
   static constexpr int B_CH = NP * 16;
   static constexpr int B_PART = NCH * B_CH;
   static constexpr int OFF_B = 2 * A_PART;
-  static constexpr int OFF_TILE = OFF_B + 2 * B_PART;
-  static constexpr int OFF_BD = OFF_TILE + 6 * PosTile<DIM>::N * (int)sizeof(double); // bounds [3][128]
+  static constexpr int OFF_BD = OFF_B + 2 * B_PART;   // limiter bounds of the block's cells [3][128]
   static constexpr int OFF_RED = OFF_BD + 3 * 128 * (int)sizeof(double);              // lam, vel [2][128], in-bounds [128]
   static constexpr int OFF_BAR = OFF_RED + 2 * 128 * 8 + 128 * 4;
   static constexpr int USED = OFF_BAR + 16;
@@ -100,7 +100,6 @@ __global__ void __launch_bounds__(kTcThreads, 2)
   using Sh = TcShape<DIM, EQ>;
   constexpr int NV = T::NV;
   extern __shared__ __align__(128) uint8_t smem[];
-  double(*tile)[PosTile<DIM>::N] = reinterpret_cast<double(*)[PosTile<DIM>::N]>(smem + Sh::OFF_TILE);
   double(*sBd)[128] = reinterpret_cast<double(*)[128]>(smem + Sh::OFF_BD);
   unsigned long long *sLam = reinterpret_cast<unsigned long long *>(smem + Sh::OFF_RED);
   unsigned long long *sVel = sLam + 128;
@@ -138,48 +137,23 @@ __global__ void __launch_bounds__(kTcThreads, 2)
       dl[t] = bl[t];
     }
   }
-  {
-    // the footprint tile, filled by all threads (pos_tile_fill strides by blockDim)
-    using P = PosTile<DIM>;
-    const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY;
-    for (int t = tid; t < P::N; t += kTcThreads) {
-      const int a = t % P::TX, b = (t / P::TX) % P::TY, cz = t / (P::TX * P::TY);
-      const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b, gk = k - (DIM == 3 ? 1 : 0) + cz;
-      if (gi > g.nx || gj > g.ny) continue;
-      const double *Uq = U + pidx(g, gi, gj, gk);
-      double st[NV];
-#pragma unroll
-      for (int v = 0; v < NV; v++) st[v] = Uq[v * g.pvol];
-      const double ir = 1.0 / st[DENS];
-      const double ei = Eos<EQ>::eint_r(st, ir);
-      tile[0][t] = st[DENS];
-      tile[1][t] = ei;
-      tile[2][t] = sqrt(g.gamma * ((g.gamma - 1.0) * ei) * ir);
-      tile[3][t] = st[MOMX] * ir;
-      tile[4][t] = st[MOMY] * ir;
-      tile[5][t] = st[MOMZ] * ir;
-    }
-  }
   if (part == 0) {
     sIn[row] = 1;
     sLam[row] = 0ull;
     sVel[row] = 0ull;
+    if (live) {
+      // limiter bounds of the cell (bounds_kernel)
+      const int64_t c = (k * g.ny + j) * g.nx + i;
+      sBd[0][row] = bnd[c];
+      sBd[1][row] = bnd[g.n + c];
+      sBd[2][row] = bnd[2 * g.n + c];
+    }
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
-  if (part == 0 && live) {
-    const PosBounds bd = pos_bounds_tile<DIM, EQ>(tile, lane, quarter);
-    sBd[0][row] = bd.minDens;
-    sBd[1][row] = bd.maxDens;
-    sBd[2][row] = bd.minEint;
-    const int64_t c = (k * g.ny + j) * g.nx + i;
-    bnd[c] = bd.minDens;
-    bnd[g.n + c] = bd.maxDens;
-    bnd[2 * g.n + c] = bd.minEint;
-  }
 
   const double *Uc = U + pidx(g, live ? i : 0, live ? j : 0, k);
   const uint32_t aHi = smem_u32(smem), aLo = aHi + Sh::A_PART;
@@ -247,8 +221,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
 #pragma unroll
       for (int rp = 0; rp < Sh::RPP; rp += 2) {
         float a0[NV], a1[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) tmem_ld2(tmem + lanes + (uint32_t)(v * Sh::NP + R0 + rp), a0[v], a1[v]);
+        tmem_ld2_n<NV>(tmem + lanes + (uint32_t)(R0 + rp), (uint32_t)Sh::NP, a0, a1);
         if (live) {
 #pragma unroll
           for (int e = 0; e < 2; e++) {
@@ -258,7 +231,10 @@ __global__ void __launch_bounds__(kTcThreads, 2)
 #pragma unroll
               for (int v = 0; v < NV; v++) st[v] = uc[v] + (double)(e ? a1[v] : a0[v]);
               // pos_inside, with the internal energy kept for the indicator's pressure
-              const double ei = Eos<EQ>::eint(st);
+              // Euler / Navier-Stokes: the certified internal energy (no IEEE division)
+              double ei;
+              if constexpr (EQ == EQ_GLM) ei = Eos<EQ>::eint(st);
+              else ei = Eos<EQ>::eint_vs(st, bd.minEint);
               inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
               if (rw < T::NF * T::NQF) {
                 const int f = rw / T::NQF, q = rw % T::NQF, d = f >> 1;
@@ -314,6 +290,280 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                  : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// The same contraction with the halo tile staged by TMA.  Per variable v one 4D
+// tensor load (x, y, z, v of the padded state; box 36 x 8 x 5 in 3D, 36 x 8 x 1 in
+// 2D) brings the block's stencil footprint into shared memory; the A rows are
+// built from it (the same FP64 differences as above, so the products are the
+// same bits), and the load of variable v + 2 is issued as soon as the build
+// of v - 1 has read its buffer (three buffers: loads run two variables ahead of
+// the build).  The cell averages of the block are kept in shared memory for the
+// FP64 epilogue; the limiter bounds come from bounds_kernel.  Used when the padded
+// row pitch is even (TMA strides are multiples of 16 bytes).
+template <int DIM>
+struct HaloTile {
+  static constexpr int R = 2;
+  static constexpr int TX = kBlockX + 2 * R, TY = kBlockY + 2 * R, TZ = DIM == 3 ? 2 * R + 1 : 1;
+  static constexpr int N = TX * TY * TZ;
+  static constexpr int BYTES = N * 8;
+  static_assert((TX * 8) % 16 == 0, "TMA box inner extent");
+};
+
+template <int DIM, int EQ>
+struct TcTmaShape {
+  using Sh = TcShape<DIM, EQ>;
+  using H = HaloTile<DIM>;
+  static constexpr int NV = Cfg<DIM, EQ>::NV;
+  static constexpr int NBUF = 3;                                           // tiles in flight: v .. v + 2
+  static constexpr int HT_BYTES = (H::BYTES + 127) / 128 * 128;
+  static constexpr int OFF_HT = (Sh::USED + 127) / 128 * 128;            // halo tiles of NBUF variables
+  static constexpr int OFF_UC = OFF_HT + NBUF * HT_BYTES;                 // cell averages [v][128]
+  static constexpr int OFF_TO = OFF_UC + NV * 128 * 8;                    // stencil offsets in the tile [KP]
+  static constexpr int OFF_BT = (OFF_TO + Sh::KP * 4 + 7) / 8 * 8;        // tile barriers [NBUF], B barrier
+  static constexpr int USED = OFF_BT + 8 * (NBUF + 1);
+  static constexpr int SMEM = USED > Sh::FLOOR ? USED : Sh::FLOOR;
+  static_assert(SMEM <= 227 * 1024, "shared memory per block");
+  static_assert(Sh::OFF_B % 16 == 0 && Sh::B_PART % 16 == 0, "bulk copy of the B operand");
+  static_assert(Sh::MAX_RES < 2 || SMEM <= 113 * 1024, "two blocks per SM where TMEM allows them");
+};
+
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(kTcThreads, 2)
+    recon_tc_tma_kernel(const __grid_constant__ CUtensorMap umap, const double *__restrict__ U, Grid g,
+                        const DevStencil *__restrict__ S, int wantInd, double *__restrict__ F0,
+                        double *__restrict__ F1, double *__restrict__ F2, float *__restrict__ W0,
+                        float *__restrict__ W1, float *__restrict__ W2, double *__restrict__ src,
+                        uint8_t *__restrict__ status, double2 *__restrict__ lamvel, double *__restrict__ bnd,
+                        DevScalars *__restrict__ sc) {
+  using T = Cfg<DIM, EQ>;
+  using Sh = TcShape<DIM, EQ>;
+  using L = TcTmaShape<DIM, EQ>;
+  using H = HaloTile<DIM>;
+  constexpr int NV = T::NV;
+  extern __shared__ __align__(128) uint8_t smem[];
+  double(*sBd)[128] = reinterpret_cast<double(*)[128]>(smem + Sh::OFF_BD);
+  unsigned long long *sLam = reinterpret_cast<unsigned long long *>(smem + Sh::OFF_RED);
+  unsigned long long *sVel = sLam + 128;
+  int *sIn = reinterpret_cast<int *>(smem + Sh::OFF_RED + 2 * 128 * 8);
+  double(*sUc)[128] = reinterpret_cast<double(*)[128]>(smem + L::OFF_UC);
+  int *sTo = reinterpret_cast<int *>(smem + L::OFF_TO);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::OFF_BAR);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + Sh::OFF_BAR + 8);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quarter = warp & 3, part = warp >> 2;
+  const int row = quarter * 32 + lane;     // tile row = TMEM lane = cell (lane, quarter) of the block
+  const int tid = threadIdx.x;
+  const int64_t i = blockIdx.x * (int64_t)kBlockX + lane;
+  const int64_t j = blockIdx.y * (int64_t)kBlockY + quarter;
+  const int64_t k = blockIdx.z;
+  const bool live = i < g.nx && j < g.ny;
+  const uint32_t barA = smem_u32(bar), barT = smem_u32(smem + L::OFF_BT);  // tile barriers barT + 8 b
+  // padded coordinates of the tile's first cell: (i0 - 2, j0 - 2, k - 2) in cells
+  const int tx0 = (int)(blockIdx.x * kBlockX), ty0 = (int)(blockIdx.y * kBlockY), tz0 = (int)k;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"((uint32_t)Sh::COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // variable v's halo tile lands in buffer v % NBUF, completing on barrier v % NBUF
+  auto issue_tile = [&](int v) {
+    const int b = v % L::NBUF;
+    mbar_arrive_expect_tx(barT + 8 * b, (uint32_t)H::BYTES);
+    tma_load_4d(smem_u32(smem + L::OFF_HT + b * L::HT_BYTES), &umap, tx0, ty0, tz0, v, barT + 8 * b);
+  };
+  if (tid == 0) {
+    mbar_init(barA, 1);
+    for (int b = 0; b < L::NBUF; b++) mbar_init(barT + 8 * b, 1);
+    mbar_init(barT + 8 * L::NBUF, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    // the split weights (B operand) on their own barrier, then the first tiles
+    mbar_arrive_expect_tx(barT + 8 * L::NBUF, (uint32_t)(2 * Sh::B_PART));
+    bulk_load(smem_u32(smem + Sh::OFF_B), S->tcw[0], Sh::B_PART, barT + 8 * L::NBUF);
+    bulk_load(smem_u32(smem + Sh::OFF_B + Sh::B_PART), S->tcw[1], Sh::B_PART, barT + 8 * L::NBUF);
+    for (int v = 0; v < L::NBUF - 1 && v < NV; v++) issue_tile(v);
+  }
+  for (int c = tid; c < Sh::KP; c += kTcThreads) {
+    // stencil cell c relative to the cell in the halo tile
+    const int dx = c < T::C ? (int)S->w.off[0][c] : 0, dy = c < T::C ? (int)S->w.off[1][c] : 0;
+    const int dz = (DIM == 3 && c < T::C) ? (int)S->w.off[2][c] : 0;
+    sTo[c] = (dz * H::TY + dy) * H::TX + dx;
+  }
+  if (part == 0) {
+    sIn[row] = 1;
+    sLam[row] = 0ull;
+    sVel[row] = 0ull;
+    if (live) {
+      // limiter bounds of the cell (bounds_kernel)
+      const int64_t c = (k * g.ny + j) * g.nx + i;
+      sBd[0][row] = bnd[c];
+      sBd[1][row] = bnd[g.n + c];
+      sBd[2][row] = bnd[2 * g.n + c];
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const int cm = ((DIM == 3 ? 2 : 0) * H::TY + quarter + 2) * H::TX + lane + 2; // the cell in the halo tile
+  const uint32_t aHi = smem_u32(smem), aLo = aHi + Sh::A_PART;
+  const uint32_t bHi = smem_u32(smem + Sh::OFF_B), bLo = bHi + Sh::B_PART;
+  constexpr uint32_t idesc = tf32_idesc<Sh::NP>();
+  // this thread's stencil cells (chunks part, part + 2, ...) as tile offsets (of
+  // either sign), kNoCell past the stencil
+  constexpr int MYCH = (Sh::NCH + kTcParts - 1) / kTcParts;
+  constexpr int kNoCell = -0x40000000;
+  int toff[MYCH * 4];
+#pragma unroll
+  for (int m = 0; m < MYCH; m++)
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int c = (part + kTcParts * m) * 4 + t;
+      toff[m * 4 + t] = (c < T::C && part + kTcParts * m < Sh::NCH) ? sTo[c] : kNoCell;
+    }
+  // matrix descriptors of K step 0; step s adds 2 s chunks to the start address
+  const uint64_t dAh = umma_desc(aHi, Sh::A_CH, 128), dAl = umma_desc(aLo, Sh::A_CH, 128);
+  const uint64_t dBh = umma_desc(bHi, Sh::B_CH, 128), dBl = umma_desc(bLo, Sh::B_CH, 128);
+
+  bool ok = mbar_wait(barT + 8 * L::NBUF, 0u);                 // the B operand
+  int issued = NV < L::NBUF - 1 ? NV : L::NBUF - 1;            // tile loads issued (thread 0)
+  int consumed = 0;                                            // tile loads waited for
+#pragma unroll 1
+  for (int v = 0; v < NV; v++) {
+    if (v > 0) ok = ok && mbar_wait(barA, (uint32_t)(v - 1) & 1u);   // the MMAs of v - 1 have read A
+    ok = ok && mbar_wait(barT + 8 * (v % L::NBUF), (uint32_t)(v / L::NBUF) & 1u);  // v's tile has landed
+    if (!__syncthreads_and(ok)) break;
+    consumed = v + 1;
+    const double *ht = reinterpret_cast<const double *>(smem + L::OFF_HT + (v % L::NBUF) * L::HT_BYTES);
+    const double ucv = live ? ht[cm] : 0.0;
+    if (part == 0) sUc[v][row] = ucv;
+#pragma unroll
+    for (int m = 0; m < MYCH; m++) {
+      const int ch = part + kTcParts * m;
+      if (ch < Sh::NCH) {
+        uint32_t hi[4], lo[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          const int o = toff[m * 4 + t];
+          const float d = (o != kNoCell && live) ? (float)(ht[cm + o] - ucv) : 0.0f;
+          hi[t] = tf32_rna_bits(d);
+          lo[t] = tf32_rna_bits(d - __uint_as_float(hi[t]));
+        }
+        st_shared_v4(aHi + ch * Sh::A_CH + row * 16, hi);
+        st_shared_v4(aLo + ch * Sh::A_CH + row * 16, lo);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      if (v + L::NBUF - 1 < NV) {
+        // variable v + NBUF - 1 into the buffer of v - 1, whose build finished last iteration
+        issue_tile(v + L::NBUF - 1);
+        issued++;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t d = tmem + (uint32_t)(v * Sh::NP);
+#pragma unroll
+      for (int s = 0; s < Sh::NKS; s++) {
+        // the descriptor's start-address field counts 16-byte units
+        const uint64_t sa = (uint64_t)(2 * s * Sh::A_CH) >> 4, sb = (uint64_t)(2 * s * Sh::B_CH) >> 4;
+        mma_tf32(d, dAl + sa, dBh + sb, idesc, s > 0);
+        mma_tf32(d, dAh + sa, dBl + sb, idesc, 1);
+        mma_tf32(d, dAh + sa, dBh + sb, idesc, 1);
+      }
+      mma_commit(barA);
+    }
+  }
+  if (ok) ok = mbar_wait(barA, (uint32_t)(NV - 1) & 1u);
+  if (__syncthreads_and(ok)) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    PosBounds bd;
+    bd.minDens = sBd[0][row];
+    bd.maxDens = sBd[1][row];
+    bd.minEint = sBd[2][row];
+    double uc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) uc[v] = sUc[v][row];
+    const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    bool inside = true;
+    double lam = 0.0, vel = 0.0;
+    auto epilogue = [&](auto partTag) {
+      constexpr int PART = decltype(partTag)::value;
+      constexpr int R0 = PART * Sh::RPP;
+#pragma unroll
+      for (int rp = 0; rp < Sh::RPP; rp += 2) {
+        float a0[NV], a1[NV];
+        tmem_ld2_n<NV>(tmem + lanes + (uint32_t)(R0 + rp), (uint32_t)Sh::NP, a0, a1);
+        if (live) {
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const int rw = R0 + rp + e;
+            if (rw < Sh::NR) {
+              double st[NV];
+#pragma unroll
+              for (int v = 0; v < NV; v++) st[v] = uc[v] + (double)(e ? a1[v] : a0[v]);
+              // Euler / Navier-Stokes: the certified internal energy (no IEEE division)
+              double ei;
+              if constexpr (EQ == EQ_GLM) ei = Eos<EQ>::eint(st);
+              else ei = Eos<EQ>::eint_vs(st, bd.minEint);
+              inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
+              if (rw < T::NF * T::NQF) {
+                const int f = rw / T::NQF, q = rw % T::NQF, d = f >> 1;
+                double *Fd = d == 0 ? F0 : (d == 1 ? F1 : F2);
+                const int64_t a = face_slot_addr(g, f, i, j, k, q, 0, T::NQF, NV);
+                const int64_t nf = g.nface[d];
+#pragma unroll
+                for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
+                if (wantInd)
+                  (d == 0 ? W0 : (d == 1 ? W1 : W2))[face_slot_addr(g, f, i, j, k, q, 0, T::NQF, 1)] =
+                      Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
+                if constexpr (T::SRC) {
+                  // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
+                  const double vv = fabs(st[MOMX] / st[DENS]);
+                  const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
+                  vel = vv > vel ? vv : vel;
+                  lam = l > lam ? l : lam;
+                }
+              } else if constexpr (T::SRC) {
+                const int q = rw - T::NF * T::NQF;
+#pragma unroll
+                for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
+              }
+            }
+          }
+        }
+      }
+    };
+    if (part == 0) epilogue(std::integral_constant<int, 0>{});
+    else epilogue(std::integral_constant<int, 1>{});
+    if (live && !inside) atomicAnd(&sIn[row], 0);
+    if constexpr (T::SRC) {
+      if (live) {
+        if (lam >= 0.0) atomicMax(&sLam[row], (unsigned long long)__double_as_longlong(lam));
+        if (vel >= 0.0) atomicMax(&sVel[row], (unsigned long long)__double_as_longlong(vel));
+      }
+    }
+    __syncthreads();
+    if (live && part == 0) {
+      if constexpr (T::SRC)
+        lamvel[c] = make_double2(__longlong_as_double((long long)sLam[row]), __longlong_as_double((long long)sVel[row]));
+      status[c] = sIn[row] ? 1 : 0;
+    }
+  } else if (tid == 0) {
+    atomicExch(&sc->fault, 1u);
+    // tile loads still in flight land before the block leaves
+    for (int v = consumed; v < issued; v++) mbar_wait(barT + 8 * (v % L::NBUF), (uint32_t)(v / L::NBUF) & 1u);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)Sh::COLS)
+                 : "memory");
+}
+
 // Self-test of the bounded wait: one block waits on an mbarrier that nothing
 // arrives on, with the given limit, and records whether it gave up and how long
 // it waited.  The kernel always returns.
@@ -334,35 +584,61 @@ cudaError_t launch_wait_probe(uint64_t limit_ns, unsigned long long *out, cudaSt
 }
 
 template <int DIM, int EQ>
-static cudaError_t recon_tc_launch(const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                                   double *const *F, float *const *W, double *src, uint8_t *status,
+static cudaError_t recon_tc_launch(const double *U, const CUtensorMap *umap, const Grid &g, const DevStencil *S,
+                                   int wantInd, double *const *F, float *const *W, double *src, uint8_t *status,
                                    double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s) {
   using Sh = TcShape<DIM, EQ>;
-  static bool attr = false; // the attribute is per function and process-wide
+  using L = TcTmaShape<DIM, EQ>;
+  const dim3 grid((unsigned)((g.nx + kBlockX - 1) / kBlockX), (unsigned)((g.ny + kBlockY - 1) / kBlockY),
+                  (unsigned)g.nz);
+  if (umap) {
+    static bool attrT = false; // the attribute is per function and process-wide
+    if (!attrT) {
+      cudaError_t e = cudaFuncSetAttribute(recon_tc_tma_kernel<DIM, EQ>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+      if (e != cudaSuccess) return e;
+      attrT = true;
+    }
+    recon_tc_tma_kernel<DIM, EQ><<<grid, kTcThreads, L::SMEM, s>>>(
+        *umap, U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd, sc);
+    return cudaGetLastError();
+  }
+  static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(recon_tc_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          Sh::SMEM);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const dim3 grid((unsigned)((g.nx + kBlockX - 1) / kBlockX), (unsigned)((g.ny + kBlockY - 1) / kBlockY),
-                  (unsigned)g.nz);
   recon_tc_kernel<DIM, EQ><<<grid, kTcThreads, Sh::SMEM, s>>>(
       U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd, sc);
   return cudaGetLastError();
 }
 
-cudaError_t launch_recon_tc(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                            double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
-                            double *bnd, DevScalars *sc, cudaStream_t s) {
+cudaError_t launch_recon_tc(int dim, int eq, const double *U, const CUtensorMap *umap, const Grid &g,
+                            const DevStencil *S, int wantInd, double *const *F, float *const *W, double *src,
+                            uint8_t *status, double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s) {
   if (dim == 2) {
-    if (eq == EQ_GLM) return recon_tc_launch<2, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
-    if (eq == EQ_NS) return recon_tc_launch<2, EQ_NS>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
-    return recon_tc_launch<2, EQ_HYDRO>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+    if (eq == EQ_GLM) return recon_tc_launch<2, EQ_GLM>(U, umap, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+    if (eq == EQ_NS) return recon_tc_launch<2, EQ_NS>(U, umap, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+    return recon_tc_launch<2, EQ_HYDRO>(U, umap, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
   }
-  if (eq == EQ_GLM) return recon_tc_launch<3, EQ_GLM>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
-  if (eq == EQ_NS) return recon_tc_launch<3, EQ_NS>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
-  return recon_tc_launch<3, EQ_HYDRO>(U, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+  if (eq == EQ_GLM) return recon_tc_launch<3, EQ_GLM>(U, umap, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+  if (eq == EQ_NS) return recon_tc_launch<3, EQ_NS>(U, umap, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+  return recon_tc_launch<3, EQ_HYDRO>(U, umap, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s);
+}
+
+// 4D map (x, y, z, variable) of a padded state for the halo-tile loads, or a
+// nonzero return where TMA cannot address it (odd row pitch)
+int recon_tc_state_map(CUtensorMap *map, const double *U, const Grid &g, int dim, int nv) {
+  if (g.px % 2 != 0) return 1;
+  const uint64_t planes = (uint64_t)(g.pvol / (g.px * g.py));
+  const uint64_t dims[4] = {(uint64_t)g.px, (uint64_t)g.py, planes, (uint64_t)nv};
+  const uint64_t strides[3] = {(uint64_t)g.px * 8, (uint64_t)(g.px * g.py) * 8, (uint64_t)g.pvol * 8};
+  const uint32_t box[4] = {(uint32_t)(dim == 3 ? HaloTile<3>::TX : HaloTile<2>::TX),
+                           (uint32_t)(dim == 3 ? HaloTile<3>::TY : HaloTile<2>::TY),
+                           (uint32_t)(dim == 3 ? HaloTile<3>::TZ : HaloTile<2>::TZ), 1u};
+  return encode_tensor_map_8b(map, U, 4, dims, strides, box);
 }
 
 // host: W = hi + lo split of the [cell][row] linear weights into the B layout

@@ -38,6 +38,12 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
   return r;
 }
 
+// the same rounding (to nearest, ties away from zero, on the magnitude) with
+// integer operations: add half a unit of the last kept bit, drop the 13 low bits
+__device__ __forceinline__ uint32_t tf32_rna_bits(float x) {
+  return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
+}
+
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, const uint32_t (&v)[4]) {
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v[0]), "r"(v[1]), "r"(v[2]),
                "r"(v[3])
@@ -96,6 +102,40 @@ __device__ __forceinline__ void tmem_ld2(uint32_t taddr, float &r0, float &r1) {
       : "memory");
   r0 = __uint_as_float(x0);
   r1 = __uint_as_float(x1);
+}
+
+// A column pair (an even column) of each of NV accumulators that lie `stride`
+// columns apart, with one wait for all of them: the loads are issued back to back
+// and the wait names every destination register, so no use can move above it.
+template <int NV>
+__device__ __forceinline__ void tmem_ld2_n(uint32_t taddr, uint32_t stride, float (&a0)[NV], float (&a1)[NV]) {
+  static_assert(NV == 5 || NV == 9, "Euler / Navier-Stokes or GLM-MHD variable counts");
+  uint32_t x[2 * NV];
+#pragma unroll
+  for (int v = 0; v < NV; v++)
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];"
+                 : "=r"(x[2 * v]), "=r"(x[2 * v + 1])
+                 : "r"(taddr + (uint32_t)v * stride)
+                 : "memory");
+  if constexpr (NV == 5) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]),
+                   "+r"(x[8]), "+r"(x[9])
+                 :
+                 : "memory");
+  } else {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]),
+                   "+r"(x[8]), "+r"(x[9]), "+r"(x[10]), "+r"(x[11]), "+r"(x[12]), "+r"(x[13]), "+r"(x[14]),
+                   "+r"(x[15]), "+r"(x[16]), "+r"(x[17])
+                 :
+                 : "memory");
+  }
+#pragma unroll
+  for (int v = 0; v < NV; v++) {
+    a0[v] = __uint_as_float(x[2 * v]);
+    a1[v] = __uint_as_float(x[2 * v + 1]);
+  }
 }
 
 // 8 consecutive TMEM columns of this warp's 32 lanes, waited for in the same asm

@@ -145,5 +145,6 @@ def test_forms_error_matches_plain(name, scale, t_end, gpu, product_lib):
     e_plain = np.abs(plain - ref).sum(axis=1)
     for form, u in forms.items():
         e = np.abs(u - ref).sum(axis=1)
+        print(name, form, "L1 error / plain FP64 L1 error:", e[[0, 1, 2, 4]] / e_plain[[0, 1, 2, 4]])
         for v in (0, 1, 2, 4):
             assert e[v] <= 1.05 * e_plain[v], (form, v, e[v] / e_plain[v])
