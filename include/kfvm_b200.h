@@ -212,8 +212,10 @@ int kfvm_err_est(kfvm_solver *s, const double *u_dev, const double *uhat_dev, do
  * kfvm_err_est); stream is a cudaStream_t (NULL for the legacy default stream).
  * Its scratch is a 1 MiB file-scope device array that every GPU loading the
  * library holds until exit; n above KFVM_NOALLOC_MAX_CELLS is rejected with
- * KFVM_ERR_ARG.  The first call on a device looks up that array's device address
- * (cudaGetSymbolAddress) and should come before any stream capture.  All calls
+ * KFVM_ERR_ARG.  Every call looks up that array's device address on the current
+ * device (cudaGetSymbolAddress, so a cudaDeviceReset in between is harmless); the
+ * first call on a device also loads the library's device code there and should
+ * come before any stream capture.  All calls
  * on one GPU share that GPU's copy of the array: calls that overlap on the same
  * GPU (for example on two streams) race and must be serialised by the caller.
  * Each call overwrites the scratch it reads, so no clearing is needed between

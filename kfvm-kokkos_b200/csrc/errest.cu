@@ -7,7 +7,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "../../include/kfvm_b200.h"
@@ -108,26 +107,16 @@ cudaError_t launch_errest(int eq, const double *u, const double *uhat, int64_t n
 static __device__ __align__(256) double g_noalloc_part[2 * (KFVM_NOALLOC_MAX_CELLS / kErrBlock)];
 
 namespace {
-std::mutex g_noalloc_mu;
-constexpr int kMaxDevices = 64;
-double *g_noalloc_ptr[kMaxDevices] = {nullptr};
-
 // Device address of g_noalloc_part on the current device.  In host code the
 // symbol names a host-side stand-in, so the address comes from
-// cudaGetSymbolAddress, taken once per device with that device current.
+// cudaGetSymbolAddress with the device current.  It is looked up on every call
+// (a host-side query, no device work): after a cudaDeviceReset the module is
+// loaded again and the array may move, so a cached address could go stale.
 cudaError_t noalloc_scratch(double **ptr) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_part);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_part);
-    if (e != cudaSuccess) return e;
-    g_noalloc_ptr[dev] = static_cast<double *>(p);
-  }
-  *ptr = g_noalloc_ptr[dev];
+  *ptr = static_cast<double *>(p);
   return cudaSuccess;
 }
 } // namespace
