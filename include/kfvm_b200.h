@@ -372,6 +372,11 @@ int kfvm_get_stream(kfvm_solver *s, void **stream);
 int kfvm_set_timing(kfvm_solver *s, int32_t on);
 int kfvm_get_timing(kfvm_solver *s, double *ms_per_class, int64_t *launches_per_class);
 int kfvm_get_launch_count(kfvm_solver *s, int64_t *launches);
+/* The equal-state Riemann variant (no counterpart in the reference): whether the
+ * next Riemann launches use it (on: 0 or 1) and the cumulative number of face
+ * points sampled for the choice and of those whose two states agree to 1e-14
+ * (any pointer may be null). */
+int kfvm_get_same_state(kfvm_solver *s, int32_t *on, int64_t *sampled, int64_t *equal);
 
 /* ---- random forcing (stirred turbulence) ----
  * The reference's ENABLE_RANDOM_FORCING path (src/ParameterStructs.H:20-74,

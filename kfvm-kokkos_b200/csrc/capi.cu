@@ -1611,4 +1611,12 @@ int kfvm_get_launch_count(kfvm_solver *s, int64_t *launches) {
   return KFVM_OK;
 }
 
+int kfvm_get_same_state(kfvm_solver *s, int32_t *on, int64_t *sampled, int64_t *equal) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (on) *on = s->sameOn ? 1 : 0;
+  if (sampled) *sampled = (int64_t)s->sampSeen;
+  if (equal) *equal = (int64_t)s->sameSeen;
+  return KFVM_OK;
+}
+
 } // extern "C"

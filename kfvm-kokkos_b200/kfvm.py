@@ -78,6 +78,7 @@ def lib():
         L.kfvm_set_timing.argtypes = [P, I32]
         L.kfvm_get_timing.argtypes = [P, P, P]
         L.kfvm_get_launch_count.argtypes = [P, C.POINTER(I64)]
+        L.kfvm_get_same_state.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(I64), C.POINTER(I64)]
         L.kfvm_flow_stats.argtypes = [P, P, C.POINTER(I32)]
         L.kfvm_forcing_num_modes.argtypes = [I32]
         L.kfvm_forcing_draw.argtypes = [I32, C.c_uint32, P]
@@ -363,6 +364,12 @@ class Solver:
         n = C.c_int64()
         _check(lib().kfvm_get_launch_count(self.h, C.byref(n)), "kfvm_get_launch_count")
         return n.value
+
+    def same_state(self):
+        """(on, sampled, equal) of the equal-state Riemann variant."""
+        on, n, e = C.c_int32(), C.c_int64(), C.c_int64()
+        _check(lib().kfvm_get_same_state(self.h, C.byref(on), C.byref(n), C.byref(e)), "kfvm_get_same_state")
+        return bool(on.value), n.value, e.value
 
     def last_step_ms(self):
         ms = C.c_double()

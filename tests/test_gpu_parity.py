@@ -324,3 +324,25 @@ def test_srhydro_against_oracle(name, scale, steps, nq, gpu, product_lib, oracle
     step_pair(g, o, steps)
     err = rel_l1(g.get_state(), o.get_state())
     assert np.all(err <= STEP_TOL), err
+
+
+@pytest.mark.parametrize("dim,n", [(2, 48), (3, 20)])
+def test_glm_equal_state_variant(dim, n, gpu, product_lib, oracle_lib):
+    """GLM-MHD with a uniform background: a spherical blast in a field-free
+    GLM-MHD gas, so most faces see equal states and the Riemann kernel's
+    equal-state variant (flux F(u), speed bound |u_n| + max(c_h, c_f)) carries them.
+    The variant must stay selected across the steps, and the states must match
+    the oracle (which runs the reference's HLL arithmetic on every face)."""
+    cfg = abi.make_config(dim, abi.KFVM_EQ_MHD_GLM, n, n, n, bc="outflow", gamma=5.0 / 3.0, rs=abi.KFVM_RS_HLL,
+                          cfl=0.4, steps=6)
+    g = product_lib.Solver(cfg)
+    o = oracle_lib.OracleSolver(cfg)
+    g.init_ic(abi.KFVM_IC_SPHERICAL_SOD)
+    o.init_ic(abi.KFVM_IC_SPHERICAL_SOD)
+    step_pair(g, o, 6)
+    on, sampled, equal = g.same_state()
+    assert sampled > 0 and equal >= sampled // 4, (sampled, equal)
+    assert on
+    err = rel_l1(g.get_state(), o.get_state())
+    assert np.all(err <= STEP_TOL), err
+    g.close()
