@@ -425,19 +425,24 @@ def run_ours(args):
     case = f"{cfg.dim}d_{('hydro', 'ns', 'glm', 'sr')[cfg.eq]}"
     per_cell = traffic_tbl.get("cases", {}).get(case, {}).get("bytes_per_cell", {}).get(dom)
     traffic = per_cell * n if per_cell is not None else None
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
-                "algorithmic_bytes": algo, "launch_ms": avg_ms,
-                "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback"}
+    hbm = {"achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+           "algorithmic_bytes": algo,
+           "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback"}
     fma = algorithmic_fma(dom, cfg)
     if fma is not None:
-        # FP64 pipe: 148 SMs x 64 FP64 FMA per clock at the maximum SM clock
-        sm_max = (peaks or {}).get("sm_max_mhz", 1965.0)
-        fp64_peak = 148 * 64 * 2 * sm_max * 1e6 / 1e12
+        # the FP64 reconstruction runs on the FP64 tensor pipe (m8n8k4 DMMA): its bound
+        # is that pipe's throughput, measured on this GPU by back-to-back MMAs
+        fp64_peak = kfvm.measure_fp64_mma()
         fp64 = 2 * fma / (avg_ms / 1e3) / 1e12
-        roofline["fp64_pipe"] = {"achieved": fp64, "peak": fp64_peak, "unit": "TFLOP/s",
-                                 "frac": fp64 / fp64_peak, "fma_per_launch": fma,
-                                 "peak_source": "nominal (148 SMs x 64 FP64 FMA/clk x max SM clock; the DMMA rate measured by ncu is the same)"}
+        roofline = {"bound": "tensor", "kernel": dom, "achieved": fp64, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": fp64 / fp64_peak, "traffic": traffic, "fma_per_launch": fma, "launch_ms": avg_ms,
+                    "peak_source": "measured on this GPU: FP64 m8n8k4 MMAs back to back on every SM "
+                                   "(kfvm_measure_fp64_mma); FP64, so not the bf16 figure of MEASURED_PEAKS.json",
+                    "hbm": hbm}
+    else:
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": achieved / hbm_peak, "traffic": traffic, "algorithmic_bytes": algo, "launch_ms": avg_ms,
+                    "peak_source": hbm["peak_source"]}
     # the whole path: attainable zone-updates/s = min(HBM / B_zu, FP64 / F_zu)
     # B_zu: per stage U, Uprev, Utmp, Uhat in and U', Utmp, Uhat out (7 NV reals),
     #       plus the error pass (2 NV reals); F_zu: per RHS evaluation and cell the
@@ -447,8 +452,7 @@ def run_ours(args):
     rows_ = 2 * d_ * nqf_ + (nqc_ if src_ else 0)
     b_zu = 4 * 7 * nv_ * 8 + 2 * nv_ * 8
     f_zu = 4 * (2 * rows_ * ncst_ * nv_ + d_ * nqf_ * 200 + 300)
-    sm_max_ = (peaks or {}).get("sm_max_mhz", 1965.0)
-    fp64_peak_ = 148 * 64 * 2 * sm_max_ * 1e6
+    fp64_peak_ = roofline["peak"] * 1e12 if roofline["unit"] == "TFLOP/s" else kfvm.measure_fp64_mma() * 1e12
     att_hbm, att_fp64 = hbm_peak * 1e9 / b_zu, fp64_peak_ / f_zu
     path_roofline = {"bytes_per_zone_update": b_zu, "flops_per_zone_update": f_zu,
                      "attainable_hbm": att_hbm, "attainable_fp64": att_fp64,
@@ -486,6 +490,22 @@ def run_ours(args):
         lf64 = time_form(cfg, ic, abi.KFVM_PREC_FP64, steps=fs, warmup=2, mlp_weights=w)
         lf64["vs_plain"] = lf64["value"] / value
         out["forms"] = {"fp32_3xtf32": form, "learned_fp32": lf, "learned_fp64": lf64}
+    if not args.no_forms and ws == 1 and cfg.eq != abi.KFVM_EQ_SRHYDRO:
+        # the target's own workloads: Taylor-Green 256^3 and Kelvin-Helmholtz 1024^2,
+        # plain FP64 against the FP32 and the learned + FP32 forms (short runs)
+        out["target_forms"] = {}
+        for wl, sc in (("taylor_green", 256), ("kelvin_helmholtz", 1024)):
+            tcfg, tic = abi.workload(wl, scale=sc, steps=40)
+            plain = time_form(tcfg, tic, abi.KFVM_PREC_FP64, steps=3, warmup=2)
+            f32 = time_form(tcfg, tic, abi.KFVM_PREC_TF32X3, steps=3, warmup=2)
+            w, info = train_indicator(wl)
+            lf32 = time_form(tcfg, tic, abi.KFVM_PREC_TF32X3, steps=3, warmup=2, mlp_weights=w)
+            entry = {"grid": [sc] * WORKLOADS[wl][1], "plain_fp64": plain["value"], "unit": UNIT}
+            for name, r in (("fp32_3xtf32", f32), ("learned_fp32", lf32)):
+                entry[name] = {"value": r["value"], "vs_plain": r["value"] / plain["value"],
+                               "l1_vs_plain": r["l1_vs_plain"], "kernel_ms": r["kernel_ms"]}
+            entry["plain_kernel_ms"] = plain["kernel_ms"]
+            out["target_forms"][f"{wl}_{sc}"] = entry
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.workload, sample_scale=cpu_sample_scale(args.workload),
                                            sample_steps=3)

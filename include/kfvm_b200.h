@@ -372,6 +372,11 @@ int kfvm_get_stream(kfvm_solver *s, void **stream);
 int kfvm_set_timing(kfvm_solver *s, int32_t on);
 int kfvm_get_timing(kfvm_solver *s, double *ms_per_class, int64_t *launches_per_class);
 int kfvm_get_launch_count(kfvm_solver *s, int64_t *launches);
+/* Measured FP64 tensor-pipe throughput of the current device (no counterpart in
+ * the reference): back-to-back independent m8n8k4 FP64 MMAs on every SM, timed
+ * with CUDA events over about 10 ms; *tflops receives the rate in TFLOP/s (an
+ * MMA = 512 flops).  The denominator of the FP64 reconstruction's roofline. */
+int kfvm_measure_fp64_mma(double *tflops);
 /* The equal-state Riemann variant (no counterpart in the reference): whether the
  * next Riemann launches use it (on: 0 or 1) and the cumulative number of face
  * points sampled for the choice and of those whose two states agree to 1e-14

@@ -1611,6 +1611,36 @@ int kfvm_get_launch_count(kfvm_solver *s, int64_t *launches) {
   return KFVM_OK;
 }
 
+int kfvm_measure_fp64_mma(double *tflops) {
+  if (!tflops) return fail(KFVM_ERR_ARG, "null argument");
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  double *out = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t st = nullptr;
+  CK(cudaMalloc((void **)&out, sizeof(double)));
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  const int blocks = 4 * sms, iters = 1 << 15;   // 16 warps per SM
+  cudaError_t e = kfvm::launch_dmma_peak(blocks, 64, out, st);   // warm-up
+  float ms = 0.0f;
+  if (e == cudaSuccess) e = cudaEventRecord(a, st);
+  if (e == cudaSuccess) e = kfvm::launch_dmma_peak(blocks, iters, out, st);
+  if (e == cudaSuccess) e = cudaEventRecord(b, st);
+  if (e == cudaSuccess) e = cudaEventSynchronize(b);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamDestroy(st);
+  cudaFree(out);
+  if (e != cudaSuccess) return set_err_cuda(e, "FP64 MMA probe");
+  const double flops = (double)blocks * 4 * (double)iters * 8 * 512.0;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return KFVM_OK;
+}
+
 int kfvm_get_same_state(kfvm_solver *s, int32_t *on, int64_t *sampled, int64_t *equal) {
   if (!s) return fail(KFVM_ERR_ARG, "null solver");
   if (on) *on = s->sameOn ? 1 : 0;

@@ -309,6 +309,29 @@ __global__ void __launch_bounds__(128) bounds_kernel(const double *__restrict__ 
   }
 }
 
+// Throughput probe of the FP64 tensor pipe (the roofline denominator of the FP64
+// reconstruction): every warp runs `iters` rounds of 8 independent m8n8k4 FP64
+// MMAs on register operands; out[0] += a checksum so nothing is optimised away.
+__global__ void __launch_bounds__(128) dmma_peak_kernel(int iters, double *out) {
+  double acc[8][2];
+  const double a = 1.0 + 1e-9 * threadIdx.x, b = 1.0 - 1e-9 * blockIdx.x;
+#pragma unroll
+  for (int q = 0; q < 8; q++) acc[q][0] = acc[q][1] = 0.0;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) dmma_884(acc[q], a, b);
+  }
+  double sum = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) sum += acc[q][0] + acc[q][1];
+  if (sum == 1.2345) out[0] += sum;  // never true for these operands; keeps the work
+}
+
+cudaError_t launch_dmma_peak(int blocks, int iters, double *out, cudaStream_t s) {
+  dmma_peak_kernel<<<blocks, 128, 0, s>>>(iters, out);
+  return cudaGetLastError();
+}
+
 // KXRCF flags (WenoSelect_K, Numeric_K.H:292-398): largest indicator jump across the
 // cell's faces over the cell value; the outer slot of a boundary face follows
 // setFaceBCs (periodic partner face, or the inner slot at an outflow boundary).

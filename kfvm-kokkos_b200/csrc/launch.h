@@ -36,6 +36,8 @@ cudaError_t launch_fill(double *p, int64_t n, double val, cudaStream_t s);
 // rcp_nr accuracy probe: out[0] = max ulp distance to 1/y, out[1] = bits of the
 // largest relative difference of x * rcp_nr(y) from x / y
 cudaError_t launch_rcp_probe(int64_t n, uint64_t seed, unsigned long long *out, cudaStream_t s);
+// FP64 tensor-pipe probe: blocks x 4 warps, each iters x 8 m8n8k4 MMAs
+cudaError_t launch_dmma_peak(int blocks, int iters, double *out, cudaStream_t s);
 // limiter bounds of every cell, [minDens | maxDens | minEint][cell] (the pre-pass
 // of the reconstruction kernels, which read them)
 cudaError_t launch_bounds(int dim, int eq, const double *U, const Grid &g, double *bnd, cudaStream_t s);

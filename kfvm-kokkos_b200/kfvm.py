@@ -78,6 +78,7 @@ def lib():
         L.kfvm_set_timing.argtypes = [P, I32]
         L.kfvm_get_timing.argtypes = [P, P, P]
         L.kfvm_get_launch_count.argtypes = [P, C.POINTER(I64)]
+        L.kfvm_measure_fp64_mma.argtypes = [C.POINTER(D)]
         L.kfvm_get_same_state.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(I64), C.POINTER(I64)]
         L.kfvm_flow_stats.argtypes = [P, P, C.POINTER(I32)]
         L.kfvm_forcing_num_modes.argtypes = [I32]
@@ -100,6 +101,13 @@ def err_est_noalloc(eq, u_dev_ptr, uhat_dev_ptr, n, atol, rtol, out_dev_ptr, str
     _check(lib().kfvm_err_est_noalloc(int(eq), C.c_void_p(u_dev_ptr), C.c_void_p(uhat_dev_ptr),
                                       int(n), float(atol), float(rtol), C.c_void_p(out_dev_ptr),
                                       C.c_void_p(stream)), "kfvm_err_est_noalloc")
+
+
+def measure_fp64_mma():
+    """kfvm_measure_fp64_mma: FP64 tensor-pipe throughput of this GPU (TFLOP/s)."""
+    t = C.c_double()
+    _check(lib().kfvm_measure_fp64_mma(C.byref(t)), "kfvm_measure_fp64_mma")
+    return t.value
 
 
 def selftest_wait(limit_s):
