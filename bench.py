@@ -10,7 +10,8 @@ one zone-update is one cell advanced by one accepted step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload sod3d|kelvin_helmholtz|taylor_green|orszag_tang|isentropic_vortex]
-                  [--scale N] [--no-forms] [--no-cpu-baseline]
+                  [--scale N] [--precision fp64|tf32x3] [--indicator kxrcf|mlp]
+                  [--no-forms] [--no-cpu-baseline]
 
 Beside the plain FP64 value the line carries "forms": the same workload with the
 3xTF32 tensor-core reconstruction (fp32_3xtf32), and with the learned
@@ -59,9 +60,11 @@ WORKLOADS = {
 }
 
 
-def metric_name(workload, scale):
+def metric_name(workload, scale, precision="fp64", indicator="kxrcf"):
     _, dim, short, _ = WORKLOADS[workload]
-    return f"zone-updates/s on 1 B200 ({short} {scale}^{dim}, plain FP64)"
+    form = {("fp64", "kxrcf"): "plain FP64", ("tf32x3", "kxrcf"): "FP32 3xTF32 form",
+            ("fp64", "mlp"): "learned indicator + FP64", ("tf32x3", "mlp"): "learned indicator + FP32"}
+    return f"zone-updates/s on 1 B200 ({short} {scale}^{dim}, {form[(precision, indicator)]})"
 
 
 def parse():
@@ -77,6 +80,8 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"],
                    help="arithmetic of the linear reconstruction contraction")
     p.add_argument("--no-forms", action="store_true", help="skip timing the FP32 and learned forms")
+    p.add_argument("--indicator", default="kxrcf", choices=["kxrcf", "mlp"],
+                   help="troubled-cell indicator of the timed run (mlp: trained untimed first)")
     a = p.parse_args()
     if a.scale is None:
         a.scale = WORKLOADS[a.workload][0]
@@ -346,6 +351,10 @@ def run_ours(args):
     solver = kfvm.Solver(cfg)
     if args.precision == "tf32x3":
         solver.set_precision(abi.KFVM_PREC_TF32X3)
+    if args.indicator == "mlp":
+        w, _ = train_indicator(args.workload)
+        solver.mlp_set_weights(w)
+        solver.set_indicator(abi.KFVM_IND_MLP)
     solver.init_ic(ic)
     n = abi.ncells(cfg)
     nv = abi.nvars(cfg)
@@ -462,7 +471,7 @@ def run_ours(args):
     share = {k: round(v[0] / max(sum(x[0] for x in per_class.values()), 1e-9), 4)
              for k, v in per_class.items() if v[1] > 0}
 
-    out = {"metric": metric_name(args.workload, args.scale), "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+    out = {"metric": metric_name(args.workload, args.scale, args.precision, args.indicator), "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (analytic initial condition)",
