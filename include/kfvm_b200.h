@@ -48,7 +48,14 @@ enum kfvm_rk {
  * and negates the normal momentum (and the normal magnetic field for GLM-MHD); a
  * no-slip wall negates every momentum component (and the normal magnetic field),
  * with the coefficient tables of src/physics/<eq>/<Eq>_BCCoeffs.H. */
-enum kfvm_bc { KFVM_BC_PERIODIC = 0, KFVM_BC_OUTFLOW = 1, KFVM_BC_REFLECTING = 2, KFVM_BC_NOSLIP = 3 };
+enum kfvm_bc {
+  KFVM_BC_PERIODIC = 0, KFVM_BC_OUTFLOW = 1, KFVM_BC_REFLECTING = 2, KFVM_BC_NOSLIP = 3,
+  /* a block face shared with another rank of a decomposed domain (the faces the
+   * reference's LayoutMPI gives an MPI neighbour, src/LayoutMPI.H:44-97): its
+   * halo cells and outer face states come from that rank through the exchange
+   * callbacks of kfvm_set_exchange */
+  KFVM_BC_EXCHANGE = 4
+};
 /* src/Types.H:40 */
 enum kfvm_ts_status { KFVM_TS_ACCEPTED = 0, KFVM_TS_TOLERANCE = 1, KFVM_TS_UNPHYSICAL = 2 };
 /* Troubled-cell indicator choice.  KXRCF is the reference's selector
@@ -116,6 +123,14 @@ typedef struct kfvm_config {
   int32_t rejection_limit;
   int32_t max_steps;  /* time:maxsteps (the stepping loop starts at nTS=1)   */
   int32_t have_sources; /* forced on for MHD_GLM (ProblemSetup.H:81)        */
+  /* Domain decomposition (mesh:numblocks, src/ProblemSetup.H:224-233): nb[d]
+   * blocks per axis, this rank's block at block[d].  nx, ny, nz are then the
+   * cells of one block and xlo..zup the extents of the whole domain; as in the
+   * reference's Geometry (src/Geometry.H:28-31) dx = (xup - xlo) / (nx nb[0])
+   * and this block starts at xlo + dx (block[0] nx).  nb = {1, 1, 1}, block =
+   * {0, 0, 0} for one domain. */
+  int32_t nb[3];
+  int32_t block[3];
   int32_t pad_;
 } kfvm_config;
 
@@ -382,6 +397,47 @@ int kfvm_measure_fp64_mma(double *tflops);
  * points sampled for the choice and of those whose two states agree to 1e-14
  * (any pointer may be null). */
 int kfvm_get_same_state(kfvm_solver *s, int32_t *on, int64_t *sampled, int64_t *equal);
+
+/* ---- domain decomposition (multi-rank) ----
+ * The reference's block decomposition and its boundary communication
+ * (src/LayoutMPI.H:44-97, src/Solver.cpp:826-1460, src/BoundaryData.cpp), one
+ * solver per rank.  kfvm_block_config turns the configuration of one block of a
+ * decomposed domain (nb set, block ignored) into rank `rank`'s configuration:
+ * its block coordinates (MPI Cartesian order, rank = (bx nb[1] + by) nb[2] + bz)
+ * and KFVM_BC_EXCHANGE on every face with a neighbouring block (a periodic axis
+ * of more than one block wraps); neighbors[6] (nullable) receives the ranks
+ * across west, east, south, north, bottom, top, -1 where there is none.
+ *
+ * kfvm_set_exchange installs the transport.  Per RHS evaluation the solver
+ *   - fills the halo axis by axis (x, then y over the x halo, then z over both,
+ *     as setCellBCs does): per axis with exchange faces it packs the r = 2 cell
+ *     layers along each exchange face, calls ex(user, axis, send_lo, recv_lo,
+ *     send_hi, recv_hi, bytes_lo, bytes_hi), unpacks into the halo, then fills
+ *     the axis's physical faces;
+ *   - exchanges the boundary face states (and, for the KXRCF selector, the
+ *     indicator values) after the linear reconstruction and again after the
+ *     limiter, as the two setFaceBCs calls of evalRHS do (axis = 3 + face
+ *     axis);
+ *   - reduces the GLM cleaning-speed maxima (max) before the Riemann solve,
+ *     and per step attempt the wave-speed maximum (max), the error sum (sum) and
+ *     the positivity minimum (min) through ar(user, op, vals, n), in place on
+ *     host doubles; kfvm_apply_forcing sums its two integrals the same way
+ *     (forceStrComm), and the equal-state Riemann variant is chosen from the
+ *     counts of all ranks (sum).
+ * In ex, send_lo goes to the rank across the low face and send_hi to the rank
+ * across the high face; recv_lo receives what the rank across the low face sent
+ * from its high side and recv_hi what the high neighbour sent from its low side.
+ * Buffers are device pointers (NULL and 0 bytes on a face without a
+ * neighbour) and stay valid during the call only; the callback returns 0 on
+ * success.  Every rank makes the same calls in the same order.  Flow
+ * statistics and the learned indicator's sample collection and training work
+ * on this rank's block only. */
+enum kfvm_reduce_op { KFVM_REDUCE_SUM = 0, KFVM_REDUCE_MAX = 1, KFVM_REDUCE_MIN = 2 };
+typedef int (*kfvm_exchange_fn)(void *user, int32_t axis, const void *send_lo, void *recv_lo,
+                                const void *send_hi, void *recv_hi, int64_t bytes_lo, int64_t bytes_hi);
+typedef int (*kfvm_allreduce_fn)(void *user, int32_t op, double *vals, int32_t n);
+int kfvm_block_config(const kfvm_config *blocks, int32_t rank, kfvm_config *out, int32_t neighbors[6]);
+int kfvm_set_exchange(kfvm_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user);
 
 /* ---- random forcing (stirred turbulence) ----
  * The reference's ENABLE_RANDOM_FORCING path (src/ParameterStructs.H:20-74,

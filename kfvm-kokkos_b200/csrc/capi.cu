@@ -20,6 +20,7 @@
 
 #include "../../include/kfvm_b200.h"
 #include "kernels.cuh"
+#include "geometry.h"
 #include "launch.h"
 
 namespace {
@@ -261,6 +262,13 @@ struct kfvm_solver {
   bool writePlot = false;
   int indicator = KFVM_IND_KXRCF;
   int precision = KFVM_PREC_FP64;
+  // domain decomposition: this block has exchange faces; the transport callbacks
+  // (kfvm_set_exchange) and their device buffers send_lo, recv_lo, send_hi, recv_hi
+  bool decomposed = false;
+  kfvm_exchange_fn xfn = nullptr;
+  kfvm_allreduce_fn rfn = nullptr;
+  void *xuser = nullptr;
+  double *xbuf[4] = {nullptr, nullptr, nullptr, nullptr};
   // TMA maps of the three state buffers for the tensor-core reconstruction's halo
   // tiles (built when the FP32 form is selected; unused where the pitch is odd)
   CUtensorMap umap[3];
@@ -375,10 +383,19 @@ void harvest(kfvm_solver *s) {
 // samples qualify (where few do, its heavier general path costs a few per cent);
 // otherwise uses the plain variant and probes again after kSameProbeSteps steps.
 constexpr int kSameProbeSteps = 4;
-void update_same_mode(kfvm_solver *s) {
-  const unsigned long long dS = s->hsc->nsame - s->sameSeen, dN = s->hsc->nsamp - s->sampSeen;
+int reduce_all(kfvm_solver *s, int op, double *vals, int n);
+
+int update_same_mode(kfvm_solver *s) {
+  unsigned long long dS = s->hsc->nsame - s->sameSeen, dN = s->hsc->nsamp - s->sampSeen;
   s->sameSeen = s->hsc->nsame;
   s->sampSeen = s->hsc->nsamp;
+  if (s->decomposed) {
+    // every rank takes the same choice, from the counts of all ranks
+    double c[2] = {(double)dS, (double)dN};
+    if (int rc = reduce_all(s, KFVM_REDUCE_SUM, c, 2)) return rc;
+    dS = (unsigned long long)c[0];
+    dN = (unsigned long long)c[1];
+  }
   if (s->sameOn) {
     if (dN > 0 && 4 * dS < dN) {
       s->sameOn = false;
@@ -387,12 +404,86 @@ void update_same_mode(kfvm_solver *s) {
   } else if (--s->sameProbe <= 0) {
     s->sameOn = true;
   }
+  return KFVM_OK;
 }
 
 // the reference's wenothresh sign switch: a positive threshold allows the sparse
 // (selected-cells) WENO mode, for KXRCF and for the learned indicator alike
 bool sparse_allowed(const kfvm_solver *s) {
   return s->cfg.weno_thresh > 0.0 && (s->indicator == KFVM_IND_KXRCF || s->indicator == KFVM_IND_MLP);
+}
+
+double bits_to_double(unsigned long long b) {
+  double d;
+  std::memcpy(&d, &b, sizeof(d));
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// boundary communication of a decomposed domain (Solver.cpp:744-1460)
+
+// in-place reduction of n host doubles over all ranks (identity on one domain)
+int reduce_all(kfvm_solver *s, int op, double *vals, int n) {
+  if (!s->decomposed) return KFVM_OK;
+  if (!s->rfn) return fail(KFVM_ERR_STATE, "exchange faces but no transport (kfvm_set_exchange)");
+  if (s->rfn(s->xuser, op, vals, n) != 0) return fail(KFVM_ERR_STATE, "the allreduce callback failed");
+  return KFVM_OK;
+}
+
+// the halo of buffer b: one launch on one domain; on a decomposed domain axis by
+// axis, exchange faces from the neighbours, the others from this block
+int fill_halo(kfvm_solver *s, int b) {
+  using namespace kfvm;
+  cudaStream_t st = s->stream;
+  double *U = s->Ub[b];
+  if (!s->decomposed) {
+    cudaError_t e = run(s, KFVM_KCLASS_BC, 1, [&] { return launch_bc(s->dim, s->eq, U, s->g, st); });
+    return e == cudaSuccess ? KFVM_OK : set_err_cuda(e, "bc");
+  }
+  if (!s->xfn) return fail(KFVM_ERR_STATE, "exchange faces but no transport (kfvm_set_exchange)");
+  for (int d = 0; d < s->dim; d++) {
+    const bool lo = s->g.bc[2 * d] == KFVM_BC_EXCHANGE, hi = s->g.bc[2 * d + 1] == KFVM_BC_EXCHANGE;
+    if (lo || hi) {
+      const int64_t bytes = cell_slab_values(s->g, s->dim, s->nv, d) * (int64_t)sizeof(double);
+      if (lo) CK(launch_cell_slab(s->dim, s->nv, U, s->g, d, 0, true, s->xbuf[0], st));
+      if (hi) CK(launch_cell_slab(s->dim, s->nv, U, s->g, d, 1, true, s->xbuf[2], st));
+      s->launches += (lo ? 1 : 0) + (hi ? 1 : 0);
+      CK(cudaStreamSynchronize(st));
+      if (s->xfn(s->xuser, d, lo ? s->xbuf[0] : nullptr, lo ? s->xbuf[1] : nullptr, hi ? s->xbuf[2] : nullptr,
+                 hi ? s->xbuf[3] : nullptr, lo ? bytes : 0, hi ? bytes : 0) != 0)
+        return fail(KFVM_ERR_STATE, "the halo exchange callback failed");
+      if (lo) CK(launch_cell_slab(s->dim, s->nv, U, s->g, d, 0, false, s->xbuf[1], st));
+      if (hi) CK(launch_cell_slab(s->dim, s->nv, U, s->g, d, 1, false, s->xbuf[3], st));
+      s->launches += (lo ? 1 : 0) + (hi ? 1 : 0);
+    }
+    cudaError_t e = run(s, KFVM_KCLASS_BC, 1, [&] { return launch_bc_axis(s->dim, s->nv, U, s->g, d, st); });
+    if (e != cudaSuccess) return set_err_cuda(e, "bc");
+  }
+  return KFVM_OK;
+}
+
+// the outer face states (and with W the KXRCF indicator) of every exchange face
+int exchange_faces(kfvm_solver *s, bool withW) {
+  using namespace kfvm;
+  if (!s->decomposed) return KFVM_OK;
+  cudaStream_t st = s->stream;
+  const int nqf = s->dim == 2 ? s->g.nq : s->g.nq * s->g.nq;
+  for (int d = 0; d < s->dim; d++) {
+    const bool lo = s->g.bc[2 * d] == KFVM_BC_EXCHANGE, hi = s->g.bc[2 * d + 1] == KFVM_BC_EXCHANGE;
+    if (!lo && !hi) continue;
+    float *W = withW ? s->W[d] : nullptr;
+    const int64_t bytes = face_plane_bytes(s->g, nqf, s->nv, d, withW);
+    if (lo) CK(launch_face_plane(s->F[d], W, s->g, nqf, s->nv, d, 0, true, s->xbuf[0], st));
+    if (hi) CK(launch_face_plane(s->F[d], W, s->g, nqf, s->nv, d, 1, true, s->xbuf[2], st));
+    CK(cudaStreamSynchronize(st));
+    if (s->xfn(s->xuser, 3 + d, lo ? s->xbuf[0] : nullptr, lo ? s->xbuf[1] : nullptr, hi ? s->xbuf[2] : nullptr,
+               hi ? s->xbuf[3] : nullptr, lo ? bytes : 0, hi ? bytes : 0) != 0)
+      return fail(KFVM_ERR_STATE, "the face exchange callback failed");
+    if (lo) CK(launch_face_plane(s->F[d], W, s->g, nqf, s->nv, d, 0, false, s->xbuf[1], st));
+    if (hi) CK(launch_face_plane(s->F[d], W, s->g, nqf, s->nv, d, 1, false, s->xbuf[3], st));
+    s->launches += 2 * ((lo ? 1 : 0) + (hi ? 1 : 0));
+  }
+  return KFVM_OK;
 }
 
 // one RHS evaluation on buffer b: BCs, selection, reconstruction, Riemann fluxes.
@@ -403,8 +494,7 @@ int eval_front(kfvm_solver *s, int b) {
   cudaStream_t st = s->stream;
   const int dim = s->dim, eq = s->eq;
   cudaError_t e;
-  if ((e = run(s, KFVM_KCLASS_BC, 1, [&] { return launch_bc(dim, eq, s->Ub[b], s->g, st); })) != cudaSuccess)
-    return set_err_cuda(e, "bc");
+  if (int rc = fill_halo(s, b)) return rc;
   // reset the per-evaluation counters (nflag, napplied, nheavy) and the GLM maxima
   CK(cudaMemsetAsync(&s->sc->glm_lam_bits, 0, 2 * sizeof(unsigned long long) + 3 * sizeof(unsigned), st));
   int mode;
@@ -436,6 +526,9 @@ int eval_front(kfvm_solver *s, int b) {
          })) != cudaSuccess)
       return set_err_cuda(e, "recon");
   }
+  // the first setFaceBCs of evalRHS: the selector reads the neighbours' states
+  if (mode == RECON_SPARSE && !mlpOn)
+    if (int rc = exchange_faces(s, wantInd)) return rc;
   if (mode == RECON_SPARSE) {
     const double thr = s->cfg.weno_thresh * std::pow(s->dmin, 1.5);
     if ((e = run(s, KFVM_KCLASS_FLAG, mlpOn ? 2 : 1, [&] {
@@ -461,6 +554,20 @@ int eval_front(kfvm_solver *s, int b) {
                              mode == RECON_FULL ? nullptr : s->bnd, s->sc, jd, s->heavyBlocks, st);
        })) != cudaSuccess)
     return set_err_cuda(e, "heavy");
+  if (s->decomposed) {
+    // the second setFaceBCs, and the GLM cleaning speed over all ranks (glmSpeedComm)
+    if (int rc = exchange_faces(s, false)) return rc;
+    if (eq == EQ_GLM) {
+      unsigned long long bits[2];
+      CK(cudaMemcpyAsync(bits, &s->sc->glm_lam_bits, sizeof(bits), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      double v[2] = {bits_to_double(bits[0]), bits_to_double(bits[1])};
+      if (int rc = reduce_all(s, KFVM_REDUCE_MAX, v, 2)) return rc;
+      std::memcpy(bits, v, sizeof(bits));
+      CK(cudaMemcpyAsync(&s->sc->glm_lam_bits, bits, sizeof(bits), cudaMemcpyHostToDevice, st));
+      CK(cudaStreamSynchronize(st));
+    }
+  }
   if ((e = run(s, KFVM_KCLASS_RIEMANN, dim,
                [&] { return launch_riemann(dim, eq, s->F, s->G, s->g, s->sc, s->sameOn, st); })) !=
       cudaSuccess)
@@ -502,12 +609,6 @@ int eval_into_K(kfvm_solver *s, int b) {
   return KFVM_OK;
 }
 
-double bits_to_double(unsigned long long b) {
-  double d;
-  std::memcpy(&d, &b, sizeof(d));
-  return d;
-}
-
 // tail of Solver::Solver: Uprev = U, prime FSAL, dt = 0.01 cfl dmin / maxVel
 int prime(kfvm_solver *s) {
   s->iCur = s->iPrev;
@@ -527,7 +628,8 @@ int prime(kfvm_solver *s) {
   CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(kfvm::DevScalars), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   if (s->hsc->fault) return fail(KFVM_ERR_CUDA, kFaultMsg);
-  const double maxVel = bits_to_double(s->hsc->maxvel_bits);
+  double maxVel = bits_to_double(s->hsc->maxvel_bits);
+  if (int rc2 = reduce_all(s, KFVM_REDUCE_MAX, &maxVel, 1)) return rc2;  // rhsSpeedComm
   s->nWenoLast = s->hsc->napplied;
   s->dt = 0.01 * s->cfg.cfl * s->dmin / maxVel;
   s->primed = true;
@@ -594,10 +696,19 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
     if (s->hsc->fault) return fail(KFVM_ERR_CUDA, kFaultMsg);
     maxVel = bits_to_double(s->hsc->maxvel_bits);
     s->nWenoLast = s->hsc->napplied;
-    update_same_mode(s);
-    const double nDofs = (double)(s->g.n * s->nv);
-    const double posFlag = s->hsc->posmin;
-    errNew = 1.0 / std::sqrt(s->hsc->err / nDofs);
+    if (int rc2 = update_same_mode(s)) return rc2;
+    // over all ranks (rhsSpeedComm, timeStepErrEstComm, timeStepStatusComm): the
+    // wave-speed maximum, the error sum over every degree of freedom of the domain
+    // and the positivity minimum (the status follows from it and the error)
+    double errSum = s->hsc->err, posFlag = s->hsc->posmin;
+    if (s->decomposed) {
+      if (int rc2 = reduce_all(s, KFVM_REDUCE_MAX, &maxVel, 1)) return rc2;
+      if (int rc2 = reduce_all(s, KFVM_REDUCE_SUM, &errSum, 1)) return rc2;
+      if (int rc2 = reduce_all(s, KFVM_REDUCE_MIN, &posFlag, 1)) return rc2;
+    }
+    const double nDofs = (double)(s->g.n * s->nv) * kfvm::cfg_nb(&s->cfg, 0) * kfvm::cfg_nb(&s->cfg, 1) *
+                         kfvm::cfg_nb(&s->cfg, 2);
+    errNew = 1.0 / std::sqrt(errSum / nDofs);
     double dtfac = std::pow(errNew, rk.ep1) * std::pow(s->errEst, rk.ep2);
     dtfac = std::isnan(dtfac) ? 1.2 : 1.0 + std::atan(dtfac - 1.0);
     if (posFlag < 0.0) lStat = KFVM_TS_UNPHYSICAL;
@@ -716,6 +827,7 @@ void kfvm_default_config(kfvm_config *c) {
   c->final_time = 1.0;
   c->rejection_limit = 4;
   c->max_steps = 1000;
+  c->nb[0] = c->nb[1] = c->nb[2] = 1;  // one block (mesh:numblocks 1 1 1)
 }
 
 int kfvm_stencil_build(const kfvm_config *cfg, kfvm_stencil *out) {
@@ -750,9 +862,12 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
     if ((cfg->bc[2 * d] == KFVM_BC_PERIODIC) != (cfg->bc[2 * d + 1] == KFVM_BC_PERIODIC))
       return fail(KFVM_ERR_ARG, "periodic boundaries must come in pairs");
     for (int f = 2 * d; f < 2 * d + 2; f++)
-      if (cfg->bc[f] < KFVM_BC_PERIODIC || cfg->bc[f] > KFVM_BC_NOSLIP)
-        return fail(KFVM_ERR_ARG, "unknown boundary condition (periodic, outflow, reflecting, noslip)");
+      if (cfg->bc[f] < KFVM_BC_PERIODIC || cfg->bc[f] > KFVM_BC_EXCHANGE)
+        return fail(KFVM_ERR_ARG, "unknown boundary condition (periodic, outflow, reflecting, noslip, exchange)");
   }
+  for (int d = 0; d < 3; d++)
+    if (cfg->nb[d] > 1 && (cfg->block[d] < 0 || cfg->block[d] >= cfg->nb[d]))
+      return fail(KFVM_ERR_ARG, "block coordinate outside the block counts");
   kfvm_solver *s = new kfvm_solver();
   s->cfg = *cfg;
   s->cfg.nz = nz;
@@ -780,15 +895,21 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
     g.fdim[d][2] = g.nz + (d == 2);
     g.nface[d] = g.fdim[d][0] * g.fdim[d][1] * g.fdim[d][2];
   }
-  g.dx = (cfg->xup - cfg->xlo) / cfg->nx;
-  g.dy = (cfg->yup - cfg->ylo) / cfg->ny;
-  g.dz = (cfg->zup - cfg->zlo) / nz;
+  // cell sizes and this block's global offset (Geometry.H:28-31; nb = 1: one domain)
+  g.dx = cfg_dx(cfg, 0);
+  g.dy = cfg_dx(cfg, 1);
+  g.dz = cfg_dx(cfg, 2);
+  for (int d = 0; d < 3; d++) {
+    g.off[d] = cfg_offset(cfg, d);
+    g.gn[d] = cfg_n(cfg, d) * cfg_nb(cfg, d);
+  }
   g.rdx = 1.0 / g.dx;
   g.rdy = 1.0 / g.dy;
   g.rdz = 1.0 / g.dz;
   for (int f = 0; f < 6; f++) {
     g.bc[f] = cfg->bc[f];
     g.bflip[f] = wall_flip(cfg->bc[f], f / 2, cfg->eq == KFVM_EQ_MHD_GLM);
+    if (f < 2 * cfg->dim && cfg->bc[f] == KFVM_BC_EXCHANGE) s->decomposed = true;
   }
   g.gamma = cfg->gamma;
   g.rs = cfg->rs;
@@ -914,6 +1035,7 @@ void kfvm_destroy(kfvm_solver *s) {
   cudaFree(s->ssum);
   cudaFree(s->fsums);
   cudaFree(s->sc);
+  for (int i = 0; i < 4; i++) cudaFree(s->xbuf[i]);
   if (s->hsc) cudaFreeHost(s->hsc);
   cudaFree(s->mlp.wb);
   cudaFree(s->mlp.wq);
@@ -983,7 +1105,9 @@ int kfvm_eval_rhs(kfvm_solver *s, double t, double *rhs, double *max_vel) {
   CK(cudaStreamSynchronize(s->stream));
   if (s->hsc->fault) return fail(KFVM_ERR_CUDA, kFaultMsg);
   s->nWenoLast = s->hsc->napplied;
-  if (max_vel) *max_vel = bits_to_double(s->hsc->maxvel_bits);
+  double mv = bits_to_double(s->hsc->maxvel_bits);
+  if (int rc2 = reduce_all(s, KFVM_REDUCE_MAX, &mv, 1)) return rc2;  // rhsSpeedComm
+  if (max_vel) *max_vel = mv;
   return KFVM_OK;
 }
 
@@ -1219,8 +1343,8 @@ int kfvm_mlp_collect(kfvm_solver *s, double tau, double keep_frac, uint64_t seed
   auto &M = s->mlp;
   if (!M.cap) return fail(KFVM_ERR_STATE, "kfvm_mlp_reserve first");
   const int b = s->iCur;
-  cudaError_t e = run(s, KFVM_KCLASS_BC, 1, [&] { return kfvm::launch_bc(s->dim, s->eq, s->Ub[b], s->g, s->stream); });
-  if (e != cudaSuccess) return set_err_cuda(e, "bc");
+  if (int rc = fill_halo(s, b)) return rc;
+  cudaError_t e;
   // labels, pairs, then the kept cells in cell order (a stable select)
   e = run(s, KFVM_KCLASS_OTHER, 3, [&] {
     return kfvm::launch_mlp_select(s->dim, s->eq, s->Ub[b], s->g, s->dS, tau, keep_frac, seed, M.tiles, M.flags,
@@ -1331,9 +1455,11 @@ int kfvm_mlp_probability(kfvm_solver *s, float *out_host) {
   cudaError_t e;
   if ((e = cudaMalloc((void **)&d, s->g.n * sizeof(float))) != cudaSuccess) return set_err_cuda(e, "alloc");
   const int b = s->iCur;
-  e = kfvm::launch_bc(s->dim, s->eq, s->Ub[b], s->g, s->stream);
-  if (e == cudaSuccess)
-    e = kfvm::launch_mlp_prob(s->dim, s->eq, s->Ub[b], s->g, s->mlp.tiles, s->mlp.img, d, s->sc,
+  if (int rc = fill_halo(s, b)) {
+    cudaFree(d);
+    return rc;
+  }
+  e = kfvm::launch_mlp_prob(s->dim, s->eq, s->Ub[b], s->g, s->mlp.tiles, s->mlp.img, d, s->sc,
                               s->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(out_host, d, s->g.n * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
@@ -1400,6 +1526,8 @@ int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
   const int64_t nd = dir == 0 ? g.nx : (dir == 1 ? g.ny : g.nz);
   const int64_t stride = dir == 0 ? 1 : (dir == 1 ? fx : fx * fy);
   const bool per = g.bc[2 * dir] == KFVM_BC_PERIODIC;
+  // an exchange face's outer slot already holds the neighbour's states
+  const bool xlo = g.bc[2 * dir] == KFVM_BC_EXCHANGE, xhi = g.bc[2 * dir + 1] == KFVM_BC_EXCHANGE;
   const unsigned flo = g.bflip[2 * dir], fhi = g.bflip[2 * dir + 1];
   for (int64_t k = 0; k < fz; k++)
     for (int64_t j = 0; j < fy; j++)
@@ -1414,11 +1542,86 @@ int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
               out[s0 + lo] = out[s0 + hi];
               out[s1 + hi] = out[s1 + lo];
             } else {
-              out[s0 + lo] = (flo >> v) & 1u ? -out[s1 + lo] : out[s1 + lo];
-              out[s1 + hi] = (fhi >> v) & 1u ? -out[s0 + hi] : out[s0 + hi];
+              if (!xlo) out[s0 + lo] = (flo >> v) & 1u ? -out[s1 + lo] : out[s1 + lo];
+              if (!xhi) out[s1 + hi] = (fhi >> v) & 1u ? -out[s0 + hi] : out[s0 + hi];
             }
           }
       }
+  return KFVM_OK;
+}
+
+int kfvm_block_config(const kfvm_config *blocks, int32_t rank, kfvm_config *out, int32_t neighbors[6]) {
+  if (!blocks || !out) return fail(KFVM_ERR_ARG, "null argument");
+  const int dim = blocks->dim;
+  if (dim != 2 && dim != 3) return fail(KFVM_ERR_ARG, "dim must be 2 or 3");
+  int nb[3];
+  for (int d = 0; d < 3; d++) {
+    nb[d] = d < dim ? kfvm::cfg_nb(blocks, d) : 1;
+    if (d >= dim && blocks->nb[d] > 1) return fail(KFVM_ERR_ARG, "blocks along z in a 2D domain");
+  }
+  const int64_t nranks = (int64_t)nb[0] * nb[1] * nb[2];
+  if (rank < 0 || rank >= nranks) return fail(KFVM_ERR_ARG, "rank outside the block count");
+  for (int f = 0; f < 2 * dim; f++)
+    if (blocks->bc[f] == KFVM_BC_EXCHANGE) return fail(KFVM_ERR_ARG, "the domain's own faces cannot be exchange faces");
+  kfvm_config c = *blocks;
+  // MPI_Cart_create's row-major order: the last axis varies fastest
+  int b[3];
+  b[2] = rank % nb[2];
+  b[1] = (rank / nb[2]) % nb[1];
+  b[0] = rank / (nb[2] * nb[1]);
+  int32_t nbr[6];
+  for (int d = 0; d < 3; d++) {
+    c.nb[d] = nb[d];
+    c.block[d] = b[d];
+    for (int side = 0; side < 2; side++) {
+      const int f = 2 * d + side;
+      nbr[f] = -1;
+      if (d >= dim || nb[d] == 1) continue;
+      const bool per = blocks->bc[f] == KFVM_BC_PERIODIC;
+      int nbd = b[d] + (side == 0 ? -1 : 1);
+      if (nbd < 0 || nbd >= nb[d]) {
+        if (!per) continue;  // a physical face of the domain
+        nbd = (nbd + nb[d]) % nb[d];
+      }
+      int q[3] = {b[0], b[1], b[2]};
+      q[d] = nbd;
+      nbr[f] = (q[0] * nb[1] + q[1]) * nb[2] + q[2];
+      c.bc[f] = KFVM_BC_EXCHANGE;
+    }
+  }
+  *out = c;
+  if (neighbors)
+    for (int f = 0; f < 6; f++) neighbors[f] = nbr[f];
+  return KFVM_OK;
+}
+
+int kfvm_set_exchange(kfvm_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (!s->decomposed) return fail(KFVM_ERR_STATE, "no exchange faces in this solver's configuration");
+  if (!ex || !ar) return fail(KFVM_ERR_ARG, "both callbacks are required");
+  // one buffer size for every use: the largest cell slab or face plane (with the
+  // indicator) over the axes
+  const int nqf = s->dim == 2 ? s->g.nq : s->g.nq * s->g.nq;
+  int64_t bytes = 0;
+  for (int d = 0; d < s->dim; d++) {
+    bytes = std::max(bytes, kfvm::cell_slab_values(s->g, s->dim, s->nv, d) * (int64_t)sizeof(double));
+    bytes = std::max(bytes, kfvm::face_plane_bytes(s->g, nqf, s->nv, d, true));
+  }
+  if (!s->xbuf[0]) {
+    for (int i = 0; i < 4; i++) {
+      cudaError_t e = cudaMalloc((void **)&s->xbuf[i], (size_t)bytes);
+      if (e != cudaSuccess) {
+        for (int k = 0; k <= i; k++) {
+          cudaFree(s->xbuf[k]);
+          s->xbuf[k] = nullptr;
+        }
+        return set_err_cuda(e, "alloc exchange buffers");
+      }
+    }
+  }
+  s->xfn = ex;
+  s->rfn = ar;
+  s->xuser = user;
   return KFVM_OK;
 }
 
@@ -1489,7 +1692,7 @@ int kfvm_flow_stats(kfvm_solver *s, double *stats, int32_t *n_stats) {
   double *U = s->Ub[s->iCur];
   // the halo as the boundary conditions set it (the reference relies on the last
   // evaluation having set it; filling again gives the same values)
-  CK(launch_bc(s->dim, s->eq, U, s->g, s->stream));
+  if (int rc = fill_halo(s, s->iCur)) return rc;
   CK(launch_stats(s->dim, s->eq, U, s->g, dvol / volume, s->spart, s->ssum, s->stream));
   s->launches += s->eq == KFVM_EQ_SRHYDRO ? 1 : 3;
   double h[3];
@@ -1549,7 +1752,7 @@ int kfvm_apply_forcing(kfvm_solver *s, const double *modes_in, double *modes_out
     x ^= x >> 31;
     forcing_draw(s->dim, (uint32_t)(x >> 32), m.data());
   }
-  const double lo[3] = {s->cfg.xlo, s->cfg.ylo, s->cfg.zlo};
+  const double lo[3] = {cfg_lo(&s->cfg, 0), cfg_lo(&s->cfg, 1), cfg_lo(&s->cfg, 2)};
   double *U = s->Ub[s->iCur];
   CK(cudaMemcpyAsync(s->fmodes, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   CK(launch_forcing_integrate(s->dim, U, s->g, s->fmodes, nm, s->fpar.ratio, lo, s->part, s->fsums, s->stream));
@@ -1557,8 +1760,9 @@ int kfvm_apply_forcing(kfvm_solver *s, const double *modes_in, double *modes_out
   double ab[2];
   CK(cudaMemcpyAsync(ab, s->fsums, sizeof(ab), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
-  // Solver::forceStrComm (Solver.cpp:395-409): the root of A s^2 + B s + C = 0 with
-  // C = -edot dt / dvol
+  // Solver::forceStrComm (Solver.cpp:395-409): the integrals summed over all ranks,
+  // then the root of A s^2 + B s + C = 0 with C = -edot dt / dvol
+  if (int rc = reduce_all(s, KFVM_REDUCE_SUM, ab, 2)) return rc;
   const double dvol = s->dim == 2 ? s->g.dx * s->g.dy : s->g.dx * s->g.dy * s->g.dz;
   const double A = ab[0], B = ab[1], C = -s->fpar.edot * s->dt / dvol;
   const double str = (-B + std::sqrt(std::fmax(0.0, B * B - 4.0 * A * C))) / (2.0 * A);

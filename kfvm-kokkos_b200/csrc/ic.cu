@@ -12,6 +12,7 @@
 
 #include <cstdint>
 
+#include "geometry.h"
 #include "kernels.cuh"
 #include "launch.h"
 
@@ -26,7 +27,8 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
 
 struct IcParams {
   int kind, dim, eq;
-  double gamma, xlo, xup, ylo, yup, zlo, zup;
+  double gamma, xlo, xup, ylo, yup, zlo, zup;  // the whole domain
+  double x0, y0, z0;                            // this block's first face per axis
 };
 
 __device__ void ic_point(const IcParams &p, double x, double y, double z, double noise,
@@ -193,11 +195,12 @@ __global__ void __launch_bounds__(128) ic_kernel(IcParams p, uint64_t seed, doub
     wt[0] = wt[1] = 1.0 / 2.0;
     wt[2] = 0.0;
   }
-  const double xc = g.dx * (double(i) + 0.5) + p.xlo, yc = g.dy * (double(j) + 0.5) + p.ylo;
-  const double zc = g.dz * (double(k) + 0.5) + p.zlo;
+  const double xc = g.dx * (double(i) + 0.5) + p.x0, yc = g.dy * (double(j) + 0.5) + p.y0;
+  const double zc = g.dz * (double(k) + 0.5) + p.z0;
   double noise = 0.0;
   if (p.kind == KFVM_IC_KELVIN_HELMHOLTZ) {
-    const uint64_t gi = (uint64_t)((k * g.ny + j) * g.nx + i);
+    // the cell's index in the whole domain (this block's offset added)
+    const uint64_t gi = (uint64_t)(((k + g.off[2]) * g.gn[1] + (j + g.off[1])) * g.gn[0] + (i + g.off[0]));
     const double u01 = (double)(splitmix64(seed ^ gi) >> 11) * (1.0 / 9007199254740992.0);
     noise = 1.0e-3 * (2.0 * u01 - 1.0);
   }
@@ -225,7 +228,8 @@ __global__ void __launch_bounds__(128) ic_kernel(IcParams p, uint64_t seed, doub
 
 cudaError_t launch_ic(int dim, int eq, int ic_kind, uint64_t seed, const kfvm_config &cfg,
                       double *U, const Grid &g, cudaStream_t s) {
-  IcParams p{ic_kind, dim, eq, cfg.gamma, cfg.xlo, cfg.xup, cfg.ylo, cfg.yup, cfg.zlo, cfg.zup};
+  IcParams p{ic_kind, dim, eq, cfg.gamma, cfg.xlo, cfg.xup, cfg.ylo, cfg.yup, cfg.zlo, cfg.zup,
+             cfg_lo(&cfg, 0), cfg_lo(&cfg, 1), cfg_lo(&cfg, 2)};
   const dim3 grid((unsigned)((g.nx + kBlockX - 1) / kBlockX), (unsigned)((g.ny + kBlockY - 1) / kBlockY),
                   (unsigned)g.nz);
   const dim3 blk(kBlockX, kBlockY);

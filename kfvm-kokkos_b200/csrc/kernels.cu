@@ -359,7 +359,7 @@ __device__ __forceinline__ void kxrcf_face(const Grid &g, int fc, int64_t i, int
   const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
   if (m == 0 || m == nd) {
     if (g.bc[fc] == KFVM_BC_PERIODIC) oidx = m == 0 ? fidx + nd * stride : fidx - nd * stride;
-    else oth = own;
+    else if (g.bc[fc] != KFVM_BC_EXCHANGE) oth = own;  // an exchange face holds the neighbour's slot
   }
 }
 
@@ -899,12 +899,13 @@ __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
     int64_t f0 = fidx, f1 = fidx;
     int s0 = 0, s1 = 1;
     const int64_t stride = D == 0 ? 1 : (D == 1 ? fx : fx * fy);
+    // (an exchange face holds the neighbour's state in its own outer slot)
     if (m == 0) {
       if (g.bc[2 * D] == KFVM_BC_PERIODIC) f0 = fidx + nd * stride;
-      else s0 = 1;
+      else if (g.bc[2 * D] != KFVM_BC_EXCHANGE) s0 = 1;
     } else if (m == nd) {
       if (g.bc[2 * D + 1] == KFVM_BC_PERIODIC) f1 = fidx - nd * stride;
-      else s1 = 0;
+      else if (g.bc[2 * D + 1] != KFVM_BC_EXCHANGE) s1 = 0;
     }
     const double ch = EQ == EQ_GLM ? __longlong_as_double((long long)sc->glm_lam_bits) -
                                          __longlong_as_double((long long)sc->glm_vel_bits)
@@ -1007,13 +1008,13 @@ __device__ void glm_sources(const double *__restrict__ Uc, const Grid &g, int64_
     unsigned flip = 0u;
     if (m == 0 && s == 0) {
       if (g.bc[2 * d] == KFVM_BC_PERIODIC) fidx += nd * stride;
-      else {
+      else if (g.bc[2 * d] != KFVM_BC_EXCHANGE) {
         s = 1;
         flip = g.bflip[2 * d];
       }
     } else if (m == nd && s == 1) {
       if (g.bc[2 * d + 1] == KFVM_BC_PERIODIC) fidx -= nd * stride;
-      else {
+      else if (g.bc[2 * d + 1] != KFVM_BC_EXCHANGE) {
         s = 0;
         flip = g.bflip[2 * d + 1];
       }
@@ -1465,13 +1466,11 @@ struct Launch {
   static cudaError_t heavy(const double *U, const Grid &g, const DevStencil *S, double *theta,
                            double *const *F, double *src, const uint32_t *heavy, const double *bnd,
                            DevScalars *sc, const JudgeArgs &jd, int heavy_blocks, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-      cudaError_t e = cudaFuncSetAttribute(heavy_var_kernel<DIM, EQ, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)HeavyShape<DIM, EQ, NQ>::BYTES);
-      if (e != cudaSuccess) return e;
-      attr = true;
-    }
+    // set once per process (a function-local static is initialised once, also when
+    // several host threads drive solvers)
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        heavy_var_kernel<DIM, EQ, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HeavyShape<DIM, EQ, NQ>::BYTES);
+    if (attr != cudaSuccess) return attr;
     heavy_var_kernel<DIM, EQ, NQ><<<heavy_blocks, dim3(32, NV), HeavyShape<DIM, EQ, NQ>::BYTES, s>>>(
         U, g, S, theta, F[0], F[1], F[2], src, heavy, bnd, sc, jd);
     return cudaGetLastError();

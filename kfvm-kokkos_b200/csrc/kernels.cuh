@@ -52,6 +52,7 @@ struct Grid {
   double gamma, ch_init;
   int rs;
   int64_t loff[KFVM_MAX_CELLS]; // stencil offsets in the padded array
+  int64_t off[3], gn[3];        // this block's first cell and the domain's cells per axis
 };
 
 // stencil on the device: weights plus linear offsets in the padded array, and the

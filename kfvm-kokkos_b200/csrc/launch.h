@@ -29,6 +29,18 @@ struct StageArgs {
 
 int64_t stage_blocks(const Grid &g);
 cudaError_t launch_bc(int dim, int eq, double *U, const Grid &g, cudaStream_t s);
+// decomposed domains (exchange.cu): the halo fill of one axis (its non-exchange
+// faces), and the pack (pack = true) / unpack of one side's r cell layers of an
+// axis ([v][layer][position], cell_slab_values values) and of one boundary face
+// plane (this block's slot packed, the outer slot unpacked; face_plane_bytes,
+// the FP32 indicator after the states when W is given)
+cudaError_t launch_bc_axis(int dim, int nv, double *U, const Grid &g, int d, cudaStream_t s);
+int64_t cell_slab_values(const Grid &g, int dim, int nv, int d);
+int64_t face_plane_bytes(const Grid &g, int nqf, int nv, int d, bool withW);
+cudaError_t launch_cell_slab(int dim, int nv, double *U, const Grid &g, int d, int side, bool pack, double *buf,
+                             cudaStream_t s);
+cudaError_t launch_face_plane(double *F, float *W, const Grid &g, int nqf, int nv, int d, int side, bool pack,
+                              double *buf, cudaStream_t s);
 // interior state between the host order (variable, k, j, i) in a flat device
 // buffer and the padded layout; one launch for all variables
 cudaError_t launch_interior(double *Up, double *flat, const Grid &g, int nv, bool toPadded, cudaStream_t s);

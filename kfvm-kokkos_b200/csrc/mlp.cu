@@ -551,13 +551,11 @@ static cudaError_t tc_t(const double *U, const Grid &g, float2 *rp, int64_t rpx,
                         const uint8_t *img, const double *theta, uint8_t *flag, uint8_t *pred, float *prob,
                         DevScalars *sc, float thr, cudaStream_t s) {
   using C = MlpTc<DIM>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(mlp_tc_kernel<DIM, EQ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         C::SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  // set once per process (a function-local static is initialised once, also when
+  // several host threads drive solvers)
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(mlp_tc_kernel<DIM, EQ, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+  if (attr != cudaSuccess) return attr;
   const int64_t planes = DIM == 3 ? g.nz + 2 * kRad : 1;
   const int64_t np = g.px * g.py * planes;
   mlp_rp_kernel<EQ><<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, g, planes, rpx, rp);
@@ -637,15 +635,17 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_
 
 int encode_tensor_map_8b(CUtensorMap *map, const void *base, int rank, const uint64_t *dims,
                          const uint64_t *strides_bytes, const uint32_t *box) {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
+  // looked up once (a function-local static is initialised once, also when several
+  // host threads drive solvers)
+  static const EncodeTiledFn fn = []() -> EncodeTiledFn {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !p)
-      return -1;
-    fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  if (!fn) return -1;
   if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return -2;
   cuuint64_t d[5], st[4];
   cuuint32_t bx[5], es[5];
@@ -696,19 +696,15 @@ cudaError_t launch_mlp_train_step(int dim, const uint16_t *feats, const uint8_t 
   const float inv = 1.0f / (float)(blocks * kTrainB);
   cudaError_t e;
   if (dim == 2) {
-    static bool attr = false;
-    if (!attr && (e = cudaFuncSetAttribute(mlp_train_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)TrainSmem<2>::BYTES)) != cudaSuccess)
-      return e;
-    attr = true;
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        mlp_train_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TrainSmem<2>::BYTES);
+    if (attr != cudaSuccess) return attr;
     mlp_train_kernel<2><<<blocks, 256, TrainSmem<2>::BYTES, s>>>(feats, labels, n, wq, gpart, lpart, pos_weight,
                                                                  inv, seed, t);
   } else {
-    static bool attr = false;
-    if (!attr && (e = cudaFuncSetAttribute(mlp_train_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)TrainSmem<3>::BYTES)) != cudaSuccess)
-      return e;
-    attr = true;
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        mlp_train_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TrainSmem<3>::BYTES);
+    if (attr != cudaSuccess) return attr;
     mlp_train_kernel<3><<<blocks, 256, TrainSmem<3>::BYTES, s>>>(feats, labels, n, wq, gpart, lpart, pos_weight,
                                                                  inv, seed, t);
   }

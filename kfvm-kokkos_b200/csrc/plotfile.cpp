@@ -27,6 +27,7 @@
 #include <string>
 #include <vector>
 
+#include "geometry.h"
 #include "../../include/kfvm_b200.h"
 #include "sr_eos.h"
 
@@ -117,12 +118,13 @@ int plotfile_write(const kfvm_config *cfg, const char *dir, const char *base, in
   const size_t n = (size_t)g.n;
   bool ok = true;
   // nodal coordinates (WriterPDI.cpp:38-52; z uses dmin in 2D)
-  const double dx = (cfg->xup - cfg->xlo) / (double)g.nx, dy = (cfg->yup - cfg->ylo) / (double)g.ny;
-  const double dz = cfg->dim == 3 ? (cfg->zup - cfg->zlo) / (double)g.nz : std::fmin(dx, dy);
+  const double dx = kfvm::cfg_dx(cfg, 0), dy = kfvm::cfg_dx(cfg, 1);
+  const double dz = cfg->dim == 3 ? kfvm::cfg_dx(cfg, 2) : std::fmin(dx, dy);
+  const double x0 = kfvm::cfg_lo(cfg, 0), y0 = kfvm::cfg_lo(cfg, 1), z0 = cfg->dim == 3 ? kfvm::cfg_lo(cfg, 2) : 0.0;
   std::vector<double> xc(g.nx + 1), yc(g.ny + 1), zc(g.nz + 1);
-  for (int64_t i = 0; i <= g.nx; i++) xc[i] = (double)i * dx + cfg->xlo;
-  for (int64_t j = 0; j <= g.ny; j++) yc[j] = (double)j * dy + cfg->ylo;
-  for (int64_t k = 0; k <= g.nz; k++) zc[k] = (double)k * dz + (cfg->dim == 3 ? cfg->zlo : 0.0);
+  for (int64_t i = 0; i <= g.nx; i++) xc[i] = (double)i * dx + x0;
+  for (int64_t j = 0; j <= g.ny; j++) yc[j] = (double)j * dy + y0;
+  for (int64_t k = 0; k <= g.nz; k++) zc[k] = (double)k * dz + z0;
   ok = ok && write_raw(stem + ".xcoord.bin", xc.data(), xc.size());
   ok = ok && write_raw(stem + ".ycoord.bin", yc.data(), yc.size());
   ok = ok && write_raw(stem + ".zcoord.bin", zc.data(), zc.size());

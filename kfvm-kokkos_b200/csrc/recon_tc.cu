@@ -592,24 +592,18 @@ static cudaError_t recon_tc_launch(const double *U, const CUtensorMap *umap, con
   const dim3 grid((unsigned)((g.nx + kBlockX - 1) / kBlockX), (unsigned)((g.ny + kBlockY - 1) / kBlockY),
                   (unsigned)g.nz);
   if (umap) {
-    static bool attrT = false; // the attribute is per function and process-wide
-    if (!attrT) {
-      cudaError_t e = cudaFuncSetAttribute(recon_tc_tma_kernel<DIM, EQ>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-      if (e != cudaSuccess) return e;
-      attrT = true;
-    }
+    // the attribute is per function and process-wide: set once (a function-local
+    // static is initialised once, also when several host threads drive solvers)
+    static const cudaError_t attrT =
+        cudaFuncSetAttribute(recon_tc_tma_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+    if (attrT != cudaSuccess) return attrT;
     recon_tc_tma_kernel<DIM, EQ><<<grid, kTcThreads, L::SMEM, s>>>(
         *umap, U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd, sc);
     return cudaGetLastError();
   }
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(recon_tc_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Sh::SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(recon_tc_kernel<DIM, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::SMEM);
+  if (attr != cudaSuccess) return attr;
   recon_tc_kernel<DIM, EQ><<<grid, kTcThreads, Sh::SMEM, s>>>(
       U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd, sc);
   return cudaGetLastError();

@@ -25,6 +25,7 @@
 #include <cstring>
 #include <vector>
 
+#include "geometry.h"
 #include "../../include/kfvm_b200.h"
 
 extern "C" {
@@ -349,8 +350,8 @@ int build_stencil(const kfvm_config *cfg, kfvm_stencil *st) {
   st->nqc = dim == 2 ? nq * nq : nq * nq * nq;
   const int nqf = st->nqf, nqc = st->nqc;
   const int polyDeg[3] = {3, 1, 1};
-  const double dx = (cfg->xup - cfg->xlo) / cfg->nx, dy = (cfg->yup - cfg->ylo) / cfg->ny,
-               dz = (cfg->zup - cfg->zlo) / cfg->nz;
+  // the cell sizes of the whole domain (Geometry.H:28-31)
+  const double dx = kfvm::cfg_dx(cfg, 0), dy = kfvm::cfg_dx(cfg, 1), dz = kfvm::cfg_dx(cfg, 2);
   const double eps = 1.0 / (cfg->lfac * std::sqrt(2.0));
 
   // Gauss-Legendre abscissae on (-1/2, 1/2) (src/numeric/Numeric.cpp:9-46)

@@ -85,6 +85,9 @@ def lib():
         L.kfvm_forcing_draw.argtypes = [I32, C.c_uint32, P]
         L.kfvm_set_forcing.argtypes = [P, C.POINTER(abi.KfvmForcing)]
         L.kfvm_apply_forcing.argtypes = [P, P, P, P]
+        L.kfvm_block_config.argtypes = [C.POINTER(abi.KfvmConfig), I32, C.POINTER(abi.KfvmConfig),
+                                        C.POINTER(I32)]
+        L.kfvm_set_exchange.argtypes = [P, abi.EXCHANGE_FN, abi.ALLREDUCE_FN, P]
         L.kfvm_last_error.restype = C.c_char_p
         _LIB = L
     return _LIB
@@ -170,6 +173,16 @@ def stencil(cfg):
     return st
 
 
+def block_config(blocks, rank):
+    """Rank `rank`'s configuration of a decomposed domain and the ranks across its six
+    faces (-1: none): the reference's LayoutMPI::distributeBlocks.  `blocks` holds
+    one block's cells, the whole domain's extents and nb."""
+    out = abi.KfvmConfig()
+    nbr = (C.c_int32 * 6)()
+    _check(lib().kfvm_block_config(C.byref(blocks), int(rank), C.byref(out), nbr), "kfvm_block_config")
+    return out, list(nbr)
+
+
 class Solver:
     """One solver on the current CUDA device (Solver::Solver .. Solver::Solve)."""
 
@@ -236,6 +249,13 @@ class Solver:
 
     def set_time(self, t, dt):
         _check(lib().kfvm_set_time(self.h, float(t), float(dt)), "kfvm_set_time")
+
+    def set_exchange(self, transport):
+        """Install a transport (decomp.DistExchange or a LocalExchange endpoint) whose
+        exchange_fn / allreduce_fn carry this block's boundary data between ranks."""
+        self._transport = transport  # the callbacks must outlive the solver's use of them
+        _check(lib().kfvm_set_exchange(self.h, transport.exchange_fn, transport.allreduce_fn, None),
+               "kfvm_set_exchange")
 
     def set_indicator(self, ind):
         _check(lib().kfvm_set_indicator(self.h, int(ind)), "kfvm_set_indicator")

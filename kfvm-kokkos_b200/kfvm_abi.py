@@ -11,7 +11,8 @@ import struct
 KFVM_EQ_HYDRO, KFVM_EQ_NAVIERSTOKES, KFVM_EQ_MHD_GLM, KFVM_EQ_SRHYDRO = 0, 1, 2, 3
 KFVM_RS_LLF, KFVM_RS_HLL, KFVM_RS_HLLC = 0, 1, 2
 KFVM_RK_THREESTARP, KFVM_RK_FOURSTARP, KFVM_RK_SSP4_3_2, KFVM_RK_SSP10_4_3 = 0, 1, 2, 3
-KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW, KFVM_BC_REFLECTING, KFVM_BC_NOSLIP = 0, 1, 2, 3
+KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW, KFVM_BC_REFLECTING, KFVM_BC_NOSLIP, KFVM_BC_EXCHANGE = 0, 1, 2, 3, 4
+KFVM_REDUCE_SUM, KFVM_REDUCE_MAX, KFVM_REDUCE_MIN = 0, 1, 2
 KFVM_TS_ACCEPTED, KFVM_TS_TOLERANCE, KFVM_TS_UNPHYSICAL = 0, 1, 2
 KFVM_IND_KXRCF, KFVM_IND_ALL, KFVM_IND_NONE, KFVM_IND_MLP = 0, 1, 2, 3
 KFVM_PREC_FP64, KFVM_PREC_TF32X3 = 0, 1
@@ -22,6 +23,13 @@ KFVM_FORCING_MAX_MODES = 57
 
 KFVM_MAX_CELLS, KFVM_MAX_SUB, KFVM_MAX_BIAS, KFVM_MAX_BCELLS = 33, 8, 6, 11
 KFVM_MAX_INDIC, KFVM_MAX_FACEQ, KFVM_MAX_CELLQ = 19, 9, 27
+
+
+# the exchange and allreduce callbacks of kfvm_set_exchange (kfvm_exchange_fn,
+# kfvm_allreduce_fn)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                          C.c_int64, C.c_int64)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_int32)
 
 
 class KfvmConfig(C.Structure):
@@ -38,7 +46,7 @@ class KfvmConfig(C.Structure):
         ("rejection_thresh", C.c_double), ("min_dt", C.c_double),
         ("final_time", C.c_double),
         ("rejection_limit", C.c_int32), ("max_steps", C.c_int32),
-        ("have_sources", C.c_int32), ("pad_", C.c_int32),
+        ("have_sources", C.c_int32), ("nb", C.c_int32 * 3), ("block", C.c_int32 * 3), ("pad_", C.c_int32),
     ]
 
 
@@ -88,6 +96,8 @@ def default_config():
     c.cfl, c.atol, c.rtol = 0.75, stof(1e-4), stof(1e-4)
     c.rejection_thresh, c.min_dt, c.final_time = stof(0.8), stof(1e-10), 1.0
     c.rejection_limit, c.max_steps, c.have_sources = 4, 1000, 0
+    for d in range(3):
+        c.nb[d], c.block[d] = 1, 0
     return c
 
 

@@ -17,7 +17,8 @@ LIB = os.path.join(HERE, "libkfvm_b200.so")
 RUN = os.path.join(HERE, "kfvm_run")
 HOST_SOURCES = ["host/kfvm_host.cpp", "host/kfvm_run.cpp"]
 
-CU_SOURCES = ["kernels.cu", "recon_tc.cu", "mlp.cu", "ic.cu", "errest.cu", "forcing.cu", "stats.cu", "capi.cu"]
+CU_SOURCES = ["kernels.cu", "recon_tc.cu", "mlp.cu", "ic.cu", "errest.cu", "forcing.cu", "stats.cu", "exchange.cu",
+              "capi.cu"]
 CXX_SOURCES = ["stencil_weights.cpp", "plotfile.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -41,6 +41,12 @@ int orc_get_faces(orc_solver *s, int32_t dir, double *out);
 int orc_get_flags(orc_solver *s, uint8_t *weno_applied, double *theta);
 int orc_weno_departure(orc_solver *s, double *out);
 int orc_set_indicator(orc_solver *s, int32_t ind);
+/* Domain decomposition: cfg->nb and cfg->block place this solver's block in the
+ * whole domain (kfvm_block_config makes such a configuration); its
+ * KFVM_BC_EXCHANGE faces take their halo cells and outer face states from the
+ * neighbouring ranks through ex, and the maxima, sums and minima of a step go
+ * through ar, with the meaning of kfvm_set_exchange's callbacks on host buffers. */
+int orc_set_exchange(orc_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user);
 /* Quadrature and RK coefficient tables used by the oracle. */
 int orc_tables(int32_t nq, int32_t rk, double *quad, double *rkt);
 /* Initial-condition cell averages alone (no FSAL priming), SoA interior. */

@@ -57,6 +57,7 @@ def lib():
         L.orc_weno_departure.argtypes = [P, P]
         L.orc_ic_cells.argtypes = [C.POINTER(abi.KfvmConfig), I32, C.c_uint64, P]
         L.orc_tables.argtypes = [I32, I32, P, P]
+        L.orc_set_exchange.argtypes = [P, abi.EXCHANGE_FN, abi.ALLREDUCE_FN, P]
         _LIB = L
     return _LIB
 
@@ -164,6 +165,11 @@ class OracleSolver:
 
     def set_time(self, t, dt):
         assert lib().orc_set_time(self.h, float(t), float(dt)) == 0
+
+    def set_exchange(self, transport):
+        """Install a host-buffer transport for the exchange faces of a decomposed domain."""
+        self._transport = transport
+        assert lib().orc_set_exchange(self.h, transport.exchange_fn, transport.allreduce_fn, None) == 0
 
     def keep_faces(self, on=True):
         assert lib().orc_keep_faces(self.h, 1 if on else 0) == 0

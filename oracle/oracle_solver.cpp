@@ -746,6 +746,23 @@ void ic_point(int kind, const kfvm_config &c, double x, double y, double z, doub
 } // namespace
 
 // ====================================================================================
+// Geometry of a block of a decomposed domain (Geometry.H:28-31, LayoutMPI.H:72-77):
+// the configured extents are the whole domain's and nx, ny, nz one block's cells,
+// so dx = (xup - xlo) / (nx nb) and the block's first face lies at xlo + dx bxLo
+// with bxLo = block nx.  nb = 1 gives the one-domain values exactly.
+static int geo_nb(const kfvm_config &c, int d) { return c.nb[d] > 0 ? c.nb[d] : 1; }
+static int64_t geo_n(const kfvm_config &c, int d) { return d == 0 ? c.nx : (d == 1 ? c.ny : (c.dim == 3 ? c.nz : 1)); }
+static int64_t geo_off(const kfvm_config &c, int d) { return geo_nb(c, d) > 1 ? (int64_t)c.block[d] * geo_n(c, d) : 0; }
+static double geo_dx(const kfvm_config &c, int d) {
+  const double lo = d == 0 ? c.xlo : (d == 1 ? c.ylo : c.zlo), up = d == 0 ? c.xup : (d == 1 ? c.yup : c.zup);
+  return (up - lo) / (double)(geo_n(c, d) * geo_nb(c, d));
+}
+static double geo_lo(const kfvm_config &c, int d) {
+  const double lo = d == 0 ? c.xlo : (d == 1 ? c.ylo : c.zlo);
+  const int64_t b = geo_off(c, d);
+  return b == 0 ? lo : lo + geo_dx(c, d) * (double)b;
+}
+
 struct orc_solver {
   kfvm_config cfg;
   kfvm_stencil st;
@@ -775,6 +792,18 @@ struct orc_solver {
   bool lastTimeStep;
   int64_t nRhs, nWenoLast;
   int nTS;
+
+  // domain decomposition: this block's first cell and the domain's cells per axis,
+  // the block's first face per axis, the transport of orc_set_exchange and its
+  // buffers (send low, receive low, send high, receive high), a transport failure
+  int64_t off[3] = {0, 0, 0}, gn[3] = {0, 0, 0};
+  double x0[3] = {0.0, 0.0, 0.0};
+  bool decomposed = false;
+  kfvm_exchange_fn xfn = nullptr;
+  kfvm_allreduce_fn rfn = nullptr;
+  void *xuser = nullptr;
+  int xerr = 0;
+  std::vector<double> xb[4];
 
   // ---- indexing ----
   int64_t ui(int64_t i, int64_t j, int64_t k, int v) const {
@@ -816,10 +845,66 @@ double wall_coef(const orc_solver &S, int f, int v) {
   return 1.0;
 }
 
+// in-place reduction of n values over all ranks (the *Comm allreduces of
+// Solver.cpp:345-409, 532-552); nothing on one domain
+void reduce_all(orc_solver &S, int op, double *v, int n) {
+  if (!S.decomposed) return;
+  if (!S.rfn || S.rfn(S.xuser, op, v, n) != 0) S.xerr = 1;
+}
+
+// one exchange call: xb[0] to the low neighbour and xb[2] to the high one, received
+// into xb[1] (from the low neighbour's high side) and xb[3]
+void transport(orc_solver &S, int axis, bool lo, bool hi, size_t count) {
+  const int64_t bytes = (int64_t)(count * sizeof(double));
+  if (!S.xfn || S.xfn(S.xuser, axis, lo ? S.xb[0].data() : nullptr, lo ? S.xb[1].data() : nullptr,
+                      hi ? S.xb[2].data() : nullptr, hi ? S.xb[3].data() : nullptr, lo ? bytes : 0,
+                      hi ? bytes : 0) != 0)
+    S.xerr = 1;
+}
+
+// the r cell layers along one side of axis d, in one order on every rank: variable,
+// layer, then the other two axes (the lower one fastest; padded for axes filled
+// before d, interior for the others).  Interior layers are the ones sent, halo
+// layers the ones received (setCellBCs with commCellBCs*, Solver.cpp:744-784).
+template <class Fn>
+void for_slab(const orc_solver &S, int d, int side, bool halo, Fn fn) {
+  const int r = KFVM_RAD;
+  const int64_t n[3] = {S.nx, S.ny, S.nz};
+  const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+  const int64_t lo1 = a1 < d ? -r : 0, up1 = n[a1] + (a1 < d ? r : 0);
+  const int64_t lo2 = a2 < d ? -r : 0, up2 = n[a2] + (a2 < d ? r : 0);
+  size_t m = 0;
+  for (int v = 0; v < S.nv; v++)
+    for (int h = 0; h < r; h++) {
+      int64_t c[3];
+      c[d] = halo ? (side == 0 ? h - r : n[d] + h) : (side == 0 ? h : n[d] - r + h);
+      for (c[a2] = lo2; c[a2] < up2; c[a2]++)
+        for (c[a1] = lo1; c[a1] < up1; c[a1]++) fn(m++, S.ui(c[0], c[1], c[2], v));
+    }
+}
+
+void exchange_cells(orc_solver &S, std::vector<double> &B, int d) {
+  const bool lo = S.cfg.bc[2 * d] == KFVM_BC_EXCHANGE, hi = S.cfg.bc[2 * d + 1] == KFVM_BC_EXCHANGE;
+  if (!lo && !hi) return;
+  size_t count = 0;
+  for_slab(S, d, 0, false, [&](size_t, int64_t) { count++; });
+  for (auto &b : S.xb)
+    if (b.size() < count) b.resize(count);
+  if (lo) for_slab(S, d, 0, false, [&](size_t m, int64_t u) { S.xb[0][m] = B[u]; });
+  if (hi) for_slab(S, d, 1, false, [&](size_t m, int64_t u) { S.xb[2][m] = B[u]; });
+  transport(S, d, lo, hi, count);
+  if (lo) for_slab(S, d, 0, true, [&](size_t m, int64_t u) { B[u] = S.xb[1][m]; });
+  if (hi) for_slab(S, d, 1, true, [&](size_t m, int64_t u) { B[u] = S.xb[3][m]; });
+}
+
 void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
   const int r = KFVM_RAD;
   auto &c = S.cfg;
+  const bool xl = c.bc[0] != KFVM_BC_EXCHANGE, xh = c.bc[1] != KFVM_BC_EXCHANGE;
+  const bool yl = c.bc[2] != KFVM_BC_EXCHANGE, yh = c.bc[3] != KFVM_BC_EXCHANGE;
+  const bool zl = c.bc[4] != KFVM_BC_EXCHANGE, zh = c.bc[5] != KFVM_BC_EXCHANGE;
   // x: j,k interior
+  exchange_cells(S, B, 0);
   for (int64_t k = 0; k < S.nz; k++)
     for (int64_t j = 0; j < S.ny; j++)
       for (int h = 0; h < r; h++)
@@ -828,11 +913,12 @@ void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
             B[S.ui(-r + h, j, k, v)] = B[S.ui(S.nx - r + h, j, k, v)];
             B[S.ui(S.nx + h, j, k, v)] = B[S.ui(h, j, k, v)];
           } else {
-            B[S.ui(-h - 1, j, k, v)] = wall_coef(S, 0, v) * B[S.ui(h, j, k, v)];
-            B[S.ui(S.nx + h, j, k, v)] = wall_coef(S, 1, v) * B[S.ui(S.nx - h - 1, j, k, v)];
+            if (xl) B[S.ui(-h - 1, j, k, v)] = wall_coef(S, 0, v) * B[S.ui(h, j, k, v)];
+            if (xh) B[S.ui(S.nx + h, j, k, v)] = wall_coef(S, 1, v) * B[S.ui(S.nx - h - 1, j, k, v)];
           }
         }
   // y: i over the full halo range, k interior
+  exchange_cells(S, B, 1);
   for (int64_t k = 0; k < S.nz; k++)
     for (int64_t i = -r; i < S.nx + r; i++)
       for (int h = 0; h < r; h++)
@@ -841,11 +927,12 @@ void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
             B[S.ui(i, -r + h, k, v)] = B[S.ui(i, S.ny - r + h, k, v)];
             B[S.ui(i, S.ny + h, k, v)] = B[S.ui(i, h, k, v)];
           } else {
-            B[S.ui(i, -h - 1, k, v)] = wall_coef(S, 2, v) * B[S.ui(i, h, k, v)];
-            B[S.ui(i, S.ny + h, k, v)] = wall_coef(S, 3, v) * B[S.ui(i, S.ny - h - 1, k, v)];
+            if (yl) B[S.ui(i, -h - 1, k, v)] = wall_coef(S, 2, v) * B[S.ui(i, h, k, v)];
+            if (yh) B[S.ui(i, S.ny + h, k, v)] = wall_coef(S, 3, v) * B[S.ui(i, S.ny - h - 1, k, v)];
           }
         }
   if (S.dim == 3) {
+    exchange_cells(S, B, 2);
     for (int64_t j = -r; j < S.ny + r; j++)
       for (int64_t i = -r; i < S.nx + r; i++)
         for (int h = 0; h < r; h++)
@@ -854,16 +941,52 @@ void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
               B[S.ui(i, j, -r + h, v)] = B[S.ui(i, j, S.nz - r + h, v)];
               B[S.ui(i, j, S.nz + h, v)] = B[S.ui(i, j, h, v)];
             } else {
-              B[S.ui(i, j, -h - 1, v)] = wall_coef(S, 4, v) * B[S.ui(i, j, h, v)];
-              B[S.ui(i, j, S.nz + h, v)] = wall_coef(S, 5, v) * B[S.ui(i, j, S.nz - h - 1, v)];
+              if (zl) B[S.ui(i, j, -h - 1, v)] = wall_coef(S, 4, v) * B[S.ui(i, j, h, v)];
+              if (zh) B[S.ui(i, j, S.nz + h, v)] = wall_coef(S, 5, v) * B[S.ui(i, j, S.nz - h - 1, v)];
             }
           }
+  }
+}
+
+// the face states of the exchange faces of axis d (commFaceBCs*, Solver.cpp:826-1460):
+// this block's slot of each boundary face point is sent (slot 1 at the low face,
+// slot 0 at the high face) and the neighbour's arrives in the outer slot; points
+// in one order on every rank (the lower of the other two axes fastest), each with
+// its nqf x nv states
+void exchange_faces(orc_solver &S, int d) {
+  const bool lo = S.cfg.bc[2 * d] == KFVM_BC_EXCHANGE, hi = S.cfg.bc[2 * d + 1] == KFVM_BC_EXCHANGE;
+  if (!lo && !hi) return;
+  const int64_t n[3] = {S.nx, S.ny, S.nz};
+  const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+  const int64_t e1 = n[a1], e2 = n[a2], w = (int64_t)S.nqf * S.nv;
+  const size_t count = (size_t)(e1 * e2 * w);
+  for (auto &b : S.xb)
+    if (b.size() < count) b.resize(count);
+  auto at = [&](int side, int64_t t, int slot) {
+    int64_t c[3];
+    c[d] = side == 0 ? 0 : n[d];
+    c[a1] = t % e1;
+    c[a2] = t / e1;
+    return S.fs(d, c[0], c[1], c[2], slot, 0);
+  };
+  for (int64_t t = 0; t < e1 * e2; t++) {
+    if (lo) std::memcpy(&S.xb[0][t * w], at(0, t, 1), w * sizeof(double));
+    if (hi) std::memcpy(&S.xb[2][t * w], at(1, t, 0), w * sizeof(double));
+  }
+  transport(S, 3 + d, lo, hi, count);
+  for (int64_t t = 0; t < e1 * e2; t++) {
+    if (lo) std::memcpy(at(0, t, 0), &S.xb[1][t * w], w * sizeof(double));
+    if (hi) std::memcpy(at(1, t, 1), &S.xb[3][t * w], w * sizeof(double));
   }
 }
 
 // setFaceBCs (Solver.cpp:785-824 and the commFaceBCs* self-copies)
 void set_face_bcs(orc_solver &S) {
   auto &c = S.cfg;
+  for (int d = 0; d < S.dim; d++) exchange_faces(S, d);
+  const bool xl = c.bc[0] != KFVM_BC_EXCHANGE, xh = c.bc[1] != KFVM_BC_EXCHANGE;
+  const bool yl = c.bc[2] != KFVM_BC_EXCHANGE, yh = c.bc[3] != KFVM_BC_EXCHANGE;
+  const bool zl = c.bc[4] != KFVM_BC_EXCHANGE, zh = c.bc[5] != KFVM_BC_EXCHANGE;
   const int nqf = S.nqf, nv = S.nv;
   auto cp = [&](double *dst, const double *src) {
     for (int q = 0; q < nqf * nv; q++) dst[q] = src[q];
@@ -880,8 +1003,8 @@ void set_face_bcs(orc_solver &S) {
         cp(S.fs(0, S.nx, j, k, 1, 0), S.fs(0, 0, j, k, 1, 0));
         cp(S.fs(0, 0, j, k, 0, 0), S.fs(0, S.nx, j, k, 0, 0));
       } else {
-        cpw(S.fs(0, 0, j, k, 0, 0), S.fs(0, 0, j, k, 1, 0), 0);
-        cpw(S.fs(0, S.nx, j, k, 1, 0), S.fs(0, S.nx, j, k, 0, 0), 1);
+        if (xl) cpw(S.fs(0, 0, j, k, 0, 0), S.fs(0, 0, j, k, 1, 0), 0);
+        if (xh) cpw(S.fs(0, S.nx, j, k, 1, 0), S.fs(0, S.nx, j, k, 0, 0), 1);
       }
     }
   for (int64_t k = 0; k < S.nz; k++)
@@ -890,8 +1013,8 @@ void set_face_bcs(orc_solver &S) {
         cp(S.fs(1, i, S.ny, k, 1, 0), S.fs(1, i, 0, k, 1, 0));
         cp(S.fs(1, i, 0, k, 0, 0), S.fs(1, i, S.ny, k, 0, 0));
       } else {
-        cpw(S.fs(1, i, 0, k, 0, 0), S.fs(1, i, 0, k, 1, 0), 2);
-        cpw(S.fs(1, i, S.ny, k, 1, 0), S.fs(1, i, S.ny, k, 0, 0), 3);
+        if (yl) cpw(S.fs(1, i, 0, k, 0, 0), S.fs(1, i, 0, k, 1, 0), 2);
+        if (yh) cpw(S.fs(1, i, S.ny, k, 1, 0), S.fs(1, i, S.ny, k, 0, 0), 3);
       }
     }
   if (S.dim == 3) {
@@ -901,8 +1024,8 @@ void set_face_bcs(orc_solver &S) {
           cp(S.fs(2, i, j, S.nz, 1, 0), S.fs(2, i, j, 0, 1, 0));
           cp(S.fs(2, i, j, 0, 0, 0), S.fs(2, i, j, S.nz, 0, 0));
         } else {
-          cpw(S.fs(2, i, j, 0, 0, 0), S.fs(2, i, j, 0, 1, 0), 4);
-          cpw(S.fs(2, i, j, S.nz, 1, 0), S.fs(2, i, j, S.nz, 0, 0), 5);
+          if (zl) cpw(S.fs(2, i, j, 0, 0, 0), S.fs(2, i, j, 0, 1, 0), 4);
+          if (zh) cpw(S.fs(2, i, j, S.nz, 1, 0), S.fs(2, i, j, S.nz, 0, 0), 5);
         }
       }
   }
@@ -1663,18 +1786,21 @@ double eval_rhs(orc_solver &S, std::vector<double> &B, double t) {
     for (int64_t k = 0; k < S.nz; k++)
       for (int64_t j = 0; j < S.ny; j++)
         for (int64_t i = 0; i < S.nx; i++) glm_speed(S, i, j, k, maxLam, maxVel);
-    S.ph.ch = maxLam - maxVel;
+    double lv[2] = {maxLam, maxVel};
+    reduce_all(S, KFVM_REDUCE_MAX, lv, 2);  // glmSpeedComm
+    S.ph.ch = lv[0] - lv[1];
   }
   if (S.haveSources) {
     FOR_CELLS glm_sources(S, B, i, j, k);
   }
   double vEW = riemann_dir(S, 0), vNS = riemann_dir(S, 1), vTB = 0.0;
   if (S.dim == 3) vTB = riemann_dir(S, 2);
-  const double maxVel = fmax(vEW, fmax(vNS, vTB));
+  double maxVel = fmax(vEW, fmax(vNS, vTB));
   FOR_CELLS integrate_rhs(S, i, j, k);
   if (S.cfg.eq == KFVM_EQ_NAVIERSTOKES) {
     FOR_CELLS viscosity(S, B, i, j, k);
   }
+  reduce_all(S, KFVM_REDUCE_MAX, &maxVel, 1);  // rhsSpeedComm
   return maxVel;
 }
 
@@ -1749,7 +1875,12 @@ void take_step(orc_solver &S, kfvm_step_info *info) {
       const double pos = hasNan ? -1.0 : S.ph.positivity(state);
       posFlag = posFlag > pos ? pos : posFlag;
     }
-    const double nDofs = (double)(S.nx * S.ny * S.nz * nv);
+    // over all ranks: the error sum (timeStepErrEstComm) and the positivity minimum
+    // (timeStepStatusComm's maximum of the status follows from it)
+    reduce_all(S, KFVM_REDUCE_SUM, &errLoc, 1);
+    reduce_all(S, KFVM_REDUCE_MIN, &posFlag, 1);
+    const double nDofs =
+        (double)(S.nx * S.ny * S.nz * nv) * geo_nb(S.cfg, 0) * geo_nb(S.cfg, 1) * geo_nb(S.cfg, 2);
     errNew = 1.0 / sqrt(errLoc / nDofs);
     double dtfac = std::pow(errNew, rk.ep1) * std::pow(S.errEst, rk.ep2);
     dtfac = std::isnan(dtfac) ? 1.2 : 1.0 + std::atan(dtfac - 1.0);
@@ -1803,11 +1934,12 @@ void ic_cells(const orc_solver &S, int kind, uint64_t seed, std::vector<double> 
   for (int64_t k = 0; k < S.nz; k++)
     for (int64_t j = 0; j < S.ny; j++)
       for (int64_t i = 0; i < S.nx; i++) {
-        const double xc = S.dx * (double(i) + 0.5) + c.xlo, yc = S.dy * (double(j) + 0.5) + c.ylo;
-        const double zc = S.dz * (double(k) + 0.5) + c.zlo;
+        const double xc = S.dx * (double(i) + 0.5) + S.x0[0], yc = S.dy * (double(j) + 0.5) + S.x0[1];
+        const double zc = S.dz * (double(k) + 0.5) + S.x0[2];
         double noise = 0.0;
         if (kind == KFVM_IC_KELVIN_HELMHOLTZ) {
-          const uint64_t g = (uint64_t)((k * S.ny + j) * S.nx + i);
+          // seeded by the cell's index in the whole domain
+          const uint64_t g = (uint64_t)(((k + S.off[2]) * S.gn[1] + (j + S.off[1])) * S.gn[0] + (i + S.off[0]));
           const double u01 = (double)(splitmix64(seed ^ g) >> 11) * (1.0 / 9007199254740992.0);
           noise = 1.0e-3 * (2.0 * u01 - 1.0);
         }
@@ -1884,9 +2016,16 @@ orc_solver *orc_create(const kfvm_config *cfg) {
   S->hy = S->ny + 2 * KFVM_RAD;
   S->hz = S->dim == 3 ? S->nz + 2 * KFVM_RAD : 1;
   S->rz = S->dim == 3 ? KFVM_RAD : 0;
-  S->dx = (cfg->xup - cfg->xlo) / S->nx;
-  S->dy = (cfg->yup - cfg->ylo) / S->ny;
-  S->dz = (cfg->zup - cfg->zlo) / S->nz;
+  S->dx = geo_dx(S->cfg, 0);
+  S->dy = geo_dx(S->cfg, 1);
+  S->dz = geo_dx(S->cfg, 2);
+  for (int d = 0; d < 3; d++) {
+    S->off[d] = geo_off(S->cfg, d);
+    S->gn[d] = geo_n(S->cfg, d) * geo_nb(S->cfg, d);
+    S->x0[d] = geo_lo(S->cfg, d);
+  }
+  for (int f = 0; f < 2 * S->dim; f++)
+    if (cfg->bc[f] == KFVM_BC_EXCHANGE) S->decomposed = true;
   S->dmin = S->dim == 2 ? fmin(S->dx, S->dy) : fmin(S->dx, fmin(S->dy, S->dz));
   orc::quad_rule(S->nq, S->ab, S->wt);
   S->haveSources = cfg->have_sources || cfg->eq == KFVM_EQ_MHD_GLM;
@@ -1978,6 +2117,15 @@ int orc_eval_rhs(orc_solver *s, double t, double *rhs, double *max_vel) {
 int orc_take_step(orc_solver *s, kfvm_step_info *info) {
   if (!s) return KFVM_ERR_ARG;
   take_step(*s, info);
+  return s->xerr ? KFVM_ERR_STATE : 0;
+}
+
+int orc_set_exchange(orc_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user) {
+  if (!s || !ex || !ar) return KFVM_ERR_ARG;
+  if (!s->decomposed) return KFVM_ERR_STATE;
+  s->xfn = ex;
+  s->rfn = ar;
+  s->xuser = user;
   return 0;
 }
 
@@ -2062,8 +2210,8 @@ int orc_apply_forcing(orc_solver *s, const double *modes, int32_t n_modes, doubl
   auto force = [&](int64_t i, int64_t j, int64_t k, double str, bool scaled, double &fu, double &fv,
                    double &fw) {
     fu = fv = fw = 0.0;
-    const double x = S.dx * (double(i) + 0.5) + S.cfg.xlo, y = S.dy * (double(j) + 0.5) + S.cfg.ylo;
-    const double z = dim == 2 ? S.dz * 0.5 + S.cfg.zlo : S.dz * (double(k) + 0.5) + S.cfg.zlo;
+    const double x = S.dx * (double(i) + 0.5) + S.x0[0], y = S.dy * (double(j) + 0.5) + S.x0[1];
+    const double z = dim == 2 ? S.dz * 0.5 + S.x0[2] : S.dz * (double(k) + 0.5) + S.x0[2];
     for (int n = 0; n < n_modes; n++) {
       auto A = [&](int d, int c) { return modes[((size_t)n * dim + d) * 3 + c]; };
       const double k1 = A(0, 0), k2 = A(1, 0), k3 = dim == 3 ? A(2, 0) : 0.0;
@@ -2091,8 +2239,10 @@ int orc_apply_forcing(orc_solver *s, const double *modes, int32_t n_modes, doubl
         intA += 0.5 * rho * (fu * fu + fv * fv + fw * fw);
         intB += S.U[S.ui(i, j, k, MOMX)] * fu + S.U[S.ui(i, j, k, MOMY)] * fv + S.U[S.ui(i, j, k, MOMZ)] * fw;
       }
+  double ints[2] = {intA, intB};
+  reduce_all(S, KFVM_REDUCE_SUM, ints, 2);  // forceStrComm
   const double dvol = dim == 2 ? S.dx * S.dy : S.dx * S.dy * S.dz;
-  const double A = intA, B = intB, C = -edot * S.dt / dvol;
+  const double A = ints[0], B = ints[1], C = -edot * S.dt / dvol;
   const double str = (-B + std::sqrt(std::fmax(0.0, B * B - 4.0 * A * C))) / (2.0 * A);
   for (int64_t k = 0; k < S.nz; k++)
     for (int64_t j = 0; j < S.ny; j++)

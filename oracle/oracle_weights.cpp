@@ -438,9 +438,10 @@ int build_stencil(const kfvm_config *cfg, kfvm_stencil *st) {
   const int monoDeg[3] = {3, 1, 1};
   auto derivSet = mono_enum(dim, nDeriv);
 
-  // geometry (Geometry.H:27-43)
-  const double dx = (cfg->xup - cfg->xlo) / cfg->nx, dy = (cfg->yup - cfg->ylo) / cfg->ny,
-               dz = (cfg->zup - cfg->zlo) / cfg->nz;
+  // geometry (Geometry.H:27-43): the whole domain's extents over its cells, nx nb
+  auto nbk = [&](int d) { return cfg->nb[d] > 0 ? cfg->nb[d] : 1; };
+  const double dx = (cfg->xup - cfg->xlo) / (cfg->nx * nbk(0)), dy = (cfg->yup - cfg->ylo) / (cfg->ny * nbk(1)),
+               dz = (cfg->zup - cfg->zlo) / (cfg->nz * nbk(2));
   const double eps = 1.0 / (cfg->lfac * std::sqrt(2.0));
 
   double ab[3], wt[3];
