@@ -425,20 +425,35 @@ def run_ours(args):
     peak_src = "measured" if peaks else "fallback"
     dom = max((k for k in per_class if per_class[k][1] > 0), key=lambda k: per_class[k][0])
     dom_ms, dom_n = per_class[dom]
-    avg_ms = dom_ms / max(dom_n, 1)
+    tf32_recon = args.precision == "tf32x3" and dom == "recon"
+    # the FP32 form's reconstruction is two launches per evaluation (the limiter
+    # bounds, then the tensor-core contraction): time per evaluation
+    avg_ms = dom_ms / max(dom_n // 2 if tf32_recon else dom_n, 1)
     algo = algorithmic_bytes(dom, cfg)
     achieved = algo / (avg_ms / 1e3) / 1e9
     # DRAM bytes per cell of each kernel class from one ncu capture (profiles/),
     # scaled by the cells one launch processes
     traffic_tbl = load_json(os.path.join(ROOT, "profiles", "dram_traffic.json")) or {}
     case = f"{cfg.dim}d_{('hydro', 'ns', 'glm', 'sr')[cfg.eq]}"
-    per_cell = traffic_tbl.get("cases", {}).get(case, {}).get("bytes_per_cell", {}).get(dom)
+    per_cell = traffic_tbl.get("cases", {}).get(case, {}).get("bytes_per_cell", {}).get(
+        "recon_tc" if args.precision == "tf32x3" and dom == "recon" else dom)
     traffic = per_cell * n if per_cell is not None else None
     hbm = {"achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
            "algorithmic_bytes": algo,
            "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback"}
     fma = algorithmic_fma(dom, cfg)
-    if fma is not None:
+    if fma is not None and tf32_recon:
+        # 3xTF32 on tcgen05: three MMAs per product (hi hi, hi lo, lo hi); TF32 runs at
+        # half the dense bf16 rate, so its peak is half the measured bf16 GEMM
+        tf32_peak = (peaks.get("bf16_tflops") if peaks else 1590.0) / 2
+        tf = 3 * 2 * fma / (avg_ms / 1e3) / 1e12
+        roofline = {"bound": "tensor", "kernel": "recon (bounds + recon_tc_tma)", "achieved": tf, "peak": tf32_peak,
+                    "unit": "TFLOP/s", "frac": tf / tf32_peak, "traffic": traffic, "tf32_mma_flop_per_launch": 6 * fma,
+                    "launch_ms": avg_ms,
+                    "peak_source": ("half of the measured dense bf16 GEMM (MEASURED_PEAKS.json bf16_tflops)" if peaks
+                                    else "half of the fallback bf16 1.59 PFLOP/s"),
+                    "hbm": hbm}
+    elif fma is not None:
         # the FP64 reconstruction runs on the FP64 tensor pipe (m8n8k4 DMMA): its bound
         # is that pipe's throughput, measured on this GPU by back-to-back MMAs
         fp64_peak = kfvm.measure_fp64_mma()
@@ -461,7 +476,8 @@ def run_ours(args):
     rows_ = 2 * d_ * nqf_ + (nqc_ if src_ else 0)
     b_zu = 4 * 7 * nv_ * 8 + 2 * nv_ * 8
     f_zu = 4 * (2 * rows_ * ncst_ * nv_ + d_ * nqf_ * 200 + 300)
-    fp64_peak_ = roofline["peak"] * 1e12 if roofline["unit"] == "TFLOP/s" else kfvm.measure_fp64_mma() * 1e12
+    fp64_peak_ = (roofline["peak"] * 1e12 if roofline["unit"] == "TFLOP/s" and not tf32_recon
+                  else kfvm.measure_fp64_mma() * 1e12)
     att_hbm, att_fp64 = hbm_peak * 1e9 / b_zu, fp64_peak_ / f_zu
     path_roofline = {"bytes_per_zone_update": b_zu, "flops_per_zone_update": f_zu,
                      "attainable_hbm": att_hbm, "attainable_fp64": att_fp64,
