@@ -54,7 +54,12 @@ enum kfvm_bc {
    * reference's LayoutMPI gives an MPI neighbour, src/LayoutMPI.H:44-97): its
    * halo cells and outer face states come from that rank through the exchange
    * callbacks of kfvm_set_exchange */
-  KFVM_BC_EXCHANGE = 4
+  KFVM_BC_EXCHANGE = 4,
+  /* a face whose halo cells and outer face states a user function supplies
+   * (BCType::user: the CellWest..CellTop and FaceWest..FaceTop functions of a
+   * problem's UserBCs.H, src/BoundaryConditions_K.H:96-128, 569-615), through
+   * the callback of kfvm_set_user_bc */
+  KFVM_BC_USER = 5
 };
 /* src/Types.H:40 */
 enum kfvm_ts_status { KFVM_TS_ACCEPTED = 0, KFVM_TS_TOLERANCE = 1, KFVM_TS_UNPHYSICAL = 2 };
@@ -438,6 +443,37 @@ typedef int (*kfvm_exchange_fn)(void *user, int32_t axis, const void *send_lo, v
 typedef int (*kfvm_allreduce_fn)(void *user, int32_t op, double *vals, int32_t n);
 int kfvm_block_config(const kfvm_config *blocks, int32_t rank, kfvm_config *out, int32_t neighbors[6]);
 int kfvm_set_exchange(kfvm_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user);
+
+/* ---- user-defined boundary conditions ----
+ * For every face with KFVM_BC_USER the solver calls
+ *   fn(user, kind, face, time, inner, outer, n_points, stream)
+ * with device buffers that stay valid during the call only, after synchronising
+ * its stream (the callback may launch work on `stream`, a cudaStream_t, or on
+ * any other stream it synchronises before returning; it returns 0 on success).
+ * face = 2 axis + side (west, east, south, north, bottom, top); time = the time
+ * of the RHS evaluation (the stage time t + c dt).
+ *   kind KFVM_USER_CELLS (setCellBCs, in its axis order: x faces, then y over the
+ *   x halo, then z over both): inner holds the r = 2 interior cell layers along
+ *   the face, outer receives the 2 halo layers, both as [v][layer][position]
+ *   doubles.  Along the face's axis (extent n) layer h of inner is cell h (low
+ *   side) or n - 2 + h (high side) and layer h of outer is cell h - 2 (low) or
+ *   n + h (high); position t = p1 + e1 p2 runs over the other two axes, the lower
+ *   one (p1) fastest, each over its padded range -2 .. n + 1 if that axis is
+ *   filled before this one and over its interior 0 .. n - 1 otherwise (in 2D the
+ *   z range is the single index 0).  Cell centres: x = x0 + dx (i + 1/2), x0 and
+ *   dx as this block's geometry (kfvm_config).
+ *   kind KFVM_USER_FACES (setFaceBCs): inner holds the face points' states from
+ *   inside the domain, outer receives the states outside, both as [q][v][point]
+ *   doubles; point runs over the face's cells in the other two axes (interior
+ *   ranges, lower axis fastest) and q over its NQF quadrature points (in 3D
+ *   q = q_a NQ + q_b, q_a along the lower of the two axes).  For the KXRCF
+ *   selector the solver derives the outer indicator from the outer states.
+ * n_points is the number of positions (cells) or face points times quadrature
+ * points; the buffers hold NV such blocks. */
+enum kfvm_user_kind { KFVM_USER_CELLS = 0, KFVM_USER_FACES = 1 };
+typedef int (*kfvm_user_bc_fn)(void *user, int32_t kind, int32_t face, double time, const double *inner,
+                               double *outer, int64_t n_points, void *stream);
+int kfvm_set_user_bc(kfvm_solver *s, kfvm_user_bc_fn fn, void *user);
 
 /* ---- random forcing (stirred turbulence) ----
  * The reference's ENABLE_RANDOM_FORCING path (src/ParameterStructs.H:20-74,

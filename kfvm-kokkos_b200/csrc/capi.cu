@@ -265,6 +265,12 @@ struct kfvm_solver {
   // domain decomposition: this block has exchange faces; the transport callbacks
   // (kfvm_set_exchange) and their device buffers send_lo, recv_lo, send_hi, recv_hi
   bool decomposed = false;
+  // user boundary conditions (kfvm_set_user_bc): some face is KFVM_BC_USER, the
+  // callback, and the time of the RHS evaluation in progress
+  bool hasUser = false;
+  kfvm_user_bc_fn ufn = nullptr;
+  void *uuser = nullptr;
+  double tEval = 0.0;
   kfvm_exchange_fn xfn = nullptr;
   kfvm_allreduce_fn rfn = nullptr;
   void *xuser = nullptr;
@@ -436,13 +442,26 @@ int fill_halo(kfvm_solver *s, int b) {
   using namespace kfvm;
   cudaStream_t st = s->stream;
   double *U = s->Ub[b];
-  if (!s->decomposed) {
+  if (!s->decomposed && !s->hasUser) {
     cudaError_t e = run(s, KFVM_KCLASS_BC, 1, [&] { return launch_bc(s->dim, s->eq, U, s->g, st); });
     return e == cudaSuccess ? KFVM_OK : set_err_cuda(e, "bc");
   }
-  if (!s->xfn) return fail(KFVM_ERR_STATE, "exchange faces but no transport (kfvm_set_exchange)");
+  if (s->decomposed && !s->xfn) return fail(KFVM_ERR_STATE, "exchange faces but no transport (kfvm_set_exchange)");
+  if (s->hasUser && !s->ufn) return fail(KFVM_ERR_STATE, "user boundary faces but no kfvm_set_user_bc");
   for (int d = 0; d < s->dim; d++) {
     const bool lo = s->g.bc[2 * d] == KFVM_BC_EXCHANGE, hi = s->g.bc[2 * d + 1] == KFVM_BC_EXCHANGE;
+    // user faces: the interior layers out, the halo layers back (CellBc*_K<user>)
+    for (int side = 0; side < 2; side++) {
+      if (s->g.bc[2 * d + side] != KFVM_BC_USER) continue;
+      const int64_t vals = cell_slab_values(s->g, s->dim, s->nv, d);
+      CK(launch_cell_slab(s->dim, s->nv, U, s->g, d, side, true, s->xbuf[0], st));
+      CK(cudaStreamSynchronize(st));
+      if (s->ufn(s->uuser, KFVM_USER_CELLS, 2 * d + side, s->tEval, s->xbuf[0], s->xbuf[1], vals / s->nv,
+                 (void *)st) != 0)
+        return fail(KFVM_ERR_STATE, "the user boundary callback failed");
+      CK(launch_cell_slab(s->dim, s->nv, U, s->g, d, side, false, s->xbuf[1], st));
+      s->launches += 2;
+    }
     if (lo || hi) {
       const int64_t bytes = cell_slab_values(s->g, s->dim, s->nv, d) * (int64_t)sizeof(double);
       if (lo) CK(launch_cell_slab(s->dim, s->nv, U, s->g, d, 0, true, s->xbuf[0], st));
@@ -465,10 +484,27 @@ int fill_halo(kfvm_solver *s, int b) {
 // the outer face states (and with W the KXRCF indicator) of every exchange face
 int exchange_faces(kfvm_solver *s, bool withW) {
   using namespace kfvm;
-  if (!s->decomposed) return KFVM_OK;
+  if (!s->decomposed && !s->hasUser) return KFVM_OK;
   cudaStream_t st = s->stream;
   const int nqf = s->dim == 2 ? s->g.nq : s->g.nq * s->g.nq;
   for (int d = 0; d < s->dim; d++) {
+    // user faces: the inner states out, the outer states back (FaceBc*_K<user>),
+    // then the outer indicator from them
+    for (int side = 0; side < 2; side++) {
+      if (s->g.bc[2 * d + side] != KFVM_BC_USER) continue;
+      const int64_t pts = face_plane_bytes(s->g, nqf, s->nv, d, false) / (int64_t)(s->nv * sizeof(double));
+      CK(launch_face_plane(s->F[d], nullptr, s->g, nqf, s->nv, d, side, true, s->xbuf[0], st));
+      CK(cudaStreamSynchronize(st));
+      if (s->ufn(s->uuser, KFVM_USER_FACES, 2 * d + side, s->tEval, s->xbuf[0], s->xbuf[1], pts, (void *)st) != 0)
+        return fail(KFVM_ERR_STATE, "the user boundary callback failed");
+      CK(launch_face_plane(s->F[d], nullptr, s->g, nqf, s->nv, d, side, false, s->xbuf[1], st));
+      s->launches += 2;
+      if (withW) {
+        CK(launch_face_indicator(s->dim, s->eq, s->F[d], s->W[d], s->g, nqf, d, side, st));
+        s->launches += 1;
+      }
+    }
+    if (!s->decomposed) continue;
     const bool lo = s->g.bc[2 * d] == KFVM_BC_EXCHANGE, hi = s->g.bc[2 * d + 1] == KFVM_BC_EXCHANGE;
     if (!lo && !hi) continue;
     float *W = withW ? s->W[d] : nullptr;
@@ -554,10 +590,10 @@ int eval_front(kfvm_solver *s, int b) {
                              mode == RECON_FULL ? nullptr : s->bnd, s->sc, jd, s->heavyBlocks, st);
        })) != cudaSuccess)
     return set_err_cuda(e, "heavy");
-  if (s->decomposed) {
+  if (s->decomposed || s->hasUser) {
     // the second setFaceBCs, and the GLM cleaning speed over all ranks (glmSpeedComm)
     if (int rc = exchange_faces(s, false)) return rc;
-    if (eq == EQ_GLM) {
+    if (eq == EQ_GLM && s->decomposed) {
       unsigned long long bits[2];
       CK(cudaMemcpyAsync(bits, &s->sc->glm_lam_bits, sizeof(bits), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
@@ -623,6 +659,7 @@ int prime(kfvm_solver *s) {
   CK(cudaMemsetAsync(s->wset, 0, n, s->stream));
   CK(cudaMemsetAsync(s->sc, 0, sizeof(kfvm::DevScalars), s->stream));
   CK(kfvm::launch_fill(s->theta, n, 1.0, s->stream));
+  s->tEval = s->time;
   int rc = eval_into_K(s, s->iPrev);
   if (rc) return rc;
   CK(cudaMemcpyAsync(s->hsc, s->sc, sizeof(kfvm::DevScalars), cudaMemcpyDeviceToHost, s->stream));
@@ -659,6 +696,7 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
   for (nT = 0; nT < s->cfg.rejection_limit; nT++) {
     CK(cudaMemsetAsync(&s->sc->maxvel_bits, 0, sizeof(unsigned long long), st));
     if (nT > 0) {
+      s->tEval = s->time;
       int rc = eval_into_K(s, s->iPrev);
       if (rc) return rc;
     }
@@ -669,6 +707,7 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
     if (e != cudaSuccess) return set_err_cuda(e, "stage_pre");
     int cur = bA, nxt = bB;
     for (int nS = 1; nS < rk.nStages; nS++) {
+      s->tEval = s->time + rk.c[nS] * s->dt;
       int rc = eval_front(s, cur);
       if (rc) return rc;
       StageArgs a = stage_args(s, cur, nxt, STAGE_UPDATE);
@@ -684,6 +723,7 @@ int take_step(kfvm_solver *s, kfvm_step_info *info) {
       std::swap(cur, nxt);
     }
     // FSAL stage: K = RHS(U), Uhat += bhatfsal dt K, error estimate
+    s->tEval = s->time + s->dt;
     int rc = eval_front(s, cur);
     if (rc) return rc;
     StageArgs a = stage_args(s, cur, -1, STAGE_FSAL);
@@ -862,8 +902,8 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
     if ((cfg->bc[2 * d] == KFVM_BC_PERIODIC) != (cfg->bc[2 * d + 1] == KFVM_BC_PERIODIC))
       return fail(KFVM_ERR_ARG, "periodic boundaries must come in pairs");
     for (int f = 2 * d; f < 2 * d + 2; f++)
-      if (cfg->bc[f] < KFVM_BC_PERIODIC || cfg->bc[f] > KFVM_BC_EXCHANGE)
-        return fail(KFVM_ERR_ARG, "unknown boundary condition (periodic, outflow, reflecting, noslip, exchange)");
+      if (cfg->bc[f] < KFVM_BC_PERIODIC || cfg->bc[f] > KFVM_BC_USER)
+        return fail(KFVM_ERR_ARG, "unknown boundary condition (periodic, outflow, reflecting, noslip, exchange, user)");
   }
   for (int d = 0; d < 3; d++)
     if (cfg->nb[d] > 1 && (cfg->block[d] < 0 || cfg->block[d] >= cfg->nb[d]))
@@ -910,6 +950,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
     g.bc[f] = cfg->bc[f];
     g.bflip[f] = wall_flip(cfg->bc[f], f / 2, cfg->eq == KFVM_EQ_MHD_GLM);
     if (f < 2 * cfg->dim && cfg->bc[f] == KFVM_BC_EXCHANGE) s->decomposed = true;
+    if (f < 2 * cfg->dim && cfg->bc[f] == KFVM_BC_USER) s->hasUser = true;
   }
   g.gamma = cfg->gamma;
   g.rs = cfg->rs;
@@ -1094,8 +1135,8 @@ int kfvm_get_state(kfvm_solver *s, double *u) {
 }
 
 int kfvm_eval_rhs(kfvm_solver *s, double t, double *rhs, double *max_vel) {
-  (void)t;
   if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  s->tEval = t;
   CK(cudaMemsetAsync(&s->sc->maxvel_bits, 0, sizeof(unsigned long long), s->stream));
   int rc = eval_into_K(s, s->iCur);
   if (rc) return rc;
@@ -1343,6 +1384,7 @@ int kfvm_mlp_collect(kfvm_solver *s, double tau, double keep_frac, uint64_t seed
   auto &M = s->mlp;
   if (!M.cap) return fail(KFVM_ERR_STATE, "kfvm_mlp_reserve first");
   const int b = s->iCur;
+  s->tEval = s->time;
   if (int rc = fill_halo(s, b)) return rc;
   cudaError_t e;
   // labels, pairs, then the kept cells in cell order (a stable select)
@@ -1455,6 +1497,7 @@ int kfvm_mlp_probability(kfvm_solver *s, float *out_host) {
   cudaError_t e;
   if ((e = cudaMalloc((void **)&d, s->g.n * sizeof(float))) != cudaSuccess) return set_err_cuda(e, "alloc");
   const int b = s->iCur;
+  s->tEval = s->time;
   if (int rc = fill_halo(s, b)) {
     cudaFree(d);
     return rc;
@@ -1526,8 +1569,8 @@ int kfvm_get_faces(kfvm_solver *s, int32_t dir, double *out) {
   const int64_t nd = dir == 0 ? g.nx : (dir == 1 ? g.ny : g.nz);
   const int64_t stride = dir == 0 ? 1 : (dir == 1 ? fx : fx * fy);
   const bool per = g.bc[2 * dir] == KFVM_BC_PERIODIC;
-  // an exchange face's outer slot already holds the neighbour's states
-  const bool xlo = g.bc[2 * dir] == KFVM_BC_EXCHANGE, xhi = g.bc[2 * dir + 1] == KFVM_BC_EXCHANGE;
+  // an exchange or user face's outer slot already holds its outer states
+  const bool xlo = kfvm::outer_in_face(g.bc[2 * dir]), xhi = kfvm::outer_in_face(g.bc[2 * dir + 1]);
   const unsigned flo = g.bflip[2 * dir], fhi = g.bflip[2 * dir + 1];
   for (int64_t k = 0; k < fz; k++)
     for (int64_t j = 0; j < fy; j++)
@@ -1595,12 +1638,9 @@ int kfvm_block_config(const kfvm_config *blocks, int32_t rank, kfvm_config *out,
   return KFVM_OK;
 }
 
-int kfvm_set_exchange(kfvm_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user) {
-  if (!s) return fail(KFVM_ERR_ARG, "null solver");
-  if (!s->decomposed) return fail(KFVM_ERR_STATE, "no exchange faces in this solver's configuration");
-  if (!ex || !ar) return fail(KFVM_ERR_ARG, "both callbacks are required");
-  // one buffer size for every use: the largest cell slab or face plane (with the
-  // indicator) over the axes
+// the four buffers of the exchange and user-boundary callbacks, one size for every
+// use: the largest cell slab or face plane (with the indicator) over the axes
+int alloc_xbuf(kfvm_solver *s) {
   const int nqf = s->dim == 2 ? s->g.nq : s->g.nq * s->g.nq;
   int64_t bytes = 0;
   for (int d = 0; d < s->dim; d++) {
@@ -1619,9 +1659,27 @@ int kfvm_set_exchange(kfvm_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar,
       }
     }
   }
+  return KFVM_OK;
+}
+
+int kfvm_set_exchange(kfvm_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (!s->decomposed) return fail(KFVM_ERR_STATE, "no exchange faces in this solver's configuration");
+  if (!ex || !ar) return fail(KFVM_ERR_ARG, "both callbacks are required");
+  if (int rc = alloc_xbuf(s)) return rc;
   s->xfn = ex;
   s->rfn = ar;
   s->xuser = user;
+  return KFVM_OK;
+}
+
+int kfvm_set_user_bc(kfvm_solver *s, kfvm_user_bc_fn fn, void *user) {
+  if (!s) return fail(KFVM_ERR_ARG, "null solver");
+  if (!s->hasUser) return fail(KFVM_ERR_STATE, "no user boundary faces in this solver's configuration");
+  if (!fn) return fail(KFVM_ERR_ARG, "null callback");
+  if (int rc = alloc_xbuf(s)) return rc;
+  s->ufn = fn;
+  s->uuser = user;
   return KFVM_OK;
 }
 
@@ -1670,8 +1728,9 @@ int kfvm_restart(kfvm_solver *s, const char *xmf_path, int32_t *time_step) {
   CK(cudaMemcpyAsync(s->theta, th.data(), n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->wset, w.data(), n, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->applied, w.data(), n, cudaMemcpyHostToDevice, s->stream));
-  // the priming evaluation again, now with the restored flags
+  // the priming evaluation again, now with the restored flags, at the file's time
   CK(cudaMemsetAsync(&s->sc->maxvel_bits, 0, sizeof(unsigned long long), s->stream));
+  s->tEval = t;
   if ((rc = eval_into_K(s, s->iPrev))) return rc;
   CK(cudaStreamSynchronize(s->stream));
   s->time = t;
@@ -1692,6 +1751,7 @@ int kfvm_flow_stats(kfvm_solver *s, double *stats, int32_t *n_stats) {
   double *U = s->Ub[s->iCur];
   // the halo as the boundary conditions set it (the reference relies on the last
   // evaluation having set it; filling again gives the same values)
+  s->tEval = s->time;
   if (int rc = fill_halo(s, s->iCur)) return rc;
   CK(launch_stats(s->dim, s->eq, U, s->g, dvol / volume, s->spart, s->ssum, s->stream));
   s->launches += s->eq == KFVM_EQ_SRHYDRO ? 1 : 3;

@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(256) bc_axis_kernel(double *__restrict__ U, Gr
     const int64_t layer = t / per, q = t % per;
     const int side = layer < kRad ? 0 : 1;
     const int f = 2 * d + side;
-    if (g.bc[f] == KFVM_BC_EXCHANGE) continue;  // comes from the neighbour
+    if (g.bc[f] == KFVM_BC_EXCHANGE || g.bc[f] == KFVM_BC_USER) continue;  // from the neighbour / the user
     int64_t i, j, k;
     slab_cell(g, DIM, d, s, side, true, side == 0 ? layer : layer - kRad, q, i, j, k);
     int64_t c[3] = {i, j, k};
@@ -138,6 +138,34 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// the FP32 KXRCF indicator of the outer slot of one boundary face plane, from the
+// outer states a user boundary condition wrote there (the value the reconstruction
+// stores for an inner state: Eos::weno_store, or D rounded for SR)
+template <int DIM, int EQ>
+__global__ void __launch_bounds__(256)
+    face_indicator_kernel(const double *__restrict__ F, float *__restrict__ W, Grid g, int nqf, int d, int side) {
+  constexpr int NV = Eos<EQ>::NV;
+  const int64_t fx = g.fdim[d][0], fy = g.fdim[d][1], fz = g.fdim[d][2];
+  const int64_t e1 = d == 0 ? fy : fx, e2 = d == 2 ? fy : fz;
+  const int64_t per = e1 * e2, nf = g.nface[d];
+  const int64_t m = side == 0 ? 0 : (d == 0 ? g.nx : (d == 1 ? g.ny : g.nz));
+  const int slot = side == 0 ? 0 : 1;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < per * nqf;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(t / per);
+    const int64_t p = t % per, a = p % e1, b = p / e1;
+    const int64_t fi = d == 0 ? m : a, fj = d == 0 ? a : (d == 1 ? m : b), fk = d == 2 ? m : b;
+    const int64_t fidx = (fk * fy + fj) * fx + fi;
+    double st[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) st[v] = F[((int64_t)(slot * nqf + q) * NV + v) * nf + fidx];
+    float w;
+    if constexpr (EQ == EQ_SR) w = __double2float_rn(st[DENS]);
+    else w = Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * Eos<EQ>::eint(st));
+    W[(int64_t)(slot * nqf + q) * nf + fidx] = w;
+  }
+}
+
 static unsigned blocks_for(int64_t n) { return (unsigned)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096); }
 
 int64_t cell_slab_values(const Grid &g, int dim, int nv, int d) {
@@ -181,6 +209,26 @@ cudaError_t launch_face_plane(double *F, float *W, const Grid &g, int nqf, int n
   const unsigned nb = blocks_for(e1 * e2);
   if (pack) face_plane_kernel<true><<<nb, 256, 0, s>>>(F, W, g, nqf, nv, d, side, buf);
   else face_plane_kernel<false><<<nb, 256, 0, s>>>(F, W, g, nqf, nv, d, side, buf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_face_indicator(int dim, int eq, const double *F, float *W, const Grid &g, int nqf, int d,
+                                  int side, cudaStream_t s) {
+  const int64_t e1 = d == 0 ? g.fdim[d][1] : g.fdim[d][0], e2 = d == 2 ? g.fdim[d][1] : g.fdim[d][2];
+  const unsigned nb = blocks_for(e1 * e2 * nqf);
+#define KFVM_FI(D, E) face_indicator_kernel<D, E><<<nb, 256, 0, s>>>(F, W, g, nqf, d, side)
+  if (dim == 2) {
+    if (eq == EQ_GLM) KFVM_FI(2, EQ_GLM);
+    else if (eq == EQ_SR) KFVM_FI(2, EQ_SR);
+    else if (eq == EQ_NS) KFVM_FI(2, EQ_NS);
+    else KFVM_FI(2, EQ_HYDRO);
+  } else {
+    if (eq == EQ_GLM) KFVM_FI(3, EQ_GLM);
+    else if (eq == EQ_SR) KFVM_FI(3, EQ_SR);
+    else if (eq == EQ_NS) KFVM_FI(3, EQ_NS);
+    else KFVM_FI(3, EQ_HYDRO);
+  }
+#undef KFVM_FI
   return cudaGetLastError();
 }
 

@@ -359,7 +359,7 @@ __device__ __forceinline__ void kxrcf_face(const Grid &g, int fc, int64_t i, int
   const int64_t stride = d == 0 ? 1 : (d == 1 ? fx : fx * fy);
   if (m == 0 || m == nd) {
     if (g.bc[fc] == KFVM_BC_PERIODIC) oidx = m == 0 ? fidx + nd * stride : fidx - nd * stride;
-    else if (g.bc[fc] != KFVM_BC_EXCHANGE) oth = own;  // an exchange face holds the neighbour's slot
+    else if (!outer_in_face(g.bc[fc])) oth = own;  // an exchange / user face holds its outer slot
   }
 }
 
@@ -899,13 +899,13 @@ __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
     int64_t f0 = fidx, f1 = fidx;
     int s0 = 0, s1 = 1;
     const int64_t stride = D == 0 ? 1 : (D == 1 ? fx : fx * fy);
-    // (an exchange face holds the neighbour's state in its own outer slot)
+    // (an exchange or user face holds the outer state in its own outer slot)
     if (m == 0) {
       if (g.bc[2 * D] == KFVM_BC_PERIODIC) f0 = fidx + nd * stride;
-      else if (g.bc[2 * D] != KFVM_BC_EXCHANGE) s0 = 1;
+      else if (!outer_in_face(g.bc[2 * D])) s0 = 1;
     } else if (m == nd) {
       if (g.bc[2 * D + 1] == KFVM_BC_PERIODIC) f1 = fidx - nd * stride;
-      else if (g.bc[2 * D + 1] != KFVM_BC_EXCHANGE) s1 = 0;
+      else if (!outer_in_face(g.bc[2 * D + 1])) s1 = 0;
     }
     const double ch = EQ == EQ_GLM ? __longlong_as_double((long long)sc->glm_lam_bits) -
                                          __longlong_as_double((long long)sc->glm_vel_bits)
@@ -1008,13 +1008,13 @@ __device__ void glm_sources(const double *__restrict__ Uc, const Grid &g, int64_
     unsigned flip = 0u;
     if (m == 0 && s == 0) {
       if (g.bc[2 * d] == KFVM_BC_PERIODIC) fidx += nd * stride;
-      else if (g.bc[2 * d] != KFVM_BC_EXCHANGE) {
+      else if (!outer_in_face(g.bc[2 * d])) {
         s = 1;
         flip = g.bflip[2 * d];
       }
     } else if (m == nd && s == 1) {
       if (g.bc[2 * d + 1] == KFVM_BC_PERIODIC) fidx -= nd * stride;
-      else if (g.bc[2 * d + 1] != KFVM_BC_EXCHANGE) {
+      else if (!outer_in_face(g.bc[2 * d + 1])) {
         s = 0;
         flip = g.bflip[2 * d + 1];
       }

@@ -55,6 +55,11 @@ struct Grid {
   int64_t off[3], gn[3];        // this block's first cell and the domain's cells per axis
 };
 
+// a boundary face whose outer face state is held in the face array itself (received
+// from the neighbouring block, or written by a user boundary condition) instead of
+// being derived from the inner state on read
+__host__ __device__ inline bool outer_in_face(int bc) { return bc == KFVM_BC_EXCHANGE || bc == KFVM_BC_USER; }
+
 // stencil on the device: weights plus linear offsets in the padded array, and the
 // full-stencil linear weights packed as [cell][row] (rows: face points f*NQF+q, then
 // interior points q) for the light reconstruction pass

@@ -41,6 +41,9 @@ cudaError_t launch_cell_slab(int dim, int nv, double *U, const Grid &g, int d, i
                              cudaStream_t s);
 cudaError_t launch_face_plane(double *F, float *W, const Grid &g, int nqf, int nv, int d, int side, bool pack,
                               double *buf, cudaStream_t s);
+// the FP32 KXRCF indicator of one face plane's outer slot from its states (user faces)
+cudaError_t launch_face_indicator(int dim, int eq, const double *F, float *W, const Grid &g, int nqf, int d,
+                                  int side, cudaStream_t s);
 // interior state between the host order (variable, k, j, i) in a flat device
 // buffer and the padded layout; one launch for all variables
 cudaError_t launch_interior(double *Up, double *flat, const Grid &g, int nv, bool toPadded, cudaStream_t s);

@@ -88,6 +88,7 @@ def lib():
         L.kfvm_block_config.argtypes = [C.POINTER(abi.KfvmConfig), I32, C.POINTER(abi.KfvmConfig),
                                         C.POINTER(I32)]
         L.kfvm_set_exchange.argtypes = [P, abi.EXCHANGE_FN, abi.ALLREDUCE_FN, P]
+        L.kfvm_set_user_bc.argtypes = [P, abi.USER_BC_FN, P]
         L.kfvm_last_error.restype = C.c_char_p
         _LIB = L
     return _LIB
@@ -173,6 +174,14 @@ def stencil(cfg):
     return st
 
 
+class _CudaBytes:
+    """A device byte range in the CUDA array interface, for torch.as_tensor."""
+
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = {"shape": (int(nbytes),), "typestr": "|u1",
+                                         "data": (int(ptr), False), "version": 3}
+
+
 def block_config(blocks, rank):
     """Rank `rank`'s configuration of a decomposed domain and the ranks across its six
     faces (-1: none): the reference's LayoutMPI::distributeBlocks.  `blocks` holds
@@ -249,6 +258,30 @@ class Solver:
 
     def set_time(self, t, dt):
         _check(lib().kfvm_set_time(self.h, float(t), float(dt)), "kfvm_set_time")
+
+    def set_user_bc(self, fn):
+        """Install user boundary conditions (the faces configured KFVM_BC_USER):
+        fn(kind, face, time, inner, outer) gets the packed inner values and fills
+        outer in place, both float64 CUDA tensors of shape (NV, points) with the
+        layouts of kfvm_set_user_bc.  fn may raise to fail the step."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+
+        def cb(user, kind, face, time, inner, outer, npts, stream):
+            try:
+                nb = int(npts) * self.nv * 8
+                a = torch.as_tensor(_CudaBytes(inner, nb), device=dev).view(torch.float64).view(self.nv, -1)
+                b = torch.as_tensor(_CudaBytes(outer, nb), device=dev).view(torch.float64).view(self.nv, -1)
+                fn(int(kind), int(face), float(time), a, b)
+                torch.cuda.current_stream(dev).synchronize()   # the solver's stream reads outer next
+                return 0
+            except Exception as e:  # noqa: BLE001 - reported through the return code
+                self.user_bc_error = e
+                return 1
+
+        self._user_bc = abi.USER_BC_FN(cb)
+        self.user_bc_error = None
+        _check(lib().kfvm_set_user_bc(self.h, self._user_bc, None), "kfvm_set_user_bc")
 
     def set_exchange(self, transport):
         """Install a transport (decomp.DistExchange or a LocalExchange endpoint) whose

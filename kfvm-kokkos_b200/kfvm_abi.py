@@ -11,7 +11,8 @@ import struct
 KFVM_EQ_HYDRO, KFVM_EQ_NAVIERSTOKES, KFVM_EQ_MHD_GLM, KFVM_EQ_SRHYDRO = 0, 1, 2, 3
 KFVM_RS_LLF, KFVM_RS_HLL, KFVM_RS_HLLC = 0, 1, 2
 KFVM_RK_THREESTARP, KFVM_RK_FOURSTARP, KFVM_RK_SSP4_3_2, KFVM_RK_SSP10_4_3 = 0, 1, 2, 3
-KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW, KFVM_BC_REFLECTING, KFVM_BC_NOSLIP, KFVM_BC_EXCHANGE = 0, 1, 2, 3, 4
+KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW, KFVM_BC_REFLECTING, KFVM_BC_NOSLIP, KFVM_BC_EXCHANGE, KFVM_BC_USER = 0, 1, 2, 3, 4, 5
+KFVM_USER_CELLS, KFVM_USER_FACES = 0, 1
 KFVM_REDUCE_SUM, KFVM_REDUCE_MAX, KFVM_REDUCE_MIN = 0, 1, 2
 KFVM_TS_ACCEPTED, KFVM_TS_TOLERANCE, KFVM_TS_UNPHYSICAL = 0, 1, 2
 KFVM_IND_KXRCF, KFVM_IND_ALL, KFVM_IND_NONE, KFVM_IND_MLP = 0, 1, 2, 3
@@ -30,6 +31,9 @@ KFVM_MAX_INDIC, KFVM_MAX_FACEQ, KFVM_MAX_CELLQ = 19, 9, 27
 EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                           C.c_int64, C.c_int64)
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.c_int32)
+# the user boundary callback of kfvm_set_user_bc (kfvm_user_bc_fn)
+USER_BC_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
+                         C.c_int64, C.c_void_p)
 
 
 class KfvmConfig(C.Structure):

@@ -47,6 +47,9 @@ int orc_set_indicator(orc_solver *s, int32_t ind);
  * neighbouring ranks through ex, and the maxima, sums and minima of a step go
  * through ar, with the meaning of kfvm_set_exchange's callbacks on host buffers. */
 int orc_set_exchange(orc_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user);
+/* User boundary conditions: KFVM_BC_USER faces call fn with host buffers, with
+ * the meaning and layouts of kfvm_set_user_bc (stream NULL). */
+int orc_set_user_bc(orc_solver *s, kfvm_user_bc_fn fn, void *user);
 /* Quadrature and RK coefficient tables used by the oracle. */
 int orc_tables(int32_t nq, int32_t rk, double *quad, double *rkt);
 /* Initial-condition cell averages alone (no FSAL priming), SoA interior. */

@@ -58,6 +58,7 @@ def lib():
         L.orc_ic_cells.argtypes = [C.POINTER(abi.KfvmConfig), I32, C.c_uint64, P]
         L.orc_tables.argtypes = [I32, I32, P, P]
         L.orc_set_exchange.argtypes = [P, abi.EXCHANGE_FN, abi.ALLREDUCE_FN, P]
+        L.orc_set_user_bc.argtypes = [P, abi.USER_BC_FN, P]
         _LIB = L
     return _LIB
 
@@ -165,6 +166,26 @@ class OracleSolver:
 
     def set_time(self, t, dt):
         assert lib().orc_set_time(self.h, float(t), float(dt)) == 0
+
+    def set_user_bc(self, fn):
+        """User boundary conditions on host buffers: fn(kind, face, time, inner, outer)
+        with float64 numpy arrays of shape (NV, points), as kfvm.Solver.set_user_bc."""
+        nv = self.nv
+
+        def cb(user, kind, face, time, inner, outer, npts, stream):
+            try:
+                n = int(npts) * nv
+                a = np.ctypeslib.as_array((C.c_double * n).from_address(inner)).reshape(nv, -1)
+                b = np.ctypeslib.as_array((C.c_double * n).from_address(outer)).reshape(nv, -1)
+                fn(int(kind), int(face), float(time), a, b)
+                return 0
+            except Exception as e:  # noqa: BLE001
+                self.user_bc_error = e
+                return 1
+
+        self._user_bc = abi.USER_BC_FN(cb)
+        self.user_bc_error = None
+        assert lib().orc_set_user_bc(self.h, self._user_bc, None) == 0
 
     def set_exchange(self, transport):
         """Install a host-buffer transport for the exchange faces of a decomposed domain."""

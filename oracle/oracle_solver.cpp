@@ -804,6 +804,9 @@ struct orc_solver {
   void *xuser = nullptr;
   int xerr = 0;
   std::vector<double> xb[4];
+  // user boundary conditions (orc_set_user_bc)
+  kfvm_user_bc_fn ufn = nullptr;
+  void *uuser = nullptr;
 
   // ---- indexing ----
   int64_t ui(int64_t i, int64_t j, int64_t k, int v) const {
@@ -897,14 +900,37 @@ void exchange_cells(orc_solver &S, std::vector<double> &B, int d) {
   if (hi) for_slab(S, d, 1, true, [&](size_t m, int64_t u) { B[u] = S.xb[3][m]; });
 }
 
-void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
+// the user faces of axis d (CellBc*_K<user>, BoundaryConditions_K.H:96-128): the r
+// interior layers out, the r halo layers back, both in the slab order above
+void user_cells(orc_solver &S, std::vector<double> &B, int d, double t) {
+  for (int side = 0; side < 2; side++) {
+    if (S.cfg.bc[2 * d + side] != KFVM_BC_USER) continue;
+    size_t count = 0;
+    for_slab(S, d, side, false, [&](size_t, int64_t) { count++; });
+    for (auto &b : S.xb)
+      if (b.size() < count) b.resize(count);
+    for_slab(S, d, side, false, [&](size_t m, int64_t u) { S.xb[0][m] = B[u]; });
+    if (!S.ufn || S.ufn(S.uuser, KFVM_USER_CELLS, 2 * d + side, t, S.xb[0].data(), S.xb[1].data(),
+                        (int64_t)(count / S.nv), nullptr) != 0) {
+      S.xerr = 1;
+      continue;
+    }
+    for_slab(S, d, side, true, [&](size_t m, int64_t u) { B[u] = S.xb[1][m]; });
+  }
+}
+
+// the faces whose halo comes from elsewhere (a neighbour or the user)
+inline bool filled_elsewhere(int bc) { return bc == KFVM_BC_EXCHANGE || bc == KFVM_BC_USER; }
+
+void set_cell_bcs(orc_solver &S, std::vector<double> &B, double t) {
   const int r = KFVM_RAD;
   auto &c = S.cfg;
-  const bool xl = c.bc[0] != KFVM_BC_EXCHANGE, xh = c.bc[1] != KFVM_BC_EXCHANGE;
-  const bool yl = c.bc[2] != KFVM_BC_EXCHANGE, yh = c.bc[3] != KFVM_BC_EXCHANGE;
-  const bool zl = c.bc[4] != KFVM_BC_EXCHANGE, zh = c.bc[5] != KFVM_BC_EXCHANGE;
+  const bool xl = !filled_elsewhere(c.bc[0]), xh = !filled_elsewhere(c.bc[1]);
+  const bool yl = !filled_elsewhere(c.bc[2]), yh = !filled_elsewhere(c.bc[3]);
+  const bool zl = !filled_elsewhere(c.bc[4]), zh = !filled_elsewhere(c.bc[5]);
   // x: j,k interior
   exchange_cells(S, B, 0);
+  user_cells(S, B, 0, t);
   for (int64_t k = 0; k < S.nz; k++)
     for (int64_t j = 0; j < S.ny; j++)
       for (int h = 0; h < r; h++)
@@ -919,6 +945,7 @@ void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
         }
   // y: i over the full halo range, k interior
   exchange_cells(S, B, 1);
+  user_cells(S, B, 1, t);
   for (int64_t k = 0; k < S.nz; k++)
     for (int64_t i = -r; i < S.nx + r; i++)
       for (int h = 0; h < r; h++)
@@ -933,6 +960,7 @@ void set_cell_bcs(orc_solver &S, std::vector<double> &B) {
         }
   if (S.dim == 3) {
     exchange_cells(S, B, 2);
+    user_cells(S, B, 2, t);
     for (int64_t j = -r; j < S.ny + r; j++)
       for (int64_t i = -r; i < S.nx + r; i++)
         for (int h = 0; h < r; h++)
@@ -980,13 +1008,51 @@ void exchange_faces(orc_solver &S, int d) {
   }
 }
 
+// the user faces of axis d (FaceBc*_K<user>, BoundaryConditions_K.H:569-615): the
+// inner states out, the outer states back, as [q][v][point] with the points over
+// the other two axes (the lower one fastest)
+void user_faces(orc_solver &S, int d, double t) {
+  const int64_t n[3] = {S.nx, S.ny, S.nz};
+  const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+  const int64_t e1 = n[a1], e2 = n[a2], per = e1 * e2;
+  const int nqf = S.nqf, nv = S.nv;
+  for (int side = 0; side < 2; side++) {
+    if (S.cfg.bc[2 * d + side] != KFVM_BC_USER) continue;
+    const size_t count = (size_t)(per * nqf * nv);
+    for (auto &b : S.xb)
+      if (b.size() < count) b.resize(count);
+    auto at = [&](int64_t p, int slot, int q) {
+      int64_t c[3];
+      c[d] = side == 0 ? 0 : n[d];
+      c[a1] = p % e1;
+      c[a2] = p / e1;
+      return S.fs(d, c[0], c[1], c[2], slot, q);
+    };
+    const int inner = side == 0 ? 1 : 0, outer = 1 - inner;
+    for (int q = 0; q < nqf; q++)
+      for (int v = 0; v < nv; v++)
+        for (int64_t p = 0; p < per; p++) S.xb[0][((size_t)q * nv + v) * per + p] = at(p, inner, q)[v];
+    if (!S.ufn || S.ufn(S.uuser, KFVM_USER_FACES, 2 * d + side, t, S.xb[0].data(), S.xb[1].data(),
+                        per * nqf, nullptr) != 0) {
+      S.xerr = 1;
+      continue;
+    }
+    for (int q = 0; q < nqf; q++)
+      for (int v = 0; v < nv; v++)
+        for (int64_t p = 0; p < per; p++) at(p, outer, q)[v] = S.xb[1][((size_t)q * nv + v) * per + p];
+  }
+}
+
 // setFaceBCs (Solver.cpp:785-824 and the commFaceBCs* self-copies)
-void set_face_bcs(orc_solver &S) {
+void set_face_bcs(orc_solver &S, double t) {
   auto &c = S.cfg;
-  for (int d = 0; d < S.dim; d++) exchange_faces(S, d);
-  const bool xl = c.bc[0] != KFVM_BC_EXCHANGE, xh = c.bc[1] != KFVM_BC_EXCHANGE;
-  const bool yl = c.bc[2] != KFVM_BC_EXCHANGE, yh = c.bc[3] != KFVM_BC_EXCHANGE;
-  const bool zl = c.bc[4] != KFVM_BC_EXCHANGE, zh = c.bc[5] != KFVM_BC_EXCHANGE;
+  for (int d = 0; d < S.dim; d++) {
+    exchange_faces(S, d);
+    user_faces(S, d, t);
+  }
+  const bool xl = !filled_elsewhere(c.bc[0]), xh = !filled_elsewhere(c.bc[1]);
+  const bool yl = !filled_elsewhere(c.bc[2]), yh = !filled_elsewhere(c.bc[3]);
+  const bool zl = !filled_elsewhere(c.bc[4]), zh = !filled_elsewhere(c.bc[5]);
   const int nqf = S.nqf, nv = S.nv;
   auto cp = [&](double *dst, const double *src) {
     for (int q = 0; q < nqf * nv; q++) dst[q] = src[q];
@@ -1732,9 +1798,8 @@ void viscosity(orc_solver &S, const std::vector<double> &B, int64_t i, int64_t j
 
 // Solver::evalRHS (Solver.cpp:410-530)
 double eval_rhs(orc_solver &S, std::vector<double> &B, double t) {
-  (void)t;
   S.nRhs++;
-  set_cell_bcs(S, B);
+  set_cell_bcs(S, B, t);
   std::fill(S.applied.begin(), S.applied.end(), 0);
   if (S.indicator == KFVM_IND_NONE) {
     FOR_CELLS linear_recon(S, B, i, j, k);
@@ -1742,7 +1807,7 @@ double eval_rhs(orc_solver &S, std::vector<double> &B, double t) {
   } else if (S.useSparseWeno) {
     const double wThresh = S.cfg.weno_thresh * std::pow(S.dmin, 1.5);
     FOR_CELLS linear_recon(S, B, i, j, k);
-    set_face_bcs(S);
+    set_face_bcs(S, t);
     int64_t nWeno = 0;
 #pragma omp parallel for collapse(2) reduction(+ : nWeno) schedule(static)
     for (int64_t k = 0; k < S.nz; k++)
@@ -1777,7 +1842,7 @@ double eval_rhs(orc_solver &S, std::vector<double> &B, double t) {
     S.useSparseWeno = S.cfg.weno_thresh > 0.0 && S.indicator == KFVM_IND_KXRCF;
   }
   FOR_CELLS positivity(S, B, i, j, k);
-  set_face_bcs(S);
+  set_face_bcs(S, t);
   if (S.keepFaces)
     for (int d = 0; d < S.dim; d++) S.faceSnap[d] = S.face[d];
   if (S.cfg.eq == KFVM_EQ_MHD_GLM) {
@@ -2120,6 +2185,13 @@ int orc_take_step(orc_solver *s, kfvm_step_info *info) {
   return s->xerr ? KFVM_ERR_STATE : 0;
 }
 
+int orc_set_user_bc(orc_solver *s, kfvm_user_bc_fn fn, void *user) {
+  if (!s || !fn) return KFVM_ERR_ARG;
+  s->ufn = fn;
+  s->uuser = user;
+  return 0;
+}
+
 int orc_set_exchange(orc_solver *s, kfvm_exchange_fn ex, kfvm_allreduce_fn ar, void *user) {
   if (!s || !ex || !ar) return KFVM_ERR_ARG;
   if (!s->decomposed) return KFVM_ERR_STATE;
@@ -2154,7 +2226,7 @@ int orc_flow_stats(orc_solver *s, double *stats, int32_t *n_stats) {
   if (n_stats) *n_stats = n;
   for (int q = 0; q < n; q++) stats[q] = 0.0;
   if (eq == KFVM_EQ_SRHYDRO) return 0;
-  set_cell_bcs(S, S.U);
+  set_cell_bcs(S, S.U, S.time);
   const std::vector<double> &B = S.U;
   auto U = [&](int64_t i, int64_t j, int64_t k, int v) { return B[S.ui(i, j, k, v)]; };
   auto vel = [&](int64_t i, int64_t j, int64_t k, int v) { return U(i, j, k, v) / U(i, j, k, DENS); };
@@ -2329,7 +2401,7 @@ int orc_get_flags(orc_solver *s, uint8_t *weno_applied, double *theta) {
 int orc_weno_departure(orc_solver *s, double *out) {
   if (!s || !out) return KFVM_ERR_ARG;
   std::vector<double> B = s->U;
-  set_cell_bcs(*s, B);
+  set_cell_bcs(*s, B, s->time);
   orc_solver &S = *s;
 #pragma omp parallel for collapse(2) schedule(static)
   for (int64_t k = 0; k < S.nz; k++)
