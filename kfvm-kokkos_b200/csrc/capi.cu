@@ -279,6 +279,9 @@ struct kfvm_solver {
   // tiles (built when the FP32 form is selected; unused where the pitch is odd)
   CUtensorMap umap[3];
   bool umapOk = false;
+  // and those of the FP64 reconstruction's halo tiles (five-variable systems, even pitch)
+  CUtensorMap dmap[3];
+  bool dmapOk = false;
   int64_t nRhs = 0, nWenoLast = 0;
   int nTS = 1;
   double dmin = 0.0;
@@ -557,8 +560,8 @@ int eval_front(kfvm_solver *s, int b) {
                                     s->F, s->W, s->src, s->status,
                                     s->lamvel, s->bnd, s->sc, st);
            }
-           return launch_recon(dim, eq, s->Ub[b], s->g, s->dS, wantInd, s->F, s->W, s->src, s->status, s->lamvel,
-                               s->bnd, st);
+           return launch_recon(dim, eq, s->Ub[b], s->dmapOk ? &s->dmap[b] : nullptr, s->g, s->dS, wantInd, s->F,
+                               s->W, s->src, s->status, s->lamvel, s->bnd, s->sc, st);
          })) != cudaSuccess)
       return set_err_cuda(e, "recon");
   }
@@ -1043,6 +1046,13 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if ((e = cudaMemsetAsync(s->sc, 0, sizeof(DevScalars), s->stream)) != cudaSuccess) return cleanup(e, "memset");
 
   if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return cleanup(e, "sync");
+  // TMA maps of the FP64 reconstruction's halo tiles (five variables, even pitch;
+  // otherwise that kernel reads the state with plain loads)
+  if (s->nv == 5) {
+    bool all = true;
+    for (int b = 0; b < 3; b++) all = all && recon_dmma_state_map(&s->dmap[b], s->Ub[b], g, s->dim, s->nv) == 0;
+    s->dmapOk = all;
+  }
   *out = s;
   return KFVM_OK;
 }

@@ -10,6 +10,7 @@
 #include "kernels.cuh"
 #include "launch.h"
 #include "recon_common.cuh"
+#include "tma.cuh"
 
 namespace kfvm {
 
@@ -120,6 +121,136 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
+// One group of 8 cells of a row: the DMMA contraction and the FP64 epilogue.
+// loadA(v, kc) gives variable v of stencil cell kc (kc < 4 NK) of this lane's cell
+// and loadLast(v) that of the last stencil cell; bdCell = the limiter bounds
+// [minDens | maxDens | minEint] of the lane's cell, `stride` apart.
+template <int DIM, int EQ, int NQ, class LoadA, class LoadLast>
+__device__ __forceinline__ void recon_group(const Grid &g, int lane, int64_t i, int64_t j, int64_t k, bool live,
+                                            const double *__restrict__ sB, const double *__restrict__ sWl,
+                                            const double *__restrict__ bdCell, int stride, int wantInd,
+                                            double *const (&F)[3], float *const (&W)[3], double *__restrict__ src,
+                                            uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
+                                            LoadA loadA, LoadLast loadLast) {
+  using T = Cfg<DIM, EQ, NQ>;
+  using Sh = DmmaShape<DIM, EQ, NQ>;
+  constexpr int NV = T::NV, NT = Sh::NT, NK = Sh::NK;
+  double acc[NV][NT][2];
+#pragma unroll
+  for (int v = 0; v < NV; v++)
+#pragma unroll
+    for (int t = 0; t < NT; t++) acc[v][t][0] = acc[v][t][1] = 0.0;
+#pragma unroll 4
+  for (int ks = 0; ks < NK; ks++) {
+    const int kc = ks * 4 + (lane & 3);
+    double a[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) a[v] = loadA(v, kc);
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      const double b = sB[(ks * NT + t) * 32 + lane];
+#pragma unroll
+      for (int v = 0; v < NV; v++) dmma_884(acc[v][t], a[v], b);
+    }
+  }
+  {
+    // the last stencil cell
+    double ul[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) ul[v] = loadLast(v);
+#pragma unroll
+    for (int t = 0; t < NT; t++)
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const double wl = sWl[t * 8 + 2 * (lane & 3) + e];
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v][t][e] = fma(wl, ul[v], acc[v][t][e]);
+      }
+  }
+  bool inside = true;
+  double lam = 0.0, vel = 0.0;
+  if (live) {
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    PosBounds bd;
+    bd.minDens = bdCell[0];
+    bd.maxDens = bdCell[stride];
+    bd.minEint = bdCell[2 * stride];
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      const int rw0 = t * 8 + 2 * (lane & 3);
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        // row 8t + 2(lane%4) + e: face point q = row % NQF of face f = row / NQF
+        // (rows past the face points are interior points); with an even NQF both
+        // rows of a lane lie on one face, which the compiler then computes once
+        const int rw = rw0 + e;
+        const int fr = (T::NQF % 2 == 0 ? rw0 : rw) / T::NQF;
+        const int f = fr < T::NF ? fr : 0;
+        const int d = f >> 1;
+        const int hi = f & 1;
+        const int64_t nf = g.nface[d];
+        const int64_t fidx = ((k + (d == 2 && hi)) * g.fdim[d][1] + (j + (d == 1 && hi))) * g.fdim[d][0] +
+                             (i + (d == 0 && hi));
+        const int slot = hi ? 0 : 1;
+        if (rw < Sh::NR) {
+          double st[NV];
+#pragma unroll
+          for (int v = 0; v < NV; v++) st[v] = acc[v][t][e];
+          // pos_inside, with the internal energy kept for the indicator's pressure
+          double ei = 0.0;
+          if constexpr (EQ == EQ_SR) {
+            inside = inside && pos_inside<EQ>(bd, st);
+          } else {
+            // Euler / Navier-Stokes: without the IEEE division (GLM-MHD, whose
+            // kernel it slowed, keeps the plain expression)
+            if constexpr (EQ == EQ_GLM) ei = Eos<EQ>::eint(st);
+            else ei = Eos<EQ>::eint_vs(st, bd.minEint);
+            inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
+          }
+          if (rw < T::NF * T::NQF) {
+            const int q = rw % T::NQF;
+            double *Fd = F[d];
+            const int64_t a = (int64_t)((slot * T::NQF + q) * NV) * nf + fidx;
+#pragma unroll
+            for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
+            if (wantInd) {
+              // SR: the indicator is the density itself, stored rounded
+              const float wv = EQ == EQ_SR ? __double2float_rn(st[DENS])
+                                           : Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
+              W[d][(int64_t)(slot * T::NQF + q) * nf + fidx] = wv;
+            }
+            if constexpr (T::SRC) {
+              // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
+              const double vv = fabs(st[MOMX] / st[DENS]);
+              const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
+              vel = vv > vel ? vv : vel;
+              lam = l > lam ? l : lam;
+            }
+          } else if constexpr (T::SRC) {
+            const int q = rw - T::NF * T::NQF;
+#pragma unroll
+            for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
+          }
+        }
+      }
+    }
+  }
+  // combine the four lanes of each cell
+  inside = __shfl_xor_sync(0xffffffffu, (int)inside, 1) && inside;
+  inside = __shfl_xor_sync(0xffffffffu, (int)inside, 2) && inside;
+  if constexpr (T::SRC) {
+    lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, 1));
+    lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, 2));
+    vel = fmax(vel, __shfl_xor_sync(0xffffffffu, vel, 1));
+    vel = fmax(vel, __shfl_xor_sync(0xffffffffu, vel, 2));
+  }
+  if (live && (lane & 3) == 0) {
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    if constexpr (T::SRC) lamvel[c] = make_double2(lam, vel);
+    status[c] = inside ? 1 : 0;
+  }
+}
+
 template <int DIM, int EQ, int NQ>
 __global__ void __launch_bounds__(128)
     recon_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
@@ -163,130 +294,207 @@ __global__ void __launch_bounds__(128)
   const int lane = threadIdx.x;
   const int64_t j = blockIdx.y * (int64_t)kBlockY + threadIdx.y;
   const bool rowLive = j < g.ny;
-  double *F[3] = {F0, F1, F2};
-  float *W[3] = {W0, W1, W2};
+  double *const F[3] = {F0, F1, F2};
+  float *const W[3] = {W0, W1, W2};
 #pragma unroll 1
   for (int grp = 0; grp < kBlockX / 8; grp++) {
     const int cx = grp * 8 + (lane >> 2);
     const int64_t i = blockIdx.x * (int64_t)kBlockX + cx;
     const bool live = rowLive && i < g.nx;
     const double *Uc = U + pidx(g, live ? i : 0, rowLive ? j : 0, k);
-    double acc[NV][NT][2];
+    recon_group<DIM, EQ, NQ>(
+        g, lane, i, j, k, live, sB, sWl, &sBd[0][threadIdx.y * kBlockX + cx], kBlockX * kBlockY, wantInd, F, W, src,
+        status, lamvel, [&](int v, int kc) { return __ldg(Uc + v * g.pvol + sOff[kc]); },
+        [&](int v) { return __ldg(Uc + v * g.pvol + oLast); });
+  }
+}
+
+// The same reconstruction with the state staged in shared memory by TMA (Euler,
+// Navier-Stokes and SR: 5 variables): one 4D tensor load per variable brings the
+// block's halo tile (the cell tile plus 2 cells on every side) into shared memory
+// on one mbarrier; the limiter footprint and every stencil operand then come from
+// there.  3D tile 32 x 4 x 2 cells, 2D 32 x 8; one warp per row of 32 cells.
+template <int DIM>
+struct DmmaTile {
+  static constexpr int BX = kBlockX, BY = DIM == 3 ? 4 : 8, BZ = DIM == 3 ? 2 : 1;
+  static constexpr int WARPS = BY * BZ, THREADS = 32 * WARPS, CELLS = BX * BY * BZ;
+  static constexpr int R = kRad;
+  static constexpr int TX = BX + 2 * R, TY = BY + 2 * R, TZ = DIM == 3 ? BZ + 2 * R : 1;
+  static constexpr int N = TX * TY * TZ;  // halo tile of one variable
+  static constexpr int PX = BX + 2, PY = BY + 2, PZ = DIM == 3 ? BZ + 2 : 1;
+  static constexpr int PN = PX * PY * PZ; // limiter footprint: the block and a one-cell ring
+  static_assert((TX * 8) % 16 == 0 && (N * 8) % 128 == 0, "TMA box inner extent, tile alignment");
+};
+
+template <int DIM, int EQ, int NQ>
+struct DmmaTmaSmem {
+  using T = Cfg<DIM, EQ, NQ>;
+  using Sh = DmmaShape<DIM, EQ, NQ>;
+  using D = DmmaTile<DIM>;
+  static constexpr int NV = T::NV;
+  static constexpr int NP = EQ == EQ_SR ? 1 : 2;  // footprint arrays besides rho: eint, sound speed (SR: E - |S|)
+  static constexpr int OFF_P = NV * D::N * 8;      // the halo tiles [v][z][y][x] come first
+  static constexpr int OFF_B = OFF_P + NP * D::PN * 8;
+  static constexpr int OFF_BD = OFF_B + Sh::BSIZE * 8;
+  static constexpr int OFF_WL = OFF_BD + 3 * D::CELLS * 8;
+  static constexpr int OFF_TO = OFF_WL + Sh::NT * 8 * 8;
+  static constexpr int OFF_BAR = (OFF_TO + (4 * Sh::NK + 1) * 4 + 7) / 8 * 8;
+  static constexpr int BYTES = OFF_BAR + 8;
+  static_assert(BYTES <= 113 * 1024, "two blocks per SM");
+};
+
+template <int DIM, int EQ, int NQ>
+__global__ void __launch_bounds__(DmmaTile<DIM>::THREADS, 2)
+    recon_tma_kernel(const __grid_constant__ CUtensorMap umap, Grid g, const DevStencil *__restrict__ S, int wantInd,
+                     double *__restrict__ F0, double *__restrict__ F1, double *__restrict__ F2,
+                     float *__restrict__ W0, float *__restrict__ W1, float *__restrict__ W2,
+                     double *__restrict__ src, uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
+                     double *__restrict__ bnd, DevScalars *__restrict__ sc) {
+  using T = Cfg<DIM, EQ, NQ>;
+  using Sh = DmmaShape<DIM, EQ, NQ>;
+  using D = DmmaTile<DIM>;
+  using L = DmmaTmaSmem<DIM, EQ, NQ>;
+  using E = Eos<EQ>;
+  constexpr int NV = T::NV, NT = Sh::NT, NK = Sh::NK;
+  static_assert(NV == 5, "the TMA-staged tile holds five variables");
+  extern __shared__ __align__(128) uint8_t smem[];
+  const double *sU = reinterpret_cast<const double *>(smem);
+  double *sP = reinterpret_cast<double *>(smem + L::OFF_P);
+  double *sB = reinterpret_cast<double *>(smem + L::OFF_B);
+  double *sBd = reinterpret_cast<double *>(smem + L::OFF_BD);
+  double *sWl = reinterpret_cast<double *>(smem + L::OFF_WL);
+  int *sTo = reinterpret_cast<int *>(smem + L::OFF_TO);
+  const uint32_t bar = smem_u32(smem + L::OFF_BAR);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ty = warp % D::BY, tz = warp / D::BY;
+  // the tile's first padded coordinates: cell (i0 - 2, j0 - 2, k0 - 2)
+  const int i0 = (int)(blockIdx.x * D::BX), j0 = (int)(blockIdx.y * D::BY), k0 = (int)(blockIdx.z * D::BZ);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_arrive_expect_tx(bar, (uint32_t)(NV * D::N * 8));
 #pragma unroll
-    for (int v = 0; v < NV; v++)
+    for (int v = 0; v < NV; v++) tma_load_4d(smem_u32(smem + v * D::N * 8), &umap, i0, j0, k0, v, bar);
+  }
+  for (int t = tid; t < Sh::BSIZE; t += D::THREADS) sB[t] = S->dmma_b[t];
+  if (tid < NT * 8) sWl[tid] = tid < Sh::NR ? S->lin[(T::C - 1) * Sh::NR + tid] : 0.0;
+  if (tid < 4 * NK + 1) {
+    // stencil cell c (the last one at 4 NK) as an offset in the halo tile
+    const int c = tid < 4 * NK ? tid : T::C - 1;
+    const int dz = DIM == 3 ? (int)S->w.off[2][c] : 0;
+    sTo[tid] = (dz * D::TY + (int)S->w.off[1][c]) * D::TX + (int)S->w.off[0][c];
+  }
+  __syncthreads();  // the barrier's initialisation is visible to every waiting thread
+  if (!mbar_wait(bar, 0)) {
+    // the tile never arrived: record it, give the copies in flight a bounded time
+    // to land, and leave
+    if (tid == 0) atomicExch(&sc->fault, 1u);
+    mbar_wait(bar, 0);
+    return;
+  }
+  // limiter footprint: eint and sound speed (SR: E - |S|) of the block and its ring
+  for (int t = tid; t < D::PN; t += D::THREADS) {
+    const int a = t % D::PX, b = (t / D::PX) % D::PY, cz = t / (D::PX * D::PY);
+    const int h = ((cz + (DIM == 3 ? 1 : 0)) * D::TY + (b + 1)) * D::TX + (a + 1);
+    double st[NV];
 #pragma unroll
-      for (int t = 0; t < NT; t++) acc[v][t][0] = acc[v][t][1] = 0.0;
-#pragma unroll 4
-    for (int ks = 0; ks < NK; ks++) {
-      const int kc = ks * 4 + (lane & 3);
-      const int64_t o = sOff[kc];
-      double a[NV];
-#pragma unroll
-      for (int v = 0; v < NV; v++) a[v] = __ldg(Uc + v * g.pvol + o);
-#pragma unroll
-      for (int t = 0; t < NT; t++) {
-        const double b = sB[(ks * NT + t) * 32 + lane];
-#pragma unroll
-        for (int v = 0; v < NV; v++) dmma_884(acc[v][t], a[v], b);
-      }
-    }
-    {
-      // the last stencil cell
-      double ul[NV];
-#pragma unroll
-      for (int v = 0; v < NV; v++) ul[v] = __ldg(Uc + v * g.pvol + oLast);
-#pragma unroll
-      for (int t = 0; t < NT; t++)
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const double wl = sWl[t * 8 + 2 * (lane & 3) + e];
-#pragma unroll
-          for (int v = 0; v < NV; v++) acc[v][t][e] = fma(wl, ul[v], acc[v][t][e]);
-        }
-    }
-    bool inside = true;
-    double lam = 0.0, vel = 0.0;
-    if (live) {
-      const int64_t c = (k * g.ny + j) * g.nx + i;
-      PosBounds bd;
-      bd.minDens = sBd[0][threadIdx.y * kBlockX + cx];
-      bd.maxDens = sBd[1][threadIdx.y * kBlockX + cx];
-      bd.minEint = sBd[2][threadIdx.y * kBlockX + cx];
-#pragma unroll
-      for (int t = 0; t < NT; t++) {
-        const int rw0 = t * 8 + 2 * (lane & 3);
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          // row 8t + 2(lane%4) + e: face point q = row % NQF of face f = row / NQF
-          // (rows past the face points are interior points); with an even NQF both
-          // rows of a lane lie on one face, which the compiler then computes once
-          const int rw = rw0 + e;
-          const int fr = (T::NQF % 2 == 0 ? rw0 : rw) / T::NQF;
-          const int f = fr < T::NF ? fr : 0;
-          const int d = f >> 1;
-          const int hi = f & 1;
-          const int64_t nf = g.nface[d];
-          const int64_t fidx = ((k + (d == 2 && hi)) * g.fdim[d][1] + (j + (d == 1 && hi))) * g.fdim[d][0] +
-                               (i + (d == 0 && hi));
-          const int slot = hi ? 0 : 1;
-          if (rw < Sh::NR) {
-            double st[NV];
-#pragma unroll
-            for (int v = 0; v < NV; v++) st[v] = acc[v][t][e];
-            // pos_inside, with the internal energy kept for the indicator's pressure
-            double ei = 0.0;
-            if constexpr (EQ == EQ_SR) {
-              inside = inside && pos_inside<EQ>(bd, st);
-            } else {
-              // Euler / Navier-Stokes: without the IEEE division (GLM-MHD, whose
-              // kernel it slowed, keeps the plain expression)
-              if constexpr (EQ == EQ_GLM) ei = Eos<EQ>::eint(st);
-              else ei = Eos<EQ>::eint_vs(st, bd.minEint);
-              inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
-            }
-            if (rw < T::NF * T::NQF) {
-              const int q = rw % T::NQF;
-              double *Fd = F[d];
-              const int64_t a = (int64_t)((slot * T::NQF + q) * NV) * nf + fidx;
-#pragma unroll
-              for (int v = 0; v < NV; v++) Fd[a + v * nf] = st[v];
-              if (wantInd) {
-                // SR: the indicator is the density itself, stored rounded
-                const float wv = EQ == EQ_SR ? __double2float_rn(st[DENS])
-                                             : Eos<EQ>::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
-                W[d][(int64_t)(slot * T::NQF + q) * nf + fidx] = wv;
-              }
-              if constexpr (T::SRC) {
-                // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
-                const double vv = fabs(st[MOMX] / st[DENS]);
-                const double l = Eos<EQ>::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
-                vel = vv > vel ? vv : vel;
-                lam = l > lam ? l : lam;
-              }
-            } else if constexpr (T::SRC) {
-              const int q = rw - T::NF * T::NQF;
-#pragma unroll
-              for (int v = 0; v < NV; v++) src[(q * NV + v) * g.n + c] = st[v];
-            }
-          }
-        }
-      }
-    }
-    // combine the four lanes of each cell
-    inside = __shfl_xor_sync(0xffffffffu, (int)inside, 1) && inside;
-    inside = __shfl_xor_sync(0xffffffffu, (int)inside, 2) && inside;
-    if constexpr (T::SRC) {
-      lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, 1));
-      lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, 2));
-      vel = fmax(vel, __shfl_xor_sync(0xffffffffu, vel, 1));
-      vel = fmax(vel, __shfl_xor_sync(0xffffffffu, vel, 2));
-    }
-    if (live && (lane & 3) == 0) {
-      const int64_t c = (k * g.ny + j) * g.nx + i;
-      if constexpr (T::SRC) lamvel[c] = make_double2(lam, vel);
-      status[c] = inside ? 1 : 0;
+    for (int v = 0; v < NV; v++) st[v] = sU[v * D::N + h];
+    if constexpr (EQ == EQ_SR) {
+      sP[t] = sr::ediff(st);
+    } else {
+      const double ir = 1.0 / st[DENS];
+      const double ei = E::eint_r(st, ir);
+      sP[t] = ei;
+      sP[D::PN + t] = sqrt(g.gamma * ((g.gamma - 1.0) * ei) * ir);
     }
   }
+  __syncthreads();
+  {
+    // PositivityPreserve_K bounds (Common_K.H:331-380; SR: SRHydro_K.H:224-246) of
+    // this thread's cell, from the footprint (the same values pos_bounds_tile gives)
+    constexpr int zr = DIM == 3 ? 1 : 0;
+    auto pt = [&](int xo, int yo, int zo) { return ((tz + zr + zo) * D::PY + (ty + 1 + yo)) * D::PX + (lane + 1 + xo); };
+    auto ht = [&](int xo, int yo, int zo) {
+      return ((tz + (DIM == 3 ? 2 : 0) + zo) * D::TY + (ty + 2 + yo)) * D::TX + (lane + 2 + xo);
+    };
+    double maxDens = -1.7976931348623157e308, minDens = 1.7976931348623157e308;
+    double minEint = 1.7976931348623157e308, minSdSp = 1.7976931348623157e308;
+#pragma unroll
+    for (int xo = -1; xo <= 1; xo++)
+#pragma unroll
+      for (int yo = -1; yo <= 1; yo++)
+#pragma unroll
+        for (int zo = -zr; zo <= zr; zo++) {
+          const double r = sU[DENS * D::N + ht(xo, yo, zo)];
+          maxDens = fmax(maxDens, r);
+          minDens = fmin(minDens, r);
+          minEint = fmin(minEint, sP[pt(xo, yo, zo)]);
+          if constexpr (EQ != EQ_SR) minSdSp = fmin(minSdSp, sP[D::PN + pt(xo, yo, zo)]);
+        }
+    PosBounds bd;
+    if constexpr (EQ == EQ_SR) {
+      bd = PosBounds{sU[DENS * D::N + ht(0, 0, 0)], minDens, maxDens, minEint};
+    } else {
+      auto vel = [&](int m, int xo, int yo, int zo) {
+        const int h = ht(xo, yo, zo);
+        return sU[m * D::N + h] * (1.0 / sU[DENS * D::N + h]);
+      };
+      const double dxU = vel(MOMX, 1, 0, 0) - vel(MOMX, -1, 0, 0);
+      const double dyV = vel(MOMY, 0, 1, 0) - vel(MOMY, 0, -1, 0);
+      const double dzW = vel(MOMZ, 0, 0, zr) - vel(MOMZ, 0, 0, -zr);
+      const double divV = (dxU + dyV + dzW) / 2.0;
+      double kappa = 0.2;
+      const double eta = fmin(1.0, fmax(0.0, -(kappa * minSdSp + divV) / (kappa * minSdSp)));
+      kappa *= (1.0 - eta);
+      bd.rDens = sU[DENS * D::N + ht(0, 0, 0)];
+      bd.maxDens = maxDens * (1.0 + kappa);
+      bd.minDens = minDens * (1.0 - kappa);
+      bd.minEint = minEint * (1.0 - kappa);
+    }
+    sBd[tid] = bd.minDens;
+    sBd[D::CELLS + tid] = bd.maxDens;
+    sBd[2 * D::CELLS + tid] = bd.minEint;
+    // and for the heavy pass
+    const int64_t bi = i0 + lane, bj = j0 + ty, bk = k0 + tz;
+    if (bi < g.nx && bj < g.ny && bk < g.nz) {
+      const int64_t c = (bk * g.ny + bj) * g.nx + bi;
+      bnd[c] = bd.minDens;
+      bnd[g.n + c] = bd.maxDens;
+      bnd[2 * g.n + c] = bd.minEint;
+    }
+  }
+  __syncthreads();
+  const int64_t j = j0 + ty, k = k0 + tz;
+  const bool rowLive = j < g.ny && k < g.nz;
+  double *const F[3] = {F0, F1, F2};
+  float *const W[3] = {W0, W1, W2};
+  const int toLast = sTo[4 * NK];
+#pragma unroll 1
+  for (int grp = 0; grp < D::BX / 8; grp++) {
+    const int cx = grp * 8 + (lane >> 2);
+    const int64_t i = i0 + cx;
+    const bool live = rowLive && i < g.nx;
+    // the lane's cell in the halo tile
+    const double *Uc = sU + ((tz + (DIM == 3 ? 2 : 0)) * D::TY + (ty + 2)) * D::TX + (cx + 2);
+    recon_group<DIM, EQ, NQ>(
+        g, lane, i, j, k, live, sB, sWl, sBd + (ty + D::BY * tz) * D::BX + cx, D::CELLS, wantInd, F, W, src,
+        status, lamvel, [&](int v, int kc) { return Uc[v * D::N + sTo[kc]]; },
+        [&](int v) { return Uc[v * D::N + toLast]; });
+  }
+}
+
+// host: the 4D tensor map of a padded state buffer for the TMA-staged tiles (x, y,
+// z, variable; box = the halo tile of one variable).  Returns nonzero where TMA
+// cannot be used (an odd pitch breaks the 16-byte stride rule).
+int recon_dmma_state_map(CUtensorMap *map, const double *U, const Grid &g, int dim, int nv) {
+  if (g.px % 2 != 0) return 1;
+  const uint64_t planes = (uint64_t)(g.pvol / (g.px * g.py));
+  const uint64_t dims[4] = {(uint64_t)g.px, (uint64_t)g.py, planes, (uint64_t)nv};
+  const uint64_t strides[3] = {(uint64_t)g.px * 8, (uint64_t)(g.px * g.py) * 8, (uint64_t)g.pvol * 8};
+  const uint32_t box[4] = {(uint32_t)(dim == 3 ? DmmaTile<3>::TX : DmmaTile<2>::TX),
+                           (uint32_t)(dim == 3 ? DmmaTile<3>::TY : DmmaTile<2>::TY),
+                           (uint32_t)(dim == 3 ? DmmaTile<3>::TZ : DmmaTile<2>::TZ), 1u};
+  return encode_tensor_map_8b(map, U, 4, dims, strides, box);
 }
 
 // PositivityPreserve_K bounds of every cell (Common_K.H:331-380; SR: SRHydro_K.H:224-246)
@@ -1443,9 +1651,24 @@ struct Launch {
     bounds_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, bnd);
     return cudaGetLastError();
   }
-  static cudaError_t recon(const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                           double *const *F, float *const *W, double *src, uint8_t *status,
-                           double2 *lamvel, double *bnd, cudaStream_t s) {
+  static cudaError_t recon(const double *U, const CUtensorMap *umap, const Grid &g, const DevStencil *S,
+                           int wantInd, double *const *F, float *const *W, double *src, uint8_t *status,
+                           double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s) {
+    if constexpr (NV == 5) {
+      if (umap) {
+        // the halo tiles staged by TMA (five variables: Euler, Navier-Stokes, SR)
+        using D = DmmaTile<DIM>;
+        using L = DmmaTmaSmem<DIM, EQ, NQ>;
+        static const cudaError_t attr = cudaFuncSetAttribute(
+            recon_tma_kernel<DIM, EQ, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
+        if (attr != cudaSuccess) return attr;
+        const dim3 grid((unsigned)((g.nx + D::BX - 1) / D::BX), (unsigned)((g.ny + D::BY - 1) / D::BY),
+                        (unsigned)((g.nz + D::BZ - 1) / D::BZ));
+        recon_tma_kernel<DIM, EQ, NQ><<<grid, D::THREADS, L::BYTES, s>>>(
+            *umap, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd, sc);
+        return cudaGetLastError();
+      }
+    }
     recon_kernel<DIM, EQ, NQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
         U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd);
     return cudaGetLastError();
@@ -1627,10 +1850,10 @@ cudaError_t launch_bounds(int dim, int eq, const double *U, const Grid &g, doubl
   KFVM_DISPATCH(dim, eq, bounds(U, g, bnd, s));
 }
 
-cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                         double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
-                         double *bnd, cudaStream_t s) {
-  KFVM_DISPATCH(dim, eq, recon(U, g, S, wantInd, F, W, src, status, lamvel, bnd, s));
+cudaError_t launch_recon(int dim, int eq, const double *U, const CUtensorMap *umap, const Grid &g,
+                         const DevStencil *S, int wantInd, double *const *F, float *const *W, double *src,
+                         uint8_t *status, double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s) {
+  KFVM_DISPATCH(dim, eq, recon(U, umap, g, S, wantInd, F, W, src, status, lamvel, bnd, sc, s));
 }
 cudaError_t launch_flag(int dim, int eq, const double *U, const Grid &g, float *const *W, double *const *F,
                         const double *theta, uint8_t *flag, DevScalars *sc, double thr,

@@ -59,9 +59,14 @@ cudaError_t launch_bounds(int dim, int eq, const double *U, const Grid &g, doubl
 // stage front end: linear states + KXRCF indicator + limiter bound status,
 // KXRCF flags, WENO decision / heavy-list compaction, heavy cells
 // bnd: the limiter bounds of every cell from launch_bounds
-cudaError_t launch_recon(int dim, int eq, const double *U, const Grid &g, const DevStencil *S, int wantInd,
-                         double *const *F, float *const *W, double *src, uint8_t *status, double2 *lamvel,
-                         double *bnd, cudaStream_t s);
+// (the FP64 form computes the limiter bounds itself and writes them to bnd).  umap
+// (recon_dmma_state_map of U, five-variable systems) stages the halo tiles by TMA;
+// null reads the state with plain global loads; a block whose wait gave up sets
+// sc->fault
+cudaError_t launch_recon(int dim, int eq, const double *U, const CUtensorMap *umap, const Grid &g,
+                         const DevStencil *S, int wantInd, double *const *F, float *const *W, double *src,
+                         uint8_t *status, double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s);
+int recon_dmma_state_map(CUtensorMap *map, const double *U, const Grid &g, int dim, int nv);
 // the same outputs with the stencil sum on the tcgen05 tensor cores (3xTF32);
 // umap (recon_tc_state_map of U) stages the halo tiles by TMA, null loads them
 // with plain global loads; a block whose wait gave up sets sc->fault
