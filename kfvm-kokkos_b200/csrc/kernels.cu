@@ -140,7 +140,10 @@ __device__ __forceinline__ void recon_group(const Grid &g, int lane, int64_t i, 
   for (int v = 0; v < NV; v++)
 #pragma unroll
     for (int t = 0; t < NT; t++) acc[v][t][0] = acc[v][t][1] = 0.0;
-#pragma unroll 4
+  // the whole K loop unrolled where the accumulators are few (Euler / NS with two
+  // Gauss points: 15 pairs), by four otherwise (register pressure)
+  constexpr int UNR = NV * NT <= 15 ? NK : 4;
+#pragma unroll UNR
   for (int ks = 0; ks < NK; ks++) {
     const int kc = ks * 4 + (lane & 3);
     double a[NV];
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(128)
                  uint8_t *__restrict__ status, double2 *__restrict__ lamvel, double *__restrict__ bnd) {
   using T = Cfg<DIM, EQ, NQ>;
   using Sh = DmmaShape<DIM, EQ, NQ>;
-  constexpr int NV = T::NV, NT = Sh::NT, NK = Sh::NK;
+  constexpr int NT = Sh::NT, NK = Sh::NK;
   __shared__ double tile[6][PosTile<DIM>::N];
   __shared__ double sB[Sh::BSIZE];
   __shared__ int64_t sOff[NK * 4];
@@ -1654,7 +1657,9 @@ struct Launch {
   static cudaError_t recon(const double *U, const CUtensorMap *umap, const Grid &g, const DevStencil *S,
                            int wantInd, double *const *F, float *const *W, double *src, uint8_t *status,
                            double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s) {
-    if constexpr (NV == 5) {
+    // (3D with three Gauss points keeps the global-load kernel: its 54 rows need
+    // more accumulator registers than two 256-thread blocks per SM leave)
+    if constexpr (NV == 5 && (DIM == 2 || NQ == 2)) {
       if (umap) {
         // the halo tiles staged by TMA (five variables: Euler, Navier-Stokes, SR)
         using D = DmmaTile<DIM>;
