@@ -279,7 +279,7 @@ struct kfvm_solver {
   // tiles (built when the FP32 form is selected; unused where the pitch is odd)
   CUtensorMap umap[3];
   bool umapOk = false;
-  // and those of the FP64 reconstruction's halo tiles (five-variable systems, even pitch)
+  // and those of the FP64 reconstruction's halo tiles (five variables or 2D, even pitch)
   CUtensorMap dmap[3];
   bool dmapOk = false;
   int64_t nRhs = 0, nWenoLast = 0;
@@ -1046,9 +1046,9 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if ((e = cudaMemsetAsync(s->sc, 0, sizeof(DevScalars), s->stream)) != cudaSuccess) return cleanup(e, "memset");
 
   if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return cleanup(e, "sync");
-  // TMA maps of the FP64 reconstruction's halo tiles (five variables, even pitch;
-  // otherwise that kernel reads the state with plain loads)
-  if (s->nv == 5) {
+  // TMA maps of the FP64 reconstruction's halo tiles (five variables, or GLM-MHD in
+  // 2D; even pitch; otherwise that kernel reads the state with plain loads)
+  if (s->nv == 5 || s->dim == 2) {
     bool all = true;
     for (int b = 0; b < 3; b++) all = all && recon_dmma_state_map(&s->dmap[b], s->Ub[b], g, s->dim, s->nv) == 0;
     s->dmapOk = all;

@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(128)
 }
 
 // The same reconstruction with the state staged in shared memory by TMA (Euler,
-// Navier-Stokes and SR: 5 variables): one 4D tensor load per variable brings the
+// Navier-Stokes and SR; GLM-MHD in 2D): one 4D tensor load per variable brings the
 // block's halo tile (the cell tile plus 2 cells on every side) into shared memory
 // on one mbarrier; the limiter footprint and every stencil operand then come from
 // there.  3D tile 32 x 4 x 2 cells, 2D 32 x 8; one warp per row of 32 cells.
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(DmmaTile<DIM>::THREADS, 2)
   using L = DmmaTmaSmem<DIM, EQ, NQ>;
   using E = Eos<EQ>;
   constexpr int NV = T::NV, NT = Sh::NT, NK = Sh::NK;
-  static_assert(NV == 5, "the TMA-staged tile holds five variables");
+  static_assert(NV == 5 || DIM == 2, "nine-variable halo tiles in 2D only");
   extern __shared__ __align__(128) uint8_t smem[];
   const double *sU = reinterpret_cast<const double *>(smem);
   double *sP = reinterpret_cast<double *>(smem + L::OFF_P);
@@ -1658,8 +1658,10 @@ struct Launch {
                            int wantInd, double *const *F, float *const *W, double *src, uint8_t *status,
                            double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s) {
     // (3D with three Gauss points keeps the global-load kernel: its 54 rows need
-    // more accumulator registers than two 256-thread blocks per SM leave)
-    if constexpr (NV == 5 && (DIM == 2 || NQ == 2)) {
+    // more accumulator registers than two 256-thread blocks per SM leave; so does
+    // GLM-MHD in 3D, whose nine halo tiles would not leave room for two blocks, and
+    // with three points in 2D)
+    if constexpr ((NV == 5 && (DIM == 2 || NQ == 2)) || (NV == 9 && DIM == 2 && NQ == 2)) {
       if (umap) {
         // the halo tiles staged by TMA (five variables: Euler, Navier-Stokes, SR)
         using D = DmmaTile<DIM>;

@@ -60,7 +60,7 @@ cudaError_t launch_bounds(int dim, int eq, const double *U, const Grid &g, doubl
 // KXRCF flags, WENO decision / heavy-list compaction, heavy cells
 // bnd: the limiter bounds of every cell from launch_bounds
 // (the FP64 form computes the limiter bounds itself and writes them to bnd).  umap
-// (recon_dmma_state_map of U, five-variable systems) stages the halo tiles by TMA;
+// (recon_dmma_state_map of U; five variables, or GLM-MHD in 2D) stages the halo tiles by TMA;
 // null reads the state with plain global loads; a block whose wait gave up sets
 // sc->fault
 cudaError_t launch_recon(int dim, int eq, const double *U, const CUtensorMap *umap, const Grid &g,
