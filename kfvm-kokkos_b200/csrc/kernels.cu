@@ -121,21 +121,17 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-// One group of 8 cells of a row: the DMMA contraction and the FP64 epilogue.
-// loadA(v, kc) gives variable v of stencil cell kc (kc < 4 NK) of this lane's cell
-// and loadLast(v) that of the last stencil cell; bdCell = the limiter bounds
-// [minDens | maxDens | minEint] of the lane's cell, `stride` apart.
+// One group of 8 cells of a row, the DMMA contraction: lane l ends with rows
+// 8t + 2(l%4) + e of cell l/4 of the group in acc[v][t][e].  loadA(v, kc) gives
+// variable v of stencil cell kc (kc < 4 NK) of this lane's cell and loadLast(v)
+// that of the last stencil cell.
 template <int DIM, int EQ, int NQ, class LoadA, class LoadLast>
-__device__ __forceinline__ void recon_group(const Grid &g, int lane, int64_t i, int64_t j, int64_t k, bool live,
-                                            const double *__restrict__ sB, const double *__restrict__ sWl,
-                                            const double *__restrict__ bdCell, int stride, int wantInd,
-                                            double *const (&F)[3], float *const (&W)[3], double *__restrict__ src,
-                                            uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
-                                            LoadA loadA, LoadLast loadLast) {
+__device__ __forceinline__ void recon_group_mma(int lane, const double *__restrict__ sB,
+                                                const double *__restrict__ sWl, LoadA loadA, LoadLast loadLast,
+                                                double (&acc)[Cfg<DIM, EQ, NQ>::NV][DmmaShape<DIM, EQ, NQ>::NT][2]) {
   using T = Cfg<DIM, EQ, NQ>;
   using Sh = DmmaShape<DIM, EQ, NQ>;
   constexpr int NV = T::NV, NT = Sh::NT, NK = Sh::NK;
-  double acc[NV][NT][2];
 #pragma unroll
   for (int v = 0; v < NV; v++)
 #pragma unroll
@@ -170,6 +166,20 @@ __device__ __forceinline__ void recon_group(const Grid &g, int lane, int64_t i, 
         for (int v = 0; v < NV; v++) acc[v][t][e] = fma(wl, ul[v], acc[v][t][e]);
       }
   }
+}
+
+// The FP64 epilogue of one group: limiter pre-check, KXRCF indicator, face-state
+// and source-point stores, the cell's status and GLM speed maxima.  bdCell = the
+// limiter bounds [minDens | maxDens | minEint] of the lane's cell, `stride` apart.
+template <int DIM, int EQ, int NQ>
+__device__ __forceinline__ void recon_group_epilogue(
+    const Grid &g, int lane, int64_t i, int64_t j, int64_t k, bool live, const double *__restrict__ bdCell,
+    int stride, int wantInd, double *const (&F)[3], float *const (&W)[3], double *__restrict__ src,
+    uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
+    const double (&acc)[Cfg<DIM, EQ, NQ>::NV][DmmaShape<DIM, EQ, NQ>::NT][2]) {
+  using T = Cfg<DIM, EQ, NQ>;
+  using Sh = DmmaShape<DIM, EQ, NQ>;
+  constexpr int NV = T::NV, NT = Sh::NT;
   bool inside = true;
   double lam = 0.0, vel = 0.0;
   if (live) {
@@ -252,6 +262,19 @@ __device__ __forceinline__ void recon_group(const Grid &g, int lane, int64_t i, 
     if constexpr (T::SRC) lamvel[c] = make_double2(lam, vel);
     status[c] = inside ? 1 : 0;
   }
+}
+
+// contraction and epilogue of one group in the same warp
+template <int DIM, int EQ, int NQ, class LoadA, class LoadLast>
+__device__ __forceinline__ void recon_group(const Grid &g, int lane, int64_t i, int64_t j, int64_t k, bool live,
+                                            const double *__restrict__ sB, const double *__restrict__ sWl,
+                                            const double *__restrict__ bdCell, int stride, int wantInd,
+                                            double *const (&F)[3], float *const (&W)[3], double *__restrict__ src,
+                                            uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
+                                            LoadA loadA, LoadLast loadLast) {
+  double acc[Cfg<DIM, EQ, NQ>::NV][DmmaShape<DIM, EQ, NQ>::NT][2];
+  recon_group_mma<DIM, EQ, NQ>(lane, sB, sWl, loadA, loadLast, acc);
+  recon_group_epilogue<DIM, EQ, NQ>(g, lane, i, j, k, live, bdCell, stride, wantInd, F, W, src, status, lamvel, acc);
 }
 
 template <int DIM, int EQ, int NQ>
