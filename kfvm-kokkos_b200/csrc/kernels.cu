@@ -762,88 +762,13 @@ struct HeavyShape {
   static constexpr int NRP = (NR + 1) & ~1;                  // rows padded to pairs
   static constexpr int FW = NRP * NSUM;                       // reconstruction weights [s][p][row]
   static constexpr int CELLS = 32;
-  static constexpr size_t BYTES = (size_t)(DER + FW + CELLS * NR * T::NV + CELLS * 2) * sizeof(double) +
+  static constexpr size_t BYTES = (size_t)(DER + FW + CELLS * NR * T::NV + CELLS * 2 + CELLS * T::NV) * sizeof(double) +
                                   (size_t)T::NB * T::CB * sizeof(int);
   __host__ __device__ static constexpr int n(int s) { return s == 0 ? T::C : (s == 1 ? T::CC : T::CB); }
   __host__ __device__ static constexpr int off(int s) {
     return s == 0 ? 0 : (s == 1 ? T::C : T::C + T::CC + (s - 2) * T::CB);
   }
 };
-
-// PositivityPreserve_K's theta procedure on a cell's states held as [row][v]
-// (rows: face points f*NQF+q, then interior points); Common_K.H:299-643
-template <int DIM, int EQ, int NQ>
-__device__ double pos_apply_rows(const double *__restrict__ ref, const PosBounds &bd, double *__restrict__ rs) {
-  using T = Cfg<DIM, EQ, NQ>;
-  using E = Eos<EQ>;
-  constexpr int NV = T::NV, NR = LinRows<DIM, EQ, NQ>::NROWS;
-  const double rDens = bd.rDens, minDens = bd.minDens, maxDens = bd.maxDens, minEint = bd.minEint;
-  const double rDP = maxDens - rDens, rDM = rDens - minDens;
-  if constexpr (EQ == EQ_SR) {
-    // PositivityPreserve_K<SRHydro> (SRHydro_K.H:248-437): density theta, mixed in;
-    // then the theta of the bound on E - sqrt(D^2 + S^2), mixed in; both applied
-    // also when they are 1
-    auto mixr = [&](double th) {
-      for (int r = 0; r < NR; r++)
-#pragma unroll
-        for (int v = 0; v < NV; v++) rs[r * NV + v] = ref[v] + th * (rs[r * NV + v] - ref[v]);
-    };
-    double thD = 1.0;
-    for (int r = 0; r < NR; r++) {
-      const double rho = rs[r * NV + DENS];
-      thD = rho < minDens ? fmin(thD, rDM / (rDens - rho)) : thD;
-      thD = rho > maxDens ? fmin(thD, rDP / (rho - rDens)) : thD;
-    }
-    mixr(thD);
-    const double edRef = sr::ediff(ref), edd = edRef - minEint;
-    double thE = 1.0;
-    for (int r = 0; r < NR; r++) {
-      const double ed = sr::ediff(rs + r * NV);
-      thE = ed < minEint ? fmin(thE, edd / (edRef - ed)) : thE;
-    }
-    mixr(thE);
-    return fmin(thE, thD);
-  }
-  double thD = 1.0;
-  for (int r = 0; r < NR; r++) {
-    const double rho = rs[r * NV + DENS];
-    thD = rho > minDens ? thD : fmin(thD, rDM / (rDens - rho));
-    thD = rho < maxDens ? thD : fmin(thD, rDP / (rho - rDens));
-  }
-  auto mix = [&](double th) {
-    for (int r = 0; r < NR; r++)
-#pragma unroll
-      for (int v = 0; v < NV; v++) rs[r * NV + v] = ref[v] + th * (rs[r * NV + v] - ref[v]);
-  };
-  auto replace = [&]() {
-    for (int r = 0; r < NR; r++)
-#pragma unroll
-      for (int v = 0; v < NV; v++) rs[r * NV + v] = ref[v];
-  };
-  if (thD > 0.0 && thD < 1.0) mix(thD);
-  else if (thD < 1.0) replace();
-  double thP = 1.0;
-  for (int r = 0; r < NR; r++) {
-    double st[NV];
-#pragma unroll
-    for (int v = 0; v < NV; v++) st[v] = rs[r * NV + v];
-    if (!(E::eint(st) > minEint)) {
-      double a = 0.0, b = 1.0;
-      for (int it = 0; it < 10; it++) {
-        const double c = 0.5 * (a + b);
-        double sm[NV];
-#pragma unroll
-        for (int v = 0; v < NV; v++) sm[v] = ref[v] + c * (st[v] - ref[v]);
-        if (E::eint(sm) - minEint > 0.0) a = c;
-        else b = c;
-      }
-      thP = fmin(thP, a);
-    }
-  }
-  if (thP > 0.0 && thP < 1.0) mix(thP);
-  else if (thP < 1.0) replace();
-  return fmin(thD, thP);
-}
 
 template <int DIM, int EQ, int NQ>
 __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
@@ -860,7 +785,8 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
   double *sFw = sDer + H::DER;              // [s][p][row]
   double *sFs = sFw + H::FW;                // [cell][row][v]
   double *sDep = sFs + H::CELLS * NR * NV;  // [cell][2]
-  int *sSub = reinterpret_cast<int *>(sDep + H::CELLS * 2);
+  double *sTh = sDep + H::CELLS * 2;        // limiter theta of each thread's rows [v][cell]
+  int *sSub = reinterpret_cast<int *>(sTh + H::CELLS * NV);
   const kfvm_stencil &st = S->w;
   const int tid = threadIdx.y * 32 + threadIdx.x, nt = 32 * NV;
   // weights transposed so that the rows of one stencil value are adjacent and
@@ -981,33 +907,42 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
 #pragma unroll
       for (int s = 1; s < T::NSUB; s++) om[s] -= om[0] * gam[s];
       // blend of the substencil reconstructions at every row; each stencil value
-      // feeds all rows of its substencil (per row the sum over p keeps its order)
-      double acc[NR];
-#pragma unroll
-      for (int r = 0; r < NR; r++) acc[r] = 0.0;
+      // feeds all rows of its substencil (per row the sum over p keeps its order).
+      // Many rows (3D with three Gauss points, GLM-MHD's interior points) go in
+      // passes of RCH rows, so the partial sums stay in registers.
+      constexpr int RCH = H::NRP <= 24 ? H::NRP : (H::NRP % 18 == 0 ? 18 : 16);
 #pragma unroll 1
-      for (int s = 0; s < T::NSUB; s++) {
-        const int n = H::n(s);
-        const double *Wr = sFw + H::NRP * H::off(s);
-        double tt[H::NRP];
+      for (int r0 = 0; r0 < H::NRP; r0 += RCH) {
+        double acc[RCH];
 #pragma unroll
-        for (int r = 0; r < H::NRP; r++) tt[r] = 0.0;
-        for (int p = 0; p < n; p++) {
-          const double val = Vf[cellOf(s, p)];
-          const double2 *W2 = reinterpret_cast<const double2 *>(Wr + p * H::NRP);
+        for (int r = 0; r < RCH; r++) acc[r] = 0.0;
+#pragma unroll 1
+        for (int s = 0; s < T::NSUB; s++) {
+          const int n = H::n(s);
+          const double *Wr = sFw + H::NRP * H::off(s) + r0;
+          double tt[RCH];
 #pragma unroll
-          for (int r2 = 0; r2 < H::NRP / 2; r2++) {
-            const double2 w = W2[r2];
-            tt[2 * r2] += w.x * val;
-            tt[2 * r2 + 1] += w.y * val;
+          for (int r = 0; r < RCH; r++) tt[r] = 0.0;
+          for (int p = 0; p < n; p++) {
+            const double val = Vf[cellOf(s, p)];
+            const double2 *W2 = reinterpret_cast<const double2 *>(Wr + p * H::NRP);
+#pragma unroll
+            for (int r2 = 0; r2 < RCH / 2; r2++) {
+              if (H::NRP % RCH == 0 || r0 + 2 * r2 < H::NRP) {
+                const double2 w = W2[r2];
+                tt[2 * r2] += w.x * val;
+                tt[2 * r2 + 1] += w.y * val;
+              }
+            }
           }
+          if (om[s] != 0.0)
+#pragma unroll
+            for (int r = 0; r < RCH; r++) acc[r] += om[s] * tt[r];
         }
-        if (om[s] != 0.0)
 #pragma unroll
-          for (int r = 0; r < NR; r++) acc[r] += om[s] * tt[r];
+        for (int r = 0; r < RCH; r++)
+          if (r0 + r < NR) rs[(r0 + r) * NV + v] = acc[r];
       }
-#pragma unroll
-      for (int r = 0; r < NR; r++) rs[r * NV + v] = acc[r];
     }
     auto load_linear = [&]() {
       // the linear states the reconstruction pass wrote
@@ -1029,25 +964,28 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
     const bool keepLinear = have && (e & kHeavyJudgeOnly) && !(fmax(sDep[x * 2], sDep[x * 2 + 1]) > jd.tau);
     if (keepLinear) load_linear();
     __syncthreads();
-    // ---- back to conserved variables and PositivityPreserve_K, one thread per cell
-    if (v == 0 && have) {
-      double ref[NV];
+    // ---- back to conserved variables and PositivityPreserve_K (Common_K.H:299-643;
+    // SR: SRHydro_K.H:248-437).  The cell's rows are shared among its NV threads
+    // (rows v, v + NV, ...); each theta is a minimum over rows, gathered through
+    // shared memory, so every row ends exactly as a one-thread procedure over the
+    // cell's rows in order would leave it.
+    double ref[NV];
+    PosBounds bd{};
+    if (have) {
 #pragma unroll
       for (int w = 0; w < NV; w++) ref[w] = Uc[w * g.pvol];
-      if (e & kHeavyWeno) {
+      if ((e & kHeavyWeno) && !keepLinear) {
         VarConv<EQ> vc(ref, g.gamma);
-        if (!keepLinear)
-          for (int r = 0; r < NR; r++) vc.linPrim2Cons(rs + r * NV);
-        if (e & kHeavyJudge) {
-          const double dep = fmax(sDep[x * 2], sDep[x * 2 + 1]);
-          const bool lab = dep > jd.tau, p = jd.pred[c] != 0;
-          atomicAdd(&sc->mlp_judged, 1ull);
-          if (lab) atomicAdd(&sc->mlp_pos, 1ull);
-          if (lab && !p) atomicAdd(&sc->mlp_missed, 1ull);
-          if (!lab && p) atomicAdd(&sc->mlp_false, 1ull);
-        }
+        for (int r = v; r < NR; r += NV) vc.linPrim2Cons(rs + r * NV);
       }
-      PosBounds bd;
+      if (v == 0 && (e & kHeavyWeno) && (e & kHeavyJudge)) {
+        const double dep = fmax(sDep[x * 2], sDep[x * 2 + 1]);
+        const bool lab = dep > jd.tau, p = jd.pred[c] != 0;
+        atomicAdd(&sc->mlp_judged, 1ull);
+        if (lab) atomicAdd(&sc->mlp_pos, 1ull);
+        if (lab && !p) atomicAdd(&sc->mlp_missed, 1ull);
+        if (!lab && p) atomicAdd(&sc->mlp_false, 1ull);
+      }
       if (bnd) {
         // the reconstruction pass computed them (pos_bounds_tile)
         bd.rDens = ref[DENS];
@@ -1057,9 +995,85 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
       } else {
         bd = pos_bounds<DIM, EQ>(Uc, g);
       }
-      theta[c] = pos_apply_rows<DIM, EQ, NQ>(ref, bd, rs);
+    }
+    const double rDens = bd.rDens, minDens = bd.minDens, maxDens = bd.maxDens, minEint = bd.minEint;
+    const double rDP = maxDens - rDens, rDM = rDens - minDens;
+    // the minimum of every thread's partial theta of this cell
+    auto gather = [&](double th) {
+      __syncthreads();  // the previous gather's reads are done
+      sTh[v * H::CELLS + x] = th;
+      __syncthreads();
+      double m = 1.0;
+#pragma unroll
+      for (int w = 0; w < NV; w++) m = fmin(m, sTh[w * H::CELLS + x]);
+      return m;
+    };
+    auto mix = [&](double th) {
+      for (int r = v; r < NR; r += NV)
+#pragma unroll
+        for (int w = 0; w < NV; w++) rs[r * NV + w] = ref[w] + th * (rs[r * NV + w] - ref[w]);
+    };
+    auto replace = [&]() {
+      for (int r = v; r < NR; r += NV)
+#pragma unroll
+        for (int w = 0; w < NV; w++) rs[r * NV + w] = ref[w];
+    };
+    __syncthreads();  // every row is converted
+    double thD = 1.0, th2 = 1.0;
+    if (have)
+      for (int r = v; r < NR; r += NV) {
+        const double rho = rs[r * NV + DENS];
+        if constexpr (EQ == EQ_SR) {
+          thD = rho < minDens ? fmin(thD, rDM / (rDens - rho)) : thD;
+          thD = rho > maxDens ? fmin(thD, rDP / (rho - rDens)) : thD;
+        } else {
+          thD = rho > minDens ? thD : fmin(thD, rDM / (rDens - rho));
+          thD = rho < maxDens ? thD : fmin(thD, rDP / (rho - rDens));
+        }
+      }
+    thD = gather(thD);
+    if (have) {
+      if constexpr (EQ == EQ_SR) {
+        // both thetas applied also when they are 1
+        mix(thD);
+        const double edRef = sr::ediff(ref), edd = edRef - minEint;
+        for (int r = v; r < NR; r += NV) {
+          const double ed = sr::ediff(rs + r * NV);
+          th2 = ed < minEint ? fmin(th2, edd / (edRef - ed)) : th2;
+        }
+      } else {
+        if (thD > 0.0 && thD < 1.0) mix(thD);
+        else if (thD < 1.0) replace();
+        for (int r = v; r < NR; r += NV) {
+          double st[NV];
+#pragma unroll
+          for (int w = 0; w < NV; w++) st[w] = rs[r * NV + w];
+          if (!(E::eint(st) > minEint)) {
+            double a = 0.0, b = 1.0;
+            for (int itb = 0; itb < 10; itb++) {
+              const double cm = 0.5 * (a + b);
+              double sm[NV];
+#pragma unroll
+              for (int w = 0; w < NV; w++) sm[w] = ref[w] + cm * (st[w] - ref[w]);
+              if (E::eint(sm) - minEint > 0.0) a = cm;
+              else b = cm;
+            }
+            th2 = fmin(th2, a);
+          }
+        }
+      }
+    }
+    th2 = gather(th2);
+    if (have) {
+      if constexpr (EQ == EQ_SR) {
+        mix(th2);
+      } else {
+        if (th2 > 0.0 && th2 < 1.0) mix(th2);
+        else if (th2 < 1.0) replace();
+      }
+      if (v == 0) theta[c] = fmin(thD, th2);
       if constexpr (T::SRC) {
-        for (int r = 0; r < T::NF * T::NQF; r++) {
+        for (int r = v; r < T::NF * T::NQF; r += NV) {
           const double *u = rs + r * NV;
           const double vv = fabs(u[MOMX] / u[DENS]);
           const double l = E::fastMagSonic(g.gamma, u, u[MAGX]) + vv;
@@ -1084,13 +1098,12 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
     __syncthreads();
   }
   if constexpr (T::SRC) {
-    if (threadIdx.y == 0) {
-      lam = warp_max(lam);
-      vel = warp_max(vel);
-      if (threadIdx.x == 0) {
-        atomic_max_pos(&sc->glm_lam_bits, lam);
-        atomic_max_pos(&sc->glm_vel_bits, vel);
-      }
+    // every variable thread holds the maxima of its share of the face rows
+    lam = warp_max(lam);
+    vel = warp_max(vel);
+    if (threadIdx.x == 0) {
+      atomic_max_pos(&sc->glm_lam_bits, lam);
+      atomic_max_pos(&sc->glm_vel_bits, vel);
     }
   }
 }
