@@ -885,9 +885,8 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
   if (!cfg || !out) return fail(KFVM_ERR_ARG, "null argument");
   *out = nullptr;
   if (cfg->dim != 2 && cfg->dim != 3) return fail(KFVM_ERR_ARG, "dim must be 2 or 3");
-  if (!(cfg->nq == 2 || (cfg->nq == 3 && (cfg->dim == 2 || cfg->eq == KFVM_EQ_HYDRO ||
-                                            cfg->eq == KFVM_EQ_NAVIERSTOKES))))
-    return fail(KFVM_ERR_ARG, "the GPU path supports NUM_QUAD_PTS = 2, and 3 in 2D and for 3D Euler / Navier-Stokes");
+  if (!(cfg->nq == 2 || (cfg->nq == 3 && (cfg->dim == 2 || cfg->eq != KFVM_EQ_SRHYDRO))))
+    return fail(KFVM_ERR_ARG, "the GPU path supports NUM_QUAD_PTS = 2, and 3 in 2D and for 3D Euler / Navier-Stokes / GLM-MHD");
   if (cfg->eq < KFVM_EQ_HYDRO || cfg->eq > KFVM_EQ_SRHYDRO) return fail(KFVM_ERR_ARG, "unknown equation type");
   if (cfg->rs < 0 || cfg->rs > 2) return fail(KFVM_ERR_ARG, "unknown Riemann solver");
   if (cfg->eq == KFVM_EQ_MHD_GLM && cfg->rs == KFVM_RS_HLLC)
@@ -981,7 +980,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
       if (cfg->eq == KFVM_EQ_MHD_GLM)
         for (int q = 0; q < hS.w.nqc; q++) hS.lin[c * nrows + r++] = hS.w.cell_w[0][q][c];
     }
-    fill_tc_weights(hS, cfg->dim, nrows);
+    if (cfg->nq == 2) fill_tc_weights(hS, cfg->dim, nrows);  // the tensor-core form takes 2 points only
     fill_dmma_weights(hS, nrows);
   }
 

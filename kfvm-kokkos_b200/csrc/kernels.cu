@@ -112,7 +112,8 @@ struct DmmaShape {
   static constexpr int NK = (Cfg<DIM, EQ, NQ>::C - 1) / 4;
   static constexpr int BSIZE = NK * NT * 32;
   static_assert((Cfg<DIM, EQ, NQ>::C - 1) % 4 == 0, "stencil of 4m + 1 cells");
-  static_assert(BSIZE <= kDmmaMaxB, "B fragment table too small");
+  // more than 7 row tiles (81 rows) go to recon_rows_kernel, not to the DMMA kernels
+  static_assert(BSIZE <= kDmmaMaxB || NT > 7, "B fragment table too small");
 };
 
 __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
@@ -523,6 +524,141 @@ int recon_dmma_state_map(CUtensorMap *map, const double *U, const Grid &g, int d
   return encode_tensor_map_8b(map, U, 4, dims, strides, box);
 }
 
+// Linear reconstruction for more rows than the DMMA kernels hold in registers
+// (3D GLM-MHD with three Gauss points: 54 face points and 27 interior points per
+// cell).  One thread per (cell, variable) sums its rows in passes, in stencil-cell
+// order as KernelLinearRecon_K does (Stencil_K.H:56-119); the face points are
+// staged in shared memory and finished per cell by the cell's NV threads (limiter
+// pre-check, indicator, GLM speed maxima), the interior points go to the source
+// array.  The limiter bounds come from pos_bounds and are stored for the heavy pass.
+template <int DIM, int EQ, int NQ>
+struct RowsShape {
+  using T = Cfg<DIM, EQ, NQ>;
+  static constexpr int NR = LinRows<DIM, EQ, NQ>::NROWS;
+  static constexpr int NFQ = T::NF * T::NQF;
+  static constexpr int CELLS = 16;
+  static constexpr int RCH = 27;  // rows per pass
+  static constexpr size_t BYTES =
+      (size_t)(T::C * NR + CELLS * NFQ * T::NV + 3 * CELLS + 3 * T::NV * CELLS) * sizeof(double);
+};
+
+template <int DIM, int EQ, int NQ>
+__global__ void __launch_bounds__(RowsShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV)
+    recon_rows_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S, int wantInd,
+                      double *__restrict__ F0, double *__restrict__ F1, double *__restrict__ F2,
+                      float *__restrict__ W0, float *__restrict__ W1, float *__restrict__ W2,
+                      double *__restrict__ src, uint8_t *__restrict__ status, double2 *__restrict__ lamvel,
+                      double *__restrict__ bnd) {
+  using T = Cfg<DIM, EQ, NQ>;
+  using R = RowsShape<DIM, EQ, NQ>;
+  using E = Eos<EQ>;
+  constexpr int NV = T::NV, NR = R::NR, NFQ = R::NFQ, C = T::C, NQF = T::NQF;
+  extern __shared__ __align__(16) double rsm[];
+  double *sW = rsm;                        // [stencil cell][row]
+  double *sS = sW + C * NR;                // face states [cell][face row][v]
+  double *sBd = sS + R::CELLS * NFQ * NV;  // [minDens | maxDens | minEint][cell]
+  double *sRed = sBd + 3 * R::CELLS;       // [inside | lam | vel][v][cell]
+  const int x = threadIdx.x, v = threadIdx.y, tid = v * R::CELLS + x, nt = R::CELLS * NV;
+  for (int t = tid; t < C * NR; t += nt) sW[t] = S->lin[t];
+  const int64_t c = blockIdx.x * (int64_t)R::CELLS + x;
+  const bool live = c < g.n;
+  const int64_t i = live ? c % g.nx : 0, j = live ? (c / g.nx) % g.ny : 0, k = live ? c / (g.nx * g.ny) : 0;
+  const double *Uc = U + pidx(g, i, j, k);
+  if (v == 0 && live) {
+    const PosBounds bd = pos_bounds<DIM, EQ>(Uc, g);
+    sBd[x] = bd.minDens;
+    sBd[R::CELLS + x] = bd.maxDens;
+    sBd[2 * R::CELLS + x] = bd.minEint;
+    bnd[c] = bd.minDens;
+    bnd[g.n + c] = bd.maxDens;
+    bnd[2 * g.n + c] = bd.minEint;
+  }
+  __syncthreads();
+  if (live) {
+    double u[C];
+#pragma unroll
+    for (int q = 0; q < C; q++) u[q] = Uc[v * g.pvol + g.loff[q]];
+#pragma unroll 1
+    for (int r0 = 0; r0 < NR; r0 += R::RCH) {
+      double acc[R::RCH];
+#pragma unroll
+      for (int r = 0; r < R::RCH; r++) acc[r] = 0.0;
+#pragma unroll
+      for (int q = 0; q < C; q++) {
+        const double uq = u[q];
+#pragma unroll
+        for (int r = 0; r < R::RCH; r++)
+          if (r0 + r < NR) acc[r] = fma(sW[q * NR + r0 + r], uq, acc[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < R::RCH; r++) {
+        const int row = r0 + r;
+        if (row < NFQ) sS[(x * NFQ + row) * NV + v] = acc[r];
+        else if (row < NR) src[((int64_t)(row - NFQ) * NV + v) * g.n + c] = acc[r];
+      }
+    }
+  }
+  __syncthreads();
+  // the cell's face rows shared among its NV threads (rows v, v + NV, ...)
+  bool inside = true;
+  double lam = 0.0, vel = 0.0;
+  if (live) {
+    PosBounds bd;
+    bd.rDens = Uc[DENS * g.pvol];
+    bd.minDens = sBd[x];
+    bd.maxDens = sBd[R::CELLS + x];
+    bd.minEint = sBd[2 * R::CELLS + x];
+    double *const F[3] = {F0, F1, F2};
+    float *const W[3] = {W0, W1, W2};
+    for (int row = v; row < NFQ; row += NV) {
+      double st[NV];
+#pragma unroll
+      for (int w = 0; w < NV; w++) st[w] = sS[(x * NFQ + row) * NV + w];
+      double ei = 0.0;
+      if constexpr (EQ == EQ_SR) {
+        inside = inside && pos_inside<EQ>(bd, st);
+      } else {
+        ei = E::eint(st);
+        inside = inside && st[DENS] > bd.minDens && st[DENS] < bd.maxDens && ei > bd.minEint;
+      }
+      const int f = row / NQF, q = row % NQF, d = f >> 1, hi = f & 1;
+      const int64_t nf = g.nface[d];
+      const int64_t fidx = ((k + (d == 2 && hi)) * g.fdim[d][1] + (j + (d == 1 && hi))) * g.fdim[d][0] +
+                           (i + (d == 0 && hi));
+      const int slot = hi ? 0 : 1;
+#pragma unroll
+      for (int w = 0; w < NV; w++) F[d][((int64_t)(slot * NQF + q) * NV + w) * nf + fidx] = st[w];
+      if (wantInd)
+        W[d][(int64_t)(slot * NQF + q) * nf + fidx] =
+            EQ == EQ_SR ? __double2float_rn(st[DENS])
+                        : E::template weno_store<DIM>(g.gamma, st[DENS], (g.gamma - 1.0) * ei);
+      if constexpr (T::SRC) {
+        // SpeedEstimate_K<MHD_GLM> (MHD_GLM_K.H:213-310): x components on every face
+        const double vv = fabs(st[MOMX] / st[DENS]);
+        const double l = E::fastMagSonic(g.gamma, st, st[MAGX]) + vv;
+        vel = vv > vel ? vv : vel;
+        lam = l > lam ? l : lam;
+      }
+    }
+  }
+  sRed[v * R::CELLS + x] = inside ? 1.0 : 0.0;
+  sRed[(NV + v) * R::CELLS + x] = lam;
+  sRed[(2 * NV + v) * R::CELLS + x] = vel;
+  __syncthreads();
+  if (v == 0 && live) {
+    bool all = true;
+    double l = 0.0, vv = 0.0;
+#pragma unroll
+    for (int w = 0; w < NV; w++) {
+      all = all && sRed[w * R::CELLS + x] != 0.0;
+      l = fmax(l, sRed[(NV + w) * R::CELLS + x]);
+      vv = fmax(vv, sRed[(2 * NV + w) * R::CELLS + x]);
+    }
+    status[c] = all ? 1 : 0;
+    if constexpr (T::SRC) lamvel[c] = make_double2(l, vv);
+  }
+}
+
 // PositivityPreserve_K bounds of every cell (Common_K.H:331-380; SR: SRHydro_K.H:224-246)
 // from a per-block footprint tile: [minDens | maxDens | minEint][cell], the same
 // values recon_kernel computes in its own prologue.  The pre-pass of the tensor-core
@@ -761,7 +897,9 @@ struct HeavyShape {
   static constexpr int DER = NIP * NSUM;                      // derivative weights [s][p][i]
   static constexpr int NRP = (NR + 1) & ~1;                  // rows padded to pairs
   static constexpr int FW = NRP * NSUM;                       // reconstruction weights [s][p][row]
-  static constexpr int CELLS = 32;
+  // cells per block (one thread per cell and variable); 16 where 32 cells' rows
+  // would not fit in shared memory (3D GLM-MHD with three points: 81 rows x 9)
+  static constexpr int CELLS = NR * T::NV > 400 ? 16 : 32;
   static constexpr size_t BYTES = (size_t)(DER + FW + CELLS * NR * T::NV + CELLS * 2 + CELLS * T::NV) * sizeof(double) +
                                   (size_t)T::NB * T::CB * sizeof(int);
   __host__ __device__ static constexpr int n(int s) { return s == 0 ? T::C : (s == 1 ? T::CC : T::CB); }
@@ -771,7 +909,7 @@ struct HeavyShape {
 };
 
 template <int DIM, int EQ, int NQ>
-__global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
+__global__ void __launch_bounds__(HeavyShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
     heavy_var_kernel(const double *__restrict__ U, Grid g, const DevStencil *__restrict__ S,
                      double *__restrict__ theta, double *__restrict__ F0, double *__restrict__ F1,
                      double *__restrict__ F2, double *__restrict__ src, const uint32_t *__restrict__ heavy,
@@ -788,7 +926,7 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
   double *sTh = sDep + H::CELLS * 2;        // limiter theta of each thread's rows [v][cell]
   int *sSub = reinterpret_cast<int *>(sTh + H::CELLS * NV);
   const kfvm_stencil &st = S->w;
-  const int tid = threadIdx.y * 32 + threadIdx.x, nt = 32 * NV;
+  const int tid = threadIdx.y * H::CELLS + threadIdx.x, nt = H::CELLS * NV;
   // weights transposed so that the rows of one stencil value are adjacent and
   // load as 16-byte pairs
   for (int t = tid; t < H::DER; t += nt) {
@@ -1098,13 +1236,11 @@ __global__ void __launch_bounds__(32 * Eos<EQ>::NV, Eos<EQ>::NV > 5 ? 1 : 2)
     __syncthreads();
   }
   if constexpr (T::SRC) {
-    // every variable thread holds the maxima of its share of the face rows
-    lam = warp_max(lam);
-    vel = warp_max(vel);
-    if (threadIdx.x == 0) {
-      atomic_max_pos(&sc->glm_lam_bits, lam);
-      atomic_max_pos(&sc->glm_vel_bits, vel);
-    }
+    // every variable thread holds the maxima of its share of the face rows; each
+    // offers them itself (a block of 16 cells x 9 variables ends in a half warp,
+    // so no warp shuffle here; the read-before-atomic skips all but the raising ones)
+    atomic_max_pos(&sc->glm_lam_bits, lam);
+    atomic_max_pos(&sc->glm_vel_bits, vel);
   }
 }
 
@@ -1693,6 +1829,16 @@ struct Launch {
   static cudaError_t recon(const double *U, const CUtensorMap *umap, const Grid &g, const DevStencil *S,
                            int wantInd, double *const *F, float *const *W, double *src, uint8_t *status,
                            double2 *lamvel, double *bnd, DevScalars *sc, cudaStream_t s) {
+    if constexpr (DmmaShape<DIM, EQ, NQ>::NT > 7) {
+      // more rows than the DMMA kernels hold (3D GLM-MHD, three points)
+      using R = RowsShape<DIM, EQ, NQ>;
+      static const cudaError_t attrR = cudaFuncSetAttribute(
+          recon_rows_kernel<DIM, EQ, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R::BYTES);
+      if (attrR != cudaSuccess) return attrR;
+      recon_rows_kernel<DIM, EQ, NQ><<<(unsigned)((g.n + R::CELLS - 1) / R::CELLS), dim3(R::CELLS, NV), R::BYTES, s>>>(
+          U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd);
+      return cudaGetLastError();
+    } else {
     // (3D with three Gauss points keeps the global-load kernel: its 54 rows need
     // more accumulator registers than two 256-thread blocks per SM leave; so does
     // GLM-MHD in 3D, whose nine halo tiles would not leave room for two blocks, and
@@ -1715,6 +1861,7 @@ struct Launch {
     recon_kernel<DIM, EQ, NQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(
         U, g, S, wantInd, F[0], F[1], F[2], W[0], W[1], W[2], src, status, lamvel, bnd);
     return cudaGetLastError();
+    }
   }
   static cudaError_t flag(const double *U, const Grid &g, float *const *W, double *const *F,
                           const double *theta, uint8_t *flag, DevScalars *sc, double thr, cudaStream_t s) {
@@ -1737,7 +1884,7 @@ struct Launch {
     static const cudaError_t attr = cudaFuncSetAttribute(
         heavy_var_kernel<DIM, EQ, NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HeavyShape<DIM, EQ, NQ>::BYTES);
     if (attr != cudaSuccess) return attr;
-    heavy_var_kernel<DIM, EQ, NQ><<<heavy_blocks, dim3(32, NV), HeavyShape<DIM, EQ, NQ>::BYTES, s>>>(
+    heavy_var_kernel<DIM, EQ, NQ><<<heavy_blocks, dim3(HeavyShape<DIM, EQ, NQ>::CELLS, NV), HeavyShape<DIM, EQ, NQ>::BYTES, s>>>(
         U, g, S, theta, F[0], F[1], F[2], src, heavy, bnd, sc, jd);
     return cudaGetLastError();
   }
@@ -1789,6 +1936,7 @@ void fill_dmma_weights(DevStencil &S, int nrows) {
   // all stencil cells but the last (added in the kernel's epilogue)
   const int C = S.w.n_cells - 1, nt = (nrows + 7) / 8, nk = (C + 3) / 4;
   std::memset(S.dmma_b, 0, sizeof(S.dmma_b));
+  if (nk * nt * 32 > kDmmaMaxB) return;  // more rows than the DMMA kernels take (they are not used)
   for (int ks = 0; ks < nk; ks++)
     for (int t = 0; t < nt; t++)
       for (int l = 0; l < 32; l++) {
@@ -1803,8 +1951,8 @@ int64_t stage_blocks(const Grid &g) {
 }
 
 // one instantiation per (dimension, equations, Gauss points): 2 points for both
-// dimensions, 3 points for 2D and for 3D Euler / Navier-Stokes (3D GLM-MHD with 3
-// points would need 81 rows per cell); the grid's nq selects
+// dimensions, 3 points for 2D and for 3D Euler / Navier-Stokes / GLM-MHD (not SR);
+// the grid's nq selects
 #define KFVM_DISPATCH(DIM_, EQ_, CALL)                                                  \
   do {                                                                                \
     if (g.nq == 2) {                                                                  \
@@ -1824,6 +1972,7 @@ int64_t stage_blocks(const Grid &g) {
     } else if (g.nq == 3 && (DIM_) == 3) {                                            \
       if ((EQ_) == EQ_HYDRO) return Launch<3, EQ_HYDRO, 3>::CALL;                     \
       if ((EQ_) == EQ_NS) return Launch<3, EQ_NS, 3>::CALL;                           \
+      if ((EQ_) == EQ_GLM) return Launch<3, EQ_GLM, 3>::CALL;                         \
     }                                                                                 \
     return cudaErrorInvalidValue;                                                     \
   } while (0)

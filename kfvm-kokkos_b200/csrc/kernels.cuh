@@ -63,7 +63,7 @@ __host__ __device__ inline bool outer_in_face(int bc) { return bc == KFVM_BC_EXC
 // stencil on the device: weights plus linear offsets in the padded array, and the
 // full-stencil linear weights packed as [cell][row] (rows: face points f*NQF+q, then
 // interior points q) for the light reconstruction pass
-constexpr int kMaxLinRows = 6 * 9; // 3D, 3 Gauss points: 6 faces x 9 points
+constexpr int kMaxLinRows = 6 * 9 + 27; // 3D, 3 Gauss points: 6 faces x 9 points (+ 27 interior, GLM-MHD)
 // The same weights for the tensor-core form: W = hi + lo, both TF32 values in FP32
 // containers, stored as the tcgen05 B operand (K-major, no swizzle): K = stencil
 // cells padded to 40, N = rows padded to 32, [cell/4][row][cell%4].

@@ -139,6 +139,8 @@ PROBLEMS = {
     "taylor_green": (3, "NavierStokes", "HLLC", "SSP4_3_2", 2, "periodic", False, IC_TGV),
     "orszag_tang": (2, "MHD_GLM", "HLL", "SSP4_3_2", 2, "periodic", True, IC_OT),
     "orszag_tang_3d": (3, "MHD_GLM", "HLL", "SSP4_3_2", 2, "periodic", True, IC_OT),
+    # three Gauss points (NUM_QUAD_PTS 3, as MHD/MagVort3d): 27 interior source points
+    "orszag_tang_3d_q3": (3, "MHD_GLM", "HLL", "SSP4_3_2", 3, "periodic", True, IC_OT),
 }
 
 

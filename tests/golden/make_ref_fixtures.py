@@ -26,39 +26,43 @@ import build_ref  # noqa: E402
 import kfvm_abi as abi  # noqa: E402
 import refrun  # noqa: E402
 
-# (case, workload, grid per axis, accepted steps, wenothresh override or None)
+# (case, workload, grid per axis, accepted steps, wenothresh override or None,
+#  Gauss points, reference problem build)
 CASES = [
-    ("vortex_128_c1", "isentropic_vortex", 128, 20, None),     # the problem list's C1, as stated
-    ("sod3d_24", "sod3d", 24, 5, None),
-    ("sod3d_16_fullweno", "sod3d", 16, 3, -1.0),               # wenothresh < 0: WENO everywhere
-    ("kelvin_helmholtz_64", "kelvin_helmholtz", 64, 10, None),
-    ("taylor_green_16", "taylor_green", 16, 4, None),
-    ("orszag_tang_64", "orszag_tang", 64, 10, None),
-    ("orszag_tang_3d_16", "orszag_tang_3d", 16, 3, None),     # 3D GLM-MHD sources at Q^3 points
+    ("vortex_128_c1", "isentropic_vortex", 128, 20, None, 2, None),   # the problem list's C1, as stated
+    ("sod3d_24", "sod3d", 24, 5, None, 2, None),
+    ("sod3d_16_fullweno", "sod3d", 16, 3, -1.0, 2, None),             # wenothresh < 0: WENO everywhere
+    ("kelvin_helmholtz_64", "kelvin_helmholtz", 64, 10, None, 2, None),
+    ("taylor_green_16", "taylor_green", 16, 4, None, 2, None),
+    ("orszag_tang_64", "orszag_tang", 64, 10, None, 2, None),
+    ("orszag_tang_3d_16", "orszag_tang_3d", 16, 3, None, 2, None),   # 3D GLM-MHD sources at Q^3 points
+    ("orszag_tang_3d_q3_12", "orszag_tang_3d", 12, 2, None, 3, "orszag_tang_3d_q3"),  # three points
 ]
 
 
-def case_config(workload, scale, steps, thresh):
+def case_config(workload, scale, steps, thresh, nq=2):
     cfg, ic = abi.workload(workload, scale=scale, steps=steps)
     if thresh is not None:
         cfg.weno_thresh = abi.stof(thresh)
         cfg.indicator = abi.KFVM_IND_ALL if thresh < 0 else abi.KFVM_IND_KXRCF
+    cfg.nq = nq
     return cfg, ic
 
 
 def main():
-    if len(sys.argv) != 2:
-        sys.exit("usage: make_ref_fixtures.py <path of the reference checkout>")
-    build_ref.build_all(sys.argv[1], sorted({c[1] for c in CASES}))
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_ref_fixtures.py <path of the reference checkout> [case ...]")
+    cases = [c for c in CASES if len(sys.argv) == 2 or c[0] in sys.argv[2:]]
+    build_ref.build_all(sys.argv[1], sorted({c[6] or c[1] for c in cases}))
     out = os.path.join(HERE, "ref")
     os.makedirs(out, exist_ok=True)
-    for case, workload, scale, steps, thresh in CASES:
-        cfg, ic = case_config(workload, scale, steps, thresh)
-        cks, _ = refrun.run(workload, cfg, steps)
+    for case, workload, scale, steps, thresh, nq, problem in cases:
+        cfg, ic = case_config(workload, scale, steps, thresh, nq)
+        cks, _ = refrun.run(problem or workload, cfg, steps)
         assert len(cks) == steps + 1, (case, len(cks))
         np.savez_compressed(
             os.path.join(out, case + ".npz"),
-            workload=workload, scale=scale, steps=steps,
+            workload=workload, scale=scale, steps=steps, nq=nq,
             weno_thresh=np.nan if thresh is None else thresh,
             times=np.array([c[1] for c in cks]), dts=np.array([c[2] for c in cks]),
             weno_counts=np.array([int((c[4][0] > 0).sum()) for c in cks]),

@@ -23,6 +23,8 @@ def load(path):
 def config(fx):
     """The configuration a fixture was made with (workload, grid, steps, indicator)."""
     cfg, ic = abi.workload(str(fx["workload"]), scale=int(fx["scale"]), steps=int(fx["steps"]))
+    if "nq" in fx:
+        cfg.nq = int(fx["nq"])
     th = float(fx["weno_thresh"])
     if not np.isnan(th):
         cfg.weno_thresh = abi.stof(th)

@@ -182,6 +182,9 @@ Q3_CASES = [
     # 3D with 3 points (54 reconstruction rows per cell; Euler / Navier-Stokes)
     ("sod3d", 12, 3),
     ("taylor_green", 10, 2),
+    # 3D GLM-MHD with 3 points: 81 rows (27 interior source points), the row-pass
+    # reconstruction and a heavy pass of 16 cells per block
+    ("orszag_tang_3d", 16, 3),
 ]
 
 
