@@ -28,11 +28,15 @@ CASES = [
 
 def rel_l1(a, b):
     """Relative L1 error per variable.  A variable whose reference L1 norm is below
-    1e-8 of the mean norm over all variables (e.g. an analytically zero RHS, or psi
-    starting at zero) is measured against that mean norm instead of its own."""
+    1e-4 of the mean norm over all variables is measured against 1e-4 of that mean
+    instead of its own norm: such a value is a near cancellation (the density RHS of
+    a divergence-free velocity field is 2e-5 of the mean in the 3D Orszag-Tang
+    problem, the psi RHS of a divergence-free magnetic field 8e-6, an analytically
+    zero RHS or psi starting at zero 0), whose own norm would magnify the rounding
+    of the flux differences it is made of."""
     den = np.abs(b).sum(axis=-1)
     mean = max(den.mean(), 1e-300)
-    den = np.where(den < 1e-8 * mean, mean, den)
+    den = np.maximum(den, 1e-4 * mean)
     num = np.abs(a - b).sum(axis=-1)
     return num / den
 
