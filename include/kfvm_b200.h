@@ -116,7 +116,7 @@ typedef struct kfvm_config {
   int32_t eq;         /* enum kfvm_eq                                        */
   int32_t rs;         /* enum kfvm_rs                                        */
   int32_t rk;         /* enum kfvm_rk                                        */
-  int32_t nq;         /* NUM_QUAD_PTS: 2, or 3 (2D; 3D Euler/Navier-Stokes)  */
+  int32_t nq;         /* NUM_QUAD_PTS: 2, or 3 (not for SRHydro in 3D)      */
   int32_t indicator;  /* enum kfvm_indicator                                 */
   int64_t nx, ny, nz; /* interior cells (nz = 1 in 2D)                       */
   double xlo, xup, ylo, yup, zlo, zup;
