@@ -1266,12 +1266,15 @@ __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
   constexpr int NV = T::NV, NQF = T::NQF;
   __shared__ double part[NQF][NV][32];
   const int64_t fx = g.fdim[D][0], fy = g.fdim[D][1], nf = g.nface[D];
-  const int64_t i = blockIdx.x * (int64_t)32 + threadIdx.x;
-  const int64_t j = blockIdx.y;
+  // the face within its (x, y) plane, split with 32-bit arithmetic (a plane holds
+  // far fewer than 2^32 faces)
+  const unsigned flat = blockIdx.x * 32u + threadIdx.x, ux = (unsigned)fx;
+  const unsigned jj = flat / ux;
+  const int64_t i = (int64_t)(flat - jj * ux), j = jj;
   const int64_t k = blockIdx.z;
   const int q = threadIdx.y;
   double vmax = 0.0;
-  const bool live = i < fx;
+  const bool live = j < fy;
   bool same = false;
   if (live) {
     const int64_t fidx = (k * fy + j) * fx + i;
@@ -1324,7 +1327,7 @@ __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
     for (int v = 0; v < NV; v++) part[q][v][threadIdx.x] = wq * Fq[v];
   }
   __shared__ unsigned cnt[2];
-  const bool sampled = SAME && (blockIdx.x + 5u * blockIdx.y + 11u * blockIdx.z) % kSameSample == 0;
+  const bool sampled = SAME && (blockIdx.x + 11u * blockIdx.z) % kSameSample == 0;
   if (sampled && threadIdx.x == 0 && q == 0) cnt[0] = cnt[1] = 0u;
   __syncthreads();
   if (sampled) {
@@ -1892,8 +1895,10 @@ struct Launch {
   static void riemann_dirs(double *const *F, double *const *G, const Grid &g, DevScalars *sc, cudaStream_t s) {
 #pragma unroll 1
     for (int d = 0; d < DIM; d++) {
-      // one block row of 32 faces per (j, k), NQF points along threadIdx.y
-      const dim3 grid((unsigned)((g.fdim[d][0] + 31) / 32), (unsigned)g.fdim[d][1], (unsigned)g.fdim[d][2]);
+      // 32 consecutive faces of an (x, y) face plane per block (rows of the x faces
+      // hold nx + 1 faces, which would leave a nearly empty block per row), NQF
+      // points along threadIdx.y
+      const dim3 grid((unsigned)((g.fdim[d][0] * g.fdim[d][1] + 31) / 32), 1u, (unsigned)g.fdim[d][2]);
       const dim3 blk(32, Cfg<DIM, EQ, NQ>::NQF);
       if (d == 0) riemann_kernel<DIM, EQ, 0, NQ, SAME><<<grid, blk, 0, s>>>(F[0], G[0], g, sc);
       if (d == 1) riemann_kernel<DIM, EQ, 1, NQ, SAME><<<grid, blk, 0, s>>>(F[1], G[1], g, sc);
