@@ -462,9 +462,10 @@ __global__ void __launch_bounds__(DmmaTile<DIM>::THREADS, 2)
     if constexpr (EQ == EQ_SR) {
       bd = PosBounds{sU[DENS * D::N + ht(0, 0, 0)], minDens, maxDens, minEint};
     } else {
+      // velocities as m / rho, as the reference's divergence estimate (Common_K.H:363-378)
       auto vel = [&](int m, int xo, int yo, int zo) {
         const int h = ht(xo, yo, zo);
-        return sU[m * D::N + h] * (1.0 / sU[DENS * D::N + h]);
+        return sU[m * D::N + h] / sU[DENS * D::N + h];
       };
       const double dxU = vel(MOMX, 1, 0, 0) - vel(MOMX, -1, 0, 0);
       const double dyV = vel(MOMY, 0, 1, 0) - vel(MOMY, 0, -1, 0);
@@ -1258,7 +1259,9 @@ constexpr int kSameSample = 1024;
 
 template <int DIM, int EQ, int D, int NQ, bool SAME>
 __global__ void __launch_bounds__(32 * Cfg<DIM, EQ, NQ>::NQF,
-                                  EQ == EQ_GLM ? 1 : (EQ == EQ_SR ? (DIM == 2 ? 8 : 4) : (DIM == 2 ? 16 : 8)))
+                                  EQ == EQ_GLM ? 1
+                                               : (EQ == EQ_SR ? (DIM == 2 ? 8 : 4)
+                                                              : (DIM == 2 ? 16 : (NQ == 3 ? 7 : 8))))
     riemann_kernel(const double *__restrict__ F, double *__restrict__ G, Grid g,
                    DevScalars *__restrict__ sc) {
   using T = Cfg<DIM, EQ, NQ>;

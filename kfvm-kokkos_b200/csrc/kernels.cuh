@@ -285,7 +285,7 @@ __device__ __forceinline__ PosBounds pos_bounds(const double *__restrict__ Uc, c
           minEint = fmin(minEint, sr::ediff(s));
         }
     return PosBounds{Uc[DENS * g.pvol], minDens, maxDens, minEint};
-  }
+  } else {
 #pragma unroll
   for (int xo = -1; xo <= 1; xo++)
 #pragma unroll
@@ -317,6 +317,7 @@ __device__ __forceinline__ PosBounds pos_bounds(const double *__restrict__ Uc, c
   b.minDens = minDens * (1.0 - kappa);
   b.minEint = minEint * (1.0 - kappa);
   return b;
+  }
 }
 
 // true when a state leaves theta at 1 in both passes of the limiter

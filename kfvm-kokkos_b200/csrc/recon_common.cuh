@@ -63,9 +63,11 @@ __device__ __forceinline__ void pos_tile_fill(const double *__restrict__ U, cons
     sm[0][t] = st[DENS];
     sm[1][t] = ei;
     sm[2][t] = sqrt(g.gamma * ((g.gamma - 1.0) * ei) * ir);
-    sm[3][t] = st[MOMX] * ir;
-    sm[4][t] = st[MOMY] * ir;
-    sm[5][t] = st[MOMZ] * ir;
+    // velocities as the reference's divergence estimate takes them (m / rho,
+    // Common_K.H:363-378)
+    sm[3][t] = st[MOMX] / st[DENS];
+    sm[4][t] = st[MOMY] / st[DENS];
+    sm[5][t] = st[MOMZ] / st[DENS];
   }
 }
 
@@ -91,7 +93,7 @@ __device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<
           minEint = fmin(minEint, sm[1][t]);
         }
     return PosBounds{sm[0][at(0, 0, 0)], minDens, maxDens, minEint};
-  }
+  } else {
 #pragma unroll
   for (int xo = -1; xo <= 1; xo++)
 #pragma unroll
@@ -117,6 +119,7 @@ __device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<
   b.minDens = minDens * (1.0 - kappa);
   b.minEint = minEint * (1.0 - kappa);
   return b;
+  }
 }
 
 } // namespace kfvm
