@@ -371,7 +371,7 @@ struct DmmaTmaSmem {
 };
 
 template <int DIM, int EQ, int NQ>
-__global__ void __launch_bounds__(DmmaTile<DIM>::THREADS, 2)
+__global__ void __launch_bounds__(DmmaTile<DIM>::THREADS, (DIM == 2 && NQ == 2 && Eos<EQ>::NV == 5) ? 4 : 2)
     recon_tma_kernel(const __grid_constant__ CUtensorMap umap, Grid g, const DevStencil *__restrict__ S, int wantInd,
                      double *__restrict__ F0, double *__restrict__ F1, double *__restrict__ F2,
                      float *__restrict__ W0, float *__restrict__ W1, float *__restrict__ W2,
