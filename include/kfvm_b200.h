@@ -49,17 +49,18 @@ enum kfvm_rk {
  * no-slip wall negates every momentum component (and the normal magnetic field),
  * with the coefficient tables of src/physics/<eq>/<Eq>_BCCoeffs.H. */
 enum kfvm_bc {
+  /* the values of the reference's BCType (src/Types.H:40), user included */
   KFVM_BC_PERIODIC = 0, KFVM_BC_OUTFLOW = 1, KFVM_BC_REFLECTING = 2, KFVM_BC_NOSLIP = 3,
-  /* a block face shared with another rank of a decomposed domain (the faces the
-   * reference's LayoutMPI gives an MPI neighbour, src/LayoutMPI.H:44-97): its
-   * halo cells and outer face states come from that rank through the exchange
-   * callbacks of kfvm_set_exchange */
-  KFVM_BC_EXCHANGE = 4,
   /* a face whose halo cells and outer face states a user function supplies
    * (BCType::user: the CellWest..CellTop and FaceWest..FaceTop functions of a
    * problem's UserBCs.H, src/BoundaryConditions_K.H:96-128, 569-615), through
    * the callback of kfvm_set_user_bc */
-  KFVM_BC_USER = 5
+  KFVM_BC_USER = 4,
+  /* a block face shared with another rank of a decomposed domain (the faces the
+   * reference's LayoutMPI gives an MPI neighbour, src/LayoutMPI.H:44-97): its
+   * halo cells and outer face states come from that rank through the exchange
+   * callbacks of kfvm_set_exchange */
+  KFVM_BC_EXCHANGE = 5
 };
 /* src/Types.H:40 */
 enum kfvm_ts_status { KFVM_TS_ACCEPTED = 0, KFVM_TS_TOLERANCE = 1, KFVM_TS_UNPHYSICAL = 2 };

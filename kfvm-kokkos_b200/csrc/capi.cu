@@ -904,7 +904,7 @@ int kfvm_create(const kfvm_config *cfg, kfvm_solver **out) {
     if ((cfg->bc[2 * d] == KFVM_BC_PERIODIC) != (cfg->bc[2 * d + 1] == KFVM_BC_PERIODIC))
       return fail(KFVM_ERR_ARG, "periodic boundaries must come in pairs");
     for (int f = 2 * d; f < 2 * d + 2; f++)
-      if (cfg->bc[f] < KFVM_BC_PERIODIC || cfg->bc[f] > KFVM_BC_USER)
+      if (cfg->bc[f] < KFVM_BC_PERIODIC || cfg->bc[f] > KFVM_BC_EXCHANGE)
         return fail(KFVM_ERR_ARG, "unknown boundary condition (periodic, outflow, reflecting, noslip, exchange, user)");
   }
   for (int d = 0; d < 3; d++)

@@ -11,7 +11,7 @@ import struct
 KFVM_EQ_HYDRO, KFVM_EQ_NAVIERSTOKES, KFVM_EQ_MHD_GLM, KFVM_EQ_SRHYDRO = 0, 1, 2, 3
 KFVM_RS_LLF, KFVM_RS_HLL, KFVM_RS_HLLC = 0, 1, 2
 KFVM_RK_THREESTARP, KFVM_RK_FOURSTARP, KFVM_RK_SSP4_3_2, KFVM_RK_SSP10_4_3 = 0, 1, 2, 3
-KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW, KFVM_BC_REFLECTING, KFVM_BC_NOSLIP, KFVM_BC_EXCHANGE, KFVM_BC_USER = 0, 1, 2, 3, 4, 5
+KFVM_BC_PERIODIC, KFVM_BC_OUTFLOW, KFVM_BC_REFLECTING, KFVM_BC_NOSLIP, KFVM_BC_USER, KFVM_BC_EXCHANGE = 0, 1, 2, 3, 4, 5
 KFVM_USER_CELLS, KFVM_USER_FACES = 0, 1
 KFVM_REDUCE_SUM, KFVM_REDUCE_MAX, KFVM_REDUCE_MIN = 0, 1, 2
 KFVM_TS_ACCEPTED, KFVM_TS_TOLERANCE, KFVM_TS_UNPHYSICAL = 0, 1, 2

@@ -62,8 +62,10 @@ def test_default_config(product_lib):
 @pytest.mark.parametrize("mutate,msg", [
     (lambda c: setattr(c, "dim", 4), "dim"),
     (lambda c: setattr(c, "nq", 4), "NUM_QUAD_PTS"),
-    (lambda c: (setattr(c, "dim", 3), setattr(c, "nz", 16), setattr(c, "nq", 3), setattr(c, "eq", abi.KFVM_EQ_MHD_GLM),
-                setattr(c, "rs", abi.KFVM_RS_HLL), setattr(c, "have_sources", 1)), "NUM_QUAD_PTS"),
+    # three points in 3D for every system but SR
+    (lambda c: (setattr(c, "dim", 3), setattr(c, "nz", 16), setattr(c, "nq", 3), setattr(c, "eq", abi.KFVM_EQ_SRHYDRO),
+                setattr(c, "rs", abi.KFVM_RS_HLL)), "NUM_QUAD_PTS"),
+    (lambda c: (c.bc.__setitem__(0, 6), c.bc.__setitem__(1, 6)), "unknown boundary"),
     (lambda c: (setattr(c, "eq", abi.KFVM_EQ_MHD_GLM), setattr(c, "rs", abi.KFVM_RS_HLLC)), "HLLC"),
     (lambda c: (setattr(c, "eq", abi.KFVM_EQ_SRHYDRO), setattr(c, "rs", abi.KFVM_RS_HLLC)), "HLL and LLF"),
     (lambda c: (setattr(c, "eq", abi.KFVM_EQ_SRHYDRO), setattr(c, "rs", abi.KFVM_RS_HLL),
