@@ -735,7 +735,7 @@ __device__ __forceinline__ void kxrcf_face(const Grid &g, int fc, int64_t i, int
 }
 
 template <int DIM, int EQ, int NQ>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 8)
     flag_kernel(const double *__restrict__ U, Grid g, const float *__restrict__ W0,
                 const float *__restrict__ W1, const float *__restrict__ W2,
                 const double *__restrict__ F0, const double *__restrict__ F1,
