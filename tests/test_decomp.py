@@ -54,9 +54,23 @@ def block_slice(full, cfg, c):
     return u[:, z0:z0 + bz, y0:y0 + c.ny, x0:x0 + c.nx].reshape(nv, -1)
 
 
-def one_domain(oracle, name, scale, steps):
-    cfg, ic = abi.workload(name, scale=scale, steps=steps)
+def workload(name, scale, steps):
+    """abi.workload, plus the three-point variant of the 3D Orszag-Tang problem."""
+    if name == "orszag_tang_3d_q3":
+        cfg, ic = abi.workload("orszag_tang_3d", scale=scale, steps=steps)
+        cfg.nq = 3
+        return cfg, ic
+    return abi.workload(name, scale=scale, steps=steps)
+
+
+def one_domain(oracle, name, scale, steps, user=None):
+    cfg, ic = workload(name, scale, steps)
+    if user is not None:
+        for f in user[0]:
+            cfg.bc[f] = abi.KFVM_BC_USER
     s = oracle.OracleSolver(cfg)
+    if user is not None:
+        s.set_user_bc(user[1])
     s.init_ic(ic)
     u0 = s.get_state()
     dts = []
@@ -115,6 +129,7 @@ def test_block_config_walls_and_errors(product_lib):
 # --------------------------------------------------------- oracle, blocks as threads
 THREAD_CASES = [
     ("kelvin_helmholtz", 32, 3, (2, 1, 1)),
+    ("orszag_tang_3d_q3", 12, 2, (1, 2, 1)),    # 3D GLM-MHD with three Gauss points (81 rows)
     ("kelvin_helmholtz", 32, 3, (2, 2, 1)),      # corners: y halo over the exchanged x halo
     ("orszag_tang", 32, 3, (1, 2, 1)),           # GLM: cleaning speed and sources across blocks
     ("sod3d", 16, 2, (2, 1, 2)),                 # exchange faces beside outflow faces
@@ -168,6 +183,39 @@ def test_oracle_block_initial_condition(name, scale, nb, exact, oracle_lib, prod
         else:
             scale_v = np.abs(full).max(axis=1, keepdims=True)
             assert np.all(np.abs(u - ref) <= 1e-14 * scale_v)
+
+
+def test_oracle_blocks_with_user_inflow(oracle_lib, product_lib):
+    """Exchange faces beside a user-supplied inflow face: Sod 16^3 in 2 x 1 x 2
+    blocks, the western face a fixed supersonic inflow (a user function), against
+    the one-domain run with the same function, bit for bit."""
+    import decomp
+    import userbc
+    state = [1.5, 1.8, 0.0, 0.0, 1.5 / (1.4 - 1.0) + 0.5 * 1.5 * 1.2 * 1.2]
+    fn = userbc.inflow(state, 4, 5)
+    cfg, ic, u0, dts, ref = one_domain(oracle_lib, "sod3d", 16, 2, user=([0], fn))
+    b = blocks_of(cfg, (2, 1, 2))
+    hub = decomp.LocalExchange(4, timeout=60)
+    out = [None] * 4
+
+    def block(r):
+        def run():
+            c, nbr = product_lib.block_config(b, r)
+            s = oracle_lib.OracleSolver(c)
+            s.set_exchange(hub.endpoint(r, nbr))
+            if c.bc[0] == abi.KFVM_BC_USER:
+                s.set_user_bc(fn)
+            s.set_state(block_slice(u0, cfg, c))
+            for t, dt in dts:
+                s.set_time(t, dt)
+                assert s.take_step().accepted == 1
+            out[r] = (c, s.get_state())
+        return run
+
+    decomp.run_blocks([block(r) for r in range(4)])
+    for c, u in out:
+        assert np.array_equal(u, block_slice(ref, cfg, c)), list(c.block)
+    assert sum(1 for c, _ in out if c.bc[0] == abi.KFVM_BC_USER) == 2
 
 
 def test_missing_transport_fails(oracle_lib, product_lib):

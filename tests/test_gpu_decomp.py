@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 
 import kfvm_abi as abi
-from test_decomp import block_slice, blocks_of
+from test_decomp import block_slice, blocks_of, workload
 
 pytestmark = pytest.mark.gpu
 
@@ -30,6 +30,7 @@ CASES = [
     ("sod3d", 32, 3, (2, 1, 2), abi.KFVM_PREC_TF32X3),
     ("taylor_green", 32, 3, (2, 2, 2), abi.KFVM_PREC_FP64),
     ("orszag_tang_3d", 16, 2, (1, 2, 1), abi.KFVM_PREC_FP64),
+    ("orszag_tang_3d_q3", 12, 2, (1, 2, 1), abi.KFVM_PREC_FP64),  # 81 rows: the row-pass reconstruction
 ]
 
 
@@ -39,7 +40,7 @@ def test_blocks_match_one_domain(name, scale, steps, nb, prec, gpu, product_lib)
 
     import decomp
     kfvm = product_lib
-    cfg, ic = abi.workload(name, scale=scale, steps=steps)
+    cfg, ic = workload(name, scale, steps)
     one = kfvm.Solver(cfg)
     one.set_precision(prec)
     one.init_ic(ic)
@@ -124,3 +125,54 @@ def test_block_faces_hold_neighbour_states(gpu, product_lib):
         f = f.reshape(f.shape[0], f.shape[1], f.shape[2], c.ny, c.nx + 1)
         x0 = c.block[0] * c.nx
         assert np.array_equal(f, full[..., x0:x0 + c.nx + 1])
+
+
+def test_blocks_with_user_inflow(gpu, product_lib):
+    """Exchange faces beside a user-supplied inflow face on the device: Sod 24^3
+    in 2 x 1 x 2 blocks, the western face a fixed supersonic inflow, against the
+    one-domain run with the same function, bit for bit."""
+    import torch
+
+    import decomp
+    import userbc
+    kfvm = product_lib
+    cfg, ic = abi.workload("sod3d", scale=24, steps=3)
+    cfg.bc[0] = abi.KFVM_BC_USER
+    state = [1.5, 1.8, 0.0, 0.0, 1.5 / (cfg.gamma - 1.0) + 0.5 * 1.5 * 1.2 * 1.2]
+    fn = userbc.inflow(state, 4, 5)
+    one = kfvm.Solver(cfg)
+    one.set_user_bc(fn)
+    one.init_ic(ic)
+    u0 = one.get_state()
+    dts = []
+    for _ in range(3):
+        dts.append(one.time_dt())
+        assert one.take_step().accepted == 1
+    ref = one.get_state()
+    one.close()
+    b = blocks_of(cfg, (2, 1, 2))
+    hub = decomp.LocalExchange(4, device=torch.device("cuda", 0), timeout=120)
+    out = [None] * 4
+
+    def block(r):
+        def run():
+            torch.cuda.set_device(0)
+            c, nbr = kfvm.block_config(b, r)
+            s = kfvm.Solver(c)
+            try:
+                s.set_exchange(hub.endpoint(r, nbr))
+                if c.bc[0] == abi.KFVM_BC_USER:
+                    s.set_user_bc(fn)
+                s.set_state(block_slice(u0, cfg, c))
+                for t, dt in dts:
+                    s.set_time(t, dt)
+                    assert s.take_step().accepted == 1
+                out[r] = (c, s.get_state())
+            finally:
+                s.close()
+        return run
+
+    decomp.run_blocks([block(r) for r in range(4)])
+    for c, u in out:
+        want = block_slice(ref, cfg, c)
+        assert np.array_equal(u, want), (list(c.block), np.abs(u - want).max())
