@@ -291,7 +291,8 @@ int kfvm_selftest_rcp(int64_t n, uint64_t seed, int64_t *max_ulp, double *max_re
  * src/numeric/Numeric_K.H:292-398) with a 2x32 MLP over the normalised 5^d
  * density / pressure patch of a cell: inputs x = (q_k - q_c) / (max|q_k - q_c| +
  * 1e-4 |q_c|), q = rho then p, 50 (2D) or 250 (3D); NI -> 32 -> 32 -> 1 with GELU
- * and a sigmoid; BF16 weights, FP32 accumulation.  Weight layout (raw BF16):
+ * in its tanh approximation, x sigma(2 sqrt(2/pi) (x + 0.044715 x^3)), and a
+ * sigmoid; BF16 weights, FP32 accumulation.  Weight layout (raw BF16):
  * W1[32][NI], b1[32], W2[32][32], b2[32], w3[32], b3.
  * Labels come from the method: a cell is troubled when the normalised WENO-JS
  * weights of its density or pressure (createOmegas, Stencil_K.H:556-580) depart

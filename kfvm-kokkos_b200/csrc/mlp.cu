@@ -282,17 +282,69 @@ struct MlpTc {
   static constexpr int OFF_B2 = OFF_B1 + W1B;
   static constexpr int OFF_W = OFF_B2 + W2B;
   static constexpr int OFF_TILE = (OFF_W + PRMB + 127) / 128 * 128;
-  static constexpr int OFF_MX = OFF_TILE + (Tl::N * 8 + 15) / 16 * 16; // patch maxima [2 parts][128][2]
-  static constexpr int OFF_SUM = OFF_MX + 2 * 128 * 2 * 4; // part 1's share of the output sum [128]
-  static constexpr int OFF_OFS = OFF_SUM + 128 * 4;        // patch offsets [P] int
-  static constexpr int OFF_BAR = OFF_OFS + (M::P + 3) / 4 * 16;
+  static constexpr int OFF_SUM = OFF_TILE + (Tl::N * 8 + 15) / 16 * 16; // part 1's share of the output sum [128]
+  static constexpr int OFF_BAR = OFF_SUM + 128 * 4;
+  // scratch of the window extrema, in the A1 bytes before the features are written
+  static constexpr int EXT_BYTES = (Tl::TY + kBlockY) * Tl::TX * 16;
   static constexpr int SMEM = OFF_BAR + 32;                // MMA barrier, TMEM slot, load barrier
   static_assert(M::P <= PAD && NQC % 2 == 0, "pressure features start past the density ones");
   static_assert(OFF_TILE % 128 == 0 && OFF_B1 % 16 == 0 && OFF_B2 % 16 == 0, "TMA destination alignment");
   static_assert((W2B + PRMB) % 16 == 0 && W1B % 16 == 0, "bulk copy sizes");
   static_assert((Tl::TX * 8) % 16 == 0, "TMA box inner extent");
   static_assert(SMEM <= 113 * 1024, "two blocks per SM");
+  static_assert(EXT_BYTES <= A1, "extrema scratch inside the A1 bytes");
 };
+
+// (max, min) of density and pressure: (max rho, min rho, max p, min p)
+__device__ __forceinline__ float4 ext_of(float2 v) { return make_float4(v.x, v.x, v.y, v.y); }
+__device__ __forceinline__ float4 ext_merge(float4 e, float4 f) {
+  return make_float4(fmaxf(e.x, f.x), fminf(e.y, f.y), fmaxf(e.z, f.z), fminf(e.w, f.w));
+}
+
+// a (density, pressure) feature pair (q - q_c) s, both components at once: the
+// packed FP32 sub.rn / mul.rn round each component as __fsub_rn / __fmul_rn do
+__device__ __forceinline__ float2 mlp_feature2(float2 v, float2 c, float2 s) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(*reinterpret_cast<const uint64_t *>(&v)),
+      "l"(*reinterpret_cast<const uint64_t *>(&c)));
+  asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(d) : "l"(*reinterpret_cast<const uint64_t *>(&s)));
+  return *reinterpret_cast<const float2 *>(&d);
+}
+
+// the layer-1 operand rows of one cell, chunks cq = PART, PART + 2, ...: every loop
+// is unrolled, so each patch offset is a constant of the shared-memory load
+template <int DIM, int PART>
+__device__ __forceinline__ void mlp_features(const float2 *__restrict__ tc, float2 ref, float2 scl, bool live,
+                                             uint32_t aB, int row) {
+  using M = MlpShape<DIM>;
+  using Tl = MlpTile<DIM>;
+  using C = MlpTc<DIM>;
+  constexpr int ZR = DIM == 3 ? Tl::R : 0;
+#pragma unroll
+  for (int cq = PART; cq < C::NQC; cq += 2) {
+    uint32_t pr[4], pp[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      float2 x[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int q = cq * 8 + 2 * u + e;
+        x[e] = make_float2(0.0f, 0.0f);
+        if (q < M::P) {
+          const int dx = q % M::SIDE - Tl::R, dy = (q / M::SIDE) % M::SIDE - Tl::R,
+                    dz = q / (M::SIDE * M::SIDE) - ZR;
+          x[e] = mlp_feature2(tc[(dz * Tl::TY + dy) * Tl::TX + dx], ref, scl);
+        }
+      }
+      const __nv_bfloat162 br = __floats2bfloat162_rn(x[0].x, x[1].x); // .x low half, .y high half
+      const __nv_bfloat162 bp = __floats2bfloat162_rn(x[0].y, x[1].y);
+      pr[u] = live ? *reinterpret_cast<const uint32_t *>(&br) : 0u;
+      pp[u] = live ? *reinterpret_cast<const uint32_t *>(&bp) : 0u;
+    }
+    st_shared_v4(aB + cq * C::A_CH + row * 16, pr);
+    st_shared_v4(aB + (C::NQC + cq) * C::A_CH + row * 16, pp);
+  }
+}
 
 // the weight image of the inference kernel: W1^T in the layer-1 B layout
 // [k / 8][n][k % 8] (k the GEMM column), then W2^T as FP32 in the layer-2 B layout
@@ -337,9 +389,7 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
   // the block's halo tile of (density, pressure) pairs, [z][y][x] as the TMA box lands
   const float2 *tile = reinterpret_cast<const float2 *>(msm + C::OFF_TILE);
   const float *sW = reinterpret_cast<const float *>(msm + C::OFF_W);   // b1 [32], b2 [32], w3 [32], b3
-  float(*sMx)[128][2] = reinterpret_cast<float(*)[128][2]>(msm + C::OFF_MX);
   float *sSum = reinterpret_cast<float *>(msm + C::OFF_SUM);
-  int *sOfs = reinterpret_cast<int *>(msm + C::OFF_OFS);
   uint64_t *bar = reinterpret_cast<uint64_t *>(msm + C::OFF_BAR);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(msm + C::OFF_BAR + 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -366,13 +416,6 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
     bulk_load(smem_u32(msm + C::OFF_B1), img, C::W1B, barL);
     bulk_load(smem_u32(msm + C::OFF_B2), img + C::W1B, C::W2B + C::PRMB, barL);
   }
-  {
-    constexpr int ZR = DIM == 3 ? Tl::R : 0;
-    for (int q = tid; q < M::P; q += kMlpThreads) {
-      const int dx = q % M::SIDE - Tl::R, dy = (q / M::SIDE) % M::SIDE - Tl::R, dz = q / (M::SIDE * M::SIDE) - ZR;
-      sOfs[q] = (dz * Tl::TY + dy) * Tl::TX + dx;
-    }
-  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -382,49 +425,45 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
   const int c0 = (ZR * Tl::TY + quarter + Tl::R) * Tl::TX + lane + Tl::R;
   const uint32_t aB = smem_u32(msm), b1B = smem_u32(msm + C::OFF_B1), b2B = smem_u32(msm + C::OFF_B2);
   const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+  float2 ref = make_float2(0.0f, 0.0f), scl = make_float2(0.0f, 0.0f);
   if (ok) {
-    // patch maxima of |q - q_c|, each part over half the patch
-    const float2 ref = tile[c0];
-    float mr = 0.0f, mp = 0.0f;
-    const int q0 = part * ((M::P + 1) / 2), q1 = part ? M::P : (M::P + 1) / 2;
-    for (int q = q0; q < q1; q++) {
-      const float2 v = tile[c0 + sOfs[q]];
-      mr = fmaxf(mr, fabsf(__fsub_rn(v.x, ref.x)));
-      mp = fmaxf(mp, fabsf(__fsub_rn(v.y, ref.y)));
+    // window extrema of the patches, separably along z, y and x, in scratch that
+    // the A1 bytes hold until the features are written
+    float4 *ez = reinterpret_cast<float4 *>(msm);           // [TY][TX] after z
+    float4 *ey = ez + Tl::TY * Tl::TX;                      // [kBlockY][TX] after y
+    if (DIM == 3) {
+      for (int n = tid; n < Tl::TY * Tl::TX; n += kMlpThreads) {
+        float4 e = ext_of(tile[n]);
+#pragma unroll
+        for (int dz = 1; dz < Tl::TZ; dz++) e = ext_merge(e, ext_of(tile[dz * Tl::TY * Tl::TX + n]));
+        ez[n] = e;
+      }
+      __syncthreads();   // ok is uniform over the block
     }
-    sMx[part][row][0] = mr;
-    sMx[part][row][1] = mp;
+    for (int n = tid; n < kBlockY * Tl::TX; n += kMlpThreads) {
+      float4 e = DIM == 3 ? ez[n] : ext_of(tile[n]);
+#pragma unroll
+      for (int dy = 1; dy < MlpShape<DIM>::SIDE; dy++)
+        e = ext_merge(e, DIM == 3 ? ez[dy * Tl::TX + n] : ext_of(tile[dy * Tl::TX + n]));
+      ey[n] = e;
+    }
+    __syncthreads();
+    ref = tile[c0];
+    float4 e = ey[quarter * Tl::TX + lane];
+#pragma unroll
+    for (int dx = 1; dx < MlpShape<DIM>::SIDE; dx++) e = ext_merge(e, ey[quarter * Tl::TX + lane + dx]);
+    // rounding is monotonic, so max_k |fl(q_k - q_c)| = max(fl(max q - q_c), fl(q_c - min q))
+    scl.x = mlp_scale(fmaxf(__fsub_rn(e.x, ref.x), __fsub_rn(ref.x, e.y)), ref.x);
+    scl.y = mlp_scale(fmaxf(__fsub_rn(e.z, ref.y), __fsub_rn(ref.y, e.w)), ref.y);
   }
-  __syncthreads();
+  __syncthreads();   // the scratch is overwritten by the features
   if (ok) {
-    const float2 ref = tile[c0];
-    const float sr = mlp_scale(fmaxf(sMx[0][row][0], sMx[1][row][0]), ref.x);
-    const float sp = mlp_scale(fmaxf(sMx[0][row][1], sMx[1][row][1]), ref.y);
     // features: chunk cq of 8 patch cells gives density chunk cq and pressure
     // chunk NQC + cq; the parts take alternate chunks
-    for (int cq = part; cq < C::NQC; cq += 2) {
-      uint32_t pr[4], pp[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        float xr[2], xp[2];
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int q = cq * 8 + 2 * u + e;
-          xr[e] = xp[e] = 0.0f;
-          if (q < M::P && live) {
-            const float2 v = tile[c0 + sOfs[q]];
-            xr[e] = mlp_feature(v.x, ref.x, sr);
-            xp[e] = mlp_feature(v.y, ref.y, sp);
-          }
-        }
-        const __nv_bfloat162 br = __floats2bfloat162_rn(xr[0], xr[1]); // .x low half, .y high half
-        const __nv_bfloat162 bp = __floats2bfloat162_rn(xp[0], xp[1]);
-        pr[u] = *reinterpret_cast<const uint32_t *>(&br);
-        pp[u] = *reinterpret_cast<const uint32_t *>(&bp);
-      }
-      st_shared_v4(aB + cq * C::A_CH + row * 16, pr);
-      st_shared_v4(aB + (C::NQC + cq) * C::A_CH + row * 16, pp);
-    }
+    if (part == 0)
+      mlp_features<DIM, 0>(tile + c0, ref, scl, live, aB, row);
+    else
+      mlp_features<DIM, 1>(tile + c0, ref, scl, live, aB, row);
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();

@@ -6,8 +6,8 @@
 // (z, y, x) order, x fastest).  With q = rho or p (computed in FP64, rounded to
 // FP32) and every operation below in FP32:
 //   d_k = q_k - q_c,  s = 1 / (max_k |d_k| + 1e-4 |q_c|),  x_k = d_k s,
-// then rounded to BF16, the operand type of the network.  Network: NI -> 32 -> 32 -> 1, GELU after both hidden layers,
-// sigmoid output.  Weights are BF16 (raw uint16 at the C ABI), every sum
+// then rounded to BF16, the operand type of the network.  Network: NI -> 32 -> 32 -> 1, GELU (tanh
+// approximation, gelu below) after both hidden layers, sigmoid output.  Weights are BF16 (raw uint16 at the C ABI), every sum
 // accumulates in FP32.  Weight layout (one flat array):
 //   W1 [32][NI], b1 [32], W2 [32][32], b2 [32], w3 [32], b3
 #pragma once
@@ -39,10 +39,24 @@ struct MlpTile {
   static constexpr int N = TX * TY * TZ;
 };
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh approximation (Hendrycks and Gimpel), written as
+// x sigma(2 sqrt(2/pi) (x + 0.044715 x^3)): one exponential and one approximate
+// division instead of erf.  Inference and training use the same function.
+constexpr float kGeluC0 = 1.5957691216057308f;   // 2 sqrt(2 / pi)
+constexpr float kGeluC1 = 0.07135481627260025f;    // 2 sqrt(2 / pi) 0.044715
+
+// sigma(2 sqrt(2/pi) (x + 0.044715 x^3)); the exponent is capped so that the
+// denominator stays below the range where __fdividef returns 0
+__device__ __forceinline__ float gelu_sig(float x) {
+  const float y = x * fmaf(kGeluC1, x * x, kGeluC0);
+  return __fdividef(1.0f, 1.0f + __expf(fminf(-y, 80.0f)));
+}
+
+__device__ __forceinline__ float gelu(float x) { return x * gelu_sig(x); }
 
 __device__ __forceinline__ float gelu_grad(float x) {
-  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float s = gelu_sig(x);
+  return s + x * s * (1.0f - s) * fmaf(3.0f * kGeluC1, x * x, kGeluC0);
 }
 
 template <int DIM, int EQ>

@@ -86,8 +86,9 @@ def unpack(w_bf16, ni):
 
 
 def gelu(x):
-    from scipy.special import erf
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    """GELU in its tanh approximation, x sigma(2 sqrt(2/pi) (x + 0.044715 x^3))."""
+    c0 = 2.0 * np.sqrt(2.0 / np.pi)
+    return x / (1.0 + np.exp(-x * (c0 + c0 * 0.044715 * x * x)))
 
 
 def probability(w_bf16, x):
