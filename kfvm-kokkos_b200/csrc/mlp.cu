@@ -282,11 +282,12 @@ struct MlpTc {
   static constexpr int OFF_B2 = OFF_B1 + W1B;
   static constexpr int OFF_W = OFF_B2 + W2B;
   static constexpr int OFF_TILE = (OFF_W + PRMB + 127) / 128 * 128;
-  static constexpr int OFF_SUM = OFF_TILE + (Tl::N * 8 + 15) / 16 * 16; // part 1's share of the output sum [128]
+  static constexpr int TILE_BYTES = (Tl::N * 8 + 127) / 128 * 128;   // one of the two tile buffers
+  static constexpr int OFF_SUM = OFF_TILE + 2 * TILE_BYTES; // part 1's share of the output sum [128]
   static constexpr int OFF_BAR = OFF_SUM + 128 * 4;
   // scratch of the window extrema, in the A1 bytes before the features are written
   static constexpr int EXT_BYTES = (Tl::TY + kBlockY) * Tl::TX * 16;
-  static constexpr int SMEM = OFF_BAR + 32;                // MMA barrier, TMEM slot, load barrier
+  static constexpr int SMEM = OFF_BAR + 48;                // 4 barriers (MMA, weights, 2 tiles), TMEM slot
   static_assert(M::P <= PAD && NQC % 2 == 0, "pressure features start past the density ones");
   static_assert(OFF_TILE % 128 == 0 && OFF_B1 % 16 == 0 && OFF_B2 % 16 == 0, "TMA destination alignment");
   static_assert((W2B + PRMB) % 16 == 0 && W1B % 16 == 0, "bulk copy sizes");
@@ -376,57 +377,94 @@ __global__ void __launch_bounds__(256)
   if (t < 4) prm[96 + t] = t == 0 ? wq[M::B3] : 0.0f;
 }
 
-// mode 0: flags (+ prediction, flagged count); mode 1: probabilities
+// mode 0: flags (+ prediction, flagged count); mode 1: probabilities.
+// Persistent: each block allocates its TMEM and loads the weight image once, then
+// takes the cell blocks b = blockIdx.x, blockIdx.x + gridDim.x, ... (nbx x nby x nz
+// of them, x fastest), with the next one's halo tile already on its way by TMA
+// into the other tile buffer.
 template <int DIM, int EQ, int MODE>
-__global__ void __launch_bounds__(kMlpThreads, 2)
+__global__ void __launch_bounds__(kMlpThreads, DIM == 2 ? 4 : 2)
     mlp_tc_kernel(const __grid_constant__ CUtensorMap rpMap, Grid g, const uint8_t *__restrict__ img,
                   const double *__restrict__ theta, uint8_t *__restrict__ flag, uint8_t *__restrict__ pred,
-                  float *__restrict__ prob, DevScalars *__restrict__ sc, float logit_thr) {
+                  float *__restrict__ prob, DevScalars *__restrict__ sc, float logit_thr, int nbx, int nby,
+                  int nblk) {
   using M = MlpShape<DIM>;
   using Tl = MlpTile<DIM>;
   using C = MlpTc<DIM>;
   extern __shared__ __align__(128) uint8_t msm[];
-  // the block's halo tile of (density, pressure) pairs, [z][y][x] as the TMA box lands
-  const float2 *tile = reinterpret_cast<const float2 *>(msm + C::OFF_TILE);
   const float *sW = reinterpret_cast<const float *>(msm + C::OFF_W);   // b1 [32], b2 [32], w3 [32], b3
   float *sSum = reinterpret_cast<float *>(msm + C::OFF_SUM);
   uint64_t *bar = reinterpret_cast<uint64_t *>(msm + C::OFF_BAR);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(msm + C::OFF_BAR + 8);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(msm + C::OFF_BAR + 32);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int quarter = warp & 3, part = warp >> 2;
   const int row = quarter * 32 + lane;
-  const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY, k = blockIdx.z;
-  const int64_t i = i0 + lane, j = j0 + quarter;
-  const bool live = i < g.nx && j < g.ny;
-  const uint32_t barA = smem_u32(bar), barL = barA + 16;
+  // barriers: MMA completion, weight image, tile buffer 0, tile buffer 1
+  const uint32_t barA = smem_u32(bar), barW = barA + 8, barT0 = barA + 16;
+  constexpr uint32_t kTileBytes = (uint32_t)(Tl::N * sizeof(float2));
+  auto tile_load = [&](int b, int buf) {   // thread 0: the halo tile of cell block b
+    const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+    const uint32_t tb = barT0 + 8u * (uint32_t)buf;
+    mbar_arrive_expect_tx(tb, kTileBytes);
+    // padded coordinates of the tile's first cell: i0 - R, j0 - R, k - R in cells
+    tma_load_3d(smem_u32(msm + C::OFF_TILE + buf * C::TILE_BYTES), &rpMap, bx * kBlockX, by * kBlockY, bz, tb);
+  };
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                  "r"(64u)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
+  // loads in flight per tile buffer and the parity of each buffer's next phase
+  // (kept by thread 0, which issues the loads, for the exit path)
+  uint32_t inflight = 0u, tpar = 0u;   // bit q: buffer q
   if (tid == 0) {
     mbar_init(barA, 1);
-    mbar_init(barL, 1);
+    mbar_init(barW, 1);
+    mbar_init(barT0, 1);
+    mbar_init(barT0 + 8, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    // the halo tile (padded coordinates of its first cell: i0 - R, j0 - R, k - R in
-    // cells) and the weight image, all on one barrier
-    mbar_arrive_expect_tx(barL, (uint32_t)(Tl::N * sizeof(float2) + C::IMG_BYTES));
-    tma_load_3d(smem_u32(msm + C::OFF_TILE), &rpMap, (int)i0, (int)j0, (int)k, barL);
-    bulk_load(smem_u32(msm + C::OFF_B1), img, C::W1B, barL);
-    bulk_load(smem_u32(msm + C::OFF_B2), img + C::W1B, C::W2B + C::PRMB, barL);
+    mbar_arrive_expect_tx(barW, (uint32_t)C::IMG_BYTES);
+    bulk_load(smem_u32(msm + C::OFF_B1), img, C::W1B, barW);
+    bulk_load(smem_u32(msm + C::OFF_B2), img + C::W1B, C::W2B + C::PRMB, barW);
+    if ((int)blockIdx.x < nblk) {
+      tile_load(blockIdx.x, 0);
+      inflight = 1u;
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
-  bool ok = __syncthreads_and(mbar_wait(barL, 0u));
+  bool ok = __syncthreads_and(mbar_wait(barW, 0u));
   constexpr int ZR = DIM == 3 ? Tl::R : 0;
   const int c0 = (ZR * Tl::TY + quarter + Tl::R) * Tl::TX + lane + Tl::R;
   const uint32_t aB = smem_u32(msm), b1B = smem_u32(msm + C::OFF_B1), b2B = smem_u32(msm + C::OFF_B2);
   const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
-  float2 ref = make_float2(0.0f, 0.0f), scl = make_float2(0.0f, 0.0f);
-  if (ok) {
+  int it = 0;
+  for (int b = blockIdx.x; ok && b < nblk; b += gridDim.x, it++) {
+    const int buf = it & 1;
+    // the next cell block's tile goes into the other buffer, whose last reads ended
+    // before the closing barrier of the previous iteration
+    if (tid == 0 && b + (int)gridDim.x < nblk) {
+      tile_load(b + gridDim.x, buf ^ 1);
+      inflight |= 1u << (buf ^ 1);
+    }
+    const bool got = mbar_wait(barT0 + 8u * (uint32_t)buf, (uint32_t)((it >> 1) & 1));
+    if (tid == 0 && got) {
+      inflight &= ~(1u << buf);
+      tpar ^= 1u << buf;
+    }
+    ok = __syncthreads_and(got);
+    if (!ok) break;
+    // the cell block's halo tile of (density, pressure) pairs, [z][y][x] as the TMA box lands
+    const float2 *tile = reinterpret_cast<const float2 *>(msm + C::OFF_TILE + buf * C::TILE_BYTES);
+    const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+    const int64_t i = (int64_t)bx * kBlockX + lane, j = (int64_t)by * kBlockY + quarter, k = bz;
+    const bool live = i < g.nx && j < g.ny;
+    const int64_t c = (k * g.ny + j) * g.nx + i;
+    // the positivity history of the cell, read now so that the load overlaps the features
+    const double th = MODE == 0 && part == 0 && live ? theta[c] : 1.0;
     // window extrema of the patches, separably along z, y and x, in scratch that
     // the A1 bytes hold until the features are written
     float4 *ez = reinterpret_cast<float4 *>(msm);           // [TY][TX] after z
@@ -438,7 +476,7 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
         for (int dz = 1; dz < Tl::TZ; dz++) e = ext_merge(e, ext_of(tile[dz * Tl::TY * Tl::TX + n]));
         ez[n] = e;
       }
-      __syncthreads();   // ok is uniform over the block
+      __syncthreads();
     }
     for (int n = tid; n < kBlockY * Tl::TX; n += kMlpThreads) {
       float4 e = DIM == 3 ? ez[n] : ext_of(tile[n]);
@@ -448,77 +486,76 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
       ey[n] = e;
     }
     __syncthreads();
-    ref = tile[c0];
-    float4 e = ey[quarter * Tl::TX + lane];
+    const float2 ref = tile[c0];
+    float2 scl;
+    {
+      float4 e = ey[quarter * Tl::TX + lane];
 #pragma unroll
-    for (int dx = 1; dx < MlpShape<DIM>::SIDE; dx++) e = ext_merge(e, ey[quarter * Tl::TX + lane + dx]);
-    // rounding is monotonic, so max_k |fl(q_k - q_c)| = max(fl(max q - q_c), fl(q_c - min q))
-    scl.x = mlp_scale(fmaxf(__fsub_rn(e.x, ref.x), __fsub_rn(ref.x, e.y)), ref.x);
-    scl.y = mlp_scale(fmaxf(__fsub_rn(e.z, ref.y), __fsub_rn(ref.y, e.w)), ref.y);
-  }
-  __syncthreads();   // the scratch is overwritten by the features
-  if (ok) {
+      for (int dx = 1; dx < MlpShape<DIM>::SIDE; dx++) e = ext_merge(e, ey[quarter * Tl::TX + lane + dx]);
+      // rounding is monotonic, so max_k |fl(q_k - q_c)| = max(fl(max q - q_c), fl(q_c - min q))
+      scl.x = mlp_scale(fmaxf(__fsub_rn(e.x, ref.x), __fsub_rn(ref.x, e.y)), ref.x);
+      scl.y = mlp_scale(fmaxf(__fsub_rn(e.z, ref.y), __fsub_rn(ref.y, e.w)), ref.y);
+    }
+    __syncthreads();   // the scratch is overwritten by the features
     // features: chunk cq of 8 patch cells gives density chunk cq and pressure
     // chunk NQC + cq; the parts take alternate chunks
     if (part == 0)
       mlp_features<DIM, 0>(tile + c0, ref, scl, live, aB, row);
     else
       mlp_features<DIM, 1>(tile + c0, ref, scl, live, aB, row);
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  __syncthreads();
-  if (ok && tid == 0) {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    constexpr uint32_t idesc1 = bf16_idesc<32>();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      constexpr uint32_t idesc1 = bf16_idesc<32>();
 #pragma unroll 1
-    for (int s = 0; s < C::NCH / 2; s++) {
-      const uint64_t ad = umma_desc(aB + 2 * s * C::A_CH, C::A_CH, 128);
-      const uint64_t bd = umma_desc(b1B + 2 * s * C::B_CH, C::B_CH, 128);
-      mma_bf16(tmem, ad, bd, idesc1, s > 0 ? 1 : 0);
-    }
-    mma_commit(barA);
-  }
-  if (ok) ok = mbar_wait(barA, 0u);
-  ok = __syncthreads_and(ok);
-  if (ok) {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // H1 = gelu(D1 + b1) of this part's 16 hidden units, split hi + lo into A2
-    float z[16];
-    tmem_ld8(tmem + lanes + (uint32_t)(16 * part), *reinterpret_cast<float(*)[8]>(z));
-    tmem_ld8(tmem + lanes + (uint32_t)(16 * part + 8), *reinterpret_cast<float(*)[8]>(z + 8));
-    const uint32_t aHi = aB, aLo = aB + 8 * C::A_CH;
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      uint32_t hi[4], lo[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int h = 16 * part + 4 * c + u;
-        const float x = gelu(z[4 * c + u] + sW[h]);
-        hi[u] = to_tf32(x);
-        lo[u] = to_tf32(x - __uint_as_float(hi[u]));
+      for (int s = 0; s < C::NCH / 2; s++) {
+        const uint64_t ad = umma_desc(aB + 2 * s * C::A_CH, C::A_CH, 128);
+        const uint64_t bd = umma_desc(b1B + 2 * s * C::B_CH, C::B_CH, 128);
+        mma_bf16(tmem, ad, bd, idesc1, s > 0 ? 1 : 0);
       }
-      st_shared_v4(aHi + (4 * part + c) * C::A_CH + row * 16, hi);
-      st_shared_v4(aLo + (4 * part + c) * C::A_CH + row * 16, lo);
+      mma_commit(barA);
     }
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (ok && tid == 0) {
+    ok = __syncthreads_and(mbar_wait(barA, 0u));   // two commits per cell block: parity 0, then 1
+    if (!ok) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    constexpr uint32_t idesc2 = tf32_idesc<32>();
-    const uint32_t aHi = aB, aLo = aB + 8 * C::A_CH;
+    {
+      // H1 = gelu(D1 + b1) of this part's 16 hidden units, split hi + lo into A2
+      float z[16];
+      tmem_ld8(tmem + lanes + (uint32_t)(16 * part), *reinterpret_cast<float(*)[8]>(z));
+      tmem_ld8(tmem + lanes + (uint32_t)(16 * part + 8), *reinterpret_cast<float(*)[8]>(z + 8));
+      const uint32_t aHi = aB, aLo = aB + 8 * C::A_CH;
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      const uint64_t bd = umma_desc(b2B + 2 * s * C::B_CH, C::B_CH, 128);
-      mma_tf32(tmem + 32, umma_desc(aLo + 2 * s * C::A_CH, C::A_CH, 128), bd, idesc2, s > 0 ? 1 : 0);
-      mma_tf32(tmem + 32, umma_desc(aHi + 2 * s * C::A_CH, C::A_CH, 128), bd, idesc2, 1);
+      for (int c = 0; c < 4; c++) {
+        uint32_t hi[4], lo[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int h = 16 * part + 4 * c + u;
+          const float x = gelu(z[4 * c + u] + sW[h]);
+          hi[u] = to_tf32(x);
+          lo[u] = to_tf32(x - __uint_as_float(hi[u]));
+        }
+        st_shared_v4(aHi + (4 * part + c) * C::A_CH + row * 16, hi);
+        st_shared_v4(aLo + (4 * part + c) * C::A_CH + row * 16, lo);
+      }
     }
-    mma_commit(barA);
-  }
-  if (ok) ok = mbar_wait(barA, 1u);
-  ok = __syncthreads_and(ok);
-  if (ok) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      constexpr uint32_t idesc2 = tf32_idesc<32>();
+      const uint32_t aHi = aB, aLo = aB + 8 * C::A_CH;
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        const uint64_t bd = umma_desc(b2B + 2 * s * C::B_CH, C::B_CH, 128);
+        mma_tf32(tmem + 32, umma_desc(aLo + 2 * s * C::A_CH, C::A_CH, 128), bd, idesc2, s > 0 ? 1 : 0);
+        mma_tf32(tmem + 32, umma_desc(aHi + 2 * s * C::A_CH, C::A_CH, 128), bd, idesc2, 1);
+      }
+      mma_commit(barA);
+    }
+    ok = __syncthreads_and(mbar_wait(barA, 1u));
+    if (!ok) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     float z[16];
     tmem_ld8(tmem + lanes + (uint32_t)(32 + 16 * part), *reinterpret_cast<float(*)[8]>(z));
@@ -535,11 +572,10 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
       bool f = false;
       if (live) {
         const float logit = sW[96] + acc + sSum[row];
-        const int64_t c = (k * g.ny + j) * g.nx + i;
         if (MODE == 0) {
           const bool p = logit > logit_thr;
           pred[c] = p ? 1 : 0;
-          f = p || theta[c] < 1.0;
+          f = p || th < 1.0;
           flag[c] = f ? 1 : 0;
         } else {
           prob[c] = 1.0f / (1.0f + expf(-logit));
@@ -550,9 +586,17 @@ __global__ void __launch_bounds__(kMlpThreads, 2)
         if (lane == 0 && ball) atomicAdd(&sc->nflag, (unsigned)__popc(ball));
       }
     }
-  } else if (tid == 0) {
+    // the tile buffer, the A bytes, sSum and TMEM are reused by the next cell block
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  if (!ok && tid == 0) {
     atomicExch(&sc->fault, 1u);
-    mbar_wait(barL, 0u);   // loads still in flight land before the block leaves
+    // the weight image and tile loads still in flight land before the block leaves
+    // (bounded waits; a completed phase returns at once)
+    mbar_wait(barW, 0u);
+    for (int q = 0; q < 2; q++)
+      if ((inflight >> q) & 1u) mbar_wait(barT0 + 8u * (uint32_t)q, (tpar >> q) & 1u);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -598,8 +642,36 @@ static cudaError_t tc_t(const double *U, const Grid &g, float2 *rp, int64_t rpx,
   const int64_t planes = DIM == 3 ? g.nz + 2 * kRad : 1;
   const int64_t np = g.px * g.py * planes;
   mlp_rp_kernel<EQ><<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, g, planes, rpx, rp);
-  mlp_tc_kernel<DIM, EQ, MODE><<<mlp_cell_grid(g), kMlpThreads, C::SMEM, s>>>(map, g, img, theta, flag, pred, prob,
-                                                                            sc, thr);
+  const dim3 cb = mlp_cell_grid(g);
+  const int nblk = (int)(cb.x * cb.y * cb.z);
+  // as many blocks as are resident at once: the SM's shared memory and registers
+  // divided by one block's (2 per SM in 3D, by shared memory; 4 in 2D); computed from
+  // the device's limits with the largest shared-memory carveout requested
+  static const int per_sm = [] {
+    cudaFuncAttributes fa;
+    int dev = 0, smem_sm = 0, smem_rsv = 0, regs_sm = 0;
+    if (cudaFuncSetAttribute(mlp_tc_kernel<DIM, EQ, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, mlp_tc_kernel<DIM, EQ, MODE>) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess)
+      return 0;
+    const int warp_regs = (fa.numRegs * 32 + 255) / 256 * 256;   // allocated per warp in units of 256
+    const int by_smem = smem_sm / (C::SMEM + (int)fa.sharedSizeBytes + smem_rsv);
+    const int by_regs = regs_sm / (warp_regs * (kMlpThreads / 32));
+    return std::min(by_smem, by_regs);
+  }();
+  static const int nsm = [] {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return 0;
+    return n;
+  }();
+  if (per_sm <= 0 || nsm <= 0) return cudaErrorInvalidConfiguration;
+  const int grid = std::min(nblk, per_sm * nsm);
+  mlp_tc_kernel<DIM, EQ, MODE><<<grid, kMlpThreads, C::SMEM, s>>>(map, g, img, theta, flag, pred, prob, sc, thr,
+                                                                 (int)cb.x, (int)cb.y, nblk);
   return cudaGetLastError();
 }
 
