@@ -87,3 +87,80 @@ def test_driver_writes_stats_rows(tmp_path, gpu, product_lib):
     assert rows.shape == (3, 3), rows.shape
     assert np.all(np.diff(rows[:, 0]) > 0.0)
     assert np.all(np.diff(rows[:, 1]) < 0.0)        # the vortex decays
+
+
+# halo signs of the wall types (Hydro_BCCoeffs.H: reflect negates the normal
+# momentum, no-slip every momentum)
+def _halo_signs(bc, axis):
+    s = np.ones(5)
+    if bc == abi.KFVM_BC_REFLECTING:
+        s[1 + axis] = -1.0
+    elif bc == abi.KFVM_BC_NOSLIP:
+        s[1:4] = -1.0
+    return s
+
+
+def _flow_stats_np(u, cfg):
+    """FlowStats<Hydro / NavierStokes> (Hydro_K.H:103-178, NavierStokes_K.H:102-175)
+    in numpy on an interior state (5, nz, ny, nx).  The one halo layer it reads is
+    filled here from the boundary types alone, independently of the solver:
+    periodic wrap, outflow copy, and the mirrored boundary cell with the sign table
+    of the wall type."""
+    a = u.copy()
+    for ax, arr_ax in ((0, 3), (1, 2), (2, 1)):      # x, y, z: array axes 3, 2, 1
+        lo, hi = cfg.bc[2 * ax], cfg.bc[2 * ax + 1]
+        if lo == abi.KFVM_BC_PERIODIC:
+            a = np.concatenate([np.take(a, [-1], axis=arr_ax), a, np.take(a, [0], axis=arr_ax)], axis=arr_ax)
+            continue
+        sl = _halo_signs(lo, ax).reshape(5, 1, 1, 1)
+        sh = _halo_signs(hi, ax).reshape(5, 1, 1, 1)
+        a = np.concatenate([sl * np.take(a, [0], axis=arr_ax), a, sh * np.take(a, [-1], axis=arr_ax)],
+                           axis=arr_ax)
+    dx = (cfg.xup - cfg.xlo) / cfg.nx
+    dy = (cfg.yup - cfg.ylo) / cfg.ny
+    dz = (cfg.zup - cfg.zlo) / cfg.nz
+    v = a[1:4] / a[0]
+    c = (slice(1, -1),) * 3
+
+    def d(comp, ax, h):
+        p = [slice(1, -1)] * 3
+        m = [slice(1, -1)] * 3
+        p[ax] = slice(2, None)
+        m[ax] = slice(0, -2)
+        return 0.5 * (v[comp][tuple(p)] - v[comp][tuple(m)]) / h
+    # array axes of v[comp]: 0 = z, 1 = y, 2 = x
+    dyu, dxv = d(0, 1, dy), d(1, 2, dx)
+    dzu, dzv, dxw, dyw = d(0, 0, dz), d(1, 0, dz), d(2, 2, dx), d(2, 1, dy)
+    om2 = (dyw - dzv) ** 2 + (dzu - dxw) ** 2 + (dxv - dyu) ** 2
+    rho = a[0][c]
+    ek = 0.5 * (a[1][c] ** 2 + a[2][c] ** 2 + a[3][c] ** 2) / rho
+    ifac = (dx * dy * dz) / ((cfg.xup - cfg.xlo) * (cfg.yup - cfg.ylo) * (cfg.zup - cfg.zlo))
+    return np.array([ifac * ek.sum(), ifac * (0.5 * rho * om2).sum()])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("walls", ["ppnnrr", "rrppnn"])
+def test_stats_after_restart_with_walls(walls, tmp_path, gpu, product_lib):
+    """Right after a restart the solver has evaluated nothing, so the halo the
+    statistics read comes from the statistics call itself.  Checked against the
+    reference's formula in numpy with a halo filled independently from the wall
+    types, on a Taylor-Green box with no-slip and reflecting walls."""
+    codes = {"p": abi.KFVM_BC_PERIODIC, "r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP}
+    cfg, ic = abi.workload("taylor_green", scale=12, steps=2)
+    for f, w in enumerate(walls):
+        cfg.bc[f] = codes[w]
+    a = product_lib.Solver(cfg)
+    a.init_ic(ic)
+    for _ in range(2):
+        assert a.take_step().accepted
+    a.write_plotfile(tmp_path / "ck", "tg", 2, ckpt=True, time_step=2)
+    b = product_lib.Solver(cfg)
+    assert b.restart(tmp_path / "ck" / "tg_0000002.xmf") == 2
+    u = b.get_state().reshape(5, cfg.nz, cfg.ny, cfg.nx)
+    ref = _flow_stats_np(u, cfg)
+    got = b.flow_stats()
+    assert np.all(np.abs(got - ref) <= 1e-12 * np.abs(ref)), (got, ref)
+    # the solver that stepped there reports the same statistics
+    assert np.all(np.abs(a.flow_stats() - ref) <= 1e-12 * np.abs(ref))
+    a.close()
+    b.close()
