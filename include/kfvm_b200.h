@@ -297,7 +297,8 @@ int kfvm_selftest_rcp(int64_t n, uint64_t seed, int64_t *max_ulp, double *max_re
  * Labels come from the method: a cell is troubled when the normalised WENO-JS
  * weights of its density or pressure (createOmegas, Stencil_K.H:556-580) depart
  * from the linear weights by more than tau somewhere.  In the stage, a hashed
- * fraction of cells (the judge) always runs full WENO; their labels are compared
+ * fraction of the runs of 32 consecutive cells along x (the judge) always runs
+ * full WENO; their labels are compared
  * with the predictions, and a step whose judged troubled cells were missed more
  * often than miss_limit sends the next two steps to KXRCF.  The kfvm_mlp_* calls
  * allocate the buffers they need; stepping still allocates nothing. */

@@ -663,7 +663,8 @@ __global__ void __launch_bounds__(RowsShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV)
 // PositivityPreserve_K bounds of every cell (Common_K.H:331-380; SR: SRHydro_K.H:224-246)
 // from a per-block footprint tile: [minDens | maxDens | minEint][cell], the same
 // values recon_kernel computes in its own prologue.  The pre-pass of the tensor-core
-// reconstruction, whose shared memory holds the halo tiles instead.
+// reconstruction, whose shared memory holds the halo tiles instead (2D; 3D uses
+// bounds_march_kernel below).
 template <int DIM, int EQ>
 __global__ void __launch_bounds__(128) bounds_kernel(const double *__restrict__ U, Grid g, double *__restrict__ bnd) {
   __shared__ double tile[6][PosTile<DIM>::N];
@@ -677,6 +678,48 @@ __global__ void __launch_bounds__(128) bounds_kernel(const double *__restrict__ 
     bnd[c] = bd.minDens;
     bnd[g.n + c] = bd.maxDens;
     bnd[2 * g.n + c] = bd.minEint;
+  }
+}
+
+// The same bounds in 3D from blocks that march along z over zc planes with a ring of
+// three footprint planes: each plane's quantities are computed once per block
+// instead of once for each of the three cell planes that read them.
+template <int EQ>
+__global__ void __launch_bounds__(128)
+    bounds_march_kernel(const double *__restrict__ U, Grid g, int zc, double *__restrict__ bnd) {
+  using P = PosTile<3>;
+  constexpr int PL = P::TX * P::TY;
+  __shared__ double ring[6][3 * PL];   // plane kp in slot (kp + 3) % 3
+  const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY;
+  const int64_t k0 = blockIdx.z * (int64_t)zc, k1 = k0 + zc < g.nz ? k0 + zc : g.nz;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  auto fill = [&](int64_t kp) {   // footprint plane kp (-1 .. nz)
+    const int slot = (int)((kp + 3) % 3);
+    for (int t = tid; t < PL; t += blockDim.x * blockDim.y) {
+      const int a = t % P::TX, b = t / P::TX;
+      const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b;
+      if (gi > g.nx || gj > g.ny) continue; // beyond the ring of any live cell
+      pos_cell<EQ>(U, g, gi, gj, kp, ring, slot * PL + t);
+    }
+  };
+  fill(k0 - 1);
+  fill(k0);
+  const int64_t i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const int base = (threadIdx.y + 1) * P::TX + threadIdx.x + 1;
+  for (int64_t k = k0; k < k1; k++) {
+    fill(k + 1);
+    __syncthreads();
+    if (i < g.nx && j < g.ny) {
+      const int sLo = (int)((k + 2) % 3) * PL, sMid = (int)(k % 3) * PL, sHi = (int)((k + 1) % 3) * PL;
+      const PosBounds bd = pos_bounds_at<3, EQ>(ring, [&](int xo, int yo, int zo) {
+        return (zo < 0 ? sLo : (zo > 0 ? sHi : sMid)) + base + yo * P::TX + xo;
+      });
+      const int64_t c = (k * g.ny + j) * g.nx + i;
+      bnd[c] = bd.minDens;
+      bnd[g.n + c] = bd.maxDens;
+      bnd[2 * g.n + c] = bd.minEint;
+    }
+    __syncthreads();   // the next plane goes into the slot of plane k - 1
   }
 }
 
@@ -841,8 +884,10 @@ __global__ void __launch_bounds__(256)
       }
     }
     // the judge's cells compute full WENO whatever the flags say (they do not enter
-    // the set); one outside the set keeps its linear states unless judged troubled
-    judged = mode == RECON_SPARSE && jd.frac > 0.0 && unit_hash(jd.seed, (uint64_t)c) < jd.frac;
+    // the set); one outside the set keeps its linear states unless judged troubled.
+    // The judge samples runs of 32 consecutive cells (along x), so that the heavy
+    // pass loads their stencils coalesced
+    judged = mode == RECON_SPARSE && jd.frac > 0.0 && unit_hash(jd.seed, (uint64_t)(c >> 5)) < jd.frac;
     judgeOnly = judged && !useWeno;
     useWeno = useWeno || judged;
     applied[c] = useWeno ? 1 : 0;
@@ -1829,7 +1874,14 @@ struct Launch {
     return cudaGetLastError();
   }
   static cudaError_t bounds(const double *U, const Grid &g, double *bnd, cudaStream_t s) {
-    bounds_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, bnd);
+    if constexpr (DIM == 3) {
+      constexpr int kZc = 16;   // planes per block
+      const dim3 cg = cell_grid(g);
+      bounds_march_kernel<EQ><<<dim3(cg.x, cg.y, (unsigned)((g.nz + kZc - 1) / kZc)), dim3(kBlockX, kBlockY), 0, s>>>(
+          U, g, kZc, bnd);
+    } else {
+      bounds_kernel<DIM, EQ><<<cell_grid(g), dim3(kBlockX, kBlockY), 0, s>>>(U, g, bnd);
+    }
     return cudaGetLastError();
   }
   static cudaError_t recon(const double *U, const CUtensorMap *umap, const Grid &g, const DevStencil *S,

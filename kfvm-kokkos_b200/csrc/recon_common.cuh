@@ -38,48 +38,54 @@ struct PosTile {
   static constexpr int N = TX * TY * TZ;
 };
 
+// the footprint quantities of padded cell (gi, gj, gk) into entry t of sm
+template <int EQ, int NT>
+__device__ __forceinline__ void pos_cell(const double *__restrict__ U, const Grid &g, int64_t gi, int64_t gj,
+                                         int64_t gk, double (*sm)[NT], int t) {
+  using E = Eos<EQ>;
+  const double *Uc = U + pidx(g, gi, gj, gk);
+  double st[E::NV];
+#pragma unroll
+  for (int v = 0; v < E::NV; v++) st[v] = Uc[v * g.pvol];
+  if constexpr (EQ == EQ_SR) {
+    // density and E - sqrt(D^2 + S^2); SR bounds need nothing else
+    sm[0][t] = st[DENS];
+    sm[1][t] = sr::ediff(st);
+    return;
+  }
+  const double ir = 1.0 / st[DENS];
+  const double ei = E::eint_r(st, ir);
+  sm[0][t] = st[DENS];
+  sm[1][t] = ei;
+  sm[2][t] = sqrt(g.gamma * ((g.gamma - 1.0) * ei) * ir);
+  // velocities as the reference's divergence estimate takes them (m / rho,
+  // Common_K.H:363-378)
+  sm[3][t] = st[MOMX] / st[DENS];
+  sm[4][t] = st[MOMY] / st[DENS];
+  sm[5][t] = st[MOMZ] / st[DENS];
+}
+
 template <int DIM, int EQ>
 __device__ __forceinline__ void pos_tile_fill(const double *__restrict__ U, const Grid &g, int64_t i0,
                                               int64_t j0, int64_t k, double (*sm)[PosTile<DIM>::N]) {
   using P = PosTile<DIM>;
-  using E = Eos<EQ>;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int t = tid; t < P::N; t += blockDim.x * blockDim.y) {
     const int a = t % P::TX, b = (t / P::TX) % P::TY, cz = t / (P::TX * P::TY);
     const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b, gk = k - (DIM == 3 ? 1 : 0) + cz;
     if (gi > g.nx || gj > g.ny) continue; // beyond the ring of any live cell
-    const double *Uc = U + pidx(g, gi, gj, gk);
-    double st[E::NV];
-#pragma unroll
-    for (int v = 0; v < E::NV; v++) st[v] = Uc[v * g.pvol];
-    if constexpr (EQ == EQ_SR) {
-      // density and E - sqrt(D^2 + S^2); SR bounds need nothing else
-      sm[0][t] = st[DENS];
-      sm[1][t] = sr::ediff(st);
-      continue;
-    }
-    const double ir = 1.0 / st[DENS];
-    const double ei = E::eint_r(st, ir);
-    sm[0][t] = st[DENS];
-    sm[1][t] = ei;
-    sm[2][t] = sqrt(g.gamma * ((g.gamma - 1.0) * ei) * ir);
-    // velocities as the reference's divergence estimate takes them (m / rho,
-    // Common_K.H:363-378)
-    sm[3][t] = st[MOMX] / st[DENS];
-    sm[4][t] = st[MOMY] / st[DENS];
-    sm[5][t] = st[MOMZ] / st[DENS];
+    pos_cell<EQ>(U, g, gi, gj, gk, sm, t);
   }
 }
 
 // PositivityPreserve_K bounds (Common_K.H:331-380; SR: SRHydro_K.H:224-246, no
 // flattening) from the footprint tile
-template <int DIM, int EQ>
-__device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<DIM>::N], int tx, int ty) {
-  using P = PosTile<DIM>;
+// (at(xo, yo, zo) gives the entry of the neighbour at that offset)
+template <int DIM, int EQ, int NT, class At>
+__device__ __forceinline__ PosBounds pos_bounds_at(const double (*sm)[NT], At at) {
   double maxDens = -1.7976931348623157e308, minDens = 1.7976931348623157e308;
   double minEint = 1.7976931348623157e308, minSdSp = 1.7976931348623157e308;
   constexpr int zr = DIM == 3 ? 1 : 0;
-  auto at = [&](int xo, int yo, int zo) { return ((zr + zo) * P::TY + (ty + 1 + yo)) * P::TX + (tx + 1 + xo); };
   if constexpr (EQ == EQ_SR) {
 #pragma unroll
     for (int xo = -1; xo <= 1; xo++)
@@ -120,6 +126,15 @@ __device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<
   b.minEint = minEint * (1.0 - kappa);
   return b;
   }
+}
+
+template <int DIM, int EQ>
+__device__ __forceinline__ PosBounds pos_bounds_tile(const double (*sm)[PosTile<DIM>::N], int tx, int ty) {
+  using P = PosTile<DIM>;
+  constexpr int zr = DIM == 3 ? 1 : 0;
+  return pos_bounds_at<DIM, EQ>(sm, [&](int xo, int yo, int zo) {
+    return ((zr + zo) * P::TY + (ty + 1 + yo)) * P::TX + (tx + 1 + xo);
+  });
 }
 
 } // namespace kfvm
