@@ -946,7 +946,19 @@ struct HeavyShape {
   // cells per block (one thread per cell and variable); 16 where 32 cells' rows
   // would not fit in shared memory (3D GLM-MHD with three points: 81 rows x 9)
   static constexpr int CELLS = NR * T::NV > 400 ? 16 : 32;
-  static constexpr size_t BYTES = (size_t)(DER + FW + CELLS * NR * T::NV + CELLS * 2 + CELLS * T::NV) * sizeof(double) +
+  // 3D Euler / Navier-Stokes with two Gauss points (24 rows): both contractions
+  // (derivative rows for the smoothness indicators, substencil rows for the blend)
+  // on the FP64 MMA.  In 2D the per-thread form is faster: its contractions are
+  // short, and the WENO cells are sparse among the listed ones, which the MMA form
+  // computes for every cell of a block that has one
+  static constexpr bool MMA = DIM == 3 && (EQ == EQ_HYDRO || EQ == EQ_NS) && NR <= 24 && CELLS == 32;
+  static constexpr int MI = (T::NI + 7) / 8;                 // m-tiles of derivative rows
+  static constexpr int MR = (NR + 7) / 8;                    // m-tiles of reconstruction rows
+  static constexpr int VS = 36;                              // row stride of the stencil values [q][cell]
+  // the MMA form's stencil values [v][q][VS] overlay the row results [cell][row][v]
+  static constexpr int UNION = MMA && T::NV * T::C * VS > CELLS * NR * T::NV ? T::NV * T::C * VS : CELLS * NR * T::NV;
+  static constexpr int COEF = MMA ? T::NV * T::NSUB * 32 : 0; // [v][s][cell]
+  static constexpr size_t BYTES = (size_t)(DER + FW + UNION + CELLS * 2 + CELLS * T::NV + COEF) * sizeof(double) +
                                   (size_t)T::NB * T::CB * sizeof(int);
   __host__ __device__ static constexpr int n(int s) { return s == 0 ? T::C : (s == 1 ? T::CC : T::CB); }
   __host__ __device__ static constexpr int off(int s) {
@@ -968,9 +980,11 @@ __global__ void __launch_bounds__(HeavyShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV, 
   double *sDer = hsm;                       // [s][p][i], i padded to NIP
   double *sFw = sDer + H::DER;              // [s][p][row]
   double *sFs = sFw + H::FW;                // [cell][row][v]
-  double *sDep = sFs + H::CELLS * NR * NV;  // [cell][2]
+  double *sV = sFs;                         // MMA form: stencil values [v][q][VS], before the rows
+  double *sDep = sFs + H::UNION;            // [cell][2]
   double *sTh = sDep + H::CELLS * 2;        // limiter theta of each thread's rows [v][cell]
-  int *sSub = reinterpret_cast<int *>(sTh + H::CELLS * NV);
+  double *sCo = sTh + H::CELLS * NV;        // MMA form: [v][s][cell] indicators, then blend coefficients
+  int *sSub = reinterpret_cast<int *>(sCo + H::COEF);
   const kfvm_stencil &st = S->w;
   const int tid = threadIdx.y * H::CELLS + threadIdx.x, nt = H::CELLS * NV;
   // weights transposed so that the rows of one stencil value are adjacent and
@@ -1003,6 +1017,188 @@ __global__ void __launch_bounds__(HeavyShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV, 
     const int64_t i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
     const double *Uc = U + pidx(g, i, j, k);
     double *rs = sFs + x * NR * NV;
+    if constexpr (H::MMA) {
+      // ---- WENO-AO with both contractions on the FP64 MMA (mma.sync m8n8k4): warp v
+      // takes variable v of the block's 32 cells as the N dimension, the derivative
+      // rows (smoothness indicators) and the substencil rows (reconstructions) as M,
+      // the substencil's stencil entries as K.  Lanes of cells outside the WENO set
+      // contribute zeros and discard their results.
+      const bool mine = have && (e & kHeavyWeno);
+      if (__syncthreads_or(mine)) {   // uniform over the block: every warp sees the same cells
+        const int lq = x & 3, ln = x >> 2;
+        double *sVw = sV + v * (T::C * H::VS);
+        double *sCw = sCo + v * (T::NSUB * 32);
+        double ref[NV];
+#pragma unroll
+        for (int w = 0; w < NV; w++) ref[w] = Uc[w * g.pvol];
+        VarConv<EQ> vc(ref, g.gamma);
+        {
+          // component v of the linearised primitives on this lane's cell's stencil,
+          // into the warp's [q][cell] table
+          auto lin = [&](auto cTag) {
+            constexpr int CV = decltype(cTag)::value;
+#pragma unroll 4
+            for (int q = 0; q < T::C; q++) {
+              const int64_t o = S->loff[q];
+              double u[NV];
+#pragma unroll
+              for (int w = 0; w < NV; w++)
+                u[w] = (CV == ETOT || w == CV || w == DENS) ? Uc[w * g.pvol + o] : 0.0;
+              sVw[q * H::VS + x] = vc.lin1(u, CV);
+            }
+          };
+          if (mine) {
+            switch (v) {
+              case DENS: lin(std::integral_constant<int, DENS>{}); break;
+              case MOMX: lin(std::integral_constant<int, MOMX>{}); break;
+              case MOMY: lin(std::integral_constant<int, MOMY>{}); break;
+              case MOMZ: lin(std::integral_constant<int, MOMZ>{}); break;
+              default: lin(std::integral_constant<int, ETOT>{}); break;
+            }
+          } else {
+            for (int q = 0; q < T::C; q++) sVw[q * H::VS + x] = 0.0;
+          }
+        }
+        __syncwarp();
+        auto cellOf = [&](int s, int p) { return s < 2 ? p : sSub[(s - 2) * T::CB + p]; };
+        // smoothness indicators: b = D_s V_s per substencil, beta = sum of b^2 over
+        // the rows (lane l holds rows 8 m + l / 4 of cells 8 t + 2 (l % 4) + e)
+#pragma unroll 1
+        for (int s = 0; s < T::NSUB; s++) {
+          const int n = H::n(s);
+          const double *D = sDer + H::NIP * H::off(s);
+          double bd[H::MI][4][2];
+#pragma unroll
+          for (int mm = 0; mm < H::MI; mm++)
+#pragma unroll
+            for (int t = 0; t < 4; t++) bd[mm][t][0] = bd[mm][t][1] = 0.0;
+          for (int p0 = 0; p0 < n; p0 += 4) {
+            const int p = p0 + lq;
+            const bool pk = p < n;
+            const int q = pk ? cellOf(s, p) : 0;
+            double bv[4];
+#pragma unroll
+            for (int t = 0; t < 4; t++) bv[t] = pk ? sVw[q * H::VS + 8 * t + ln] : 0.0;
+#pragma unroll
+            for (int mm = 0; mm < H::MI; mm++) {
+              const int row = 8 * mm + ln;
+              const double av = pk && row < T::NI ? D[p * H::NIP + row] : 0.0;
+#pragma unroll
+              for (int t = 0; t < 4; t++) dmma_884(bd[mm][t], av, bv[t]);
+            }
+          }
+#pragma unroll
+          for (int t = 0; t < 4; t++)
+#pragma unroll
+            for (int ee = 0; ee < 2; ee++) {
+              double sq = 0.0;
+#pragma unroll
+              for (int mm = 0; mm < H::MI; mm++) sq += bd[mm][t][ee] * bd[mm][t][ee];
+#pragma unroll
+              for (int o = 4; o < 32; o <<= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+              if (ln == 0) sCw[s * 32 + 8 * t + 2 * lq + ee] = sq;
+            }
+        }
+        __syncwarp();
+        double om[T::NSUB];
+#pragma unroll
+        for (int s = 0; s < T::NSUB; s++) om[s] = sCw[s * 32 + x];
+        if (mine) {
+          // nonlinear weights, the judge's departure and the adaptive-order transform,
+          // as the per-thread kernel computes them
+          bool sig = false;
+          if (jd.frac > 0.0 && (e & kHeavyJudge) && (v == DENS || v == ETOT)) {
+            double lin[NV];
+#pragma unroll
+            for (int w = 0; w < NV; w++) lin[w] = ref[w];
+            vc.cons2LinPrim(lin);
+            sig = sqrt(om[0]) > kMlpFloor * fabs(v == DENS ? lin[DENS] : lin[ETOT]);
+          }
+          constexpr double gHi = 0.7, gLo = 0.7;
+          double gam[T::NSUB];
+          gam[0] = gHi;
+          gam[1] = (1.0 - gHi) * gLo;
+#pragma unroll
+          for (int s = 2; s < T::NSUB; s++) gam[s] = (1.0 - gHi) * (1.0 - gLo) / (DIM == 2 ? 4.0 : 6.0);
+          double tot = 0.0;
+#pragma unroll
+          for (int s = 0; s < T::NSUB; s++) {
+            om[s] = gam[s] / (om[s] * om[s] + 1.e-40);
+            tot += om[s];
+          }
+#pragma unroll
+          for (int s = 0; s < T::NSUB; s++) om[s] /= tot;
+          double dep = 0.0;
+          if (sig)
+#pragma unroll
+            for (int s = 0; s < T::NSUB; s++) dep = fmax(dep, fabs(om[s] - gam[s]));
+          if (v == DENS) sDep[x * 2] = dep;
+          if (v == ETOT) sDep[x * 2 + 1] = dep;
+          om[0] /= gam[0];
+#pragma unroll
+          for (int s = 1; s < T::NSUB; s++) om[s] -= om[0] * gam[s];
+        }
+        // each lane overwrites only its own cell's column
+#pragma unroll
+        for (int s = 0; s < T::NSUB; s++) sCw[s * 32 + x] = mine ? om[s] : 0.0;
+        __syncwarp();
+        // blend: acc = sum over s of om_s (W_s V_s), each W_s V_s summed first as the
+        // reference does (per row and cell)
+        double acc[H::MR][4][2];
+#pragma unroll
+        for (int mm = 0; mm < H::MR; mm++)
+#pragma unroll
+          for (int t = 0; t < 4; t++) acc[mm][t][0] = acc[mm][t][1] = 0.0;
+#pragma unroll 1
+        for (int s = 0; s < T::NSUB; s++) {
+          const int n = H::n(s);
+          const double *Wr = sFw + H::NRP * H::off(s);
+          double tt[H::MR][4][2];
+#pragma unroll
+          for (int mm = 0; mm < H::MR; mm++)
+#pragma unroll
+            for (int t = 0; t < 4; t++) tt[mm][t][0] = tt[mm][t][1] = 0.0;
+          for (int p0 = 0; p0 < n; p0 += 4) {
+            const int p = p0 + lq;
+            const bool pk = p < n;
+            const int q = pk ? cellOf(s, p) : 0;
+            double bv[4];
+#pragma unroll
+            for (int t = 0; t < 4; t++) bv[t] = pk ? sVw[q * H::VS + 8 * t + ln] : 0.0;
+#pragma unroll
+            for (int mm = 0; mm < H::MR; mm++) {
+              const int row = 8 * mm + ln;
+              const double av = pk && row < NR ? Wr[p * H::NRP + row] : 0.0;
+#pragma unroll
+              for (int t = 0; t < 4; t++) dmma_884(tt[mm][t], av, bv[t]);
+            }
+          }
+#pragma unroll
+          for (int t = 0; t < 4; t++)
+#pragma unroll
+            for (int ee = 0; ee < 2; ee++) {
+              const double c = sCw[s * 32 + 8 * t + 2 * lq + ee];
+              if (c != 0.0)
+#pragma unroll
+                for (int mm = 0; mm < H::MR; mm++) acc[mm][t][ee] += c * tt[mm][t][ee];
+            }
+        }
+        __syncthreads();   // every warp is done with the stencil values the rows overlay
+        const unsigned wm = __ballot_sync(0xffffffffu, mine);
+#pragma unroll
+        for (int t = 0; t < 4; t++)
+#pragma unroll
+          for (int ee = 0; ee < 2; ee++) {
+            const int cell = 8 * t + 2 * lq + ee;
+            if ((wm >> cell) & 1u)
+#pragma unroll
+              for (int mm = 0; mm < H::MR; mm++) {
+                const int row = 8 * mm + ln;
+                if (row < NR) sFs[(cell * NR + row) * NV + v] = acc[mm][t][ee];
+              }
+          }
+      }
+    } else
     if (have && (e & kHeavyWeno)) {
       // ---- variable v of WENO-AO on the linearised primitives
       double ref[NV];
