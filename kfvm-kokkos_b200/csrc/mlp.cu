@@ -255,9 +255,10 @@ __global__ void __launch_bounds__(256)
 //            the product carries about 21 bits of H1, as the FP32 layer of
 //            training does.
 //   output   gelu(D2 + b2) . w3 + b3, each part summing 16 hidden units.
-// The block's halo tile of pairs arrives by one TMA load.  Every mbarrier wait is
-// bounded; on timeout the block sets DevScalars::fault, waits (bounded) for its
-// tile load, frees its TMEM and returns.
+// Each cell block's halo tile of pairs arrives by one TMA load, issued while the
+// previous cell block is processed.  Every mbarrier wait is bounded; on timeout
+// the block sets DevScalars::fault, waits (bounded) for the loads it has in
+// flight, frees its TMEM and returns.
 constexpr int kMlpThreads = 256;
 
 template <int DIM>
