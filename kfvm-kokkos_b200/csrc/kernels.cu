@@ -683,32 +683,60 @@ __global__ void __launch_bounds__(128) bounds_kernel(const double *__restrict__ 
 
 // The same bounds in 3D from blocks that march along z over zc planes with a ring of
 // three footprint planes: each plane's quantities are computed once per block
-// instead of once for each of the three cell planes that read them.
+// instead of once for each of the three cell planes that read them.  The state of
+// plane k + 2 is loaded into registers while the bounds of plane k are computed,
+// so the global loads do not sit between the barriers of consecutive planes.
 template <int EQ>
 __global__ void __launch_bounds__(128)
     bounds_march_kernel(const double *__restrict__ U, Grid g, int zc, double *__restrict__ bnd) {
   using P = PosTile<3>;
+  using E = Eos<EQ>;
+  constexpr int NV = E::NV;
   constexpr int PL = P::TX * P::TY;
-  __shared__ double ring[6][3 * PL];   // plane kp in slot (kp + 3) % 3
+  constexpr int NPT = (PL + 127) / 128;   // plane positions per thread (block of 128 threads)
+  __shared__ double ring[6][3 * PL];      // plane kp in slot (kp + 3) % 3
   const int64_t i0 = blockIdx.x * (int64_t)kBlockX, j0 = blockIdx.y * (int64_t)kBlockY;
   const int64_t k0 = blockIdx.z * (int64_t)zc, k1 = k0 + zc < g.nz ? k0 + zc : g.nz;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  auto fill = [&](int64_t kp) {   // footprint plane kp (-1 .. nz)
-    const int slot = (int)((kp + 3) % 3);
-    for (int t = tid; t < PL; t += blockDim.x * blockDim.y) {
-      const int a = t % P::TX, b = t / P::TX;
-      const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b;
-      if (gi > g.nx || gj > g.ny) continue; // beyond the ring of any live cell
-      pos_cell<EQ>(U, g, gi, gj, kp, ring, slot * PL + t);
-    }
+  // this thread's plane positions t = tid + 128 n; false beyond the ring of any live cell
+  bool use[NPT];
+  int64_t off[NPT];
+#pragma unroll
+  for (int n = 0; n < NPT; n++) {
+    const int t = tid + 128 * n;
+    const int a = t % P::TX, b = t / P::TX;
+    const int64_t gi = i0 - 1 + a, gj = j0 - 1 + b;
+    use[n] = t < PL && gi <= g.nx && gj <= g.ny;
+    off[n] = use[n] ? pidx(g, gi, gj, 0) : 0;
+  }
+  const int64_t pz = pidx(g, 0, 0, 1) - pidx(g, 0, 0, 0);   // one plane along z
+  double st[NPT][NV];
+  auto load = [&](int64_t kp) {   // the state of footprint plane kp (-1 .. nz) into st
+#pragma unroll
+    for (int n = 0; n < NPT; n++)
+      if (use[n]) {
+        const double *Uc = U + off[n] + kp * pz;
+#pragma unroll
+        for (int v = 0; v < NV; v++) st[n][v] = Uc[v * g.pvol];
+      }
   };
-  fill(k0 - 1);
-  fill(k0);
+  auto put = [&](int64_t kp) {    // its quantities into the plane's ring slot
+    const int slot = (int)((kp + 3) % 3);
+#pragma unroll
+    for (int n = 0; n < NPT; n++)
+      if (use[n]) pos_quantities<EQ>(st[n], g, ring, slot * PL + tid + 128 * n);
+  };
+  load(k0 - 1);
+  put(k0 - 1);
+  load(k0);
+  put(k0);
+  load(k0 + 1);
   const int64_t i = i0 + threadIdx.x, j = j0 + threadIdx.y;
   const int base = (threadIdx.y + 1) * P::TX + threadIdx.x + 1;
   for (int64_t k = k0; k < k1; k++) {
-    fill(k + 1);
+    put(k + 1);
     __syncthreads();
+    if (k + 2 <= k1) load(k + 2);   // consumed by the next plane
     if (i < g.nx && j < g.ny) {
       const int sLo = (int)((k + 2) % 3) * PL, sMid = (int)(k % 3) * PL, sHi = (int)((k + 1) % 3) * PL;
       const PosBounds bd = pos_bounds_at<3, EQ>(ring, [&](int xo, int yo, int zo) {

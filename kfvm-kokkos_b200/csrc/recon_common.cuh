@@ -38,15 +38,11 @@ struct PosTile {
   static constexpr int N = TX * TY * TZ;
 };
 
-// the footprint quantities of padded cell (gi, gj, gk) into entry t of sm
+// the footprint quantities of a cell state st into entry t of sm
 template <int EQ, int NT>
-__device__ __forceinline__ void pos_cell(const double *__restrict__ U, const Grid &g, int64_t gi, int64_t gj,
-                                         int64_t gk, double (*sm)[NT], int t) {
+__device__ __forceinline__ void pos_quantities(const double (&st)[Eos<EQ>::NV], const Grid &g, double (*sm)[NT],
+                                               int t) {
   using E = Eos<EQ>;
-  const double *Uc = U + pidx(g, gi, gj, gk);
-  double st[E::NV];
-#pragma unroll
-  for (int v = 0; v < E::NV; v++) st[v] = Uc[v * g.pvol];
   if constexpr (EQ == EQ_SR) {
     // density and E - sqrt(D^2 + S^2); SR bounds need nothing else
     sm[0][t] = st[DENS];
@@ -63,6 +59,18 @@ __device__ __forceinline__ void pos_cell(const double *__restrict__ U, const Gri
   sm[3][t] = st[MOMX] / st[DENS];
   sm[4][t] = st[MOMY] / st[DENS];
   sm[5][t] = st[MOMZ] / st[DENS];
+}
+
+// the footprint quantities of padded cell (gi, gj, gk) into entry t of sm
+template <int EQ, int NT>
+__device__ __forceinline__ void pos_cell(const double *__restrict__ U, const Grid &g, int64_t gi, int64_t gj,
+                                         int64_t gk, double (*sm)[NT], int t) {
+  using E = Eos<EQ>;
+  const double *Uc = U + pidx(g, gi, gj, gk);
+  double st[E::NV];
+#pragma unroll
+  for (int v = 0; v < E::NV; v++) st[v] = Uc[v * g.pvol];
+  pos_quantities<EQ>(st, g, sm, t);
 }
 
 template <int DIM, int EQ>
