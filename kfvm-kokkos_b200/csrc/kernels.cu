@@ -983,8 +983,12 @@ struct HeavyShape {
   static constexpr int MI = (T::NI + 7) / 8;                 // m-tiles of derivative rows
   static constexpr int MR = (NR + 7) / 8;                    // m-tiles of reconstruction rows
   static constexpr int VS = 36;                              // row stride of the stencil values [q][cell]
-  // the MMA form's stencil values [v][q][VS] overlay the row results [cell][row][v]
-  static constexpr int UNION = MMA && T::NV * T::C * VS > CELLS * NR * T::NV ? T::NV * T::C * VS : CELLS * NR * T::NV;
+  // cell stride of the row results [cell][row][v], made odd so that the lanes of a
+  // warp (its cells) fall on different banks (an even stride of 120 doubles put
+  // all 32 lanes on two banks)
+  static constexpr int CS = (NR * T::NV) | 1;
+  // the MMA form's stencil values [v][q][VS] overlay the row results
+  static constexpr int UNION = MMA && T::NV * T::C * VS > CELLS * CS ? T::NV * T::C * VS : CELLS * CS;
   static constexpr int COEF = MMA ? T::NV * T::NSUB * 32 : 0; // [v][s][cell]
   static constexpr size_t BYTES = (size_t)(DER + FW + UNION + CELLS * 2 + CELLS * T::NV + COEF) * sizeof(double) +
                                   (size_t)T::NB * T::CB * sizeof(int);
@@ -1007,7 +1011,7 @@ __global__ void __launch_bounds__(HeavyShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV, 
   extern __shared__ __align__(16) double hsm[];
   double *sDer = hsm;                       // [s][p][i], i padded to NIP
   double *sFw = sDer + H::DER;              // [s][p][row]
-  double *sFs = sFw + H::FW;                // [cell][row][v]
+  double *sFs = sFw + H::FW;                // [cell][row][v], cell stride CS
   double *sV = sFs;                         // MMA form: stencil values [v][q][VS], before the rows
   double *sDep = sFs + H::UNION;            // [cell][2]
   double *sTh = sDep + H::CELLS * 2;        // limiter theta of each thread's rows [v][cell]
@@ -1044,7 +1048,7 @@ __global__ void __launch_bounds__(HeavyShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV, 
     const int64_t c = e & kHeavyCell;
     const int64_t i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
     const double *Uc = U + pidx(g, i, j, k);
-    double *rs = sFs + x * NR * NV;
+    double *rs = sFs + x * H::CS;
     if constexpr (H::MMA) {
       // ---- WENO-AO with both contractions on the FP64 MMA (mma.sync m8n8k4): warp v
       // takes variable v of the block's 32 cells as the N dimension, the derivative
@@ -1222,7 +1226,7 @@ __global__ void __launch_bounds__(HeavyShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV, 
 #pragma unroll
               for (int mm = 0; mm < H::MR; mm++) {
                 const int row = 8 * mm + ln;
-                if (row < NR) sFs[(cell * NR + row) * NV + v] = acc[mm][t][ee];
+                if (row < NR) sFs[cell * H::CS + row * NV + v] = acc[mm][t][ee];
               }
           }
       }
