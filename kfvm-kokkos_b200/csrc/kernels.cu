@@ -539,8 +539,11 @@ struct RowsShape {
   static constexpr int NFQ = T::NF * T::NQF;
   static constexpr int CELLS = 16;
   static constexpr int RCH = 27;  // rows per pass
+  // cell stride of the face-state table, odd so that a warp's cells fall on
+  // different shared-memory banks
+  static constexpr int CS = (NFQ * T::NV) | 1;
   static constexpr size_t BYTES =
-      (size_t)(T::C * NR + CELLS * NFQ * T::NV + 3 * CELLS + 3 * T::NV * CELLS) * sizeof(double);
+      (size_t)(T::C * NR + CELLS * CS + 3 * CELLS + 3 * T::NV * CELLS) * sizeof(double);
 };
 
 template <int DIM, int EQ, int NQ>
@@ -556,8 +559,8 @@ __global__ void __launch_bounds__(RowsShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV)
   constexpr int NV = T::NV, NR = R::NR, NFQ = R::NFQ, C = T::C, NQF = T::NQF;
   extern __shared__ __align__(16) double rsm[];
   double *sW = rsm;                        // [stencil cell][row]
-  double *sS = sW + C * NR;                // face states [cell][face row][v]
-  double *sBd = sS + R::CELLS * NFQ * NV;  // [minDens | maxDens | minEint][cell]
+  double *sS = sW + C * NR;                // face states [cell][face row][v], cell stride CS
+  double *sBd = sS + R::CELLS * R::CS;     // [minDens | maxDens | minEint][cell]
   double *sRed = sBd + 3 * R::CELLS;       // [inside | lam | vel][v][cell]
   const int x = threadIdx.x, v = threadIdx.y, tid = v * R::CELLS + x, nt = R::CELLS * NV;
   for (int t = tid; t < C * NR; t += nt) sW[t] = S->lin[t];
@@ -594,7 +597,7 @@ __global__ void __launch_bounds__(RowsShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV)
 #pragma unroll
       for (int r = 0; r < R::RCH; r++) {
         const int row = r0 + r;
-        if (row < NFQ) sS[(x * NFQ + row) * NV + v] = acc[r];
+        if (row < NFQ) sS[x * R::CS + row * NV + v] = acc[r];
         else if (row < NR) src[((int64_t)(row - NFQ) * NV + v) * g.n + c] = acc[r];
       }
     }
@@ -614,7 +617,7 @@ __global__ void __launch_bounds__(RowsShape<DIM, EQ, NQ>::CELLS * Eos<EQ>::NV)
     for (int row = v; row < NFQ; row += NV) {
       double st[NV];
 #pragma unroll
-      for (int w = 0; w < NV; w++) st[w] = sS[(x * NFQ + row) * NV + w];
+      for (int w = 0; w < NV; w++) st[w] = sS[x * R::CS + row * NV + w];
       double ei = 0.0;
       if constexpr (EQ == EQ_SR) {
         inside = inside && pos_inside<EQ>(bd, st);
