@@ -131,6 +131,27 @@ IC_OT = r"""
   state[8] = 0.0;
 """
 
+IC_SR_RIEM2D = r"""
+  (void)z; (void)userParams;
+  // four-quadrant special-relativistic Riemann problem (the states of the
+  // repository's sr_riemann_2d workload), as D, S and E from the primitives
+  const Real gR = eosParams.gamma / (eosParams.gamma - 1.0), v0 = 0.99;
+  Real rho, vx, vy, p;
+  if (x > 0.0) {
+    if (y > 0.0) { rho = 0.1; vx = 0.0; vy = 0.0; p = 0.01; }
+    else { rho = 0.1; vx = 0.0; vy = v0; p = 1.0; }
+  } else {
+    if (y > 0.0) { rho = 0.1; vx = v0; vy = 0.0; p = 1.0; }
+    else { rho = 0.5; vx = 0.0; vy = 0.0; p = 1.0; }
+  }
+  const Real W = 1.0 / std::sqrt(1.0 - vx * vx - vy * vy), h = 1.0 + p * gR / rho;
+  state[0] = rho * W;
+  state[1] = rho * W * W * h * vx;
+  state[2] = rho * W * W * h * vy;
+  state[3] = 0.0;
+  state[4] = rho * W * W * h - p;
+"""
+
 PROBLEMS = {
     # name: (dim, eq, rs, rk, nq, bc, sources, ic body)
     "isentropic_vortex": (2, "Hydro", "HLLC", "SSP4_3_2", 2, "periodic", False, IC_VORTEX),
@@ -141,6 +162,8 @@ PROBLEMS = {
     "orszag_tang_3d": (3, "MHD_GLM", "HLL", "SSP4_3_2", 2, "periodic", True, IC_OT),
     # three Gauss points (NUM_QUAD_PTS 3, as MHD/MagVort3d): 27 interior source points
     "orszag_tang_3d_q3": (3, "MHD_GLM", "HLL", "SSP4_3_2", 3, "periodic", True, IC_OT),
+    # special-relativistic hydro (the Newton pressure recovery and its limiter)
+    "sr_riemann_2d": (2, "SRHydro", "LLF", "SSP4_3_2", 2, "outflow", False, IC_SR_RIEM2D),
 }
 
 

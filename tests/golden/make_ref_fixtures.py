@@ -37,6 +37,7 @@ CASES = [
     ("orszag_tang_64", "orszag_tang", 64, 10, None, 2, None),
     ("orszag_tang_3d_16", "orszag_tang_3d", 16, 3, None, 2, None),   # 3D GLM-MHD sources at Q^3 points
     ("orszag_tang_3d_q3_12", "orszag_tang_3d", 12, 2, None, 3, "orszag_tang_3d_q3"),  # three points
+    ("sr_riemann_2d_32", "sr_riemann_2d", 32, 4, None, 2, None),      # special-relativistic hydro
 ]
 
 

@@ -53,7 +53,7 @@ def test_oracle_matches_reference_bitwise(path, oracle_lib):
 
 
 # direct runs of the reference build when it is present
-DIRECT = [("kelvin_helmholtz", 24, 3), ("sod3d", 12, 2), ("orszag_tang", 24, 2)]
+DIRECT = [("kelvin_helmholtz", 24, 3), ("sod3d", 12, 2), ("orszag_tang", 24, 2), ("sr_riemann_2d", 24, 2)]
 
 
 @pytest.mark.parametrize("name,scale,steps", DIRECT)
