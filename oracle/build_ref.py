@@ -164,6 +164,11 @@ PROBLEMS = {
     "orszag_tang_3d_q3": (3, "MHD_GLM", "HLL", "SSP4_3_2", 3, "periodic", True, IC_OT),
     # special-relativistic hydro (the Newton pressure recovery and its limiter)
     "sr_riemann_2d": (2, "SRHydro", "LLF", "SSP4_3_2", 2, "outflow", False, IC_SR_RIEM2D),
+    # walls: reflecting on every face of the blast; no-slip y faces of the
+    # otherwise periodic Taylor-Green box (west east south north bottom top)
+    "sod3d_reflecting": (3, "Hydro", "HLLC", "SSP4_3_2", 2, ("reflecting",) * 6, False, IC_SOD),
+    "taylor_green_noslip": (3, "NavierStokes", "HLLC", "SSP4_3_2", 2,
+                            ("periodic", "periodic", "noslip", "noslip", "periodic", "periodic"), False, IC_TGV),
 }
 
 
@@ -265,12 +270,14 @@ KOKKOS_INLINE_FUNCTION void Face{side}(const DataViewType &, int {a}, int {b}, i
 
 
 def problem_setup_cpp(bc, sources):
-    b = f"KFVM::BCType::{bc}"
+    """bc: one boundary type for every face, or six (west east south north bottom top)."""
+    names = (bc,) * 6 if isinstance(bc, str) else tuple(bc)
+    b = ", ".join(f"KFVM::BCType::{n}" for n in names)
     return f"""// Boundary types and source-term switch of this problem (generated by oracle/build_ref.py)
 #include <array>
 #include "BoundaryConditions_K.H"
 #include "ProblemSetup.H"
-std::array<KFVM::BCType, 6> KFVM::ProblemSetup::bcType = {{{b}, {b}, {b}, {b}, {b}, {b}}};
+std::array<KFVM::BCType, 6> KFVM::ProblemSetup::bcType = {{{b}}};
 bool KFVM::ProblemSetup::haveSourceTerms = {"true" if sources else "false"};
 """
 

@@ -27,7 +27,7 @@ import kfvm_abi as abi  # noqa: E402
 import refrun  # noqa: E402
 
 # (case, workload, grid per axis, accepted steps, wenothresh override or None,
-#  Gauss points, reference problem build)
+#  Gauss points, reference problem build[, wall codes])
 CASES = [
     ("vortex_128_c1", "isentropic_vortex", 128, 20, None, 2, None),   # the problem list's C1, as stated
     ("sod3d_24", "sod3d", 24, 5, None, 2, None),
@@ -38,15 +38,21 @@ CASES = [
     ("orszag_tang_3d_16", "orszag_tang_3d", 16, 3, None, 2, None),   # 3D GLM-MHD sources at Q^3 points
     ("orszag_tang_3d_q3_12", "orszag_tang_3d", 12, 2, None, 3, "orszag_tang_3d_q3"),  # three points
     ("sr_riemann_2d_32", "sr_riemann_2d", 32, 4, None, 2, None),      # special-relativistic hydro
+    # walls (codes west east south north bottom top: r reflecting, n no-slip, p periodic)
+    ("sod3d_reflecting_16", "sod3d", 16, 3, None, 2, "sod3d_reflecting", "rrrrrr"),
+    ("taylor_green_noslip_12", "taylor_green", 12, 3, None, 2, "taylor_green_noslip", "ppnnpp"),
 ]
+WALLS = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC}
 
 
-def case_config(workload, scale, steps, thresh, nq=2):
+def case_config(workload, scale, steps, thresh, nq=2, walls=""):
     cfg, ic = abi.workload(workload, scale=scale, steps=steps)
     if thresh is not None:
         cfg.weno_thresh = abi.stof(thresh)
         cfg.indicator = abi.KFVM_IND_ALL if thresh < 0 else abi.KFVM_IND_KXRCF
     cfg.nq = nq
+    for f, w in enumerate(walls):
+        cfg.bc[f] = WALLS[w]
     return cfg, ic
 
 
@@ -57,13 +63,14 @@ def main():
     build_ref.build_all(sys.argv[1], sorted({c[6] or c[1] for c in cases}))
     out = os.path.join(HERE, "ref")
     os.makedirs(out, exist_ok=True)
-    for case, workload, scale, steps, thresh, nq, problem in cases:
-        cfg, ic = case_config(workload, scale, steps, thresh, nq)
+    for case, workload, scale, steps, thresh, nq, problem, *walls in cases:
+        walls = walls[0] if walls else ""
+        cfg, ic = case_config(workload, scale, steps, thresh, nq, walls)
         cks, _ = refrun.run(problem or workload, cfg, steps)
         assert len(cks) == steps + 1, (case, len(cks))
         np.savez_compressed(
             os.path.join(out, case + ".npz"),
-            workload=workload, scale=scale, steps=steps, nq=nq,
+            workload=workload, scale=scale, steps=steps, nq=nq, walls=walls,
             weno_thresh=np.nan if thresh is None else thresh,
             times=np.array([c[1] for c in cks]), dts=np.array([c[2] for c in cks]),
             weno_counts=np.array([int((c[4][0] > 0).sum()) for c in cks]),
