@@ -169,6 +169,14 @@ PROBLEMS = {
     "sod3d_reflecting": (3, "Hydro", "HLLC", "SSP4_3_2", 2, ("reflecting",) * 6, False, IC_SOD),
     "taylor_green_noslip": (3, "NavierStokes", "HLLC", "SSP4_3_2", 2,
                             ("periodic", "periodic", "noslip", "noslip", "periodic", "periodic"), False, IC_TGV),
+    # the other Runge-Kutta schemes, Riemann solvers and the three-point rule in 2D
+    "sod3d_ssp10": (3, "Hydro", "HLLC", "SSP10_4_3", 2, "outflow", False, IC_SOD),
+    "vortex_threestar": (2, "Hydro", "HLLC", "ThreeStarP", 2, "periodic", False, IC_VORTEX),
+    "sod3d_fourstar": (3, "Hydro", "HLLC", "FourStarP", 2, "outflow", False, IC_SOD),
+    "kelvin_helmholtz_hll": (2, "Hydro", "HLL", "SSP4_3_2", 2, "periodic", False, IC_KH),
+    "kelvin_helmholtz_q3": (2, "Hydro", "HLLC", "SSP4_3_2", 3, "periodic", False, IC_KH),
+    "sod3d_llf": (3, "Hydro", "LLF", "SSP4_3_2", 2, "outflow", False, IC_SOD),
+    "orszag_tang_llf": (2, "MHD_GLM", "LLF", "SSP4_3_2", 2, "periodic", True, IC_OT),
 }
 
 

@@ -27,7 +27,7 @@ import kfvm_abi as abi  # noqa: E402
 import refrun  # noqa: E402
 
 # (case, workload, grid per axis, accepted steps, wenothresh override or None,
-#  Gauss points, reference problem build[, wall codes])
+#  Gauss points, reference problem build[, wall codes[, configuration overrides]])
 CASES = [
     ("vortex_128_c1", "isentropic_vortex", 128, 20, None, 2, None),   # the problem list's C1, as stated
     ("sod3d_24", "sod3d", 24, 5, None, 2, None),
@@ -41,12 +41,26 @@ CASES = [
     # walls (codes west east south north bottom top: r reflecting, n no-slip, p periodic)
     ("sod3d_reflecting_16", "sod3d", 16, 3, None, 2, "sod3d_reflecting", "rrrrrr"),
     ("taylor_green_noslip_12", "taylor_green", 12, 3, None, 2, "taylor_green_noslip", "ppnnpp"),
+    # the other schemes and solvers (Runge-Kutta and Riemann overrides), three points in 2D
+    ("sod3d_ssp10_16", "sod3d", 16, 3, None, 2, "sod3d_ssp10", "", {"rk": abi.KFVM_RK_SSP10_4_3}),
+    ("vortex_threestar_32", "isentropic_vortex", 32, 4, None, 2, "vortex_threestar", "",
+     {"rk": abi.KFVM_RK_THREESTARP}),
+    # (on the vortex at 32^2 the embedded error of SSP(10,4) and FourStarP sits near
+    # the rounding floor, so their step-size proposals are noise; the blast's are not)
+    ("sod3d_fourstar_16", "sod3d", 16, 3, None, 2, "sod3d_fourstar", "", {"rk": abi.KFVM_RK_FOURSTARP}),
+    ("kelvin_helmholtz_hll_32", "kelvin_helmholtz", 32, 5, None, 2, "kelvin_helmholtz_hll", "",
+     {"rs": abi.KFVM_RS_HLL}),
+    ("kelvin_helmholtz_q3_32", "kelvin_helmholtz", 32, 5, None, 3, "kelvin_helmholtz_q3"),
+    ("sod3d_llf_16", "sod3d", 16, 3, None, 2, "sod3d_llf", "", {"rs": abi.KFVM_RS_LLF}),
+    ("orszag_tang_llf_32", "orszag_tang", 32, 5, None, 2, "orszag_tang_llf", "", {"rs": abi.KFVM_RS_LLF}),
 ]
 WALLS = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC}
 
 
-def case_config(workload, scale, steps, thresh, nq=2, walls=""):
+def case_config(workload, scale, steps, thresh, nq=2, walls="", over=None):
     cfg, ic = abi.workload(workload, scale=scale, steps=steps)
+    for key, val in (over or {}).items():   # Runge-Kutta scheme, Riemann solver
+        setattr(cfg, key, val)
     if thresh is not None:
         cfg.weno_thresh = abi.stof(thresh)
         cfg.indicator = abi.KFVM_IND_ALL if thresh < 0 else abi.KFVM_IND_KXRCF
@@ -63,14 +77,15 @@ def main():
     build_ref.build_all(sys.argv[1], sorted({c[6] or c[1] for c in cases}))
     out = os.path.join(HERE, "ref")
     os.makedirs(out, exist_ok=True)
-    for case, workload, scale, steps, thresh, nq, problem, *walls in cases:
-        walls = walls[0] if walls else ""
-        cfg, ic = case_config(workload, scale, steps, thresh, nq, walls)
+    for case, workload, scale, steps, thresh, nq, problem, *extra in cases:
+        walls = extra[0] if extra else ""
+        over = extra[1] if len(extra) > 1 else {}
+        cfg, ic = case_config(workload, scale, steps, thresh, nq, walls, over)
         cks, _ = refrun.run(problem or workload, cfg, steps)
         assert len(cks) == steps + 1, (case, len(cks))
         np.savez_compressed(
             os.path.join(out, case + ".npz"),
-            workload=workload, scale=scale, steps=steps, nq=nq, walls=walls,
+            workload=workload, scale=scale, steps=steps, nq=nq, walls=walls, rk=cfg.rk, rs=cfg.rs,
             weno_thresh=np.nan if thresh is None else thresh,
             times=np.array([c[1] for c in cks]), dts=np.array([c[2] for c in cks]),
             weno_counts=np.array([int((c[4][0] > 0).sum()) for c in cks]),
