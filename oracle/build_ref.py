@@ -177,6 +177,9 @@ PROBLEMS = {
     "kelvin_helmholtz_q3": (2, "Hydro", "HLLC", "SSP4_3_2", 3, "periodic", False, IC_KH),
     "sod3d_llf": (3, "Hydro", "LLF", "SSP4_3_2", 2, "outflow", False, IC_SOD),
     "orszag_tang_llf": (2, "MHD_GLM", "LLF", "SSP4_3_2", 2, "periodic", True, IC_OT),
+    # three Gauss points in 3D for Euler and Navier-Stokes (54 reconstruction rows)
+    "sod3d_q3": (3, "Hydro", "HLLC", "SSP4_3_2", 3, "outflow", False, IC_SOD),
+    "taylor_green_q3": (3, "NavierStokes", "HLLC", "SSP4_3_2", 3, "periodic", False, IC_TGV),
 }
 
 

@@ -53,6 +53,9 @@ CASES = [
     ("kelvin_helmholtz_q3_32", "kelvin_helmholtz", 32, 5, None, 3, "kelvin_helmholtz_q3"),
     ("sod3d_llf_16", "sod3d", 16, 3, None, 2, "sod3d_llf", "", {"rs": abi.KFVM_RS_LLF}),
     ("orszag_tang_llf_32", "orszag_tang", 32, 5, None, 2, "orszag_tang_llf", "", {"rs": abi.KFVM_RS_LLF}),
+    # three points in 3D (54 rows): the blast puts the WENO and limiter paths under test
+    ("sod3d_q3_12", "sod3d", 12, 2, None, 3, "sod3d_q3"),
+    ("taylor_green_q3_10", "taylor_green", 10, 2, None, 3, "taylor_green_q3"),
 ]
 WALLS = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC}
 
