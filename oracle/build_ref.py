@@ -152,6 +152,18 @@ IC_SR_RIEM2D = r"""
   state[4] = rho * W * W * h - p;
 """
 
+# a supersonic inflow through the western face (the kind of boundary the
+# DoubleMach problem writes in its UserBCs.H): rho 1.5, u 1.2, p 1.5 in every
+# halo cell and every outer face point
+INFLOW_STATE = r"""
+  state[0] = 1.5;
+  state[1] = 1.5 * 1.2;
+  state[2] = 0.0;
+  state[3] = 0.0;
+  state[4] = 1.5 / (eosParams.gamma - 1.0) + 0.5 * 1.5 * 1.2 * 1.2;
+"""
+
+
 PROBLEMS = {
     # name: (dim, eq, rs, rk, nq, bc, sources, ic body)
     "isentropic_vortex": (2, "Hydro", "HLLC", "SSP4_3_2", 2, "periodic", False, IC_VORTEX),
@@ -180,7 +192,11 @@ PROBLEMS = {
     # three Gauss points in 3D for Euler and Navier-Stokes (54 reconstruction rows)
     "sod3d_q3": (3, "Hydro", "HLLC", "SSP4_3_2", 3, "outflow", False, IC_SOD),
     "taylor_green_q3": (3, "NavierStokes", "HLLC", "SSP4_3_2", 3, "periodic", False, IC_TGV),
+    # a user boundary: the supersonic inflow through the western face of the blast
+    "sod3d_inflow": (3, "Hydro", "HLLC", "SSP4_3_2", 2, ("user",) + ("outflow",) * 5, False, IC_SOD),
 }
+# user boundary hooks of the problems that have BCType::user faces
+USER_BCS = {"sod3d_inflow": {"CellWest": INFLOW_STATE, "FaceWest": INFLOW_STATE}}
 
 
 def definitions_h(dim, eq, rs, rk, nq):
@@ -262,20 +278,23 @@ struct UserParameters : ParameterStructs {
 """
 
 
-def user_bcs_h():
-    """The twelve user boundary hooks every problem must define; no problem here
-    uses BCType::user, so they are empty."""
+def user_bcs_h(bodies=None):
+    """The twelve user boundary hooks every problem must define; bodies maps a hook
+    name (CellWest, FaceWest, ...) to its code, the others are empty."""
+    bodies = bodies or {}
     out = ["#ifndef USERBCS_H_", "#define USERBCS_H_",
-           "// Empty user boundary hooks (generated by oracle/build_ref.py)"]
+           "// User boundary hooks (generated by oracle/build_ref.py)"]
     for side, (a, b) in (("West", ("j", "k")), ("East", ("j", "k")), ("South", ("i", "k")),
                          ("North", ("i", "k")), ("Bottom", ("i", "j")), ("Top", ("i", "j"))):
         n = {"West": "nX", "East": "nX", "South": "nY", "North": "nY", "Bottom": "nZ", "Top": "nZ"}[side]
+        cell = bodies.get("Cell" + side, f"(void){n}; (void){a}; (void){b}; (void)eosParams; (void)state;")
+        face = bodies.get("Face" + side, f"(void){a}; (void){b}; (void)eosParams; (void)state;")
         out.append(f"""template <class DataViewType>
 KOKKOS_INLINE_FUNCTION void Cell{side}(const DataViewType &, int, int {n}, int {a}, int {b},
-    int, Real, Real, Real, Real, EosParameters, UserParameters, Real[NUM_VARS]) {{ (void){n}; (void){a}; (void){b}; }}
+    int, Real, Real, Real, Real, EosParameters eosParams, UserParameters, Real state[NUM_VARS]) {{ {cell} }}
 template <class DataViewType>
 KOKKOS_INLINE_FUNCTION void Face{side}(const DataViewType &, int {a}, int {b}, int, Real, Real,
-    Real, Real, EosParameters, UserParameters, Real[NUM_VARS]) {{ (void){a}; (void){b}; }}""")
+    Real, Real, EosParameters eosParams, UserParameters, Real state[NUM_VARS]) {{ {face} }}""")
     out.append("#endif")
     return "\n".join(out) + "\n"
 
@@ -339,7 +358,7 @@ def write_problem(name):
         "Definitions.H": definitions_h(dim, eq, rs, rk, nq),
         "InitialCondition.H": initial_condition_h(ic),
         "SourceTerms.H": SOURCE_TERMS_H,
-        "UserBCs.H": user_bcs_h(),
+        "UserBCs.H": user_bcs_h(USER_BCS.get(name)),
         "UserParameters.H": USER_PARAMETERS_H,
         "ProblemSetup.cpp": problem_setup_cpp(bc, sources),
     }

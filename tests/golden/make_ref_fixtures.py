@@ -56,8 +56,13 @@ CASES = [
     # three points in 3D (54 rows): the blast puts the WENO and limiter paths under test
     ("sod3d_q3_12", "sod3d", 12, 2, None, 3, "sod3d_q3"),
     ("taylor_green_q3_10", "taylor_green", 10, 2, None, 3, "taylor_green_q3"),
+    # a user boundary (u): the western inflow of oracle/build_ref.py's sod3d_inflow
+    ("sod3d_inflow_16", "sod3d", 16, 3, None, 2, "sod3d_inflow", "uooooo"),
 ]
-WALLS = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC}
+WALLS = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC,
+         "o": abi.KFVM_BC_OUTFLOW, "u": abi.KFVM_BC_USER}
+# the state the user boundary of the sod3d_inflow build sets (rho 1.5, u 1.2, p 1.5)
+INFLOW = {"sod3d_inflow": (1.5, 1.2, 1.5)}
 
 
 def case_config(workload, scale, steps, thresh, nq=2, walls="", over=None):
@@ -85,10 +90,12 @@ def main():
         over = extra[1] if len(extra) > 1 else {}
         cfg, ic = case_config(workload, scale, steps, thresh, nq, walls, over)
         cks, _ = refrun.run(problem or workload, cfg, steps)
+        inflow = INFLOW.get(problem, ())
         assert len(cks) == steps + 1, (case, len(cks))
         np.savez_compressed(
             os.path.join(out, case + ".npz"),
             workload=workload, scale=scale, steps=steps, nq=nq, walls=walls, rk=cfg.rk, rs=cfg.rs,
+            inflow=np.array(inflow, dtype=np.float64),
             weno_thresh=np.nan if thresh is None else thresh,
             times=np.array([c[1] for c in cks]), dts=np.array([c[2] for c in cks]),
             weno_counts=np.array([int((c[4][0] > 0).sum()) for c in cks]),

@@ -29,12 +29,25 @@ def config(fx):
         if key in fx:
             setattr(cfg, key, int(fx[key]))
     for f, w in enumerate(str(fx["walls"]) if "walls" in fx else ""):
-        cfg.bc[f] = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC}[w]
+        cfg.bc[f] = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC,
+                     "o": abi.KFVM_BC_OUTFLOW, "u": abi.KFVM_BC_USER}[w]
     th = float(fx["weno_thresh"])
     if not np.isnan(th):
         cfg.weno_thresh = abi.stof(th)
         cfg.indicator = abi.KFVM_IND_ALL if th < 0 else abi.KFVM_IND_KXRCF
     return cfg, ic
+
+
+def install_user_bc(solver, fx, cfg):
+    """The user boundary a fixture's reference build had (its hooks set a fixed
+    inflow state rho, u, p on the faces marked u), as the same callback."""
+    if "inflow" not in fx or len(fx["inflow"]) == 0:
+        return
+    import userbc
+    rho, u, p = (float(x) for x in fx["inflow"])
+    state = [rho, rho * u, 0.0, 0.0, p / (cfg.gamma - 1.0) + 0.5 * rho * u * u]
+    nqf = cfg.nq * cfg.nq if cfg.dim == 3 else cfg.nq
+    solver.set_user_bc(userbc.inflow(state, nqf, 5))
 
 
 def replay(solver, fx):

@@ -24,6 +24,7 @@ def test_cuda_path_matches_reference(path, gpu, product_lib):
     fx = refpin.load(path)
     cfg, ic = refpin.config(fx)
     g = product_lib.Solver(cfg)
+    refpin.install_user_bc(g, fx, cfg)
     g.init_ic(ic)
     err0 = refpin.rel_l1(g.get_state().sum(axis=1, keepdims=True), fx["sums"][0][:, None])
     assert np.all(err0 <= 1e-14), err0

@@ -28,6 +28,7 @@ def test_oracle_matches_reference_bitwise(path, oracle_lib):
     fx = refpin.load(path)
     cfg, ic = refpin.config(fx)
     o = oracle_lib.OracleSolver(cfg)
+    refpin.install_user_bc(o, fx, cfg)
     o.init_ic(ic)
     # the initial condition: the reference's first checkpoint
     u0 = o.get_state()
