@@ -164,6 +164,19 @@ INFLOW_STATE = r"""
 """
 
 
+IC_SR_SHOCK_TUBE = r"""
+  (void)y; (void)z; (void)userParams;
+  // the repository's relativistic shock tube: a dense hot slab for x < 0.5 at rest
+  const Real gR = eosParams.gamma / (eosParams.gamma - 1.0), ax = std::fabs(x), W = 1.0;
+  const Real rho = ax < 0.5 ? 10.0 : 1.0, p = ax < 0.5 ? 40.0 / 3.0 : 1.e-6;
+  const Real h = 1.0 + p * gR / rho;
+  state[0] = rho * W;
+  state[1] = 0.0;
+  state[2] = 0.0;
+  state[3] = 0.0;
+  state[4] = rho * h * W * W - p;
+"""
+
 PROBLEMS = {
     # name: (dim, eq, rs, rk, nq, bc, sources, ic body)
     "isentropic_vortex": (2, "Hydro", "HLLC", "SSP4_3_2", 2, "periodic", False, IC_VORTEX),
@@ -194,6 +207,15 @@ PROBLEMS = {
     "taylor_green_q3": (3, "NavierStokes", "HLLC", "SSP4_3_2", 3, "periodic", False, IC_TGV),
     # a user boundary: the supersonic inflow through the western face of the blast
     "sod3d_inflow": (3, "Hydro", "HLLC", "SSP4_3_2", 2, ("user",) + ("outflow",) * 5, False, IC_SOD),
+    # 2D walls (reflecting y faces) for Euler and GLM-MHD, and SR in 3D with HLL
+    "kelvin_helmholtz_reflect": (2, "Hydro", "HLLC", "SSP4_3_2", 2,
+                                 ("periodic", "periodic", "reflecting", "reflecting", "periodic", "periodic"),
+                                 False, IC_KH),
+    "orszag_tang_reflect": (2, "MHD_GLM", "HLL", "SSP4_3_2", 2,
+                            ("periodic", "periodic", "reflecting", "reflecting", "periodic", "periodic"),
+                            True, IC_OT),
+    "sr_shock_tube": (3, "SRHydro", "HLL", "SSP4_3_2", 2, ("outflow", "outflow") + ("periodic",) * 4, False,
+                      IC_SR_SHOCK_TUBE),
 }
 # user boundary hooks of the problems that have BCType::user faces
 USER_BCS = {"sod3d_inflow": {"CellWest": INFLOW_STATE, "FaceWest": INFLOW_STATE}}

@@ -58,6 +58,9 @@ CASES = [
     ("taylor_green_q3_10", "taylor_green", 10, 2, None, 3, "taylor_green_q3"),
     # a user boundary (u): the western inflow of oracle/build_ref.py's sod3d_inflow
     ("sod3d_inflow_16", "sod3d", 16, 3, None, 2, "sod3d_inflow", "uooooo"),
+    ("kelvin_helmholtz_reflect_32", "kelvin_helmholtz", 32, 4, None, 2, "kelvin_helmholtz_reflect", "pprrpp"),
+    ("orszag_tang_reflect_32", "orszag_tang", 32, 4, None, 2, "orszag_tang_reflect", "pprrpp"),
+    ("sr_shock_tube_64", "sr_shock_tube", 64, 3, None, 2, None),       # 64 x 4 x 4, HLL
 ]
 WALLS = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC,
          "o": abi.KFVM_BC_OUTFLOW, "u": abi.KFVM_BC_USER}
