@@ -216,6 +216,8 @@ PROBLEMS = {
                             True, IC_OT),
     "sr_shock_tube": (3, "SRHydro", "HLL", "SSP4_3_2", 2, ("outflow", "outflow") + ("periodic",) * 4, False,
                       IC_SR_SHOCK_TUBE),
+    # Navier-Stokes in 2D (the two-dimensional viscous terms) on the shear layers
+    "kelvin_helmholtz_ns": (2, "NavierStokes", "HLLC", "SSP4_3_2", 2, "periodic", False, IC_KH),
 }
 # user boundary hooks of the problems that have BCType::user faces
 USER_BCS = {"sod3d_inflow": {"CellWest": INFLOW_STATE, "FaceWest": INFLOW_STATE}}

@@ -61,6 +61,8 @@ CASES = [
     ("kelvin_helmholtz_reflect_32", "kelvin_helmholtz", 32, 4, None, 2, "kelvin_helmholtz_reflect", "pprrpp"),
     ("orszag_tang_reflect_32", "orszag_tang", 32, 4, None, 2, "orszag_tang_reflect", "pprrpp"),
     ("sr_shock_tube_64", "sr_shock_tube", 64, 3, None, 2, None),       # 64 x 4 x 4, HLL
+    ("kelvin_helmholtz_ns_32", "kelvin_helmholtz", 32, 4, None, 2, "kelvin_helmholtz_ns", "",
+     {"eq": abi.KFVM_EQ_NAVIERSTOKES, "reynolds": abi.stof(1000.0), "prandtl": abi.stof(0.71)}),
 ]
 WALLS = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC,
          "o": abi.KFVM_BC_OUTFLOW, "u": abi.KFVM_BC_USER}
@@ -98,6 +100,7 @@ def main():
         np.savez_compressed(
             os.path.join(out, case + ".npz"),
             workload=workload, scale=scale, steps=steps, nq=nq, walls=walls, rk=cfg.rk, rs=cfg.rs,
+            eq=cfg.eq, reynolds=cfg.reynolds, prandtl=cfg.prandtl,
             inflow=np.array(inflow, dtype=np.float64),
             weno_thresh=np.nan if thresh is None else thresh,
             times=np.array([c[1] for c in cks]), dts=np.array([c[2] for c in cks]),

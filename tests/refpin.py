@@ -25,9 +25,12 @@ def config(fx):
     cfg, ic = abi.workload(str(fx["workload"]), scale=int(fx["scale"]), steps=int(fx["steps"]))
     if "nq" in fx:
         cfg.nq = int(fx["nq"])
-    for key in ("rk", "rs"):   # the Runge-Kutta scheme and Riemann solver of the run
+    for key in ("rk", "rs", "eq"):   # the Runge-Kutta scheme, Riemann solver, equations of the run
         if key in fx:
             setattr(cfg, key, int(fx[key]))
+    for key in ("reynolds", "prandtl"):
+        if key in fx:
+            setattr(cfg, key, float(fx[key]))
     for f, w in enumerate(str(fx["walls"]) if "walls" in fx else ""):
         cfg.bc[f] = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC,
                      "o": abi.KFVM_BC_OUTFLOW, "u": abi.KFVM_BC_USER}[w]
