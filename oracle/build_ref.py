@@ -218,6 +218,13 @@ PROBLEMS = {
                       IC_SR_SHOCK_TUBE),
     # Navier-Stokes in 2D (the two-dimensional viscous terms) on the shear layers
     "kelvin_helmholtz_ns": (2, "NavierStokes", "HLLC", "SSP4_3_2", 2, "periodic", False, IC_KH),
+    # the remaining wall combinations: no-slip for Euler, reflecting for Navier-Stokes,
+    # reflecting z walls for 3D GLM-MHD
+    "sod3d_noslip": (3, "Hydro", "HLLC", "SSP4_3_2", 2, ("noslip",) * 6, False, IC_SOD),
+    "taylor_green_reflect": (3, "NavierStokes", "HLLC", "SSP4_3_2", 2,
+                             ("reflecting",) * 2 + ("periodic",) * 4, False, IC_TGV),
+    "orszag_tang_3d_reflect": (3, "MHD_GLM", "HLL", "SSP4_3_2", 2, ("periodic",) * 4 + ("reflecting",) * 2,
+                               True, IC_OT),
 }
 # user boundary hooks of the problems that have BCType::user faces
 USER_BCS = {"sod3d_inflow": {"CellWest": INFLOW_STATE, "FaceWest": INFLOW_STATE}}

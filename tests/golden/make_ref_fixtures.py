@@ -63,6 +63,9 @@ CASES = [
     ("sr_shock_tube_64", "sr_shock_tube", 64, 3, None, 2, None),       # 64 x 4 x 4, HLL
     ("kelvin_helmholtz_ns_32", "kelvin_helmholtz", 32, 4, None, 2, "kelvin_helmholtz_ns", "",
      {"eq": abi.KFVM_EQ_NAVIERSTOKES, "reynolds": abi.stof(1000.0), "prandtl": abi.stof(0.71)}),
+    ("sod3d_noslip_16", "sod3d", 16, 3, None, 2, "sod3d_noslip", "nnnnnn"),
+    ("taylor_green_reflect_12", "taylor_green", 12, 3, None, 2, "taylor_green_reflect", "rrpppp"),
+    ("orszag_tang_3d_reflect_16", "orszag_tang_3d", 16, 2, None, 2, "orszag_tang_3d_reflect", "pppprr"),
 ]
 WALLS = {"r": abi.KFVM_BC_REFLECTING, "n": abi.KFVM_BC_NOSLIP, "p": abi.KFVM_BC_PERIODIC,
          "o": abi.KFVM_BC_OUTFLOW, "u": abi.KFVM_BC_USER}
