@@ -72,3 +72,24 @@ def test_oracle_matches_reference_build(name, scale, steps, oracle_lib):
         o.set_time(cks[n - 1][1], cks[1][1] if n == 1 else cks[n - 1][2])
         o.take_step()
         np.testing.assert_array_equal(o.get_state(), cks[n][3])
+
+
+def test_fixtures_cover_the_path():
+    """Between them the reference's own runs cover every equation system, Riemann
+    solver, Runge-Kutta scheme, Gauss-point count and boundary type of the path."""
+    import kfvm_abi as abi
+    eqs, rss, rks, nqs, bcs, dims = set(), set(), set(), set(), set(), set()
+    for path in FIXTURES:
+        cfg, _ = refpin.config(refpin.load(path))
+        eqs.add(cfg.eq)
+        rss.add(cfg.rs)
+        rks.add(cfg.rk)
+        nqs.add(cfg.nq)
+        dims.add(cfg.dim)
+        bcs.update(cfg.bc[f] for f in range(2 * cfg.dim))
+    assert eqs == {abi.KFVM_EQ_HYDRO, abi.KFVM_EQ_NAVIERSTOKES, abi.KFVM_EQ_MHD_GLM, abi.KFVM_EQ_SRHYDRO}
+    assert rss == {abi.KFVM_RS_LLF, abi.KFVM_RS_HLL, abi.KFVM_RS_HLLC}
+    assert rks == {abi.KFVM_RK_THREESTARP, abi.KFVM_RK_FOURSTARP, abi.KFVM_RK_SSP4_3_2, abi.KFVM_RK_SSP10_4_3}
+    assert nqs == {2, 3} and dims == {2, 3}
+    assert bcs == {abi.KFVM_BC_PERIODIC, abi.KFVM_BC_OUTFLOW, abi.KFVM_BC_REFLECTING, abi.KFVM_BC_NOSLIP,
+                   abi.KFVM_BC_USER}
